@@ -1,0 +1,307 @@
+"""Python binding of libasohf_gpu.so (ctypes) -- the host mirror of the
+reference's subroutine interface for the particle hot path.
+
+``Asohf`` owns one library context (device, CUDA stream, device particle
+store).  Its methods are named after the reference subroutines they replace
+and take numpy arrays (host: the library stages them) or torch CUDA tensors
+(device: no copies).  There is no CPU fallback: without the built library or
+a CUDA device every call raises.
+
+``GpuBackend`` adapts ``Asohf`` to the method set the hot-path driver
+(asohf_b200.driver) uses.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_LIB = None
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_vp = C.c_void_p
+
+
+class AsohfError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        detail = ""
+        if _LIB is not None and code == 2:
+            detail = ": " + _LIB.asohf_last_error_detail().decode()
+        super().__init__(f"{what}: {abi.ERRORS.get(code, 'status %d' % code)}{detail}")
+
+
+def lib_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "libasohf_gpu.so")
+
+
+def load():
+    """Loads libasohf_gpu.so; raises if it was not built."""
+    global _LIB
+    if _LIB is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m asohf_b200.build` "
+                               "(the hot path has no CPU fallback)")
+        L = C.CDLL(path)
+        L.asohf_strerror.restype = C.c_char_p
+        L.asohf_last_error_detail.restype = C.c_char_p
+        L.asohf_launch_count.restype = C.c_int64
+        L.asohf_launch_count.argtypes = [_vp]
+        for name in ["asohf_create", "asohf_destroy", "asohf_set_stream", "asohf_synchronize",
+                     "asohf_upload_particles", "asohf_download_particles",
+                     "asohf_sort_dm_particles_localdensity", "asohf_density",
+                     "asohf_renorm_density", "asohf_interpolate_density_tsc", "asohf_poisson_fft",
+                     "asohf_tsc_poisson_forward", "asohf_tsc_poisson_adjoint",
+                     "asohf_sort_dm_particles_x", "asohf_prune_poor_haloes",
+                     "asohf_halofind_particles", "asohf_substructure_particles",
+                     "asohf_get_particles_per_halo"]:
+            getattr(L, name).restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a):
+    """Pointer of a numpy array or torch tensor (contiguous)."""
+    if a is None:
+        return None
+    if _is_torch(a):
+        assert a.is_contiguous()
+        return C.c_void_p(a.data_ptr())
+    assert a.flags.c_contiguous
+    return C.c_void_p(a.ctypes.data)
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise AsohfError(rc, what)
+
+
+class Asohf:
+    """One library context on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.h = C.c_void_p()
+        _check(self.L.asohf_create(C.c_int(device), C.byref(self.h)), "asohf_create")
+        self.device = device
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            self.L.asohf_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        _check(self.L.asohf_set_stream(self.h, C.c_void_p(stream_ptr)), "asohf_set_stream")
+
+    def synchronize(self):
+        _check(self.L.asohf_synchronize(self.h), "asohf_synchronize")
+
+    def launch_count(self) -> int:
+        return int(self.L.asohf_launch_count(self.h))
+
+    # -------------------------------------------------------------- particles
+    def upload_particles(self, x, y, z, vx, vy, vz, m, ids):
+        dev = _is_torch(x) and x.is_cuda
+        p = abi.ParticlesC()
+        p.n = int(x.shape[0])
+        for f, a in zip(["x", "y", "z", "vx", "vy", "vz", "m"], [x, y, z, vx, vy, vz, m]):
+            setattr(p, f, C.cast(_ptr(a), _fp))
+        p.id = C.cast(_ptr(ids), _ip)
+        _check(self.L.asohf_upload_particles(self.h, C.byref(p), C.c_int(int(dev))),
+               "asohf_upload_particles")
+        self.n = p.n
+
+    def download_particles(self, out=None):
+        """Returns (x, y, z, vx, vy, vz, m, id) numpy arrays in store order."""
+        n = self.n
+        if out is None:
+            out = [np.empty(n, np.float32) for _ in range(7)] + [np.empty(n, np.int32)]
+        p = abi.ParticlesC()
+        p.n = n
+        for f, a in zip(["x", "y", "z", "vx", "vy", "vz", "m"], out[:7]):
+            setattr(p, f, C.cast(_ptr(a), _fp))
+        p.id = C.cast(_ptr(out[7]), _ip)
+        dev = _is_torch(out[0])
+        _check(self.L.asohf_download_particles(self.h, C.byref(p), C.c_int(int(dev))),
+               "asohf_download_particles")
+        return out
+
+    # -------------------------------------------------------------- mesh stage
+    def sort_dm_particles_localdensity(self, nx, dx, rodo, re0):
+        """SORT_DM_PARTICLES_LOCALDENSITY (reader.f:140-336)."""
+        npe = np.zeros(abi.N_ESP, np.int32)
+        _check(self.L.asohf_sort_dm_particles_localdensity(
+            self.h, C.c_int(nx), C.c_float(dx), C.c_float(rodo), C.c_float(re0),
+            npe.ctypes.data_as(_ip)), "SORT_DM_PARTICLES_LOCALDENSITY")
+        return npe
+
+    def density(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, u1, u11):
+        """DENSITY (grids.f:710-994) into u1 (NX^3) and u11 (P x 32^3)."""
+        mh = abi.MeshHolder(mesh)
+        dev = _is_torch(u1)
+        npe = np.ascontiguousarray(npart_esp, np.int32)
+        _check(self.L.asohf_density(self.h, C.c_int(nx), C.c_float(lado0), C.c_float(dx),
+                                    C.c_float(rote), C.c_float(rete), npe.ctypes.data_as(_ip),
+                                    C.byref(mh.c), C.c_int(interp_degree), _ptr(u1), _ptr(u11),
+                                    C.c_int(int(dev))), "DENSITY")
+
+    def renorm_density(self, nx, mesh, fdm, u1, u11):
+        """RENORM_DENSITY (grids.f:2668-2722), in place."""
+        mh = abi.MeshHolder(mesh)
+        _check(self.L.asohf_renorm_density(self.h, C.c_int(nx), C.byref(mh.c), C.c_float(fdm),
+                                           _ptr(u1), _ptr(u11), C.c_int(int(_is_torch(u1)))),
+               "RENORM_DENSITY")
+
+    def interpolate_density_tsc(self, nx, lado0, dx, radx, rote, rete, mesh, u1, u11):
+        """INTERPOLATE_DENSITY_TSC (grids.f:1070-1398)."""
+        mh = abi.MeshHolder(mesh)
+        r = np.ascontiguousarray(radx, np.float32)
+        _check(self.L.asohf_interpolate_density_tsc(
+            self.h, C.c_int(nx), C.c_float(lado0), C.c_float(dx), r.ctypes.data_as(_fp),
+            C.c_float(rote), C.c_float(rete), C.byref(mh.c), _ptr(u1), _ptr(u11),
+            C.c_int(int(_is_torch(u1)))), "INTERPOLATE_DENSITY_TSC")
+
+    def poisson_fft(self, nx, dx, rho, pot, batch=1):
+        """MOMENTO + POFFT3D (poisson.f:98-249)."""
+        _check(self.L.asohf_poisson_fft(self.h, C.c_int(nx), C.c_float(dx), C.c_int(batch),
+                                        _ptr(rho), _ptr(pot), C.c_int(int(_is_torch(rho)))),
+               "POFFT3D")
+
+    def tsc_poisson_forward(self, nx, lado0, dx, radx, rote, rete, x, y, z, m, rho, pot, batch):
+        r = np.ascontiguousarray(radx, np.float32)
+        n_per = int(x.numel()) // batch
+        _check(self.L.asohf_tsc_poisson_forward(
+            self.h, C.c_int(nx), C.c_float(lado0), C.c_float(dx), r.ctypes.data_as(_fp),
+            C.c_float(rote), C.c_float(rete), C.c_int(batch), C.c_int64(n_per), _ptr(x), _ptr(y),
+            _ptr(z), _ptr(m), _ptr(rho), _ptr(pot)), "deposit+Poisson forward")
+
+    def tsc_poisson_adjoint(self, nx, lado0, dx, radx, rote, rete, x, y, z, m, w, gx, gy, gz, gm,
+                            batch):
+        r = np.ascontiguousarray(radx, np.float32)
+        n_per = int(x.numel()) // batch
+        _check(self.L.asohf_tsc_poisson_adjoint(
+            self.h, C.c_int(nx), C.c_float(lado0), C.c_float(dx), r.ctypes.data_as(_fp),
+            C.c_float(rote), C.c_float(rete), C.c_int(batch), C.c_int64(n_per), _ptr(x), _ptr(y),
+            _ptr(z), _ptr(m), _ptr(w), _ptr(gx), _ptr(gy), _ptr(gz), _ptr(gm)),
+            "deposit+Poisson adjoint")
+
+    # -------------------------------------------------------------- halo stage
+    def sort_dm_particles_x(self, nx, lado0):
+        """SORT_DM_PARTICLES_X (grids.f:2726-2838); returns NDMPART_X(0:NX)."""
+        nd = np.zeros(nx + 1, np.int32)
+        _check(self.L.asohf_sort_dm_particles_x(self.h, C.c_int(nx), C.c_float(lado0),
+                                                nd.ctypes.data_as(_ip)), "SORT_DM_PARTICLES_X")
+        return nd
+
+    def prune_poor_haloes(self, consts, cat, low1, low2, facrad, do_need_to_count):
+        cc = cat.as_c()
+        _check(self.L.asohf_prune_poor_haloes(self.h, C.byref(consts), C.byref(cc), C.c_int(low1),
+                                              C.c_int(low2), C.c_float(facrad),
+                                              C.c_int(do_need_to_count), C.c_int(0)),
+               "PRUNE_POOR_HALOES")
+
+    def halofind_particles(self, consts, mesh, cat, low1, low2):
+        mh = abi.MeshHolder(mesh)
+        cc = cat.as_c()
+        _check(self.L.asohf_halofind_particles(self.h, C.byref(consts), C.byref(mh.c), C.byref(cc),
+                                               C.c_int(low1), C.c_int(low2), C.c_int(0)),
+               "HALOFIND_PARTICLES")
+
+    def substructure_particles(self, consts, mesh, cat, ir, subs_lev):
+        mh = abi.MeshHolder(mesh)
+        cc = cat.as_c()
+        sl = np.ascontiguousarray(subs_lev, np.int32)
+        _check(self.L.asohf_substructure_particles(self.h, C.byref(consts), C.byref(mh.c),
+                                                   C.byref(cc), C.c_int(ir), sl.ctypes.data_as(_ip),
+                                                   C.c_int(0)), "SUBSTRUCTURE_PARTICLES")
+
+    def particles_per_halo(self) -> np.ndarray:
+        n = C.c_int64()
+        _check(self.L.asohf_get_particles_per_halo(self.h, None, C.c_int64(0), C.byref(n), C.c_int(0)),
+               "PARTICLES_PER_HALO")
+        out = np.zeros(max(n.value, 1), np.int32)
+        _check(self.L.asohf_get_particles_per_halo(self.h, out.ctypes.data_as(_ip),
+                                                   C.c_int64(out.shape[0]), C.byref(n), C.c_int(0)),
+               "PARTICLES_PER_HALO")
+        return out[: n.value]
+
+
+class GpuBackend:
+    """Backend of asohf_b200.driver on the B200 library (host arrays)."""
+
+    name = "gpu"
+
+    def __init__(self, device: int = 0):
+        self.a = Asohf(device)
+
+    def upload(self, parts):
+        self.a.upload_particles(parts.x, parts.y, parts.z, parts.vx, parts.vy, parts.vz, parts.m,
+                                parts.id)
+
+    def download(self):
+        from types import SimpleNamespace
+        x, y, z, vx, vy, vz, m, i = self.a.download_particles()
+        return SimpleNamespace(x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m, id=i, n=x.shape[0])
+
+    def species_sort(self, nx, dx, rodo, re0):
+        return self.a.sort_dm_particles_localdensity(nx, dx, rodo, re0)
+
+    def density(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree=2, fp64=True):
+        u1 = np.zeros(nx ** 3, np.float32)
+        u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)
+        self.a.density(nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, u1, u11)
+        return u1.reshape(nx, nx, nx), u11[: mesh.total]
+
+    def renorm_density(self, nx, mesh, fdm, u1, u11):
+        u1 = np.ascontiguousarray(u1, np.float32).copy()
+        u11 = np.ascontiguousarray(u11, np.float32).copy()
+        if u11.shape[0] == 0:
+            u11 = np.zeros((1, abi.NAMRX ** 3), np.float32)
+        self.a.renorm_density(nx, mesh, fdm, u1, u11)
+        return u1, u11[: mesh.total]
+
+    def tsc_deposit(self, nx, lado0, dx, radx, rote, rete, mesh, fp64=True):
+        u1 = np.zeros(nx ** 3, np.float32)
+        u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)
+        self.a.interpolate_density_tsc(nx, lado0, dx, radx, rote, rete, mesh, u1, u11)
+        return u1.reshape(nx, nx, nx), u11[: mesh.total]
+
+    def sort_x(self, nx, lado0):
+        return self.a.sort_dm_particles_x(nx, lado0)
+
+    def prune_poor_haloes(self, consts, cat, low1, low2, facrad, do_need_to_count):
+        self.a.prune_poor_haloes(consts, cat, low1, low2, facrad, do_need_to_count)
+
+    def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
+        self.a.halofind_particles(consts, mesh, cat, low1, low2)
+        ids = self.a.particles_per_halo()
+        pph[: ids.shape[0]] = ids
+        return ids.shape[0]
+
+    def substructure_particles(self, consts, mesh, cat, ir, subs_lev, pph):
+        self.a.substructure_particles(consts, mesh, cat, ir, subs_lev)
+        ids = self.a.particles_per_halo()
+        pph[: ids.shape[0]] = ids
+        return ids.shape[0]
+
+    def poisson_fft(self, u1, dx):
+        nx = u1.shape[0]
+        u1 = np.ascontiguousarray(u1, np.float32)
+        pot = np.zeros_like(u1)
+        self.a.poisson_fft(nx, dx, u1, pot)
+        return pot

@@ -1,0 +1,239 @@
+// common.cuh -- internals shared by the sm_100a kernels of libasohf_gpu.so:
+// status handling, the per-caller context (stream, device particle store,
+// scratch arena) and warp/block reduction helpers.
+//
+// Every kernel that restates a reference statement is compiled with
+// -fmad=false, so a*b+c keeps two roundings like the Fortran it restates;
+// sqrtf and '/' are IEEE (nvcc's -prec-sqrt / -prec-div defaults).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/asohf_gpu.h"
+
+#define ASOHF_CUDA(call)                                                   \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      asohf_set_last_cuda_error(e_, #call, __FILE__, __LINE__);            \
+      return ASOHF_ERR_CUDA;                                               \
+    }                                                                      \
+  } while (0)
+
+#define ASOHF_CHECK(rc_expr)      \
+  do {                            \
+    int rc_ = (rc_expr);          \
+    if (rc_ != ASOHF_OK) return rc_; \
+  } while (0)
+
+void asohf_set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+// Device particle store owned by the context (SoA, MODULE PARTICLES order).
+struct DevParticles {
+  int64_t n = 0, cap = 0;
+  float *x = nullptr, *y = nullptr, *z = nullptr;
+  float *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  float *m = nullptr;
+  int32_t* id = nullptr;
+};
+
+struct asohf_ctx {
+  int device = 0;
+  cudaStream_t stream = 0;
+  int num_sms = 148;
+  DevParticles p;      // current store
+  DevParticles alt;    // second buffer set for permutations
+  float norma = 0.f;   // MAXVAL(MASAP), refreshed on upload
+  float mmin = 0.f;
+  // x-slab index (SORT_DM_PARTICLES_X) and the column index built from it
+  int nx_sorted = 0;
+  int32_t* d_ndmpart_x = nullptr;   // NX+1 entries
+  int64_t ncols = 0;                // columns of the (y,z) index
+  float col_xl = 0.f, col_dx = 0.f;
+  int col_n = 0;                    // columns per axis
+  int64_t* d_colstart = nullptr;    // ncols+1
+  float4* d_colpart = nullptr;      // (x, y, z, position in x-sorted store as int bits)
+  int64_t colpart_cap = 0;
+  // bound-particle ID stream (PARTICLES_PER_HALO)
+  int32_t* d_pph = nullptr;
+  int64_t pph_len = 0, pph_cap = 0;
+  // scratch arena (bump allocator, reset at the start of every entry point)
+  char* arena = nullptr;
+  size_t arena_size = 0, arena_used = 0;
+  // per-halo segment buffers (keys, distances, potentials...), grown between
+  // kernel phases of one call, when the stream is idle
+  char* seg = nullptr;
+  size_t seg_size = 0, seg_used = 0;
+  // counters of kernels launched by this context (reported by the bench)
+  int64_t launches = 0;
+};
+
+// Scratch: reserve() may grow the arena only when nothing is allocated from it.
+int arena_reserve(asohf_ctx* c, size_t bytes);
+void* arena_alloc(asohf_ctx* c, size_t bytes);  // 256-byte aligned, nullptr if full
+inline void arena_reset(asohf_ctx* c) { c->arena_used = 0; }
+
+// Segment buffer: reserve() syncs the stream and regrows it (contents lost).
+int seg_reserve(asohf_ctx* c, size_t bytes);
+void* seg_alloc(asohf_ctx* c, size_t bytes);
+
+int ctx_ensure_particles(asohf_ctx* c, int64_t n);
+void ctx_swap_particles(asohf_ctx* c);
+int ctx_refresh_mass_range(asohf_ctx* c);
+
+inline int grid_for(int64_t n, int block, int max_blocks = 148 * 32) {
+  int64_t g = (n + block - 1) / block;
+  if (g > max_blocks) g = max_blocks;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_sum_i(int v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of a double, result valid in every thread.  sbuf >= 32 doubles.
+__device__ __forceinline__ double block_sum_d(double v, double* sbuf) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum_d(v);
+  __syncthreads();
+  if (lane == 0) sbuf[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (wid == 0) {
+    t = lane < nw ? sbuf[lane] : 0.0;
+    t = warp_sum_d(t);
+    if (lane == 0) sbuf[0] = t;
+  }
+  __syncthreads();
+  t = sbuf[0];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ long long block_sum_ll(long long v, long long* sbuf) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) sbuf[wid] = v;
+  __syncthreads();
+  long long t = 0;
+  if (wid == 0) {
+    t = lane < nw ? sbuf[lane] : 0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sbuf[0] = t;
+  }
+  __syncthreads();
+  t = sbuf[0];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ long long block_min_ll(long long v, long long* sbuf) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    long long w = __shfl_down_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
+  }
+  __syncthreads();
+  if (lane == 0) sbuf[wid] = v;
+  __syncthreads();
+  long long t = LLONG_MAX;
+  if (wid == 0) {
+    t = lane < nw ? sbuf[lane] : LLONG_MAX;
+    for (int o = 16; o > 0; o >>= 1) {
+      long long w = __shfl_down_sync(0xffffffffu, t, o);
+      t = w < t ? w : t;
+    }
+    if (lane == 0) sbuf[0] = t;
+  }
+  __syncthreads();
+  t = sbuf[0];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float block_max_f(float v, float* sbuf) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) sbuf[wid] = v;
+  __syncthreads();
+  float t = -INFINITY;
+  if (wid == 0) {
+    t = lane < nw ? sbuf[lane] : -INFINITY;
+    for (int o = 16; o > 0; o >>= 1) t = fmaxf(t, __shfl_down_sync(0xffffffffu, t, o));
+    if (lane == 0) sbuf[0] = t;
+  }
+  __syncthreads();
+  t = sbuf[0];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float block_min_f(float v, float* sbuf) {
+  return -block_max_f(-v, sbuf);
+}
+
+// Inclusive block scan of ints; returns the inclusive prefix; *total gets the
+// block total.  sbuf >= 33 ints.
+__device__ __forceinline__ int block_scan_i(int v, int* sbuf, int* total) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) sbuf[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int s = lane < nw ? sbuf[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) sbuf[lane] = s;
+  }
+  __syncthreads();
+  int off = wid > 0 ? sbuf[wid - 1] : 0;
+  int tot = sbuf[nw - 1];
+  __syncthreads();
+  if (total) *total = tot;
+  return x + off;
+}
+
+// Inclusive block scan of doubles (left-to-right within the block).
+__device__ __forceinline__ double block_scan_d(double v, double* sbuf, double* total) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  double x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    double y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) sbuf[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    double s = lane < nw ? sbuf[lane] : 0.0;
+    for (int o = 1; o < 32; o <<= 1) {
+      double y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) sbuf[lane] = s;
+  }
+  __syncthreads();
+  double off = wid > 0 ? sbuf[wid - 1] : 0.0;
+  double tot = sbuf[nw - 1];
+  __syncthreads();
+  if (total) *total = tot;
+  return x + off;
+}

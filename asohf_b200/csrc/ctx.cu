@@ -1,0 +1,227 @@
+// ctx.cu -- context lifetime, scratch arena, device particle store.
+#include <stdlib.h>
+#include <string.h>
+
+#include "common.cuh"
+
+static char g_last_detail[512] = "";
+
+void asohf_set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  snprintf(g_last_detail, sizeof(g_last_detail), "%s: %s (%s:%d)", cudaGetErrorString(e), what,
+           file, line);
+}
+
+extern "C" const char* asohf_last_error_detail(void) { return g_last_detail; }
+
+extern "C" const char* asohf_strerror(int code) {
+  switch (code) {
+    case ASOHF_OK: return "ok";
+    case ASOHF_ERR_INVALID: return "invalid argument";
+    case ASOHF_ERR_CUDA: return "CUDA error";
+    case ASOHF_ERR_CAPACITY: return "capacity exceeded";
+    case ASOHF_ERR_TIMEOUT: return "device wait timed out";
+    case ASOHF_ERR_NOT_PREFOUND_VIRIAL: return "NOT PRE-FOUND VIRIAL RADIUS!";
+    case ASOHF_ERR_WRONG_SORTING: return "wrong sorting, cannot continue";
+    case ASOHF_ERR_NO_DEVICE: return "no usable CUDA device";
+    case ASOHF_ERR_UNSUPPORTED: return "unsupported option";
+    default: return "unknown status";
+  }
+}
+
+static void free_particles(DevParticles& p) {
+  cudaFree(p.x); cudaFree(p.y); cudaFree(p.z);
+  cudaFree(p.vx); cudaFree(p.vy); cudaFree(p.vz);
+  cudaFree(p.m); cudaFree(p.id);
+  p = DevParticles();
+}
+
+static int alloc_particles(DevParticles& p, int64_t cap) {
+  size_t fb = sizeof(float) * (size_t)cap;
+  ASOHF_CUDA(cudaMalloc(&p.x, fb)); ASOHF_CUDA(cudaMalloc(&p.y, fb)); ASOHF_CUDA(cudaMalloc(&p.z, fb));
+  ASOHF_CUDA(cudaMalloc(&p.vx, fb)); ASOHF_CUDA(cudaMalloc(&p.vy, fb)); ASOHF_CUDA(cudaMalloc(&p.vz, fb));
+  ASOHF_CUDA(cudaMalloc(&p.m, fb));
+  ASOHF_CUDA(cudaMalloc(&p.id, sizeof(int32_t) * (size_t)cap));
+  p.cap = cap;
+  return ASOHF_OK;
+}
+
+int ctx_ensure_particles(asohf_ctx* c, int64_t n) {
+  if (c->p.cap < n) {
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    free_particles(c->p);
+    free_particles(c->alt);
+    ASOHF_CHECK(alloc_particles(c->p, n));
+    ASOHF_CHECK(alloc_particles(c->alt, n));
+  }
+  c->p.n = n;
+  c->alt.n = n;
+  return ASOHF_OK;
+}
+
+void ctx_swap_particles(asohf_ctx* c) {
+  DevParticles t = c->p;
+  c->p = c->alt;
+  c->alt = t;
+}
+
+int arena_reserve(asohf_ctx* c, size_t bytes) {
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (c->arena_size >= bytes) return ASOHF_OK;
+  if (c->arena_used != 0) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(c->arena);
+  c->arena = nullptr;
+  c->arena_size = 0;
+  size_t want = bytes + bytes / 4;
+  ASOHF_CUDA(cudaMalloc(&c->arena, want));
+  c->arena_size = want;
+  return ASOHF_OK;
+}
+
+void* arena_alloc(asohf_ctx* c, size_t bytes) {
+  size_t b = (bytes + 255) & ~(size_t)255;
+  if (c->arena_used + b > c->arena_size) return nullptr;
+  void* p = c->arena + c->arena_used;
+  c->arena_used += b;
+  return p;
+}
+
+int seg_reserve(asohf_ctx* c, size_t bytes) {
+  c->seg_used = 0;
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (c->seg_size >= bytes) return ASOHF_OK;
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(c->seg);
+  c->seg = nullptr;
+  c->seg_size = 0;
+  size_t want = bytes + bytes / 4;
+  ASOHF_CUDA(cudaMalloc(&c->seg, want));
+  c->seg_size = want;
+  return ASOHF_OK;
+}
+
+void* seg_alloc(asohf_ctx* c, size_t bytes) {
+  size_t b = (bytes + 255) & ~(size_t)255;
+  if (c->seg_used + b > c->seg_size) return nullptr;
+  void* p = c->seg + c->seg_used;
+  c->seg_used += b;
+  return p;
+}
+
+__global__ void k_minmax(const float* __restrict__ m, int64_t n, float* out) {
+  __shared__ float sb[32];
+  float lo = INFINITY, hi = -INFINITY;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float v = m[i];
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+  hi = block_max_f(hi, sb);
+  lo = block_min_f(lo, sb);
+  if (threadIdx.x == 0) {
+    // float max/min through ordered int bit patterns (masses are >= 0)
+    atomicMax((int*)&out[1], __float_as_int(hi));
+    atomicMin((int*)&out[0], __float_as_int(lo));
+  }
+}
+
+int ctx_refresh_mass_range(asohf_ctx* c) {
+  float* d = (float*)arena_alloc(c, 2 * sizeof(float));
+  if (!d) return ASOHF_ERR_CAPACITY;
+  float init[2] = {INFINITY, 0.0f};
+  ASOHF_CUDA(cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  k_minmax<<<grid_for(c->p.n, 256, 1024), 256, 0, c->stream>>>(c->p.m, c->p.n, d);
+  c->launches++;
+  float h[2];
+  ASOHF_CUDA(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  c->mmin = h[0];
+  c->norma = h[1];
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_create(int device, asohf_ctx** out) {
+  if (!out) return ASOHF_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    return ASOHF_ERR_NO_DEVICE;
+  ASOHF_CUDA(cudaSetDevice(device));
+  asohf_ctx* c = new asohf_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (arena_reserve(c, 64u << 20) != ASOHF_OK) {
+    delete c;
+    return ASOHF_ERR_CUDA;
+  }
+  *out = c;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_destroy(asohf_ctx* c) {
+  if (!c) return ASOHF_ERR_INVALID;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  free_particles(c->p);
+  free_particles(c->alt);
+  cudaFree(c->d_ndmpart_x);
+  cudaFree(c->d_colstart);
+  cudaFree(c->d_colpart);
+  cudaFree(c->d_pph);
+  cudaFree(c->arena);
+  cudaFree(c->seg);
+  delete c;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_set_stream(asohf_ctx* c, void* s) {
+  if (!c) return ASOHF_ERR_INVALID;
+  c->stream = (cudaStream_t)s;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_synchronize(asohf_ctx* c) {
+  if (!c) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+extern "C" int64_t asohf_launch_count(asohf_ctx* c) { return c ? c->launches : -1; }
+
+extern "C" int asohf_upload_particles(asohf_ctx* c, const asohf_particles* s, int on_device) {
+  if (!c || !s || s->n < 0) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  ASOHF_CHECK(ctx_ensure_particles(c, s->n));
+  cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  size_t fb = sizeof(float) * (size_t)s->n;
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.x, s->x, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.y, s->y, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.z, s->z, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.vx, s->vx, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.vy, s->vy, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.vz, s->vz, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.m, s->m, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(c->p.id, s->id, sizeof(int32_t) * (size_t)s->n, k, c->stream));
+  c->nx_sorted = 0;  // slab table and column index are stale
+  if (s->n > 0) ASOHF_CHECK(ctx_refresh_mass_range(c));
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_download_particles(asohf_ctx* c, asohf_particles* d, int on_device) {
+  if (!c || !d || d->n < c->p.n) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  size_t fb = sizeof(float) * (size_t)c->p.n;
+  ASOHF_CUDA(cudaMemcpyAsync(d->x, c->p.x, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->y, c->p.y, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->z, c->p.z, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->vx, c->p.vx, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->vy, c->p.vy, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->vz, c->p.vz, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->m, c->p.m, fb, k, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(d->id, c->p.id, sizeof(int32_t) * (size_t)c->p.n, k, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}

@@ -1,0 +1,1002 @@
+// deposit.cu -- species sort, kernel deposit (DENSITY), RENORM_DENSITY and
+// the true-TSC deposit (INTERPOLATE_DENSITY_TSC) on sm_100a.
+//
+// Accumulation: every cloud term keeps the reference's REAL*4 expression
+// (BAS*W(i)*W(j)*W(k), left to right).  Terms are summed exactly where the
+// dynamic range allows -- 64-bit fixed point for the base-grid kernel
+// deposit, whose weights are dyadic -- and otherwise in float64, then
+// rounded once to float32.  The result no longer depends on the particle
+// order or thread count, unlike the reference's REDUCTION(+:U1)
+// (grids.f:787-791) whose float32 sum does.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "common.cuh"
+
+#define KW (2 * ASOHF_NMAX_KERNELS + 1)
+
+// ------------------------------------------------------------ host tables
+// COMPUTE_KERNELS (grids.f:997-1067), host side, same REAL*4 arithmetic.
+static void compute_kernels_host(int nl, int deg, float* k /* (NLEVELS+1)*KW */) {
+  memset(k, 0, sizeof(float) * KW * (ASOHF_NLEVELS + 1));
+  for (int ir = 0; ir <= nl; ir++) {
+    int n = 1 << ir;
+    float h32 = (float)n + 0.5f;
+    float h = 2.0f * h32 / 3.0f;
+    float* kk = k + (size_t)ir * KW + ASOHF_NMAX_KERNELS;
+    for (int i = -n; i <= n; i++) {
+      if (deg == 2) {
+        float bas = (float)abs(i) / h;
+        if (bas <= 0.5f) {
+          kk[i] = 0.75f - bas * bas;
+        } else {
+          float t = 1.5f - bas;
+          kk[i] = 0.5f * (t * t);
+        }
+      } else {
+        float bas = (float)abs(i) / h32;
+        kk[i] = 1.0f - bas;
+      }
+    }
+    float bas = 0.0f;
+    for (int i = -n; i <= n; i++)
+      for (int j = -n; j <= n; j++)
+        for (int q = -n; q <= n; q++) {
+          volatile float t = kk[i] * kk[j];  // keep two roundings on the host too
+          t = t * kk[q];
+          bas = bas + t;
+        }
+    bas = 1.0f / powf(bas, 1.0f / 3.0f);
+    for (int i = -n; i <= n; i++) kk[i] = bas * kk[i];
+  }
+}
+
+// ------------------------------------------------------------ species sort
+__device__ __forceinline__ int ngp_index(float v, float xmin, float dx, int nx) {
+  int i = (int)((v - xmin) / dx) + 1;
+  if (i < 1) i = 1;
+  if (i > nx) i = nx;
+  return i - 1;
+}
+
+__global__ void k_ngp_count(const float* __restrict__ x, const float* __restrict__ y,
+                            const float* __restrict__ z, int64_t n, int nx, float dx, float xmin,
+                            int32_t* __restrict__ cell, int32_t* __restrict__ counts) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int ix = ngp_index(x[i], xmin, dx, nx), jy = ngp_index(y[i], xmin, dx, nx),
+        kz = ngp_index(z[i], xmin, dx, nx);
+    int c = (kz * nx + jy) * nx + ix;
+    cell[i] = c;
+    atomicAdd(&counts[c], 1);
+  }
+}
+
+// dens(cell) for equal masses: the float32 running sum of `count` copies of
+// m, as the sequential loop of reader.f:190-201 produces it, divided by bas.
+__global__ void k_cell_density_eqmass(const int32_t* __restrict__ counts, int64_t g, float m,
+                                      float bas, float* __restrict__ dens) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int k = counts[c];
+    float s = 0.0f;
+    for (int q = 0; q < k; q++) s = __fadd_rn(s, m);
+    dens[c] = s / bas;
+  }
+}
+
+// General masses: the particles of a cell in input order (stable sort).
+__global__ void k_cell_density_general(const int32_t* __restrict__ offs, const int32_t* __restrict__ order,
+                                       const float* __restrict__ m, int64_t g, float bas,
+                                       float* __restrict__ dens) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int q = offs[c]; q < offs[c + 1]; q++) s = __fadd_rn(s, m[order[q]]);
+    dens[c] = s / bas;
+  }
+}
+
+__global__ void k_species(const int32_t* __restrict__ cell, const float* __restrict__ dens,
+                          int64_t n, int n_esp, float log8, uint8_t* __restrict__ spec) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float b = dens[cell[i]];
+    int l = 0;
+    if (b > 0.0f) {
+      // LOG of a REAL*4 rounded to float32 (correctly rounded), then the
+      // REAL*4 quotient by LOG(8.0) and INT truncation.
+      float lb = (float)log((double)b);
+      l = (int)(lb / log8);
+      if (l > n_esp - 1) l = n_esp - 1;
+      if (l < 0) l = 0;
+    }
+    spec[i] = (uint8_t)l;
+  }
+}
+
+#define SPEC_CHUNK 4096
+#define SPEC_BLOCK 256
+
+__global__ void k_species_block_counts(const uint8_t* __restrict__ spec, int64_t n, int nb,
+                                       int32_t* __restrict__ bc) {
+  __shared__ int cnt[ASOHF_N_ESP];
+  if (threadIdx.x < ASOHF_N_ESP) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  int64_t lo = (int64_t)blockIdx.x * SPEC_CHUNK, hi = min(lo + SPEC_CHUNK, n);
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&cnt[spec[i]], 1);
+  __syncthreads();
+  if (threadIdx.x < ASOHF_N_ESP) bc[(int64_t)threadIdx.x * nb + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Stable scatter: perm[dst] = i, dst = offset(species, block) + rank in block.
+__global__ void k_species_scatter(const uint8_t* __restrict__ spec, int64_t n, int nb,
+                                  const int32_t* __restrict__ boff, int64_t* __restrict__ perm) {
+  __shared__ int wcnt[SPEC_BLOCK / 32][ASOHF_N_ESP];
+  __shared__ int run[ASOHF_N_ESP];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x < ASOHF_N_ESP) run[threadIdx.x] = boff[(int64_t)threadIdx.x * nb + blockIdx.x];
+  __syncthreads();
+  int64_t lo = (int64_t)blockIdx.x * SPEC_CHUNK, hi = min(lo + SPEC_CHUNK, n);
+  for (int64_t base = lo; base < hi; base += SPEC_BLOCK) {
+    int64_t i = base + threadIdx.x;
+    int s = i < hi ? spec[i] : -1;
+    int myrank = 0;
+    for (int q = 0; q < ASOHF_N_ESP; q++) {
+      unsigned msk = __ballot_sync(0xffffffffu, s == q);
+      if (s == q) myrank = __popc(msk & ((1u << lane) - 1));
+      if (lane == 0) wcnt[wid][q] = __popc(msk);
+    }
+    __syncthreads();
+    if (s >= 0) {
+      int off = run[s];
+      for (int w = 0; w < wid; w++) off += wcnt[w][s];
+      perm[off + myrank] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x < ASOHF_N_ESP) {
+      int t = 0;
+      for (int w = 0; w < SPEC_BLOCK / 32; w++) t += wcnt[w][threadIdx.x];
+      run[threadIdx.x] += t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_gather8(const int64_t* __restrict__ perm, int64_t n, DevParticles s, DevParticles d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = perm[i];
+    d.x[i] = s.x[j]; d.y[i] = s.y[j]; d.z[i] = s.z[j];
+    d.vx[i] = s.vx[j]; d.vy[i] = s.vy[j]; d.vz[i] = s.vz[j];
+    d.m[i] = s.m[j]; d.id[i] = s.id[j];
+  }
+}
+
+__global__ void k_iota(int32_t* __restrict__ a, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = (int32_t)i;
+}
+
+int permute_store(asohf_ctx* c, const int64_t* perm) {
+  k_gather8<<<grid_for(c->p.n, 256), 256, 0, c->stream>>>(perm, c->p.n, c->p, c->alt);
+  c->launches++;
+  ASOHF_CUDA(cudaGetLastError());
+  ctx_swap_particles(c);
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_sort_dm_particles_localdensity(asohf_ctx* c, int nx, float dx, float rodo,
+                                                    float re0, int32_t* npart_esp) {
+  if (!c || nx <= 0 || !npart_esp) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t n = c->p.n;
+  int64_t g = (int64_t)nx * nx * nx;
+  int nb = (int)((n + SPEC_CHUNK - 1) / SPEC_CHUNK);
+  if (nb < 1) nb = 1;
+  bool eq = (c->mmin == c->norma);
+  size_t cub_bytes = 0;
+  if (!eq) {
+    cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (int32_t*)nullptr, (int32_t*)nullptr,
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n);
+  }
+  size_t cub_scan = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, cub_scan, (int32_t*)nullptr, (int32_t*)nullptr,
+                                (int)(nb * ASOHF_N_ESP));
+  size_t cub_scan2 = 0;
+  if (!eq) cub::DeviceScan::ExclusiveSum(nullptr, cub_scan2, (int32_t*)nullptr, (int32_t*)nullptr, (int)(g + 1));
+  size_t need = 4 * n + 4 * g + 4 * g + n + 4 * (size_t)nb * ASOHF_N_ESP * 2 + 8 * n +
+                (eq ? 0 : (16 * n + 4 * (g + 1) * 2 + cub_bytes + cub_scan2)) + cub_scan + 8192;
+  ASOHF_CHECK(arena_reserve(c, need));
+  int32_t* cell = (int32_t*)arena_alloc(c, 4 * n);
+  int32_t* counts = (int32_t*)arena_alloc(c, 4 * g);
+  float* dens = (float*)arena_alloc(c, 4 * g);
+  uint8_t* spec = (uint8_t*)arena_alloc(c, n + 16);
+  int32_t* bc = (int32_t*)arena_alloc(c, 4 * (size_t)nb * ASOHF_N_ESP);
+  int32_t* boff = (int32_t*)arena_alloc(c, 4 * (size_t)nb * ASOHF_N_ESP);
+  int64_t* perm = (int64_t*)arena_alloc(c, 8 * n);
+  void* tscan = arena_alloc(c, cub_scan);
+  ASOHF_CUDA(cudaMemsetAsync(counts, 0, 4 * g, c->stream));
+  float xmin = -((float)nx * dx) / 2.0f;
+  k_ngp_count<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, nx, dx, xmin,
+                                                       cell, counts);
+  c->launches++;
+  float bas = dx * dx * dx * rodo * (re0 * re0 * re0);
+  if (eq) {
+    k_cell_density_eqmass<<<grid_for(g, 256), 256, 0, c->stream>>>(counts, g, c->norma, bas, dens);
+    c->launches++;
+  } else {
+    // particles of each cell in input order: stable radix sort of (cell, i)
+    int32_t* idx = (int32_t*)arena_alloc(c, 4 * n);
+    int32_t* cell_s = (int32_t*)arena_alloc(c, 4 * n);
+    int32_t* order = (int32_t*)arena_alloc(c, 4 * n);
+    int32_t* offs = (int32_t*)arena_alloc(c, 4 * (g + 1));
+    int32_t* cnt1 = (int32_t*)arena_alloc(c, 4 * (g + 1));
+    void* tsort = arena_alloc(c, cub_bytes);
+    void* tscan2 = arena_alloc(c, cub_scan2);
+    if (!idx || !cell_s || !order || !offs || !cnt1 || !tsort || !tscan2) return ASOHF_ERR_CAPACITY;
+    k_iota<<<grid_for(n, 256), 256, 0, c->stream>>>(idx, n);
+    ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(tsort, cub_bytes, cell, cell_s, idx, order, (int)n, 0,
+                                               32, c->stream));
+    ASOHF_CUDA(cudaMemsetAsync(cnt1 + g, 0, 4, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(cnt1, counts, 4 * g, cudaMemcpyDeviceToDevice, c->stream));
+    ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(tscan2, cub_scan2, cnt1, offs, (int)(g + 1), c->stream));
+    k_cell_density_general<<<grid_for(g, 256), 256, 0, c->stream>>>(offs, order, c->p.m, g, bas, dens);
+    c->launches += 2;
+  }
+  k_species<<<grid_for(n, 256), 256, 0, c->stream>>>(cell, dens, n, ASOHF_N_ESP, logf(8.0f), spec);
+  k_species_block_counts<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, bc);
+  ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(tscan, cub_scan, bc, boff, nb * ASOHF_N_ESP, c->stream));
+  k_species_scatter<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, boff, perm);
+  c->launches += 4;
+  ASOHF_CUDA(cudaGetLastError());
+  int32_t tot[ASOHF_N_ESP];
+  int32_t last_off[ASOHF_N_ESP], last_cnt[ASOHF_N_ESP];
+  for (int s = 0; s < ASOHF_N_ESP; s++) {
+    ASOHF_CUDA(cudaMemcpyAsync(&last_off[s], boff + (int64_t)s * nb + nb - 1, 4, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(&last_cnt[s], bc + (int64_t)s * nb + nb - 1, 4, cudaMemcpyDeviceToHost, c->stream));
+  }
+  ASOHF_CHECK(permute_store(c, perm));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  int64_t prev = 0;
+  for (int s = 0; s < ASOHF_N_ESP; s++) {
+    int64_t end = (int64_t)last_off[s] + last_cnt[s];
+    tot[s] = (int32_t)(end - prev);
+    prev = end;
+  }
+  if (prev != n) return ASOHF_ERR_WRONG_SORTING;
+  memcpy(npart_esp, tot, sizeof(tot));
+  return ASOHF_OK;
+}
+
+// ------------------------------------------------------------ base deposit
+// Fixed point: every REAL*4 cloud term t is an integer multiple of
+// 2^fx_shift (fx_shift = exponent of the smallest term - 24), summed in
+// 64-bit integers.  The host checks the worst-case sum fits.
+__global__ void k_density_base_fixed(const float* __restrict__ x, const float* __restrict__ y,
+                                     const float* __restrict__ z, const float* __restrict__ m,
+                                     int64_t n, int nx, float xl, float dx, const float* __restrict__ k0,
+                                     double inv_unit, unsigned long long* __restrict__ acc) {
+  float w[3] = {k0[0], k0[1], k0[2]};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float bas = m[i];
+    int ix = (int)((x[i] - xl) / dx) + 1;
+    int jy = (int)((y[i] - xl) / dx) + 1;
+    int kz = (int)((z[i] - xl) / dx) + 1;
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      int k1 = kz + kk;
+      if (k1 > nx) k1 -= nx;
+      if (k1 < 1) k1 += nx;
+#pragma unroll
+      for (int jj = -1; jj <= 1; jj++) {
+        int j1 = jy + jj;
+        if (j1 > nx) j1 -= nx;
+        if (j1 < 1) j1 += nx;
+#pragma unroll
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = ix + ii;
+          if (i1 > nx) i1 -= nx;
+          if (i1 < 1) i1 += nx;
+          if (i1 < 1 || i1 > nx || j1 < 1 || j1 > nx || k1 < 1 || k1 > nx) continue;  // outside the box
+          float t = __fmul_rn(__fmul_rn(__fmul_rn(bas, w[ii + 1]), w[jj + 1]), w[kk + 1]);
+          unsigned long long q = (unsigned long long)__double2ll_rn(__dmul_rn((double)t, inv_unit));
+          size_t c = ((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1);
+          atomicAdd(&acc[c], q);
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_density_base_f64(const float* __restrict__ x, const float* __restrict__ y,
+                                   const float* __restrict__ z, const float* __restrict__ m,
+                                   int64_t n, int nx, float xl, float dx, const float* __restrict__ k0,
+                                   double* __restrict__ acc) {
+  float w[3] = {k0[0], k0[1], k0[2]};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float bas = m[i];
+    int ix = (int)((x[i] - xl) / dx) + 1;
+    int jy = (int)((y[i] - xl) / dx) + 1;
+    int kz = (int)((z[i] - xl) / dx) + 1;
+    for (int kk = -1; kk <= 1; kk++)
+      for (int jj = -1; jj <= 1; jj++)
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = ix + ii, j1 = jy + jj, k1 = kz + kk;
+          if (i1 > nx) i1 -= nx;
+          if (i1 < 1) i1 += nx;
+          if (j1 > nx) j1 -= nx;
+          if (j1 < 1) j1 += nx;
+          if (k1 > nx) k1 -= nx;
+          if (k1 < 1) k1 += nx;
+          if (i1 < 1 || i1 > nx || j1 < 1 || j1 > nx || k1 < 1 || k1 > nx) continue;  // outside the box
+          float t = __fmul_rn(__fmul_rn(__fmul_rn(bas, w[ii + 1]), w[jj + 1]), w[kk + 1]);
+          atomicAdd(&acc[((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1)], (double)t);
+        }
+  }
+}
+
+__global__ void k_finish_fixed(const unsigned long long* __restrict__ acc, int64_t g, double unit,
+                               float denbas, float* __restrict__ u1) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    float v = (float)((double)(long long)acc[c] * unit);
+    u1[c] = v / denbas;
+  }
+}
+
+__global__ void k_finish_f64(const double* __restrict__ acc, int64_t g, float denbas,
+                             float* __restrict__ u1) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
+       c += (int64_t)gridDim.x * blockDim.x)
+    u1[c] = (float)acc[c] / denbas;
+}
+
+// ------------------------------------------------------------ spatial bins
+// Coarse binning of the store (bins of `bw` base cells) so a patch finds the
+// particles near it without scanning all N (the reference tests every
+// particle against every patch, grids.f:879-893).
+struct Bins {
+  int nb;          // bins per axis
+  float xl, bsz;   // origin and bin size
+  int32_t* start;  // nb^3+1
+  int32_t* idx;    // particle indices grouped by bin
+};
+
+__device__ __forceinline__ int bin_of(float v, float xl, float bsz, int nb) {
+  int b = (int)floorf((v - xl) / bsz);
+  return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+}
+
+__global__ void k_bin_count(const float* __restrict__ x, const float* __restrict__ y,
+                            const float* __restrict__ z, int64_t n, Bins B, int32_t* __restrict__ binof,
+                            int32_t* __restrict__ cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int b = (bin_of(z[i], B.xl, B.bsz, B.nb) * B.nb + bin_of(y[i], B.xl, B.bsz, B.nb)) * B.nb +
+            bin_of(x[i], B.xl, B.bsz, B.nb);
+    binof[i] = b;
+    atomicAdd(&cnt[b], 1);
+  }
+}
+
+__global__ void k_bin_fill(const int32_t* __restrict__ binof, int64_t n, const int32_t* __restrict__ start,
+                           int32_t* __restrict__ fill, int32_t* __restrict__ idx) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int b = binof[i];
+    int pos = start[b] + atomicAdd(&fill[b], 1);
+    idx[pos] = (int32_t)i;
+  }
+}
+
+static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B) {
+  int64_t n = c->p.n;
+  int nx = (int)lrintf(lado0 / dx);
+  int nb = (nx + bw - 1) / bw;
+  if (nb < 1) nb = 1;
+  int64_t nbin = (int64_t)nb * nb * nb;
+  B->nb = nb;
+  B->xl = -lado0 / 2.0f;
+  B->bsz = lado0 / (float)nb;
+  int32_t* binof = (int32_t*)arena_alloc(c, 4 * n);
+  int32_t* cnt = (int32_t*)arena_alloc(c, 4 * (nbin + 1));
+  B->start = (int32_t*)arena_alloc(c, 4 * (nbin + 1));
+  B->idx = (int32_t*)arena_alloc(c, 4 * n);
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, B->start, (int)(nbin + 1));
+  void* t = arena_alloc(c, tb);
+  if (!binof || !cnt || !B->start || !B->idx || !t) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (nbin + 1), c->stream));
+  k_bin_count<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, *B, binof, cnt);
+  ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(t, tb, cnt, B->start, (int)(nbin + 1), c->stream));
+  ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (nbin + 1), c->stream));
+  k_bin_fill<<<grid_for(n, 256), 256, 0, c->stream>>>(binof, n, B->start, cnt, B->idx);
+  c->launches += 2;
+  return ASOHF_OK;
+}
+
+static size_t bins_bytes(int64_t n, float lado0, float dx, int bw) {
+  int nx = (int)lrintf(lado0 / dx);
+  int nb = (nx + bw - 1) / bw;
+  int64_t nbin = (int64_t)nb * nb * nb;
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, (int32_t*)nullptr, (int32_t*)nullptr, (int)(nbin + 1));
+  return 8 * (size_t)n + 8 * (size_t)(nbin + 1) + tb + 4096;
+}
+
+// Device copy of the patch table.
+struct DevMesh {
+  int np;
+  int32_t *nx, *ny, *nz, *level;
+  float *rx, *ry, *rz;
+};
+
+static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d) {
+  int np = 0;
+  for (int ir = 1; ir <= mh->nl; ir++) np += mh->npatch[ir];
+  d->np = np;
+  if (np == 0) return ASOHF_OK;
+  int base = mh->npatch[0];
+  for (int q = 0; q < np; q++) {
+    int ip = base + q;
+    if (mh->patchnx[ip] < 1 || mh->patchnx[ip] > ASOHF_NAMRX || mh->patchny[ip] < 1 || mh->patchny[ip] > ASOHF_NAMRX ||
+        mh->patchnz[ip] < 1 || mh->patchnz[ip] > ASOHF_NAMRX)
+      return ASOHF_ERR_INVALID;
+  }
+  int32_t* hi = (int32_t*)malloc(4 * (size_t)np * 4);
+  float* hf = (float*)malloc(4 * (size_t)np * 3);
+  int q = 0;
+  for (int ir = 1; ir <= mh->nl; ir++)
+    for (int p = 0; p < mh->npatch[ir]; p++, q++) {
+      int ip = base + q;
+      hi[q] = mh->patchnx[ip];
+      hi[np + q] = mh->patchny[ip];
+      hi[2 * np + q] = mh->patchnz[ip];
+      hi[3 * np + q] = ir;
+      hf[q] = mh->patchrx[ip];
+      hf[np + q] = mh->patchry[ip];
+      hf[2 * np + q] = mh->patchrz[ip];
+    }
+  int32_t* di = (int32_t*)arena_alloc(c, 16 * (size_t)np);
+  float* df = (float*)arena_alloc(c, 12 * (size_t)np);
+  if (!di || !df) { free(hi); free(hf); return ASOHF_ERR_CAPACITY; }
+  cudaMemcpyAsync(di, hi, 16 * (size_t)np, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(df, hf, 12 * (size_t)np, cudaMemcpyHostToDevice, c->stream);
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  free(hi);
+  free(hf);
+  d->nx = di; d->ny = di + np; d->nz = di + 2 * np; d->level = di + 3 * np;
+  d->rx = df; d->ry = df + np; d->rz = df + 2 * np;
+  return ASOHF_OK;
+}
+
+// ------------------------------------------------------------ patch deposit
+// One CTA per (patch, z-half): the 32x32x16 float64 accumulator lives in
+// shared memory; candidate particles come from the bins that overlap the
+// patch box extended by MAXKERNELEXT = DX (grids.f:837-893); their clipped
+// clouds are flattened into one work list so all threads share the cells.
+#define PD_BLOCK 512
+#define PD_BATCH 512
+#define NA ASOHF_NAMRX
+#define ZH (NA / 2)
+
+struct PatchWork {
+  int n;
+  float m;
+  int ix, jy, kz, lev;     // host cell and kernel level
+  int i1, j1, k1, di, dj;  // clipped cloud origin and extents
+  int vol;
+};
+
+__global__ void __launch_bounds__(PD_BLOCK)
+k_density_patches(DevMesh M, Bins B, const float* __restrict__ x, const float* __restrict__ y,
+                  const float* __restrict__ z, const float* __restrict__ m,
+                  const int64_t* __restrict__ esp_end /* N_ESP cumulative */, float dx,
+                  const float* __restrict__ kernels, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
+  extern __shared__ double acc[];  // NA*NA*ZH
+  __shared__ int s_vol[PD_BATCH + 1];
+  __shared__ PatchWork s_w[PD_BATCH];
+  __shared__ int s_nw;
+  __shared__ int s_scan[33];
+  int ip = blockIdx.x >> 1, half = blockIdx.x & 1;
+  int n1 = M.nx[ip], n2 = M.ny[ip], n3 = M.nz[ip], ir = M.level[ip];
+  int zlo = half * ZH + 1, zhi = min(half * ZH + ZH, n3);
+  for (int q = threadIdx.x; q < NA * NA * ZH; q += blockDim.x) acc[q] = 0.0;
+  float dxpa = dx / exp2f((float)ir);
+  float xlfix = M.rx[ip] - dxpa, ylfix = M.ry[ip] - dxpa, zlfix = M.rz[ip] - dxpa;
+  float pxl = xlfix - dx, pyl = ylfix - dx, pzl = zlfix - dx;
+  float pxr = (xlfix + (float)n1 * dxpa) + dx, pyr = (ylfix + (float)n2 * dxpa) + dx,
+        pzr = (zlfix + (float)n3 * dxpa) + dx;
+  __syncthreads();
+  if (zlo <= zhi) {
+    int bx0 = bin_of(pxl, B.xl, B.bsz, B.nb), bx1 = bin_of(pxr, B.xl, B.bsz, B.nb);
+    int by0 = bin_of(pyl, B.xl, B.bsz, B.nb), by1 = bin_of(pyr, B.xl, B.bsz, B.nb);
+    int bz0 = bin_of(pzl, B.xl, B.bsz, B.nb), bz1 = bin_of(pzr, B.xl, B.bsz, B.nb);
+    for (int bz = bz0; bz <= bz1; bz++)
+      for (int by = by0; by <= by1; by++) {
+        int b0 = (bz * B.nb + by) * B.nb + bx0, b1 = (bz * B.nb + by) * B.nb + bx1;
+        int lo = B.start[b0], hi = B.start[b1 + 1];
+        for (int base = lo; base < hi; base += PD_BATCH) {
+          // 1. candidate particles of this batch -> work items
+          if (threadIdx.x == 0) s_nw = 0;
+          __syncthreads();
+          for (int t = threadIdx.x; t < PD_BATCH && base + t < hi; t += blockDim.x) {
+            int p = B.idx[base + t];
+            float xp = x[p], yp = y[p], zp = z[p];
+            if (!(pxl < xp && xp < pxr && pyl < yp && yp < pyr && pzl < zp && zp < pzr)) continue;
+            int s = 0;
+            while (s < ASOHF_N_ESP - 1 && (int64_t)p >= esp_end[s]) s++;
+            int lev = ir - s;
+            if (lev < 0) lev = 0;
+            int nk = 1 << lev;
+            int ix = (int)floorf((xp - xlfix) / dxpa) + 1;
+            int jy = (int)floorf((yp - ylfix) / dxpa) + 1;
+            int kz = (int)floorf((zp - zlfix) / dxpa) + 1;
+            int i1 = ix - nk, i2 = ix + nk, j1 = jy - nk, j2 = jy + nk, k1 = kz - nk, k2 = kz + nk;
+            if (i1 > n1 || i2 < 1 || j1 > n2 || j2 < 1 || k1 > n3 || j2 < 1) continue;
+            if (i1 < 1) i1 = 1;
+            if (i2 > n1) i2 = n1;
+            if (j1 < 1) j1 = 1;
+            if (j2 > n2) j2 = n2;
+            if (k1 < 1) k1 = 1;
+            if (k2 > n3) k2 = n3;
+            if (k1 < zlo) k1 = zlo;
+            if (k2 > zhi) k2 = zhi;
+            if (k1 > k2) continue;
+            int slot = atomicAdd(&s_nw, 1);
+            PatchWork w;
+            w.m = m[p];
+            w.ix = ix; w.jy = jy; w.kz = kz; w.lev = lev;
+            w.i1 = i1; w.j1 = j1; w.k1 = k1; w.di = i2 - i1 + 1; w.dj = j2 - j1 + 1;
+            w.vol = w.di * w.dj * (k2 - k1 + 1);
+            s_w[slot] = w;
+          }
+          __syncthreads();
+          int nw = s_nw;
+          // 2. prefix of volumes
+          int v = threadIdx.x < nw ? s_w[threadIdx.x].vol : 0;
+          int tot;
+          int inc = block_scan_i(v, s_scan, &tot);
+          if (threadIdx.x < nw) s_vol[threadIdx.x + 1] = inc;
+          if (threadIdx.x == 0) s_vol[0] = 0;
+          __syncthreads();
+          // 3. flattened cells
+          for (int f = threadIdx.x; f < tot; f += blockDim.x) {
+            int lo2 = 0, hi2 = nw - 1;
+            while (lo2 < hi2) {
+              int mid = (lo2 + hi2 + 1) >> 1;
+              if (s_vol[mid] <= f) lo2 = mid; else hi2 = mid - 1;
+            }
+            const PatchWork& w = s_w[lo2];
+            int r = f - s_vol[lo2];
+            int ii = w.i1 + r % w.di;
+            int jj = w.j1 + (r / w.di) % w.dj;
+            int kk = w.k1 + r / (w.di * w.dj);
+            const float* kern = kernels + (size_t)w.lev * KW + ASOHF_NMAX_KERNELS;
+            float t = __fmul_rn(__fmul_rn(__fmul_rn(w.m, kern[ii - w.ix]), kern[jj - w.jy]), kern[kk - w.kz]);
+            atomicAdd(&acc[((kk - zlo) * NA + (jj - 1)) * NA + (ii - 1)], (double)t);
+          }
+          __syncthreads();
+        }
+      }
+  }
+  __syncthreads();
+  float den = denbas_lev[ir];
+  float* out = u11 + (size_t)ip * NA * NA * NA;
+  for (int q = threadIdx.x; q < NA * NA * ZH; q += blockDim.x) {
+    int i = q % NA, j = (q / NA) % NA, kl = q / (NA * NA);
+    int k = half * ZH + kl;
+    float v = 0.0f;
+    if (i < n1 && j < n2 && k < n3) v = (float)acc[q] / den;
+    out[((size_t)k * NA + j) * NA + i] = v;
+  }
+}
+
+static int frexp_exp(double v) {
+  int e;
+  frexp(v, &e);
+  return e;  // v = f * 2^e, f in [0.5, 1)
+}
+
+static float* upload_floats(asohf_ctx* c, const float* h, size_t n) {
+  float* d = (float*)arena_alloc(c, 4 * n);
+  if (d) cudaMemcpyAsync(d, h, 4 * n, cudaMemcpyHostToDevice, c->stream);
+  return d;
+}
+
+// Output staging: returns a device pointer for `bytes` of output.
+static int stage_out(asohf_ctx* c, float* user, size_t bytes, int on_device, float** dev) {
+  if (on_device) { *dev = user; return ASOHF_OK; }
+  *dev = (float*)arena_alloc(c, bytes);
+  return *dev ? ASOHF_OK : ASOHF_ERR_CAPACITY;
+}
+
+extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float rote, float rete,
+                             const int32_t* npart_esp, const asohf_mesh* mesh, int interp_degree,
+                             float* u1, float* u11, int on_device) {
+  if (!c || nx <= 0 || !npart_esp || !u1 || (interp_degree != 1 && interp_degree != 2))
+    return ASOHF_ERR_INVALID;
+  int nl = mesh ? mesh->nl : 0;
+  if (nl < 0 || nl > ASOHF_NLEVELS) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t n = 0;
+  for (int s = 0; s < ASOHF_N_ESP; s++) n += npart_esp[s];
+  if (n > c->p.n) return ASOHF_ERR_INVALID;
+  int64_t g = (int64_t)nx * nx * nx;
+  int np = 0;
+  for (int ir = 1; ir <= nl; ir++) np += mesh->npatch[ir];
+  if (np > 0 && !u11) return ASOHF_ERR_INVALID;
+  size_t need = 8 * g + (on_device ? 0 : 4 * g + 4 * (size_t)np * NA * NA * NA) +
+                4 * KW * (ASOHF_NLEVELS + 1) + 64 * (size_t)np + 4096 +
+                (np ? bins_bytes(n, lado0, dx, 2) : 0);
+  ASOHF_CHECK(arena_reserve(c, need));
+  float* hk = (float*)malloc(sizeof(float) * KW * (ASOHF_NLEVELS + 1));
+  compute_kernels_host(nl, interp_degree, hk);
+  float* dk = upload_floats(c, hk, (size_t)KW * (ASOHF_NLEVELS + 1));
+  float* du1;
+  ASOHF_CHECK(stage_out(c, u1, 4 * g, on_device, &du1));
+  float xl = -lado0 / 2.0f;
+  float denbas = dx * dx * dx * rote * (rete * rete * rete);
+  // fixed point unit from the smallest possible term
+  const float* k0 = hk + ASOHF_NMAX_KERNELS;
+  float kmin = fminf(k0[-1], fminf(k0[0], k0[1])), kmax = fmaxf(k0[-1], fmaxf(k0[0], k0[1]));
+  double tmin = (double)c->mmin * kmin * kmin * kmin, tmax = (double)c->norma * kmax * kmax * kmax;
+  int emin = frexp_exp(tmin) - 2, emax = frexp_exp(tmax) + 1;
+  int shift = emin - 25;
+  double lg_n = n > 1 ? log2((double)n) : 0.0;
+  bool fixed = tmin > 0.0 && (emax - shift) + lg_n + 1.0 < 62.0;
+  void* acc = arena_alloc(c, 8 * g);
+  if (!acc || !dk) { free(hk); return ASOHF_ERR_CAPACITY; }
+  ASOHF_CUDA(cudaMemsetAsync(acc, 0, 8 * g, c->stream));
+  if (n > 0) {
+    if (fixed) {
+      double inv_unit = ldexp(1.0, -shift);
+      k_density_base_fixed<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+          c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, dk + ASOHF_NMAX_KERNELS - 1, inv_unit,
+          (unsigned long long*)acc);
+    } else {
+      k_density_base_f64<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+          c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, dk + ASOHF_NMAX_KERNELS - 1, (double*)acc);
+    }
+    c->launches++;
+  }
+  if (fixed)
+    k_finish_fixed<<<grid_for(g, 256), 256, 0, c->stream>>>((unsigned long long*)acc, g,
+                                                            ldexp(1.0, shift), denbas, du1);
+  else
+    k_finish_f64<<<grid_for(g, 256), 256, 0, c->stream>>>((double*)acc, g, denbas, du1);
+  c->launches++;
+  ASOHF_CUDA(cudaGetLastError());
+  if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(u1, du1, 4 * g, cudaMemcpyDeviceToHost, c->stream));
+  if (np > 0) {
+    DevMesh M;
+    ASOHF_CHECK(upload_mesh(c, mesh, &M));
+    Bins B;
+    ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B));
+    int64_t hend[ASOHF_N_ESP];
+    int64_t acc_n = 0;
+    for (int s = 0; s < ASOHF_N_ESP; s++) { acc_n += npart_esp[s]; hend[s] = acc_n; }
+    int64_t* dend = (int64_t*)arena_alloc(c, sizeof(hend));
+    float hden[ASOHF_NLEVELS + 1];
+    for (int ir = 0; ir <= ASOHF_NLEVELS; ir++) {
+      float dxpa = dx / powf(2.0f, (float)ir);
+      hden[ir] = dxpa * dxpa * dxpa * rote * (rete * rete * rete);
+    }
+    float* dden = upload_floats(c, hden, ASOHF_NLEVELS + 1);
+    float* du11;
+    ASOHF_CHECK(stage_out(c, u11, 4 * (size_t)np * NA * NA * NA, on_device, &du11));
+    if (!dend || !dden) { free(hk); return ASOHF_ERR_CAPACITY; }
+    ASOHF_CUDA(cudaMemcpyAsync(dend, hend, sizeof(hend), cudaMemcpyHostToDevice, c->stream));
+    size_t smem = sizeof(double) * NA * NA * ZH;
+    ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_density_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m,
+                                                           dend, dx, dk, du11, dden);
+    c->launches++;
+    ASOHF_CUDA(cudaGetLastError());
+    if (!on_device)
+      ASOHF_CUDA(cudaMemcpyAsync(u11, du11, 4 * (size_t)np * NA * NA * NA, cudaMemcpyDeviceToHost, c->stream));
+  }
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  free(hk);
+  return ASOHF_OK;
+}
+
+// ------------------------------------------------------------ renorm
+__global__ void k_scale(float* __restrict__ a, int64_t n, float f) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = a[i] / f;
+}
+
+__global__ void k_scale_patches(float* __restrict__ u11, const int32_t* __restrict__ dims, int np,
+                                float f) {
+  int ip = blockIdx.x;
+  int n1 = dims[ip], n2 = dims[np + ip], n3 = dims[2 * np + ip];
+  float* u = u11 + (size_t)ip * NA * NA * NA;
+  for (int q = threadIdx.x; q < NA * NA * NA; q += blockDim.x) {
+    int i = q % NA, j = (q / NA) % NA, k = q / (NA * NA);
+    if (i < n1 && j < n2 && k < n3) u[q] = u[q] / f;
+  }
+}
+
+extern "C" int asohf_renorm_density(asohf_ctx* c, int nx, const asohf_mesh* mesh, float fdm,
+                                    float* u1, float* u11, int on_device) {
+  if (!c || nx <= 0 || !u1) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t g = (int64_t)nx * nx * nx;
+  int np = 0, nl = mesh ? mesh->nl : 0;
+  for (int ir = 1; ir <= nl; ir++) np += mesh->npatch[ir];
+  ASOHF_CHECK(arena_reserve(c, (on_device ? 0 : 4 * g + 4 * (size_t)np * NA * NA * NA) + 16 * (size_t)np + 1024));
+  float *d1 = u1, *d11 = u11;
+  if (!on_device) {
+    d1 = (float*)arena_alloc(c, 4 * g);
+    ASOHF_CUDA(cudaMemcpyAsync(d1, u1, 4 * g, cudaMemcpyHostToDevice, c->stream));
+    if (np) {
+      d11 = (float*)arena_alloc(c, 4 * (size_t)np * NA * NA * NA);
+      ASOHF_CUDA(cudaMemcpyAsync(d11, u11, 4 * (size_t)np * NA * NA * NA, cudaMemcpyHostToDevice, c->stream));
+    }
+  }
+  k_scale<<<grid_for(g, 256), 256, 0, c->stream>>>(d1, g, fdm);
+  c->launches++;
+  if (np) {
+    int base = mesh->npatch[0];
+    int32_t* hd = (int32_t*)malloc(12 * (size_t)np);
+    for (int q = 0; q < np; q++) {
+      hd[q] = mesh->patchnx[base + q];
+      hd[np + q] = mesh->patchny[base + q];
+      hd[2 * np + q] = mesh->patchnz[base + q];
+    }
+    int32_t* dd = (int32_t*)arena_alloc(c, 12 * (size_t)np);
+    ASOHF_CUDA(cudaMemcpyAsync(dd, hd, 12 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+    k_scale_patches<<<np, 256, 0, c->stream>>>(d11, dd, np, fdm);
+    c->launches++;
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    free(hd);
+  }
+  ASOHF_CUDA(cudaGetLastError());
+  if (!on_device) {
+    ASOHF_CUDA(cudaMemcpyAsync(u1, d1, 4 * g, cudaMemcpyDeviceToHost, c->stream));
+    if (np)
+      ASOHF_CUDA(cudaMemcpyAsync(u11, d11, 4 * (size_t)np * NA * NA * NA, cudaMemcpyDeviceToHost, c->stream));
+  }
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+// ------------------------------------------------------------ TSC deposit
+// TSC weights of grids.f:1194-1213: BAS=|x-r|/d, 0.5(1.5-BAS)^2, 0.75-BAS^2.
+__device__ __forceinline__ void tsc_weights(float xp, float rm, float r0, float rp, float d, float* v) {
+  float b = fabsf(__fsub_rn(xp, rm)) / d;
+  float t = __fsub_rn(1.5f, b);
+  v[0] = __fmul_rn(0.5f, __fmul_rn(t, t));
+  b = fabsf(__fsub_rn(xp, r0)) / d;
+  v[1] = __fsub_rn(0.75f, __fmul_rn(b, b));
+  b = fabsf(__fsub_rn(xp, rp)) / d;
+  t = __fsub_rn(1.5f, b);
+  v[2] = __fmul_rn(0.5f, __fmul_rn(t, t));
+}
+
+__device__ __forceinline__ int tsc_cell(float v, float xl, float dx, int nx) {
+  int i = (int)((v - xl) / dx) + 1;
+  return i < 1 ? 1 : (i > nx ? nx : i);
+}
+
+// Base grid TSC for a batch of particle sets; acc has batch*nx^3 doubles or floats.
+template <typename T>
+__global__ void k_tsc_base(const float* __restrict__ x, const float* __restrict__ y,
+                           const float* __restrict__ z, const float* __restrict__ m, int64_t n_per,
+                           int batch, int nx, float xl, float dx, const float* __restrict__ radx,
+                           T* __restrict__ acc) {
+  int64_t ntot = n_per * batch;
+  size_t g = (size_t)nx * nx * nx;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < ntot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int b = (int)(q / n_per);
+    float xp = x[q], yp = y[q], zp = z[q];
+    int ix = tsc_cell(xp, xl, dx, nx), jy = tsc_cell(yp, xl, dx, nx), kz = tsc_cell(zp, xl, dx, nx);
+    float wx[3], wy[3], wz[3];
+    tsc_weights(xp, radx[ix - 1], radx[ix], radx[ix + 1], dx, wx);
+    tsc_weights(yp, radx[jy - 1], radx[jy], radx[jy + 1], dx, wy);
+    tsc_weights(zp, radx[kz - 1], radx[kz], radx[kz + 1], dx, wz);
+    float mp = m[q];
+    T* a = acc + (size_t)b * g;
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      int k1 = kz + kk;
+      if (k1 == nx + 1) k1 = 1;
+      if (k1 == 0) k1 = nx;
+#pragma unroll
+      for (int jj = -1; jj <= 1; jj++) {
+        int j1 = jy + jj;
+        if (j1 == nx + 1) j1 = 1;
+        if (j1 == 0) j1 = nx;
+#pragma unroll
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = ix + ii;
+          if (i1 == nx + 1) i1 = 1;
+          if (i1 == 0) i1 = nx;
+          float t = __fmul_rn(__fmul_rn(__fmul_rn(mp, wx[ii + 1]), wy[jj + 1]), wz[kk + 1]);
+          atomicAdd(&a[((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1)], (T)t);
+        }
+      }
+    }
+  }
+}
+
+// PLEV (grids.f:1121-1152): the finest level with a patch that contains the
+// particle inside a one-cell buffer.  One CTA per patch raises plev by
+// atomicMax over the particles of the bins it overlaps.
+__global__ void k_tsc_plev(DevMesh M, Bins B, const float* __restrict__ x, const float* __restrict__ y,
+                           const float* __restrict__ z, float dx, int32_t* __restrict__ plev) {
+  int ip = blockIdx.x;
+  int ir = M.level[ip];
+  float dxpa = dx / exp2f((float)ir);
+  float xl = M.rx[ip] - 2.0f * dxpa, yl = M.ry[ip] - 2.0f * dxpa, zl = M.rz[ip] - 2.0f * dxpa;
+  float xr = xl + (float)(M.nx[ip] + 2) * dxpa, yr = yl + (float)(M.ny[ip] + 2) * dxpa,
+        zr = zl + (float)(M.nz[ip] + 2) * dxpa;
+  int bx0 = bin_of(xl, B.xl, B.bsz, B.nb), bx1 = bin_of(xr, B.xl, B.bsz, B.nb);
+  int by0 = bin_of(yl, B.xl, B.bsz, B.nb), by1 = bin_of(yr, B.xl, B.bsz, B.nb);
+  int bz0 = bin_of(zl, B.xl, B.bsz, B.nb), bz1 = bin_of(zr, B.xl, B.bsz, B.nb);
+  for (int bz = bz0; bz <= bz1; bz++)
+    for (int by = by0; by <= by1; by++) {
+      int lo = B.start[(bz * B.nb + by) * B.nb + bx0], hi = B.start[(bz * B.nb + by) * B.nb + bx1 + 1];
+      for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+        int p = B.idx[t];
+        if (xl < x[p] && x[p] < xr && yl < y[p] && y[p] < yr && zl < z[p] && z[p] < zr)
+          atomicMax(&plev[p], ir);
+      }
+    }
+}
+
+// Patch TSC (grids.f:1286-1372): one CTA per (patch, z-half).
+__global__ void __launch_bounds__(PD_BLOCK)
+k_tsc_patches(DevMesh M, Bins B, const float* __restrict__ x, const float* __restrict__ y,
+              const float* __restrict__ z, const float* __restrict__ m, const int32_t* __restrict__ plev,
+              float dx, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
+  extern __shared__ double acc[];
+  int ip = blockIdx.x >> 1, half = blockIdx.x & 1;
+  int n1 = M.nx[ip], n2 = M.ny[ip], n3 = M.nz[ip], ir = M.level[ip];
+  int zlo = half * ZH + 1, zhi = min(half * ZH + ZH, n3);
+  for (int q = threadIdx.x; q < NA * NA * ZH; q += blockDim.x) acc[q] = 0.0;
+  __syncthreads();
+  float dxpa = dx / exp2f((float)ir);
+  float xl = M.rx[ip] - 2.0f * dxpa, yl = M.ry[ip] - 2.0f * dxpa, zl = M.rz[ip] - 2.0f * dxpa;
+  float xr = xl + (float)(n1 + 2) * dxpa, yr = yl + (float)(n2 + 2) * dxpa, zr = zl + (float)(n3 + 2) * dxpa;
+  if (zlo <= zhi) {
+    int bx0 = bin_of(xl, B.xl, B.bsz, B.nb), bx1 = bin_of(xr, B.xl, B.bsz, B.nb);
+    int by0 = bin_of(yl, B.xl, B.bsz, B.nb), by1 = bin_of(yr, B.xl, B.bsz, B.nb);
+    int bz0 = bin_of(zl, B.xl, B.bsz, B.nb), bz1 = bin_of(zr, B.xl, B.bsz, B.nb);
+    for (int bz = bz0; bz <= bz1; bz++)
+      for (int by = by0; by <= by1; by++) {
+        int lo = B.start[(bz * B.nb + by) * B.nb + bx0], hi = B.start[(bz * B.nb + by) * B.nb + bx1 + 1];
+        for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+          int p = B.idx[t];
+          if (plev[p] < ir) continue;
+          float xp = x[p], yp = y[p], zp = z[p];
+          if (!(xl < xp && xp < xr && yl < yp && yp < yr && zl < zp && zp < zr)) continue;
+          int ix = (int)((xp - xl) / dxpa) + 1 - 1;
+          int jy = (int)((yp - yl) / dxpa) + 1 - 1;
+          int kz = (int)((zp - zl) / dxpa) + 1 - 1;
+          // MINIRADX(II) = PATCHRX + (II - 1.5) DXPA
+          float wx[3], wy[3], wz[3];
+          float rxm = M.rx[ip] + ((float)(ix - 1) - 1.5f) * dxpa, rx0 = M.rx[ip] + ((float)ix - 1.5f) * dxpa,
+                rxp = M.rx[ip] + ((float)(ix + 1) - 1.5f) * dxpa;
+          float rym = M.ry[ip] + ((float)(jy - 1) - 1.5f) * dxpa, ry0 = M.ry[ip] + ((float)jy - 1.5f) * dxpa,
+                ryp = M.ry[ip] + ((float)(jy + 1) - 1.5f) * dxpa;
+          float rzm = M.rz[ip] + ((float)(kz - 1) - 1.5f) * dxpa, rz0 = M.rz[ip] + ((float)kz - 1.5f) * dxpa,
+                rzp = M.rz[ip] + ((float)(kz + 1) - 1.5f) * dxpa;
+          tsc_weights(xp, rxm, rx0, rxp, dxpa, wx);
+          tsc_weights(yp, rym, ry0, ryp, dxpa, wy);
+          tsc_weights(zp, rzm, rz0, rzp, dxpa, wz);
+          float mp = m[p];
+          for (int kk = -1; kk <= 1; kk++)
+            for (int jj = -1; jj <= 1; jj++)
+              for (int ii = -1; ii <= 1; ii++) {
+                int i1 = ix + ii, j1 = jy + jj, k1 = kz + kk;
+                if (i1 > 0 && i1 <= n1 && j1 > 0 && j1 <= n2 && k1 >= zlo && k1 <= zhi) {
+                  float tt = __fmul_rn(__fmul_rn(__fmul_rn(mp, wx[ii + 1]), wy[jj + 1]), wz[kk + 1]);
+                  atomicAdd(&acc[((k1 - zlo) * NA + (j1 - 1)) * NA + (i1 - 1)], (double)tt);
+                }
+              }
+        }
+      }
+  }
+  __syncthreads();
+  float den = denbas_lev[ir];
+  float* out = u11 + (size_t)ip * NA * NA * NA;
+  for (int q = threadIdx.x; q < NA * NA * ZH; q += blockDim.x) {
+    int i = q % NA, j = (q / NA) % NA, kl = q / (NA * NA);
+    int k = half * ZH + kl;
+    float v = 0.0f;
+    if (i < n1 && j < n2 && k < n3) v = (float)acc[q] / den;
+    out[((size_t)k * NA + j) * NA + i] = v;
+  }
+}
+
+extern "C" int asohf_interpolate_density_tsc(asohf_ctx* c, int nx, float lado0, float dx,
+                                             const float* radx, float rote, float rete,
+                                             const asohf_mesh* mesh, float* u1, float* u11,
+                                             int on_device) {
+  if (!c || nx <= 0 || !radx || !u1) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t n = c->p.n;
+  int64_t g = (int64_t)nx * nx * nx;
+  int nl = mesh ? mesh->nl : 0;
+  int np = 0;
+  for (int ir = 1; ir <= nl; ir++) np += mesh->npatch[ir];
+  if (np > 0 && !u11) return ASOHF_ERR_INVALID;
+  size_t need = 8 * g + 4 * g + 4 * (size_t)np * NA * NA * NA + 4 * (nx + 2) + 4 * n +
+                64 * (size_t)np + 8192 + (np ? bins_bytes(n, lado0, dx, 2) : 0);
+  ASOHF_CHECK(arena_reserve(c, need));
+  float* dradx = upload_floats(c, radx, nx + 2);
+  double* acc = (double*)arena_alloc(c, 8 * g);
+  float* du1;
+  ASOHF_CHECK(stage_out(c, u1, 4 * g, on_device, &du1));
+  if (!dradx || !acc) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaMemsetAsync(acc, 0, 8 * g, c->stream));
+  float xl = -lado0 / 2.0f;
+  if (n > 0) {
+    k_tsc_base<double><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        c->p.x, c->p.y, c->p.z, c->p.m, n, 1, nx, xl, dx, dradx, acc);
+    c->launches++;
+  }
+  float denbas = dx * dx * dx * rote * (rete * rete * rete);
+  k_finish_f64<<<grid_for(g, 256), 256, 0, c->stream>>>(acc, g, denbas, du1);
+  c->launches++;
+  ASOHF_CUDA(cudaGetLastError());
+  if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(u1, du1, 4 * g, cudaMemcpyDeviceToHost, c->stream));
+  if (np > 0) {
+    DevMesh M;
+    ASOHF_CHECK(upload_mesh(c, mesh, &M));
+    Bins B;
+    ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B));
+    int32_t* plev = (int32_t*)arena_alloc(c, 4 * n);
+    float hden[ASOHF_NLEVELS + 1];
+    for (int ir = 0; ir <= ASOHF_NLEVELS; ir++) {
+      float dxpa = dx / powf(2.0f, (float)ir);
+      hden[ir] = dxpa * dxpa * dxpa * rote * (rete * rete * rete);
+    }
+    float* dden = upload_floats(c, hden, ASOHF_NLEVELS + 1);
+    float* du11;
+    ASOHF_CHECK(stage_out(c, u11, 4 * (size_t)np * NA * NA * NA, on_device, &du11));
+    if (!plev || !dden) return ASOHF_ERR_CAPACITY;
+    ASOHF_CUDA(cudaMemsetAsync(plev, 0, 4 * n, c->stream));
+    k_tsc_plev<<<np, 256, 0, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, dx, plev);
+    size_t smem = sizeof(double) * NA * NA * ZH;
+    ASOHF_CUDA(cudaFuncSetAttribute(k_tsc_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tsc_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m, plev, dx,
+                                                         du11, dden);
+    c->launches += 2;
+    ASOHF_CUDA(cudaGetLastError());
+    if (!on_device)
+      ASOHF_CUDA(cudaMemcpyAsync(u11, du11, 4 * (size_t)np * NA * NA * NA, cudaMemcpyDeviceToHost, c->stream));
+  }
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+// exported for poisson.cu (batched forward deposit)
+int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* dradx, int batch,
+                         int64_t n_per, const float* x, const float* y, const float* z,
+                         const float* m, float* acc) {
+  int64_t n = n_per * batch;
+  if (n > 0) {
+    k_tsc_base<float><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(x, y, z, m, n_per, batch,
+                                                                              nx, xl, dx, dradx, acc);
+    c->launches++;
+  }
+  ASOHF_CUDA(cudaGetLastError());
+  return ASOHF_OK;
+}

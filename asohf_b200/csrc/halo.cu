@@ -1,0 +1,1288 @@
+// halo.cu -- PRUNE_POOR_HALOES and HALOFIND_PARTICLES on sm_100a.
+//
+// Pipeline of one call (haloes lowh1..lowh2, largest first):
+//   k_halo_grow   one CTA per halo: density-peak recentering and the
+//                 spherical-overdensity growth (counts and sums only);
+//   (scan)        segment offsets from the final member counts;
+//   k_halo_gather one CTA per halo writes (halo, distance) keys and x-sorted
+//                 positions of its members into its segment;
+//   radix sort    of all segments at once on (halo, distance), then
+//   k_tiefix      orders equal distances by position, descending, which is
+//                 ARGSORT's order (num.f:181) over the slab-ordered list;
+//   k_halo_main   one CTA per halo: virial index, escape-velocity and
+//                 sigma-clipping unbinding, SO walk, bound-particle
+//                 properties;
+//   k_write_ids   bound-particle IDs in halo order (PARTICLES_PER_HALO).
+// The reference scans a full-(y,z) x-slab per query (haloes_particles.f:
+// 117-143); the column index returns the same member sets from the columns a
+// sphere overlaps.
+#include <stdlib.h>
+#include <string.h>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "halo_dev.cuh"
+
+// ---------------------------------------------------------------- catalogue mirror
+struct CatMirror {
+  asohf_catalogue h;  // caller's
+  asohf_catalogue d;  // device
+  int n;              // entries mirrored
+  bool host;
+};
+
+#define CAT_F1(X) X(masa) X(radio) X(clusrx) X(clusry) X(clusrz) X(clusrxcm) X(clusrycm) X(clusrzcm) \
+  X(msub) X(rsub) X(concentra) X(vmaxclus) X(vx) X(vy) X(vz) X(mean_vr) X(vcmax) X(mcmax) X(rcmax)     \
+  X(m200c) X(r200c) X(m500c) X(r500c) X(m2500c) X(r2500c) X(m200m) X(r200m) X(m500m) X(r500m)          \
+  X(m2500m) X(r2500m) X(velocity_dispersion) X(kinetic_e) X(potential_e)
+#define CAT_I1(X) X(patchclus) X(realclus) X(levhal) X(dmpclus) X(iplip)
+#define CAT_FM(X) X(angularm, 3) X(profiles, 2 * ASOHF_NBINS) X(eigenval, 3) X(inertia_tensor, 6)
+
+static size_t cat_bytes(int n) {
+  size_t b = 0;
+#define F(f) b += 4 * (size_t)n + 256;
+  CAT_F1(F) CAT_I1(F)
+#undef F
+#define M(f, w) b += 4 * (size_t)n * (w) + 256;
+  CAT_FM(M)
+#undef M
+  b += 8 * (size_t)n + 256;  // indcs
+  return b;
+}
+
+static int cat_mirror_in(asohf_ctx* c, asohf_catalogue* h, int n, int on_device, CatMirror* m) {
+  m->h = *h;
+  m->n = n;
+  m->host = !on_device;
+  if (on_device) { m->d = *h; return ASOHF_OK; }
+  m->d = *h;
+#define F(f)                                                                                  \
+  m->d.f = (decltype(m->d.f))arena_alloc(c, 4 * (size_t)n + 4);                              \
+  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                     \
+  if (n) ASOHF_CUDA(cudaMemcpyAsync(m->d.f, h->f, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  CAT_F1(F) CAT_I1(F)
+#undef F
+#define M(f, w)                                                                               \
+  m->d.f = (float*)arena_alloc(c, 4 * (size_t)n * (w) + 4);                                  \
+  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                     \
+  if (n) ASOHF_CUDA(cudaMemcpyAsync(m->d.f, h->f, 4 * (size_t)n * (w), cudaMemcpyHostToDevice, c->stream));
+  CAT_FM(M)
+#undef M
+  m->d.indcs = (int32_t*)arena_alloc(c, 8 * (size_t)n + 8);
+  if (!m->d.indcs) return ASOHF_ERR_CAPACITY;
+  if (n) ASOHF_CUDA(cudaMemcpyAsync(m->d.indcs, h->indcs, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  return ASOHF_OK;
+}
+
+static int cat_mirror_out(asohf_ctx* c, CatMirror* m) {
+  if (!m->host || m->n == 0) return ASOHF_OK;
+  int n = m->n;
+#define F(f) ASOHF_CUDA(cudaMemcpyAsync(m->h.f, m->d.f, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  CAT_F1(F) CAT_I1(F)
+#undef F
+#define M(f, w) ASOHF_CUDA(cudaMemcpyAsync(m->h.f, m->d.f, 4 * (size_t)n * (w), cudaMemcpyDeviceToHost, c->stream));
+  CAT_FM(M)
+#undef M
+  ASOHF_CUDA(cudaMemcpyAsync(m->h.indcs, m->d.indcs, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+static ColIdx col_idx(asohf_ctx* c, const asohf_consts* k) {
+  ColIdx ci;
+  ci.cp = c->d_colpart;
+  ci.start = c->d_colstart;
+  ci.ncol = c->col_n;
+  ci.xl = c->col_xl;
+  ci.cdx = c->col_dx;
+  ci.nd = c->d_ndmpart_x;
+  ci.nmax = k->nx;
+  ci.dx = k->dx;
+  ci.xldom = -k->lado0 / 2.0f;
+  return ci;
+}
+
+static Store store_of(asohf_ctx* c) {
+  Store S;
+  S.x = c->p.x; S.y = c->p.y; S.z = c->p.z;
+  S.vx = c->p.vx; S.vy = c->p.vy; S.vz = c->p.vz;
+  S.m = c->p.m; S.id = c->p.id;
+  S.norma = c->norma;
+  S.eqmass_lt8 = c->norma / c->mmin < 8.0f;
+  return S;
+}
+
+static HConst hconst(const asohf_consts* k, const asohf_mesh* mesh) {
+  HConst h;
+  h.rote = k->rote; h.rete = k->rete; h.pi = k->pi; h.cgr = k->cgr; h.um = k->um; h.uv = k->uv;
+  h.contrastec = k->contrastec; h.omegaz = k->omegaz; h.fdm = k->fdm; h.zeta = k->zeta;
+  h.min_num_part = k->min_num_part;
+  h.want_ids = (k->flag_wdm == 1 || k->var > 1);
+  h.nl = mesh ? mesh->nl : 0;
+  int acc = mesh ? mesh->npatch[0] : 0;
+  for (int ir = 0; ir <= ASOHF_NLEVELS + 1; ir++) { h.lev_lo[ir] = 0; h.lev_hi[ir] = -1; }
+  for (int ir = 1; ir <= h.nl; ir++) {
+    h.lev_lo[ir] = acc + 1;
+    h.lev_hi[ir] = acc + mesh->npatch[ir];
+    acc += mesh->npatch[ir];
+  }
+  return h;
+}
+
+// ---------------------------------------------------------------- prune
+// COUNT_PARTICLES_HALO (haloes_particles.f:147-182) for haloes low1..low2.
+__global__ void __launch_bounds__(HB) k_prune(ColIdx ci, asohf_catalogue cat, int low1, float facrad,
+                                             int min_num_part) {
+  __shared__ long long lred[32];
+  int i0 = low1 - 1 + blockIdx.x;
+  float cx = cat.clusrx[i0], cy = cat.clusry[i0], cz = cat.clusrz[i0];
+  float r = __fmul_rn(facrad, cat.radio[i0]);
+  float r2 = __fmul_rn(r, r);
+  int64_t lo, hi;
+  slab_range(ci, cx, r, &lo, &hi);
+  long long cnt = 0;
+  query_box(ci, cx, cy, cz, r, [&](const float4& e) {
+    int p = ppos(e);
+    if (p < lo || p >= hi) return;
+    float bx = __fsub_rn(e.x, cx);
+    bx = __fmul_rn(bx, bx);
+    if (bx > r2) return;
+    float by = __fsub_rn(e.y, cy);
+    by = __fmul_rn(by, by);
+    if (by > r2) return;
+    float bz = __fsub_rn(e.z, cz);
+    bz = __fmul_rn(bz, bz);
+    if (bz > r2) return;
+    if (__fadd_rn(__fadd_rn(bx, by), bz) < r2) cnt++;
+  });
+  cnt = block_sum_ll(cnt, lred);
+  if (threadIdx.x == 0) {
+    if (cnt < min_num_part) cat.realclus[i0] = 0;
+    cat.dmpclus[i0] = (int32_t)cnt;
+  }
+}
+
+__global__ void k_prune_nocount(asohf_catalogue cat, int low1, int low2, int min_num_part) {
+  int i0 = low1 - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i0 < low2 && cat.dmpclus[i0] < min_num_part) cat.realclus[i0] = 0;
+}
+
+extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asohf_catalogue* cat,
+                                       int low1, int low2, float facrad, int do_need_to_count,
+                                       int on_device) {
+  if (!c || !k || !cat || low1 < 1 || low2 > cat->nclus) return ASOHF_ERR_INVALID;
+  if (low2 < low1) return ASOHF_OK;
+  if (do_need_to_count == 1 && c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  ASOHF_CHECK(arena_reserve(c, cat_bytes(low2) + 4096));
+  CatMirror m;
+  ASOHF_CHECK(cat_mirror_in(c, cat, low2, on_device, &m));
+  int nh = low2 - low1 + 1;
+  if (do_need_to_count == 1)
+    k_prune<<<nh, HB, 0, c->stream>>>(col_idx(c, k), m.d, low1, facrad, k->min_num_part);
+  else
+    k_prune_nocount<<<(nh + 255) / 256, 256, 0, c->stream>>>(m.d, low1, low2, k->min_num_part);
+  c->launches++;
+  ASOHF_CUDA(cudaGetLastError());
+  ASOHF_CHECK(cat_mirror_out(c, &m));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+// ---------------------------------------------------------------- grow
+struct GrowOut {
+  float *cx, *cy, *cz;     // recentred centre
+  float *rgather;          // radius of the last gather (members)
+  float *rclus;            // RCLUS after the last growth step
+  int32_t* konta;          // members
+  double* masadm;          // their mass
+  int32_t* status;
+};
+
+__device__ __forceinline__ int level_of_patch(const HConst& H, int ipatch) {
+  int irr;
+  for (irr = 1; irr <= H.nl; irr++)
+    if (H.lev_lo[irr] <= ipatch && ipatch <= H.lev_hi[irr]) break;
+  return irr;
+}
+
+// Recentering + growth of HALOFIND_PARTICLES (haloes_particles.f:741-849).
+__global__ void __launch_bounds__(HB)
+k_halo_grow(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work,
+            GrowOut o) {
+  __shared__ RecShared sh;
+  int slot = blockIdx.x;
+  int i0 = work[slot];
+  if (cat.realclus[i0] == 0) {
+    if (threadIdx.x == 0) { o.konta[slot] = 0; o.status[slot] = 0; }
+    return;
+  }
+  int irr = level_of_patch(H, cat.patchclus[i0]);
+  float cx = cat.clusrx[i0], cy = cat.clusry[i0], cz = cat.clusrz[i0];
+  float dxpamin = __fdiv_rn(ci.dx, exp2f((float)irr));
+  if (!recenter_block(S, ci, &cx, &cy, &cz, cat.radio[i0], dxpamin, sh)) {
+    if (threadIdx.x == 0) { o.konta[slot] = 0; o.status[slot] = ASOHF_ERR_CAPACITY; }
+    return;
+  }
+  float mino = __fmul_rn(fminf(200.0f, H.contrastec), H.fdm);
+  float den0 = __fmul_rn(__fmul_rn(H.rote, __fmul_rn(__fmul_rn(H.rete, H.rete), H.rete)),
+                         __fdiv_rn(__fmul_rn(4.0f, H.pi), 3.0f));
+  float rclus = cat.radio[i0];
+  float delta2 = __fmul_rn(100.0f, mino);
+  float rg = rclus;
+  long long konta = 0;
+  double masadm = 0.0;
+  int guard = 0;
+  while (delta2 > __fmul_rn(0.99f, mino)) {
+    int64_t lo, hi;
+    slab_range(ci, cx, rclus, &lo, &hi);
+    long long c = 0;
+    double ms = 0.0;
+    float bas = -1.0f;
+    query_box(ci, cx, cy, cz, rclus, [&](const float4& e) {
+      int p = ppos(e);
+      if (p < lo || p >= hi) return;
+      float a = dist3(e.x, e.y, e.z, cx, cy, cz);
+      if (a < rclus) {
+        c++;
+        ms += (double)S.m[p];
+        bas = fmaxf(bas, a);
+      }
+    });
+    konta = block_sum_ll(c, sh.lred);
+    masadm = block_sum_d(ms, sh.dred);
+    bas = block_max_f(bas, sh.fred);
+    float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(bas, bas), bas));
+    delta2 = (float)(masadm / (double)den);
+    rg = rclus;
+    if (delta2 > __fmul_rn(0.9f, mino)) rclus = __fmul_rn(1.25f, rclus);
+    if (++guard > 100000) break;
+  }
+  if (threadIdx.x == 0) {
+    cat.clusrx[i0] = cx; cat.clusry[i0] = cy; cat.clusrz[i0] = cz;
+    o.cx[slot] = cx; o.cy[slot] = cy; o.cz[slot] = cz;
+    o.rgather[slot] = rg;
+    o.rclus[slot] = rclus;
+    o.masadm[slot] = masadm;
+    o.status[slot] = 0;
+    if (masadm <= 0.0 || konta == 0) {
+      cat.realclus[i0] = 0;
+      o.konta[slot] = 0;
+    } else {
+      o.konta[slot] = (int32_t)konta;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- gather
+__global__ void __launch_bounds__(HB)
+k_halo_gather(Store S, ColIdx ci, const int32_t* __restrict__ konta, const int64_t* __restrict__ off,
+              const float* __restrict__ hcx, const float* __restrict__ hcy, const float* __restrict__ hcz,
+              const float* __restrict__ rg, unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
+  __shared__ int fill;
+  int slot = blockIdx.x;
+  if (konta[slot] == 0) return;
+  if (threadIdx.x == 0) fill = 0;
+  __syncthreads();
+  float cx = hcx[slot], cy = hcy[slot], cz = hcz[slot], r = rg[slot];
+  int64_t lo, hi;
+  slab_range(ci, cx, r, &lo, &hi);
+  int64_t base = off[slot];
+  unsigned long long hk = (unsigned long long)slot << 32;
+  query_box(ci, cx, cy, cz, r, [&](const float4& e) {
+    int p = ppos(e);
+    if (p < lo || p >= hi) return;
+    float a = dist3(e.x, e.y, e.z, cx, cy, cz);
+    if (a < r) {
+      int q = atomicAdd(&fill, 1);
+      if (q < konta[slot]) {
+        keys[base + q] = hk | __float_as_uint(a);
+        vals[base + q] = p;
+      }
+    }
+  });
+}
+
+// Runs of equal (halo, distance) get their positions in descending (desc=1)
+// or ascending order.
+__global__ void k_tiefix(const unsigned long long* __restrict__ keys, int32_t* __restrict__ vals,
+                         int64_t n, int desc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i > 0 && keys[i] == keys[i - 1]) continue;
+    if (i + 1 >= n || keys[i + 1] != keys[i]) continue;
+    int64_t e = i + 1;
+    while (e < n && keys[e] == keys[i]) e++;
+    for (int64_t a = i + 1; a < e; a++) {
+      int32_t v = vals[a];
+      int64_t b = a - 1;
+      while (b >= i && (desc ? vals[b] < v : vals[b] > v)) {
+        vals[b + 1] = vals[b];
+        b--;
+      }
+      vals[b + 1] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- main
+struct Seg {
+  const int32_t* konta;
+  const int64_t* off;      // element offset of the segment (segments padded by 1)
+  const unsigned long long* keys;
+  const int32_t* vals;
+  float* dista;            // DISTA(1..K) at [off], DISTA(K+1) pad
+  int32_t* lip;
+  double* pot;
+  uint8_t* flag;
+  int32_t* nbound;         // IDs to write per slot (KONTA2 of the property loop)
+  int32_t* nscan;          // entries the property loop scanned (NCAPAS)
+  int32_t* status;
+};
+
+struct MainShared {
+  double dred[32];
+  float fred[32];
+  long long lred[32];
+  double v[16];
+  long long iv[16];
+  float inertia[9];
+  float eig[3];
+  double bestv[HB];
+  long long bestj[HB];
+  double bestb[HB];
+};
+
+// Block-wide minimum of an index (LLONG_MAX when none).
+__device__ __forceinline__ long long bmin(long long v, MainShared& sh) { return block_min_ll(v, sh.lred); }
+
+// CENTROMASAS_PART (haloes_particles.f:1731-1824) over j <= n with flag=1.
+__device__ void centromasas_block(const Store& S, const float* dista_unused, const int32_t* lip,
+                                  const uint8_t* flag, bool all_kept, int64_t n, float* cm, float* vcm,
+                                  float* masa, MainShared& sh) {
+  double a[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+    if (!all_kept && !flag[j]) continue;
+    int p = lip[j];
+    double bas = (double)S.m[p];
+    a[0] += (double)S.x[p] * bas;
+    a[1] += (double)S.y[p] * bas;
+    a[2] += (double)S.z[p] * bas;
+    a[3] += (double)S.vx[p] * bas;
+    a[4] += (double)S.vy[p] * bas;
+    a[5] += (double)S.vz[p] * bas;
+    a[6] += bas;
+  }
+  for (int q = 0; q < 7; q++) a[q] = block_sum_d(a[q], sh.dred);
+  if (a[6] > 0.0) {
+    for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
+    *masa = (float)a[6];
+  } else {
+    for (int q = 0; q < 3; q++) { cm[q] = 0.0f; vcm[q] = 0.0f; }
+    *masa = 0.0f;
+  }
+}
+
+// REORDENAR(...,0,...) (haloes_particles.f:1696-1722): stable in-place
+// compaction of the kept entries of j <= k2, IDX_VIR relocated to the first
+// kept entry at or after it.  Entries past the new length keep their values.
+__device__ void reordenar_compact(float* dista, int32_t* lip, const uint8_t* flag, int64_t k2,
+                                  int64_t* idx_vir, int64_t* k2new, MainShared& sh) {
+  int64_t carry = 0;
+  long long reloc = LLONG_MAX;
+  int64_t iv = *idx_vir;  // 1-based
+  __shared__ int sb[33];
+  for (int64_t t0 = 0; t0 < k2; t0 += HB) {
+    int64_t j = t0 + threadIdx.x;
+    bool keep = j < k2 && flag[j];
+    float d = keep ? dista[j] : 0.0f;
+    int32_t l = keep ? lip[j] : 0;
+    int tot;
+    int inc = block_scan_i(keep ? 1 : 0, sb, &tot);
+    int64_t dst = carry + inc - 1;
+    if (keep) {
+      dista[dst] = d;
+      lip[dst] = l;
+      if (j + 1 >= iv && dst + 1 < reloc) reloc = dst + 1;
+    }
+    carry += tot;
+    __syncthreads();
+  }
+  reloc = bmin(reloc, sh);
+  *k2new = carry;
+  *idx_vir = reloc == LLONG_MAX ? carry : reloc;
+}
+
+struct HaloState {
+  float cm[3], v[3], masa, radio;
+  int realclus;
+};
+
+__device__ __forceinline__ void unbind_result(HaloState& h, long long konta3, const float* cm,
+                                              const float* vcm, float mmm, float um) {
+  if (konta3 == 0) {
+    for (int q = 0; q < 3; q++) { h.cm[q] = 0.0f; h.v[q] = 0.0f; }
+    h.masa = 0.0f;
+    h.radio = 0.0f;
+    h.realclus = 0;
+  } else {
+    for (int q = 0; q < 3; q++) { h.cm[q] = cm[q]; h.v[q] = vcm[q]; }
+    h.masa = __fmul_rn(mmm, um);
+  }
+}
+
+// UNBINDING8 (haloes_particles.f:1828-1983).  dista/lip/flag/pot are the
+// 0-based views of the segment (element j-1 = Fortran J).
+__device__ void unbinding8_block(const Store& S, const HConst& H, int fac, float ref_max, float* dista,
+                                 int32_t* lip, uint8_t* flag, double* pot, int64_t k2, int64_t idx_vir,
+                                 HaloState& h, MainShared& sh) {
+  float cm[3] = {0, 0, 0}, vcm[3] = {0, 0, 0}, mmm = 0.0f;
+  long long konta3 = 0;
+  if (k2 > 0) {
+    double norma = (double)S.norma;
+    float lim = __fmul_rn(0.01f, ref_max);
+    long long jj = LLONG_MAX;
+    for (int64_t t0 = 0; t0 < k2 && jj == LLONG_MAX; t0 += HB) {
+      int64_t j = t0 + threadIdx.x;
+      long long cand = (j < k2 && dista[j] > lim) ? (long long)(j + 1) : LLONG_MAX;
+      jj = bmin(cand, sh);
+    }
+    if (jj == LLONG_MAX) jj = k2 + 1;
+    // cumulative mass MASA8 (stored in pot for now)
+    double mjj = 0.0, mk2 = 0.0;
+    __shared__ double s_m[2];
+    tile_prefix_d(0, k2, 0.0, [&](int64_t j) { return (double)S.m[lip[j]] / norma; },
+                  [&](int64_t j, double v) {
+                    pot[j] = v;
+                    if (j + 1 == jj) s_m[0] = v;
+                    if (j + 1 == k2) s_m[1] = v;
+                  },
+                  sh.dred);
+    __syncthreads();
+    mk2 = s_m[1];
+    if (jj == k2 + 1) mjj = mk2; else mjj = s_m[0];
+    double pot_jj = mjj / (double)dista[jj - 1];
+    // POT(J) for J > JJ: POT(J-1) + MASA8*BAS8/DISTA(J)^2
+    tile_prefix_d(jj, k2, pot_jj,
+                  [&](int64_t j) {
+                    float dj = dista[j], dm = dista[j - 1];
+                    double bas8 = (dj != dm) ? (double)__fsub_rn(dj, dm) : 0.0;
+                    double djd = (double)dj;
+                    return pot[j] * bas8 / (djd * djd);
+                  },
+                  [&](int64_t j, double v) { pot[j] = v; }, sh.dred);
+    __syncthreads();
+    for (int64_t j = threadIdx.x; j < jj && j < k2; j += blockDim.x) pot[j] = pot_jj;
+    __syncthreads();
+    double pot1 = pot[k2 - 1] + mk2 / (double)ref_max;
+    double aa8 = norma * (double)__fdiv_rn(H.cgr, H.rete);
+    float bb = 2.0f;
+    if (fac == 1) bb = 8.0f;
+    if (fac == 2) bb = 4.0f;
+    bb = __fmul_rn(bb, bb);
+    double a[7] = {0, 0, 0, 0, 0, 0, 0};
+    long long kept = 0;
+    for (int64_t j = threadIdx.x; j < k2; j += blockDim.x) {
+      float potok = (float)((pot[j] - pot1) * aa8);
+      float vesc2 = __fmul_rn(2.0f, fabsf(potok));
+      int p = lip[j];
+      float ax = __fsub_rn(S.vx[p], h.v[0]), ay = __fsub_rn(S.vy[p], h.v[1]), az = __fsub_rn(S.vz[p], h.v[2]);
+      float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+      bool keep = !(vvv2 > __fmul_rn(bb, vesc2));
+      flag[j] = keep;
+      kept += keep;
+      if (keep && j < idx_vir) {
+        double bas = (double)S.m[p];
+        a[0] += (double)S.x[p] * bas;
+        a[1] += (double)S.y[p] * bas;
+        a[2] += (double)S.z[p] * bas;
+        a[3] += (double)S.vx[p] * bas;
+        a[4] += (double)S.vy[p] * bas;
+        a[5] += (double)S.vz[p] * bas;
+        a[6] += bas;
+      }
+    }
+    konta3 = block_sum_ll(kept, sh.lred);
+    for (int q = 0; q < 7; q++) a[q] = block_sum_d(a[q], sh.dred);
+    if (a[6] > 0.0) {
+      for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
+      mmm = (float)a[6];
+    }
+  }
+  unbind_result(h, konta3, cm, vcm, mmm, H.um);
+}
+
+// UNBINDING_SIGMA (haloes_particles.f:1987-2095).
+__device__ void unbinding_sigma_block(const Store& S, const HConst& H, int fac, int32_t* lip, uint8_t* flag,
+                                      int64_t k2, int64_t idx_vir, HaloState& h, MainShared& sh) {
+  float bb = fmaxf(__fsub_rn(6.0f, __fmul_rn(1.0f, (float)(fac - 1))), 3.0f);
+  bb = __fmul_rn(bb, bb);
+  float cm[3] = {h.cm[0], h.cm[1], h.cm[2]}, vcm[3] = {h.v[0], h.v[1], h.v[2]}, mmm = 0.0f;
+  long long konta3 = 0;
+  if (k2 > 0) {
+    double s2 = 0.0;
+    for (int64_t j = threadIdx.x; j < idx_vir && j < k2; j += blockDim.x) {
+      int p = lip[j];
+      float ax = __fsub_rn(S.vx[p], vcm[0]), ay = __fsub_rn(S.vy[p], vcm[1]), az = __fsub_rn(S.vz[p], vcm[2]);
+      s2 += (double)__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+    }
+    double sigma2 = block_sum_d(s2, sh.dred);
+    if (idx_vir > 1) sigma2 = sigma2 / (double)(idx_vir - 1);
+    double thr = (double)bb * sigma2;
+    double a[7] = {0, 0, 0, 0, 0, 0, 0};
+    long long kept = 0;
+    for (int64_t j = threadIdx.x; j < k2; j += blockDim.x) {
+      int p = lip[j];
+      float ax = __fsub_rn(S.vx[p], vcm[0]), ay = __fsub_rn(S.vy[p], vcm[1]), az = __fsub_rn(S.vz[p], vcm[2]);
+      float bas = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+      bool keep = !((double)bas > thr);
+      flag[j] = keep;
+      kept += keep;
+      if (keep && j < idx_vir) {
+        double w = (double)S.m[p];
+        a[0] += (double)S.x[p] * w;
+        a[1] += (double)S.y[p] * w;
+        a[2] += (double)S.z[p] * w;
+        a[3] += (double)S.vx[p] * w;
+        a[4] += (double)S.vy[p] * w;
+        a[5] += (double)S.vz[p] * w;
+        a[6] += w;
+      }
+    }
+    konta3 = block_sum_ll(kept, sh.lred);
+    for (int q = 0; q < 7; q++) a[q] = block_sum_d(a[q], sh.dred);
+    if (a[6] > 0.0) {
+      for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
+      mmm = (float)a[6];
+    } else {
+      for (int q = 0; q < 3; q++) { cm[q] = 0.0f; vcm[q] = 0.0f; }
+      mmm = 0.0f;
+    }
+  }
+  unbind_result(h, konta3, cm, vcm, mmm, H.um);
+}
+
+// DIAGONALISE (num.f:2-116), REAL*8 Jacobi; `in` is column-major REAL*4.
+__device__ void diagonalise_dev(const float* in, float* eig) {
+  const int n = 3;
+  double a[3][3], e[3], aux1[3], aux2[3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) a[i][j] = (double)in[j * 3 + i];
+  for (int i = 0; i < n; i++) { aux1[i] = a[i][i]; e[i] = aux1[i]; aux2[i] = 0.0; }
+  double sum_el = 0.0;
+  for (int i = 0; i < n; i++)
+    for (int j = i; j < n; j++) sum_el = __dadd_rn(sum_el, fabs(a[i][j]));
+  for (int it = 1; it <= 100; it++) {
+    double suma = 0.0;
+    for (int i = 0; i < n - 1; i++)
+      for (int j = i + 1; j < n; j++) suma = __dadd_rn(suma, fabs(a[i][j]));
+    if (suma < __dmul_rn((double)1.e-4f, sum_el)) break;
+    double upper = (it < 4) ? __dmul_rn(0.2, __dmul_rn(suma, suma)) : 0.0;
+    for (int p = 0; p < n - 1; p++) {
+      for (int q = p + 1; q < n; q++) {
+        double var1 = __dmul_rn(100.0, fabs(a[p][q]));
+        if (it > 4 && __dadd_rn(fabs(e[p]), var1) == fabs(e[p]) && __dadd_rn(fabs(e[q]), var1) == fabs(e[q])) {
+          a[p][q] = 0.0;
+        } else if (fabs(a[p][q]) > upper) {
+          double var2 = __dsub_rn(e[q], e[p]), t;
+          if (__dadd_rn(fabs(var2), var1) == fabs(var2)) {
+            t = __ddiv_rn(a[p][q], var2);
+          } else {
+            double th = __ddiv_rn(__dmul_rn(0.5, var2), a[p][q]);
+            t = __ddiv_rn(1.0, __dadd_rn(fabs(th), __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(th, th)))));
+            if (th < 0.0) t = -t;
+          }
+          double cth = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(t, t))));
+          double s = __dmul_rn(t, cth);
+          double tau = __ddiv_rn(s, __dadd_rn(1.0, cth));
+          var2 = __dmul_rn(t, a[p][q]);
+          aux2[p] = __dsub_rn(aux2[p], var2);
+          aux2[q] = __dadd_rn(aux2[q], var2);
+          e[p] = __dsub_rn(e[p], var2);
+          e[q] = __dadd_rn(e[q], var2);
+          a[p][q] = 0.0;
+          for (int j = 0; j < p; j++) {
+            double v1 = a[j][p], v2 = a[j][q];
+            a[j][p] = __dsub_rn(v1, __dmul_rn(s, __dadd_rn(v2, __dmul_rn(v1, tau))));
+            a[j][q] = __dadd_rn(v2, __dmul_rn(s, __dsub_rn(v1, __dmul_rn(v2, tau))));
+          }
+          for (int j = p + 1; j < q; j++) {
+            double v1 = a[p][j], v2 = a[j][q];
+            a[p][j] = __dsub_rn(v1, __dmul_rn(s, __dadd_rn(v2, __dmul_rn(v1, tau))));
+            a[j][q] = __dadd_rn(v2, __dmul_rn(s, __dsub_rn(v1, __dmul_rn(v2, tau))));
+          }
+          for (int j = q + 1; j < n; j++) {
+            double v1 = a[p][j], v2 = a[q][j];
+            a[p][j] = __dsub_rn(v1, __dmul_rn(s, __dadd_rn(v2, __dmul_rn(v1, tau))));
+            a[q][j] = __dadd_rn(v2, __dmul_rn(s, __dsub_rn(v1, __dmul_rn(v2, tau))));
+          }
+        }
+      }
+    }
+    for (int i = 0; i < n; i++) { aux1[i] = __dadd_rn(aux1[i], aux2[i]); e[i] = aux1[i]; aux2[i] = 0.0; }
+  }
+  for (int i = 0; i < n; i++) eig[i] = (float)e[i];
+}
+
+__device__ void sort_eigen_dev(float* e) {
+  for (int ii = 0; ii < 2; ii++) {
+    int kk = ii;
+    float valor = e[ii];
+    for (int jj = ii + 1; jj < 3; jj++)
+      if (e[jj] >= valor) { kk = jj; valor = e[jj]; }
+    if (kk != ii) { e[kk] = e[ii]; e[ii] = valor; }
+  }
+}
+
+// Bound-particle properties (haloes_particles.f:1187-1353 and
+// substructure.f:1478-1660) over j <= konta; flag[j] receives the ID mask.
+// Returns the number of bound particles (KONTA2).
+__device__ long long properties_block(const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
+                                      float* dista, int32_t* lip, uint8_t* flag, int64_t konta, float rshell,
+                                      float cx, float cy, float cz, const float* cmv, bool sym,
+                                      MainShared& sh) {
+  float norma = S.norma;
+  float vc[3] = {cat.vx[i0], cat.vy[i0], cat.vz[i0]};
+  int64_t each_prof = konta / ASOHF_NBINS;
+  if (each_prof == 0) each_prof = 1;
+  double acc[16];
+  for (int q = 0; q < 16; q++) acc[q] = 0.0;
+  float vmax = -1.0f;
+  long long cnt = 0;
+  // masked cumulative mass for the profile entries, then the sums
+  tile_prefix_d(0, konta,
+                0.0,
+                [&](int64_t j) {
+                  int p = lip[j];
+                  float a = dist3(S.x[p], S.y[p], S.z[p], cx, cy, cz);
+                  bool in = a <= rshell;
+                  flag[j] = in;
+                  return in ? (double)__fdiv_rn(S.m[p], norma) : 0.0;
+                },
+                [&](int64_t j, double basmas) {
+                  int64_t J = j + 1;
+                  if (!flag[j]) return;
+                  int p = lip[j];
+                  float bv[3] = {__fsub_rn(S.x[p], cx), __fsub_rn(S.y[p], cy), __fsub_rn(S.z[p], cz)};
+                  float aadm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(bv[0], bv[0]), __fmul_rn(bv[1], bv[1])),
+                                                    __fmul_rn(bv[2], bv[2])));
+                  cnt++;
+                  if (J % each_prof == 0 && J / each_prof <= ASOHF_NBINS) {
+                    int64_t b = J / each_prof;
+                    cat.profiles[(size_t)i0 * 2 * ASOHF_NBINS + (b - 1)] = aadm;
+                    cat.profiles[(size_t)i0 * 2 * ASOHF_NBINS + ASOHF_NBINS + (b - 1)] =
+                        (float)(basmas * (double)norma * (double)H.um);
+                  }
+                  float bc[3] = {__fsub_rn(S.x[p], cmv[0]), __fsub_rn(S.y[p], cmv[1]), __fsub_rn(S.z[p], cmv[2])};
+                  float bvc[3] = {__fsub_rn(S.vx[p], vc[0]), __fsub_rn(S.vy[p], vc[1]), __fsub_rn(S.vz[p], vc[2])};
+                  float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(bvc[0], bvc[0]), __fmul_rn(bvc[1], bvc[1])),
+                                         __fmul_rn(bvc[2], bvc[2]));
+                  float mp = S.m[p];
+                  acc[0] += (double)vvv2;
+                  acc[1] += (double)__fmul_rn(mp, vvv2);
+                  acc[2] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[1], bvc[2]), __fmul_rn(bc[2], bvc[1])));
+                  acc[3] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[2], bvc[0]), __fmul_rn(bc[0], bvc[2])));
+                  acc[4] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[0], bvc[1]), __fmul_rn(bc[1], bvc[0])));
+                  for (int jy = 0; jy < 3; jy++)
+                    for (int ix = 0; ix < 3; ix++)
+                      acc[5 + jy * 3 + ix] += (double)__fmul_rn(__fmul_rn(mp, bc[ix]), bc[jy]);
+                  vmax = fmaxf(vmax, vvv2);
+                  if (aadm != 0.0f) {
+                    float aa = __fadd_rn(__fadd_rn(__fmul_rn(__fdiv_rn(bv[0], aadm), bvc[0]),
+                                                   __fmul_rn(__fdiv_rn(bv[1], aadm), bvc[1])),
+                                         __fmul_rn(__fdiv_rn(bv[2], aadm), bvc[2]));
+                    acc[14] += (double)__fmul_rn(aa, mp);
+                  }
+                  acc[15] += (double)__fdiv_rn(mp, norma);
+                },
+                sh.dred);
+  for (int q = 0; q < 16; q++) acc[q] = block_sum_d(acc[q], sh.dred);
+  cnt = block_sum_ll(cnt, sh.lred);
+  vmax = block_max_f(vmax, sh.fred);
+  if (threadIdx.x == 0) {
+    cat.dmpclus[i0] = (int32_t)cnt;
+    if (cnt < H.min_num_part) {
+      cat.realclus[i0] = 0;
+    } else {
+      cat.potential_e[i0] = 0.0f;
+      cat.iplip[i0] = S.id[lip[0]];
+      double basmas = acc[15];
+      double den = basmas * (double)norma;
+      cat.angularm[i0 * 3 + 0] = (float)(acc[2] * (double)H.uv / den);
+      cat.angularm[i0 * 3 + 1] = (float)(acc[3] * (double)H.uv / den);
+      cat.angularm[i0 * 3 + 2] = (float)(acc[4] * (double)H.uv / den);
+      cat.mean_vr[i0] = (float)(acc[14] / den * (double)H.uv);
+      float in[9];
+      for (int jy = 0; jy < 3; jy++)
+        for (int ix = 0; ix < 3; ix++) in[jy * 3 + ix] = (float)(acc[5 + jy * 3 + ix] / den);
+      if (sym) {
+        in[3] = in[1];
+        in[6] = in[2];
+        in[7] = in[5];
+      }
+      float* it = cat.inertia_tensor + (size_t)i0 * 6;
+      it[0] = in[0]; it[1] = in[3]; it[2] = in[6]; it[3] = in[4]; it[4] = in[7]; it[5] = in[8];
+      cat.velocity_dispersion[i0] = (float)(sqrt(acc[0] / (double)(float)cnt) * (double)H.uv);
+      cat.vmaxclus[i0] = __fmul_rn(__fsqrt_rn(vmax), H.uv);
+      float be[3] = {0.0f, 0.0f, 0.0f};
+      diagonalise_dev(in, be);
+      sort_eigen_dev(be);
+      for (int q = 0; q < 3; q++) cat.eigenval[(size_t)i0 * 3 + q] = __fsqrt_rn(__fmul_rn(5.0f, be[q]));
+    }
+  }
+  __syncthreads();
+  return cnt;
+}
+
+__device__ __forceinline__ float so_den(float d, float rete, float pi) {
+  float dr = __fmul_rn(d, rete);
+  return __fmul_rn(__fmul_rn(pi, 1.3333334f), __fmul_rn(__fmul_rn(dr, dr), dr));
+}
+
+__global__ void __launch_bounds__(HB)
+k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work, GrowOut g, Seg sg) {
+  __shared__ MainShared sh;
+  int slot = blockIdx.x;
+  int i0 = work[slot];
+  int64_t K = g.konta[slot];
+  if (threadIdx.x == 0) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; }
+  if (K == 0) return;
+  int64_t base = sg.off[slot] + slot;
+  float* dista = sg.dista + base;
+  int32_t* lip = sg.lip + base;
+  double* pot = sg.pot + base;
+  uint8_t* flag = sg.flag + base;
+  int64_t kbase = sg.off[slot];
+  for (int64_t j = threadIdx.x; j < K; j += blockDim.x) {
+    unsigned long long kk = sg.keys[kbase + j];
+    dista[j] = __uint_as_float((uint32_t)(kk & 0xffffffffull));
+    lip[j] = sg.vals[kbase + j];
+    flag[j] = 1;
+  }
+  if (threadIdx.x == 0) dista[K] = 1.e10f;
+  __syncthreads();
+  float cx = g.cx[slot], cy = g.cy[slot], cz = g.cz[slot];
+  int kk_entero = cat.realclus[i0];
+  float pi = H.pi, rote = H.rote, rete = H.rete, fdm = H.fdm, um = H.um;
+  float norma = S.norma;
+  int64_t k2 = K, idx_vir = K;
+  float ref_max = dista[K - 1];
+  HaloState h;
+  h.radio = g.rclus[slot];
+  h.masa = (float)(g.masadm[slot] * (double)um);
+  h.realclus = kk_entero;
+  // FIND_IDX_VIR (haloes_particles.f:1453-1491)
+  {
+    int64_t jjcore = min(idx_vir / 10, (int64_t)50);
+    float den0 = __fmul_rn(__fmul_rn(rote, __fmul_rn(__fmul_rn(rete, rete), rete)),
+                           __fdiv_rn(__fmul_rn(4.0f, pi), 3.0f));
+    float cvir = __fmul_rn(H.contrastec, fdm);
+    long long best = LLONG_MAX;
+    tile_prefix_d(0, idx_vir, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                  [&](int64_t j, double menc) {
+                    if (j + 1 <= jjcore) return;
+                    float d = dista[j];
+                    float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(d, d), d));
+                    float delta = (float)(menc / (double)den);
+                    if (delta < cvir && (long long)(j + 1) < best) best = j + 1;
+                  },
+                  sh.dred);
+    best = bmin(best, sh);
+    if (best == LLONG_MAX) {
+      if (threadIdx.x == 0) sg.status[slot] = ASOHF_ERR_NOT_PREFOUND_VIRIAL;
+      return;
+    }
+    idx_vir = best;
+  }
+  float cm0[3], v0[3], m2;
+  centromasas_block(S, dista, lip, flag, true, idx_vir, cm0, v0, &m2, sh);
+  for (int q = 0; q < 3; q++) { h.cm[q] = cm0[q]; h.v[q] = v0[q]; }
+  // escape-velocity unbinding (haloes_particles.f:894-907)
+  int64_t contaerr = K;
+  int fac = 0;
+  while (contaerr > 0 || fac < 3) {
+    fac++;
+    int64_t prev = k2;
+    unbinding8_block(S, H, fac, ref_max, dista, lip, flag, pot, k2, idx_vir, h, sh);
+    int64_t nk2;
+    reordenar_compact(dista, lip, flag, k2, &idx_vir, &nk2, sh);
+    k2 = nk2;
+    __syncthreads();
+    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
+    contaerr = prev - k2;
+    if (fac > 100000) break;
+  }
+  // sigma clipping (haloes_particles.f:918-933)
+  fac = 0;
+  contaerr = k2;
+  while (contaerr > 0 || fac < 4) {
+    fac++;
+    int64_t prev = k2;
+    unbinding_sigma_block(S, H, fac, lip, flag, k2, idx_vir, h, sh);
+    int64_t nk2;
+    reordenar_compact(dista, lip, flag, k2, &idx_vir, &nk2, sh);
+    k2 = nk2;
+    __syncthreads();
+    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
+    contaerr = prev - k2;
+    if (fac > 100000) break;
+  }
+  if (k2 < H.min_num_part) {
+    if (threadIdx.x == 0) {
+      cat.realclus[i0] = 0;
+      cat.radio[i0] = h.radio; cat.masa[i0] = h.masa;
+      cat.clusrxcm[i0] = h.cm[0]; cat.clusrycm[i0] = h.cm[1]; cat.clusrzcm[i0] = h.cm[2];
+      cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2];
+      cat.dmpclus[i0] = (int32_t)K;
+    }
+    return;
+  }
+  // ---------------------------------------------------------- SO walk
+  // haloes_particles.f:973-1182.  BAS8 is the cumulative mass; once the
+  // virial crossing is found the loop subtracts that particle from BAS8 and
+  // keeps walking until 200m is found too, so crossings past it see
+  // BAS8 - m(J_vir).
+  int64_t jjcore = (int64_t)fmaxf(10.0f, __fdiv_rn((float)k2, 100.0f));
+  float thr[6] = {__fmul_rn(__fdiv_rn(2500.0f, H.omegaz), fdm), __fmul_rn(__fdiv_rn(500.0f, H.omegaz), fdm),
+                  __fmul_rn(__fdiv_rn(200.0f, H.omegaz), fdm), __fmul_rn(2500.0f, fdm),
+                  __fmul_rn(500.0f, fdm), __fmul_rn(200.0f, fdm)};
+  float cvir = __fmul_rn(H.contrastec, fdm);
+  int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
+  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(S.m[lip[j]], norma); };
+  // pass A: virial crossing and the crossings at or before it
+  long long jt[7];
+  for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
+  tile_prefix_d(0, k2, 0.0, mn_of,
+                [&](int64_t j, double bas8) {
+                  int64_t J = j + 1;
+                  if (J <= jjcore) return;
+                  float vol = so_den(dista[j], rete, pi);
+                  float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
+                  for (int q = 0; q < 6; q++)
+                    if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+                  if (delta2 <= cvir && J > jvir_min && J < jt[6]) jt[6] = J;
+                },
+                sh.dred);
+  for (int q = 0; q < 7; q++) jt[q] = bmin(jt[q], sh);
+  long long jvir = jt[6];
+  double mvir = 0.0;
+  if (jvir != LLONG_MAX) {
+    mvir = (double)__fdiv_rn(S.m[lip[jvir - 1]], norma);
+    bool again = false;
+    for (int q = 0; q < 6; q++)
+      if (jt[q] > jvir) { jt[q] = LLONG_MAX; again = true; }
+    if (again) {  // pass A2: crossings after the virial one, with BAS8 - m(J_vir)
+      tile_prefix_d(0, k2, 0.0, mn_of,
+                    [&](int64_t j, double bas8) {
+                      int64_t J = j + 1;
+                      if (J <= jvir) return;
+                      double b8 = bas8 - mvir;
+                      float vol = so_den(dista[j], rete, pi);
+                      float delta2 = (float)((double)norma * b8 / (double)vol / (double)rote);
+                      for (int q = 0; q < 6; q++)
+                        if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+                    },
+                    sh.dred);
+      for (int q = 0; q < 6; q++) jt[q] = bmin(jt[q], sh);
+    }
+  }
+  bool exit_found = jvir != LLONG_MAX && jt[5] != LLONG_MAX;
+  int64_t jend = exit_found ? max(jvir, jt[5]) : k2;
+  // pass B: BAS8 at the crossings, V_c max over the walked range, and the
+  // velocity sums up to the virial crossing (or the whole walk)
+  __shared__ double s_at[7];
+  __shared__ double s_vs[4];
+  double best_v = -1.0;
+  long long best_j = LLONG_MAX;
+  double best_b = 0.0;
+  int64_t jv = jvir != LLONG_MAX ? jvir : jend;
+  double vacc[3] = {0.0, 0.0, 0.0};
+  double btot = tile_prefix_d(0, jend, 0.0, mn_of,
+                [&](int64_t j, double bas8) {
+                  int64_t J = j + 1;
+                  double b8 = (jvir != LLONG_MAX && J > jvir) ? bas8 - mvir : bas8;
+                  for (int q = 0; q < 7; q++)
+                    if (J == jt[q]) s_at[q] = (q == 6) ? bas8 : b8;
+                  if (J == jv) s_vs[0] = bas8;
+                  if (J <= jjcore) return;
+                  float bas2 = (float)(b8 / (double)dista[j]);
+                  if ((double)bas2 > best_v || ((double)bas2 == best_v && J < best_j)) {
+                    best_v = bas2;
+                    best_j = J;
+                    best_b = b8;
+                  }
+                },
+                sh.dred);
+  (void)btot;
+  for (int ax = 0; ax < 3; ax++) {
+    const float* vv = ax == 0 ? S.vx : (ax == 1 ? S.vy : S.vz);
+    vacc[ax] = tile_prefix_d(0, jv, 0.0, [&](int64_t j) {
+                               int p = lip[j];
+                               return (double)__fmul_rn(__fdiv_rn(S.m[p], norma), vv[p]);
+                             },
+                             [&](int64_t, double) {}, sh.dred);
+  }
+  if (threadIdx.x == 0) { s_vs[1] = vacc[0]; s_vs[2] = vacc[1]; s_vs[3] = vacc[2]; }
+  sh.bestv[threadIdx.x] = best_v;
+  sh.bestj[threadIdx.x] = best_j;
+  sh.bestb[threadIdx.x] = best_b;
+  __syncthreads();
+  float rshell = 0.0f;
+  int64_t ncapas = 0;
+  if (threadIdx.x == 0) {
+    double bv = -1.0;
+    long long bj = LLONG_MAX;
+    double bb = 0.0;
+    for (int t = 0; t < HB; t++) {
+      if (sh.bestj[t] == LLONG_MAX) continue;
+      if (sh.bestv[t] > bv || (sh.bestv[t] == bv && sh.bestj[t] < bj)) {
+        bv = sh.bestv[t]; bj = sh.bestj[t]; bb = sh.bestb[t];
+      }
+    }
+    if (bj != LLONG_MAX) {
+      cat.vcmax[i0] = (float)bv;
+      cat.mcmax[i0] = (float)bb;
+      cat.rcmax[i0] = dista[bj - 1];
+    }
+    float* mo[6] = {cat.m2500c, cat.m500c, cat.m200c, cat.m2500m, cat.m500m, cat.m200m};
+    float* ro[6] = {cat.r2500c, cat.r500c, cat.r200c, cat.r2500m, cat.r500m, cat.r200m};
+    bool f200m = false;
+    for (int q = 0; q < 6; q++) {
+      if (jt[q] != LLONG_MAX && jt[q] <= jend) {
+        int64_t J = jt[q];
+        float d = dista[J - 1];
+        float vol = so_den(d, rete, pi);
+        float delta2 = (float)((double)norma * s_at[q] / (double)vol / (double)rote);
+        mo[q][i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
+        ro[q][i0] = d;
+        if (J == jjcore + 1) { mo[q][i0] = -1.0f; ro[q][i0] = -1.0f; }
+        if (q == 5) f200m = true;
+      }
+    }
+    bool salida = false;
+    if (jvir != LLONG_MAX) {
+      int p = lip[jvir - 1];
+      float mn = __fdiv_rn(S.m[p], norma);
+      double bas8 = s_vs[0] - (double)mn;
+      double bvx = s_vs[1] - (double)__fmul_rn(mn, S.vx[p]);
+      double bvy = s_vs[2] - (double)__fmul_rn(mn, S.vy[p]);
+      double bvz = s_vs[3] - (double)__fmul_rn(mn, S.vz[p]);
+      h.masa = (float)(bas8 * (double)norma * (double)um);
+      float vol = (float)(((double)norma * bas8) / (double)__fmul_rn(__fmul_rn(H.contrastec, fdm), rote));
+      h.radio = __fdiv_rn(powf(__fdiv_rn(__fmul_rn(3.0f, vol), __fmul_rn(4.0f, pi)), 1.0f / 3.0f), rete);
+      h.v[0] = (float)(bvx / bas8);
+      h.v[1] = (float)(bvy / bas8);
+      h.v[2] = (float)(bvz / bas8);
+      ncapas = jvir - 1;
+      rshell = h.radio;
+      salida = true;
+    }
+    {
+      float bas = __fdiv_rn(__fmul_rn(__fmul_rn(cat.vcmax[i0], norma), H.cgr), rete);
+      cat.vcmax[i0] = __fmul_rn(__fsqrt_rn(bas), H.uv);
+      cat.mcmax[i0] = __fmul_rn(__fmul_rn(cat.mcmax[i0], norma), um);
+    }
+    if (kk_entero == -1 && !salida) {
+      double bas8 = s_vs[0];
+      h.masa = (float)(bas8 * (double)norma * (double)um);
+      float vol = (float)(((double)norma * bas8) / (double)__fmul_rn(__fmul_rn(H.contrastec, fdm), rote));
+      h.radio = __fdiv_rn(powf(__fdiv_rn(__fmul_rn(3.0f, vol), __fmul_rn(4.0f, pi)), 1.0f / 3.0f), rete);
+      h.v[0] = (float)(s_vs[1] / bas8);
+      h.v[1] = (float)(s_vs[2] / bas8);
+      h.v[2] = (float)(s_vs[3] / bas8);
+      ncapas = jend;  // J - 1 with J = KONTA2 + 1
+      rshell = h.radio;
+      if (!f200m) {
+        cat.m200m[i0] = h.masa;
+        cat.r200m[i0] = __fmul_rn(h.radio, powf(__fdiv_rn(H.contrastec, 200.0f), 1.0f / 3.0f));
+      }
+    }
+    cat.radio[i0] = h.radio; cat.masa[i0] = h.masa;
+    cat.clusrxcm[i0] = h.cm[0]; cat.clusrycm[i0] = h.cm[1]; cat.clusrzcm[i0] = h.cm[2];
+    cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2];
+    cat.realclus[i0] = h.realclus;
+    cat.dmpclus[i0] = (int32_t)K;
+    sh.v[0] = rshell;
+    sh.iv[0] = ncapas;
+  }
+  __syncthreads();
+  rshell = (float)sh.v[0];
+  ncapas = sh.iv[0];
+  __syncthreads();
+  if (ncapas < H.min_num_part) {
+    if (threadIdx.x == 0) cat.realclus[i0] = 0;
+    return;
+  }
+  long long nb = properties_block(S, H, cat, i0, dista, lip, flag, ncapas, rshell, cx, cy, cz, cm0, true, sh);
+  if (threadIdx.x == 0) {
+    bool ok = nb >= H.min_num_part && H.want_ids;
+    sg.nbound[slot] = ok ? (int32_t)nb : 0;
+    sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
+    sg.status[slot] = 0;
+  }
+}
+
+// IDs of the bound particles, in radial order, at ids_off[slot].
+__global__ void __launch_bounds__(HB)
+k_write_ids(const int32_t* __restrict__ nscan, const int64_t* __restrict__ off, const int64_t* __restrict__ ids_off,
+            const int32_t* __restrict__ lip_all, const uint8_t* __restrict__ flag_all, const int32_t* __restrict__ id,
+            int32_t* __restrict__ out) {
+  __shared__ int sb[33];
+  int slot = blockIdx.x;
+  int64_t n = nscan[slot];
+  if (n == 0) return;
+  int64_t base = off[slot] + slot;
+  const int32_t* lip = lip_all + base;
+  const uint8_t* flag = flag_all + base;
+  int64_t carry = ids_off[slot];
+  for (int64_t t0 = 0; t0 < n; t0 += HB) {
+    int64_t j = t0 + threadIdx.x;
+    bool k = j < n && flag[j];
+    int tot;
+    int inc = block_scan_i(k ? 1 : 0, sb, &tot);
+    if (k) out[carry + inc - 1] = id[lip[j]];
+    carry += tot;
+  }
+}
+
+// ---------------------------------------------------------------- host driver
+struct HaloRun {
+  int nslots;
+  int32_t* d_work;
+  GrowOut g;
+  int64_t* d_off;
+  int64_t total;
+  unsigned long long* keys;
+  int32_t* vals;
+  Seg sg;
+};
+
+int ensure_pph(asohf_ctx* c, int64_t need) {
+  if (need <= c->pph_cap) return ASOHF_OK;
+  int64_t cap = need + need / 2 + 1024;
+  int32_t* nb = nullptr;
+  ASOHF_CUDA(cudaMalloc(&nb, 4 * (size_t)cap));
+  if (c->d_pph && c->pph_len > 0)
+    ASOHF_CUDA(cudaMemcpyAsync(nb, c->d_pph, 4 * (size_t)c->pph_len, cudaMemcpyDeviceToDevice, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(c->d_pph);
+  c->d_pph = nb;
+  c->pph_cap = cap;
+  return ASOHF_OK;
+}
+
+// Host part of the ID concatenation (haloes_particles.f:1377-1408): INDCS of
+// haloes low1..low2 from the counts, offsets for k_write_ids.
+int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int32_t* work, int nslots,
+                      const int32_t* d_nbound, int64_t* d_ids_off, int64_t* total_out) {
+  int n = low2;
+  int32_t* realclus = (int32_t*)malloc(4 * (size_t)n);
+  int32_t* indcs = (int32_t*)malloc(8 * (size_t)n);
+  int32_t* nbound = (int32_t*)malloc(4 * (size_t)(nslots > 0 ? nslots : 1));
+  int64_t* ids_off = (int64_t*)malloc(8 * (size_t)(nslots > 0 ? nslots : 1));
+  int32_t* slot_of = (int32_t*)malloc(4 * (size_t)(low2 - low1 + 1));
+  ASOHF_CUDA(cudaMemcpyAsync(realclus, m.d.realclus, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(indcs, m.d.indcs, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  if (nslots)
+    ASOHF_CUDA(cudaMemcpyAsync(nbound, d_nbound, 4 * (size_t)nslots, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < low2 - low1 + 1; i++) slot_of[i] = -1;
+  for (int s = 0; s < nslots; s++) slot_of[work[s] - (low1 - 1)] = s;
+  int64_t j = 0;
+  for (int i = 1; i < low1; i++)
+    if (realclus[i - 1] != 0 && indcs[(i - 1) * 2 + 1] > j) j = indcs[(i - 1) * 2 + 1];
+  for (int i = low1; i <= low2; i++) {
+    if (realclus[i - 1] == 0) {
+      indcs[(i - 1) * 2] = -1;
+      indcs[(i - 1) * 2 + 1] = -1;
+      continue;
+    }
+    int s = slot_of[i - low1];
+    indcs[(i - 1) * 2] = (int32_t)(j + 1);
+    if (s >= 0) {
+      ids_off[s] = j;
+      j += nbound[s];
+    }
+    indcs[(i - 1) * 2 + 1] = (int32_t)j;
+  }
+  for (int s = 0; s < nslots; s++)
+    if (realclus[work[s]] == 0) ids_off[s] = 0;
+  ASOHF_CUDA(cudaMemcpyAsync(m.d.indcs + 2 * (size_t)(low1 - 1), indcs + 2 * (size_t)(low1 - 1),
+                             8 * (size_t)(low2 - low1 + 1), cudaMemcpyHostToDevice, c->stream));
+  if (nslots)
+    ASOHF_CUDA(cudaMemcpyAsync(d_ids_off, ids_off, 8 * (size_t)nslots, cudaMemcpyHostToDevice, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  *total_out = j;
+  free(realclus); free(indcs); free(nbound); free(ids_off); free(slot_of);
+  return ASOHF_OK;
+}
+
+// Work list: haloes of [low1, low2] with REALCLUS != 0, DMPCLUS descending
+// (largest first keeps the longest CTAs from finishing last).
+int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots) {
+  int nh = low2 - low1 + 1;
+  int32_t* rc = (int32_t*)malloc(4 * (size_t)nh);
+  int32_t* dm = (int32_t*)malloc(4 * (size_t)nh);
+  ASOHF_CUDA(cudaMemcpyAsync(rc, m.d.realclus + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(dm, m.d.dmpclus + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  int32_t* w = (int32_t*)malloc(4 * (size_t)(nh > 0 ? nh : 1));
+  int k = 0;
+  for (int i = 0; i < nh; i++)
+    if (rc[i] != 0) w[k++] = low1 - 1 + i;
+  // sort by DMPCLUS descending (stable)
+  int32_t* tmp = (int32_t*)malloc(4 * (size_t)(k > 0 ? k : 1));
+  for (int width = 1; width < k; width *= 2) {
+    for (int i = 0; i < k; i += 2 * width) {
+      int a = i, am = min(i + width, k), b = am, bm = min(i + 2 * width, k), o = i;
+      while (a < am && b < bm) {
+        if (dm[w[b] - (low1 - 1)] > dm[w[a] - (low1 - 1)]) tmp[o++] = w[b++];
+        else tmp[o++] = w[a++];
+      }
+      while (a < am) tmp[o++] = w[a++];
+      while (b < bm) tmp[o++] = w[b++];
+    }
+    memcpy(w, tmp, 4 * (size_t)k);
+  }
+  free(tmp);
+  free(rc);
+  free(dm);
+  *h_work = w;
+  *nslots = k;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, const asohf_mesh* mesh,
+                                        asohf_catalogue* cat, int lowh1, int lowh2, int on_device) {
+  if (!c || !k || !cat || lowh1 < 1 || lowh2 > cat->nclus) return ASOHF_ERR_INVALID;
+  if (lowh2 < lowh1) return ASOHF_OK;
+  if (c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
+  if (k->do_compute_energies == 1) return ASOHF_ERR_UNSUPPORTED;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int nh = lowh2 - lowh1 + 1;
+  size_t need = cat_bytes(lowh2) + (size_t)nh * 64 + 65536;
+  ASOHF_CHECK(arena_reserve(c, need));
+  CatMirror m;
+  ASOHF_CHECK(cat_mirror_in(c, cat, lowh2, on_device, &m));
+  int32_t* hw;
+  int ns;
+  ASOHF_CHECK(make_work(c, m, lowh1, lowh2, &hw, &ns));
+  Store S = store_of(c);
+  ColIdx ci = col_idx(c, k);
+  HConst H = hconst(k, mesh);
+  int rc = ASOHF_OK;
+  if (ns > 0) {
+    // per-slot buffers
+    int32_t* d_work = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    GrowOut g;
+    g.cx = (float*)arena_alloc(c, 4 * (size_t)ns);
+    g.cy = (float*)arena_alloc(c, 4 * (size_t)ns);
+    g.cz = (float*)arena_alloc(c, 4 * (size_t)ns);
+    g.rgather = (float*)arena_alloc(c, 4 * (size_t)ns);
+    g.rclus = (float*)arena_alloc(c, 4 * (size_t)ns);
+    g.konta = (int32_t*)arena_alloc(c, 4 * (size_t)ns + 4);
+    g.masadm = (double*)arena_alloc(c, 8 * (size_t)ns);
+    g.status = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int64_t* d_off = (int64_t*)arena_alloc(c, 8 * (size_t)(ns + 1));
+    int32_t* d_nbound = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_nscan = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int64_t* d_ids_off = (int64_t*)arena_alloc(c, 8 * (size_t)ns);
+    if (!d_work || !g.cx || !g.cy || !g.cz || !g.rgather || !g.rclus || !g.konta || !g.masadm || !g.status ||
+        !d_off || !d_nbound || !d_nscan || !d_ids_off) { free(hw); return ASOHF_ERR_CAPACITY; }
+    ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+    k_halo_grow<<<ns, HB, 0, c->stream>>>(S, ci, H, m.d, d_work, g);
+    c->launches++;
+    ASOHF_CUDA(cudaGetLastError());
+    // offsets (host scan: ns is the number of haloes of one level)
+    int32_t* hk = (int32_t*)malloc(4 * (size_t)ns);
+    int32_t* hst = (int32_t*)malloc(4 * (size_t)ns);
+    int64_t* hoff = (int64_t*)malloc(8 * (size_t)(ns + 1));
+    ASOHF_CUDA(cudaMemcpyAsync(hk, g.konta, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    hoff[0] = 0;
+    for (int s = 0; s < ns; s++) {
+      if (hst[s]) rc = hst[s];
+      hoff[s + 1] = hoff[s] + hk[s];
+    }
+    int64_t T = hoff[ns];
+    ASOHF_CUDA(cudaMemcpyAsync(d_off, hoff, 8 * (size_t)(ns + 1), cudaMemcpyHostToDevice, c->stream));
+    // element buffers (allocated after the per-slot ones: the arena grows
+    // only when empty, so reserve everything now)
+    int bits = 1;
+    while ((1ll << bits) < ns) bits++;
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)(T > 0 ? T : 1), 0, 32 + bits);
+    size_t elem = (size_t)T * (8 + 8 + 4 + 4) + tb + ((size_t)T + ns) * (4 + 4 + 8 + 1) + 16384;
+    ASOHF_CHECK(seg_reserve(c, elem));
+    unsigned long long* k0 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
+    unsigned long long* k1 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
+    int32_t* v0 = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
+    int32_t* v1 = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
+    void* t = seg_alloc(c, tb);
+    Seg sg;
+    sg.konta = g.konta;
+    sg.off = d_off;
+    sg.dista = (float*)seg_alloc(c, 4 * ((size_t)T + ns));
+    sg.lip = (int32_t*)seg_alloc(c, 4 * ((size_t)T + ns));
+    sg.pot = (double*)seg_alloc(c, 8 * ((size_t)T + ns));
+    sg.flag = (uint8_t*)seg_alloc(c, (size_t)T + ns);
+    sg.nbound = d_nbound;
+    sg.nscan = d_nscan;
+    sg.status = g.status;
+    if (!k0 || !k1 || !v0 || !v1 || !t || !sg.dista || !sg.lip || !sg.pot || !sg.flag) {
+      free(hk); free(hst); free(hoff); free(hw);
+      return ASOHF_ERR_CAPACITY;
+    }
+    if (T > 0) {
+      k_halo_gather<<<ns, HB, 0, c->stream>>>(S, ci, g.konta, d_off, g.cx, g.cy, g.cz, g.rgather, k0, v0);
+      ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)T, 0, 32 + bits, c->stream));
+      k_tiefix<<<grid_for(T, 256), 256, 0, c->stream>>>(k1, v1, T, 1);
+      c->launches += 2;
+    }
+    sg.keys = k1;
+    sg.vals = v1;
+    k_halo_main<<<ns, HB, 0, c->stream>>>(S, H, m.d, d_work, g, sg);
+    c->launches++;
+    ASOHF_CUDA(cudaGetLastError());
+    ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < ns; s++)
+      if (hst[s] && !rc) rc = hst[s];
+    if (H.want_ids && rc == ASOHF_OK) {
+      int64_t total;
+      ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, ns, d_nbound, d_ids_off, &total));
+      ASOHF_CHECK(ensure_pph(c, total));
+      k_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+      c->launches++;
+      ASOHF_CUDA(cudaGetLastError());
+      c->pph_len = total;
+    }
+    free(hk); free(hst); free(hoff);
+  } else if (H.want_ids) {
+    int64_t total;
+    ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, 0, nullptr, nullptr, &total));
+    c->pph_len = total;
+  }
+  free(hw);
+  ASOHF_CHECK(cat_mirror_out(c, &m));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+extern "C" int asohf_get_particles_per_halo(asohf_ctx* c, int32_t* out, int64_t cap, int64_t* n,
+                                            int on_device) {
+  if (!c || !n) return ASOHF_ERR_INVALID;
+  *n = c->pph_len;
+  if (!out) return ASOHF_OK;
+  if (cap < c->pph_len) return ASOHF_ERR_CAPACITY;
+  if (c->pph_len > 0)
+    ASOHF_CUDA(cudaMemcpyAsync(out, c->d_pph, 4 * (size_t)c->pph_len,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}

@@ -1,0 +1,274 @@
+// poisson.cu -- periodic FFT Poisson solve (MOMENTO + POFFT3D, poisson.f:98-249)
+// and the differentiable deposit+Poisson layer with its adjoint.
+//
+// The reference packs the real density into a full complex array and runs a
+// complex FFT (Numerical-Recipes FOURN) forward, multiplies by KKK, inverse,
+// real part / N^3.  For real input that is exactly an R2C / C2R pair on the
+// half spectrum, which is what cuFFT runs here; the Green's function
+// KKK = -(DX/2)^2 / sum sin^2(pi k/N) (KKK(1,1,1) from the 1e30 denominator)
+// and the 1/N^3 normalisation are applied in one pass over the half
+// spectrum.
+#include <cufft.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "common.cuh"
+
+int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* dradx, int batch,
+                         int64_t n_per, const float* x, const float* y, const float* z,
+                         const float* m, float* acc);
+
+#define ASOHF_CUFFT(call)                                                        \
+  do {                                                                           \
+    cufftResult r_ = (call);                                                     \
+    if (r_ != CUFFT_SUCCESS) {                                                   \
+      asohf_set_last_cuda_error(cudaErrorUnknown, #call, __FILE__, __LINE__);    \
+      return ASOHF_ERR_CUDA;                                                     \
+    }                                                                            \
+  } while (0)
+
+struct FftPlan {
+  int nx = 0, batch = 0;
+  cufftHandle r2c = 0, c2r = 0;
+  cudaStream_t stream = 0;
+};
+
+static FftPlan g_plans[8];
+
+static int get_plan(asohf_ctx* c, int nx, int batch, FftPlan** out) {
+  for (auto& p : g_plans)
+    if (p.nx == nx && p.batch == batch) {
+      if (p.stream != c->stream) {
+        ASOHF_CUFFT(cufftSetStream(p.r2c, c->stream));
+        ASOHF_CUFFT(cufftSetStream(p.c2r, c->stream));
+        p.stream = c->stream;
+      }
+      *out = &p;
+      return ASOHF_OK;
+    }
+  FftPlan* slot = nullptr;
+  for (auto& p : g_plans)
+    if (p.nx == 0) { slot = &p; break; }
+  if (!slot) {
+    slot = &g_plans[0];
+    cufftDestroy(slot->r2c);
+    cufftDestroy(slot->c2r);
+    *slot = FftPlan();
+  }
+  int n[3] = {nx, nx, nx};
+  int64_t g = (int64_t)nx * nx * nx, gc = (int64_t)nx * nx * (nx / 2 + 1);
+  ASOHF_CUFFT(cufftPlanMany(&slot->r2c, 3, n, nullptr, 1, (int)g, nullptr, 1, (int)gc, CUFFT_R2C, batch));
+  ASOHF_CUFFT(cufftPlanMany(&slot->c2r, 3, n, nullptr, 1, (int)gc, nullptr, 1, (int)g, CUFFT_C2R, batch));
+  ASOHF_CUFFT(cufftSetStream(slot->r2c, c->stream));
+  ASOHF_CUFFT(cufftSetStream(slot->c2r, c->stream));
+  slot->nx = nx;
+  slot->batch = batch;
+  slot->stream = c->stream;
+  *out = slot;
+  return ASOHF_OK;
+}
+
+// sin^2(pi k / N) per axis index, REAL*4 as MOMENTO computes it (host sinf).
+static void momento_axis(int nx, float* s2) {
+  float pi = acosf(-1.0f);
+  float consta = pi / (float)nx;
+  int n2 = nx / 2 + 2;
+  for (int i = 1; i <= nx; i++) {
+    int k = (i >= n2) ? i - nx - 1 : i - 1;
+    float s = sinf(consta * (float)k);
+    s2[i - 1] = s * s;
+  }
+}
+
+// Half-spectrum multiply: spec[(k*N + j)*(N/2+1) + i] *= KKK(i,j,k) / N^3.
+__global__ void k_green(cufftComplex* __restrict__ spec, int nx, int batch, const float* __restrict__ s2,
+                        float del2, float inv_n3) {
+  int nh = nx / 2 + 1;
+  int64_t per = (int64_t)nx * nx * nh;
+  int64_t tot = per * batch;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = q % per;
+    int i = (int)(r % nh);
+    int j = (int)((r / nh) % nx);
+    int k = (int)(r / ((int64_t)nh * nx));
+    float den = (i == 0 && j == 0 && k == 0) ? 1.0e30f : __fadd_rn(__fadd_rn(s2[i], s2[j]), s2[k]);
+    float kkk = -del2 / den;
+    float f = __fmul_rn(kkk, inv_n3);
+    cufftComplex v = spec[q];
+    v.x = __fmul_rn(v.x, f);
+    v.y = __fmul_rn(v.y, f);
+    spec[q] = v;
+  }
+}
+
+static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* rho, float* pot) {
+  int64_t gc = (int64_t)nx * nx * (nx / 2 + 1) * batch;
+  cufftComplex* spec = (cufftComplex*)arena_alloc(c, sizeof(cufftComplex) * gc);
+  float* ds2 = (float*)arena_alloc(c, 4 * (size_t)nx);
+  if (!spec || !ds2) return ASOHF_ERR_CAPACITY;
+  float* hs2 = (float*)malloc(4 * (size_t)nx);
+  momento_axis(nx, hs2);
+  ASOHF_CUDA(cudaMemcpyAsync(ds2, hs2, 4 * (size_t)nx, cudaMemcpyHostToDevice, c->stream));
+  FftPlan* P;
+  int rc = get_plan(c, nx, batch, &P);
+  if (rc) { free(hs2); return rc; }
+  ASOHF_CUFFT(cufftExecR2C(P->r2c, (cufftReal*)rho, spec));
+  float del2 = (dx * 0.5f) * (dx * 0.5f);
+  float inv_n3 = 1.0f / ((float)nx * (float)nx * (float)nx);
+  k_green<<<grid_for(gc, 256, c->num_sms * 8), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2, inv_n3);
+  c->launches++;
+  ASOHF_CUFFT(cufftExecC2R(P->c2r, spec, (cufftReal*)pot));
+  ASOHF_CUDA(cudaGetLastError());
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  free(hs2);
+  return ASOHF_OK;
+}
+
+static size_t poisson_bytes(int nx, int batch) {
+  return sizeof(cufftComplex) * (size_t)nx * nx * (nx / 2 + 1) * batch + 4 * (size_t)nx + 4096;
+}
+
+extern "C" int asohf_poisson_fft(asohf_ctx* c, int nx, float dx, int batch, const float* rho,
+                                 float* pot, int on_device) {
+  if (!c || nx < 2 || batch < 1 || !rho || !pot) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t g = (int64_t)nx * nx * nx * batch;
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + (on_device ? 0 : 8 * g) + 1024));
+  const float* drho = rho;
+  float* dpot = pot;
+  if (!on_device) {
+    float* t = (float*)arena_alloc(c, 4 * g);
+    dpot = (float*)arena_alloc(c, 4 * g);
+    ASOHF_CUDA(cudaMemcpyAsync(t, rho, 4 * g, cudaMemcpyHostToDevice, c->stream));
+    drho = t;
+  }
+  ASOHF_CHECK(poisson_dev(c, nx, dx, batch, drho, dpot));
+  if (!on_device) {
+    ASOHF_CUDA(cudaMemcpyAsync(pot, dpot, 4 * g, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return ASOHF_OK;
+}
+
+// ------------------------------------------------------------ layer
+__global__ void k_scale_inv(float* __restrict__ a, int64_t n, float d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = a[i] / d;
+}
+
+extern "C" int asohf_tsc_poisson_forward(asohf_ctx* c, int nx, float lado0, float dx,
+                                         const float* radx, float rote, float rete, int batch,
+                                         int64_t n_per, const float* x, const float* y,
+                                         const float* z, const float* m, float* rho, float* pot) {
+  if (!c || nx < 2 || batch < 1 || n_per < 0 || !radx || !rho || !pot) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t g = (int64_t)nx * nx * nx * batch;
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * (size_t)(nx + 2) + 1024));
+  float* dradx = (float*)arena_alloc(c, 4 * (size_t)(nx + 2));
+  ASOHF_CUDA(cudaMemcpyAsync(dradx, radx, 4 * (size_t)(nx + 2), cudaMemcpyHostToDevice, c->stream));
+  ASOHF_CUDA(cudaMemsetAsync(rho, 0, 4 * g, c->stream));
+  ASOHF_CHECK(tsc_base_batched_f32(c, nx, -lado0 / 2.0f, dx, dradx, batch, n_per, x, y, z, m, rho));
+  float denbas = dx * dx * dx * rote * (rete * rete * rete);
+  k_scale_inv<<<grid_for(g, 256, c->num_sms * 8), 256, 0, c->stream>>>(rho, g, denbas);
+  c->launches++;
+  return poisson_dev(c, nx, dx, batch, rho, pot);
+}
+
+// dW/dx of the three TSC weights (grids.f:1194-1213):
+//   W- = 0.5 (1.5-b)^2, W0 = 0.75-b^2, W+ = 0.5 (1.5-b)^2, b = |x-r|/d.
+__device__ __forceinline__ void tsc_w_dw(float xp, float rm, float r0, float rp, float d, float* w, float* dw) {
+  float s, b, t;
+  s = xp - rm; b = fabsf(s) / d; t = 1.5f - b;
+  w[0] = 0.5f * t * t; dw[0] = -t * copysignf(1.0f, s) / d;
+  s = xp - r0; b = fabsf(s) / d;
+  w[1] = 0.75f - b * b; dw[1] = -2.0f * b * copysignf(1.0f, s) / d;
+  s = xp - rp; b = fabsf(s) / d; t = 1.5f - b;
+  w[2] = 0.5f * t * t; dw[2] = -t * copysignf(1.0f, s) / d;
+}
+
+// dL/dx_p = m_p/DENBAS * sum_c d(Wx Wy Wz)/dx_p * g_c,  g = G * w.
+__global__ void k_tsc_adjoint(const float* __restrict__ x, const float* __restrict__ y,
+                              const float* __restrict__ z, const float* __restrict__ m, int64_t n_per,
+                              int batch, int nx, float xl, float dx, const float* __restrict__ radx,
+                              const float* __restrict__ gfield, float inv_denbas, float* __restrict__ gx,
+                              float* __restrict__ gy, float* __restrict__ gz, float* __restrict__ gm) {
+  int64_t ntot = n_per * batch;
+  size_t G = (size_t)nx * nx * nx;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < ntot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int b = (int)(q / n_per);
+    float xp = x[q], yp = y[q], zp = z[q];
+    int ix = (int)((xp - xl) / dx) + 1, jy = (int)((yp - xl) / dx) + 1, kz = (int)((zp - xl) / dx) + 1;
+    ix = ix < 1 ? 1 : (ix > nx ? nx : ix);
+    jy = jy < 1 ? 1 : (jy > nx ? nx : jy);
+    kz = kz < 1 ? 1 : (kz > nx ? nx : kz);
+    float wx[3], wy[3], wz[3], dwx[3], dwy[3], dwz[3];
+    tsc_w_dw(xp, radx[ix - 1], radx[ix], radx[ix + 1], dx, wx, dwx);
+    tsc_w_dw(yp, radx[jy - 1], radx[jy], radx[jy + 1], dx, wy, dwy);
+    tsc_w_dw(zp, radx[kz - 1], radx[kz], radx[kz + 1], dx, wz, dwz);
+    const float* g = gfield + (size_t)b * G;
+    float ax = 0.f, ay = 0.f, az = 0.f, am = 0.f;
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      int k1 = kz + kk;
+      if (k1 == nx + 1) k1 = 1;
+      if (k1 == 0) k1 = nx;
+#pragma unroll
+      for (int jj = -1; jj <= 1; jj++) {
+        int j1 = jy + jj;
+        if (j1 == nx + 1) j1 = 1;
+        if (j1 == 0) j1 = nx;
+#pragma unroll
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = ix + ii;
+          if (i1 == nx + 1) i1 = 1;
+          if (i1 == 0) i1 = nx;
+          float gv = g[((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1)];
+          ax += dwx[ii + 1] * wy[jj + 1] * wz[kk + 1] * gv;
+          ay += wx[ii + 1] * dwy[jj + 1] * wz[kk + 1] * gv;
+          az += wx[ii + 1] * wy[jj + 1] * dwz[kk + 1] * gv;
+          am += wx[ii + 1] * wy[jj + 1] * wz[kk + 1] * gv;
+        }
+      }
+    }
+    float mp = m[q] * inv_denbas;
+    gx[q] = mp * ax;
+    gy[q] = mp * ay;
+    gz[q] = mp * az;
+    if (gm) gm[q] = am * inv_denbas;
+  }
+}
+
+extern "C" int asohf_tsc_poisson_adjoint(asohf_ctx* c, int nx, float lado0, float dx,
+                                         const float* radx, float rote, float rete, int batch,
+                                         int64_t n_per, const float* x, const float* y,
+                                         const float* z, const float* m, const float* w,
+                                         float* grad_x, float* grad_y, float* grad_z, float* grad_m) {
+  if (!c || nx < 2 || batch < 1 || !radx || !w || !grad_x || !grad_y || !grad_z) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int64_t g = (int64_t)nx * nx * nx * batch;
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * g + 4 * (size_t)(nx + 2) + 2048));
+  float* dradx = (float*)arena_alloc(c, 4 * (size_t)(nx + 2));
+  float* gfield = (float*)arena_alloc(c, 4 * g);
+  if (!dradx || !gfield) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaMemcpyAsync(dradx, radx, 4 * (size_t)(nx + 2), cudaMemcpyHostToDevice, c->stream));
+  // the Green's operator is real and symmetric: its adjoint is itself
+  ASOHF_CHECK(poisson_dev(c, nx, dx, batch, w, gfield));
+  float denbas = dx * dx * dx * rote * (rete * rete * rete);
+  int64_t ntot = n_per * batch;
+  if (ntot > 0) {
+    k_tsc_adjoint<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        x, y, z, m, n_per, batch, nx, -lado0 / 2.0f, dx, dradx, gfield, 1.0f / denbas, grad_x, grad_y,
+        grad_z, grad_m);
+    c->launches++;
+  }
+  ASOHF_CUDA(cudaGetLastError());
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}

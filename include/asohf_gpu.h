@@ -1,0 +1,134 @@
+/*
+ * asohf_gpu.h -- C ABI of libasohf_gpu.so, the B200 (sm_100a) implementation
+ * of the ASOHF particle hot path.
+ *
+ * Each entry point replaces one subroutine of the reference Fortran driver
+ * (dvallesp/ASOHF) and keeps its argument meaning; the Fortran side binds
+ * them with ISO_C_BINDING (fortran/asohf_gpu_mod.f90).  All calls:
+ *   - return 0 on success or an ASOHF_ERR_* status (asohf_types.h), the
+ *     reference's `STOP 1` exits; asohf_strerror() gives the message;
+ *   - run on the context's CUDA stream and return once their results are in
+ *     the output arrays (host outputs) or enqueued (device outputs);
+ *   - never fall back to the CPU: without a usable device they return
+ *     ASOHF_ERR_NO_DEVICE.
+ * `on_device` = 0: array arguments are host pointers (the library stages
+ * them); 1: they are device pointers of the context's device.
+ * A context is not re-entrant: one host thread drives it at a time.
+ */
+#ifndef ASOHF_GPU_H
+#define ASOHF_GPU_H
+
+#include <stdint.h>
+#include "asohf_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct asohf_ctx asohf_ctx;
+
+/* Status text (for the Fortran shim's `WRITE(*,*)` before `STOP 1`). */
+const char *asohf_strerror(int code);
+/* Detail of the last CUDA failure seen by the library in this process. */
+const char *asohf_last_error_detail(void);
+
+/* Context: device, stream, device particle store and scratch arena. */
+int asohf_create(int device, asohf_ctx **out);
+int asohf_destroy(asohf_ctx *ctx);
+int asohf_set_stream(asohf_ctx *ctx, void *cuda_stream);
+int asohf_synchronize(asohf_ctx *ctx);
+/* Number of kernels this context has launched (diagnostics). */
+int64_t asohf_launch_count(asohf_ctx *ctx);
+
+/* MODULE PARTICLES (particles.f:1-14) / READ_AND_ALLOC_PARTICLES
+ * (alloc.f:196-528): copies the particle arrays into the device store,
+ * which stays resident across calls.  Download copies the store back (in
+ * its current order: the sorts below permute it in place, as the Fortran
+ * permutes RXPA.., ORIPA). */
+int asohf_upload_particles(asohf_ctx *ctx, const asohf_particles *src, int on_device);
+int asohf_download_particles(asohf_ctx *ctx, asohf_particles *dst, int on_device);
+
+/* SORT_DM_PARTICLES_LOCALDENSITY (reader.f:140-336): NGP density on the
+ * NX^3 grid, species INT(LOG(rho)/LOG(8)) in [0, N_ESP-1], stable sort of
+ * the store by species.  npart_esp: host array of N_ESP counts (out). */
+int asohf_sort_dm_particles_localdensity(asohf_ctx *ctx, int nx, float dx, float rodo,
+                                         float re0, int32_t *npart_esp);
+
+/* DENSITY (grids.f:710-994) with COMPUTE_KERNELS (grids.f:997-1067): kernel
+ * deposit of the store (species-sorted, counts npart_esp) onto the periodic
+ * base grid u1 (NX^3, column-major) and the patches u11 (32^3 per patch,
+ * sum(mesh->npatch) patches). */
+int asohf_density(asohf_ctx *ctx, int nx, float lado0, float dx, float rote, float rete,
+                  const int32_t *npart_esp, const asohf_mesh *mesh, int interp_degree,
+                  float *u1, float *u11, int on_device);
+
+/* RENORM_DENSITY (grids.f:2668-2722): u1, u11 /= fdm in place. */
+int asohf_renorm_density(asohf_ctx *ctx, int nx, const asohf_mesh *mesh, float fdm,
+                         float *u1, float *u11, int on_device);
+
+/* INTERPOLATE_DENSITY_TSC (grids.f:1070-1398): true TSC deposit of the store
+ * onto u1 and u11.  radx: host array RADX(0:NX+1) from MALLA. */
+int asohf_interpolate_density_tsc(asohf_ctx *ctx, int nx, float lado0, float dx,
+                                  const float *radx, float rote, float rete,
+                                  const asohf_mesh *mesh, float *u1, float *u11, int on_device);
+
+/* MOMENTO + POFFT3D (poisson.f:98-249): periodic potential of `batch`
+ * fields rho (NX^3 each) into pot.  Green's function -(DX/2)^2/sum sin^2,
+ * zero mode from the 1e30 denominator. */
+int asohf_poisson_fft(asohf_ctx *ctx, int nx, float dx, int batch, const float *rho,
+                      float *pot, int on_device);
+
+/* Deposit + Poisson for `batch` particle sets of n_per particles each
+ * (device arrays of batch*n_per): base-grid TSC of INTERPOLATE_DENSITY_TSC
+ * (grids.f:1163-1239, periodic) scaled by 1/(DX^3 ROTE RETE^3), then the
+ * FFT solve; rho and pot receive batch*NX^3 values.  No counterpart routine
+ * in the reference: it chains the two routines POISSON calls
+ * (poisson.f:41-51) for the differentiable layer. */
+int asohf_tsc_poisson_forward(asohf_ctx *ctx, int nx, float lado0, float dx, const float *radx,
+                              float rote, float rete, int batch, int64_t n_per,
+                              const float *x, const float *y, const float *z, const float *m,
+                              float *rho, float *pot);
+/* Adjoint of asohf_tsc_poisson_forward: given w = dL/dpot (batch*NX^3),
+ * writes dL/dx, dL/dy, dL/dz (batch*n_per) and, if grad_m is not NULL,
+ * dL/dm.  The Green's multiply is self-adjoint; the deposit's adjoint is a
+ * TSC gather of the gradient of G*w. */
+int asohf_tsc_poisson_adjoint(asohf_ctx *ctx, int nx, float lado0, float dx, const float *radx,
+                              float rote, float rete, int batch, int64_t n_per,
+                              const float *x, const float *y, const float *z, const float *m,
+                              const float *w, float *grad_x, float *grad_y, float *grad_z,
+                              float *grad_m);
+
+/* SORT_DM_PARTICLES_X (grids.f:2726-2838): ARGSORT of x with its tie rule
+ * (num.f:150-203), store permuted, slab table NDMPART_X(0:NX) written to
+ * the host array ndmpart_x (nx+1 entries).  Also builds the (y,z) column
+ * index the per-halo queries use. */
+int asohf_sort_dm_particles_x(asohf_ctx *ctx, int nx, float lado0, int32_t *ndmpart_x);
+
+/* PRUNE_POOR_HALOES (haloes_particles.f:185-256) over haloes low1..low2
+ * (Fortran 1-based, inclusive). */
+int asohf_prune_poor_haloes(asohf_ctx *ctx, const asohf_consts *k, asohf_catalogue *cat,
+                            int low1, int low2, float facrad, int do_need_to_count,
+                            int on_device);
+
+/* HALOFIND_PARTICLES (haloes_particles.f:578-1411) over haloes
+ * lowh1..lowh2: recentering, SO growth, radial sort, unbinding, SO walk,
+ * properties and bound-particle IDs (appended to the context's
+ * PARTICLES_PER_HALO stream; INDCS_PARTICLES_PER_HALO in cat). */
+int asohf_halofind_particles(asohf_ctx *ctx, const asohf_consts *k, const asohf_mesh *mesh,
+                             asohf_catalogue *cat, int lowh1, int lowh2, int on_device);
+
+/* SUBSTRUCTURE_PARTICLES (substructure.f:756-1697) over the subhaloes of
+ * level ir; subs_lev: host array SUBS_LEV(0:NL) (mesh->nl+1 entries). */
+int asohf_substructure_particles(asohf_ctx *ctx, const asohf_consts *k, const asohf_mesh *mesh,
+                                 asohf_catalogue *cat, int ir, const int32_t *subs_lev,
+                                 int on_device);
+
+/* PARTICLES_PER_HALO (particles.f:12): copies the ID stream (host out);
+ * *n receives its length (the largest INDCS_PARTICLES_PER_HALO(2,.)). */
+int asohf_get_particles_per_halo(asohf_ctx *ctx, int32_t *out, int64_t cap, int64_t *n,
+                                 int on_device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASOHF_GPU_H */

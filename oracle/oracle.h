@@ -1,0 +1,84 @@
+/*
+ * oracle.h -- CPU oracle of the ASOHF particle hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: loaded by tests/, the smoke check and the CPU
+ * baseline leg of bench.py, as the checker.  The product library never links
+ * or calls it.  Parity status: unpinned by the reference (no Fortran compiler
+ * to build it, no reference tests or fixtures); pinned instead by analytic
+ * known-answer tests and by golden vectors generated from this restatement.
+ */
+#ifndef ASOHF_ORACLE_H
+#define ASOHF_ORACLE_H
+
+#include <stdint.h>
+#include "../include/asohf_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_FP32 = 0, ORC_FP64 = 1 };
+
+typedef struct orc_cosmo {
+  float pi, ache, rodo, re0, cgr, rote, rete, uv, um, contrastec, omegaz;
+} orc_cosmo;
+
+void orc_malla(int nx, float lado0, float *radx, float *dx_out);
+void orc_cosmology(float hubble_h, float omega0, float zeta, orc_cosmo *c);
+void orc_compute_kernels(int nl, int interp_degree, float *kernels);
+void orc_density(int nx, float lado0, float dx, float rote, float rete,
+                 const float *x, const float *y, const float *z,
+                 const float *m, const int32_t *npart_esp,
+                 const asohf_mesh *mesh, int interp_degree, int mode,
+                 float *u1, float *u11);
+void orc_renorm_density(int nx, const asohf_mesh *mesh, float fdm, float *u1, float *u11);
+int orc_species_sort(int64_t n, float *x, float *y, float *z, float *vx,
+                     float *vy, float *vz, float *m, int32_t *id, int nx,
+                     float dx, float rodo, float re0, int32_t *npart_esp,
+                     int32_t *species_out);
+void orc_permute(int64_t n, const int64_t *idx, float *x, float *y, float *z,
+                 float *vx, float *vy, float *vz, float *m, int32_t *id);
+void orc_tsc_deposit(int nx, float lado0, float dx, const float *radx, float rote,
+                     float rete, int64_t n, const float *x, const float *y,
+                     const float *z, const float *m, const asohf_mesh *mesh,
+                     int mode, float *u1, float *u11);
+void orc_momento(int nx, float dx, float *kkk);
+void orc_poisson_fft(int nx, float dx, const float *u1, float *pot);
+void orc_argsort(int64_t n, const float *a, int64_t *indx);
+void orc_sort_x(int64_t n, float *x, float *y, float *z, float *vx, float *vy,
+                float *vz, float *m, int32_t *id, int nx, float lado0,
+                int32_t *ndmpart_x);
+
+/* Halo side (oracle_halo.c). The particle arrays are the x-sorted store. */
+typedef struct orc_store {
+  int64_t n;
+  const float *x, *y, *z, *vx, *vy, *vz, *m;
+  const int32_t *id;
+  const int32_t *ndmpart_x; /* NDMPART_X(0:NX) */
+  float norma;              /* MAXVAL(MASAP) */
+} orc_store;
+
+void orc_find_particle_indices(float cx, float r, float xldom, float dx, int nmax,
+                               const int32_t *ndmpart_x, int64_t *lowp1, int64_t *lowp2);
+void orc_prune_poor_haloes(const orc_store *st, const asohf_consts *k,
+                           asohf_catalogue *cat, int low1, int low2,
+                           float facrad, int do_need_to_count);
+/* HALOFIND_PARTICLES for haloes low1..low2 (Fortran 1-based, inclusive).
+ * The bound-particle ID stream is written to pph (capacity pph_cap) and the
+ * total used length returned in *pph_len.  Returns a status code. */
+int orc_halofind_particles(const orc_store *st, const asohf_consts *k,
+                           const asohf_mesh *mesh, asohf_catalogue *cat,
+                           int low1, int low2, int32_t *pph, int64_t pph_cap,
+                           int64_t *pph_len, int nthreads);
+/* SUBSTRUCTURE_PARTICLES for sub-level ir; subs_lev has nl+1 entries. */
+int orc_substructure_particles(const orc_store *st, const asohf_consts *k,
+                               const asohf_mesh *mesh, asohf_catalogue *cat,
+                               int ir, const int32_t *subs_lev, int32_t *pph,
+                               int64_t pph_cap, int64_t *pph_len, int nthreads);
+void orc_diagonalise(const float *input_matrix, float *eigen_out);
+void orc_sort_eigen(float *e, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

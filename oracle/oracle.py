@@ -1,0 +1,239 @@
+"""Python binding of the CPU oracle (liboracle.so).  TEST INFRASTRUCTURE ONLY.
+
+The oracle is a C restatement of the reference Fortran routines of the
+particle hot path (oracle_grid.c, oracle_halo.c).  Only tests/, the smoke
+check and bench.py's CPU-baseline leg use it, as the checker.  Parity status:
+unpinned by the reference (no Fortran compiler here, no reference tests or
+fixtures); pinned by analytic known-answer tests and committed golden vectors.
+
+``OracleBackend`` exposes the same methods as the GPU backend
+(asohf_b200.api.GpuBackend) so one driver (asohf_b200.driver) runs either.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from asohf_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+class CosmoC(C.Structure):
+    _fields_ = [(f, C.c_float) for f in
+                ["pi", "ache", "rodo", "re0", "cgr", "rote", "rete", "uv", "um",
+                 "contrastec", "omegaz"]]
+
+
+class StoreC(C.Structure):
+    _fields_ = [("n", C.c_int64), ("x", _fp), ("y", _fp), ("z", _fp), ("vx", _fp),
+                ("vy", _fp), ("vz", _fp), ("m", _fp), ("id", _ip), ("ndmpart_x", _ip),
+                ("norma", C.c_float)]
+
+
+def build():
+    """Compiles liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        srcs = [os.path.join(_HERE, f) for f in ("oracle_grid.c", "oracle_halo.c", "oracle.h")]
+        if not os.path.exists(path) or any(os.path.getmtime(s) > os.path.getmtime(path) for s in srcs):
+            build()
+        _LIB = C.CDLL(path)
+        _LIB.orc_species_sort.restype = C.c_int
+        _LIB.orc_halofind_particles.restype = C.c_int
+        _LIB.orc_substructure_particles.restype = C.c_int
+    return _LIB
+
+
+def P(a, t=_fp):
+    return a.ctypes.data_as(t)
+
+
+def malla(nx, lado0):
+    radx = np.zeros(nx + 2, np.float32)
+    dx = C.c_float()
+    lib().orc_malla(C.c_int(nx), C.c_float(lado0), P(radx), C.byref(dx))
+    return radx, np.float32(dx.value)
+
+
+def cosmology(h, omega0, zeta):
+    c = CosmoC()
+    lib().orc_cosmology(C.c_float(h), C.c_float(omega0), C.c_float(zeta), C.byref(c))
+    return {f: np.float32(getattr(c, f)) for f, _ in CosmoC._fields_}
+
+
+def compute_kernels(nl, interp_degree=2):
+    W = 2 * 512 + 1
+    k = np.zeros((abi.NLEVELS + 1, W), np.float32)
+    lib().orc_compute_kernels(C.c_int(nl), C.c_int(interp_degree), P(k))
+    return k
+
+
+def argsort(a):
+    a = np.ascontiguousarray(a, np.float32)
+    idx = np.zeros(a.shape[0], np.int64)
+    lib().orc_argsort(C.c_int64(a.shape[0]), P(a), P(idx, _lp))
+    return idx - 1
+
+
+def momento(nx, dx):
+    k = np.zeros(nx ** 3, np.float32)
+    lib().orc_momento(C.c_int(nx), C.c_float(dx), P(k))
+    return k.reshape(nx, nx, nx)  # [k][j][i]
+
+
+def poisson_fft(u1, dx):
+    nx = u1.shape[0]
+    u1 = np.ascontiguousarray(u1, np.float32)
+    pot = np.zeros_like(u1)
+    lib().orc_poisson_fft(C.c_int(nx), C.c_float(dx), P(u1), P(pot))
+    return pot
+
+
+class Particles:
+    """Host SoA particle arrays (owned copies)."""
+
+    def __init__(self, x, y, z, vx, vy, vz, m, id):
+        f = lambda a: np.ascontiguousarray(a, np.float32).copy()
+        self.x, self.y, self.z = f(x), f(y), f(z)
+        self.vx, self.vy, self.vz = f(vx), f(vy), f(vz)
+        self.m = f(m)
+        self.id = np.ascontiguousarray(id, np.int32).copy()
+
+    @property
+    def n(self):
+        return self.x.shape[0]
+
+    def ptrs(self):
+        return (P(self.x), P(self.y), P(self.z), P(self.vx), P(self.vy), P(self.vz), P(self.m),
+                P(self.id, _ip))
+
+    @classmethod
+    def from_snapshot(cls, s):
+        return cls(s.x, s.y, s.z, s.vx, s.vy, s.vz, s.m, s.id)
+
+
+class OracleBackend:
+    """Runs each hot-path routine on the CPU oracle.  Methods mirror the
+    reference subroutines; arrays are numpy, Fortran layouts."""
+
+    name = "oracle"
+
+    def __init__(self, nthreads: int = 0):
+        self.nthreads = nthreads or (os.cpu_count() or 1)
+        self.p = None
+        self.ndmpart_x = None
+
+    # particle store
+    def upload(self, parts):
+        self.p = Particles(parts.x, parts.y, parts.z, parts.vx, parts.vy, parts.vz, parts.m, parts.id)
+
+    def download(self) -> Particles:
+        return self.p
+
+    def species_sort(self, nx, dx, rodo, re0):
+        p = self.p
+        npe = np.zeros(abi.N_ESP, np.int32)
+        spec = np.zeros(p.n, np.int32)
+        rc = lib().orc_species_sort(C.c_int64(p.n), *p.ptrs(), C.c_int(nx), C.c_float(dx),
+                                    C.c_float(rodo), C.c_float(re0), P(npe, _ip), P(spec, _ip))
+        if rc:
+            raise RuntimeError(abi.ERRORS[rc])
+        self.species = spec
+        return npe
+
+    def density(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree=2, fp64=True):
+        p = self.p
+        mh = abi.MeshHolder(mesh)
+        u1 = np.zeros(nx ** 3, np.float32)
+        u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)
+        lib().orc_density(C.c_int(nx), C.c_float(lado0), C.c_float(dx), C.c_float(rote),
+                          C.c_float(rete), P(p.x), P(p.y), P(p.z), P(p.m),
+                          P(np.ascontiguousarray(npart_esp, np.int32), _ip), C.byref(mh.c),
+                          C.c_int(interp_degree), C.c_int(1 if fp64 else 0), P(u1), P(u11))
+        return u1.reshape(nx, nx, nx), u11[: mesh.total]
+
+    def renorm_density(self, nx, mesh, fdm, u1, u11):
+        mh = abi.MeshHolder(mesh)
+        u1 = np.ascontiguousarray(u1, np.float32).copy()
+        u11 = np.ascontiguousarray(u11, np.float32).copy()
+        if u11.shape[0] == 0:
+            u11 = np.zeros((1, abi.NAMRX ** 3), np.float32)
+        lib().orc_renorm_density(C.c_int(nx), C.byref(mh.c), C.c_float(fdm), P(u1), P(u11))
+        return u1, u11[: mesh.total]
+
+    def tsc_deposit(self, nx, lado0, dx, radx, rote, rete, mesh, fp64=True, parts=None):
+        p = parts or self.p
+        mh = abi.MeshHolder(mesh)
+        u1 = np.zeros(nx ** 3, np.float32)
+        u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)
+        lib().orc_tsc_deposit(C.c_int(nx), C.c_float(lado0), C.c_float(dx), P(radx),
+                              C.c_float(rote), C.c_float(rete), C.c_int64(p.n), P(p.x), P(p.y),
+                              P(p.z), P(p.m), C.byref(mh.c), C.c_int(1 if fp64 else 0), P(u1),
+                              P(u11))
+        return u1.reshape(nx, nx, nx), u11[: mesh.total]
+
+    def sort_x(self, nx, lado0):
+        p = self.p
+        nd = np.zeros(nx + 1, np.int32)
+        lib().orc_sort_x(C.c_int64(p.n), *p.ptrs(), C.c_int(nx), C.c_float(lado0), P(nd, _ip))
+        self.ndmpart_x = nd
+        return nd
+
+    def _store(self):
+        p = self.p
+        s = StoreC()
+        s.n = p.n
+        s.x, s.y, s.z, s.vx, s.vy, s.vz, s.m, s.id = p.ptrs()
+        s.ndmpart_x = P(self.ndmpart_x, _ip)
+        s.norma = float(p.m.max())
+        return s
+
+    def prune_poor_haloes(self, consts, cat, low1, low2, facrad, do_need_to_count):
+        s = self._store()
+        cc = cat.as_c()
+        lib().orc_prune_poor_haloes(C.byref(s), C.byref(consts), C.byref(cc), C.c_int(low1),
+                                    C.c_int(low2), C.c_float(facrad), C.c_int(do_need_to_count))
+
+    def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
+        s = self._store()
+        cc = cat.as_c()
+        mh = abi.MeshHolder(mesh)
+        n = C.c_int64()
+        rc = lib().orc_halofind_particles(C.byref(s), C.byref(consts), C.byref(mh.c),
+                                          C.byref(cc), C.c_int(low1), C.c_int(low2),
+                                          P(pph, _ip), C.c_int64(pph.shape[0]), C.byref(n),
+                                          C.c_int(self.nthreads))
+        if rc:
+            raise RuntimeError(abi.ERRORS[rc])
+        return n.value
+
+    def substructure_particles(self, consts, mesh, cat, ir, subs_lev, pph):
+        s = self._store()
+        cc = cat.as_c()
+        mh = abi.MeshHolder(mesh)
+        n = C.c_int64()
+        sl = np.ascontiguousarray(subs_lev, np.int32)
+        rc = lib().orc_substructure_particles(C.byref(s), C.byref(consts), C.byref(mh.c),
+                                              C.byref(cc), C.c_int(ir), P(sl, _ip),
+                                              P(pph, _ip), C.c_int64(pph.shape[0]),
+                                              C.byref(n), C.c_int(self.nthreads))
+        if rc:
+            raise RuntimeError(abi.ERRORS[rc])
+        return n.value
+
+    def poisson_fft(self, u1, dx):
+        return poisson_fft(u1, dx)
