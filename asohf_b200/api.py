@@ -58,7 +58,7 @@ def load():
                      "asohf_tsc_poisson_forward", "asohf_tsc_poisson_adjoint",
                      "asohf_sort_dm_particles_x", "asohf_prune_poor_haloes",
                      "asohf_halofind_particles", "asohf_substructure_particles",
-                     "asohf_get_particles_per_halo"]:
+                     "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -113,6 +113,24 @@ class Asohf:
 
     def launch_count(self) -> int:
         return int(self.L.asohf_launch_count(self.h))
+
+    def set_profiling(self, on: bool):
+        """Brackets the main kernels with CUDA events (diagnostics)."""
+        _check(self.L.asohf_set_profiling(self.h, C.c_int(int(on))), "asohf_set_profiling")
+
+    def kernel_stats(self) -> dict:
+        """{kernel name: (total device ms, launches)} since profiling was enabled."""
+        out = {}
+        i = 0
+        while True:
+            name = C.c_char_p()
+            ms = C.c_double()
+            n = C.c_int64()
+            if self.L.asohf_kernel_stats(self.h, C.c_int(i), C.byref(name), C.byref(ms), C.byref(n)) != 0:
+                break
+            out[name.value.decode()] = (ms.value, n.value)
+            i += 1
+        return out
 
     # -------------------------------------------------------------- particles
     def upload_particles(self, x, y, z, vx, vy, vz, m, ids):
@@ -289,15 +307,13 @@ class GpuBackend:
 
     def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
         self.a.halofind_particles(consts, mesh, cat, low1, low2)
-        ids = self.a.particles_per_halo()
-        pph[: ids.shape[0]] = ids
-        return ids.shape[0]
 
     def substructure_particles(self, consts, mesh, cat, ir, subs_lev, pph):
         self.a.substructure_particles(consts, mesh, cat, ir, subs_lev)
-        ids = self.a.particles_per_halo()
-        pph[: ids.shape[0]] = ids
-        return ids.shape[0]
+
+    def final_ids(self, pph, n):
+        """PARTICLES_PER_HALO(1:n), fetched once at the end."""
+        return self.a.particles_per_halo()[:n]
 
     def poisson_fft(self, u1, dx):
         nx = u1.shape[0]
@@ -305,3 +321,36 @@ class GpuBackend:
         pot = np.zeros_like(u1)
         self.a.poisson_fft(nx, dx, u1, pot)
         return pot
+
+
+class DeviceBackend(GpuBackend):
+    """Backend whose particle input and density grids stay on the GPU
+    (torch tensors): nothing crosses PCIe but the catalogue."""
+
+    name = "gpu-device"
+
+    def __init__(self, device: int = 0):
+        super().__init__(device)
+        self._u1 = None
+        self._u11 = None
+
+    def download(self):
+        return None
+
+    def _grids(self, nx, mesh):
+        import torch
+        n11 = max(mesh.total, 1) * abi.NAMRX ** 3
+        if self._u1 is None or self._u1.numel() != nx ** 3:
+            self._u1 = torch.empty(nx ** 3, dtype=torch.float32, device=f"cuda:{self.a.device}")
+        if self._u11 is None or self._u11.numel() < n11:
+            self._u11 = torch.empty(n11, dtype=torch.float32, device=f"cuda:{self.a.device}")
+        return self._u1, self._u11
+
+    def density(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree=2, fp64=True):
+        u1, u11 = self._grids(nx, mesh)
+        self.a.density(nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, u1, u11)
+        return u1, u11
+
+    def renorm_density(self, nx, mesh, fdm, u1, u11):
+        self.a.renorm_density(nx, mesh, fdm, u1, u11)
+        return u1, u11

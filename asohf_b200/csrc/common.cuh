@@ -68,7 +68,19 @@ struct asohf_ctx {
   size_t seg_size = 0, seg_used = 0;
   // counters of kernels launched by this context (reported by the bench)
   int64_t launches = 0;
+  // optional CUDA-event timing of named kernels (asohf_set_profiling)
+  int profiling = 0;
+  struct KRec { const char* name; cudaEvent_t a, b; };
+  KRec* krec = nullptr;
+  int nkrec = 0, capkrec = 0;
+  struct KSum { const char* name; double ms; int64_t n; };
+  KSum ksum[64];
+  int nksum = 0;
 };
+
+// Brackets a kernel launch with events on the context stream when profiling.
+int ktime_begin(asohf_ctx* c, const char* name);
+void ktime_end(asohf_ctx* c, int slot);
 
 // Scratch: reserve() may grow the arena only when nothing is allocated from it.
 int arena_reserve(asohf_ctx* c, size_t bytes);

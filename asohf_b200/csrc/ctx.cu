@@ -171,6 +171,8 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaFree(c->d_pph);
   cudaFree(c->arena);
   cudaFree(c->seg);
+  for (int i = 0; i < c->nkrec; i++) { cudaEventDestroy(c->krec[i].a); cudaEventDestroy(c->krec[i].b); }
+  free(c->krec);
   delete c;
   return ASOHF_OK;
 }
@@ -188,6 +190,71 @@ extern "C" int asohf_synchronize(asohf_ctx* c) {
 }
 
 extern "C" int64_t asohf_launch_count(asohf_ctx* c) { return c ? c->launches : -1; }
+
+int ktime_begin(asohf_ctx* c, const char* name) {
+  if (!c->profiling) return -1;
+  if (c->nkrec == c->capkrec) {
+    int cap = c->capkrec ? 2 * c->capkrec : 256;
+    asohf_ctx::KRec* n = (asohf_ctx::KRec*)realloc(c->krec, sizeof(asohf_ctx::KRec) * cap);
+    if (!n) return -1;
+    c->krec = n;
+    c->capkrec = cap;
+  }
+  asohf_ctx::KRec& r = c->krec[c->nkrec];
+  r.name = name;
+  if (cudaEventCreate(&r.a) != cudaSuccess) return -1;
+  if (cudaEventCreate(&r.b) != cudaSuccess) { cudaEventDestroy(r.a); return -1; }
+  cudaEventRecord(r.a, c->stream);
+  return c->nkrec++;
+}
+
+void ktime_end(asohf_ctx* c, int slot) {
+  if (slot < 0) return;
+  cudaEventRecord(c->krec[slot].b, c->stream);
+}
+
+static void ktime_flush(asohf_ctx* c) {
+  cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < c->nkrec; i++) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->krec[i].a, c->krec[i].b);
+    int k;
+    for (k = 0; k < c->nksum; k++)
+      if (strcmp(c->ksum[k].name, c->krec[i].name) == 0) break;
+    if (k == c->nksum && c->nksum < 64) {
+      c->ksum[k].name = c->krec[i].name;
+      c->ksum[k].ms = 0.0;
+      c->ksum[k].n = 0;
+      c->nksum++;
+    }
+    if (k < 64) {
+      c->ksum[k].ms += ms;
+      c->ksum[k].n++;
+    }
+    cudaEventDestroy(c->krec[i].a);
+    cudaEventDestroy(c->krec[i].b);
+  }
+  c->nkrec = 0;
+}
+
+extern "C" int asohf_set_profiling(asohf_ctx* c, int on) {
+  if (!c) return ASOHF_ERR_INVALID;
+  ktime_flush(c);
+  c->profiling = on;
+  c->nksum = 0;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_kernel_stats(asohf_ctx* c, int i, const char** name, double* total_ms,
+                                  int64_t* launches) {
+  if (!c || !name || !total_ms || !launches) return ASOHF_ERR_INVALID;
+  ktime_flush(c);
+  if (i < 0 || i >= c->nksum) return ASOHF_ERR_INVALID;
+  *name = c->ksum[i].name;
+  *total_ms = c->ksum[i].ms;
+  *launches = c->ksum[i].n;
+  return ASOHF_OK;
+}
 
 extern "C" int asohf_upload_particles(asohf_ctx* c, const asohf_particles* s, int on_device) {
   if (!c || !s || s->n < 0) return ASOHF_ERR_INVALID;

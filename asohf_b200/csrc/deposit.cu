@@ -184,7 +184,11 @@ __global__ void k_iota(int32_t* __restrict__ a, int64_t n) {
 }
 
 int permute_store(asohf_ctx* c, const int64_t* perm) {
-  k_gather8<<<grid_for(c->p.n, 256), 256, 0, c->stream>>>(perm, c->p.n, c->p, c->alt);
+  {
+    int kt_ = ktime_begin(c, "store_permute");
+    k_gather8<<<grid_for(c->p.n, 256), 256, 0, c->stream>>>(perm, c->p.n, c->p, c->alt);
+    ktime_end(c, kt_);
+  }
   c->launches++;
   ASOHF_CUDA(cudaGetLastError());
   ctx_swap_particles(c);
@@ -224,12 +228,20 @@ extern "C" int asohf_sort_dm_particles_localdensity(asohf_ctx* c, int nx, float 
   void* tscan = arena_alloc(c, cub_scan);
   ASOHF_CUDA(cudaMemsetAsync(counts, 0, 4 * g, c->stream));
   float xmin = -((float)nx * dx) / 2.0f;
-  k_ngp_count<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, nx, dx, xmin,
+  {
+    int kt_ = ktime_begin(c, "species_ngp_count");
+    k_ngp_count<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, nx, dx, xmin,
                                                        cell, counts);
+    ktime_end(c, kt_);
+  }
   c->launches++;
   float bas = dx * dx * dx * rodo * (re0 * re0 * re0);
   if (eq) {
-    k_cell_density_eqmass<<<grid_for(g, 256), 256, 0, c->stream>>>(counts, g, c->norma, bas, dens);
+    {
+      int kt_ = ktime_begin(c, "species_cell_density");
+      k_cell_density_eqmass<<<grid_for(g, 256), 256, 0, c->stream>>>(counts, g, c->norma, bas, dens);
+      ktime_end(c, kt_);
+    }
     c->launches++;
   } else {
     // particles of each cell in input order: stable radix sort of (cell, i)
@@ -253,7 +265,11 @@ extern "C" int asohf_sort_dm_particles_localdensity(asohf_ctx* c, int nx, float 
   k_species<<<grid_for(n, 256), 256, 0, c->stream>>>(cell, dens, n, ASOHF_N_ESP, logf(8.0f), spec);
   k_species_block_counts<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, bc);
   ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(tscan, cub_scan, bc, boff, nb * ASOHF_N_ESP, c->stream));
-  k_species_scatter<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, boff, perm);
+  {
+    int kt_ = ktime_begin(c, "species_scatter");
+    k_species_scatter<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, boff, perm);
+    ktime_end(c, kt_);
+  }
   c->launches += 4;
   ASOHF_CUDA(cudaGetLastError());
   int32_t tot[ASOHF_N_ESP];
@@ -661,12 +677,20 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
   if (n > 0) {
     if (fixed) {
       double inv_unit = ldexp(1.0, -shift);
-      k_density_base_fixed<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      {
+        int kt_ = ktime_begin(c, "density_base");
+        k_density_base_fixed<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
           c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, dk + ASOHF_NMAX_KERNELS - 1, inv_unit,
           (unsigned long long*)acc);
+        ktime_end(c, kt_);
+      }
     } else {
-      k_density_base_f64<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      {
+        int kt_ = ktime_begin(c, "density_base");
+        k_density_base_f64<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
           c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, dk + ASOHF_NMAX_KERNELS - 1, (double*)acc);
+        ktime_end(c, kt_);
+      }
     }
     c->launches++;
   }
@@ -699,8 +723,12 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
     ASOHF_CUDA(cudaMemcpyAsync(dend, hend, sizeof(hend), cudaMemcpyHostToDevice, c->stream));
     size_t smem = sizeof(double) * NA * NA * ZH;
     ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_density_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m,
+    {
+      int kt_ = ktime_begin(c, "density_patches");
+      k_density_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m,
                                                            dend, dx, dk, du11, dden);
+      ktime_end(c, kt_);
+    }
     c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     if (!on_device)
@@ -948,8 +976,12 @@ extern "C" int asohf_interpolate_density_tsc(asohf_ctx* c, int nx, float lado0, 
   ASOHF_CUDA(cudaMemsetAsync(acc, 0, 8 * g, c->stream));
   float xl = -lado0 / 2.0f;
   if (n > 0) {
-    k_tsc_base<double><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+    {
+      int kt_ = ktime_begin(c, "tsc_base");
+      k_tsc_base<double><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
         c->p.x, c->p.y, c->p.z, c->p.m, n, 1, nx, xl, dx, dradx, acc);
+      ktime_end(c, kt_);
+    }
     c->launches++;
   }
   float denbas = dx * dx * dx * rote * (rete * rete * rete);
@@ -973,11 +1005,19 @@ extern "C" int asohf_interpolate_density_tsc(asohf_ctx* c, int nx, float lado0, 
     ASOHF_CHECK(stage_out(c, u11, 4 * (size_t)np * NA * NA * NA, on_device, &du11));
     if (!plev || !dden) return ASOHF_ERR_CAPACITY;
     ASOHF_CUDA(cudaMemsetAsync(plev, 0, 4 * n, c->stream));
-    k_tsc_plev<<<np, 256, 0, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, dx, plev);
+    {
+      int kt_ = ktime_begin(c, "tsc_plev");
+      k_tsc_plev<<<np, 256, 0, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, dx, plev);
+      ktime_end(c, kt_);
+    }
     size_t smem = sizeof(double) * NA * NA * ZH;
     ASOHF_CUDA(cudaFuncSetAttribute(k_tsc_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tsc_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m, plev, dx,
+    {
+      int kt_ = ktime_begin(c, "tsc_patches");
+      k_tsc_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m, plev, dx,
                                                          du11, dden);
+      ktime_end(c, kt_);
+    }
     c->launches += 2;
     ASOHF_CUDA(cudaGetLastError());
     if (!on_device)
@@ -993,8 +1033,12 @@ int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* 
                          const float* m, float* acc) {
   int64_t n = n_per * batch;
   if (n > 0) {
-    k_tsc_base<float><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(x, y, z, m, n_per, batch,
+    {
+      int kt_ = ktime_begin(c, "tsc_base_batched");
+      k_tsc_base<float><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(x, y, z, m, n_per, batch,
                                                                               nx, xl, dx, dradx, acc);
+      ktime_end(c, kt_);
+    }
     c->launches++;
   }
   ASOHF_CUDA(cudaGetLastError());

@@ -181,7 +181,11 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
   ASOHF_CHECK(cat_mirror_in(c, cat, low2, on_device, &m));
   int nh = low2 - low1 + 1;
   if (do_need_to_count == 1)
-    k_prune<<<nh, HB, 0, c->stream>>>(col_idx(c, k), m.d, low1, facrad, k->min_num_part);
+    {
+      int kt_ = ktime_begin(c, "prune");
+      k_prune<<<nh, HB, 0, c->stream>>>(col_idx(c, k), m.d, low1, facrad, k->min_num_part);
+      ktime_end(c, kt_);
+    }
   else
     k_prune_nocount<<<(nh + 255) / 256, 256, 0, c->stream>>>(m.d, low1, low2, k->min_num_part);
   c->launches++;
@@ -1193,7 +1197,11 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     if (!d_work || !g.cx || !g.cy || !g.cz || !g.rgather || !g.rclus || !g.konta || !g.masadm || !g.status ||
         !d_off || !d_nbound || !d_nscan || !d_ids_off) { free(hw); return ASOHF_ERR_CAPACITY; }
     ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
-    k_halo_grow<<<ns, HB, 0, c->stream>>>(S, ci, H, m.d, d_work, g);
+    {
+      int kt_ = ktime_begin(c, "halo_grow");
+      k_halo_grow<<<ns, HB, 0, c->stream>>>(S, ci, H, m.d, d_work, g);
+      ktime_end(c, kt_);
+    }
     c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     // offsets (host scan: ns is the number of haloes of one level)
@@ -1239,14 +1247,28 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       return ASOHF_ERR_CAPACITY;
     }
     if (T > 0) {
-      k_halo_gather<<<ns, HB, 0, c->stream>>>(S, ci, g.konta, d_off, g.cx, g.cy, g.cz, g.rgather, k0, v0);
+      {
+        int kt_ = ktime_begin(c, "halo_gather");
+        k_halo_gather<<<ns, HB, 0, c->stream>>>(S, ci, g.konta, d_off, g.cx, g.cy, g.cz, g.rgather, k0, v0);
+        ktime_end(c, kt_);
+      }
+      int kt_ = ktime_begin(c, "halo_radix_sort");
       ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)T, 0, 32 + bits, c->stream));
-      k_tiefix<<<grid_for(T, 256), 256, 0, c->stream>>>(k1, v1, T, 1);
+      ktime_end(c, kt_);
+      {
+        int kt_ = ktime_begin(c, "halo_tiefix");
+        k_tiefix<<<grid_for(T, 256), 256, 0, c->stream>>>(k1, v1, T, 1);
+        ktime_end(c, kt_);
+      }
       c->launches += 2;
     }
     sg.keys = k1;
     sg.vals = v1;
-    k_halo_main<<<ns, HB, 0, c->stream>>>(S, H, m.d, d_work, g, sg);
+    {
+      int kt_ = ktime_begin(c, "halo_main");
+      k_halo_main<<<ns, HB, 0, c->stream>>>(S, H, m.d, d_work, g, sg);
+      ktime_end(c, kt_);
+    }
     c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
@@ -1257,7 +1279,11 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       int64_t total;
       ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, ns, d_nbound, d_ids_off, &total));
       ASOHF_CHECK(ensure_pph(c, total));
-      k_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+      {
+        int kt_ = ktime_begin(c, "halo_write_ids");
+        k_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+        ktime_end(c, kt_);
+      }
       c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       c->pph_len = total;

@@ -114,12 +114,20 @@ static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* r
   FftPlan* P;
   int rc = get_plan(c, nx, batch, &P);
   if (rc) { free(hs2); return rc; }
+  int kt_ = ktime_begin(c, "fft_r2c");
   ASOHF_CUFFT(cufftExecR2C(P->r2c, (cufftReal*)rho, spec));
+  ktime_end(c, kt_);
   float del2 = (dx * 0.5f) * (dx * 0.5f);
   float inv_n3 = 1.0f / ((float)nx * (float)nx * (float)nx);
-  k_green<<<grid_for(gc, 256, c->num_sms * 8), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2, inv_n3);
+  {
+    int kt_ = ktime_begin(c, "green_multiply");
+    k_green<<<grid_for(gc, 256, c->num_sms * 8), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2, inv_n3);
+    ktime_end(c, kt_);
+  }
   c->launches++;
+  kt_ = ktime_begin(c, "fft_c2r");
   ASOHF_CUFFT(cufftExecC2R(P->c2r, spec, (cufftReal*)pot));
+  ktime_end(c, kt_);
   ASOHF_CUDA(cudaGetLastError());
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   free(hs2);
@@ -263,9 +271,13 @@ extern "C" int asohf_tsc_poisson_adjoint(asohf_ctx* c, int nx, float lado0, floa
   float denbas = dx * dx * dx * rote * (rete * rete * rete);
   int64_t ntot = n_per * batch;
   if (ntot > 0) {
-    k_tsc_adjoint<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+    {
+      int kt_ = ktime_begin(c, "tsc_adjoint_gather");
+      k_tsc_adjoint<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(
         x, y, z, m, n_per, batch, nx, -lado0 / 2.0f, dx, dradx, gfield, 1.0f / denbas, grad_x, grad_y,
         grad_z, grad_m);
+      ktime_end(c, kt_);
+    }
     c->launches++;
   }
   ASOHF_CUDA(cudaGetLastError());

@@ -125,9 +125,15 @@ int build_column_index(asohf_ctx* c, int nx, float lado0) {
   void* t = arena_alloc(c, tb);
   if (!k0 || !k1 || !v0 || !v1 || !t) return ASOHF_ERR_CAPACITY;
   k_colkeys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.y, c->p.z, n, c->col_xl, c->col_dx, ncol, k0, v0);
+  int kt_ = ktime_begin(c, "column_index_radix");
   ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)n, 0, bits, c->stream));
-  k_colfill<<<grid_for(n, 256), 256, 0, c->stream>>>(v1, k1, n, c->p.x, c->p.y, c->p.z, c->d_colpart,
+  ktime_end(c, kt_);
+  {
+    int kt_ = ktime_begin(c, "column_index_fill");
+    k_colfill<<<grid_for(n, 256), 256, 0, c->stream>>>(v1, k1, n, c->p.x, c->p.y, c->p.z, c->d_colpart,
                                                      c->d_colstart, ncols);
+    ktime_end(c, kt_);
+  }
   c->launches += 2;
   ASOHF_CUDA(cudaGetLastError());
   return ASOHF_OK;
@@ -167,7 +173,9 @@ extern "C" int asohf_sort_dm_particles_x(asohf_ctx* c, int nx, float lado0, int3
     void* t = arena_alloc(c, tb);
     if (!k0 || !k1 || !v0 || !v1 || !perm || !t) return ASOHF_ERR_CAPACITY;
     k_xkeys_reversed<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, n, k0, v0);
+    int kt_ = ktime_begin(c, "sort_x_radix");
     ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)n, 0, 32, c->stream));
+    ktime_end(c, kt_);
     k_widen<<<grid_for(n, 256), 256, 0, c->stream>>>(v1, n, perm);
     c->launches += 2;
     ASOHF_CHECK(permute_store(c, perm));

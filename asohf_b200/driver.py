@@ -2,9 +2,11 @@
 (asohf.f:418-763), in the same order, on a backend (the B200 library, or
 any object with the same methods).
 
-Stages outside the hot path are stood in for by asohf_b200.synth: the patch
-table (CREATE_MESH) and the halo and subhalo candidates (HALOFIND_GRID,
-SEARCH_SUBSTRUCTURE_GRID).  The catalogue cleaning passes CHECK_RUBISH and
+Stages outside the hot path are stood in for by asohf_b200.synth and
+prepared before the hot path runs (``prepare``): the patch table
+(CREATE_MESH) and the halo candidates (HALOFIND_GRID).  Subhalo candidates
+(SEARCH_SUBSTRUCTURE_GRID) are listed during the run, once the host haloes
+are known.  The catalogue cleaning passes CHECK_RUBISH and
 ACCIDENTAL_SUBSTRUCTURE are not run.  RE_SORT_HALOES (haloes_particles.f:
 2-56), a compaction of the candidate list, is done here on the host.
 """
@@ -12,10 +14,23 @@ from __future__ import annotations
 
 import dataclasses
 import time
+from types import SimpleNamespace
 
 import numpy as np
 
 from . import abi, grid, synth
+
+
+@dataclasses.dataclass
+class Plan:
+    snap: synth.Snapshot
+    radx: np.ndarray
+    dx: np.float32
+    cos: dict
+    consts: abi.ConstsC
+    mesh: synth.Mesh
+    cand: synth.Candidates
+    capacity: int
 
 
 @dataclasses.dataclass
@@ -33,26 +48,33 @@ class RunResult:
     mesh: object
 
 
+CAT_MOVE = ["clusrx", "clusry", "clusrz", "radio", "masa", "levhal", "patchclus", "dmpclus",
+            "clusrxcm", "clusrycm", "clusrzcm"]
+
+
 def re_sort_haloes(cat: abi.Catalogue, nhallev: np.ndarray, ir: int):
     """RE_SORT_HALOES (haloes_particles.f:2-56): drops REALCLUS=0 entries of
-    level ir (the last level appended) and renumbers positive REALCLUS."""
+    level ir (the last level appended), keeping order, and renumbers
+    positive REALCLUS through the old->new map."""
     low1 = int(nhallev[:ir].sum()) + 1
     low2 = int(nhallev[: ir + 1].sum())
-    j = low1 - 1
-    resort = {}
-    for i in range(low1, low2 + 1):
-        if cat.realclus[i - 1] == 0:
-            continue
-        j += 1
-        resort[i] = j
-        for f in ["clusrx", "clusry", "clusrz", "radio", "masa", "levhal", "patchclus", "dmpclus",
-                  "clusrxcm", "clusrycm", "clusrzcm"]:
-            a = getattr(cat, f)
-            a[j - 1] = a[i - 1]
-        rc = cat.realclus[i - 1]
-        cat.realclus[j - 1] = rc if rc <= 0 else resort.get(int(rc), rc)
-    nhallev[ir] = j - (low1 - 1)
-    cat.nclus = j
+    sl = slice(low1 - 1, low2)
+    rc = cat.realclus[sl].copy()
+    keep = rc != 0
+    k = int(keep.sum())
+    resort = np.zeros(low2 - low1 + 1, np.int64)
+    resort[keep] = np.arange(low1, low1 + k)
+    for f in CAT_MOVE:
+        a = getattr(cat, f)
+        a[low1 - 1: low1 - 1 + k] = a[sl][keep]
+    new = rc[keep]
+    pos = new > 0
+    inside = pos & (new >= low1) & (new <= low2)
+    new[inside] = resort[new[inside] - low1]
+    cat.realclus[low1 - 1: low1 - 1 + k] = new
+    nhallev[ir] = k
+    cat.nclus = low1 - 1 + k
+    return keep
 
 
 def make_consts(cfg, dx, cos):
@@ -60,26 +82,32 @@ def make_consts(cfg, dx, cos):
                         np.float32(cfg.zeta), cfg.min_num_part)
 
 
-def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: bool = True,
-        interp_degree: int = 2) -> RunResult:
-    """Runs the hot path on `backend` and returns every stage's output."""
+def prepare(snap: synth.Snapshot, capacity: int | None = None) -> Plan:
     cfg = snap.cfg
-    nx = cfg.nx
-    lado0 = np.float32(cfg.lado0)
-    radx, dx = grid.malla(nx, lado0)
+    radx, dx = grid.malla(cfg.nx, cfg.lado0)
     cos = grid.cosmology(cfg.h, cfg.omega_m, cfg.zeta)
-    consts = make_consts(cfg, dx, cos)
+    mesh = synth.build_mesh(snap, float(dx))
+    cand = synth.build_candidates(snap, mesh, float(dx))
+    nsub = int((snap.halo_host >= 0).sum())
+    cap = capacity or (cand.clusrx.shape[0] + nsub + 16)
+    return Plan(snap, radx, dx, cos, make_consts(cfg, dx, cos), mesh, cand, cap)
+
+
+def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
+            particles=None, download: bool = True) -> RunResult:
+    """Runs the hot path on `backend`; returns every stage's output."""
+    snap, cfg = plan.snap, plan.snap.cfg
+    nx, lado0, dx, cos, consts, mesh, cand = (cfg.nx, np.float32(cfg.lado0), plan.dx, plan.cos,
+                                              plan.consts, plan.mesh, plan.cand)
     T = {}
-    from types import SimpleNamespace
-    parts = SimpleNamespace(x=snap.x, y=snap.y, z=snap.z, vx=snap.vx, vy=snap.vy, vz=snap.vz,
-                            m=snap.m, id=snap.id, n=snap.x.shape[0])
+    parts = particles or SimpleNamespace(x=snap.x, y=snap.y, z=snap.z, vx=snap.vx, vy=snap.vy,
+                                         vz=snap.vz, m=snap.m, id=snap.id, n=snap.x.shape[0])
     t0 = time.perf_counter()
     backend.upload(parts)
     T["upload"] = time.perf_counter() - t0
     t0 = time.perf_counter()
     npe = backend.species_sort(nx, dx, cos["rodo"], cos["re0"])
     T["species_sort"] = time.perf_counter() - t0
-    mesh = synth.build_mesh(snap, float(dx))
     t0 = time.perf_counter()
     u1, u11 = backend.density(nx, lado0, dx, cos["rote"], cos["rete"], npe, mesh, interp_degree)
     u1, u11 = backend.renorm_density(nx, mesh, np.float32(cfg.fdm), u1, u11)
@@ -87,12 +115,9 @@ def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: b
     t0 = time.perf_counter()
     nd = backend.sort_x(nx, lado0)
     T["sort_x"] = time.perf_counter() - t0
-    cand = synth.build_candidates(snap, mesh, float(dx))
-    H = cand.clusrx.shape[0]
-    nsub_max = int((snap.halo_host >= 0).sum())
-    cap = capacity or (H + nsub_max + 16)
-    cat = abi.Catalogue(cap)
-    pph = np.zeros(max(snap.x.shape[0], 1), np.int32)
+    cat = abi.Catalogue(plan.capacity)
+    n_id_cap = max(snap.x.shape[0], 1)
+    pph = np.zeros(n_id_cap, np.int32)
     nhallev = np.zeros(mesh.nl + 1, np.int32)
     base_of_level = np.concatenate([[0], np.cumsum(cand.nhallev)])
     slot_of_truth = {}
@@ -102,7 +127,6 @@ def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: b
         n_new = hi - lo
         if n_new == 0:
             continue
-        # HALOFIND_GRID appends the candidates of level ir
         s0 = cat.nclus
         sl = slice(s0, s0 + n_new)
         cat.clusrx[sl] = cand.clusrx[lo:hi]
@@ -115,17 +139,15 @@ def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: b
         cat.realclus[sl] = -1
         cat.nclus = s0 + n_new
         nhallev[ir] = n_new
-        truth_slots = list(cand.truth[lo:hi])
-        re_sort_haloes(cat, nhallev, ir)
+        truth = cand.truth[lo:hi]
+        truth = truth[re_sort_haloes(cat, nhallev, ir)]
         low1 = int(nhallev[:ir].sum()) + 1
         low2 = int(nhallev[: ir + 1].sum())
         backend.prune_poor_haloes(consts, cat, low1, low2, np.float32(1.0), 1)
-        # RE_SORT_HALOES again, keeping track of which truth halo is where
-        keep = [t for q, t in enumerate(truth_slots) if cat.realclus[low1 - 1 + q] != 0]
-        re_sort_haloes(cat, nhallev, ir)
+        truth = truth[re_sort_haloes(cat, nhallev, ir)]
         low1 = int(nhallev[:ir].sum()) + 1
         low2 = int(nhallev[: ir + 1].sum())
-        for q, t in enumerate(keep):
+        for q, t in enumerate(truth):
             if t >= 0:
                 slot_of_truth[int(t)] = low1 + q
         if nhallev[ir] == 0:
@@ -135,6 +157,7 @@ def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: b
     T["halofind"] = time.perf_counter() - t0
     subs_lev = np.zeros(mesh.nl + 1, np.int32)
     subs_lev[0] = cat.nclus
+    nsub_max = int((snap.halo_host >= 0).sum())
     if with_subs and nsub_max > 0 and mesh.nl >= 1:
         t0 = time.perf_counter()
         sx, sy, sz, srad, shost, struth, slev = synth.build_sub_candidates(
@@ -158,6 +181,14 @@ def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: b
             cat.nclus = s0 + n_new
             backend.substructure_particles(consts, mesh, cat, ir, subs_lev, pph)
         T["substructure"] = time.perf_counter() - t0
-    n_ids = int(max([cat.indcs[i, 1] for i in range(cat.nclus) if cat.realclus[i] != 0] + [0]))
-    return RunResult(npe, u1, u11, nd, cat, pph[:n_ids].copy(), nhallev, subs_lev,
-                     backend.download(), T, mesh)
+    live = cat.realclus[: cat.nclus] != 0
+    n_ids = int(cat.indcs[: cat.nclus][live][:, 1].max()) if live.any() else 0
+    ids = backend.final_ids(pph, n_ids)
+    return RunResult(npe, u1, u11, nd, cat, ids, nhallev, subs_lev,
+                     backend.download() if download else None, T, mesh)
+
+
+def run(snap: synth.Snapshot, backend, capacity: int | None = None, with_subs: bool = True,
+        interp_degree: int = 2) -> RunResult:
+    """prepare + execute."""
+    return execute(prepare(snap, capacity), backend, with_subs=with_subs, interp_degree=interp_degree)

@@ -211,7 +211,7 @@ def generate(cfg: SnapshotConfig | str) -> Snapshot:
     P = P[perm].astype(np.float32)
     V = V[perm].astype(np.float32)
     # float32 rounding can land exactly on +L/2: fold back inside
-    P[P >= np.float32(L / 2)] = np.float32(-L / 2)
+    P[P >= float(np.float32(L / 2))] = float(np.float32(-L / 2))
     m = np.full(n, np.float32(mp_msun / UM), dtype=np.float32)
     ids = np.arange(1, n + 1, dtype=np.int32)
     halo_pos = np.concatenate([pos, spos]) if S else pos
@@ -239,6 +239,7 @@ class Mesh:
     patchry: np.ndarray
     patchrz: np.ndarray
     pare: np.ndarray
+    owner: np.ndarray | None = None   # generator halo a stand-in patch was built for
 
     @property
     def total(self) -> int:
@@ -264,8 +265,6 @@ def build_mesh(snap: Snapshot, dx: float, nl: int | None = None) -> Mesh:
             if snap.halo_npart[i] < 64 * 4 ** (ir - 1):
                 break
             rr = snap.halo_r200[i]
-            if rr < 4 * dxpa:
-                continue
             side = int(min(32, max(14, 2 * math.ceil(1.2 * rr / dxpa))))
             side += side % 2
             c = snap.halo_pos[i]
@@ -282,7 +281,8 @@ def build_mesh(snap: Snapshot, dx: float, nl: int | None = None) -> Mesh:
         npatch.append(cnt)
     P = len(rows)
     m = Mesh(nl, np.array(npatch, np.int32), *(np.zeros(P, np.int32) for _ in range(6)),
-             *(np.zeros(P, np.float32) for _ in range(3)), np.zeros(P, np.int32))
+             *(np.zeros(P, np.float32) for _ in range(3)), np.zeros(P, np.int32),
+             np.array([r[3] for r in rows], np.int64))
     for q, (ir, side, org, _) in enumerate(rows):
         dxpa = np.float32(dx / 2.0 ** ir)
         dxpar = np.float32(dx / 2.0 ** (ir - 1))
@@ -308,22 +308,6 @@ class Candidates:
     nhallev: np.ndarray    # (nl+1,)
 
 
-def _patch_of(mesh: Mesh, dx: float, c, ir_max: int):
-    """Finest patch (level <= ir_max) containing c; returns (level, 1-based index)."""
-    base = 0
-    best = (0, 0)
-    for ir in range(1, mesh.nl + 1):
-        dxpa = dx / 2.0 ** ir
-        for q in range(base, base + int(mesh.npatch[ir])):
-            lo = np.array([mesh.patchrx[q], mesh.patchry[q], mesh.patchrz[q]]) - dxpa
-            hi = lo + np.array([mesh.patchnx[q], mesh.patchny[q], mesh.patchnz[q]]) * dxpa
-            if ir <= ir_max and np.all(c >= lo) and np.all(c < hi):
-                best = (ir, q + 1)
-                break
-        base += int(mesh.npatch[ir])
-    return best
-
-
 def build_candidates(snap: Snapshot, mesh: Mesh, dx: float, seed: int = 99,
                      spurious_frac: float = 0.05) -> Candidates:
     """Stand-in for the grid finder: one candidate per generated main halo
@@ -341,11 +325,20 @@ def build_candidates(snap: Snapshot, mesh: Mesh, dx: float, seed: int = 99,
     truth = np.concatenate([np.arange(H), np.full(ns, -1)])
     lev = np.zeros(H + ns, np.int32)
     pc = np.zeros(H + ns, np.int32)
-    # level: finest level whose cell is < R/4, limited to patches present
+    # level: the finest level <= the one whose cell is < R/4 that has a patch
+    # built around this halo (the grid finder reports a peak on its patch)
     want = np.clip(np.floor(np.log2(np.maximum(dx / np.maximum(rad / 4.0, 1e-9), 1.0))), 0, mesh.nl).astype(int)
-    for i in range(H + ns):
-        if want[i] > 0:
-            lev[i], pc[i] = _patch_of(mesh, dx, pos[i], want[i])
+    patch_of = {}
+    if mesh.owner is not None:
+        lev_of_patch = np.repeat(np.arange(mesh.nl + 1), mesh.npatch)
+        for q in range(mesh.total):
+            patch_of[(int(mesh.owner[q]), int(lev_of_patch[q]))] = q + 1
+    for i in range(H):
+        for ir in range(int(want[i]), 0, -1):
+            q = patch_of.get((i, ir))
+            if q is not None:
+                lev[i], pc[i] = ir, q
+                break
     order = np.argsort(lev, kind="stable")
     mp = float(snap.m[0])
     npart_est = np.concatenate([snap.halo_npart[:H], np.full(ns, 1)])
@@ -386,3 +379,128 @@ def build_sub_candidates(snap: Snapshot, host_slot: dict, host_ok, dx: float, nl
     return (c[:, 0].astype(np.float32), c[:, 1].astype(np.float32), c[:, 2].astype(np.float32),
             np.array([t[2] for t in rows], np.float32), np.array([t[3] for t in rows], np.int32),
             np.array([t[4] for t in rows], np.int64), subs_lev)
+
+
+def _halo_table(cfg: SnapshotConfig, rng):
+    """Per-halo and per-subhalo parameters of the recipe (small arrays)."""
+    n = cfg.n
+    L = cfg.lado0
+    rho_c = 2.775e11 * cfg.h * cfg.h
+    mp_msun = cfg.fdm * cfg.omega_m * rho_c * L ** 3 / n
+    a = -0.9
+    u = rng.random(cfg.n_haloes)
+    lo, hi = cfg.mlo ** a, cfg.mhi ** a
+    mh = np.sort((lo + u * (hi - lo)) ** (1.0 / a))[::-1]
+    npart = np.maximum(np.floor(mh / mh.sum() * int(round(cfg.frac_haloes * n))).astype(np.int64), 1)
+    sub_host, sub_np = [], []
+    if cfg.sub_host_min > 0:
+        for i in np.nonzero(mh >= cfg.sub_host_min)[0]:
+            ns = int(rng.integers(1, cfg.sub_max + 1))
+            take = int(cfg.sub_frac * npart[i])
+            if take < 2 * cfg.min_num_part * ns:
+                continue
+            w = np.maximum((rng.dirichlet(np.ones(ns)) * take).astype(np.int64), 1)
+            npart[i] -= w.sum()
+            sub_host += [i] * ns
+            sub_np += list(w)
+    sub_host = np.array(sub_host, dtype=np.int64)
+    sub_np = np.array(sub_np, dtype=np.int64)
+    H = cfg.n_haloes
+    conc = 8.0 * (mh / 1e12) ** -0.1
+    mtot = npart * mp_msun + np.bincount(sub_host, weights=sub_np * mp_msun, minlength=H)
+    m200 = mtot * _nfw_mu(conc) / _nfw_mu(2.0 * conc)
+    r200 = (3.0 * m200 / (4.0 * math.pi * 200.0 * rho_c)) ** (1.0 / 3.0)
+    v200 = np.sqrt(GCONS * m200 / r200)
+    margin = 2.0 * r200
+    pos = np.empty((H, 3))
+    for d in range(3):
+        pos[:, d] = -L / 2 + margin + rng.random(H) * (L - 2 * margin)
+    bulk = rng.standard_normal((H, 3)) * cfg.bulk_kms
+    S = sub_host.shape[0]
+    sr200 = np.zeros(S)
+    sv200 = np.zeros(S)
+    spos = np.zeros((S, 3))
+    sbulk = np.zeros((S, 3))
+    if S:
+        sm200 = sub_np * mp_msun
+        sr200 = (3.0 * sm200 / (4.0 * math.pi * 200.0 * rho_c)) ** (1.0 / 3.0)
+        sv200 = np.sqrt(GCONS * sm200 / sr200)
+        sdist = (0.3 + 0.6 * rng.random(S)) * r200[sub_host]
+        spos = pos[sub_host] + _random_dirs(rng, S) * sdist[:, None]
+        sbulk = bulk[sub_host] + _random_dirs(rng, S) * cfg.sub_vkick_kms
+    return dict(mp=mp_msun, npart=npart, conc=conc, r200=r200, v200=v200, pos=pos, bulk=bulk,
+                sub_host=sub_host, sub_np=sub_np, sr200=sr200, sv200=sv200, spos=spos, sbulk=sbulk)
+
+
+def generate_fast(cfg: SnapshotConfig | str, device: str | None = None, keep_on_device: bool = False):
+    """Same recipe as ``generate`` with the per-particle sampling in torch
+    (on the GPU when one is present): a 512^3 snapshot in seconds.  The
+    random stream differs from ``generate``'s; it is seeded and repeatable
+    on a given device type.  With keep_on_device the particle arrays are
+    torch tensors on `device`."""
+    import torch
+    if isinstance(cfg, str):
+        cfg = CONFIGS[cfg]
+    if device is None:
+        device = "cuda" if torch.cuda.is_available() else "cpu"
+    rng = np.random.Generator(np.random.PCG64(cfg.seed))
+    t = _halo_table(cfg, rng)
+    n, L = cfg.n, cfg.lado0
+    g = torch.Generator(device=device)
+    g.manual_seed(cfg.seed)
+    dd = dict(device=device, dtype=torch.float64)
+    xs = torch.cat([torch.zeros(1, **dd), torch.logspace(-5, math.log10(80.0), 4000, **dd)])
+    mu_tab = torch.log1p(xs) - xs / (1.0 + xs)
+
+    def nfw_r(conc, counts, scale):
+        c = torch.repeat_interleave(torch.as_tensor(conc, **dd), torch.as_tensor(counts, device=device))
+        mu_max = torch.log1p(2.0 * c) - 2.0 * c / (1.0 + 2.0 * c)
+        u = torch.rand(c.shape[0], generator=g, **dd) * mu_max
+        k = torch.clamp(torch.searchsorted(mu_tab, u), 1, xs.shape[0] - 1)
+        x0, x1, m0, m1 = xs[k - 1], xs[k], mu_tab[k - 1], mu_tab[k]
+        x = x0 + (u - m0) * (x1 - x0) / torch.clamp(m1 - m0, min=1e-300)
+        s = torch.repeat_interleave(torch.as_tensor(scale, **dd), torch.as_tensor(counts, device=device))
+        return x / c * s
+
+    def dirs(m):
+        v = torch.randn(m, 3, generator=g, **dd)
+        return v / torch.linalg.norm(v, dim=1, keepdim=True)
+
+    def rep(a, counts):
+        return torch.repeat_interleave(torch.as_tensor(a, **dd), torch.as_tensor(counts, device=device), dim=0)
+
+    r = nfw_r(t["conc"], t["npart"], t["r200"])
+    P = [rep(t["pos"], t["npart"]) + dirs(r.shape[0]) * r[:, None]]
+    V = [rep(t["bulk"], t["npart"]) + torch.randn(r.shape[0], 3, generator=g, **dd)
+         * rep(t["v200"] / math.sqrt(2.0), t["npart"])[:, None]]
+    del r
+    S = t["sub_host"].shape[0]
+    if S:
+        rs = nfw_r(np.full(S, cfg.sub_conc), t["sub_np"], 0.5 * t["sr200"])
+        P.append(rep(t["spos"], t["sub_np"]) + dirs(rs.shape[0]) * rs[:, None])
+        V.append(rep(t["sbulk"], t["sub_np"]) + torch.randn(rs.shape[0], 3, generator=g, **dd)
+                 * rep(t["sv200"] / math.sqrt(2.0), t["sub_np"])[:, None])
+        del rs
+    nbg = n - int(t["npart"].sum()) - int(t["sub_np"].sum())
+    P.append(-L / 2 + torch.rand(nbg, 3, generator=g, **dd) * L)
+    V.append(torch.randn(nbg, 3, generator=g, **dd) * cfg.bg_kms)
+    P = torch.remainder(torch.cat(P) + L / 2, L) - L / 2
+    V = torch.cat(V) / UV
+    perm = torch.randperm(n, generator=g, device=device)
+    P = P[perm].to(torch.float32)
+    V = V[perm].to(torch.float32)
+    del perm
+    P[P >= float(np.float32(L / 2))] = float(np.float32(-L / 2))
+    m = torch.full((n,), float(np.float32(t["mp"] / UM)), dtype=torch.float32, device=device)
+    ids = torch.arange(1, n + 1, dtype=torch.int32, device=device)
+    cols = [P[:, 0].contiguous(), P[:, 1].contiguous(), P[:, 2].contiguous(), V[:, 0].contiguous(),
+            V[:, 1].contiguous(), V[:, 2].contiguous(), m, ids]
+    del P, V
+    if not keep_on_device:
+        cols = [c.cpu().numpy() for c in cols]
+    H = cfg.n_haloes
+    halo_pos = np.concatenate([t["pos"], t["spos"]]) if S else t["pos"]
+    halo_r200 = np.concatenate([t["r200"], t["sr200"]]) if S else t["r200"]
+    halo_np = np.concatenate([t["npart"], t["sub_np"]]) if S else t["npart"]
+    halo_host = np.concatenate([np.full(H, -1), t["sub_host"]]) if S else np.full(H, -1)
+    return Snapshot(cfg, *cols, halo_pos, halo_r200, halo_np, halo_host)

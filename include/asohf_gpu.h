@@ -39,6 +39,13 @@ int asohf_set_stream(asohf_ctx *ctx, void *cuda_stream);
 int asohf_synchronize(asohf_ctx *ctx);
 /* Number of kernels this context has launched (diagnostics). */
 int64_t asohf_launch_count(asohf_ctx *ctx);
+/* Diagnostics, no counterpart in the reference: with profiling on, the main
+ * kernels are bracketed by CUDA events on the context stream; stats entry i
+ * gives a kernel's name, summed device time (ms) and launch count since
+ * profiling was (re)enabled. */
+int asohf_set_profiling(asohf_ctx *ctx, int on);
+int asohf_kernel_stats(asohf_ctx *ctx, int i, const char **name, double *total_ms,
+                       int64_t *launches);
 
 /* MODULE PARTICLES (particles.f:1-14) / READ_AND_ALLOC_PARTICLES
  * (alloc.f:196-528): copies the particle arrays into the device store,

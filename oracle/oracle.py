@@ -237,3 +237,6 @@ class OracleBackend:
 
     def poisson_fft(self, u1, dx):
         return poisson_fft(u1, dx)
+
+    def final_ids(self, pph, n):
+        return pph[:n].copy()
