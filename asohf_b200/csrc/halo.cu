@@ -709,6 +709,7 @@ __device__ long long properties_block(const Store& S, const HConst& H, asohf_cat
     cat.dmpclus[i0] = (int32_t)cnt;
     if (cnt < H.min_num_part) {
       cat.realclus[i0] = 0;
+      cat.vmaxclus[i0] = vmax;  // the running maximum of |v|^2 (-1 if none) stays
     } else {
       cat.potential_e[i0] = 0.0f;
       cat.iplip[i0] = S.id[lip[0]];
@@ -1311,4 +1312,753 @@ extern "C" int asohf_get_particles_per_halo(asohf_ctx* c, int32_t* out, int64_t 
                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return ASOHF_OK;
+}
+
+// ================================================================ substructure
+// SUBSTRUCTURE_PARTICLES (substructure.f:756-1697).  Per call (subhaloes of
+// one level): recentering and the host's enclosed mass (k_sub_prep); the
+// Jacobi-radius search (gather, sort, k_sub_jacobi) repeated for the
+// subhaloes whose radius must grow x1.5; a last gather at the final radius;
+// then k_sub_main: unbinding, Jacobi trim, SO walk, properties.
+
+struct SubPrep {
+  float *cx, *cy, *cz;
+  float *mhost, *disthost;
+  float *r;          // current Jacobi gather radius
+  int32_t* status;
+};
+
+// Recentering (substructure.f:879-899) and host characterisation
+// (substructure.f:933-983).
+__global__ void __launch_bounds__(HB)
+k_sub_prep(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work, SubPrep o) {
+  __shared__ RecShared sh;
+  int slot = blockIdx.x;
+  int i0 = work[slot];
+  int irr = level_of_patch(H, cat.patchclus[i0]);
+  float cx = cat.clusrx[i0], cy = cat.clusry[i0], cz = cat.clusrz[i0];
+  float dxpamin = __fdiv_rn(ci.dx, exp2f((float)irr));
+  if (!recenter_block(S, ci, &cx, &cy, &cz, cat.rsub[i0], dxpamin, sh)) {
+    if (threadIdx.x == 0) o.status[slot] = ASOHF_ERR_CAPACITY;
+    return;
+  }
+  if (threadIdx.x != 0) return;
+  cat.clusrx[i0] = cx; cat.clusry[i0] = cy; cat.clusrz[i0] = cz;
+  int ih = cat.realclus[i0] - 1;
+  float mhost = (cat.realclus[ih] == -1) ? cat.masa[ih] : cat.msub[ih];
+  float disthost = dist3(cat.clusrx[ih], cat.clusry[ih], cat.clusrz[ih], cx, cy, cz);
+  const float* p1 = cat.profiles + (size_t)ih * 2 * ASOHF_NBINS;
+  const float* p2 = p1 + ASOHF_NBINS;
+  int nbp = ASOHF_NBINS, jj;
+  for (jj = 1; jj <= ASOHF_NBINS; jj++)
+    if (p1[jj - 1] == 0.0f) { nbp = jj - 1; break; }
+  for (jj = 1; jj <= nbp; jj++)
+    if (p1[jj - 1] > disthost) break;
+  if (jj == 1) {
+    float q = __fdiv_rn(disthost, p1[0]);
+    mhost = __fmul_rn(p2[0], __fmul_rn(__fmul_rn(q, q), q));
+  } else if (jj <= nbp) {
+    float a1 = p1[jj - 2], a2 = p1[jj - 1];
+    float d3 = __fmul_rn(__fmul_rn(disthost, disthost), disthost);
+    float a13 = __fmul_rn(__fmul_rn(a1, a1), a1), a23 = __fmul_rn(__fmul_rn(a2, a2), a2);
+    mhost = __fadd_rn(p2[jj - 2], __fdiv_rn(__fmul_rn(__fsub_rn(p2[jj - 1], p2[jj - 2]), __fsub_rn(d3, a13)),
+                                            __fsub_rn(a23, a13)));
+  } else {
+    mhost = p2[nbp - 1 >= 0 ? nbp - 1 : 0];
+  }
+  o.cx[slot] = cx; o.cy[slot] = cy; o.cz[slot] = cz;
+  o.mhost[slot] = mhost;
+  o.disthost[slot] = disthost;
+  o.r[slot] = __fmul_rn(2.0f, cat.rsub[i0]);
+  o.status[slot] = 0;
+}
+
+// Members of the sphere r around the centre (count only).
+__global__ void __launch_bounds__(HB)
+k_sphere_count(ColIdx ci, const int32_t* __restrict__ act, const float* __restrict__ hcx,
+               const float* __restrict__ hcy, const float* __restrict__ hcz, const float* __restrict__ r,
+               int32_t* __restrict__ konta) {
+  __shared__ long long lred[32];
+  int s = act[blockIdx.x];
+  float cx = hcx[s], cy = hcy[s], cz = hcz[s], rr = r[s];
+  int64_t lo, hi;
+  slab_range(ci, cx, rr, &lo, &hi);
+  long long c = 0;
+  query_box(ci, cx, cy, cz, rr, [&](const float4& e) {
+    int p = ppos(e);
+    if (p >= lo && p < hi && dist3(e.x, e.y, e.z, cx, cy, cz) < rr) c++;
+  });
+  c = block_sum_ll(c, lred);
+  if (threadIdx.x == 0) konta[blockIdx.x] = (int32_t)c;
+}
+
+__device__ __forceinline__ double eq_jacobi_dev(double basx, double basy) {
+  double t = __dsub_rn(1.0, basx);
+  return __dadd_rn(__dsub_rn(__dsub_rn(__ddiv_rn(1.0, __dmul_rn(t, t)), 1.0), __ddiv_rn(basy, __dmul_rn(basx, basx))),
+                   __dmul_rn(__dadd_rn(1.0, basy), basx));
+}
+
+struct JacOut {
+  int32_t* done;      // 1: radius fixed
+  int32_t* jjac;      // J_JACOBI
+  double* masadm;
+  float* rclus;       // RCLUS = DISTA(J_JACOBI)
+};
+
+// Jacobi radius on the sorted members (substructure.f:1016-1112).  Slot s of
+// the active list; segment [off[b], off[b]+konta[b]).
+__global__ void __launch_bounds__(HB)
+k_sub_jacobi(Store S, HConst H, const int32_t* __restrict__ act, const int32_t* __restrict__ konta,
+             const int64_t* __restrict__ off, const unsigned long long* __restrict__ keys,
+             const int32_t* __restrict__ vals, const float* __restrict__ mhost_a,
+             const float* __restrict__ disthost_a, float* __restrict__ r, JacOut o) {
+  __shared__ MainShared sh;
+  __shared__ double s_m[4];
+  int b = blockIdx.x, s = act[b];
+  int64_t K = konta[b];
+  const unsigned long long* kk = keys + off[b];
+  const int32_t* lip = vals + off[b];
+  double um = (double)H.um;
+  float mhost = mhost_a[s], disthost = disthost_a[s];
+  auto dista = [&](int64_t J) -> float {  // DISTA(J), 1-based; 1e10 past the members
+    return (J >= 1 && J <= K) ? __uint_as_float((uint32_t)(kk[J - 1] & 0xffffffffull)) : 1.e10f;
+  };
+  int64_t minj = max((int64_t)10, K / 50);
+  double mh3 = (double)__fmul_rn(3.0f, mhost);
+  double expo = (double)(1.0f / 3.0f);
+  // estimation: first J > MINJ with r/D - (m/(m+3M))^(1/3) > 0
+  long long jest = LLONG_MAX;
+  tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                [&](int64_t j, double mas) {
+                  int64_t J = j + 1;
+                  if (J <= minj) return;
+                  double mu = mas * um;
+                  double eq = (double)__fdiv_rn(dista(J), disthost) - pow(mu / (mu + mh3), expo);
+                  if (eq > 0.0 && J < jest) jest = J;
+                },
+                sh.dred);
+  jest = bmin(jest, sh);
+  int64_t jj = jest == LLONG_MAX ? K : jest;
+  // masses at jj and prefix lookups
+  double mjj = 0.0;
+  if (threadIdx.x == 0) s_m[0] = 0.0;
+  __syncthreads();
+  tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                [&](int64_t j, double mas) { if (j + 1 == jj) s_m[0] = mas; }, sh.dred);
+  __syncthreads();
+  mjj = s_m[0];
+  double basx = (double)__fdiv_rn(dista(jj), disthost);
+  double basy = mjj * um / (double)mhost;
+  double eq = eq_jacobi_dev(basx, basy);
+  int flag = 0, dir = -1;
+  long long jfound = LLONG_MAX;
+  double masadm = mjj;
+  // ABS(EQ_JACOBI_R).LT.0.D01 compares with 0.0D+01 = 0: never true
+  if (eq < 0.0) {
+    dir = 1;  // forward: first J > jj with EQ > 0
+    long long f = LLONG_MAX;
+    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                  [&](int64_t j, double mas) {
+                    int64_t J = j + 1;
+                    if (J <= jj) return;
+                    double bx = (double)__fdiv_rn(dista(J), disthost);
+                    double e2 = eq_jacobi_dev(bx, mas * um / (double)mhost);
+                    if (e2 > 0.0 && J < f) f = J;
+                  },
+                  sh.dred);
+    f = bmin(f, sh);
+    if (f != LLONG_MAX) { flag = 1; jfound = f; }
+  } else {
+    // backward: largest J in [MINJ, jj-1] with EQ(prefix(J)) < 0
+    long long f = -1;
+    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                  [&](int64_t j, double mas) {
+                    int64_t J = j + 1;
+                    if (J < minj || J > jj - 1) return;
+                    double bx = (double)__fdiv_rn(dista(J), disthost);
+                    double e2 = eq_jacobi_dev(bx, mas * um / (double)mhost);
+                    if (e2 < 0.0 && J > f) f = J;
+                  },
+                  sh.dred);
+    f = -bmin(-f, sh);  // max (-1: none)
+    if (f > 0) { flag = 1; jfound = f; }
+  }
+  int64_t jj2 = jj;
+  if (flag) {
+    jj2 = jfound;
+  } else if (dir == -1) {
+    jj2 = minj;
+    flag = 1;
+  }
+  if (flag) {
+    // MASADM at the final J: prefix(J) (forward and backward searches) or,
+    // when the backward loop ran out, prefix(MINJ); a zero-trip backward
+    // loop keeps prefix(jj)
+    if (threadIdx.x == 0) s_m[1] = 0.0;
+    __syncthreads();
+    int64_t jm = jj2;
+    if (dir == -1 && jfound == LLONG_MAX && jj - 1 < minj) jm = jj;
+    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                  [&](int64_t j, double mas) { if (j + 1 == jm) s_m[1] = mas; }, sh.dred);
+    __syncthreads();
+    masadm = (jm >= 1 && jm <= K) ? s_m[1] : (jm > K ? mjj : 0.0);
+  }
+  if (threadIdx.x == 0) {
+    o.done[b] = flag;
+    if (flag) {
+      o.jjac[b] = (int32_t)jj2;
+      o.masadm[b] = masadm;
+      o.rclus[b] = dista(jj2);
+    } else {
+      r[s] = __fmul_rn(1.5f, r[s]);
+    }
+  }
+}
+
+// Reverses runs of equal distance in the first n entries (the tie order of
+// ARGSORT applied to an already sorted list, substructure.f:1161-1162).
+__device__ void reverse_tie_runs(float* dista, int32_t* lip, int64_t n) {
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    if (i > 0 && dista[i] == dista[i - 1]) continue;
+    int64_t e = i + 1;
+    while (e < n && dista[e] == dista[i]) e++;
+    for (int64_t a = i, z = e - 1; a < z; a++, z--) {
+      int32_t t = lip[a];
+      lip[a] = lip[z];
+      lip[z] = t;
+    }
+  }
+  __syncthreads();
+}
+
+struct SubMainIn {
+  const int32_t* konta;   // gathered members
+  const int32_t* jjac;    // members kept (J_JACOBI)
+  const double* masadm;
+  const float* rclus;
+  const float *cx, *cy, *cz, *mhost, *disthost;
+};
+
+__global__ void __launch_bounds__(HB)
+k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work, SubMainIn in, Seg sg) {
+  __shared__ MainShared sh;
+  int slot = blockIdx.x;
+  int i0 = work[slot];
+  if (threadIdx.x == 0) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; }
+  int64_t Kg = in.konta[slot];
+  int64_t konta = in.jjac[slot];
+  double masadm = in.masadm[slot];
+  float um = H.um;
+  if (masadm <= 0.0 || konta < H.min_num_part || konta > Kg) {
+    // RSUB/MSUB were set when the Jacobi radius was fixed (substructure.f:1115-1117)
+    if (threadIdx.x == 0) {
+      cat.rsub[i0] = in.rclus[slot];
+      cat.msub[i0] = (float)(masadm * (double)um);
+      cat.realclus[i0] = 0;
+    }
+    return;
+  }
+  int64_t base = sg.off[slot] + slot;
+  float* dista = sg.dista + base;
+  int32_t* lip = sg.lip + base;
+  double* pot = sg.pot + base;
+  uint8_t* flag = sg.flag + base;
+  int64_t kbase = sg.off[slot];
+  for (int64_t j = threadIdx.x; j < konta; j += blockDim.x) {
+    dista[j] = __uint_as_float((uint32_t)(sg.keys[kbase + j] & 0xffffffffull));
+    lip[j] = sg.vals[kbase + j];
+    flag[j] = 1;
+  }
+  if (threadIdx.x == 0) dista[konta] = 1.e10f;
+  __syncthreads();
+  float cx = in.cx[slot], cy = in.cy[slot], cz = in.cz[slot];
+  float mhost = in.mhost[slot], disthost = in.disthost[slot];
+  float cm0[3], v0[3], m2;
+  centromasas_block(S, dista, lip, flag, true, konta, cm0, v0, &m2, sh);
+  HaloState h;
+  for (int q = 0; q < 3; q++) { h.cm[q] = cm0[q]; h.v[q] = v0[q]; }
+  h.radio = in.rclus[slot];                 // RSUB
+  h.masa = (float)(masadm * (double)um);    // MSUB
+  h.realclus = cat.realclus[i0];
+  reverse_tie_runs(dista, lip, konta);
+  int64_t k2 = konta, iv;
+  float ref_max = dista[k2 - 1];
+  int64_t contaerr = konta;
+  int fac = 0;
+  auto write_back = [&]() {
+    if (threadIdx.x == 0) {
+      cat.clusrxcm[i0] = h.cm[0]; cat.clusrycm[i0] = h.cm[1]; cat.clusrzcm[i0] = h.cm[2];
+      cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2];
+      cat.rsub[i0] = h.radio; cat.msub[i0] = h.masa;
+      cat.dmpclus[i0] = (int32_t)konta;
+    }
+  };
+  while (contaerr > 0 || fac < 3) {
+    fac++;
+    int64_t prev = k2;
+    iv = k2;
+    unbinding8_block(S, H, fac, ref_max, dista, lip, flag, pot, k2, iv, h, sh);
+    int64_t nk2;
+    reordenar_compact(dista, lip, flag, k2, &iv, &nk2, sh);
+    k2 = nk2;
+    __syncthreads();
+    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
+    contaerr = prev - k2;
+    if (fac > 100000) break;
+  }
+  if (k2 < H.min_num_part) {
+    write_back();
+    if (threadIdx.x == 0) cat.realclus[i0] = 0;
+    return;
+  }
+  fac = 0;
+  contaerr = k2;
+  while (contaerr > 0 || fac < 4) {
+    fac++;
+    int64_t prev = k2;
+    iv = k2;
+    unbinding_sigma_block(S, H, fac, lip, flag, k2, iv, h, sh);
+    int64_t nk2;
+    reordenar_compact(dista, lip, flag, k2, &iv, &nk2, sh);
+    k2 = nk2;
+    __syncthreads();
+    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
+    contaerr = prev - k2;
+    if (fac > 100000) break;
+  }
+  if (k2 < H.min_num_part) {
+    write_back();
+    if (threadIdx.x == 0) cat.realclus[i0] = 0;
+    return;
+  }
+  // Jacobi trim after unbinding (substructure.f:1241-1264)
+  int64_t ncapas = 0;
+  float rshell = 0.0f;
+  {
+    double m0 = (double)__fdiv_rn(h.masa, um);
+    double bx = (double)__fdiv_rn(dista[k2 - 1], disthost);
+    double e0 = eq_jacobi_dev(bx, m0 * (double)um / (double)mhost);
+    if (e0 > 0.0) {
+      // M(J) = MASADM - sum_{i >= J} m_i ; largest J in [1, k2] with EQ < 0
+      __shared__ double s_tot;
+      double tot = tile_prefix_d(0, k2, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                                 [&](int64_t, double) {}, sh.dred);
+      if (threadIdx.x == 0) s_tot = tot;
+      __syncthreads();
+      tot = s_tot;
+      long long f = -1;
+      double mf = 0.0;
+      tile_prefix_d(0, k2, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+                    [&](int64_t j, double pre) {
+                      int64_t J = j + 1;
+                      double mj = m0 - (tot - pre + (double)S.m[lip[j]]);  // after subtracting m(J..K2)
+                      double bxj = (double)__fdiv_rn(dista[j], disthost);
+                      double e2 = eq_jacobi_dev(bxj, mj * (double)um / (double)mhost);
+                      if (e2 < 0.0 && J > f) { f = J; mf = mj; }
+                    },
+                    sh.dred);
+      long long fmax = -bmin(-f, sh);  // -1: none
+      __shared__ double s_mf;
+      if (f == fmax && f > 0) s_mf = mf;
+      __syncthreads();
+      int64_t J;
+      double mj;
+      if (fmax <= 0) {
+        J = 0;
+        mj = m0 - tot;
+      } else {
+        J = fmax;
+        mj = s_mf;
+      }
+      h.radio = J + 1 <= k2 ? dista[J] : (J + 1 == k2 + 1 ? dista[k2] : 1.e10f);
+      h.masa = (float)(mj * (double)um);
+      k2 = J;
+      ncapas = J;
+      rshell = J >= 1 ? dista[J - 1] : 1.e10f;
+      __syncthreads();
+    }
+  }
+  if (k2 < H.min_num_part) {
+    write_back();
+    if (threadIdx.x == 0) cat.realclus[i0] = 0;
+    return;
+  }
+  // SO walk without early exit (substructure.f:1293-1463)
+  float pi = H.pi, rote = H.rote, rete = H.rete;
+  float norma = S.norma;
+  int64_t jjcore = (int64_t)fmaxf(10.0f, __fdiv_rn((float)k2, 100.0f));
+  float thr[6] = {__fdiv_rn(2500.0f, H.omegaz), __fdiv_rn(500.0f, H.omegaz), __fdiv_rn(200.0f, H.omegaz),
+                  2500.0f, 500.0f, 200.0f};
+  int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
+  long long jt[7];
+  for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
+  double best_v = -1.0;
+  long long best_j = LLONG_MAX;
+  double best_b = 0.0;
+  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(S.m[lip[j]], norma); };
+  double btot = tile_prefix_d(0, k2, 0.0, mn_of,
+                              [&](int64_t j, double bas8) {
+                                int64_t J = j + 1;
+                                if (J <= jjcore) return;
+                                float d = dista[j];
+                                float vol = so_den(d, rete, pi);
+                                float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
+                                for (int q = 0; q < 6; q++)
+                                  if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+                                if (delta2 <= H.contrastec && J > jvir_min && J < jt[6]) jt[6] = J;
+                                float bas2 = (float)(bas8 / (double)d);
+                                if ((double)bas2 > best_v || ((double)bas2 == best_v && J < best_j)) {
+                                  best_v = bas2; best_j = J; best_b = bas8;
+                                }
+                              },
+                              sh.dred);
+  for (int q = 0; q < 7; q++) jt[q] = bmin(jt[q], sh);
+  __shared__ double s_at[7];
+  tile_prefix_d(0, k2, 0.0, mn_of,
+                [&](int64_t j, double bas8) {
+                  for (int q = 0; q < 7; q++)
+                    if (j + 1 == jt[q]) s_at[q] = bas8;
+                },
+                sh.dred);
+  double vacc[3];
+  for (int ax = 0; ax < 3; ax++) {
+    const float* vv = ax == 0 ? S.vx : (ax == 1 ? S.vy : S.vz);
+    vacc[ax] = tile_prefix_d(0, k2, 0.0, [&](int64_t j) {
+                               int p = lip[j];
+                               return (double)__fmul_rn(__fdiv_rn(S.m[p], norma), vv[p]);
+                             },
+                             [&](int64_t, double) {}, sh.dred);
+  }
+  sh.bestv[threadIdx.x] = best_v;
+  sh.bestj[threadIdx.x] = best_j;
+  sh.bestb[threadIdx.x] = best_b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bv = -1.0;
+    long long bj = LLONG_MAX;
+    double bb = 0.0;
+    for (int t = 0; t < HB; t++) {
+      if (sh.bestj[t] == LLONG_MAX) continue;
+      if (sh.bestv[t] > bv || (sh.bestv[t] == bv && sh.bestj[t] < bj)) {
+        bv = sh.bestv[t]; bj = sh.bestj[t]; bb = sh.bestb[t];
+      }
+    }
+    if (bj != LLONG_MAX) {
+      cat.vcmax[i0] = (float)bv;
+      cat.mcmax[i0] = (float)bb;
+      cat.rcmax[i0] = dista[bj - 1];
+    }
+    float* mo[6] = {cat.m2500c, cat.m500c, cat.m200c, cat.m2500m, cat.m500m, cat.m200m};
+    float* ro[6] = {cat.r2500c, cat.r500c, cat.r200c, cat.r2500m, cat.r500m, cat.r200m};
+    for (int q = 0; q < 6; q++) {
+      if (jt[q] != LLONG_MAX) {
+        int64_t J = jt[q];
+        float d = dista[J - 1];
+        float vol = so_den(d, rete, pi);
+        float delta2 = (float)((double)norma * s_at[q] / (double)vol / (double)rote);
+        mo[q][i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
+        ro[q][i0] = d;
+        if (J == jjcore + 1) { mo[q][i0] = -1.0f; ro[q][i0] = -1.0f; }
+      } else {
+        mo[q][i0] = 0.0f;
+        ro[q][i0] = 0.0f;
+      }
+    }
+    if (jt[6] != LLONG_MAX) {
+      int64_t J = jt[6];
+      float d = dista[J - 1];
+      float vol = so_den(d, rete, pi);
+      float delta2 = (float)((double)norma * s_at[6] / (double)vol / (double)rote);
+      cat.masa[i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
+      cat.radio[i0] = d;
+    } else {
+      cat.masa[i0] = 0.0f;
+      cat.radio[i0] = 0.0f;
+    }
+    h.v[0] = (float)(vacc[0] / btot);
+    h.v[1] = (float)(vacc[1] / btot);
+    h.v[2] = (float)(vacc[2] / btot);
+    float bas = __fdiv_rn(__fmul_rn(__fmul_rn(cat.vcmax[i0], norma), H.cgr), rete);
+    cat.vcmax[i0] = __fmul_rn(__fsqrt_rn(bas), H.uv);
+    cat.mcmax[i0] = __fmul_rn(__fmul_rn(cat.mcmax[i0], norma), um);
+  }
+  __syncthreads();
+  write_back();
+  // the properties read VX(I) from the catalogue
+  if (threadIdx.x == 0) { cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2]; }
+  __syncthreads();
+  long long nb = properties_block(S, H, cat, i0, dista, lip, flag, ncapas, rshell, cx, cy, cz, cm0, false, sh);
+  if (threadIdx.x == 0) {
+    bool ok = nb >= H.min_num_part && H.want_ids;
+    sg.nbound[slot] = ok ? (int32_t)nb : 0;
+    sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
+    sg.status[slot] = 0;
+  }
+}
+
+// Work list of a substructure level: REALCLUS != 0, largest RSUB first.
+static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots) {
+  int nh = low2 - low1 + 1;
+  int32_t* rc = (int32_t*)malloc(4 * (size_t)nh);
+  float* rs = (float*)malloc(4 * (size_t)nh);
+  ASOHF_CUDA(cudaMemcpyAsync(rc, m.d.realclus + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(rs, m.d.rsub + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  int32_t* w = (int32_t*)malloc(4 * (size_t)(nh > 0 ? nh : 1));
+  int k = 0;
+  for (int i = 0; i < nh; i++)
+    if (rc[i] != 0) w[k++] = low1 - 1 + i;
+  for (int i = 1; i < k; i++) {  // insertion sort by RSUB descending (stable)
+    int32_t v = w[i];
+    int j = i - 1;
+    while (j >= 0 && rs[w[j] - (low1 - 1)] < rs[v - (low1 - 1)]) { w[j + 1] = w[j]; j--; }
+    w[j + 1] = v;
+  }
+  free(rc);
+  free(rs);
+  *h_work = w;
+  *nslots = k;
+  return ASOHF_OK;
+}
+
+// gather + segmented sort of the members of `na` spheres (active list act);
+// keys/vals sorted in segments at offsets off (device).
+static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na, const int32_t* d_act,
+                         const float* cx, const float* cy, const float* cz, const float* r,
+                         int32_t* d_konta, int64_t* d_off, int64_t* h_off, unsigned long long** keys,
+                         int32_t** vals, int64_t* total, bool with_work) {
+  {
+    int kt_ = ktime_begin(c, "sub_sphere_count");
+    k_sphere_count<<<na, HB, 0, c->stream>>>(ci, d_act, cx, cy, cz, r, d_konta);
+    ktime_end(c, kt_);
+  }
+  c->launches++;
+  int32_t* hk = (int32_t*)malloc(4 * (size_t)na);
+  ASOHF_CUDA(cudaMemcpyAsync(hk, d_konta, 4 * (size_t)na, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  h_off[0] = 0;
+  for (int s = 0; s < na; s++) h_off[s + 1] = h_off[s] + hk[s];
+  free(hk);
+  int64_t T = h_off[na];
+  ASOHF_CUDA(cudaMemcpyAsync(d_off, h_off, 8 * (size_t)(na + 1), cudaMemcpyHostToDevice, c->stream));
+  int bits = 1;
+  while ((1ll << bits) < na) bits++;
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                  (int32_t*)nullptr, (int32_t*)nullptr, (int)(T > 0 ? T : 1), 0, 32 + bits);
+  size_t work = with_work ? ((size_t)T + na) * (4 + 4 + 8 + 1) + 4096 : 0;
+  ASOHF_CHECK(seg_reserve(c, (size_t)T * 24 + tb + work + 16384));
+  unsigned long long* k0 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
+  unsigned long long* k1 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
+  int32_t* v0 = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
+  int32_t* v1 = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
+  void* t = seg_alloc(c, tb);
+  if (!k0 || !k1 || !v0 || !v1 || !t) return ASOHF_ERR_CAPACITY;
+  if (T > 0) {
+    // k_halo_gather reads per-slot arrays through the active list order: it
+    // indexes by blockIdx (slot in the active list), so pass compacted views
+    {
+      int kt_ = ktime_begin(c, "sub_gather");
+      k_halo_gather<<<na, HB, 0, c->stream>>>(S, ci, d_konta, d_off, cx, cy, cz, r, k0, v0);
+      ktime_end(c, kt_);
+    }
+    int kt_ = ktime_begin(c, "sub_radix_sort");
+    ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)T, 0, 32 + bits, c->stream));
+    ktime_end(c, kt_);
+    k_tiefix<<<grid_for(T, 256), 256, 0, c->stream>>>(k1, v1, T, 1);
+    c->launches += 2;
+  }
+  *keys = k1;
+  *vals = v1;
+  *total = T;
+  return ASOHF_OK;
+}
+
+__global__ void k_jacobi_scatter(const int32_t* __restrict__ act, int na, JacOut o, const float* __restrict__ rlast,
+                                 int32_t* __restrict__ f_jjac, double* __restrict__ f_masadm,
+                                 float* __restrict__ f_rclus, float* __restrict__ f_rlast) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= na || !o.done[b]) return;
+  int s = act[b];
+  f_jjac[s] = o.jjac[b];
+  f_masadm[s] = o.masadm[b];
+  f_rclus[s] = o.rclus[b];
+  f_rlast[s] = rlast[b];
+}
+
+__global__ void k_iota32(int32_t* __restrict__ a, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
+__global__ void k_gather_f(const int32_t* __restrict__ act, int na, const float* __restrict__ src, float* __restrict__ dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < na) dst[i] = src[act[i]];
+}
+
+extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k, const asohf_mesh* mesh,
+                                            asohf_catalogue* cat, int ir, const int32_t* subs_lev,
+                                            int on_device) {
+  if (!c || !k || !cat || !subs_lev || !mesh || ir < 1 || ir > mesh->nl) return ASOHF_ERR_INVALID;
+  if (c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
+  if (k->do_compute_energies == 1) return ASOHF_ERR_UNSUPPORTED;
+  int lowh1 = 1, lowh2 = 0;
+  for (int q = 0; q < ir; q++) lowh1 += subs_lev[q];
+  for (int q = 0; q <= ir; q++) lowh2 += subs_lev[q];
+  if (lowh2 > cat->nclus) return ASOHF_ERR_INVALID;
+  if (lowh2 < lowh1) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int nh = lowh2 - lowh1 + 1;
+  size_t need = cat_bytes(cat->nclus) + (size_t)nh * 160 + 65536;
+  ASOHF_CHECK(arena_reserve(c, need));
+  CatMirror m;
+  ASOHF_CHECK(cat_mirror_in(c, cat, cat->nclus, on_device, &m));
+  int32_t* hw;
+  int ns;
+  ASOHF_CHECK(make_sub_work(c, m, lowh1, lowh2, &hw, &ns));
+  Store S = store_of(c);
+  ColIdx ci = col_idx(c, k);
+  HConst H = hconst(k, mesh);
+  int rc = ASOHF_OK;
+  if (ns > 0) {
+    int32_t* d_work = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    SubPrep pr;
+    pr.cx = (float*)arena_alloc(c, 4 * (size_t)ns); pr.cy = (float*)arena_alloc(c, 4 * (size_t)ns);
+    pr.cz = (float*)arena_alloc(c, 4 * (size_t)ns); pr.mhost = (float*)arena_alloc(c, 4 * (size_t)ns);
+    pr.disthost = (float*)arena_alloc(c, 4 * (size_t)ns); pr.r = (float*)arena_alloc(c, 4 * (size_t)ns);
+    pr.status = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_act = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_konta = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int64_t* d_off = (int64_t*)arena_alloc(c, 8 * (size_t)(ns + 1));
+    float* t_cx = (float*)arena_alloc(c, 4 * (size_t)ns); float* t_cy = (float*)arena_alloc(c, 4 * (size_t)ns);
+    float* t_cz = (float*)arena_alloc(c, 4 * (size_t)ns); float* t_r = (float*)arena_alloc(c, 4 * (size_t)ns);
+    JacOut jo;
+    jo.done = (int32_t*)arena_alloc(c, 4 * (size_t)ns); jo.jjac = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    jo.masadm = (double*)arena_alloc(c, 8 * (size_t)ns); jo.rclus = (float*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* f_jjac = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    double* f_masadm = (double*)arena_alloc(c, 8 * (size_t)ns);
+    float* f_rclus = (float*)arena_alloc(c, 4 * (size_t)ns);
+    float* f_rlast = (float*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_nbound = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_nscan = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int64_t* d_ids_off = (int64_t*)arena_alloc(c, 8 * (size_t)ns);
+    int64_t* h_off = (int64_t*)malloc(8 * (size_t)(ns + 1));
+    int32_t* h_act = (int32_t*)malloc(4 * (size_t)ns);
+    int32_t* h_done = (int32_t*)malloc(4 * (size_t)ns);
+    int32_t* h_st = (int32_t*)malloc(4 * (size_t)ns);
+    if (!d_work || !pr.cx || !pr.status || !d_act || !d_konta || !d_off || !t_r || !jo.done || !jo.rclus ||
+        !f_jjac || !f_masadm || !f_rclus || !f_rlast || !d_nbound || !d_nscan || !d_ids_off) {
+      free(hw); free(h_off); free(h_act); free(h_done); free(h_st);
+      return ASOHF_ERR_CAPACITY;
+    }
+    ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+    {
+      int kt_ = ktime_begin(c, "sub_prep");
+      k_sub_prep<<<ns, HB, 0, c->stream>>>(S, ci, H, m.d, d_work, pr);
+      ktime_end(c, kt_);
+    }
+    c->launches++;
+    ASOHF_CUDA(cudaMemcpyAsync(h_st, pr.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    int na = 0;
+    for (int s = 0; s < ns; s++) {
+      if (h_st[s]) rc = h_st[s];
+      else h_act[na++] = s;
+    }
+    // Jacobi radius, growing the unresolved ones
+    int32_t* d_pos = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    if (!d_pos) rc = ASOHF_ERR_CAPACITY;
+    else k_iota32<<<(ns + 255) / 256, 256, 0, c->stream>>>(d_pos, ns);
+    for (int iter = 0; na > 0 && rc == ASOHF_OK; iter++) {
+      if (iter > 200) { rc = ASOHF_ERR_TIMEOUT; break; }
+      ASOHF_CUDA(cudaMemcpyAsync(d_act, h_act, 4 * (size_t)na, cudaMemcpyHostToDevice, c->stream));
+      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cx, t_cx);
+      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cy, t_cy);
+      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cz, t_cz);
+      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.r, t_r);
+      c->launches += 4;
+      unsigned long long* keys;
+      int32_t* vals;
+      int64_t T;
+      ASOHF_CHECK(gather_sorted(c, S, ci, na, d_pos, t_cx, t_cy, t_cz, t_r, d_konta, d_off, h_off, &keys, &vals,
+                                &T, false));
+      {
+        int kt_ = ktime_begin(c, "sub_jacobi");
+        k_sub_jacobi<<<na, HB, 0, c->stream>>>(S, H, d_act, d_konta, d_off, keys, vals, pr.mhost, pr.disthost,
+                                               pr.r, jo);
+        ktime_end(c, kt_);
+      }
+      k_jacobi_scatter<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, jo, t_r, f_jjac, f_masadm, f_rclus,
+                                                                f_rlast);
+      c->launches += 2;
+      ASOHF_CUDA(cudaGetLastError());
+      ASOHF_CUDA(cudaMemcpyAsync(h_done, jo.done, 4 * (size_t)na, cudaMemcpyDeviceToHost, c->stream));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      int nn = 0;
+      for (int q = 0; q < na; q++)
+        if (!h_done[q]) h_act[nn++] = h_act[q];
+      na = nn;
+    }
+    if (rc == ASOHF_OK) {
+      // last gather of every subhalo at its final radius, then the main pass
+      unsigned long long* keys;
+      int32_t* vals;
+      int64_t T;
+      ASOHF_CHECK(gather_sorted(c, S, ci, ns, d_pos, pr.cx, pr.cy, pr.cz, f_rlast, d_konta, d_off, h_off, &keys,
+                                &vals, &T, true));
+      Seg sg;
+      sg.konta = d_konta;
+      sg.off = d_off;
+      sg.keys = keys;
+      sg.vals = vals;
+      sg.dista = (float*)seg_alloc(c, 4 * ((size_t)T + ns));
+      sg.lip = (int32_t*)seg_alloc(c, 4 * ((size_t)T + ns));
+      sg.pot = (double*)seg_alloc(c, 8 * ((size_t)T + ns));
+      sg.flag = (uint8_t*)seg_alloc(c, (size_t)T + ns);
+      sg.nbound = d_nbound;
+      sg.nscan = d_nscan;
+      sg.status = pr.status;
+      if (!sg.dista || !sg.lip || !sg.pot || !sg.flag) {
+        free(hw); free(h_off); free(h_act); free(h_done); free(h_st);
+        return ASOHF_ERR_CAPACITY;
+      }
+      SubMainIn in;
+      in.konta = d_konta; in.jjac = f_jjac; in.masadm = f_masadm; in.rclus = f_rclus;
+      in.cx = pr.cx; in.cy = pr.cy; in.cz = pr.cz; in.mhost = pr.mhost; in.disthost = pr.disthost;
+      {
+        int kt_ = ktime_begin(c, "sub_main");
+        k_sub_main<<<ns, HB, 0, c->stream>>>(S, H, m.d, d_work, in, sg);
+        ktime_end(c, kt_);
+      }
+      c->launches++;
+      ASOHF_CUDA(cudaGetLastError());
+      ASOHF_CUDA(cudaMemcpyAsync(h_st, pr.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      for (int s = 0; s < ns; s++)
+        if (h_st[s] && !rc) rc = h_st[s];
+      if (H.want_ids && rc == ASOHF_OK) {
+        int64_t total;
+        ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, ns, d_nbound, d_ids_off, &total));
+        ASOHF_CHECK(ensure_pph(c, total));
+        {
+          int kt_ = ktime_begin(c, "sub_write_ids");
+          k_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+          ktime_end(c, kt_);
+        }
+        c->launches++;
+        ASOHF_CUDA(cudaGetLastError());
+        c->pph_len = total;
+      }
+    }
+    free(h_off); free(h_act); free(h_done); free(h_st);
+  } else if (H.want_ids) {
+    int64_t total;
+    ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, 0, nullptr, nullptr, &total));
+    c->pph_len = total;
+  }
+  free(hw);
+  ASOHF_CHECK(cat_mirror_out(c, &m));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
 }

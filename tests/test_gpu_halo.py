@@ -49,3 +49,14 @@ def test_halofind_matches_oracle(gpu_lib, name):
     ro = driver.run(s, O.OracleBackend(), with_subs=False)
     assert (ro.cat.realclus[: ro.cat.nclus] != 0).sum() > 0
     compare(rg, ro)
+
+
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_substructure_matches_oracle(gpu_lib, name):
+    s = synth.generate(name)
+    rg = driver.run(s, api.GpuBackend(), with_subs=True)
+    ro = driver.run(s, O.OracleBackend(), with_subs=True)
+    assert np.array_equal(rg.subs_lev, ro.subs_lev)
+    sub = ro.cat.realclus[ro.subs_lev[0]: ro.cat.nclus]
+    assert (sub > 0).sum() > 0
+    compare(rg, ro)
