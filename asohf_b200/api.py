@@ -58,7 +58,8 @@ def load():
                      "asohf_tsc_poisson_forward", "asohf_tsc_poisson_adjoint",
                      "asohf_sort_dm_particles_x", "asohf_prune_poor_haloes",
                      "asohf_halofind_particles", "asohf_substructure_particles",
-                     "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats"]:
+                     "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
+                     "asohf_work_counters"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -117,6 +118,13 @@ class Asohf:
     def set_profiling(self, on: bool):
         """Brackets the main kernels with CUDA events (diagnostics)."""
         _check(self.L.asohf_set_profiling(self.h, C.c_int(int(on))), "asohf_set_profiling")
+
+    def work_counters(self, reset: bool = False):
+        """Element-passes of the halo (entry 0) and subhalo (entry 1) kernels."""
+        out = np.zeros(8, np.int64)
+        _check(self.L.asohf_work_counters(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)), C.c_int(int(reset))),
+               "asohf_work_counters")
+        return out
 
     def kernel_stats(self) -> dict:
         """{kernel name: (total device ms, launches)} since profiling was enabled."""

@@ -68,6 +68,8 @@ struct asohf_ctx {
   size_t seg_size = 0, seg_used = 0;
   // counters of kernels launched by this context (reported by the bench)
   int64_t launches = 0;
+  // work counters written by kernels (element-passes of the per-halo kernels)
+  unsigned long long* d_work = nullptr;  // 8 counters
   // optional CUDA-event timing of named kernels (asohf_set_profiling)
   int profiling = 0;
   struct KRec { const char* name; cudaEvent_t a, b; };

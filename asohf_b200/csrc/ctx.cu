@@ -151,7 +151,9 @@ extern "C" int asohf_create(int device, asohf_ctx** out) {
   asohf_ctx* c = new asohf_ctx();
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
-  if (arena_reserve(c, 64u << 20) != ASOHF_OK) {
+  if (arena_reserve(c, 64u << 20) != ASOHF_OK || cudaMalloc(&c->d_work, 64) != cudaSuccess ||
+      cudaMemset(c->d_work, 0, 64) != cudaSuccess) {
+    cudaFree(c->arena);
     delete c;
     return ASOHF_ERR_CUDA;
   }
@@ -171,6 +173,7 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaFree(c->d_pph);
   cudaFree(c->arena);
   cudaFree(c->seg);
+  cudaFree(c->d_work);
   for (int i = 0; i < c->nkrec; i++) { cudaEventDestroy(c->krec[i].a); cudaEventDestroy(c->krec[i].b); }
   free(c->krec);
   delete c;
@@ -289,6 +292,14 @@ extern "C" int asohf_download_particles(asohf_ctx* c, asohf_particles* d, int on
   ASOHF_CUDA(cudaMemcpyAsync(d->vz, c->p.vz, fb, k, c->stream));
   ASOHF_CUDA(cudaMemcpyAsync(d->m, c->p.m, fb, k, c->stream));
   ASOHF_CUDA(cudaMemcpyAsync(d->id, c->p.id, sizeof(int32_t) * (size_t)c->p.n, k, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_work_counters(asohf_ctx* c, int64_t* out, int reset) {
+  if (!c || !out) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaMemcpyAsync(out, c->d_work, 64, cudaMemcpyDeviceToHost, c->stream));
+  if (reset) ASOHF_CUDA(cudaMemsetAsync(c->d_work, 0, 64, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return ASOHF_OK;
 }

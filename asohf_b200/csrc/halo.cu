@@ -343,6 +343,7 @@ struct Seg {
   uint8_t* flag;
   int32_t* nbound;         // IDs to write per slot (KONTA2 of the property loop)
   int32_t* nscan;          // entries the property loop scanned (NCAPAS)
+  unsigned long long* work;  // element-pass counter of this kernel
   int32_t* status;
 };
 
@@ -804,12 +805,14 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
   float cm0[3], v0[3], m2;
   centromasas_block(S, dista, lip, flag, true, idx_vir, cm0, v0, &m2, sh);
   for (int q = 0; q < 3; q++) { h.cm[q] = cm0[q]; h.v[q] = v0[q]; }
+  unsigned long long ep = (unsigned long long)K + (unsigned long long)idx_vir;  // element-passes
   // escape-velocity unbinding (haloes_particles.f:894-907)
   int64_t contaerr = K;
   int fac = 0;
   while (contaerr > 0 || fac < 3) {
     fac++;
     int64_t prev = k2;
+    ep += (unsigned long long)k2;
     unbinding8_block(S, H, fac, ref_max, dista, lip, flag, pot, k2, idx_vir, h, sh);
     int64_t nk2;
     reordenar_compact(dista, lip, flag, k2, &idx_vir, &nk2, sh);
@@ -825,6 +828,7 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
   while (contaerr > 0 || fac < 4) {
     fac++;
     int64_t prev = k2;
+    ep += (unsigned long long)k2;
     unbinding_sigma_block(S, H, fac, lip, flag, k2, idx_vir, h, sh);
     int64_t nk2;
     reordenar_compact(dista, lip, flag, k2, &idx_vir, &nk2, sh);
@@ -1021,7 +1025,9 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
     return;
   }
   long long nb = properties_block(S, H, cat, i0, dista, lip, flag, ncapas, rshell, cx, cy, cz, cm0, true, sh);
+  ep += (unsigned long long)(k2 + ncapas);  // SO walk and property loop
   if (threadIdx.x == 0) {
+    atomicAdd(&sg.work[0], ep);
     bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
@@ -1242,6 +1248,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.flag = (uint8_t*)seg_alloc(c, (size_t)T + ns);
     sg.nbound = d_nbound;
     sg.nscan = d_nscan;
+    sg.work = c->d_work;
     sg.status = g.status;
     if (!k0 || !k1 || !v0 || !v1 || !t || !sg.dista || !sg.lip || !sg.pot || !sg.flag) {
       free(hk); free(hst); free(hoff); free(hw);
@@ -1581,6 +1588,7 @@ k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ w
   h.masa = (float)(masadm * (double)um);    // MSUB
   h.realclus = cat.realclus[i0];
   reverse_tie_runs(dista, lip, konta);
+  unsigned long long ep = 2ull * (unsigned long long)konta;
   int64_t k2 = konta, iv;
   float ref_max = dista[k2 - 1];
   int64_t contaerr = konta;
@@ -1597,6 +1605,7 @@ k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ w
     fac++;
     int64_t prev = k2;
     iv = k2;
+    ep += (unsigned long long)k2;
     unbinding8_block(S, H, fac, ref_max, dista, lip, flag, pot, k2, iv, h, sh);
     int64_t nk2;
     reordenar_compact(dista, lip, flag, k2, &iv, &nk2, sh);
@@ -1617,6 +1626,7 @@ k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ w
     fac++;
     int64_t prev = k2;
     iv = k2;
+    ep += (unsigned long long)k2;
     unbinding_sigma_block(S, H, fac, lip, flag, k2, iv, h, sh);
     int64_t nk2;
     reordenar_compact(dista, lip, flag, k2, &iv, &nk2, sh);
@@ -1788,7 +1798,9 @@ k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ w
   if (threadIdx.x == 0) { cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2]; }
   __syncthreads();
   long long nb = properties_block(S, H, cat, i0, dista, lip, flag, ncapas, rshell, cx, cy, cz, cm0, false, sh);
+  ep += (unsigned long long)(k2 + ncapas);
   if (threadIdx.x == 0) {
+    atomicAdd(&sg.work[1], ep);
     bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
@@ -2018,6 +2030,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       sg.flag = (uint8_t*)seg_alloc(c, (size_t)T + ns);
       sg.nbound = d_nbound;
       sg.nscan = d_nscan;
+      sg.work = c->d_work;
       sg.status = pr.status;
       if (!sg.dista || !sg.lip || !sg.pot || !sg.flag) {
         free(hw); free(h_off); free(h_act); free(h_done); free(h_st);

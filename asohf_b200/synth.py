@@ -78,6 +78,10 @@ CONFIGS = {
     # 512^3 in 250 Mpc/h, ~2e5 haloes in 1e10-1e15 (20..1e6 particles)
     "cfg4": SnapshotConfig("cfg4", 512, 250.0, 512, 6, 200000, 1e10, 1e15, 0.70,
                            sub_host_min=1e12),
+    # the 512^3 workload at 1/64 of its volume (same density and recipe):
+    # the bounded sample the CPU oracle is timed on
+    "cfg4s": SnapshotConfig("cfg4s", 128, 62.5, 128, 6, 3125, 1e10, 1e15, 0.70,
+                            sub_host_min=1e12),
     # small cases for tests
     "tiny": SnapshotConfig("tiny", 32, 10.0, 32, 2, 6, 1e11, 1e12, 0.70,
                            sub_host_min=3e11, seed=7),

@@ -1,0 +1,320 @@
+"""Benchmark of the ASOHF particle hot path on B200.
+
+One step = one pass of the hot path over one synthetic snapshot: species
+sort, kernel deposit (base grid + AMR patches) and renormalisation, x-slab
+sort, then per level PRUNE_POOR_HALOES / HALOFIND_PARTICLES and per
+substructure level SUBSTRUCTURE_PARTICLES, ending with the catalogue and the
+bound-particle ID lists.  The workload is the 512^3-particle snapshot
+(134M particles, 250 Mpc/h, 512^3 base grid, 6 AMR levels, ~2e5 haloes with
+subhaloes); inputs (4.3 GB of particles) are far larger than L2.
+
+  value  particles/s with the particles already in HBM (device timing);
+  e2e    particles/s through the same public API from pinned host arrays,
+         host->device copy of the particles and device->host copy of the
+         catalogue and IDs inside the timed region.
+Multi-GPU: the path does not exchange data, so every rank runs a replica
+on its own snapshot (weak scaling).
+
+--impl reference times the CPU restatement of the reference routines (the
+reference is Fortran and no Fortran compiler exists here) on a bounded
+sample of the same workload (the 512^3 recipe at 1/64 of the volume).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CPU_SAMPLE = "cfg4s"
+BYTES_PER_ELEMENT_PASS = 32  # d, m, |v| 12, position index read + dist/index written
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def clock_sampler(device):
+    f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                              "-lms", "200", "-i", str(device)], stdout=f, stderr=subprocess.DEVNULL)
+    except Exception:
+        p = None
+    return p, f.name
+
+
+def clock_summary(proc, path):
+    if proc is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    sm, smax, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    with open(path) as f:
+        for line in f:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+    os.unlink(path)
+    return {"sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_run(name, steps, warmup, nthreads):
+    """The oracle pipeline (CPU restatement of the reference routines)."""
+    from asohf_b200 import driver, synth
+    from oracle import oracle as O
+    snap = synth.generate(name)
+    plan = driver.prepare(snap)
+    b = O.OracleBackend(nthreads=nthreads)
+    for _ in range(warmup):
+        driver.execute(plan, b, download=False)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        driver.execute(plan, b, download=False)
+    dt = (time.perf_counter() - t0) / steps
+    return snap.cfg.n, dt
+
+
+def layer_bench(iters=10, warmup=3):
+    """Deposit+Poisson forward vs forward+adjoint: 8 jittered copies of the
+    64^3-particle set (positions + N(0, 0.01 cell)) onto a periodic 256^3 grid."""
+    import torch
+    from asohf_b200 import synth
+    from asohf_b200.autograd import DepositPoissonLayer
+    s = synth.generate("cfg1")
+    L = s.cfg.lado0
+    nx = 256
+    layer = DepositPoissonLayer(nx, L)
+    B = 8
+    rng = np.random.default_rng(3)
+    cell = L / nx
+    base = np.stack([s.x, s.y, s.z])
+    pos = base[:, None, :] + rng.normal(0.0, 0.01 * cell, (3, B, base.shape[1]))
+    pos = (np.mod(pos + L / 2, L) - L / 2).astype(np.float32)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x, y, z = (torch.tensor(pos[i], device=dev) for i in range(3))
+    m = torch.tensor(np.broadcast_to(s.m, (B, s.m.shape[0])).copy(), device=dev)
+    w = torch.randn((B, nx, nx, nx), generator=torch.Generator(device=dev).manual_seed(7), device=dev)
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(iters):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / iters
+
+    fwd = timed(lambda: layer.forward(x, y, z, m))
+    both = timed(lambda: (layer.forward(x, y, z, m), layer.adjoint(x, y, z, m, w, need_m=False)))
+    G = B * nx ** 3
+    N = B * base.shape[1]
+    # algorithmic bytes: deposit (read 16 B/particle, write rho), FFT pair
+    # (read rho, write/read half spectrum, write phi); adjoint: FFT pair on w,
+    # read 16 B/particle, write 12 B/particle of gradient
+    fwd_bytes = 16 * N + 4 * G + 16 * G
+    adj_bytes = 16 * G + 4 * G + 16 * N + 12 * N
+    hbm, src = peaks()
+    gbs = (fwd_bytes + adj_bytes) / (both * 1e-3) / 1e9
+    return {"config": "8 x 262144 particles (64^3 set, jittered N(0,0.01 cell)) -> periodic 256^3, FFT Poisson",
+            "fwd_ms": round(fwd, 4), "fwd_adj_ms": round(both, 4), "ratio": round(both / fwd, 4),
+            "fwd_adj_GBps": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4), "peak_source": src}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg4")
+    ap.add_argument("--no-subs", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-layer", action="store_true", help="skip the deposit+Poisson layer leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    metric = "particles/s (512^3 snapshot, hot path end to end)"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        nth = os.cpu_count() or 1
+        n, dt = cpu_oracle_run(CPU_SAMPLE, args.steps, args.warmup, nth)
+        v = n / dt
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": v, "unit": "particles/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": f"{CPU_SAMPLE}: 128^3 particles, 62.5 Mpc/h, the 512^3 recipe at 1/64 volume",
+                       "parallelism": "cpu"},
+            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": nth, "kind": "port",
+                             "sample": "full hot path on the 128^3 sample of the 512^3 recipe (C restatement of the Fortran)"},
+            "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    import torch
+    import torch.distributed as dist
+    from types import SimpleNamespace
+    from asohf_b200 import api, driver, synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    cfg = synth.CONFIGS[args.config]
+    cfg = synth.SnapshotConfig(**{**cfg.__dict__, "seed": cfg.seed + rank})
+    snap = synth.generate_fast(cfg, device=f"cuda:{local}", keep_on_device=True)
+    plan = driver.prepare(snap)
+    with_subs = not args.no_subs
+    b = api.DeviceBackend(local)
+    b.a.set_stream(torch.cuda.current_stream().cuda_stream)
+
+    def step():
+        return driver.execute(plan, b, with_subs=with_subs, download=False)
+
+    for _ in range(args.warmup):
+        r = step()
+    st = torch.cuda.current_stream()
+    clk, clk_path = clock_sampler(local)
+    b.a.set_profiling(True)
+    b.a.work_counters(reset=True)
+    l0 = b.a.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        r = step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clocks = clock_summary(clk, clk_path)
+    launches = (b.a.launch_count() - l0) // args.steps
+    kstats = b.a.kernel_stats()
+    work = b.a.work_counters()
+    b.a.set_profiling(False)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    n = cfg.n
+    value = world * n / (ms_max * 1e-3)
+
+    # e2e: pinned host particles in, catalogue and IDs out, through the API
+    host = [a.cpu().pin_memory() for a in (snap.x, snap.y, snap.z, snap.vx, snap.vy, snap.vz, snap.m, snap.id)]
+    parts_h = SimpleNamespace(x=host[0].numpy(), y=host[1].numpy(), z=host[2].numpy(), vx=host[3].numpy(),
+                              vy=host[4].numpy(), vz=host[5].numpy(), m=host[6].numpy(), id=host[7].numpy(), n=n)
+    be = api.GpuBackend(local)
+    be.a.set_stream(torch.cuda.current_stream().cuda_stream)
+
+    def step_e2e():
+        return driver.execute(plan, be, with_subs=with_subs, particles=parts_h, download=False)
+
+    re = step_e2e()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(st)
+    for _ in range(args.steps):
+        re = step_e2e()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms_e2e = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / args.steps
+    t = torch.tensor([ms_e2e], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e2e = float(t.item())
+    ncat = re.cat.nclus
+    cat_bytes = ncat * 4 * (45 + 2 * 20 + 3 + 3 + 6 + 2)
+    h2d = n * 32
+    d2h = int(re.pph.shape[0]) * 4 + cat_bytes
+    e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "particles/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
+
+    # roofline of the dominant kernel
+    hbm, src = peaks()
+    top = max(kstats.items(), key=lambda kv: kv[1][0]) if kstats else ("none", (0.0, 1))
+    name, (tot_ms, nl) = top
+    roofline = None
+    if name == "halo_main" and tot_ms > 0:
+        alg = float(work[0]) * BYTES_PER_ELEMENT_PASS
+        ach = alg / (tot_ms * 1e-3) / 1e9
+        roofline = {"kernel": name, "bound": "hbm", "achieved": round(ach, 2), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 5), "traffic": None, "peak_source": src,
+                    "algorithmic_bytes_per_launch": alg / nl, "avg_launch_ms": tot_ms / nl,
+                    "note": f"{BYTES_PER_ELEMENT_PASS} B per element-pass, element-passes counted on device"}
+    out = {
+        "metric": metric, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+        "config": {"workload": f"{cfg.name}: {cfg.npart_side}^3 particles, {cfg.box_mpc_h} Mpc/h box, "
+                               f"NX={cfg.nx}, NL={cfg.nl}, {cfg.n_haloes} NFW haloes"
+                               + (" + subhaloes" if with_subs else ""),
+                   "global_batch": world * n, "parallelism": f"replicas x{world}",
+                   "l2": "inputs > L2 (4.3 GB of particles per step)"},
+        "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches),
+        "kernels_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in
+                                sorted(kstats.items(), key=lambda kv: -kv[1][0])[:12]},
+        "stage_s": {k: round(v, 4) for k, v in r.stage_s.items()},
+        "catalogue": {"haloes": int((r.cat.realclus[: r.cat.nclus] == -1).sum()),
+                      "subhaloes": int((r.cat.realclus[: r.cat.nclus] > 0).sum()),
+                      "bound_ids": int(r.pph.shape[0])},
+    }
+    if rank == 0 and not args.no_layer:
+        out["deposit_poisson"] = layer_bench()
+    if rank == 0 and not args.no_cpu:
+        nth = os.cpu_count() or 1
+        n_s, dt = cpu_oracle_run(CPU_SAMPLE, 1, 0, nth)
+        out["cpu_baseline"] = {"value": n_s / dt, "unit": "particles/s", "cores": nth, "kind": "port",
+                               "sample": f"{CPU_SAMPLE}: 128^3 particles, the 512^3 recipe at 1/64 volume, "
+                                         "full hot path, 1 step"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

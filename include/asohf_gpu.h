@@ -46,6 +46,10 @@ int64_t asohf_launch_count(asohf_ctx *ctx);
 int asohf_set_profiling(asohf_ctx *ctx, int on);
 int asohf_kernel_stats(asohf_ctx *ctx, int i, const char **name, double *total_ms,
                        int64_t *launches);
+/* Diagnostics, no counterpart in the reference: 8 work counters (entry 0:
+ * element-passes of the halo kernel, 1: of the subhalo kernel), optionally
+ * reset after reading. */
+int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
 
 /* MODULE PARTICLES (particles.f:1-14) / READ_AND_ALLOC_PARTICLES
  * (alloc.f:196-528): copies the particle arrays into the device store,
