@@ -134,6 +134,26 @@ int asohf_substructure_particles(asohf_ctx *ctx, const asohf_consts *k, const as
                                  asohf_catalogue *cat, int ir, const int32_t *subs_lev,
                                  int on_device);
 
+/* No counterpart in the reference.  The periodic base-grid deposit of
+ * DENSITY (the same cloud terms as asohf_density's u1) for callers that
+ * cannot allocate device memory while they run -- an application that gives
+ * all GPU memory to its own pool up front and forbids later cudaMalloc, or
+ * code that must avoid the device synchronisation cudaMalloc/cudaFree can
+ * cause.  It allocates nothing and needs no context: x, y, z, m (n
+ * particles) and u1 (nx^3, column-major) are the caller's device pointers,
+ * cuda_stream the stream to run on.  Its float64 scratch is a fixed
+ * file-scope device array of ASOHF_NOALLOC_MAX_CELLS cells (16 MiB on every
+ * GPU that loads the library, until exit); grids with more cells are refused
+ * with ASOHF_ERR_CAPACITY.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  Every call shares the array and
+ * clears the part it uses: calls that overlap on the GPU (other streams,
+ * other host threads) race. */
+#define ASOHF_NOALLOC_MAX_CELLS (128 * 128 * 128)
+int asohf_density_base_noalloc(int nx, float lado0, float dx, float rote, float rete,
+                               int interp_degree, int64_t n, const float *x, const float *y,
+                               const float *z, const float *m, float *u1, void *cuda_stream);
+
 /* PARTICLES_PER_HALO (particles.f:12): copies the ID stream (host out);
  * *n receives its length (the largest INDCS_PARTICLES_PER_HALO(2,.)). */
 int asohf_get_particles_per_halo(asohf_ctx *ctx, int32_t *out, int64_t cap, int64_t *n,
