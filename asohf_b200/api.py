@@ -59,7 +59,7 @@ def load():
                      "asohf_sort_dm_particles_x", "asohf_prune_poor_haloes",
                      "asohf_halofind_particles", "asohf_substructure_particles",
                      "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
-                     "asohf_work_counters"]:
+                     "asohf_work_counters", "asohf_set_cluster_threshold"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -114,6 +114,12 @@ class Asohf:
 
     def launch_count(self) -> int:
         return int(self.L.asohf_launch_count(self.h))
+
+    def set_cluster_threshold(self, min_members: int):
+        """Haloes with at least min_members members go to the cluster path
+        (0: default)."""
+        _check(self.L.asohf_set_cluster_threshold(self.h, C.c_int64(int(min_members))),
+               "asohf_set_cluster_threshold")
 
     def set_profiling(self, on: bool):
         """Brackets the main kernels with CUDA events (diagnostics)."""
@@ -272,8 +278,10 @@ class GpuBackend:
 
     name = "gpu"
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, cluster_threshold: int = 0):
         self.a = Asohf(device)
+        if cluster_threshold:
+            self.a.set_cluster_threshold(cluster_threshold)
 
     def upload(self, parts):
         self.a.upload_particles(parts.x, parts.y, parts.z, parts.vx, parts.vy, parts.vz, parts.m,

@@ -42,7 +42,13 @@ struct DevParticles {
 struct asohf_ctx {
   int device = 0;
   cudaStream_t stream = 0;
+  // second stream for per-halo launches that run beside the cluster launch,
+  // forked from and joined back into `stream` with the two events
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int num_sms = 148;
+  // haloes of at least this many members are refined by a CTA cluster
+  int64_t cluster_min = 32768;
   DevParticles p;      // current store
   DevParticles alt;    // second buffer set for permutations
   float norma = 0.f;   // MAXVAL(MASAP), refreshed on upload

@@ -152,7 +152,13 @@ extern "C" int asohf_create(int device, asohf_ctx** out) {
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (arena_reserve(c, 64u << 20) != ASOHF_OK || cudaMalloc(&c->d_work, 64) != cudaSuccess ||
-      cudaMemset(c->d_work, 0, 64) != cudaSuccess) {
+      cudaMemset(c->d_work, 0, 64) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->side) cudaStreamDestroy(c->side);
+    cudaFree(c->d_work);
     cudaFree(c->arena);
     delete c;
     return ASOHF_ERR_CUDA;
@@ -174,6 +180,10 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaFree(c->arena);
   cudaFree(c->seg);
   cudaFree(c->d_work);
+  cudaStreamSynchronize(c->side);
+  cudaEventDestroy(c->ev_fork);
+  cudaEventDestroy(c->ev_join);
+  cudaStreamDestroy(c->side);
   for (int i = 0; i < c->nkrec; i++) { cudaEventDestroy(c->krec[i].a); cudaEventDestroy(c->krec[i].b); }
   free(c->krec);
   delete c;

@@ -1,18 +1,23 @@
 // halo.cu -- PRUNE_POOR_HALOES and HALOFIND_PARTICLES on sm_100a.
 //
 // Pipeline of one call (haloes lowh1..lowh2, largest first):
-//   k_halo_grow   one CTA per halo: density-peak recentering and the
-//                 spherical-overdensity growth (counts and sums only);
+//   k_halo_grow   density-peak recentering and the spherical-overdensity
+//                 growth (counts and sums only);
 //   (scan)        segment offsets from the final member counts;
-//   k_halo_gather one CTA per halo writes (halo, distance) keys and x-sorted
-//                 positions of its members into its segment;
+//   k_halo_gather (halo, distance) keys and x-sorted positions of the
+//                 members into each halo's segment;
 //   radix sort    of all segments at once on (halo, distance), then
 //   k_tiefix      orders equal distances by position, descending, which is
 //                 ARGSORT's order (num.f:181) over the slab-ordered list;
-//   k_halo_main   one CTA per halo: virial index, escape-velocity and
-//                 sigma-clipping unbinding, SO walk, bound-particle
-//                 properties;
+//   k_halo_main   virial index, escape-velocity and sigma-clipping
+//                 unbinding, SO walk, bound-particle properties;
 //   k_write_ids   bound-particle IDs in halo order (PARTICLES_PER_HALO).
+// Each per-halo kernel runs in two tiers: haloes of 32768 members or more
+// (asohf_set_cluster_threshold)
+// are refined by a thread-block cluster (16 CTAs, or 8 where 16 cannot be
+// co-scheduled) that splits every pass over the members, the others by one
+// CTA each on a second stream, so the clusters and the single CTAs share the
+// SMs instead of the largest halo finishing alone.
 // The reference scans a full-(y,z) x-slab per query (haloes_particles.f:
 // 117-143); the column index returns the same member sets from the columns a
 // sphere overlaps.
@@ -195,6 +200,73 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
   return ASOHF_OK;
 }
 
+// ---------------------------------------------------------------- launch helpers
+// Haloes whose member count reaches ctx->cluster_min are refined by a
+// cluster of CTAs; the others by one CTA each, launched concurrently on the
+// context's side stream.
+#define BIG_K 32768
+
+template <typename... P, typename... A>
+static cudaError_t launch_grp(void (*kern)(P...), int C, int ngroups, cudaStream_t s, A&&... args) {
+  if (ngroups <= 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ngroups * C));
+  cfg.blockDim = dim3(HB);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = C > 1 ? 1 : 0;
+  if (C > 8) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
+// Runs `big` (cluster kernel) on the context stream and `small` (one CTA per
+// halo) on the side stream, joined back into the context stream.
+static int fork_join(asohf_ctx* c) {
+  ASOHF_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+  ASOHF_CUDA(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+  return ASOHF_OK;
+}
+static int join(asohf_ctx* c) {
+  ASOHF_CUDA(cudaEventRecord(c->ev_join, c->side));
+  ASOHF_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  return ASOHF_OK;
+}
+
+// Splits slots 0..n-1 into big (count >= cluster_min) and small lists (device).
+static int split_slots(asohf_ctx* c, const int32_t* hcount, int n, int32_t* d_big, int32_t* d_small, int* nb,
+                       int* nsm) {
+  const int64_t big_k = c->cluster_min;
+  int32_t* hb = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
+  int32_t* hs = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
+  int b = 0, s = 0;
+  for (int i = 0; i < n; i++) {
+    if (hcount[i] >= big_k) hb[b++] = i;
+    else hs[s++] = i;
+  }
+  if (b) ASOHF_CUDA(cudaMemcpyAsync(d_big, hb, 4 * (size_t)b, cudaMemcpyHostToDevice, c->stream));
+  if (s) ASOHF_CUDA(cudaMemcpyAsync(d_small, hs, 4 * (size_t)s, cudaMemcpyHostToDevice, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  free(hb);
+  free(hs);
+  *nb = b;
+  *nsm = s;
+  return ASOHF_OK;
+}
+
+template <int C>
+__device__ __forceinline__ int group_slot(const int32_t* slots) { return slots[blockIdx.x / C]; }
+
+__device__ __forceinline__ bool leader(unsigned rank) { return rank == 0 && threadIdx.x == 0; }
+
 // ---------------------------------------------------------------- grow
 struct GrowOut {
   float *cx, *cy, *cz;     // recentred centre
@@ -213,27 +285,31 @@ __device__ __forceinline__ int level_of_patch(const HConst& H, int ipatch) {
 }
 
 // Recentering + growth of HALOFIND_PARTICLES (haloes_particles.f:741-849).
+template <int C>
 __global__ void __launch_bounds__(HB)
-k_halo_grow(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work,
-            GrowOut o) {
+k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, asohf_catalogue cat,
+            const int32_t* __restrict__ work, GrowOut o) {
   __shared__ RecShared sh;
-  int slot = blockIdx.x;
+  Grp<C> G;
+  int slot = group_slot<C>(slots);
   int i0 = work[slot];
+  unsigned rk = G.rank();
   if (cat.realclus[i0] == 0) {
-    if (threadIdx.x == 0) { o.konta[slot] = 0; o.status[slot] = 0; }
+    if (leader(rk)) { o.konta[slot] = 0; o.status[slot] = 0; }
     return;
   }
   int irr = level_of_patch(H, cat.patchclus[i0]);
   float cx = cat.clusrx[i0], cy = cat.clusry[i0], cz = cat.clusrz[i0];
+  float r_in = cat.radio[i0];
   float dxpamin = __fdiv_rn(ci.dx, exp2f((float)irr));
-  if (!recenter_block(S, ci, &cx, &cy, &cz, cat.radio[i0], dxpamin, sh)) {
-    if (threadIdx.x == 0) { o.konta[slot] = 0; o.status[slot] = ASOHF_ERR_CAPACITY; }
+  if (!recenter_group(G, S, ci, &cx, &cy, &cz, r_in, dxpamin, sh)) {
+    if (leader(rk)) { o.konta[slot] = 0; o.status[slot] = ASOHF_ERR_CAPACITY; }
     return;
   }
   float mino = __fmul_rn(fminf(200.0f, H.contrastec), H.fdm);
   float den0 = __fmul_rn(__fmul_rn(H.rote, __fmul_rn(__fmul_rn(H.rete, H.rete), H.rete)),
                          __fdiv_rn(__fmul_rn(4.0f, H.pi), 3.0f));
-  float rclus = cat.radio[i0];
+  float rclus = r_in;
   float delta2 = __fmul_rn(100.0f, mino);
   float rg = rclus;
   long long konta = 0;
@@ -245,7 +321,7 @@ k_halo_grow(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __
     long long c = 0;
     double ms = 0.0;
     float bas = -1.0f;
-    query_box(ci, cx, cy, cz, rclus, [&](const float4& e) {
+    gquery_box(G, ci, cx, cy, cz, rclus, [&](const float4& e) {
       int p = ppos(e);
       if (p < lo || p >= hi) return;
       float a = dist3(e.x, e.y, e.z, cx, cy, cz);
@@ -255,16 +331,16 @@ k_halo_grow(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __
         bas = fmaxf(bas, a);
       }
     });
-    konta = block_sum_ll(c, sh.lred);
-    masadm = block_sum_d(ms, sh.dred);
-    bas = block_max_f(bas, sh.fred);
+    konta = gsum_ll(G, c, sh.lred, sh.x);
+    masadm = gsum_d(G, ms, sh.dred, sh.x);
+    bas = gmax_f(G, bas, sh.fred, sh.x);
     float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(bas, bas), bas));
     delta2 = (float)(masadm / (double)den);
     rg = rclus;
     if (delta2 > __fmul_rn(0.9f, mino)) rclus = __fmul_rn(1.25f, rclus);
     if (++guard > 100000) break;
   }
-  if (threadIdx.x == 0) {
+  if (leader(rk)) {
     cat.clusrx[i0] = cx; cat.clusry[i0] = cy; cat.clusrz[i0] = cz;
     o.cx[slot] = cx; o.cy[slot] = cy; o.cz[slot] = cz;
     o.rgather[slot] = rg;
@@ -281,8 +357,48 @@ k_halo_grow(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __
 }
 
 // ---------------------------------------------------------------- gather
+// Members of sphere (cx, r) of each slot into its segment as (slot, distance)
+// keys and x-sorted positions; fill[] counts per slot (zeroed by the caller).
+template <int C>
 __global__ void __launch_bounds__(HB)
-k_halo_gather(Store S, ColIdx ci, const int32_t* __restrict__ konta, const int64_t* __restrict__ off,
+k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32_t* __restrict__ konta,
+              const int64_t* __restrict__ off, const float* __restrict__ hcx, const float* __restrict__ hcy,
+              const float* __restrict__ hcz, const float* __restrict__ rg, int32_t* __restrict__ fill,
+              unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
+  Grp<C> G;
+  int slot = group_slot<C>(slots);
+  int kmax = konta[slot];
+  if (kmax == 0) return;
+  float cx = hcx[slot], cy = hcy[slot], cz = hcz[slot], r = rg[slot];
+  int64_t lo, hi;
+  slab_range(ci, cx, r, &lo, &hi);
+  int64_t base = off[slot];
+  unsigned long long hk = (unsigned long long)slot << 32;
+  gquery_box(G, ci, cx, cy, cz, r, [&](const float4& e) {
+    int p = ppos(e);
+    float a = dist3(e.x, e.y, e.z, cx, cy, cz);
+    bool hit = p >= lo && p < hi && a < r;
+    // one counter update per warp
+    cg::coalesced_group act = cg::coalesced_threads();
+    unsigned hm = act.ballot(hit);
+    if (hm == 0u) return;
+    int lead = __ffs(hm) - 1;
+    int q0 = 0;
+    if ((int)act.thread_rank() == lead) q0 = atomicAdd(&fill[slot], __popc(hm));
+    q0 = act.shfl(q0, lead);
+    if (hit) {
+      int q = q0 + __popc(hm & ((1u << act.thread_rank()) - 1u));
+      if (q < kmax) {
+        keys[base + q] = hk | __float_as_uint(a);
+        vals[base + q] = p;
+      }
+    }
+  });
+}
+
+// Members of sphere (cx, r) of active entry blockIdx.x (substructure search).
+__global__ void __launch_bounds__(HB)
+k_sub_gather(Store S, ColIdx ci, const int32_t* __restrict__ konta, const int64_t* __restrict__ off,
               const float* __restrict__ hcx, const float* __restrict__ hcy, const float* __restrict__ hcz,
               const float* __restrict__ rg, unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
   __shared__ int fill;
@@ -747,37 +863,500 @@ __device__ __forceinline__ float so_den(float d, float rete, float pi) {
   return __fmul_rn(__fmul_rn(pi, 1.3333334f), __fmul_rn(__fmul_rn(dr, dr), dr));
 }
 
+// IDs of the bound subhalo particles, in radial order, at ids_off[slot].
 __global__ void __launch_bounds__(HB)
-k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work, GrowOut g, Seg sg) {
-  __shared__ MainShared sh;
+k_sub_write_ids(const int32_t* __restrict__ nscan, const int64_t* __restrict__ off, const int64_t* __restrict__ ids_off,
+            const int32_t* __restrict__ lip_all, const uint8_t* __restrict__ flag_all, const int32_t* __restrict__ id,
+            int32_t* __restrict__ out) {
+  __shared__ int sb[33];
   int slot = blockIdx.x;
-  int i0 = work[slot];
-  int64_t K = g.konta[slot];
-  if (threadIdx.x == 0) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; }
-  if (K == 0) return;
-  int64_t base = sg.off[slot] + slot;
-  float* dista = sg.dista + base;
-  int32_t* lip = sg.lip + base;
-  double* pot = sg.pot + base;
-  uint8_t* flag = sg.flag + base;
-  int64_t kbase = sg.off[slot];
-  for (int64_t j = threadIdx.x; j < K; j += blockDim.x) {
-    unsigned long long kk = sg.keys[kbase + j];
-    dista[j] = __uint_as_float((uint32_t)(kk & 0xffffffffull));
-    lip[j] = sg.vals[kbase + j];
+  int64_t n = nscan[slot];
+  if (n == 0) return;
+  int64_t base = off[slot] + slot;
+  const int32_t* lip = lip_all + base;
+  const uint8_t* flag = flag_all + base;
+  int64_t carry = ids_off[slot];
+  for (int64_t t0 = 0; t0 < n; t0 += HB) {
+    int64_t j = t0 + threadIdx.x;
+    bool k = j < n && flag[j];
+    int tot;
+    int inc = block_scan_i(k ? 1 : 0, sb, &tot);
+    if (k) out[carry + inc - 1] = id[lip[j]];
+    carry += tot;
+  }
+}
+
+// ================================================================ main (group)
+// The member list of one halo is staged contiguously (distance, x-sorted
+// position, mass and velocity, position) so the unbinding passes, the SO
+// walk and the property loop stream through it.  REORDENAR's in-place
+// compaction becomes a copy into the second buffer set: entries past the new
+// length are copied from the old list, so both sets hold what the in-place
+// compaction would leave there (DISTA(K2+1) is read by the next UNBINDING8).
+struct SegBuf {
+  float* d;
+  float4* mv;  // (m, vx, vy, vz)
+  float4* px;  // (x, y, z, x-sorted position as int bits)
+};
+
+struct SegView {
+  float* d;
+  float4* mv;
+  float4* px;
+};
+
+__device__ __forceinline__ SegView view_at(const SegBuf& b, int64_t base) {
+  return SegView{b.d + base, b.mv + base, b.px + base};
+}
+
+struct SegG {
+  const int32_t* konta;
+  const int64_t* off;       // element offset of the segment (segments padded by 1)
+  const unsigned long long* keys;
+  const int32_t* vals;
+  SegBuf a, b;
+  double* pot;
+  uint8_t* flag;
+  uint8_t* final_b;         // 1: the final member list is in set b
+  int32_t* nbound;          // IDs to write per slot (KONTA2 of the property loop)
+  int32_t* nscan;           // entries the property loop scanned (NCAPAS)
+  unsigned long long* work; // element-pass counter
+  int32_t* status;
+};
+
+struct GShared {
+  double dred[32];
+  float fred[32];
+  long long lred[32];
+  int sb[33];
+  double wv[32];
+  long long wj[32];
+  double wb[32];
+  double bc_d[2];
+  long long bc_l[2];
+  double at[16];
+  GX x;
+};
+
+// Values the leader (rank 0, thread 0) stored in sh.bc_* , seen by the group.
+template <int C>
+__device__ __forceinline__ void gbcast(const Grp<C>& g, double* d, long long* l, GShared& sh) {
+  if constexpr (C == 1) {
+    __syncthreads();
+    *d = sh.bc_d[0];
+    *l = sh.bc_l[0];
+    __syncthreads();
+  } else {
+    g.sync();
+    cg::cluster_group cl = cg::this_cluster();
+    *d = *cl.map_shared_rank(&sh.bc_d[0], 0);
+    *l = *cl.map_shared_rank(&sh.bc_l[0], 0);
+    g.sync();
+  }
+}
+
+// (v, j, b) with the largest v, the smallest j among equal v; j = LLONG_MAX
+// marks an empty entry.
+__device__ __forceinline__ bool best_before(double v1, long long j1, double v2, long long j2) {
+  if (j1 == LLONG_MAX) return false;
+  if (j2 == LLONG_MAX) return true;
+  return v1 > v2 || (v1 == v2 && j1 < j2);
+}
+
+template <int C>
+__device__ void gbest(const Grp<C>& g, double* v, long long* j, double* b, GShared& sh) {
+  double bv = *v, bb = *b;
+  long long bj = *j;
+  for (int o = 16; o > 0; o >>= 1) {
+    double ov = __shfl_down_sync(0xffffffffu, bv, o);
+    long long oj = __shfl_down_sync(0xffffffffu, bj, o);
+    double ob = __shfl_down_sync(0xffffffffu, bb, o);
+    if (best_before(ov, oj, bv, bj)) { bv = ov; bj = oj; bb = ob; }
+  }
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sh.wv[wid] = bv; sh.wj[wid] = bj; sh.wb[wid] = bb; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+      if (best_before(sh.wv[w], sh.wj[w], sh.wv[0], sh.wj[0])) {
+        sh.wv[0] = sh.wv[w]; sh.wj[0] = sh.wj[w]; sh.wb[0] = sh.wb[w];
+      }
+  }
+  __syncthreads();
+  bv = sh.wv[0]; bj = sh.wj[0]; bb = sh.wb[0];
+  __syncthreads();
+  if constexpr (C > 1) {
+    if (threadIdx.x == 0) { sh.x.d[0] = bv; sh.x.d[1] = bb; sh.x.l[0] = bj; }
+    g.sync();
+    if (threadIdx.x == 0) {
+      cg::cluster_group cl = cg::this_cluster();
+#pragma unroll 1
+      for (int r = 0; r < C; r++) {
+        double ov = *cl.map_shared_rank(&sh.x.d[0], r);
+        double ob = *cl.map_shared_rank(&sh.x.d[1], r);
+        long long oj = *cl.map_shared_rank(&sh.x.l[0], r);
+        if (best_before(ov, oj, bv, bj)) { bv = ov; bj = oj; bb = ob; }
+      }
+      sh.x.dres[0] = bv; sh.x.dres[1] = bb; sh.x.lres[0] = bj;
+    }
+    g.sync();
+    bv = sh.x.dres[0]; bb = sh.x.dres[1]; bj = sh.x.lres[0];
+  }
+  *v = bv; *j = bj; *b = bb;
+}
+
+// Stages the sorted members of one halo into set a.
+template <int C>
+__device__ void load_segment(const Grp<C>& g, const Store& S, const unsigned long long* keys,
+                             const int32_t* vals, int64_t K, const SegView& a, const SegView& b, uint8_t* flag) {
+  int64_t lo, hi;
+  g.chunk(0, K, &lo, &hi);
+  for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    unsigned long long kk = keys[j];
+    int p = vals[j];
+    a.d[j] = __uint_as_float((uint32_t)(kk & 0xffffffffull));
+    a.mv[j] = make_float4(S.m[p], S.vx[p], S.vy[p], S.vz[p]);
+    a.px[j] = make_float4(S.x[p], S.y[p], S.z[p], __int_as_float(p));
     flag[j] = 1;
   }
-  if (threadIdx.x == 0) dista[K] = 1.e10f;
-  __syncthreads();
-  float cx = g.cx[slot], cy = g.cy[slot], cz = g.cz[slot];
-  int kk_entero = cat.realclus[i0];
-  float pi = H.pi, rote = H.rote, rete = H.rete, fdm = H.fdm, um = H.um;
+  if (g.rank() == 0 && threadIdx.x == 0) {  // DISTA(K+1) of the sorted list
+    a.d[K] = 1.e10f; b.d[K] = 1.e10f;
+    a.mv[K] = make_float4(0.f, 0.f, 0.f, 0.f); b.mv[K] = a.mv[K];
+    a.px[K] = make_float4(0.f, 0.f, 0.f, 0.f); b.px[K] = a.px[K];
+  }
+  g.sync();
+}
+
+// CENTROMASAS_PART (haloes_particles.f:1731-1824) over the first n entries.
+template <int C>
+__device__ void centromasas_g(const Grp<C>& g, const SegView& v, int64_t n, float* cm, float* vcm, float* masa,
+                              GShared& sh) {
+  double a[7] = {0, 0, 0, 0, 0, 0, 0};
+  int64_t lo, hi;
+  g.chunk(0, n, &lo, &hi);
+  for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    float4 q = v.mv[j], p = v.px[j];
+    double bas = (double)q.x;
+    a[0] += (double)p.x * bas;
+    a[1] += (double)p.y * bas;
+    a[2] += (double)p.z * bas;
+    a[3] += (double)q.y * bas;
+    a[4] += (double)q.z * bas;
+    a[5] += (double)q.w * bas;
+    a[6] += bas;
+  }
+  gsum_dv<7>(g, a, sh.x);
+  if (a[6] > 0.0) {
+    for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
+    *masa = (float)a[6];
+  } else {
+    for (int q = 0; q < 3; q++) { cm[q] = 0.0f; vcm[q] = 0.0f; }
+    *masa = 0.0f;
+  }
+}
+
+// REORDENAR(...,0,...) (haloes_particles.f:1696-1722): the kept entries of
+// j < k2 in order into dst, IDX_VIR relocated to the first kept entry at or
+// after it; dst[k2new, k2) = src[k2new, k2).
+template <int C>
+__device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& dst, const uint8_t* flag,
+                          int64_t k2, int64_t* idx_vir, int64_t* k2new, GShared& sh) {
+  int64_t lo, hi;
+  g.chunk(0, k2, &lo, &hi);
+  long long mine = 0;
+  if constexpr (C > 1) {
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) mine += flag[j];
+    mine = block_sum_ll(mine, sh.lred);
+  }
+  long long off = 0, tot = 0;
+  gexcl_ll(g, mine, &off, &tot, sh.x);
+  int64_t carry = off;
+  long long reloc = LLONG_MAX;
+  int64_t iv = *idx_vir;  // 1-based
+  for (int64_t t0 = lo; t0 < hi; t0 += blockDim.x) {
+    int64_t j = t0 + threadIdx.x;
+    bool keep = j < hi && flag[j];
+    int tt;
+    int inc = block_scan_i(keep ? 1 : 0, sh.sb, &tt);
+    int64_t d = carry + inc - 1;
+    if (keep) {
+      dst.d[d] = src.d[j];
+      dst.mv[d] = src.mv[j];
+      dst.px[d] = src.px[j];
+      if (j + 1 >= iv && d + 1 < reloc) reloc = d + 1;
+    }
+    carry += tt;
+    __syncthreads();
+  }
+  int64_t nn = (C == 1) ? carry : tot;
+  g.chunk(nn, k2, &lo, &hi);
+  for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    dst.d[j] = src.d[j];
+    dst.mv[j] = src.mv[j];
+    dst.px[j] = src.px[j];
+  }
+  gmin_llv<1>(g, &reloc, sh.lred, sh.x);
+  *k2new = nn;
+  *idx_vir = reloc == LLONG_MAX ? nn : reloc;
+  g.sync();
+}
+
+// UNBINDING8 (haloes_particles.f:1828-1983) on the staged list.
+template <int C>
+__device__ void unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int fac, float ref_max,
+                             const SegView& v, uint8_t* flag, double* pot, int64_t k2, int64_t idx_vir,
+                             HaloState& h, GShared& sh) {
+  float cm[3] = {0, 0, 0}, vcm[3] = {0, 0, 0}, mmm = 0.0f;
+  long long konta3 = 0;
+  if (k2 > 0) {
+    double norma = (double)normaf;
+    float lim = __fmul_rn(0.01f, ref_max);
+    // first J with DISTA(J) > lim (the list is sorted by distance); K2+1 if none
+    int64_t a = 0, b = k2;
+    while (a < b) {
+      int64_t mid = (a + b) >> 1;
+      if (v.d[mid] > lim) b = mid; else a = mid + 1;
+    }
+    int64_t jj = a + 1;
+    // cumulative mass MASA8 (kept in pot for now)
+    gprefix_d(g, 0, k2, 0.0, [&](int64_t j) { return (double)v.mv[j].x / norma; },
+              [&](int64_t j, double s) { pot[j] = s; }, sh.dred, sh.x);
+    g.sync();
+    double mk2 = pot[k2 - 1];
+    double mjj = (jj == k2 + 1) ? mk2 : pot[jj - 1];
+    double pot_jj = mjj / (double)v.d[jj - 1];
+    // POT(J) for J > JJ: POT(J-1) + MASA8*BAS8/DISTA(J)^2
+    gprefix_d(g, jj, k2, pot_jj,
+              [&](int64_t j) {
+                float dj = v.d[j], dm = v.d[j - 1];
+                double bas8 = (dj != dm) ? (double)__fsub_rn(dj, dm) : 0.0;
+                double djd = (double)dj;
+                return pot[j] * bas8 / (djd * djd);
+              },
+              [&](int64_t j, double s) { pot[j] = s; }, sh.dred, sh.x);
+    int64_t lo, hi;
+    g.chunk(0, jj < k2 ? jj : k2, &lo, &hi);
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) pot[j] = pot_jj;
+    g.sync();
+    double pot1 = pot[k2 - 1] + mk2 / (double)ref_max;
+    double aa8 = norma * (double)__fdiv_rn(H.cgr, H.rete);
+    float bb = 2.0f;
+    if (fac == 1) bb = 8.0f;
+    if (fac == 2) bb = 4.0f;
+    bb = __fmul_rn(bb, bb);
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // 7 sums and the kept count
+    g.chunk(0, k2, &lo, &hi);
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+      float potok = (float)((pot[j] - pot1) * aa8);
+      float vesc2 = __fmul_rn(2.0f, fabsf(potok));
+      float4 q = v.mv[j];
+      float ax = __fsub_rn(q.y, h.v[0]), ay = __fsub_rn(q.z, h.v[1]), az = __fsub_rn(q.w, h.v[2]);
+      float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+      bool keep = !(vvv2 > __fmul_rn(bb, vesc2));
+      flag[j] = keep;
+      s[7] += keep ? 1.0 : 0.0;
+      if (keep && j < idx_vir) {
+        float4 p = v.px[j];
+        double bas = (double)q.x;
+        s[0] += (double)p.x * bas;
+        s[1] += (double)p.y * bas;
+        s[2] += (double)p.z * bas;
+        s[3] += (double)q.y * bas;
+        s[4] += (double)q.z * bas;
+        s[5] += (double)q.w * bas;
+        s[6] += bas;
+      }
+    }
+    gsum_dv<8>(g, s, sh.x);
+    konta3 = (long long)s[7];
+    if (s[6] > 0.0) {
+      for (int q = 0; q < 3; q++) { cm[q] = (float)(s[q] / s[6]); vcm[q] = (float)(s[3 + q] / s[6]); }
+      mmm = (float)s[6];
+    }
+  }
+  unbind_result(h, konta3, cm, vcm, mmm, H.um);
+}
+
+// UNBINDING_SIGMA (haloes_particles.f:1987-2095) on the staged list.
+template <int C>
+__device__ void unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, const SegView& v, uint8_t* flag,
+                                  int64_t k2, int64_t idx_vir, HaloState& h, GShared& sh) {
+  float bb = fmaxf(__fsub_rn(6.0f, __fmul_rn(1.0f, (float)(fac - 1))), 3.0f);
+  bb = __fmul_rn(bb, bb);
+  float cm[3] = {h.cm[0], h.cm[1], h.cm[2]}, vcm[3] = {h.v[0], h.v[1], h.v[2]}, mmm = 0.0f;
+  long long konta3 = 0;
+  if (k2 > 0) {
+    int64_t lo, hi;
+    g.chunk(0, idx_vir < k2 ? idx_vir : k2, &lo, &hi);
+    double s2 = 0.0;
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+      float4 q = v.mv[j];
+      float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
+      s2 += (double)__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+    }
+    double sigma2 = gsum_d(g, s2, sh.dred, sh.x);
+    if (idx_vir > 1) sigma2 = sigma2 / (double)(idx_vir - 1);
+    double thr = (double)bb * sigma2;
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    g.chunk(0, k2, &lo, &hi);
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+      float4 q = v.mv[j];
+      float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
+      float bas = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+      bool keep = !((double)bas > thr);
+      flag[j] = keep;
+      s[7] += keep ? 1.0 : 0.0;
+      if (keep && j < idx_vir) {
+        float4 p = v.px[j];
+        double w = (double)q.x;
+        s[0] += (double)p.x * w;
+        s[1] += (double)p.y * w;
+        s[2] += (double)p.z * w;
+        s[3] += (double)q.y * w;
+        s[4] += (double)q.z * w;
+        s[5] += (double)q.w * w;
+        s[6] += w;
+      }
+    }
+    gsum_dv<8>(g, s, sh.x);
+    konta3 = (long long)s[7];
+    if (s[6] > 0.0) {
+      for (int q = 0; q < 3; q++) { cm[q] = (float)(s[q] / s[6]); vcm[q] = (float)(s[3 + q] / s[6]); }
+      mmm = (float)s[6];
+    } else {
+      for (int q = 0; q < 3; q++) { cm[q] = 0.0f; vcm[q] = 0.0f; }
+      mmm = 0.0f;
+    }
+  }
+  unbind_result(h, konta3, cm, vcm, mmm, H.um);
+}
+
+// Bound-particle properties (haloes_particles.f:1187-1353) over j < konta of
+// the staged list; flag[j] receives the ID mask.  Returns KONTA2.
+template <int C>
+__device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
+                                  const SegView& v, uint8_t* flag, int64_t konta, float rshell, float cx, float cy,
+                                  float cz, const float* cmv, GShared& sh) {
   float norma = S.norma;
+  float vc[3] = {cat.vx[i0], cat.vy[i0], cat.vz[i0]};
+  int64_t each_prof = konta / ASOHF_NBINS;
+  if (each_prof == 0) each_prof = 1;
+  double acc[18];
+  for (int q = 0; q < 18; q++) acc[q] = 0.0;
+  float vmax = -1.0f;
+  gprefix_d(g, 0, konta, 0.0,
+            [&](int64_t j) {
+              float4 p = v.px[j];
+              float a = dist3(p.x, p.y, p.z, cx, cy, cz);
+              bool in = a <= rshell;
+              flag[j] = in;
+              return in ? (double)__fdiv_rn(v.mv[j].x, norma) : 0.0;
+            },
+            [&](int64_t j, double basmas) {
+              int64_t J = j + 1;
+              if (!flag[j]) return;
+              float4 p = v.px[j], q = v.mv[j];
+              float bv[3] = {__fsub_rn(p.x, cx), __fsub_rn(p.y, cy), __fsub_rn(p.z, cz)};
+              float aadm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(bv[0], bv[0]), __fmul_rn(bv[1], bv[1])),
+                                                __fmul_rn(bv[2], bv[2])));
+              acc[16] += 1.0;
+              if (J % each_prof == 0 && J / each_prof <= ASOHF_NBINS) {
+                int64_t b = J / each_prof;
+                cat.profiles[(size_t)i0 * 2 * ASOHF_NBINS + (b - 1)] = aadm;
+                cat.profiles[(size_t)i0 * 2 * ASOHF_NBINS + ASOHF_NBINS + (b - 1)] =
+                    (float)(basmas * (double)norma * (double)H.um);
+              }
+              float bc[3] = {__fsub_rn(p.x, cmv[0]), __fsub_rn(p.y, cmv[1]), __fsub_rn(p.z, cmv[2])};
+              float bvc[3] = {__fsub_rn(q.y, vc[0]), __fsub_rn(q.z, vc[1]), __fsub_rn(q.w, vc[2])};
+              float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(bvc[0], bvc[0]), __fmul_rn(bvc[1], bvc[1])),
+                                     __fmul_rn(bvc[2], bvc[2]));
+              float mp = q.x;
+              acc[0] += (double)vvv2;
+              acc[1] += (double)__fmul_rn(mp, vvv2);
+              acc[2] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[1], bvc[2]), __fmul_rn(bc[2], bvc[1])));
+              acc[3] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[2], bvc[0]), __fmul_rn(bc[0], bvc[2])));
+              acc[4] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[0], bvc[1]), __fmul_rn(bc[1], bvc[0])));
+              for (int jy = 0; jy < 3; jy++)
+                for (int ix = 0; ix < 3; ix++)
+                  acc[5 + jy * 3 + ix] += (double)__fmul_rn(__fmul_rn(mp, bc[ix]), bc[jy]);
+              vmax = fmaxf(vmax, vvv2);
+              if (aadm != 0.0f) {
+                float aa = __fadd_rn(__fadd_rn(__fmul_rn(__fdiv_rn(bv[0], aadm), bvc[0]),
+                                               __fmul_rn(__fdiv_rn(bv[1], aadm), bvc[1])),
+                                     __fmul_rn(__fdiv_rn(bv[2], aadm), bvc[2]));
+                acc[14] += (double)__fmul_rn(aa, mp);
+              }
+              acc[15] += (double)__fdiv_rn(mp, norma);
+            },
+            sh.dred, sh.x);
+  // the inertia tensor is symmetric by construction of its entries; only the
+  // six distinct sums are reduced
+  double r[13] = {acc[0], acc[2], acc[3], acc[4], acc[5], acc[6], acc[7], acc[9], acc[10], acc[13],
+                  acc[14], acc[15], acc[16]};
+  gsum_dv<13>(g, r, sh.x);
+  const double* r2 = r + 10;
+  vmax = gmax_f(g, vmax, sh.fred, sh.x);
+  long long cnt = (long long)r2[2];
+  if (g.rank() == 0 && threadIdx.x == 0) {
+    cat.dmpclus[i0] = (int32_t)cnt;
+    if (cnt < H.min_num_part) {
+      cat.realclus[i0] = 0;
+      cat.vmaxclus[i0] = vmax;  // the running maximum of |v|^2 (-1 if none) stays
+    } else {
+      cat.potential_e[i0] = 0.0f;
+      cat.iplip[i0] = S.id[__float_as_int(v.px[0].w)];
+      double basmas = r2[1];
+      double den = basmas * (double)norma;
+      cat.angularm[i0 * 3 + 0] = (float)(r[1] * (double)H.uv / den);
+      cat.angularm[i0 * 3 + 1] = (float)(r[2] * (double)H.uv / den);
+      cat.angularm[i0 * 3 + 2] = (float)(r[3] * (double)H.uv / den);
+      cat.mean_vr[i0] = (float)(r2[0] / den * (double)H.uv);
+      // in(ix, jy) column-major from the sums of bc(ix)*bc(jy) (jy <= ix kept)
+      float xx = (float)(r[4] / den), yx = (float)(r[5] / den), zx = (float)(r[6] / den);
+      float yy = (float)(r[7] / den), zy = (float)(r[8] / den), zz = (float)(r[9] / den);
+      float in[9] = {xx, yx, zx, yx, yy, zy, zx, zy, zz};
+      float* it = cat.inertia_tensor + (size_t)i0 * 6;
+      it[0] = xx; it[1] = yx; it[2] = zx; it[3] = yy; it[4] = zy; it[5] = zz;
+      cat.velocity_dispersion[i0] = (float)(sqrt(r[0] / (double)(float)cnt) * (double)H.uv);
+      cat.vmaxclus[i0] = __fmul_rn(__fsqrt_rn(vmax), H.uv);
+      float be[3] = {0.0f, 0.0f, 0.0f};
+      diagonalise_dev(in, be);
+      sort_eigen_dev(be);
+      for (int q = 0; q < 3; q++) cat.eigenval[(size_t)i0 * 3 + q] = __fsqrt_rn(__fmul_rn(5.0f, be[q]));
+    }
+  }
+  g.sync();
+  return cnt;
+}
+
+template <int C>
+__global__ void __launch_bounds__(HB)
+k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogue cat,
+            const int32_t* __restrict__ work, GrowOut go, SegG sg) {
+  __shared__ GShared sh;
+  Grp<C> g;
+  const int slot = group_slot<C>(slots);
+  const bool lead = leader(g.rank());
+  const int i0 = work[slot];
+  const int64_t K = go.konta[slot];
+  if (lead) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; sg.final_b[slot] = 0; }
+  if (K == 0) return;
+  const int64_t base = sg.off[slot] + slot;
+  SegView va = view_at(sg.a, base), vb = view_at(sg.b, base);
+  double* pot = sg.pot + base;
+  uint8_t* flag = sg.flag + base;
+  load_segment(g, S, sg.keys + sg.off[slot], sg.vals + sg.off[slot], K, va, vb, flag);
+  SegView cur = va, nxt = vb;
+  int which = 0;
+  float cx = go.cx[slot], cy = go.cy[slot], cz = go.cz[slot];
+  const int kk_entero = cat.realclus[i0];
+  const float pi = H.pi, rote = H.rote, rete = H.rete, fdm = H.fdm, um = H.um;
+  const float norma = S.norma;
   int64_t k2 = K, idx_vir = K;
-  float ref_max = dista[K - 1];
+  float ref_max = cur.d[K - 1];
   HaloState h;
-  h.radio = g.rclus[slot];
-  h.masa = (float)(g.masadm[slot] * (double)um);
+  h.radio = go.rclus[slot];
+  h.masa = (float)(go.masadm[slot] * (double)um);
   h.realclus = kk_entero;
   // FIND_IDX_VIR (haloes_particles.f:1453-1491)
   {
@@ -786,24 +1365,24 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
                            __fdiv_rn(__fmul_rn(4.0f, pi), 3.0f));
     float cvir = __fmul_rn(H.contrastec, fdm);
     long long best = LLONG_MAX;
-    tile_prefix_d(0, idx_vir, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
-                  [&](int64_t j, double menc) {
-                    if (j + 1 <= jjcore) return;
-                    float d = dista[j];
-                    float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(d, d), d));
-                    float delta = (float)(menc / (double)den);
-                    if (delta < cvir && (long long)(j + 1) < best) best = j + 1;
-                  },
-                  sh.dred);
-    best = bmin(best, sh);
+    gprefix_d(g, 0, idx_vir, 0.0, [&](int64_t j) { return (double)cur.mv[j].x; },
+              [&](int64_t j, double menc) {
+                if (j + 1 <= jjcore) return;
+                float d = cur.d[j];
+                float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(d, d), d));
+                float delta = (float)(menc / (double)den);
+                if (delta < cvir && (long long)(j + 1) < best) best = j + 1;
+              },
+              sh.dred, sh.x);
+    gmin_llv<1>(g, &best, sh.lred, sh.x);
     if (best == LLONG_MAX) {
-      if (threadIdx.x == 0) sg.status[slot] = ASOHF_ERR_NOT_PREFOUND_VIRIAL;
+      if (lead) sg.status[slot] = ASOHF_ERR_NOT_PREFOUND_VIRIAL;
       return;
     }
     idx_vir = best;
   }
   float cm0[3], v0[3], m2;
-  centromasas_block(S, dista, lip, flag, true, idx_vir, cm0, v0, &m2, sh);
+  centromasas_g(g, cur, idx_vir, cm0, v0, &m2, sh);
   for (int q = 0; q < 3; q++) { h.cm[q] = cm0[q]; h.v[q] = v0[q]; }
   unsigned long long ep = (unsigned long long)K + (unsigned long long)idx_vir;  // element-passes
   // escape-velocity unbinding (haloes_particles.f:894-907)
@@ -813,12 +1392,12 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
     fac++;
     int64_t prev = k2;
     ep += (unsigned long long)k2;
-    unbinding8_block(S, H, fac, ref_max, dista, lip, flag, pot, k2, idx_vir, h, sh);
+    unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, idx_vir, h, sh);
     int64_t nk2;
-    reordenar_compact(dista, lip, flag, k2, &idx_vir, &nk2, sh);
+    compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
+    SegView t = cur; cur = nxt; nxt = t; which ^= 1;
     k2 = nk2;
-    __syncthreads();
-    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
+    ref_max = k2 > 0 ? cur.d[k2 - 1] : 1.e10f;
     contaerr = prev - k2;
     if (fac > 100000) break;
   }
@@ -829,17 +1408,18 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
     fac++;
     int64_t prev = k2;
     ep += (unsigned long long)k2;
-    unbinding_sigma_block(S, H, fac, lip, flag, k2, idx_vir, h, sh);
+    unbinding_sigma_g(g, H, fac, cur, flag, k2, idx_vir, h, sh);
     int64_t nk2;
-    reordenar_compact(dista, lip, flag, k2, &idx_vir, &nk2, sh);
+    compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
+    SegView t = cur; cur = nxt; nxt = t; which ^= 1;
     k2 = nk2;
-    __syncthreads();
-    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
+    ref_max = k2 > 0 ? cur.d[k2 - 1] : 1.e10f;
     contaerr = prev - k2;
     if (fac > 100000) break;
   }
+  if (lead) sg.final_b[slot] = (uint8_t)which;
   if (k2 < H.min_num_part) {
-    if (threadIdx.x == 0) {
+    if (lead) {
       cat.realclus[i0] = 0;
       cat.radio[i0] = h.radio; cat.masa[i0] = h.masa;
       cat.clusrxcm[i0] = h.cm[0]; cat.clusrycm[i0] = h.cm[1]; cat.clusrzcm[i0] = h.cm[2];
@@ -859,101 +1439,96 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
                   __fmul_rn(500.0f, fdm), __fmul_rn(200.0f, fdm)};
   float cvir = __fmul_rn(H.contrastec, fdm);
   int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
-  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(S.m[lip[j]], norma); };
+  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(cur.mv[j].x, norma); };
   // pass A: virial crossing and the crossings at or before it
   long long jt[7];
   for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
-  tile_prefix_d(0, k2, 0.0, mn_of,
-                [&](int64_t j, double bas8) {
-                  int64_t J = j + 1;
-                  if (J <= jjcore) return;
-                  float vol = so_den(dista[j], rete, pi);
-                  float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
-                  for (int q = 0; q < 6; q++)
-                    if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
-                  if (delta2 <= cvir && J > jvir_min && J < jt[6]) jt[6] = J;
-                },
-                sh.dred);
-  for (int q = 0; q < 7; q++) jt[q] = bmin(jt[q], sh);
+  gprefix_d(g, 0, k2, 0.0, mn_of,
+            [&](int64_t j, double bas8) {
+              int64_t J = j + 1;
+              if (J <= jjcore) return;
+              float vol = so_den(cur.d[j], rete, pi);
+              float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
+              for (int q = 0; q < 6; q++)
+                if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+              if (delta2 <= cvir && J > jvir_min && J < jt[6]) jt[6] = J;
+            },
+            sh.dred, sh.x);
+  gmin_llv<7>(g, jt, sh.lred, sh.x);
   long long jvir = jt[6];
   double mvir = 0.0;
   if (jvir != LLONG_MAX) {
-    mvir = (double)__fdiv_rn(S.m[lip[jvir - 1]], norma);
+    mvir = (double)__fdiv_rn(cur.mv[jvir - 1].x, norma);
     bool again = false;
     for (int q = 0; q < 6; q++)
       if (jt[q] > jvir) { jt[q] = LLONG_MAX; again = true; }
     if (again) {  // pass A2: crossings after the virial one, with BAS8 - m(J_vir)
-      tile_prefix_d(0, k2, 0.0, mn_of,
-                    [&](int64_t j, double bas8) {
-                      int64_t J = j + 1;
-                      if (J <= jvir) return;
-                      double b8 = bas8 - mvir;
-                      float vol = so_den(dista[j], rete, pi);
-                      float delta2 = (float)((double)norma * b8 / (double)vol / (double)rote);
-                      for (int q = 0; q < 6; q++)
-                        if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
-                    },
-                    sh.dred);
-      for (int q = 0; q < 6; q++) jt[q] = bmin(jt[q], sh);
+      gprefix_d(g, 0, k2, 0.0, mn_of,
+                [&](int64_t j, double bas8) {
+                  int64_t J = j + 1;
+                  if (J <= jvir) return;
+                  double b8 = bas8 - mvir;
+                  float vol = so_den(cur.d[j], rete, pi);
+                  float delta2 = (float)((double)norma * b8 / (double)vol / (double)rote);
+                  for (int q = 0; q < 6; q++)
+                    if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+                },
+                sh.dred, sh.x);
+      gmin_llv<6>(g, jt, sh.lred, sh.x);
     }
   }
   bool exit_found = jvir != LLONG_MAX && jt[5] != LLONG_MAX;
   int64_t jend = exit_found ? max(jvir, jt[5]) : k2;
   // pass B: BAS8 at the crossings, V_c max over the walked range, and the
   // velocity sums up to the virial crossing (or the whole walk)
-  __shared__ double s_at[7];
-  __shared__ double s_vs[4];
+  if (threadIdx.x < 16) sh.at[threadIdx.x] = 0.0;
+  __syncthreads();
   double best_v = -1.0;
   long long best_j = LLONG_MAX;
   double best_b = 0.0;
   int64_t jv = jvir != LLONG_MAX ? jvir : jend;
-  double vacc[3] = {0.0, 0.0, 0.0};
-  double btot = tile_prefix_d(0, jend, 0.0, mn_of,
-                [&](int64_t j, double bas8) {
-                  int64_t J = j + 1;
-                  double b8 = (jvir != LLONG_MAX && J > jvir) ? bas8 - mvir : bas8;
-                  for (int q = 0; q < 7; q++)
-                    if (J == jt[q]) s_at[q] = (q == 6) ? bas8 : b8;
-                  if (J == jv) s_vs[0] = bas8;
-                  if (J <= jjcore) return;
-                  float bas2 = (float)(b8 / (double)dista[j]);
-                  if ((double)bas2 > best_v || ((double)bas2 == best_v && J < best_j)) {
-                    best_v = bas2;
-                    best_j = J;
-                    best_b = b8;
-                  }
-                },
-                sh.dred);
-  (void)btot;
-  for (int ax = 0; ax < 3; ax++) {
-    const float* vv = ax == 0 ? S.vx : (ax == 1 ? S.vy : S.vz);
-    vacc[ax] = tile_prefix_d(0, jv, 0.0, [&](int64_t j) {
-                               int p = lip[j];
-                               return (double)__fmul_rn(__fdiv_rn(S.m[p], norma), vv[p]);
-                             },
-                             [&](int64_t, double) {}, sh.dred);
-  }
-  if (threadIdx.x == 0) { s_vs[1] = vacc[0]; s_vs[2] = vacc[1]; s_vs[3] = vacc[2]; }
-  sh.bestv[threadIdx.x] = best_v;
-  sh.bestj[threadIdx.x] = best_j;
-  sh.bestb[threadIdx.x] = best_b;
+  gprefix_d(g, 0, jend, 0.0, mn_of,
+            [&](int64_t j, double bas8) {
+              int64_t J = j + 1;
+              double b8 = (jvir != LLONG_MAX && J > jvir) ? bas8 - mvir : bas8;
+              for (int q = 0; q < 7; q++)
+                if (J == jt[q]) sh.at[q] = (q == 6) ? bas8 : b8;
+              if (J == jv) sh.at[7] = bas8;
+              if (J <= jjcore) return;
+              float bas2 = (float)(b8 / (double)cur.d[j]);
+              if (best_before((double)bas2, J, best_v, best_j)) {
+                best_v = bas2;
+                best_j = J;
+                best_b = b8;
+              }
+            },
+            sh.dred, sh.x);
   __syncthreads();
+  double sv[11];
+  for (int q = 0; q < 8; q++) sv[q] = threadIdx.x == 0 ? sh.at[q] : 0.0;
+  sv[8] = sv[9] = sv[10] = 0.0;
+  {
+    int64_t lo, hi;
+    g.chunk(0, jv, &lo, &hi);
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+      float4 q = cur.mv[j];
+      float mn = __fdiv_rn(q.x, norma);
+      sv[8] += (double)__fmul_rn(mn, q.y);
+      sv[9] += (double)__fmul_rn(mn, q.z);
+      sv[10] += (double)__fmul_rn(mn, q.w);
+    }
+  }
+  gsum_dv<11>(g, sv, sh.x);
+  gbest(g, &best_v, &best_j, &best_b, sh);
   float rshell = 0.0f;
   int64_t ncapas = 0;
-  if (threadIdx.x == 0) {
-    double bv = -1.0;
-    long long bj = LLONG_MAX;
-    double bb = 0.0;
-    for (int t = 0; t < HB; t++) {
-      if (sh.bestj[t] == LLONG_MAX) continue;
-      if (sh.bestv[t] > bv || (sh.bestv[t] == bv && sh.bestj[t] < bj)) {
-        bv = sh.bestv[t]; bj = sh.bestj[t]; bb = sh.bestb[t];
-      }
-    }
-    if (bj != LLONG_MAX) {
-      cat.vcmax[i0] = (float)bv;
-      cat.mcmax[i0] = (float)bb;
-      cat.rcmax[i0] = dista[bj - 1];
+  if (lead) {
+    const double* s_at = sv;       // BAS8 at the crossings
+    double s_vs[4] = {sv[7], sv[8], sv[9], sv[10]};
+    if (best_j != LLONG_MAX) {
+      cat.vcmax[i0] = (float)best_v;
+      cat.mcmax[i0] = (float)best_b;
+      cat.rcmax[i0] = cur.d[best_j - 1];
     }
     float* mo[6] = {cat.m2500c, cat.m500c, cat.m200c, cat.m2500m, cat.m500m, cat.m200m};
     float* ro[6] = {cat.r2500c, cat.r500c, cat.r200c, cat.r2500m, cat.r500m, cat.r200m};
@@ -961,7 +1536,7 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
     for (int q = 0; q < 6; q++) {
       if (jt[q] != LLONG_MAX && jt[q] <= jend) {
         int64_t J = jt[q];
-        float d = dista[J - 1];
+        float d = cur.d[J - 1];
         float vol = so_den(d, rete, pi);
         float delta2 = (float)((double)norma * s_at[q] / (double)vol / (double)rote);
         mo[q][i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
@@ -972,12 +1547,12 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
     }
     bool salida = false;
     if (jvir != LLONG_MAX) {
-      int p = lip[jvir - 1];
-      float mn = __fdiv_rn(S.m[p], norma);
+      float4 q = cur.mv[jvir - 1];
+      float mn = __fdiv_rn(q.x, norma);
       double bas8 = s_vs[0] - (double)mn;
-      double bvx = s_vs[1] - (double)__fmul_rn(mn, S.vx[p]);
-      double bvy = s_vs[2] - (double)__fmul_rn(mn, S.vy[p]);
-      double bvz = s_vs[3] - (double)__fmul_rn(mn, S.vz[p]);
+      double bvx = s_vs[1] - (double)__fmul_rn(mn, q.y);
+      double bvy = s_vs[2] - (double)__fmul_rn(mn, q.z);
+      double bvz = s_vs[3] - (double)__fmul_rn(mn, q.w);
       h.masa = (float)(bas8 * (double)norma * (double)um);
       float vol = (float)(((double)norma * bas8) / (double)__fmul_rn(__fmul_rn(H.contrastec, fdm), rote));
       h.radio = __fdiv_rn(powf(__fdiv_rn(__fmul_rn(3.0f, vol), __fmul_rn(4.0f, pi)), 1.0f / 3.0f), rete);
@@ -1013,20 +1588,23 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
     cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2];
     cat.realclus[i0] = h.realclus;
     cat.dmpclus[i0] = (int32_t)K;
-    sh.v[0] = rshell;
-    sh.iv[0] = ncapas;
+    sh.bc_d[0] = rshell;
+    sh.bc_l[0] = ncapas;
   }
-  __syncthreads();
-  rshell = (float)sh.v[0];
-  ncapas = sh.iv[0];
-  __syncthreads();
+  {
+    double rs;
+    long long nc;
+    gbcast(g, &rs, &nc, sh);
+    rshell = (float)rs;
+    ncapas = nc;
+  }
   if (ncapas < H.min_num_part) {
-    if (threadIdx.x == 0) cat.realclus[i0] = 0;
+    if (lead) cat.realclus[i0] = 0;
     return;
   }
-  long long nb = properties_block(S, H, cat, i0, dista, lip, flag, ncapas, rshell, cx, cy, cz, cm0, true, sh);
+  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh);
   ep += (unsigned long long)(k2 + ncapas);  // SO walk and property loop
-  if (threadIdx.x == 0) {
+  if (lead) {
     atomicAdd(&sg.work[0], ep);
     bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
@@ -1036,40 +1614,44 @@ k_halo_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ 
 }
 
 // IDs of the bound particles, in radial order, at ids_off[slot].
+template <int C>
 __global__ void __launch_bounds__(HB)
-k_write_ids(const int32_t* __restrict__ nscan, const int64_t* __restrict__ off, const int64_t* __restrict__ ids_off,
-            const int32_t* __restrict__ lip_all, const uint8_t* __restrict__ flag_all, const int32_t* __restrict__ id,
-            int32_t* __restrict__ out) {
+k_write_ids(const int32_t* __restrict__ slots, const int32_t* __restrict__ nscan, const int64_t* __restrict__ off,
+            const int64_t* __restrict__ ids_off, const uint8_t* __restrict__ final_b,
+            const float4* __restrict__ px_a, const float4* __restrict__ px_b,
+            const uint8_t* __restrict__ flag_all, const int32_t* __restrict__ id, int32_t* __restrict__ out) {
   __shared__ int sb[33];
-  int slot = blockIdx.x;
+  __shared__ long long lred[32];
+  __shared__ GX x;
+  Grp<C> g;
+  int slot = group_slot<C>(slots);
   int64_t n = nscan[slot];
   if (n == 0) return;
   int64_t base = off[slot] + slot;
-  const int32_t* lip = lip_all + base;
+  const float4* px = (final_b[slot] ? px_b : px_a) + base;
   const uint8_t* flag = flag_all + base;
-  int64_t carry = ids_off[slot];
-  for (int64_t t0 = 0; t0 < n; t0 += HB) {
+  int64_t lo, hi;
+  g.chunk(0, n, &lo, &hi);
+  long long mine = 0;
+  if constexpr (C > 1) {
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) mine += flag[j];
+    mine = block_sum_ll(mine, lred);
+  }
+  long long o = 0, tot = 0;
+  gexcl_ll(g, mine, &o, &tot, x);
+  int64_t carry = ids_off[slot] + o;
+  for (int64_t t0 = lo; t0 < hi; t0 += blockDim.x) {
     int64_t j = t0 + threadIdx.x;
-    bool k = j < n && flag[j];
-    int tot;
-    int inc = block_scan_i(k ? 1 : 0, sb, &tot);
-    if (k) out[carry + inc - 1] = id[lip[j]];
-    carry += tot;
+    bool k = j < hi && flag[j];
+    int tt;
+    int inc = block_scan_i(k ? 1 : 0, sb, &tt);
+    if (k) out[carry + inc - 1] = id[__float_as_int(px[j].w)];
+    carry += tt;
+    __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------- host driver
-struct HaloRun {
-  int nslots;
-  int32_t* d_work;
-  GrowOut g;
-  int64_t* d_off;
-  int64_t total;
-  unsigned long long* keys;
-  int32_t* vals;
-  Seg sg;
-};
-
 int ensure_pph(asohf_ctx* c, int64_t need) {
   if (need <= c->pph_cap) return ASOHF_OK;
   int64_t cap = need + need / 2 + 1024;
@@ -1132,7 +1714,8 @@ int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int3
 
 // Work list: haloes of [low1, low2] with REALCLUS != 0, DMPCLUS descending
 // (largest first keeps the longest CTAs from finishing last).
-int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots) {
+int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots,
+              int32_t** h_dm = nullptr) {
   int nh = low2 - low1 + 1;
   int32_t* rc = (int32_t*)malloc(4 * (size_t)nh);
   int32_t* dm = (int32_t*)malloc(4 * (size_t)nh);
@@ -1158,10 +1741,82 @@ int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, 
     memcpy(w, tmp, 4 * (size_t)k);
   }
   free(tmp);
+  if (h_dm) {  // DMPCLUS of each slot
+    int32_t* d = (int32_t*)malloc(4 * (size_t)(k > 0 ? k : 1));
+    for (int i = 0; i < k; i++) d[i] = dm[w[i] - (low1 - 1)];
+    *h_dm = d;
+  }
   free(rc);
   free(dm);
   *h_work = w;
   *nslots = k;
+  return ASOHF_OK;
+}
+
+// Cluster size for the large haloes on this device: 16 CTAs where the
+// device can co-schedule such clusters of k_halo_main, else 8, else 1.
+static int g_big_cluster[64];
+
+template <typename... P>
+static int max_clusters(void (*kern)(P...), int C) {
+  if (C > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)C);
+  cfg.blockDim = dim3(HB);
+  cudaLaunchAttribute a[1];
+  a[0].id = cudaLaunchAttributeClusterDimension;
+  a[0].val.clusterDim.x = C;
+  a[0].val.clusterDim.y = 1;
+  a[0].val.clusterDim.z = 1;
+  cfg.attrs = a;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+static int big_cluster(asohf_ctx* c) {
+  int d = c->device;
+  if (d < 0 || d >= 64) return 1;
+  if (g_big_cluster[d] == 0) {
+    int C = 1;
+    if (max_clusters(k_halo_main<16>, 16) > 0 && max_clusters(k_halo_grow<16>, 16) > 0 &&
+        max_clusters(k_halo_gather<16>, 16) > 0 && max_clusters(k_write_ids<16>, 16) > 0)
+      C = 16;
+    else if (max_clusters(k_halo_main<8>, 8) > 0 && max_clusters(k_halo_grow<8>, 8) > 0 &&
+             max_clusters(k_halo_gather<8>, 8) > 0 && max_clusters(k_write_ids<8>, 8) > 0)
+      C = 8;
+    g_big_cluster[d] = C;
+  }
+  return g_big_cluster[d];
+}
+
+// Launches kern<C> for the `n` groups of slots[] on stream s (C in {1, 8, 16}).
+#define LAUNCH_TIER(KERN, C, n, s, ...)                                              \
+  ((C) == 16 ? launch_grp(KERN<16>, 16, (n), (s), __VA_ARGS__)                       \
+             : (C) == 8 ? launch_grp(KERN<8>, 8, (n), (s), __VA_ARGS__)              \
+                        : launch_grp(KERN<1>, 1, (n), (s), __VA_ARGS__))
+
+// The big tier on the context stream and the small tier on the side stream,
+// the context stream waiting for both.
+#define LAUNCH_SPLIT(KERN, CB, nb, big, ns_, small, ...)                                      \
+  do {                                                                                         \
+    ASOHF_CHECK(fork_join(c));                                                                 \
+    if ((nb) > 0) ASOHF_CUDA(LAUNCH_TIER(KERN, CB, (nb), c->stream, big, __VA_ARGS__));        \
+    if ((ns_) > 0) ASOHF_CUDA(launch_grp(KERN<1>, 1, (ns_), c->side, small, __VA_ARGS__));     \
+    ASOHF_CHECK(join(c));                                                                      \
+    c->launches += ((nb) > 0) + ((ns_) > 0);                                                   \
+  } while (0)
+
+extern "C" int asohf_set_cluster_threshold(asohf_ctx* c, int64_t min_members) {
+  if (!c || min_members < 0) return ASOHF_ERR_INVALID;
+  c->cluster_min = min_members == 0 ? BIG_K : min_members;
   return ASOHF_OK;
 }
 
@@ -1174,20 +1829,26 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
   int nh = lowh2 - lowh1 + 1;
-  size_t need = cat_bytes(lowh2) + (size_t)nh * 64 + 65536;
+  size_t need = cat_bytes(lowh2) + (size_t)nh * 96 + 65536;
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
   ASOHF_CHECK(cat_mirror_in(c, cat, lowh2, on_device, &m));
-  int32_t* hw;
+  int32_t *hw, *hdm;
   int ns;
-  ASOHF_CHECK(make_work(c, m, lowh1, lowh2, &hw, &ns));
+  ASOHF_CHECK(make_work(c, m, lowh1, lowh2, &hw, &ns, &hdm));
   Store S = store_of(c);
   ColIdx ci = col_idx(c, k);
   HConst H = hconst(k, mesh);
+  const int CB = big_cluster(c);
   int rc = ASOHF_OK;
   if (ns > 0) {
     // per-slot buffers
     int32_t* d_work = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_iota = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_big = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_small = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_fill = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    uint8_t* d_final = (uint8_t*)arena_alloc(c, (size_t)ns);
     GrowOut g;
     g.cx = (float*)arena_alloc(c, 4 * (size_t)ns);
     g.cy = (float*)arena_alloc(c, 4 * (size_t)ns);
@@ -1201,16 +1862,28 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     int32_t* d_nbound = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int32_t* d_nscan = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int64_t* d_ids_off = (int64_t*)arena_alloc(c, 8 * (size_t)ns);
-    if (!d_work || !g.cx || !g.cy || !g.cz || !g.rgather || !g.rclus || !g.konta || !g.masadm || !g.status ||
-        !d_off || !d_nbound || !d_nscan || !d_ids_off) { free(hw); return ASOHF_ERR_CAPACITY; }
+    if (!d_work || !d_iota || !d_big || !d_small || !d_fill || !d_final || !g.cx || !g.cy || !g.cz ||
+        !g.rgather || !g.rclus || !g.konta || !g.masadm || !g.status || !d_off || !d_nbound || !d_nscan ||
+        !d_ids_off) {
+      free(hw); free(hdm);
+      return ASOHF_ERR_CAPACITY;
+    }
     ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+    // growth: slots are in DMPCLUS-descending order, so the big tier is a prefix
+    int nbig = 0;
+    while (CB > 1 && nbig < ns && hdm[nbig] >= c->cluster_min) nbig++;
+    {
+      int32_t* io = (int32_t*)malloc(4 * (size_t)ns);
+      for (int s = 0; s < ns; s++) io[s] = s;
+      ASOHF_CUDA(cudaMemcpyAsync(d_iota, io, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      free(io);
+    }
     {
       int kt_ = ktime_begin(c, "halo_grow");
-      k_halo_grow<<<ns, HB, 0, c->stream>>>(S, ci, H, m.d, d_work, g);
+      LAUNCH_SPLIT(k_halo_grow, CB, nbig, d_iota, ns - nbig, d_iota + nbig, S, ci, H, m.d, d_work, g);
       ktime_end(c, kt_);
     }
-    c->launches++;
-    ASOHF_CUDA(cudaGetLastError());
     // offsets (host scan: ns is the number of haloes of one level)
     int32_t* hk = (int32_t*)malloc(4 * (size_t)ns);
     int32_t* hst = (int32_t*)malloc(4 * (size_t)ns);
@@ -1225,6 +1898,13 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     }
     int64_t T = hoff[ns];
     ASOHF_CUDA(cudaMemcpyAsync(d_off, hoff, 8 * (size_t)(ns + 1), cudaMemcpyHostToDevice, c->stream));
+    int nb2 = 0, ns2 = 0;
+    if (CB > 1) {
+      ASOHF_CHECK(split_slots(c, hk, ns, d_big, d_small, &nb2, &ns2));
+    } else {
+      ASOHF_CUDA(cudaMemcpyAsync(d_small, d_iota, 4 * (size_t)ns, cudaMemcpyDeviceToDevice, c->stream));
+      ns2 = ns;
+    }
     // element buffers (allocated after the per-slot ones: the arena grows
     // only when empty, so reserve everything now)
     int bits = 1;
@@ -1232,32 +1912,41 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     size_t tb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                     (int32_t*)nullptr, (int32_t*)nullptr, (int)(T > 0 ? T : 1), 0, 32 + bits);
-    size_t elem = (size_t)T * (8 + 8 + 4 + 4) + tb + ((size_t)T + ns) * (4 + 4 + 8 + 1) + 16384;
+    size_t E = (size_t)T + ns;
+    size_t elem = (size_t)T * (8 + 8 + 4 + 4) + tb + E * (2 * (4 + 16 + 16) + 8 + 1) + 32768;
     ASOHF_CHECK(seg_reserve(c, elem));
     unsigned long long* k0 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
     unsigned long long* k1 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
     int32_t* v0 = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
     int32_t* v1 = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
     void* t = seg_alloc(c, tb);
-    Seg sg;
+    SegG sg;
     sg.konta = g.konta;
     sg.off = d_off;
-    sg.dista = (float*)seg_alloc(c, 4 * ((size_t)T + ns));
-    sg.lip = (int32_t*)seg_alloc(c, 4 * ((size_t)T + ns));
-    sg.pot = (double*)seg_alloc(c, 8 * ((size_t)T + ns));
-    sg.flag = (uint8_t*)seg_alloc(c, (size_t)T + ns);
+    sg.a.d = (float*)seg_alloc(c, 4 * E);
+    sg.a.mv = (float4*)seg_alloc(c, 16 * E);
+    sg.a.px = (float4*)seg_alloc(c, 16 * E);
+    sg.b.d = (float*)seg_alloc(c, 4 * E);
+    sg.b.mv = (float4*)seg_alloc(c, 16 * E);
+    sg.b.px = (float4*)seg_alloc(c, 16 * E);
+    sg.pot = (double*)seg_alloc(c, 8 * E);
+    sg.flag = (uint8_t*)seg_alloc(c, E);
+    sg.final_b = d_final;
     sg.nbound = d_nbound;
     sg.nscan = d_nscan;
     sg.work = c->d_work;
     sg.status = g.status;
-    if (!k0 || !k1 || !v0 || !v1 || !t || !sg.dista || !sg.lip || !sg.pot || !sg.flag) {
-      free(hk); free(hst); free(hoff); free(hw);
+    if (!k0 || !k1 || !v0 || !v1 || !t || !sg.a.d || !sg.a.mv || !sg.a.px || !sg.b.d || !sg.b.mv || !sg.b.px ||
+        !sg.pot || !sg.flag) {
+      free(hk); free(hst); free(hoff); free(hw); free(hdm);
       return ASOHF_ERR_CAPACITY;
     }
     if (T > 0) {
+      ASOHF_CUDA(cudaMemsetAsync(d_fill, 0, 4 * (size_t)ns, c->stream));
       {
         int kt_ = ktime_begin(c, "halo_gather");
-        k_halo_gather<<<ns, HB, 0, c->stream>>>(S, ci, g.konta, d_off, g.cx, g.cy, g.cz, g.rgather, k0, v0);
+        LAUNCH_SPLIT(k_halo_gather, CB, nb2, d_big, ns2, d_small, S, ci, g.konta, d_off, g.cx, g.cy, g.cz,
+                     g.rgather, d_fill, k0, v0);
         ktime_end(c, kt_);
       }
       int kt_ = ktime_begin(c, "halo_radix_sort");
@@ -1274,10 +1963,9 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.vals = v1;
     {
       int kt_ = ktime_begin(c, "halo_main");
-      k_halo_main<<<ns, HB, 0, c->stream>>>(S, H, m.d, d_work, g, sg);
+      LAUNCH_SPLIT(k_halo_main, CB, nb2, d_big, ns2, d_small, S, H, m.d, d_work, g, sg);
       ktime_end(c, kt_);
     }
-    c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
@@ -1289,10 +1977,10 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       ASOHF_CHECK(ensure_pph(c, total));
       {
         int kt_ = ktime_begin(c, "halo_write_ids");
-        k_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+        LAUNCH_SPLIT(k_write_ids, CB, nb2, d_big, ns2, d_small, d_nscan, d_off, d_ids_off, d_final, sg.a.px,
+                     sg.b.px, sg.flag, c->p.id, c->d_pph);
         ktime_end(c, kt_);
       }
-      c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       c->pph_len = total;
     }
@@ -1303,6 +1991,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     c->pph_len = total;
   }
   free(hw);
+  free(hdm);
   ASOHF_CHECK(cat_mirror_out(c, &m));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return rc;
@@ -1345,7 +2034,7 @@ k_sub_prep(Store S, ColIdx ci, HConst H, asohf_catalogue cat, const int32_t* __r
   int irr = level_of_patch(H, cat.patchclus[i0]);
   float cx = cat.clusrx[i0], cy = cat.clusry[i0], cz = cat.clusrz[i0];
   float dxpamin = __fdiv_rn(ci.dx, exp2f((float)irr));
-  if (!recenter_block(S, ci, &cx, &cy, &cz, cat.rsub[i0], dxpamin, sh)) {
+  if (!recenter_group(Grp<1>(), S, ci, &cx, &cy, &cz, cat.rsub[i0], dxpamin, sh)) {
     if (threadIdx.x == 0) o.status[slot] = ASOHF_ERR_CAPACITY;
     return;
   }
@@ -1867,11 +2556,11 @@ static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na,
   void* t = seg_alloc(c, tb);
   if (!k0 || !k1 || !v0 || !v1 || !t) return ASOHF_ERR_CAPACITY;
   if (T > 0) {
-    // k_halo_gather reads per-slot arrays through the active list order: it
+    // k_sub_gather reads per-slot arrays through the active list order: it
     // indexes by blockIdx (slot in the active list), so pass compacted views
     {
       int kt_ = ktime_begin(c, "sub_gather");
-      k_halo_gather<<<na, HB, 0, c->stream>>>(S, ci, d_konta, d_off, cx, cy, cz, r, k0, v0);
+      k_sub_gather<<<na, HB, 0, c->stream>>>(S, ci, d_konta, d_off, cx, cy, cz, r, k0, v0);
       ktime_end(c, kt_);
     }
     int kt_ = ktime_begin(c, "sub_radix_sort");
@@ -2056,7 +2745,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
         ASOHF_CHECK(ensure_pph(c, total));
         {
           int kt_ = ktime_begin(c, "sub_write_ids");
-          k_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+          k_sub_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
           ktime_end(c, kt_);
         }
         c->launches++;

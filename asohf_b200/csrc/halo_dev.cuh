@@ -6,12 +6,246 @@
 // uniform across the CTA.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
+
+namespace cg = cooperative_groups;
 
 #define HB 256          // threads per CTA of the per-halo kernels
 #define IPT 4           // items per thread per tile
 #define TILE (HB * IPT)
 #define MAX_HIST 48     // recentering shrink steps kept in shared memory
+
+// A halo is refined by a group of C CTAs: one CTA (C = 1) or a thread-block
+// cluster whose CTAs split every element loop into contiguous chunks and
+// combine partial results through distributed shared memory.
+template <int C>
+struct Grp {
+  __device__ __forceinline__ unsigned rank() const {
+    if constexpr (C == 1) return 0;
+    else return cg::this_cluster().block_rank();
+  }
+  __device__ __forceinline__ void sync() const {
+    if constexpr (C == 1) __syncthreads();
+    else cg::this_cluster().sync();
+  }
+  // this CTA's contiguous part of [a, b)
+  __device__ __forceinline__ void chunk(int64_t a, int64_t b, int64_t* lo, int64_t* hi) const {
+    if constexpr (C == 1) {
+      *lo = a;
+      *hi = b;
+    } else {
+      int64_t n = b > a ? b - a : 0, per = (n + C - 1) / C, r = rank();
+      *lo = a + (per * r < n ? per * r : n);
+      *hi = a + (per * (r + 1) < n ? per * (r + 1) : n);
+    }
+  }
+  // first global warp and warp stride for warp-strided loops
+  __device__ __forceinline__ int warp0() const { return (int)rank() * (blockDim.x >> 5) + (threadIdx.x >> 5); }
+  __device__ __forceinline__ int nwarps() const { return C * (blockDim.x >> 5); }
+};
+
+// Per-CTA exchange slots for group reductions.  A group reduction first
+// reduces over the CTA, then (C > 1) thread 0 publishes the CTA's value and
+// a few threads combine the C published values in rank order, so results are
+// identical on every CTA and do not depend on scheduling.
+struct GX {
+  double vred[16][32];  // per-warp partials of vector sums
+  double bres[16];      // CTA totals
+  double d[16];         // published CTA values
+  double dres[16];      // group totals
+  long long l[8];
+  long long lres[8];
+  float f[2];
+  float fres[2];
+};
+
+// Sum of K doubles over the CTA; every thread receives the totals.
+template <int K>
+__device__ __forceinline__ void block_sum_dv(double* v, GX& x) {
+  static_assert(K <= 16, "at most 16 sums");
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < K; q++) v[q] = warp_sum_d(v[q]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < K; q++) x.vred[q][wid] = v[q];
+  }
+  __syncthreads();
+  for (int q = wid; q < K; q += nw) {
+    double t = lane < nw ? x.vred[q][lane] : 0.0;
+    t = warp_sum_d(t);
+    if (lane == 0) x.bres[q] = t;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < K; q++) v[q] = x.bres[q];
+  __syncthreads();
+}
+
+// Sum of K doubles over the group (v: per-thread values, in/out).
+template <int K, int C>
+__device__ __forceinline__ void gsum_dv(const Grp<C>& g, double* v, GX& x) {
+  block_sum_dv<K>(v, x);
+  if constexpr (C > 1) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < K; q++) x.d[q] = v[q];
+    }
+    g.sync();
+    if (threadIdx.x < K) {
+      cg::cluster_group cl = cg::this_cluster();
+      double t = 0.0;
+#pragma unroll 1
+      for (int r = 0; r < C; r++) t += *cl.map_shared_rank(&x.d[threadIdx.x], r);
+      x.dres[threadIdx.x] = t;
+    }
+    g.sync();
+#pragma unroll
+    for (int q = 0; q < K; q++) v[q] = x.dres[q];
+  }
+}
+
+template <int C>
+__device__ __forceinline__ double gsum_d(const Grp<C>& g, double v, double* /*dred*/, GX& x) {
+  gsum_dv<1>(g, &v, x);
+  return v;
+}
+
+template <int C>
+__device__ __forceinline__ long long gsum_ll(const Grp<C>& g, long long v, long long* lred, GX& x) {
+  v = block_sum_ll(v, lred);
+  if constexpr (C > 1) {
+    if (threadIdx.x == 0) x.l[0] = v;
+    g.sync();
+    if (threadIdx.x == 0) {
+      cg::cluster_group cl = cg::this_cluster();
+      long long t = 0;
+#pragma unroll 1
+      for (int r = 0; r < C; r++) t += *cl.map_shared_rank(&x.l[0], r);
+      x.lres[0] = t;
+    }
+    g.sync();
+    v = x.lres[0];
+  }
+  return v;
+}
+
+// Minimum of K indices over the group (K <= 8).
+template <int K, int C>
+__device__ __forceinline__ void gmin_llv(const Grp<C>& g, long long* v, long long* lred, GX& x) {
+  static_assert(K <= 8, "at most 8 minima");
+#pragma unroll
+  for (int q = 0; q < K; q++) v[q] = block_min_ll(v[q], lred);
+  if constexpr (C > 1) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < K; q++) x.l[q] = v[q];
+    }
+    g.sync();
+    if (threadIdx.x < K) {
+      cg::cluster_group cl = cg::this_cluster();
+      long long t = LLONG_MAX;
+#pragma unroll 1
+      for (int r = 0; r < C; r++) {
+        long long w = *cl.map_shared_rank(&x.l[threadIdx.x], r);
+        t = w < t ? w : t;
+      }
+      x.lres[threadIdx.x] = t;
+    }
+    g.sync();
+#pragma unroll
+    for (int q = 0; q < K; q++) v[q] = x.lres[q];
+  }
+}
+
+template <int C>
+__device__ __forceinline__ long long gmin_ll(const Grp<C>& g, long long v, long long* lred, GX& x) {
+  gmin_llv<1>(g, &v, lred, x);
+  return v;
+}
+
+template <int C>
+__device__ __forceinline__ float gmax_f(const Grp<C>& g, float v, float* fred, GX& x) {
+  v = block_max_f(v, fred);
+  if constexpr (C > 1) {
+    if (threadIdx.x == 0) x.f[0] = v;
+    g.sync();
+    if (threadIdx.x == 0) {
+      cg::cluster_group cl = cg::this_cluster();
+      float t = -INFINITY;
+#pragma unroll 1
+      for (int r = 0; r < C; r++) t = fmaxf(t, *cl.map_shared_rank(&x.f[0], r));
+      x.fres[0] = t;
+    }
+    g.sync();
+    v = x.fres[0];
+  }
+  return v;
+}
+
+template <int C>
+__device__ __forceinline__ float gmin_f(const Grp<C>& g, float v, float* fred, GX& x) {
+  return -gmax_f(g, -v, fred, x);
+}
+
+// Exclusive prefix (over ranks, in rank order) and total of one value per
+// CTA (v: the CTA's value, the same in all its threads).
+template <int C>
+__device__ __forceinline__ void gexcl_d(const Grp<C>& g, double v, double* off, double* tot, GX& x) {
+  if constexpr (C == 1) {
+    *off = 0.0;
+    *tot = v;
+  } else {
+    if (threadIdx.x == 0) x.d[0] = v;
+    g.sync();
+    if (threadIdx.x == 0) {
+      cg::cluster_group cl = cg::this_cluster();
+      double o = 0.0, t = 0.0;
+      unsigned me = g.rank();
+#pragma unroll 1
+      for (unsigned r = 0; r < (unsigned)C; r++) {
+        double w = *cl.map_shared_rank(&x.d[0], r);
+        if (r == me) o = t;
+        t += w;
+      }
+      x.dres[0] = o;
+      x.dres[1] = t;
+    }
+    g.sync();
+    *off = x.dres[0];
+    *tot = x.dres[1];
+  }
+}
+
+template <int C>
+__device__ __forceinline__ void gexcl_ll(const Grp<C>& g, long long v, long long* off, long long* tot, GX& x) {
+  if constexpr (C == 1) {
+    *off = 0;
+    *tot = v;
+  } else {
+    if (threadIdx.x == 0) x.l[0] = v;
+    g.sync();
+    if (threadIdx.x == 0) {
+      cg::cluster_group cl = cg::this_cluster();
+      long long o = 0, t = 0;
+      unsigned me = g.rank();
+#pragma unroll 1
+      for (unsigned r = 0; r < (unsigned)C; r++) {
+        long long w = *cl.map_shared_rank(&x.l[0], r);
+        if (r == me) o = t;
+        t += w;
+      }
+      x.lres[0] = o;
+      x.lres[1] = t;
+    }
+    g.sync();
+    *off = x.lres[0];
+    *tot = x.lres[1];
+  }
+}
 
 struct Store {
   const float *x, *y, *z, *vx, *vy, *vz, *m;
@@ -62,15 +296,16 @@ __device__ __forceinline__ int col_index(float v, float xl, float cdx, int n) {
 // of (cx, cy, cz) (a superset of any open-cube or sphere test of radius r).
 // Warps take columns round-robin; lanes stride the binary-searched x range.
 template <class F>
-__device__ __forceinline__ void query_box(const ColIdx& ci, float cx, float cy, float cz, float r, F&& f) {
+__device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy, float cz, float r, int w0, int nw,
+                                           F&& f) {
   float rr = r * 1.0001f + 1e-6f;
   int iy0 = col_index(cy - rr, ci.xl, ci.cdx, ci.ncol), iy1 = col_index(cy + rr, ci.xl, ci.cdx, ci.ncol);
   int iz0 = col_index(cz - rr, ci.xl, ci.cdx, ci.ncol), iz1 = col_index(cz + rr, ci.xl, ci.cdx, ci.ncol);
   float xlo = cx - rr, xhi = cx + rr;
   int ny = iy1 - iy0 + 1;
   int ncols = ny * (iz1 - iz0 + 1);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int c = wid; c < ncols; c += nw) {
+  int lane = threadIdx.x & 31;
+  for (int c = w0; c < ncols; c += nw) {
     int64_t cid = (int64_t)(iz0 + c / ny) * ci.ncol + iy0 + c % ny;
     int64_t s = 0, e = 0;
     if (lane == 0) {
@@ -94,6 +329,17 @@ __device__ __forceinline__ void query_box(const ColIdx& ci, float cx, float cy, 
   }
 }
 
+template <class F>
+__device__ __forceinline__ void query_box(const ColIdx& ci, float cx, float cy, float cz, float r, F&& f) {
+  query_box_w(ci, cx, cy, cz, r, threadIdx.x >> 5, blockDim.x >> 5, f);
+}
+
+template <int C, class F>
+__device__ __forceinline__ void gquery_box(const Grp<C>& g, const ColIdx& ci, float cx, float cy, float cz,
+                                           float r, F&& f) {
+  query_box_w(ci, cx, cy, cz, r, g.warp0(), g.nwarps(), f);
+}
+
 __device__ __forceinline__ int ppos(const float4& e) { return __float_as_int(e.w); }
 
 // Open cube of haloes_particles.f:405-407.
@@ -115,14 +361,16 @@ struct RecShared {
   float fred[32];
   long long lred[32];
   int best;
+  GX x;
 };
 
 // RECENTER_DENSITY_PEAK_PARTICLES (haloes_particles.f:367-574).  The member
 // list of each shrink step is the first cube intersected with every later
 // cube, so each step re-reads the first cube from the column index instead
 // of storing the list.  Returns false if the shrink history overflows.
-static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* pcx, float* pcy, float* pcz,
-                               float R, float dxpamin, RecShared& sh) {
+template <int C>
+__device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci, float* pcx, float* pcy,
+                               float* pcz, float R, float dxpamin, RecShared& sh) {
   float cx = *pcx, cy = *pcy, cz = *pcz;
   float radio = fmaxf(__fmul_rn(0.05f, R), dxpamin);
   int64_t lo, hi;
@@ -132,7 +380,7 @@ static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* p
     slab_range(ci, cx, radio, &lo, &hi);
     long long c = 0;
     float mx = -1.e30f, mn = 1.e30f;
-    query_box(ci, cx, cy, cz, radio, [&](const float4& e) {
+    gquery_box(g, ci, cx, cy, cz, radio, [&](const float4& e) {
       int p = ppos(e);
       if (p >= lo && p < hi && in_cube(e.x, e.y, e.z, cx, cy, cz, radio)) {
         c++;
@@ -141,9 +389,9 @@ static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* p
         mn = fminf(mn, mp);
       }
     });
-    cnt = block_sum_ll(c, sh.lred);
-    maxm = block_max_f(mx, sh.fred);
-    minm = block_min_f(mn, sh.fred);
+    cnt = gsum_ll(g, c, sh.lred, sh.x);
+    maxm = gmax_f(g, mx, sh.fred, sh.x);
+    minm = gmin_f(g, mn, sh.fred, sh.x);
     if (cnt > 32) break;
     radio = __fmul_rn(radio, 1.2f);
     if (it > 10000) return false;
@@ -157,15 +405,15 @@ static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* p
   auto member = [&](const float4& e, int upto) -> bool {
     int p = ppos(e);
     if (!(p >= lo0 && p < hi0 && in_cube(e.x, e.y, e.z, c0x, c0y, c0z, r0))) return false;
-    for (int h = 0; h < upto; h++)
-      if (!in_cube(e.x, e.y, e.z, sh.hist[h][0], sh.hist[h][1], sh.hist[h][2], sh.hist[h][3])) return false;
+    for (int hh = 0; hh < upto; hh++)
+      if (!in_cube(e.x, e.y, e.z, sh.hist[hh][0], sh.hist[hh][1], sh.hist[hh][2], sh.hist[hh][3])) return false;
     return true;
   };
   for (;;) {
     for (int q = threadIdx.x; q < 64; q += blockDim.x) sh.dens[q] = 0.0;
     __syncthreads();
     bool ngp = __fdiv_rn(maxm, minm) < 8.0f;
-    query_box(ci, c0x, c0y, c0z, r0, [&](const float4& e) {
+    gquery_box(g, ci, c0x, c0y, c0z, r0, [&](const float4& e) {
       if (!member(e, nh)) return;
       int p = ppos(e);
       float mp = S.m[p];
@@ -208,6 +456,16 @@ static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* p
       }
     });
     __syncthreads();
+    if constexpr (C > 1) {  // sum the 4^3 grids of the cluster
+      g.sync();
+      cg::cluster_group cl = cg::this_cluster();
+      double t = 0.0;
+      if (threadIdx.x < 64)
+        for (int r = 0; r < C; r++) t += *cl.map_shared_rank(&sh.dens[threadIdx.x], r);
+      g.sync();
+      if (threadIdx.x < 64) sh.dens[threadIdx.x] = t;
+      __syncthreads();
+    }
     if (threadIdx.x == 0) {  // MAXLOC: first maximum, column-major
       int b = 0;
       for (int q = 1; q < 64; q++)
@@ -233,7 +491,7 @@ static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* p
     nh++;
     long long c = 0;
     float mx = -1.e30f, mn = 1.e30f;
-    query_box(ci, c0x, c0y, c0z, r0, [&](const float4& e) {
+    gquery_box(g, ci, c0x, c0y, c0z, r0, [&](const float4& e) {
       if (member(e, nh)) {
         c++;
         float mp = S.m[ppos(e)];
@@ -241,28 +499,25 @@ static __device__ bool recenter_block(const Store& S, const ColIdx& ci, float* p
         mn = fminf(mn, mp);
       }
     });
-    cnt = block_sum_ll(c, sh.lred);
-    maxm = block_max_f(mx, sh.fred);
-    minm = block_min_f(mn, sh.fred);
+    cnt = gsum_ll(g, c, sh.lred, sh.x);
+    maxm = gmax_f(g, mx, sh.fred, sh.x);
+    minm = gmin_f(g, mn, sh.fred, sh.x);
     if (cnt < 32) break;
   }
-  double bs = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
-  query_box(ci, c0x, c0y, c0z, r0, [&](const float4& e) {
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  gquery_box(g, ci, c0x, c0y, c0z, r0, [&](const float4& e) {
     if (member(e, nh)) {
       float mp = S.m[ppos(e)];
-      bs += (double)mp;
-      bx += (double)__fmul_rn(e.x, mp);
-      by += (double)__fmul_rn(e.y, mp);
-      bz += (double)__fmul_rn(e.z, mp);
+      v[0] += (double)mp;
+      v[1] += (double)__fmul_rn(e.x, mp);
+      v[2] += (double)__fmul_rn(e.y, mp);
+      v[3] += (double)__fmul_rn(e.z, mp);
     }
   });
-  bs = block_sum_d(bs, sh.dred);
-  bx = block_sum_d(bx, sh.dred);
-  by = block_sum_d(by, sh.dred);
-  bz = block_sum_d(bz, sh.dred);
-  *pcx = (float)(bx / bs);
-  *pcy = (float)(by / bs);
-  *pcz = (float)(bz / bs);
+  gsum_dv<4>(g, v, sh.x);
+  *pcx = (float)(v[1] / v[0]);
+  *pcy = (float)(v[2] / v[0]);
+  *pcz = (float)(v[3] / v[0]);
   return true;
 }
 
@@ -295,4 +550,24 @@ __device__ __forceinline__ double tile_prefix_d(int64_t a, int64_t b, double car
     carry += tot;
   }
   return carry;
+}
+
+// Inclusive prefix over [a, b) split across the group: each CTA scans its
+// chunk after adding the totals of the chunks before it.  Returns
+// carry + total.  With C > 1 `val` is evaluated twice per element.
+template <int C, class V, class U>
+__device__ __forceinline__ double gprefix_d(const Grp<C>& g, int64_t a, int64_t b, double carry, V val, U use,
+                                            double* sbuf, GX& x) {
+  int64_t lo, hi;
+  g.chunk(a, b, &lo, &hi);
+  if constexpr (C == 1) {
+    return tile_prefix_d(lo, hi, carry, val, use, sbuf);
+  } else {
+    double part = tile_prefix_d(lo, hi, 0.0, val, [](int64_t, double) {}, sbuf);
+    double off, tot;
+    gexcl_d(g, part, &off, &tot, x);
+    tile_prefix_d(lo, hi, carry + off, val, use, sbuf);
+    g.sync();
+    return carry + tot;
+  }
 }

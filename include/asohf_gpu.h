@@ -50,6 +50,11 @@ int asohf_kernel_stats(asohf_ctx *ctx, int i, const char **name, double *total_m
  * element-passes of the halo kernel, 1: of the subhalo kernel), optionally
  * reset after reading. */
 int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
+/* Tuning, no counterpart in the reference: haloes with at least
+ * min_members members are refined by a thread-block cluster, the others by
+ * one CTA each (results are the same either way).  0 restores the default
+ * (32768); 1 sends every halo to the cluster path. */
+int asohf_set_cluster_threshold(asohf_ctx *ctx, int64_t min_members);
 
 /* MODULE PARTICLES (particles.f:1-14) / READ_AND_ALLOC_PARTICLES
  * (alloc.f:196-528): copies the particle arrays into the device store,

@@ -42,10 +42,13 @@ def compare(rg, ro, rtol=1e-5):
     assert np.array_equal(rg.pph, ro.pph)
 
 
-@pytest.mark.parametrize("name", ["tiny", "small"])
-def test_halofind_matches_oracle(gpu_lib, name):
+@pytest.mark.parametrize("name,cluster_min", [("tiny", 0), ("small", 0), ("tiny", 1), ("small", 1),
+                                              ("small", 300)])
+def test_halofind_matches_oracle(gpu_lib, name, cluster_min):
+    """cluster_min 1 sends every halo through the thread-block-cluster
+    kernels, 300 splits the haloes between the two tiers."""
     s = synth.generate(name)
-    rg = driver.run(s, api.GpuBackend(), with_subs=False)
+    rg = driver.run(s, api.GpuBackend(cluster_threshold=cluster_min), with_subs=False)
     ro = driver.run(s, O.OracleBackend(), with_subs=False)
     assert (ro.cat.realclus[: ro.cat.nclus] != 0).sum() > 0
     compare(rg, ro)
