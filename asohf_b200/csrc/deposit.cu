@@ -2,15 +2,15 @@
 // the true-TSC deposit (INTERPOLATE_DENSITY_TSC) on sm_100a.
 //
 // Accumulation: every cloud term keeps the reference's REAL*4 expression
-// (BAS*W(i)*W(j)*W(k), left to right).  Terms are summed exactly where the
-// dynamic range allows -- 64-bit fixed point for the base-grid kernel
-// deposit, whose weights are dyadic -- and otherwise in float64, then
-// rounded once to float32.  The result no longer depends on the particle
-// order or thread count, unlike the reference's REDUCTION(+:U1)
+// (BAS*W(i)*W(j)*W(k), left to right).  Terms are summed in float64 and
+// rounded once to float32, so the result depends on the particle order only
+// through float64 rounding, unlike the reference's REDUCTION(+:U1)
 // (grids.f:787-791) whose float32 sum does.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include <algorithm>
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -292,67 +292,33 @@ extern "C" int asohf_sort_dm_particles_localdensity(asohf_ctx* c, int nx, float 
 }
 
 // ------------------------------------------------------------ base deposit
-// Fixed point: every REAL*4 cloud term t is an integer multiple of
-// 2^fx_shift (fx_shift = exponent of the smallest term - 24), summed in
-// 64-bit integers.  The host checks the worst-case sum fits.
-__global__ void k_density_base_fixed(const float* __restrict__ x, const float* __restrict__ y,
-                                     const float* __restrict__ z, const float* __restrict__ m,
-                                     int64_t n, int nx, float xl, float dx, const float* __restrict__ k0,
-                                     double inv_unit, unsigned long long* __restrict__ acc) {
-  float w[3] = {k0[0], k0[1], k0[2]};
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    float bas = m[i];
-    int ix = (int)((x[i] - xl) / dx) + 1;
-    int jy = (int)((y[i] - xl) / dx) + 1;
-    int kz = (int)((z[i] - xl) / dx) + 1;
-#pragma unroll
-    for (int kk = -1; kk <= 1; kk++) {
-      int k1 = kz + kk;
-      if (k1 > nx) k1 -= nx;
-      if (k1 < 1) k1 += nx;
-#pragma unroll
-      for (int jj = -1; jj <= 1; jj++) {
-        int j1 = jy + jj;
-        if (j1 > nx) j1 -= nx;
-        if (j1 < 1) j1 += nx;
-#pragma unroll
-        for (int ii = -1; ii <= 1; ii++) {
-          int i1 = ix + ii;
-          if (i1 > nx) i1 -= nx;
-          if (i1 < 1) i1 += nx;
-          if (i1 < 1 || i1 > nx || j1 < 1 || j1 > nx || k1 < 1 || k1 > nx) continue;  // outside the box
-          float t = __fmul_rn(__fmul_rn(__fmul_rn(bas, w[ii + 1]), w[jj + 1]), w[kk + 1]);
-          unsigned long long q = (unsigned long long)__double2ll_rn(__dmul_rn((double)t, inv_unit));
-          size_t c = ((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1);
-          atomicAdd(&acc[c], q);
-        }
-      }
-    }
-  }
+// The 27-cell periodic cloud of grids.f:787-820 for particles whose host
+// cell lies in the box; BASE_OUTLIER handles the rest (positions more than
+// one cell outside the box), with the same wrap-once arithmetic.
+__device__ __forceinline__ int wrap_once(int i, int nx) {
+  if (i > nx) i -= nx;
+  if (i < 1) i += nx;
+  return i;
 }
 
-__global__ void k_density_base_f64(const float* __restrict__ x, const float* __restrict__ y,
-                                   const float* __restrict__ z, const float* __restrict__ m,
-                                   int64_t n, int nx, float xl, float dx, const float* __restrict__ k0,
-                                   double* __restrict__ acc) {
+// Particles whose host cell lies outside the box, summed into the float64
+// grid the tile kernel wrote.
+__global__ void k_density_base_outliers(const float* __restrict__ x, const float* __restrict__ y,
+                                        const float* __restrict__ z, const float* __restrict__ m, int64_t n,
+                                        int nx, float xl, float dx, const float* __restrict__ k0,
+                                        double* __restrict__ acc) {
   float w[3] = {k0[0], k0[1], k0[2]};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    float bas = m[i];
     int ix = (int)((x[i] - xl) / dx) + 1;
     int jy = (int)((y[i] - xl) / dx) + 1;
     int kz = (int)((z[i] - xl) / dx) + 1;
+    if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx) continue;
+    float bas = m[i];
     for (int kk = -1; kk <= 1; kk++)
       for (int jj = -1; jj <= 1; jj++)
         for (int ii = -1; ii <= 1; ii++) {
-          int i1 = ix + ii, j1 = jy + jj, k1 = kz + kk;
-          if (i1 > nx) i1 -= nx;
-          if (i1 < 1) i1 += nx;
-          if (j1 > nx) j1 -= nx;
-          if (j1 < 1) j1 += nx;
-          if (k1 > nx) k1 -= nx;
-          if (k1 < 1) k1 += nx;
+          int i1 = wrap_once(ix + ii, nx), j1 = wrap_once(jy + jj, nx), k1 = wrap_once(kz + kk, nx);
           if (i1 < 1 || i1 > nx || j1 < 1 || j1 > nx || k1 < 1 || k1 > nx) continue;  // outside the box
           float t = __fmul_rn(__fmul_rn(__fmul_rn(bas, w[ii + 1]), w[jj + 1]), w[kk + 1]);
           atomicAdd(&acc[((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1)], (double)t);
@@ -360,12 +326,25 @@ __global__ void k_density_base_f64(const float* __restrict__ x, const float* __r
   }
 }
 
-__global__ void k_finish_fixed(const unsigned long long* __restrict__ acc, int64_t g, double unit,
-                               float denbas, float* __restrict__ u1) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
-       c += (int64_t)gridDim.x * blockDim.x) {
-    float v = (float)((double)(long long)acc[c] * unit);
-    u1[c] = v / denbas;
+// Every particle with global float64 atomics (grids smaller than one tile).
+__global__ void k_density_base_all(const float* __restrict__ x, const float* __restrict__ y,
+                                   const float* __restrict__ z, const float* __restrict__ m, int64_t n, int nx,
+                                   float xl, float dx, const float* __restrict__ k0, double* __restrict__ acc) {
+  float w[3] = {k0[0], k0[1], k0[2]};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int ix = (int)((x[i] - xl) / dx) + 1;
+    int jy = (int)((y[i] - xl) / dx) + 1;
+    int kz = (int)((z[i] - xl) / dx) + 1;
+    float bas = m[i];
+    for (int kk = -1; kk <= 1; kk++)
+      for (int jj = -1; jj <= 1; jj++)
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = wrap_once(ix + ii, nx), j1 = wrap_once(jy + jj, nx), k1 = wrap_once(kz + kk, nx);
+          if (i1 < 1 || i1 > nx || j1 < 1 || j1 > nx || k1 < 1 || k1 > nx) continue;  // outside the box
+          float t = __fmul_rn(__fmul_rn(__fmul_rn(bas, w[ii + 1]), w[jj + 1]), w[kk + 1]);
+          atomicAdd(&acc[((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1)], (double)t);
+        }
   }
 }
 
@@ -495,132 +474,359 @@ static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d) {
   return ASOHF_OK;
 }
 
-// ------------------------------------------------------------ patch deposit
-// One CTA per (patch, z-half): the 32x32x16 float64 accumulator lives in
-// shared memory; candidate particles come from the bins that overlap the
-// patch box extended by MAXKERNELEXT = DX (grids.f:837-893); their clipped
-// clouds are flattened into one work list so all threads share the cells.
-#define PD_BLOCK 512
-#define PD_BATCH 512
+// ------------------------------------------------------------ staging
+// The store in bin order as float4 (x, y, z, m) plus the species index, so
+// a patch reads its candidates as contiguous runs (one run per (y, z) row of
+// bins).
 #define NA ASOHF_NAMRX
 #define ZH (NA / 2)
+#define PD_BLOCK 512
 
-struct PatchWork {
-  int n;
-  float m;
-  int ix, jy, kz, lev;     // host cell and kernel level
-  int i1, j1, k1, di, dj;  // clipped cloud origin and extents
-  int vol;
-};
-
-__global__ void __launch_bounds__(PD_BLOCK)
-k_density_patches(DevMesh M, Bins B, const float* __restrict__ x, const float* __restrict__ y,
-                  const float* __restrict__ z, const float* __restrict__ m,
-                  const int64_t* __restrict__ esp_end /* N_ESP cumulative */, float dx,
-                  const float* __restrict__ kernels, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
-  extern __shared__ double acc[];  // NA*NA*ZH
-  __shared__ int s_vol[PD_BATCH + 1];
-  __shared__ PatchWork s_w[PD_BATCH];
-  __shared__ int s_nw;
-  __shared__ int s_scan[33];
-  int ip = blockIdx.x >> 1, half = blockIdx.x & 1;
-  int n1 = M.nx[ip], n2 = M.ny[ip], n3 = M.nz[ip], ir = M.level[ip];
-  int zlo = half * ZH + 1, zhi = min(half * ZH + ZH, n3);
-  for (int q = threadIdx.x; q < NA * NA * ZH; q += blockDim.x) acc[q] = 0.0;
-  float dxpa = dx / exp2f((float)ir);
-  float xlfix = M.rx[ip] - dxpa, ylfix = M.ry[ip] - dxpa, zlfix = M.rz[ip] - dxpa;
-  float pxl = xlfix - dx, pyl = ylfix - dx, pzl = zlfix - dx;
-  float pxr = (xlfix + (float)n1 * dxpa) + dx, pyr = (ylfix + (float)n2 * dxpa) + dx,
-        pzr = (zlfix + (float)n3 * dxpa) + dx;
-  __syncthreads();
-  if (zlo <= zhi) {
-    int bx0 = bin_of(pxl, B.xl, B.bsz, B.nb), bx1 = bin_of(pxr, B.xl, B.bsz, B.nb);
-    int by0 = bin_of(pyl, B.xl, B.bsz, B.nb), by1 = bin_of(pyr, B.xl, B.bsz, B.nb);
-    int bz0 = bin_of(pzl, B.xl, B.bsz, B.nb), bz1 = bin_of(pzr, B.xl, B.bsz, B.nb);
-    for (int bz = bz0; bz <= bz1; bz++)
-      for (int by = by0; by <= by1; by++) {
-        int b0 = (bz * B.nb + by) * B.nb + bx0, b1 = (bz * B.nb + by) * B.nb + bx1;
-        int lo = B.start[b0], hi = B.start[b1 + 1];
-        for (int base = lo; base < hi; base += PD_BATCH) {
-          // 1. candidate particles of this batch -> work items
-          if (threadIdx.x == 0) s_nw = 0;
-          __syncthreads();
-          for (int t = threadIdx.x; t < PD_BATCH && base + t < hi; t += blockDim.x) {
-            int p = B.idx[base + t];
-            float xp = x[p], yp = y[p], zp = z[p];
-            if (!(pxl < xp && xp < pxr && pyl < yp && yp < pyr && pzl < zp && zp < pzr)) continue;
-            int s = 0;
-            while (s < ASOHF_N_ESP - 1 && (int64_t)p >= esp_end[s]) s++;
-            int lev = ir - s;
-            if (lev < 0) lev = 0;
-            int nk = 1 << lev;
-            int ix = (int)floorf((xp - xlfix) / dxpa) + 1;
-            int jy = (int)floorf((yp - ylfix) / dxpa) + 1;
-            int kz = (int)floorf((zp - zlfix) / dxpa) + 1;
-            int i1 = ix - nk, i2 = ix + nk, j1 = jy - nk, j2 = jy + nk, k1 = kz - nk, k2 = kz + nk;
-            if (i1 > n1 || i2 < 1 || j1 > n2 || j2 < 1 || k1 > n3 || j2 < 1) continue;
-            if (i1 < 1) i1 = 1;
-            if (i2 > n1) i2 = n1;
-            if (j1 < 1) j1 = 1;
-            if (j2 > n2) j2 = n2;
-            if (k1 < 1) k1 = 1;
-            if (k2 > n3) k2 = n3;
-            if (k1 < zlo) k1 = zlo;
-            if (k2 > zhi) k2 = zhi;
-            if (k1 > k2) continue;
-            int slot = atomicAdd(&s_nw, 1);
-            PatchWork w;
-            w.m = m[p];
-            w.ix = ix; w.jy = jy; w.kz = kz; w.lev = lev;
-            w.i1 = i1; w.j1 = j1; w.k1 = k1; w.di = i2 - i1 + 1; w.dj = j2 - j1 + 1;
-            w.vol = w.di * w.dj * (k2 - k1 + 1);
-            s_w[slot] = w;
-          }
-          __syncthreads();
-          int nw = s_nw;
-          // 2. prefix of volumes
-          int v = threadIdx.x < nw ? s_w[threadIdx.x].vol : 0;
-          int tot;
-          int inc = block_scan_i(v, s_scan, &tot);
-          if (threadIdx.x < nw) s_vol[threadIdx.x + 1] = inc;
-          if (threadIdx.x == 0) s_vol[0] = 0;
-          __syncthreads();
-          // 3. flattened cells
-          for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-            int lo2 = 0, hi2 = nw - 1;
-            while (lo2 < hi2) {
-              int mid = (lo2 + hi2 + 1) >> 1;
-              if (s_vol[mid] <= f) lo2 = mid; else hi2 = mid - 1;
-            }
-            const PatchWork& w = s_w[lo2];
-            int r = f - s_vol[lo2];
-            int ii = w.i1 + r % w.di;
-            int jj = w.j1 + (r / w.di) % w.dj;
-            int kk = w.k1 + r / (w.di * w.dj);
-            const float* kern = kernels + (size_t)w.lev * KW + ASOHF_NMAX_KERNELS;
-            float t = __fmul_rn(__fmul_rn(__fmul_rn(w.m, kern[ii - w.ix]), kern[jj - w.jy]), kern[kk - w.kz]);
-            atomicAdd(&acc[((kk - zlo) * NA + (jj - 1)) * NA + (ii - 1)], (double)t);
-          }
-          __syncthreads();
-        }
-      }
-  }
-  __syncthreads();
-  float den = denbas_lev[ir];
-  float* out = u11 + (size_t)ip * NA * NA * NA;
-  for (int q = threadIdx.x; q < NA * NA * ZH; q += blockDim.x) {
-    int i = q % NA, j = (q / NA) % NA, kl = q / (NA * NA);
-    int k = half * ZH + kl;
-    float v = 0.0f;
-    if (i < n1 && j < n2 && k < n3) v = (float)acc[q] / den;
-    out[((size_t)k * NA + j) * NA + i] = v;
+__global__ void k_bin_stage(const int32_t* __restrict__ idx, int64_t n, int64_t ndep, const float* __restrict__ x,
+                            const float* __restrict__ y, const float* __restrict__ z, const float* __restrict__ m,
+                            const int64_t* __restrict__ esp_end, float4* __restrict__ P, uint8_t* __restrict__ S) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    int p = idx[t];
+    P[t] = make_float4(x[p], y[p], z[p], m[p]);
+    int s = 0;
+    while (s < ASOHF_N_ESP - 1 && (int64_t)p >= esp_end[s]) s++;
+    S[t] = (int64_t)p < ndep ? (uint8_t)s : (uint8_t)255;  // 255: not deposited
   }
 }
 
-static int frexp_exp(double v) {
-  int e;
-  frexp(v, &e);
-  return e;  // v = f * 2^e, f in [0.5, 1)
+// ------------------------------------------------------------ base deposit, equal masses
+// With one particle mass every particle of a host cell deposits the same
+// 27 REAL*4 terms, so the grid is the 27-point stencil of the host-cell
+// counts: U1(c) = sum_o count(c - o) * t_o, each product exact in float64.
+__global__ void k_base_counts(const float* __restrict__ x, const float* __restrict__ y,
+                              const float* __restrict__ z, int64_t n, int nx, float xl, float dx,
+                              int32_t* __restrict__ cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int ix = (int)((x[i] - xl) / dx) + 1;
+    int jy = (int)((y[i] - xl) / dx) + 1;
+    int kz = (int)((z[i] - xl) / dx) + 1;
+    if (ix >= 1 && ix <= nx && jy >= 1 && jy <= nx && kz >= 1 && kz <= nx)
+      atomicAdd(&cnt[((int64_t)(kz - 1) * nx + (jy - 1)) * nx + (ix - 1)], 1);
+  }
+}
+
+struct Terms27 {
+  double t[27];  // t[(kk+1)*9 + (jj+1)*3 + (ii+1)] = ((m*W(ii))*W(jj))*W(kk) in REAL*4
+};
+
+__global__ void k_base_stencil(const int32_t* __restrict__ cnt, int nx, Terms27 T, double* __restrict__ acc) {
+  int64_t g = (int64_t)nx * nx * nx;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(c % nx) + 1, j = (int)((c / nx) % nx) + 1, k = (int)(c / ((int64_t)nx * nx)) + 1;
+    double s = 0.0;
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      int hk = wrap_once(k - kk, nx);
+#pragma unroll
+      for (int jj = -1; jj <= 1; jj++) {
+        int hj = wrap_once(j - jj, nx);
+        const int32_t* row = cnt + ((int64_t)(hk - 1) * nx + (hj - 1)) * nx;
+#pragma unroll
+        for (int ii = -1; ii <= 1; ii++) {
+          int hi = wrap_once(i - ii, nx);
+          int q = row[hi - 1];
+          if (q) s += (double)q * T.t[(kk + 1) * 9 + (jj + 1) * 3 + (ii + 1)];
+        }
+      }
+    }
+    acc[c] = s;
+  }
+}
+
+// ------------------------------------------------------------ patch deposit
+// Work unit: PZ z-planes of one patch, accumulated in float64 shared memory.
+// A unit's candidates are the particles of the bins that overlap the patch
+// box extended by MAXKERNELEXT = DX (grids.f:837-893), restricted in z to
+// the unit's planes +- DX; they are split into slices of PSLICE so that a
+// dense unit is shared by several CTAs, whose sums meet in a float64 scratch
+// slab.  Inside a CTA all warps stride over the unit's candidates as one
+// flat range.  A hit whose kernel level is 0 (27-cell cloud) is counted in
+// a host-cell grid when all masses are equal and spread by the 27-point
+// stencil at the end; every other hit deposits its clipped cloud with all 32
+// lanes of the warp, hits with the same host cell, level and mass once with
+// the group size as factor.
+#define PZ 4              // z planes per unit
+#define PZ_BLOCK 256
+#define NSLAB (NA / PZ)
+#define PSLICE 8192       // candidates per work item
+#define PROWS 128         // bin rows staged in shared memory at a time
+#define CGX (NA + 2)      // host-cell count grid: x, y in [0, NA+1]
+#define CGZ (PZ + 2)      //                       z in [zlo-1, zhi+1]
+
+// Offset of the centre of level l in the compact kernel table that stores
+// levels 0, 1, ... back to back (2*2^l+1 entries each).
+__host__ __device__ __forceinline__ int ktab_center(int l) { return 3 * (1 << l) - 2 + l; }
+__host__ __device__ __forceinline__ int ktab_size(int lmax) { return (1 << (lmax + 2)) - 1 + lmax; }
+
+struct UnitGeo {
+  int ip, slab, n1, n2, n3, ir, zlo, zhi;
+  float dxpa, xlfix, ylfix, zlfix, pxl, pyl, pzl, pxr, pyr, pzr;
+  int bx0, bx1, by0, by1, bz0, bz1, nby, rows;
+};
+
+__device__ __forceinline__ void unit_geo(const DevMesh& M, const Bins& B, const int32_t* order, int u, float dx,
+                                         UnitGeo& g) {
+  g.ip = order[u / NSLAB];
+  g.slab = u % NSLAB;
+  g.n1 = M.nx[g.ip]; g.n2 = M.ny[g.ip]; g.n3 = M.nz[g.ip]; g.ir = M.level[g.ip];
+  g.zlo = g.slab * PZ + 1;
+  g.zhi = min(g.slab * PZ + PZ, g.n3);
+  g.dxpa = dx / exp2f((float)g.ir);
+  g.xlfix = M.rx[g.ip] - g.dxpa; g.ylfix = M.ry[g.ip] - g.dxpa; g.zlfix = M.rz[g.ip] - g.dxpa;
+  g.pxl = g.xlfix - dx; g.pyl = g.ylfix - dx; g.pzl = g.zlfix - dx;
+  g.pxr = (g.xlfix + (float)g.n1 * g.dxpa) + dx;
+  g.pyr = (g.ylfix + (float)g.n2 * g.dxpa) + dx;
+  g.pzr = (g.zlfix + (float)g.n3 * g.dxpa) + dx;
+  g.bx0 = bin_of(g.pxl, B.xl, B.bsz, B.nb); g.bx1 = bin_of(g.pxr, B.xl, B.bsz, B.nb);
+  g.by0 = bin_of(g.pyl, B.xl, B.bsz, B.nb); g.by1 = bin_of(g.pyr, B.xl, B.bsz, B.nb);
+  // a cloud reaches at most 2^ir cells = DX from its host cell: planes
+  // zlo..zhi take hosts with z in [zlfix + (zlo-1) dxpa - DX, zlfix + zhi dxpa + DX]
+  float za = fmaxf(g.pzl, (g.zlfix + (float)(g.zlo - 1) * g.dxpa) - dx);
+  float zb = fminf(g.pzr, (g.zlfix + (float)g.zhi * g.dxpa) + dx);
+  g.bz0 = bin_of(za, B.xl, B.bsz, B.nb); g.bz1 = bin_of(zb, B.xl, B.bsz, B.nb);
+  g.nby = g.by1 - g.by0 + 1;
+  g.rows = (g.zlo > g.zhi) ? 0 : g.nby * (g.bz1 - g.bz0 + 1);
+}
+
+__device__ __forceinline__ void row_range(const Bins& B, const UnitGeo& g, int row, int* lo, int* len) {
+  int bz = g.bz0 + row / g.nby, by = g.by0 + row % g.nby;
+  int64_t rb = ((int64_t)bz * B.nb + by) * B.nb;
+  int a = B.start[rb + g.bx0], b = B.start[rb + g.bx1 + 1];
+  *lo = a;
+  *len = b - a;
+}
+
+// Candidates per unit (one warp per unit).
+__global__ void k_patch_unit_counts(DevMesh M, Bins B, const int32_t* __restrict__ order, int nunits, float dx,
+                                    int64_t* __restrict__ cnt) {
+  int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (u >= nunits) return;
+  UnitGeo g;
+  unit_geo(M, B, order, u, dx, g);
+  long long s = 0;
+  for (int r = lane; r < g.rows; r += 32) {
+    int lo, len;
+    row_range(B, g, r, &lo, &len);
+    s += len;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) cnt[u] = s;
+}
+
+struct PatchWork {
+  const int2* items;         // (unit, slice)
+  const int32_t* scratch_of; // per unit: scratch slab index, -1 for single-slice units
+  double* scratch;           // NA*NA*PZ doubles per multi-slice unit
+};
+
+__global__ void __launch_bounds__(PZ_BLOCK, 3)
+k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t* __restrict__ S,
+                  const int32_t* __restrict__ order, PatchWork W, float dx, const float* __restrict__ kernels,
+                  int eqmass, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
+  extern __shared__ double acc[];  // NA*NA*PZ doubles, count grid, kernel table
+  int32_t* scnt = (int32_t*)(acc + NA * NA * PZ);
+  float* ktab = (float*)(scnt + CGX * CGX * CGZ);
+  __shared__ int s_lo[PROWS], s_pre[PROWS + 1];
+  __shared__ double s_t27[27];
+  const int2 it = W.items[blockIdx.x];
+  UnitGeo g;
+  unit_geo(M, B, order, it.x, dx, g);
+  float* out = u11 + (size_t)g.ip * NA * NA * NA + (size_t)g.slab * PZ * NA * NA;
+  if (g.zlo > g.zhi) {  // planes past the patch
+    for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) out[q] = 0.0f;
+    return;
+  }
+  for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) acc[q] = 0.0;
+  for (int q = threadIdx.x; q < CGX * CGX * CGZ; q += blockDim.x) scnt[q] = 0;
+  for (int l = 0; l <= g.ir; l++) {
+    int nk = 1 << l, c0 = ktab_center(l);
+    for (int i = threadIdx.x - nk; i <= nk; i += blockDim.x)
+      ktab[c0 + i] = kernels[(size_t)l * KW + ASOHF_NMAX_KERNELS + i];
+  }
+  __syncthreads();
+  if (eqmass && threadIdx.x < 27) {  // level-0 terms of the common mass
+    const float* kc = ktab + ktab_center(0);
+    float m0 = P[0].w;  // any staged particle: all masses are equal
+    int a = threadIdx.x % 3 - 1, b = (threadIdx.x / 3) % 3 - 1, cc = threadIdx.x / 9 - 1;
+    s_t27[threadIdx.x] = (double)__fmul_rn(__fmul_rn(__fmul_rn(m0, kc[a]), kc[b]), kc[cc]);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int64_t v0 = (int64_t)it.y * PSLICE, v1 = v0 + PSLICE;
+  int64_t vbase = 0;
+  for (int r0 = 0; r0 < g.rows; r0 += PROWS) {
+    int nr = min(PROWS, g.rows - r0);
+    __syncthreads();
+    if (threadIdx.x < nr) {
+      int lo, len;
+      row_range(B, g, r0 + threadIdx.x, &lo, &len);
+      s_lo[threadIdx.x] = lo;
+      s_pre[threadIdx.x + 1] = len;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_pre[0] = 0;
+      for (int r = 1; r <= nr; r++) s_pre[r] += s_pre[r - 1];
+    }
+    __syncthreads();
+    const int64_t tot = s_pre[nr];
+    const int64_t a = max(v0, vbase) - vbase, b = min(v1, vbase + tot) - vbase;
+    for (int64_t cbase = a + (int64_t)warp * 32; cbase < b; cbase += (int64_t)nwarp * 32) {
+      int64_t v = cbase + lane;
+      bool hit = false;
+      float mp = 0.f;
+      int ix = 0, jy = 0, kz = 0, lev = 0, i1 = 0, j1 = 0, k1 = 0, di = 0, dj = 0, vol = 0;
+      if (v < b) {
+        int lo2 = 0, hi2 = nr - 1;  // row of v: last r with s_pre[r] <= v
+        while (lo2 < hi2) {
+          int mid = (lo2 + hi2 + 1) >> 1;
+          if (s_pre[mid] <= v) lo2 = mid; else hi2 = mid - 1;
+        }
+        int e = s_lo[lo2] + (int)(v - s_pre[lo2]);
+        int s = S[e];
+        float4 q = P[e];
+        if (s != 255 && g.pxl < q.x && q.x < g.pxr && g.pyl < q.y && q.y < g.pyr && g.pzl < q.z && q.z < g.pzr) {
+          lev = g.ir - s;
+          if (lev < 0) lev = 0;
+          int nk = 1 << lev;
+          ix = (int)floorf((q.x - g.xlfix) / g.dxpa) + 1;
+          jy = (int)floorf((q.y - g.ylfix) / g.dxpa) + 1;
+          kz = (int)floorf((q.z - g.zlfix) / g.dxpa) + 1;
+          int i2 = ix + nk, j2 = jy + nk, k2 = kz + nk;
+          i1 = ix - nk; j1 = jy - nk; k1 = kz - nk;
+          if (!(i1 > g.n1 || i2 < 1 || j1 > g.n2 || j2 < 1 || k1 > g.n3 || k2 < 1)) {
+            i1 = max(i1, 1); i2 = min(i2, g.n1);
+            j1 = max(j1, 1); j2 = min(j2, g.n2);
+            k1 = max(max(k1, 1), g.zlo); k2 = min(min(k2, g.n3), g.zhi);
+            if (k1 <= k2) {
+              mp = q.w;
+              if (eqmass && lev == 0) {  // host cell count (ix in [0, n1+1], kz in [zlo-1, zhi+1])
+                atomicAdd(&scnt[((kz - g.zlo + 1) * CGX + jy) * CGX + ix], 1);
+              } else {
+                hit = true;
+                di = i2 - i1 + 1;
+                dj = j2 - j1 + 1;
+                vol = di * dj * (k2 - k1 + 1);
+              }
+            }
+          }
+        }
+      }
+      unsigned long long key =
+          hit ? ((unsigned long long)(ix + 1024) << 52) | ((unsigned long long)(jy + 1024) << 41) |
+                    ((unsigned long long)(kz + 1024) << 30) | ((unsigned long long)lev << 26) |
+                    (unsigned long long)(__float_as_uint(mp) >> 6)
+              : ~0ull - (unsigned long long)lane;
+      unsigned grp = __match_any_sync(0xffffffffu, key);
+      if (hit) {  // the key keeps 26 bits of the mass: confirm equal masses inside the group
+        float m0 = __shfl_sync(grp, mp, __ffs(grp) - 1);
+        unsigned same = __ballot_sync(grp, mp == m0);
+        if (same != grp) grp = 1u << lane;
+      }
+      float gcnt = (float)__popc(grp);
+      unsigned hm = __ballot_sync(0xffffffffu, hit && lane == __ffs(grp) - 1);
+      while (hm) {
+        int src = __ffs(hm) - 1;
+        hm &= hm - 1;
+        float wm = __shfl_sync(0xffffffffu, mp, src);
+        double wc = (double)__shfl_sync(0xffffffffu, gcnt, src);
+        int wix = __shfl_sync(0xffffffffu, ix, src), wjy = __shfl_sync(0xffffffffu, jy, src);
+        int wkz = __shfl_sync(0xffffffffu, kz, src), wlev = __shfl_sync(0xffffffffu, lev, src);
+        int wi1 = __shfl_sync(0xffffffffu, i1, src), wj1 = __shfl_sync(0xffffffffu, j1, src);
+        int wk1 = __shfl_sync(0xffffffffu, k1, src), wdi = __shfl_sync(0xffffffffu, di, src);
+        int wdj = __shfl_sync(0xffffffffu, dj, src), wvol = __shfl_sync(0xffffffffu, vol, src);
+        const float* kc = ktab + ktab_center(wlev);
+        // cell f of the clipped cloud: f = (kk-k1)*di*dj + (jj-j1)*di + (ii-i1); the
+        // quotients are exact in float (f < 2^13, divisors <= 32)
+        float rdi = 1.0f / (float)wdi, rdj = 1.0f / (float)wdj;
+        for (int f = lane; f < wvol; f += 32) {
+          int qa = (int)(((float)f + 0.5f) * rdi);
+          int ii = wi1 + (f - qa * wdi);
+          int qb = (int)(((float)qa + 0.5f) * rdj);
+          int jj = wj1 + (qa - qb * wdj);
+          int kk = wk1 + qb;
+          float tt = __fmul_rn(__fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]), kc[kk - wkz]);
+          atomicAdd(&acc[((kk - g.zlo) * NA + (jj - 1)) * NA + (ii - 1)], (double)tt * wc);
+        }
+      }
+    }
+    vbase += tot;
+  }
+  __syncthreads();
+  // level-0 hosts: 27-point stencil of the counts (cells inside the patch)
+  if (eqmass) {
+    for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
+      int i = q % NA + 1, j = (q / NA) % NA + 1, k = g.zlo + q / (NA * NA);
+      if (i > g.n1 || j > g.n2 || k > g.zhi) continue;
+      double s = 0.0;
+      for (int kk = -1; kk <= 1; kk++)
+        for (int jj = -1; jj <= 1; jj++)
+          for (int ii = -1; ii <= 1; ii++) {
+            int c = scnt[((k - kk - g.zlo + 1) * CGX + (j - jj)) * CGX + (i - ii)];
+            if (c) s += (double)c * s_t27[(kk + 1) * 9 + (jj + 1) * 3 + (ii + 1)];
+          }
+      acc[q] += s;
+    }
+  }
+  const int sidx = W.scratch_of[it.x];
+  if (sidx < 0) {
+    __syncthreads();
+    const float den = denbas_lev[g.ir];
+    for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
+      int i = q % NA, j = (q / NA) % NA, k = g.slab * PZ + q / (NA * NA);
+      float v = 0.0f;
+      if (i < g.n1 && j < g.n2 && k < g.n3) v = (float)acc[q] / den;
+      out[q] = v;
+    }
+  } else {  // one slice of a shared unit
+    __syncthreads();
+    double* sc = W.scratch + (size_t)sidx * NA * NA * PZ;
+    for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x)
+      if (acc[q] != 0.0) atomicAdd(&sc[q], acc[q]);
+  }
+}
+
+// Units shared by several slices: the summed scratch slab to U11.
+__global__ void k_patch_finish(DevMesh M, const int32_t* __restrict__ order, const int32_t* __restrict__ multi,
+                               const double* __restrict__ scratch, float* __restrict__ u11,
+                               const float* __restrict__ denbas_lev) {
+  int u = multi[blockIdx.x];
+  int ip = order[u / NSLAB], slab = u % NSLAB;
+  int n1 = M.nx[ip], n2 = M.ny[ip], n3 = M.nz[ip];
+  float den = denbas_lev[M.level[ip]];
+  const double* sc = scratch + (size_t)blockIdx.x * NA * NA * PZ;
+  float* out = u11 + (size_t)ip * NA * NA * NA + (size_t)slab * PZ * NA * NA;
+  for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
+    int i = q % NA, j = (q / NA) % NA, k = slab * PZ + q / (NA * NA);
+    float v = 0.0f;
+    if (i < n1 && j < n2 && k < n3) v = (float)sc[q] / den;
+    out[q] = v;
+  }
+}
+
+// Patch order of the deposit: finest level first, table order within a level.
+static int patch_order(asohf_ctx* c, const asohf_mesh* mh, int32_t** d_order) {
+  int np = 0;
+  for (int ir = 1; ir <= mh->nl; ir++) np += mh->npatch[ir];
+  int32_t* h = (int32_t*)malloc(4 * (size_t)(np > 0 ? np : 1));
+  int q = 0;
+  for (int ir = mh->nl; ir >= 1; ir--) {
+    int first = 0;
+    for (int l = 1; l < ir; l++) first += mh->npatch[l];
+    for (int p = 0; p < mh->npatch[ir]; p++) h[q++] = first + p;
+  }
+  *d_order = (int32_t*)arena_alloc(c, 4 * (size_t)(np > 0 ? np : 1));
+  if (!*d_order) { free(h); return ASOHF_ERR_CAPACITY; }
+  ASOHF_CUDA(cudaMemcpyAsync(*d_order, h, 4 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  free(h);
+  return ASOHF_OK;
 }
 
 static float* upload_floats(asohf_ctx* c, const float* h, size_t n) {
@@ -652,65 +858,67 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
   int np = 0;
   for (int ir = 1; ir <= nl; ir++) np += mesh->npatch[ir];
   if (np > 0 && !u11) return ASOHF_ERR_INVALID;
-  size_t need = 8 * g + (on_device ? 0 : 4 * g + 4 * (size_t)np * NA * NA * NA) +
-                4 * KW * (ASOHF_NLEVELS + 1) + 64 * (size_t)np + 4096 +
-                (np ? bins_bytes(n, lado0, dx, 2) : 0);
+  const int64_t nall = c->p.n;
+  const bool eqmass = c->mmin == c->norma;  // one particle mass in the store
+  size_t need = 12 * g + (on_device ? 0 : 4 * g + 4 * (size_t)np * NA * NA * NA) +
+                4 * KW * (ASOHF_NLEVELS + 1) + 96 * (size_t)np + 16384 +
+                (np ? bins_bytes(nall, lado0, dx, 2) + 17 * (size_t)nall : 0);
   ASOHF_CHECK(arena_reserve(c, need));
   float* hk = (float*)malloc(sizeof(float) * KW * (ASOHF_NLEVELS + 1));
   compute_kernels_host(nl, interp_degree, hk);
   float* dk = upload_floats(c, hk, (size_t)KW * (ASOHF_NLEVELS + 1));
+  const float* h0 = hk + ASOHF_NMAX_KERNELS;  // level 0: W(-1), W(0), W(1) at h0[-1..1]
+  Terms27 T27;
+  for (int kk = -1; kk <= 1; kk++)
+    for (int jj = -1; jj <= 1; jj++)
+      for (int ii = -1; ii <= 1; ii++) {
+        volatile float t = c->norma * h0[ii];
+        t = t * h0[jj];
+        t = t * h0[kk];
+        T27.t[(kk + 1) * 9 + (jj + 1) * 3 + (ii + 1)] = (double)t;
+      }
+  free(hk);
   float* du1;
   ASOHF_CHECK(stage_out(c, u1, 4 * g, on_device, &du1));
-  float xl = -lado0 / 2.0f;
-  float denbas = dx * dx * dx * rote * (rete * rete * rete);
-  // fixed point unit from the smallest possible term
-  const float* k0 = hk + ASOHF_NMAX_KERNELS;
-  float kmin = fminf(k0[-1], fminf(k0[0], k0[1])), kmax = fmaxf(k0[-1], fmaxf(k0[0], k0[1]));
-  double tmin = (double)c->mmin * kmin * kmin * kmin, tmax = (double)c->norma * kmax * kmax * kmax;
-  int emin = frexp_exp(tmin) - 2, emax = frexp_exp(tmax) + 1;
-  int shift = emin - 25;
-  double lg_n = n > 1 ? log2((double)n) : 0.0;
-  bool fixed = tmin > 0.0 && (emax - shift) + lg_n + 1.0 < 62.0;
-  void* acc = arena_alloc(c, 8 * g);
-  if (!acc || !dk) { free(hk); return ASOHF_ERR_CAPACITY; }
-  ASOHF_CUDA(cudaMemsetAsync(acc, 0, 8 * g, c->stream));
-  if (n > 0) {
-    if (fixed) {
-      double inv_unit = ldexp(1.0, -shift);
-      {
-        int kt_ = ktime_begin(c, "density_base");
-        k_density_base_fixed<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-          c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, dk + ASOHF_NMAX_KERNELS - 1, inv_unit,
-          (unsigned long long*)acc);
-        ktime_end(c, kt_);
-      }
-    } else {
-      {
-        int kt_ = ktime_begin(c, "density_base");
-        k_density_base_f64<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-          c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, dk + ASOHF_NMAX_KERNELS - 1, (double*)acc);
-        ktime_end(c, kt_);
-      }
+  const float xl = -lado0 / 2.0f;
+  const float denbas = dx * dx * dx * rote * (rete * rete * rete);
+  double* acc = (double*)arena_alloc(c, 8 * g);
+  int64_t hend[ASOHF_N_ESP];
+  int64_t acc_n = 0;
+  for (int s = 0; s < ASOHF_N_ESP; s++) { acc_n += npart_esp[s]; hend[s] = acc_n; }
+  int64_t* dend = (int64_t*)arena_alloc(c, sizeof(hend));
+  if (!acc || !dk || !dend) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaMemcpyAsync(dend, hend, sizeof(hend), cudaMemcpyHostToDevice, c->stream));
+  const float* k0 = dk + ASOHF_NMAX_KERNELS - 1;  // level 0: W(-1), W(0), W(1)
+  if (n > 0 && eqmass) {
+    int32_t* cnt = (int32_t*)arena_alloc(c, 4 * g);
+    if (!cnt) return ASOHF_ERR_CAPACITY;
+    ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * g, c->stream));
+    int kt_ = ktime_begin(c, "density_base");
+    k_base_counts<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, nx, xl,
+                                                                          dx, cnt);
+    k_base_stencil<<<grid_for(g, 256, c->num_sms * 16), 256, 0, c->stream>>>(cnt, nx, T27, acc);
+    k_density_base_outliers<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, k0, acc);
+    ktime_end(c, kt_);
+    c->launches += 3;
+  } else {
+    ASOHF_CUDA(cudaMemsetAsync(acc, 0, 8 * g, c->stream));
+    if (n > 0) {
+      int kt_ = ktime_begin(c, "density_base");
+      k_density_base_all<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, k0, acc);
+      ktime_end(c, kt_);
+      c->launches++;
     }
-    c->launches++;
   }
-  if (fixed)
-    k_finish_fixed<<<grid_for(g, 256), 256, 0, c->stream>>>((unsigned long long*)acc, g,
-                                                            ldexp(1.0, shift), denbas, du1);
-  else
-    k_finish_f64<<<grid_for(g, 256), 256, 0, c->stream>>>((double*)acc, g, denbas, du1);
+  k_finish_f64<<<grid_for(g, 256), 256, 0, c->stream>>>(acc, g, denbas, du1);
   c->launches++;
   ASOHF_CUDA(cudaGetLastError());
   if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(u1, du1, 4 * g, cudaMemcpyDeviceToHost, c->stream));
   if (np > 0) {
     DevMesh M;
     ASOHF_CHECK(upload_mesh(c, mesh, &M));
-    Bins B;
-    ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B));
-    int64_t hend[ASOHF_N_ESP];
-    int64_t acc_n = 0;
-    for (int s = 0; s < ASOHF_N_ESP; s++) { acc_n += npart_esp[s]; hend[s] = acc_n; }
-    int64_t* dend = (int64_t*)arena_alloc(c, sizeof(hend));
     float hden[ASOHF_NLEVELS + 1];
     for (int ir = 0; ir <= ASOHF_NLEVELS; ir++) {
       float dxpa = dx / powf(2.0f, (float)ir);
@@ -719,23 +927,84 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
     float* dden = upload_floats(c, hden, ASOHF_NLEVELS + 1);
     float* du11;
     ASOHF_CHECK(stage_out(c, u11, 4 * (size_t)np * NA * NA * NA, on_device, &du11));
-    if (!dend || !dden) { free(hk); return ASOHF_ERR_CAPACITY; }
-    ASOHF_CUDA(cudaMemcpyAsync(dend, hend, sizeof(hend), cudaMemcpyHostToDevice, c->stream));
-    size_t smem = sizeof(double) * NA * NA * ZH;
-    ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    {
+    int32_t* order = nullptr;
+    if (!dden) return ASOHF_ERR_CAPACITY;
+    ASOHF_CHECK(patch_order(c, mesh, &order));
+    if (n > 0) {
+      Bins B;
+      ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B));
+      float4* bp = (float4*)arena_alloc(c, 16 * (size_t)nall);
+      uint8_t* bs = (uint8_t*)arena_alloc(c, (size_t)nall);
+      const int nunits = NSLAB * np;
+      int64_t* ucnt = (int64_t*)arena_alloc(c, 8 * (size_t)nunits);
+      int32_t* sof = (int32_t*)arena_alloc(c, 4 * (size_t)nunits);
+      if (!bp || !bs || !ucnt || !sof) return ASOHF_ERR_CAPACITY;
+      {
+        int kt_ = ktime_begin(c, "density_bin_stage");
+        k_bin_stage<<<grid_for(nall, 256, c->num_sms * 16), 256, 0, c->stream>>>(B.idx, nall, n, c->p.x, c->p.y,
+                                                                               c->p.z, c->p.m, dend, bp, bs);
+        k_patch_unit_counts<<<(nunits + 7) / 8, 256, 0, c->stream>>>(M, B, order, nunits, dx, ucnt);
+        ktime_end(c, kt_);
+        c->launches += 2;
+      }
+      // work list: slices of PSLICE candidates, the densest units first
+      int64_t* hc = (int64_t*)malloc(8 * (size_t)nunits);
+      int32_t* hs = (int32_t*)malloc(4 * (size_t)nunits);
+      int32_t* ord = (int32_t*)malloc(4 * (size_t)nunits);
+      ASOHF_CUDA(cudaMemcpyAsync(hc, ucnt, 8 * (size_t)nunits, cudaMemcpyDeviceToHost, c->stream));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      int64_t nitems = 0;
+      int nmulti = 0;
+      for (int u = 0; u < nunits; u++) {
+        int64_t ns = hc[u] > 0 ? (hc[u] + PSLICE - 1) / PSLICE : 1;
+        hs[u] = ns > 1 ? nmulti++ : -1;
+        nitems += ns;
+        ord[u] = u;
+      }
+      std::sort(ord, ord + nunits, [&](int a2, int b2) { return hc[a2] > hc[b2] || (hc[a2] == hc[b2] && a2 < b2); });
+      int2* hitems = (int2*)malloc(sizeof(int2) * (size_t)nitems);
+      int32_t* hmulti = (int32_t*)malloc(4 * (size_t)(nmulti > 0 ? nmulti : 1));
+      int64_t w = 0;
+      for (int k = 0; k < nunits; k++) {
+        int u = ord[k];
+        int64_t ns = hc[u] > 0 ? (hc[u] + PSLICE - 1) / PSLICE : 1;
+        for (int64_t q = 0; q < ns; q++) hitems[w++] = make_int2(u, (int)q);
+        if (hs[u] >= 0) hmulti[hs[u]] = u;
+      }
+      size_t scratch_b = sizeof(double) * NA * NA * PZ * (size_t)nmulti;
+      int rcs = seg_reserve(c, sizeof(int2) * (size_t)nitems + 4 * (size_t)nmulti + scratch_b + 4096);
+      int2* ditems = rcs == ASOHF_OK ? (int2*)seg_alloc(c, sizeof(int2) * (size_t)nitems) : nullptr;
+      int32_t* dmulti = rcs == ASOHF_OK ? (int32_t*)seg_alloc(c, 4 * (size_t)(nmulti > 0 ? nmulti : 1)) : nullptr;
+      double* scratch = rcs == ASOHF_OK ? (double*)seg_alloc(c, scratch_b > 0 ? scratch_b : 8) : nullptr;
+      if (!ditems || !dmulti || !scratch) {
+        free(hc); free(hs); free(ord); free(hitems); free(hmulti);
+        return rcs != ASOHF_OK ? rcs : ASOHF_ERR_CAPACITY;
+      }
+      ASOHF_CUDA(cudaMemcpyAsync(ditems, hitems, sizeof(int2) * (size_t)nitems, cudaMemcpyHostToDevice, c->stream));
+      ASOHF_CUDA(cudaMemcpyAsync(sof, hs, 4 * (size_t)nunits, cudaMemcpyHostToDevice, c->stream));
+      if (nmulti) {
+        ASOHF_CUDA(cudaMemcpyAsync(dmulti, hmulti, 4 * (size_t)nmulti, cudaMemcpyHostToDevice, c->stream));
+        ASOHF_CUDA(cudaMemsetAsync(scratch, 0, scratch_b, c->stream));
+      }
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      free(hc); free(hs); free(ord); free(hitems); free(hmulti);
+      PatchWork W{ditems, sof, scratch};
+      size_t smem = sizeof(double) * NA * NA * PZ + sizeof(int32_t) * CGX * CGX * CGZ + sizeof(float) * ktab_size(nl);
+      ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       int kt_ = ktime_begin(c, "density_patches");
-      k_density_patches<<<2 * np, PD_BLOCK, smem, c->stream>>>(M, B, c->p.x, c->p.y, c->p.z, c->p.m,
-                                                           dend, dx, dk, du11, dden);
+      k_density_patches<<<(unsigned)nitems, PZ_BLOCK, smem, c->stream>>>(M, B, bp, bs, order, W, dx, dk,
+                                                                       eqmass ? 1 : 0, du11, dden);
+      if (nmulti) k_patch_finish<<<nmulti, 256, 0, c->stream>>>(M, order, dmulti, scratch, du11, dden);
       ktime_end(c, kt_);
+      c->launches += 1 + (nmulti > 0);
+    } else {  // no particles: empty patches
+      ASOHF_CUDA(cudaMemsetAsync(du11, 0, 4 * (size_t)np * NA * NA * NA, c->stream));
     }
-    c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     if (!on_device)
       ASOHF_CUDA(cudaMemcpyAsync(u11, du11, 4 * (size_t)np * NA * NA * NA, cudaMemcpyDeviceToHost, c->stream));
   }
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(hk);
   return ASOHF_OK;
 }
 

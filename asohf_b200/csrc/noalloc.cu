@@ -56,7 +56,7 @@ static Level0Kernel level0_kernel(int deg) {
 }
 
 // The 27-cell periodic cloud of grids.f:787-820 accumulated in float64 into
-// the file-scope array (same cloud terms as k_density_base_f64).
+// the file-scope array (same cloud terms as k_density_base_all).
 __global__ void k_density_base_noalloc(const float* __restrict__ x, const float* __restrict__ y,
                                        const float* __restrict__ z, const float* __restrict__ m,
                                        int64_t n, int nx, float xl, float dx, Level0Kernel K,

@@ -10,8 +10,11 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def _prep(name):
+def _prep(name, vary_mass=False):
     s = synth.generate(name)
+    if vary_mass:  # unequal masses: the general (non-count) deposit paths
+        rng = np.random.default_rng(7)
+        s.m = (s.m * (1.0 + 0.5 * rng.random(s.m.shape[0]))).astype(np.float32)
     cfg = s.cfg
     radx, dx = grid.malla(cfg.nx, cfg.lado0)
     cos = grid.cosmology(cfg.h, cfg.omega_m, cfg.zeta)
@@ -33,9 +36,10 @@ def test_species_sort_bit_exact(gpu_lib, name):
         assert np.array_equal(getattr(pg, f), getattr(po, f)), f
 
 
-@pytest.mark.parametrize("name", ["tiny", "small"])
-def test_density_matches_fp64_oracle(gpu_lib, name):
-    s, cfg, radx, dx, cos = _prep(name)
+@pytest.mark.parametrize("name,vary_mass", [("tiny", False), ("small", False), ("tiny", True),
+                                            ("small", True)])
+def test_density_matches_fp64_oracle(gpu_lib, name, vary_mass):
+    s, cfg, radx, dx, cos = _prep(name, vary_mass)
     g = api.GpuBackend()
     o = O.OracleBackend()
     g.upload(s)
