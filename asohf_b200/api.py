@@ -59,7 +59,7 @@ def load():
                      "asohf_sort_dm_particles_x", "asohf_prune_poor_haloes",
                      "asohf_halofind_particles", "asohf_substructure_particles",
                      "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
-                     "asohf_work_counters", "asohf_set_cluster_threshold"]:
+                     "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -120,6 +120,11 @@ class Asohf:
         (0: default)."""
         _check(self.L.asohf_set_cluster_threshold(self.h, C.c_int64(int(min_members))),
                "asohf_set_cluster_threshold")
+
+    def set_group_tiers(self, tier1: int, tier2: int):
+        """Member counts from which a halo gets 128 / 256 threads (0: default)."""
+        _check(self.L.asohf_set_group_tiers(self.h, C.c_int64(int(tier1)), C.c_int64(int(tier2))),
+               "asohf_set_group_tiers")
 
     def set_profiling(self, on: bool):
         """Brackets the main kernels with CUDA events (diagnostics)."""
@@ -278,10 +283,12 @@ class GpuBackend:
 
     name = "gpu"
 
-    def __init__(self, device: int = 0, cluster_threshold: int = 0):
+    def __init__(self, device: int = 0, cluster_threshold: int = 0, tiers=(0, 0)):
         self.a = Asohf(device)
         if cluster_threshold:
             self.a.set_cluster_threshold(cluster_threshold)
+        if tiers != (0, 0):
+            self.a.set_group_tiers(*tiers)
 
     def upload(self, parts):
         self.a.upload_particles(parts.x, parts.y, parts.z, parts.vx, parts.vy, parts.vz, parts.m,

@@ -42,13 +42,16 @@ struct DevParticles {
 struct asohf_ctx {
   int device = 0;
   cudaStream_t stream = 0;
-  // second stream for per-halo launches that run beside the cluster launch,
-  // forked from and joined back into `stream` with the two events
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // streams for per-halo launches that run beside the cluster launch,
+  // forked from and joined back into `stream` with the events
+  static const int NSIDE = 3;
+  cudaStream_t side[NSIDE] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[NSIDE] = {nullptr, nullptr, nullptr};
   int num_sms = 148;
-  // haloes of at least this many members are refined by a CTA cluster
+  // size tiers of the per-halo launches (members): >= cluster_min a CTA
+  // cluster, >= tier2_k 256 threads, >= tier1_k 128 threads, else 32
   int64_t cluster_min = 32768;
+  int64_t tier2_k = 4096, tier1_k = 512;
   DevParticles p;      // current store
   DevParticles alt;    // second buffer set for permutations
   float norma = 0.f;   // MAXVAL(MASAP), refreshed on upload
@@ -78,7 +81,7 @@ struct asohf_ctx {
   unsigned long long* d_work = nullptr;  // 8 counters
   // optional CUDA-event timing of named kernels (asohf_set_profiling)
   int profiling = 0;
-  struct KRec { const char* name; cudaEvent_t a, b; };
+  struct KRec { const char* name; cudaEvent_t a, b; };  // events on the launch's stream
   KRec* krec = nullptr;
   int nkrec = 0, capkrec = 0;
   struct KSum { const char* name; double ms; int64_t n; };
@@ -87,8 +90,10 @@ struct asohf_ctx {
 };
 
 // Brackets a kernel launch with events on the context stream when profiling.
-int ktime_begin(asohf_ctx* c, const char* name);
-void ktime_end(asohf_ctx* c, int slot);
+int ktime_begin(asohf_ctx* c, const char* name, cudaStream_t s);
+void ktime_end(asohf_ctx* c, int slot, cudaStream_t s);
+inline int ktime_begin(asohf_ctx* c, const char* name) { return ktime_begin(c, name, c->stream); }
+inline void ktime_end(asohf_ctx* c, int slot) { ktime_end(c, slot, c->stream); }
 
 // Scratch: reserve() may grow the arena only when nothing is allocated from it.
 int arena_reserve(asohf_ctx* c, size_t bytes);

@@ -151,13 +151,18 @@ extern "C" int asohf_create(int device, asohf_ctx** out) {
   asohf_ctx* c = new asohf_ctx();
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
-  if (arena_reserve(c, 64u << 20) != ASOHF_OK || cudaMalloc(&c->d_work, 64) != cudaSuccess ||
-      cudaMemset(c->d_work, 0, 64) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+  bool ok = arena_reserve(c, 64u << 20) == ASOHF_OK && cudaMalloc(&c->d_work, 64) == cudaSuccess &&
+            cudaMemset(c->d_work, 0, 64) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; ok && i < asohf_ctx::NSIDE; i++)
+    ok = cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    for (int i = 0; i < asohf_ctx::NSIDE; i++) {
+      if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
+      if (c->side[i]) cudaStreamDestroy(c->side[i]);
+    }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-    if (c->side) cudaStreamDestroy(c->side);
     cudaFree(c->d_work);
     cudaFree(c->arena);
     delete c;
@@ -180,10 +185,12 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaFree(c->arena);
   cudaFree(c->seg);
   cudaFree(c->d_work);
-  cudaStreamSynchronize(c->side);
+  for (int i = 0; i < asohf_ctx::NSIDE; i++) {
+    cudaStreamSynchronize(c->side[i]);
+    cudaEventDestroy(c->ev_join[i]);
+    cudaStreamDestroy(c->side[i]);
+  }
   cudaEventDestroy(c->ev_fork);
-  cudaEventDestroy(c->ev_join);
-  cudaStreamDestroy(c->side);
   for (int i = 0; i < c->nkrec; i++) { cudaEventDestroy(c->krec[i].a); cudaEventDestroy(c->krec[i].b); }
   free(c->krec);
   delete c;
@@ -204,7 +211,7 @@ extern "C" int asohf_synchronize(asohf_ctx* c) {
 
 extern "C" int64_t asohf_launch_count(asohf_ctx* c) { return c ? c->launches : -1; }
 
-int ktime_begin(asohf_ctx* c, const char* name) {
+int ktime_begin(asohf_ctx* c, const char* name, cudaStream_t s) {
   if (!c->profiling) return -1;
   if (c->nkrec == c->capkrec) {
     int cap = c->capkrec ? 2 * c->capkrec : 256;
@@ -217,13 +224,13 @@ int ktime_begin(asohf_ctx* c, const char* name) {
   r.name = name;
   if (cudaEventCreate(&r.a) != cudaSuccess) return -1;
   if (cudaEventCreate(&r.b) != cudaSuccess) { cudaEventDestroy(r.a); return -1; }
-  cudaEventRecord(r.a, c->stream);
+  cudaEventRecord(r.a, s);
   return c->nkrec++;
 }
 
-void ktime_end(asohf_ctx* c, int slot) {
+void ktime_end(asohf_ctx* c, int slot, cudaStream_t s) {
   if (slot < 0) return;
-  cudaEventRecord(c->krec[slot].b, c->stream);
+  cudaEventRecord(c->krec[slot].b, s);
 }
 
 static void ktime_flush(asohf_ctx* c) {

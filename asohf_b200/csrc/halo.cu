@@ -201,17 +201,23 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
 }
 
 // ---------------------------------------------------------------- launch helpers
-// Haloes whose member count reaches ctx->cluster_min are refined by a
-// cluster of CTAs; the others by one CTA each, launched concurrently on the
-// context's side stream.
+// Size tiers of the per-halo launches, by member count: at least
+// ctx->cluster_min -> a thread-block cluster; at least ctx->tier2_k -> one
+// CTA of 256 threads; at least ctx->tier1_k -> 128 threads; the rest -> 32
+// threads.  The small CTAs keep many small haloes resident per SM, whose
+// passes are short and bound by latency.  The tiers run concurrently on four
+// streams.
 #define BIG_K 32768
+#define TIER2_K 4096
+#define TIER1_K 512
+static const int kTierThreads[3] = {32, 128, 256};
 
 template <typename... P, typename... A>
-static cudaError_t launch_grp(void (*kern)(P...), int C, int ngroups, cudaStream_t s, A&&... args) {
+static cudaError_t launch_grp(void (*kern)(P...), int C, int ngroups, int threads, cudaStream_t s, A&&... args) {
   if (ngroups <= 0) return cudaSuccess;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(ngroups * C));
-  cfg.blockDim = dim3(HB);
+  cfg.blockDim = dim3((unsigned)threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -228,42 +234,58 @@ static cudaError_t launch_grp(void (*kern)(P...), int C, int ngroups, cudaStream
   return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
 }
 
-// Runs `big` (cluster kernel) on the context stream and `small` (one CTA per
-// halo) on the side stream, joined back into the context stream.
-static int fork_join(asohf_ctx* c) {
+// The side streams start after the work queued so far on the context stream;
+// the context stream then waits for all of them.
+static int fork_all(asohf_ctx* c) {
   ASOHF_CUDA(cudaEventRecord(c->ev_fork, c->stream));
-  ASOHF_CUDA(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+  for (int i = 0; i < asohf_ctx::NSIDE; i++) ASOHF_CUDA(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
   return ASOHF_OK;
 }
-static int join(asohf_ctx* c) {
-  ASOHF_CUDA(cudaEventRecord(c->ev_join, c->side));
-  ASOHF_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+static int join_all(asohf_ctx* c) {
+  for (int i = 0; i < asohf_ctx::NSIDE; i++) {
+    ASOHF_CUDA(cudaEventRecord(c->ev_join[i], c->side[i]));
+    ASOHF_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join[i], 0));
+  }
   return ASOHF_OK;
 }
 
-// Splits slots 0..n-1 into big (count >= cluster_min) and small lists (device).
-static int split_slots(asohf_ctx* c, const int32_t* hcount, int n, int32_t* d_big, int32_t* d_small, int* nb,
-                       int* nsm) {
-  const int64_t big_k = c->cluster_min;
-  int32_t* hb = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
-  int32_t* hs = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
-  int b = 0, s = 0;
-  for (int i = 0; i < n; i++) {
-    if (hcount[i] >= big_k) hb[b++] = i;
-    else hs[s++] = i;
-  }
-  if (b) ASOHF_CUDA(cudaMemcpyAsync(d_big, hb, 4 * (size_t)b, cudaMemcpyHostToDevice, c->stream));
-  if (s) ASOHF_CUDA(cudaMemcpyAsync(d_small, hs, 4 * (size_t)s, cudaMemcpyHostToDevice, c->stream));
+struct Tiers {
+  int n[4];           // slots per tier (0: 32 threads, 1: 128, 2: 256, 3: cluster)
+  int32_t* slots[4];  // device slot lists
+};
+
+// Buckets entries 0..n-1 by hcount[] into the tiers; entry i stands for
+// slot ids[i] (slot i when ids is null).  dbuf holds n entries.
+static int split_tiers(asohf_ctx* c, const int32_t* hcount, int n, int32_t* dbuf, Tiers* T,
+                       const int32_t* ids = nullptr) {
+  int32_t* h = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
+  int cnt[4] = {0, 0, 0, 0};
+  auto tier = [&](int32_t k) {
+    return k >= c->cluster_min ? 3 : (k >= c->tier2_k ? 2 : (k >= c->tier1_k ? 1 : 0));
+  };
+  for (int i = 0; i < n; i++) cnt[tier(hcount[i])]++;
+  int off[4];
+  off[3] = 0;
+  off[2] = cnt[3];
+  off[1] = off[2] + cnt[2];
+  off[0] = off[1] + cnt[1];
+  int fill[4] = {off[0], off[1], off[2], off[3]};
+  for (int i = 0; i < n; i++) h[fill[tier(hcount[i])]++] = ids ? ids[i] : i;
+  if (n) ASOHF_CUDA(cudaMemcpyAsync(dbuf, h, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(hb);
-  free(hs);
-  *nb = b;
-  *nsm = s;
+  free(h);
+  for (int t = 0; t < 4; t++) {
+    T->n[t] = cnt[t];
+    T->slots[t] = dbuf + off[t];
+  }
   return ASOHF_OK;
 }
 
 template <int C>
-__device__ __forceinline__ int group_slot(const int32_t* slots) { return slots[blockIdx.x / C]; }
+__device__ __forceinline__ int group_slot(const int32_t* slots) {
+  if constexpr (C == 1) return slots[blockIdx.x];
+  else return slots[blockIdx.x / C];
+}
 
 __device__ __forceinline__ bool leader(unsigned rank) { return rank == 0 && threadIdx.x == 0; }
 
@@ -284,11 +306,21 @@ __device__ __forceinline__ int level_of_patch(const HConst& H, int ipatch) {
   return irr;
 }
 
-// Recentering + growth of HALOFIND_PARTICLES (haloes_particles.f:741-849).
+// Member-count caps of the growth by launch shape: a halo whose sphere
+// outgrows the cap of its CTA size stops, leaves its centre and radius in
+// GrowOut and is resumed by a larger group (the cost of the growth is known
+// only as it runs: a small candidate inside a large halo grows to its size).
+struct GrowCaps {
+  int64_t c32, c128, c256;
+};
+#define GROW_ESCALATE 100  // status of a halo handed to a larger group
+
+// Recentering + growth of HALOFIND_PARTICLES (haloes_particles.f:741-849);
+// with resume set, the growth restarts from the saved centre and radius.
 template <int C>
 __global__ void __launch_bounds__(HB)
 k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, asohf_catalogue cat,
-            const int32_t* __restrict__ work, GrowOut o) {
+            const int32_t* __restrict__ work, GrowOut o, GrowCaps caps, int resume) {
   __shared__ RecShared sh;
   Grp<C> G;
   int slot = group_slot<C>(slots);
@@ -298,18 +330,25 @@ k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, aso
     if (leader(rk)) { o.konta[slot] = 0; o.status[slot] = 0; }
     return;
   }
-  int irr = level_of_patch(H, cat.patchclus[i0]);
-  float cx = cat.clusrx[i0], cy = cat.clusry[i0], cz = cat.clusrz[i0];
-  float r_in = cat.radio[i0];
-  float dxpamin = __fdiv_rn(ci.dx, exp2f((float)irr));
-  if (!recenter_group(G, S, ci, &cx, &cy, &cz, r_in, dxpamin, sh)) {
-    if (leader(rk)) { o.konta[slot] = 0; o.status[slot] = ASOHF_ERR_CAPACITY; }
-    return;
+  const int64_t kcap = C > 1 ? LLONG_MAX
+                             : (blockDim.x <= 32 ? caps.c32 : (blockDim.x <= 128 ? caps.c128 : caps.c256));
+  float cx, cy, cz, rclus;
+  if (!resume) {
+    int irr = level_of_patch(H, cat.patchclus[i0]);
+    cx = cat.clusrx[i0]; cy = cat.clusry[i0]; cz = cat.clusrz[i0];
+    float dxpamin = __fdiv_rn(ci.dx, exp2f((float)irr));
+    if (!recenter_group(G, S, ci, &cx, &cy, &cz, cat.radio[i0], dxpamin, sh)) {
+      if (leader(rk)) { o.konta[slot] = 0; o.status[slot] = ASOHF_ERR_CAPACITY; }
+      return;
+    }
+    rclus = cat.radio[i0];
+  } else {
+    cx = o.cx[slot]; cy = o.cy[slot]; cz = o.cz[slot];
+    rclus = o.rclus[slot];
   }
   float mino = __fmul_rn(fminf(200.0f, H.contrastec), H.fdm);
   float den0 = __fmul_rn(__fmul_rn(H.rote, __fmul_rn(__fmul_rn(H.rete, H.rete), H.rete)),
                          __fdiv_rn(__fmul_rn(4.0f, H.pi), 3.0f));
-  float rclus = r_in;
   float delta2 = __fmul_rn(100.0f, mino);
   float rg = rclus;
   long long konta = 0;
@@ -332,6 +371,15 @@ k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, aso
       }
     });
     konta = gsum_ll(G, c, sh.lred, sh.x);
+    if (konta > kcap) {  // hand over to a larger group at this radius
+      if (leader(rk)) {
+        o.cx[slot] = cx; o.cy[slot] = cy; o.cz[slot] = cz;
+        o.rclus[slot] = rclus;
+        o.konta[slot] = (int32_t)(konta < INT32_MAX ? konta : INT32_MAX);
+        o.status[slot] = GROW_ESCALATE;
+      }
+      return;
+    }
     masadm = gsum_d(G, ms, sh.dred, sh.x);
     bas = gmax_f(G, bas, sh.fred, sh.x);
     float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(bas, bas), bas));
@@ -1799,24 +1847,45 @@ static int big_cluster(asohf_ctx* c) {
 
 // Launches kern<C> for the `n` groups of slots[] on stream s (C in {1, 8, 16}).
 #define LAUNCH_TIER(KERN, C, n, s, ...)                                              \
-  ((C) == 16 ? launch_grp(KERN<16>, 16, (n), (s), __VA_ARGS__)                       \
-             : (C) == 8 ? launch_grp(KERN<8>, 8, (n), (s), __VA_ARGS__)              \
-                        : launch_grp(KERN<1>, 1, (n), (s), __VA_ARGS__))
+  ((C) == 16 ? launch_grp(KERN<16>, 16, (n), 256, (s), __VA_ARGS__)                  \
+             : (C) == 8 ? launch_grp(KERN<8>, 8, (n), 256, (s), __VA_ARGS__)         \
+                        : launch_grp(KERN<1>, 1, (n), 256, (s), __VA_ARGS__))
 
-// The big tier on the context stream and the small tier on the side stream,
-// the context stream waiting for both.
-#define LAUNCH_SPLIT(KERN, CB, nb, big, ns_, small, ...)                                      \
-  do {                                                                                         \
-    ASOHF_CHECK(fork_join(c));                                                                 \
-    if ((nb) > 0) ASOHF_CUDA(LAUNCH_TIER(KERN, CB, (nb), c->stream, big, __VA_ARGS__));        \
-    if ((ns_) > 0) ASOHF_CUDA(launch_grp(KERN<1>, 1, (ns_), c->side, small, __VA_ARGS__));     \
-    ASOHF_CHECK(join(c));                                                                      \
-    c->launches += ((nb) > 0) + ((ns_) > 0);                                                   \
+// The cluster tier on the context stream, the CTA tiers on the side streams,
+// the context stream waiting for all.
+#define LAUNCH_TIERS(KERN, CB, T, ...)                                                              \
+  do {                                                                                              \
+    ASOHF_CHECK(fork_all(c));                                                                       \
+    if ((T).n[3] > 0) {                                                                             \
+      int k3_ = ktime_begin(c, #KERN "/cluster", c->stream);                                        \
+      ASOHF_CUDA(LAUNCH_TIER(KERN, CB, (T).n[3], c->stream, (T).slots[3], __VA_ARGS__));            \
+      ktime_end(c, k3_, c->stream);                                                                 \
+    }                                                                                               \
+    for (int t_ = 2; t_ >= 0; t_--)                                                                 \
+      if ((T).n[t_] > 0) {                                                                          \
+        static const char* const nm_[3] = {#KERN "/cta32", #KERN "/cta128", #KERN "/cta256"};       \
+        cudaStream_t s_ = c->side[2 - t_];                                                          \
+        int k_ = ktime_begin(c, nm_[t_], s_);                                                       \
+        ASOHF_CUDA(launch_grp(KERN<1>, 1, (T).n[t_], kTierThreads[t_], s_, (T).slots[t_], __VA_ARGS__)); \
+        ktime_end(c, k_, s_);                                                                       \
+      }                                                                                             \
+    ASOHF_CHECK(join_all(c));                                                                       \
+    for (int t_ = 0; t_ < 4; t_++) c->launches += (T).n[t_] > 0;                                    \
   } while (0)
 
 extern "C" int asohf_set_cluster_threshold(asohf_ctx* c, int64_t min_members) {
   if (!c || min_members < 0) return ASOHF_ERR_INVALID;
   c->cluster_min = min_members == 0 ? BIG_K : min_members;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_set_group_tiers(asohf_ctx* c, int64_t tier1_members, int64_t tier2_members) {
+  if (!c || tier1_members < 0 || tier2_members < 0) return ASOHF_ERR_INVALID;
+  int64_t t1 = tier1_members == 0 ? TIER1_K : tier1_members;
+  int64_t t2 = tier2_members == 0 ? TIER2_K : tier2_members;
+  if (t2 < t1) return ASOHF_ERR_INVALID;
+  c->tier1_k = t1;
+  c->tier2_k = t2;
   return ASOHF_OK;
 }
 
@@ -1844,9 +1913,8 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   if (ns > 0) {
     // per-slot buffers
     int32_t* d_work = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
-    int32_t* d_iota = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
-    int32_t* d_big = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
-    int32_t* d_small = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_tg = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_tm = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int32_t* d_fill = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     uint8_t* d_final = (uint8_t*)arena_alloc(c, (size_t)ns);
     GrowOut g;
@@ -1862,49 +1930,54 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     int32_t* d_nbound = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int32_t* d_nscan = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int64_t* d_ids_off = (int64_t*)arena_alloc(c, 8 * (size_t)ns);
-    if (!d_work || !d_iota || !d_big || !d_small || !d_fill || !d_final || !g.cx || !g.cy || !g.cz ||
+    if (!d_work || !d_tg || !d_tm || !d_fill || !d_final || !g.cx || !g.cy || !g.cz ||
         !g.rgather || !g.rclus || !g.konta || !g.masadm || !g.status || !d_off || !d_nbound || !d_nscan ||
         !d_ids_off) {
       free(hw); free(hdm);
       return ASOHF_ERR_CAPACITY;
     }
     ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
-    // growth: slots are in DMPCLUS-descending order, so the big tier is a prefix
-    int nbig = 0;
-    while (CB > 1 && nbig < ns && hdm[nbig] >= c->cluster_min) nbig++;
-    {
-      int32_t* io = (int32_t*)malloc(4 * (size_t)ns);
-      for (int s = 0; s < ns; s++) io[s] = s;
-      ASOHF_CUDA(cudaMemcpyAsync(d_iota, io, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
-      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-      free(io);
-    }
-    {
-      int kt_ = ktime_begin(c, "halo_grow");
-      LAUNCH_SPLIT(k_halo_grow, CB, nbig, d_iota, ns - nbig, d_iota + nbig, S, ci, H, m.d, d_work, g);
-      ktime_end(c, kt_);
-    }
-    // offsets (host scan: ns is the number of haloes of one level)
+    // growth, tiered first by DMPCLUS (the members counted when the candidate
+    // was pruned); haloes that outgrow their group size resume in a larger one
+    Tiers tg, tm;
+    GrowCaps caps{c->tier2_k, 4 * c->tier2_k, CB > 1 ? c->cluster_min : (int64_t)LLONG_MAX};
     int32_t* hk = (int32_t*)malloc(4 * (size_t)ns);
     int32_t* hst = (int32_t*)malloc(4 * (size_t)ns);
     int64_t* hoff = (int64_t*)malloc(8 * (size_t)(ns + 1));
-    ASOHF_CUDA(cudaMemcpyAsync(hk, g.konta, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
-    ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
-    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    int32_t* hesc = (int32_t*)malloc(4 * (size_t)ns);
+    int32_t* kesc = (int32_t*)malloc(4 * (size_t)ns);
+    ASOHF_CHECK(split_tiers(c, hdm, ns, d_tg, &tg));
+    for (int round = 0;; round++) {
+      {
+        int kt_ = ktime_begin(c, "halo_grow");
+        LAUNCH_TIERS(k_halo_grow, CB, tg, S, ci, H, m.d, d_work, g, caps, round > 0 ? 1 : 0);
+        ktime_end(c, kt_);
+      }
+      ASOHF_CUDA(cudaMemcpyAsync(hk, g.konta, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+      ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      int ne = 0;
+      for (int s = 0; s < ns; s++)
+        if (hst[s] == GROW_ESCALATE) { hesc[ne] = s; kesc[ne++] = hk[s]; }
+      if (ne == 0) break;
+      // escalated haloes: tiers by their member count at hand-over, slot ids
+      // through the escalation list
+      if (round >= 3) break;  // every tier was tried: reported below
+      ASOHF_CHECK(split_tiers(c, kesc, ne, d_tg, &tg, hesc));
+    }
+    free(hesc);
+    free(kesc);
     hoff[0] = 0;
+    bool left = false;  // haloes no group size could finish (not expected)
     for (int s = 0; s < ns; s++) {
-      if (hst[s]) rc = hst[s];
+      if (hst[s]) rc = hst[s] == GROW_ESCALATE ? ASOHF_ERR_CAPACITY : hst[s];
+      if (hst[s] == GROW_ESCALATE) { hk[s] = 0; left = true; }
       hoff[s + 1] = hoff[s] + hk[s];
     }
+    if (left) ASOHF_CUDA(cudaMemcpyAsync(g.konta, hk, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
     int64_t T = hoff[ns];
     ASOHF_CUDA(cudaMemcpyAsync(d_off, hoff, 8 * (size_t)(ns + 1), cudaMemcpyHostToDevice, c->stream));
-    int nb2 = 0, ns2 = 0;
-    if (CB > 1) {
-      ASOHF_CHECK(split_slots(c, hk, ns, d_big, d_small, &nb2, &ns2));
-    } else {
-      ASOHF_CUDA(cudaMemcpyAsync(d_small, d_iota, 4 * (size_t)ns, cudaMemcpyDeviceToDevice, c->stream));
-      ns2 = ns;
-    }
+    ASOHF_CHECK(split_tiers(c, hk, ns, d_tm, &tm));
     // element buffers (allocated after the per-slot ones: the arena grows
     // only when empty, so reserve everything now)
     int bits = 1;
@@ -1945,7 +2018,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       ASOHF_CUDA(cudaMemsetAsync(d_fill, 0, 4 * (size_t)ns, c->stream));
       {
         int kt_ = ktime_begin(c, "halo_gather");
-        LAUNCH_SPLIT(k_halo_gather, CB, nb2, d_big, ns2, d_small, S, ci, g.konta, d_off, g.cx, g.cy, g.cz,
+        LAUNCH_TIERS(k_halo_gather, CB, tm, S, ci, g.konta, d_off, g.cx, g.cy, g.cz,
                      g.rgather, d_fill, k0, v0);
         ktime_end(c, kt_);
       }
@@ -1963,7 +2036,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.vals = v1;
     {
       int kt_ = ktime_begin(c, "halo_main");
-      LAUNCH_SPLIT(k_halo_main, CB, nb2, d_big, ns2, d_small, S, H, m.d, d_work, g, sg);
+      LAUNCH_TIERS(k_halo_main, CB, tm, S, H, m.d, d_work, g, sg);
       ktime_end(c, kt_);
     }
     ASOHF_CUDA(cudaGetLastError());
@@ -1977,7 +2050,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       ASOHF_CHECK(ensure_pph(c, total));
       {
         int kt_ = ktime_begin(c, "halo_write_ids");
-        LAUNCH_SPLIT(k_write_ids, CB, nb2, d_big, ns2, d_small, d_nscan, d_off, d_ids_off, d_final, sg.a.px,
+        LAUNCH_TIERS(k_write_ids, CB, tm, d_nscan, d_off, d_ids_off, d_final, sg.a.px,
                      sg.b.px, sg.flag, c->p.id, c->d_pph);
         ktime_end(c, kt_);
       }

@@ -12,9 +12,8 @@
 
 namespace cg = cooperative_groups;
 
-#define HB 256          // threads per CTA of the per-halo kernels
-#define IPT 4           // items per thread per tile
-#define TILE (HB * IPT)
+#define HB 256          // threads per CTA of the per-halo kernels (at most)
+#define IPT 4           // items per thread per tile of the block scans
 #define MAX_HIST 48     // recentering shrink steps kept in shared memory
 
 // A halo is refined by a group of C CTAs: one CTA (C = 1) or a thread-block
@@ -294,7 +293,8 @@ __device__ __forceinline__ int col_index(float v, float xl, float cdx, int n) {
 
 // Calls f(e) for every column-index entry whose x, y, z lie within r' >= r
 // of (cx, cy, cz) (a superset of any open-cube or sphere test of radius r).
-// Warps take columns round-robin; lanes stride the binary-searched x range.
+// Warp w of nw takes columns w, w+nw, ...; its lanes binary-search the x
+// ranges of 32 of those columns at once, then stride through each range.
 template <class F>
 __device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy, float cz, float r, int w0, int nw,
                                            F&& f) {
@@ -305,10 +305,11 @@ __device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy
   int ny = iy1 - iy0 + 1;
   int ncols = ny * (iz1 - iz0 + 1);
   int lane = threadIdx.x & 31;
-  for (int c = w0; c < ncols; c += nw) {
-    int64_t cid = (int64_t)(iz0 + c / ny) * ci.ncol + iy0 + c % ny;
+  for (int base = 0; w0 + base * nw < ncols; base += 32) {
+    int c = w0 + (base + lane) * nw;
     int64_t s = 0, e = 0;
-    if (lane == 0) {
+    if (c < ncols) {
+      int64_t cid = (int64_t)(iz0 + c / ny) * ci.ncol + iy0 + c % ny;
       int64_t a = ci.start[cid], b = ci.start[cid + 1];
       int64_t lo = a, hi = b;
       while (lo < hi) {  // first x >= xlo
@@ -323,9 +324,10 @@ __device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy
       }
       e = lo;
     }
-    s = __shfl_sync(0xffffffffu, s, 0);
-    e = __shfl_sync(0xffffffffu, e, 0);
-    for (int64_t k = s + lane; k < e; k += 32) f(ci.cp[k]);
+    for (int q = 0; q < 32 && w0 + (base + q) * nw < ncols; q++) {
+      int64_t sq = __shfl_sync(0xffffffffu, s, q), eq = __shfl_sync(0xffffffffu, e, q);
+      for (int64_t k = sq + lane; k < eq; k += 32) f(ci.cp[k]);
+    }
   }
 }
 
@@ -528,7 +530,8 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
 template <class V, class U>
 __device__ __forceinline__ double tile_prefix_d(int64_t a, int64_t b, double carry, V val, U use,
                                                 double* sbuf) {
-  for (int64_t t0 = a; t0 < b; t0 += TILE) {
+  const int64_t tile = (int64_t)blockDim.x * IPT;
+  for (int64_t t0 = a; t0 < b; t0 += tile) {
     double loc[IPT];
     double run = 0.0;
     int64_t j0 = t0 + (int64_t)threadIdx.x * IPT;

@@ -295,7 +295,7 @@ def main():
                    "l2": "inputs > L2 (4.3 GB of particles per step)"},
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches),
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in
-                                sorted(kstats.items(), key=lambda kv: -kv[1][0])[:12]},
+                                sorted(kstats.items(), key=lambda kv: -kv[1][0])[:40]},
         "stage_s": {k: round(v, 4) for k, v in r.stage_s.items()},
         "catalogue": {"haloes": int((r.cat.realclus[: r.cat.nclus] == -1).sum()),
                       "subhaloes": int((r.cat.realclus[: r.cat.nclus] > 0).sum()),

@@ -55,6 +55,12 @@ int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
  * one CTA each (results are the same either way).  0 restores the default
  * (32768); 1 sends every halo to the cluster path. */
 int asohf_set_cluster_threshold(asohf_ctx *ctx, int64_t min_members);
+/* Tuning, no counterpart in the reference: haloes below the cluster
+ * threshold are refined by one CTA of 256 threads from tier2_members
+ * members, of 128 threads from tier1_members, else of 32 threads; a halo
+ * whose growth sphere outgrows its CTA moves to a larger one.  0 restores
+ * a default (512, 4096). */
+int asohf_set_group_tiers(asohf_ctx *ctx, int64_t tier1_members, int64_t tier2_members);
 
 /* MODULE PARTICLES (particles.f:1-14) / READ_AND_ALLOC_PARTICLES
  * (alloc.f:196-528): copies the particle arrays into the device store,

@@ -42,13 +42,17 @@ def compare(rg, ro, rtol=1e-5):
     assert np.array_equal(rg.pph, ro.pph)
 
 
-@pytest.mark.parametrize("name,cluster_min", [("tiny", 0), ("small", 0), ("tiny", 1), ("small", 1),
-                                              ("small", 300)])
-def test_halofind_matches_oracle(gpu_lib, name, cluster_min):
+@pytest.mark.parametrize("name,cluster_min,tiers", [("tiny", 0, (0, 0)), ("small", 0, (0, 0)),
+                                                    ("tiny", 1, (0, 0)), ("small", 1, (0, 0)),
+                                                    ("small", 300, (0, 0)), ("tiny", 0, (16, 64)),
+                                                    ("small", 2000, (16, 64))])
+def test_halofind_matches_oracle(gpu_lib, name, cluster_min, tiers):
     """cluster_min 1 sends every halo through the thread-block-cluster
-    kernels, 300 splits the haloes between the two tiers."""
+    kernels, 300 splits the haloes between clusters and single CTAs; the
+    small tier bounds (16, 64) put haloes in all four launch shapes and make
+    growing haloes move to larger groups mid-growth."""
     s = synth.generate(name)
-    rg = driver.run(s, api.GpuBackend(cluster_threshold=cluster_min), with_subs=False)
+    rg = driver.run(s, api.GpuBackend(cluster_threshold=cluster_min, tiers=tiers), with_subs=False)
     ro = driver.run(s, O.OracleBackend(), with_subs=False)
     assert (ro.cat.realclus[: ro.cat.nclus] != 0).sum() > 0
     compare(rg, ro)
