@@ -30,10 +30,15 @@
 #include "halo_dev.cuh"
 
 // ---------------------------------------------------------------- catalogue mirror
+// A call reads and writes the entries of its own haloes, [w0, n), and (the
+// subhalo calls) a few fields of earlier entries, their hosts.  With a host
+// catalogue only those ranges cross PCIe; the device arrays keep the
+// caller's indexing.
 struct CatMirror {
   asohf_catalogue h;  // caller's
   asohf_catalogue d;  // device
-  int n;              // entries mirrored
+  int n;              // entries 0..n-1 addressable
+  int w0;             // first entry of the call's window
   bool host;
 };
 
@@ -43,6 +48,9 @@ struct CatMirror {
   X(m2500m) X(r2500m) X(velocity_dispersion) X(kinetic_e) X(potential_e)
 #define CAT_I1(X) X(patchclus) X(realclus) X(levhal) X(dmpclus) X(iplip)
 #define CAT_FM(X) X(angularm, 3) X(profiles, 2 * ASOHF_NBINS) X(eigenval, 3) X(inertia_tensor, 6)
+// fields of host entries the subhalo kernels read
+#define CAT_HOST(X) X(realclus, 1) X(masa, 1) X(msub, 1) X(clusrx, 1) X(clusry, 1) X(clusrz, 1) \
+  X(profiles, 2 * ASOHF_NBINS)
 
 static size_t cat_bytes(int n) {
   size_t b = 0;
@@ -56,40 +64,50 @@ static size_t cat_bytes(int n) {
   return b;
 }
 
-static int cat_mirror_in(asohf_ctx* c, asohf_catalogue* h, int n, int on_device, CatMirror* m) {
+static int cat_mirror_in(asohf_ctx* c, asohf_catalogue* h, int n, int on_device, CatMirror* m, int w0,
+                         bool hosts = false) {
   m->h = *h;
   m->n = n;
+  m->w0 = w0 < 0 ? 0 : (w0 > n ? n : w0);
   m->host = !on_device;
   if (on_device) { m->d = *h; return ASOHF_OK; }
   m->d = *h;
-#define F(f)                                                                                  \
-  m->d.f = (decltype(m->d.f))arena_alloc(c, 4 * (size_t)n + 4);                              \
-  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                     \
-  if (n) ASOHF_CUDA(cudaMemcpyAsync(m->d.f, h->f, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  const size_t a = (size_t)m->w0, cnt = (size_t)(n - m->w0);
+#define F(f)                                                                                        \
+  m->d.f = (decltype(m->d.f))arena_alloc(c, 4 * (size_t)n + 4);                                    \
+  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                           \
+  if (cnt) ASOHF_CUDA(cudaMemcpyAsync(m->d.f + a, h->f + a, 4 * cnt, cudaMemcpyHostToDevice, c->stream));
   CAT_F1(F) CAT_I1(F)
 #undef F
-#define M(f, w)                                                                               \
-  m->d.f = (float*)arena_alloc(c, 4 * (size_t)n * (w) + 4);                                  \
-  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                     \
-  if (n) ASOHF_CUDA(cudaMemcpyAsync(m->d.f, h->f, 4 * (size_t)n * (w), cudaMemcpyHostToDevice, c->stream));
+#define M(f, w)                                                                                     \
+  m->d.f = (float*)arena_alloc(c, 4 * (size_t)n * (w) + 4);                                        \
+  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                           \
+  if (cnt) ASOHF_CUDA(cudaMemcpyAsync(m->d.f + a * (w), h->f + a * (w), 4 * cnt * (w), cudaMemcpyHostToDevice, \
+                                      c->stream));
   CAT_FM(M)
 #undef M
   m->d.indcs = (int32_t*)arena_alloc(c, 8 * (size_t)n + 8);
   if (!m->d.indcs) return ASOHF_ERR_CAPACITY;
-  if (n) ASOHF_CUDA(cudaMemcpyAsync(m->d.indcs, h->indcs, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  if (cnt) ASOHF_CUDA(cudaMemcpyAsync(m->d.indcs + 2 * a, h->indcs + 2 * a, 8 * cnt, cudaMemcpyHostToDevice, c->stream));
+  if (hosts && a) {
+#define H(f, w) ASOHF_CUDA(cudaMemcpyAsync(m->d.f, h->f, 4 * a * (w), cudaMemcpyHostToDevice, c->stream));
+    CAT_HOST(H)
+#undef H
+  }
   return ASOHF_OK;
 }
 
 static int cat_mirror_out(asohf_ctx* c, CatMirror* m) {
-  if (!m->host || m->n == 0) return ASOHF_OK;
-  int n = m->n;
-#define F(f) ASOHF_CUDA(cudaMemcpyAsync(m->h.f, m->d.f, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  if (!m->host || m->n == m->w0) return ASOHF_OK;
+  const size_t a = (size_t)m->w0, cnt = (size_t)(m->n - m->w0);
+#define F(f) ASOHF_CUDA(cudaMemcpyAsync(m->h.f + a, m->d.f + a, 4 * cnt, cudaMemcpyDeviceToHost, c->stream));
   CAT_F1(F) CAT_I1(F)
 #undef F
-#define M(f, w) ASOHF_CUDA(cudaMemcpyAsync(m->h.f, m->d.f, 4 * (size_t)n * (w), cudaMemcpyDeviceToHost, c->stream));
+#define M(f, w) \
+  ASOHF_CUDA(cudaMemcpyAsync(m->h.f + a * (w), m->d.f + a * (w), 4 * cnt * (w), cudaMemcpyDeviceToHost, c->stream));
   CAT_FM(M)
 #undef M
-  ASOHF_CUDA(cudaMemcpyAsync(m->h.indcs, m->d.indcs, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(m->h.indcs + 2 * a, m->d.indcs + 2 * a, 8 * cnt, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return ASOHF_OK;
 }
@@ -183,7 +201,7 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
   arena_reset(c);
   ASOHF_CHECK(arena_reserve(c, cat_bytes(low2) + 4096));
   CatMirror m;
-  ASOHF_CHECK(cat_mirror_in(c, cat, low2, on_device, &m));
+  ASOHF_CHECK(cat_mirror_in(c, cat, low2, on_device, &m, low1 - 1));
   int nh = low2 - low1 + 1;
   if (do_need_to_count == 1)
     {
@@ -1724,8 +1742,16 @@ int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int3
   int32_t* nbound = (int32_t*)malloc(4 * (size_t)(nslots > 0 ? nslots : 1));
   int64_t* ids_off = (int64_t*)malloc(8 * (size_t)(nslots > 0 ? nslots : 1));
   int32_t* slot_of = (int32_t*)malloc(4 * (size_t)(low2 - low1 + 1));
-  ASOHF_CUDA(cudaMemcpyAsync(realclus, m.d.realclus, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
-  ASOHF_CUDA(cudaMemcpyAsync(indcs, m.d.indcs, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  // entries before the window: from the caller's arrays when they are on the host
+  int h0 = m.host ? m.w0 : 0;
+  if (h0) {
+    memcpy(realclus, m.h.realclus, 4 * (size_t)h0);
+    memcpy(indcs, m.h.indcs, 8 * (size_t)h0);
+  }
+  ASOHF_CUDA(cudaMemcpyAsync(realclus + h0, m.d.realclus + h0, 4 * (size_t)(n - h0), cudaMemcpyDeviceToHost,
+                             c->stream));
+  ASOHF_CUDA(cudaMemcpyAsync(indcs + 2 * (size_t)h0, m.d.indcs + 2 * (size_t)h0, 8 * (size_t)(n - h0),
+                             cudaMemcpyDeviceToHost, c->stream));
   if (nslots)
     ASOHF_CUDA(cudaMemcpyAsync(nbound, d_nbound, 4 * (size_t)nslots, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
@@ -1901,7 +1927,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   size_t need = cat_bytes(lowh2) + (size_t)nh * 96 + 65536;
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
-  ASOHF_CHECK(cat_mirror_in(c, cat, lowh2, on_device, &m));
+  ASOHF_CHECK(cat_mirror_in(c, cat, lowh2, on_device, &m, lowh1 - 1));
   int32_t *hw, *hdm;
   int ns;
   ASOHF_CHECK(make_work(c, m, lowh1, lowh2, &hw, &ns, &hdm));
@@ -2687,7 +2713,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   size_t need = cat_bytes(cat->nclus) + (size_t)nh * 160 + 65536;
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
-  ASOHF_CHECK(cat_mirror_in(c, cat, cat->nclus, on_device, &m));
+  ASOHF_CHECK(cat_mirror_in(c, cat, cat->nclus, on_device, &m, lowh1 - 1, true));
   int32_t* hw;
   int ns;
   ASOHF_CHECK(make_sub_work(c, m, lowh1, lowh2, &hw, &ns));
