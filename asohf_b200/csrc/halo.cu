@@ -336,7 +336,7 @@ struct GrowCaps {
 // Recentering + growth of HALOFIND_PARTICLES (haloes_particles.f:741-849);
 // with resume set, the growth restarts from the saved centre and radius.
 template <int C>
-__global__ void __launch_bounds__(HB)
+__global__ void __launch_bounds__(HB, 3)
 k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, asohf_catalogue cat,
             const int32_t* __restrict__ work, GrowOut o, GrowCaps caps, int resume) {
   __shared__ RecShared sh;
@@ -1001,6 +1001,8 @@ struct GShared {
   double bc_d[2];
   long long bc_l[2];
   double at[16];
+  double wsum[32];  // per-warp totals of the scans
+  long long wcnt[32];
   GX x;
 };
 
@@ -1100,6 +1102,7 @@ __device__ void centromasas_g(const Grp<C>& g, const SegView& v, int64_t n, floa
   double a[7] = {0, 0, 0, 0, 0, 0, 0};
   int64_t lo, hi;
   g.chunk(0, n, &lo, &hi);
+#pragma unroll 4
   for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
     float4 q = v.mv[j], p = v.px[j];
     double bas = (double)q.x;
@@ -1127,34 +1130,39 @@ __device__ void centromasas_g(const Grp<C>& g, const SegView& v, int64_t n, floa
 template <int C>
 __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& dst, const uint8_t* flag,
                           int64_t k2, int64_t* idx_vir, int64_t* k2new, GShared& sh) {
-  int64_t lo, hi;
+  int64_t lo, hi, wlo, whi;
   g.chunk(0, k2, &lo, &hi);
-  long long mine = 0;
-  if constexpr (C > 1) {
-    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) mine += flag[j];
-    mine = block_sum_ll(mine, sh.lred);
-  }
-  long long off = 0, tot = 0;
-  gexcl_ll(g, mine, &off, &tot, sh.x);
-  int64_t carry = off;
+  warp_run(lo, hi, &wlo, &whi);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  long long cnt = 0;
+#pragma unroll 4
+  for (int64_t j = wlo + lane; j < whi; j += 32) cnt += flag[j];
+  cnt = warp_allsum_ll(cnt);
+  if (lane == 0) sh.wcnt[w] = cnt;
+  __syncthreads();
+  const long long woff = warp_allsum_ll(lane < w ? sh.wcnt[lane] : 0);
+  const long long ctot = warp_allsum_ll(lane < nw ? sh.wcnt[lane] : 0);
+  long long off = 0, tot = ctot;
+  if constexpr (C > 1) gexcl_ll(g, ctot, &off, &tot, sh.x);
+  int64_t d0 = off + woff;
   long long reloc = LLONG_MAX;
-  int64_t iv = *idx_vir;  // 1-based
-  for (int64_t t0 = lo; t0 < hi; t0 += blockDim.x) {
-    int64_t j = t0 + threadIdx.x;
-    bool keep = j < hi && flag[j];
-    int tt;
-    int inc = block_scan_i(keep ? 1 : 0, sh.sb, &tt);
-    int64_t d = carry + inc - 1;
+  const int64_t iv = *idx_vir;  // 1-based
+  const unsigned below = (1u << lane) - 1u;
+#pragma unroll 2
+  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
+    const int64_t j = j0 + lane;
+    const bool keep = j < whi && flag[j];
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
     if (keep) {
+      const int64_t d = d0 + __popc(m & below);
       dst.d[d] = src.d[j];
       dst.mv[d] = src.mv[j];
       dst.px[d] = src.px[j];
       if (j + 1 >= iv && d + 1 < reloc) reloc = d + 1;
     }
-    carry += tt;
-    __syncthreads();
+    d0 += __popc(m);
   }
-  int64_t nn = (C == 1) ? carry : tot;
+  const int64_t nn = tot;
   g.chunk(nn, k2, &lo, &hi);
   for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
     dst.d[j] = src.d[j];
@@ -1185,21 +1193,21 @@ __device__ void unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int
     }
     int64_t jj = a + 1;
     // cumulative mass MASA8 (kept in pot for now)
-    gprefix_d(g, 0, k2, 0.0, [&](int64_t j) { return (double)v.mv[j].x / norma; },
-              [&](int64_t j, double s) { pot[j] = s; }, sh.dred, sh.x);
+    gscan_d(g, 0, k2, 0.0, [&](int64_t j) { return (double)v.mv[j].x / norma; },
+              [&](int64_t j, double s) { pot[j] = s; }, sh.wsum, sh.x);
     g.sync();
     double mk2 = pot[k2 - 1];
     double mjj = (jj == k2 + 1) ? mk2 : pot[jj - 1];
     double pot_jj = mjj / (double)v.d[jj - 1];
     // POT(J) for J > JJ: POT(J-1) + MASA8*BAS8/DISTA(J)^2
-    gprefix_d(g, jj, k2, pot_jj,
+    gscan_d(g, jj, k2, pot_jj,
               [&](int64_t j) {
                 float dj = v.d[j], dm = v.d[j - 1];
                 double bas8 = (dj != dm) ? (double)__fsub_rn(dj, dm) : 0.0;
                 double djd = (double)dj;
                 return pot[j] * bas8 / (djd * djd);
               },
-              [&](int64_t j, double s) { pot[j] = s; }, sh.dred, sh.x);
+              [&](int64_t j, double s) { pot[j] = s; }, sh.wsum, sh.x);
     int64_t lo, hi;
     g.chunk(0, jj < k2 ? jj : k2, &lo, &hi);
     for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) pot[j] = pot_jj;
@@ -1212,6 +1220,7 @@ __device__ void unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int
     bb = __fmul_rn(bb, bb);
     double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // 7 sums and the kept count
     g.chunk(0, k2, &lo, &hi);
+#pragma unroll 4
     for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
       float potok = (float)((pot[j] - pot1) * aa8);
       float vesc2 = __fmul_rn(2.0f, fabsf(potok));
@@ -1255,6 +1264,7 @@ __device__ void unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, con
     int64_t lo, hi;
     g.chunk(0, idx_vir < k2 ? idx_vir : k2, &lo, &hi);
     double s2 = 0.0;
+#pragma unroll 4
     for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
       float4 q = v.mv[j];
       float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
@@ -1265,6 +1275,7 @@ __device__ void unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, con
     double thr = (double)bb * sigma2;
     double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     g.chunk(0, k2, &lo, &hi);
+#pragma unroll 4
     for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
       float4 q = v.mv[j];
       float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
@@ -1310,7 +1321,7 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
   double acc[18];
   for (int q = 0; q < 18; q++) acc[q] = 0.0;
   float vmax = -1.0f;
-  gprefix_d(g, 0, konta, 0.0,
+  gscan_d(g, 0, konta, 0.0,
             [&](int64_t j) {
               float4 p = v.px[j];
               float a = dist3(p.x, p.y, p.z, cx, cy, cz);
@@ -1354,7 +1365,7 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
               }
               acc[15] += (double)__fdiv_rn(mp, norma);
             },
-            sh.dred, sh.x);
+            sh.wsum, sh.x);
   // the inertia tensor is symmetric by construction of its entries; only the
   // six distinct sums are reduced
   double r[13] = {acc[0], acc[2], acc[3], acc[4], acc[5], acc[6], acc[7], acc[9], acc[10], acc[13],
@@ -1396,7 +1407,7 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
 }
 
 template <int C>
-__global__ void __launch_bounds__(HB)
+__global__ void __launch_bounds__(HB, 3)
 k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogue cat,
             const int32_t* __restrict__ work, GrowOut go, SegG sg) {
   __shared__ GShared sh;
@@ -1431,7 +1442,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                            __fdiv_rn(__fmul_rn(4.0f, pi), 3.0f));
     float cvir = __fmul_rn(H.contrastec, fdm);
     long long best = LLONG_MAX;
-    gprefix_d(g, 0, idx_vir, 0.0, [&](int64_t j) { return (double)cur.mv[j].x; },
+    gscan_d(g, 0, idx_vir, 0.0, [&](int64_t j) { return (double)cur.mv[j].x; },
               [&](int64_t j, double menc) {
                 if (j + 1 <= jjcore) return;
                 float d = cur.d[j];
@@ -1439,7 +1450,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                 float delta = (float)(menc / (double)den);
                 if (delta < cvir && (long long)(j + 1) < best) best = j + 1;
               },
-              sh.dred, sh.x);
+              sh.wsum, sh.x);
     gmin_llv<1>(g, &best, sh.lred, sh.x);
     if (best == LLONG_MAX) {
       if (lead) sg.status[slot] = ASOHF_ERR_NOT_PREFOUND_VIRIAL;
@@ -1509,7 +1520,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   // pass A: virial crossing and the crossings at or before it
   long long jt[7];
   for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
-  gprefix_d(g, 0, k2, 0.0, mn_of,
+  gscan_d(g, 0, k2, 0.0, mn_of,
             [&](int64_t j, double bas8) {
               int64_t J = j + 1;
               if (J <= jjcore) return;
@@ -1519,7 +1530,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                 if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
               if (delta2 <= cvir && J > jvir_min && J < jt[6]) jt[6] = J;
             },
-            sh.dred, sh.x);
+            sh.wsum, sh.x);
   gmin_llv<7>(g, jt, sh.lred, sh.x);
   long long jvir = jt[6];
   double mvir = 0.0;
@@ -1529,7 +1540,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     for (int q = 0; q < 6; q++)
       if (jt[q] > jvir) { jt[q] = LLONG_MAX; again = true; }
     if (again) {  // pass A2: crossings after the virial one, with BAS8 - m(J_vir)
-      gprefix_d(g, 0, k2, 0.0, mn_of,
+      gscan_d(g, 0, k2, 0.0, mn_of,
                 [&](int64_t j, double bas8) {
                   int64_t J = j + 1;
                   if (J <= jvir) return;
@@ -1539,7 +1550,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                   for (int q = 0; q < 6; q++)
                     if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
                 },
-                sh.dred, sh.x);
+                sh.wsum, sh.x);
       gmin_llv<6>(g, jt, sh.lred, sh.x);
     }
   }
@@ -1553,7 +1564,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   long long best_j = LLONG_MAX;
   double best_b = 0.0;
   int64_t jv = jvir != LLONG_MAX ? jvir : jend;
-  gprefix_d(g, 0, jend, 0.0, mn_of,
+  gscan_d(g, 0, jend, 0.0, mn_of,
             [&](int64_t j, double bas8) {
               int64_t J = j + 1;
               double b8 = (jvir != LLONG_MAX && J > jvir) ? bas8 - mvir : bas8;
@@ -1568,7 +1579,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                 best_b = b8;
               }
             },
-            sh.dred, sh.x);
+            sh.wsum, sh.x);
   __syncthreads();
   double sv[11];
   for (int q = 0; q < 8; q++) sv[q] = threadIdx.x == 0 ? sh.at[q] : 0.0;

@@ -293,8 +293,10 @@ __device__ __forceinline__ int col_index(float v, float xl, float cdx, int n) {
 
 // Calls f(e) for every column-index entry whose x, y, z lie within r' >= r
 // of (cx, cy, cz) (a superset of any open-cube or sphere test of radius r).
-// Warp w of nw takes columns w, w+nw, ...; its lanes binary-search the x
-// ranges of 32 of those columns at once, then stride through each range.
+// When the query has fewer columns than twice the warps, each column's x
+// range is cut into parts so every warp gets work.  Warp w of nw takes
+// (column, part) items w, w+nw, ...; its lanes binary-search the x ranges of
+// 32 items at once, then stride through each range.
 template <class F>
 __device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy, float cz, float r, int w0, int nw,
                                            F&& f) {
@@ -304,11 +306,14 @@ __device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy
   float xlo = cx - rr, xhi = cx + rr;
   int ny = iy1 - iy0 + 1;
   int ncols = ny * (iz1 - iz0 + 1);
+  int parts = ncols >= 2 * nw ? 1 : (2 * nw + ncols - 1) / ncols;
+  int nitems = ncols * parts;
   int lane = threadIdx.x & 31;
-  for (int base = 0; w0 + base * nw < ncols; base += 32) {
-    int c = w0 + (base + lane) * nw;
+  for (int base = 0; w0 + base * nw < nitems; base += 32) {
+    int it = w0 + (base + lane) * nw;
     int64_t s = 0, e = 0;
-    if (c < ncols) {
+    if (it < nitems) {
+      int c = it / parts, part = it - c * parts;
       int64_t cid = (int64_t)(iz0 + c / ny) * ci.ncol + iy0 + c % ny;
       int64_t a = ci.start[cid], b = ci.start[cid + 1];
       int64_t lo = a, hi = b;
@@ -323,9 +328,17 @@ __device__ __forceinline__ void query_box_w(const ColIdx& ci, float cx, float cy
         if (ci.cp[mid].x <= xhi) lo = mid + 1; else hi = mid;
       }
       e = lo;
+      if (parts > 1) {
+        int64_t len = e - s, per = (len + parts - 1) / parts;
+        int64_t ps = s + (per * part < len ? per * part : len);
+        int64_t pe = s + (per * (part + 1) < len ? per * (part + 1) : len);
+        s = ps;
+        e = pe;
+      }
     }
-    for (int q = 0; q < 32 && w0 + (base + q) * nw < ncols; q++) {
+    for (int q = 0; q < 32 && w0 + (base + q) * nw < nitems; q++) {
       int64_t sq = __shfl_sync(0xffffffffu, s, q), eq = __shfl_sync(0xffffffffu, e, q);
+#pragma unroll 4
       for (int64_t k = sq + lane; k < eq; k += 32) f(ci.cp[k]);
     }
   }
@@ -555,22 +568,60 @@ __device__ __forceinline__ double tile_prefix_d(int64_t a, int64_t b, double car
   return carry;
 }
 
-// Inclusive prefix over [a, b) split across the group: each CTA scans its
-// chunk after adding the totals of the chunks before it.  Returns
-// carry + total.  With C > 1 `val` is evaluated twice per element.
+__device__ __forceinline__ double warp_allsum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ long long warp_allsum_ll(long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Contiguous run of [lo, hi) taken by warp w of nw.
+__device__ __forceinline__ void warp_run(int64_t lo, int64_t hi, int64_t* wlo, int64_t* whi) {
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int64_t n = hi - lo, per = (n + nw - 1) / nw;
+  *wlo = lo + (per * w < n ? per * w : n);
+  *whi = lo + (per * (w + 1) < n ? per * (w + 1) : n);
+}
+
+// Inclusive prefix over [a, b) in index order: val(j) gives the term,
+// use(j, prefix) consumes it.  The range is split into the group's CTA
+// chunks and each chunk into one contiguous run per warp; a first pass sums
+// the runs, a second walks each run 32 entries at a time with a warp scan,
+// starting from the totals of everything before it, so a CTA synchronises a
+// fixed number of times per call whatever the length.  val is evaluated
+// twice per entry.  Returns carry + the group total; ends synchronised.
 template <int C, class V, class U>
-__device__ __forceinline__ double gprefix_d(const Grp<C>& g, int64_t a, int64_t b, double carry, V val, U use,
-                                            double* sbuf, GX& x) {
-  int64_t lo, hi;
+__device__ __forceinline__ double gscan_d(const Grp<C>& g, int64_t a, int64_t b, double carry, V val, U use,
+                                          double* wbuf, GX& x) {
+  int64_t lo, hi, wlo, whi;
   g.chunk(a, b, &lo, &hi);
-  if constexpr (C == 1) {
-    return tile_prefix_d(lo, hi, carry, val, use, sbuf);
-  } else {
-    double part = tile_prefix_d(lo, hi, 0.0, val, [](int64_t, double) {}, sbuf);
-    double off, tot;
-    gexcl_d(g, part, &off, &tot, x);
-    tile_prefix_d(lo, hi, carry + off, val, use, sbuf);
-    g.sync();
-    return carry + tot;
+  warp_run(lo, hi, &wlo, &whi);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double t = 0.0;
+#pragma unroll 4
+  for (int64_t j = wlo + lane; j < whi; j += 32) t += val(j);
+  t = warp_allsum_d(t);
+  if (lane == 0) wbuf[w] = t;
+  __syncthreads();
+  const double woff = warp_allsum_d(lane < w ? wbuf[lane] : 0.0);
+  const double ctot = warp_allsum_d(lane < nw ? wbuf[lane] : 0.0);
+  double off = 0.0, tot = ctot;
+  if constexpr (C > 1) gexcl_d(g, ctot, &off, &tot, x);
+  double run = carry + off + woff;
+#pragma unroll 2
+  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
+    const int64_t j = j0 + lane;
+    double s = j < whi ? val(j) : 0.0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      double y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (j < whi) use(j, run + s);
+    run += __shfl_sync(0xffffffffu, s, 31);
   }
+  g.sync();
+  return carry + tot;
 }
