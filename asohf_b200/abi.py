@@ -89,16 +89,28 @@ class Catalogue:
     """Host catalogue with the driver's initial values (INIT_OUTVARS,
     alloc.f:2-193: zeros everywhere)."""
 
-    def __init__(self, capacity: int):
+    def __init__(self, capacity: int, pinned: bool = False):
+        """pinned: arrays in page-locked host memory (torch), so the library's
+        host<->device copies of the catalogue run at full PCIe speed."""
         self.capacity = int(capacity)
         self.nclus = 0
+        self._keep = []
+
+        def zeros(shape, dt):
+            if not pinned:
+                return np.zeros(shape, dt)
+            import torch
+            t = torch.zeros(shape, dtype=torch.int32 if dt == np.int32 else torch.float32).pin_memory()
+            self._keep.append(t)
+            return t.numpy()
+
         for f in CAT_SCALAR_FLOAT:
-            setattr(self, f, np.zeros(capacity, np.float32))
+            setattr(self, f, zeros(capacity, np.float32))
         for f in CAT_SCALAR_INT:
-            setattr(self, f, np.zeros(capacity, np.int32))
+            setattr(self, f, zeros(capacity, np.int32))
         for f, w in CAT_MULTI.items():
             dt = np.int32 if f == "indcs" else np.float32
-            setattr(self, f, np.zeros((capacity, w), dt))
+            setattr(self, f, zeros((capacity, w), dt))
 
     def fields(self):
         return CAT_SCALAR_FLOAT + CAT_SCALAR_INT + list(CAT_MULTI)
@@ -106,6 +118,7 @@ class Catalogue:
     def copy(self) -> "Catalogue":
         c = Catalogue.__new__(Catalogue)
         c.capacity, c.nclus = self.capacity, self.nclus
+        c._keep = []
         for f in self.fields():
             setattr(c, f, getattr(self, f).copy())
         return c

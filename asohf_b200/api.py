@@ -267,13 +267,18 @@ class Asohf:
                                                    C.byref(cc), C.c_int(ir), sl.ctypes.data_as(_ip),
                                                    C.c_int(0)), "SUBSTRUCTURE_PARTICLES")
 
-    def particles_per_halo(self) -> np.ndarray:
+    def particles_per_halo(self, out=None):
+        """The bound-particle ID stream.  out: None (a new numpy array), a
+        host numpy array or a torch CUDA tensor of at least the stream's
+        length; returns the filled prefix."""
         n = C.c_int64()
         _check(self.L.asohf_get_particles_per_halo(self.h, None, C.c_int64(0), C.byref(n), C.c_int(0)),
                "PARTICLES_PER_HALO")
-        out = np.zeros(max(n.value, 1), np.int32)
-        _check(self.L.asohf_get_particles_per_halo(self.h, out.ctypes.data_as(_ip),
-                                                   C.c_int64(out.shape[0]), C.byref(n), C.c_int(0)),
+        if out is None:
+            out = np.zeros(max(n.value, 1), np.int32)
+        on_dev = _is_torch(out) and out.is_cuda
+        _check(self.L.asohf_get_particles_per_halo(self.h, C.cast(_ptr(out), _ip),
+                                                   C.c_int64(out.shape[0]), C.byref(n), C.c_int(int(on_dev))),
                "PARTICLES_PER_HALO")
         return out[: n.value]
 
@@ -283,8 +288,11 @@ class GpuBackend:
 
     name = "gpu"
 
+    pinned_host = True  # host catalogue in page-locked memory
+
     def __init__(self, device: int = 0, cluster_threshold: int = 0, tiers=(0, 0)):
         self.a = Asohf(device)
+        self._ids = None
         if cluster_threshold:
             self.a.set_cluster_threshold(cluster_threshold)
         if tiers != (0, 0):
@@ -316,6 +324,27 @@ class GpuBackend:
         self.a.renorm_density(nx, mesh, fdm, u1, u11)
         return u1, u11[: mesh.total]
 
+    def density_renorm(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, fdm):
+        """DENSITY then RENORM_DENSITY with the grids kept on the device
+        between the two calls and copied once into page-locked host arrays
+        owned by the backend (valid until its next density_renorm)."""
+        import torch
+        n11 = max(mesh.total, 1) * abi.NAMRX ** 3
+        dev = f"cuda:{self.a.device}"
+        if getattr(self, "_g1", None) is None or self._g1.numel() != nx ** 3:
+            self._g1 = torch.empty(nx ** 3, dtype=torch.float32, device=dev)
+            self._h1 = torch.empty(nx ** 3, dtype=torch.float32).pin_memory()
+        if getattr(self, "_g11", None) is None or self._g11.numel() < n11:
+            self._g11 = torch.empty(n11, dtype=torch.float32, device=dev)
+            self._h11 = torch.empty(n11, dtype=torch.float32).pin_memory()
+        self.a.density(nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, self._g1, self._g11)
+        self.a.renorm_density(nx, mesh, fdm, self._g1, self._g11)
+        self._h1.copy_(self._g1)
+        self._h11[:n11].copy_(self._g11[:n11])
+        u1 = self._h1.numpy().reshape(nx, nx, nx)
+        u11 = self._h11[:n11].numpy().reshape(-1, abi.NAMRX ** 3)[: mesh.total]
+        return u1, u11
+
     def tsc_deposit(self, nx, lado0, dx, radx, rote, rete, mesh, fp64=True):
         u1 = np.zeros(nx ** 3, np.float32)
         u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)
@@ -335,8 +364,18 @@ class GpuBackend:
         self.a.substructure_particles(consts, mesh, cat, ir, subs_lev)
 
     def final_ids(self, pph, n):
-        """PARTICLES_PER_HALO(1:n), fetched once at the end."""
-        return self.a.particles_per_halo()[:n]
+        """PARTICLES_PER_HALO(1:n), fetched once at the end into page-locked
+        host memory owned by the backend (valid until its next final_ids)."""
+        import torch
+        cnt = C.c_int64()
+        _check(self.L_len(cnt), "PARTICLES_PER_HALO")
+        if self._ids is None or self._ids.shape[0] < max(cnt.value, 1):
+            self._ids_t = torch.empty(max(cnt.value, 1), dtype=torch.int32).pin_memory()
+            self._ids = self._ids_t.numpy()
+        return self.a.particles_per_halo(self._ids)[:n]
+
+    def L_len(self, cnt):
+        return self.a.L.asohf_get_particles_per_halo(self.a.h, None, C.c_int64(0), C.byref(cnt), C.c_int(0))
 
     def poisson_fft(self, u1, dx):
         nx = u1.shape[0]
@@ -360,6 +399,16 @@ class DeviceBackend(GpuBackend):
     def download(self):
         return None
 
+    def final_ids(self, pph, n):
+        """PARTICLES_PER_HALO(1:n), left on the device (a torch tensor owned
+        by the backend, valid until its next final_ids)."""
+        import torch
+        cnt = C.c_int64()
+        _check(self.L_len(cnt), "PARTICLES_PER_HALO")
+        if self._ids is None or self._ids.shape[0] < max(cnt.value, 1):
+            self._ids = torch.empty(max(cnt.value, 1), dtype=torch.int32, device=f"cuda:{self.a.device}")
+        return self.a.particles_per_halo(self._ids)[:n]
+
     def _grids(self, nx, mesh):
         import torch
         n11 = max(mesh.total, 1) * abi.NAMRX ** 3
@@ -377,3 +426,7 @@ class DeviceBackend(GpuBackend):
     def renorm_density(self, nx, mesh, fdm, u1, u11):
         self.a.renorm_density(nx, mesh, fdm, u1, u11)
         return u1, u11
+
+    def density_renorm(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, fdm):
+        u1, u11 = self.density(nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree)
+        return self.renorm_density(nx, mesh, fdm, u1, u11)

@@ -109,13 +109,17 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
     npe = backend.species_sort(nx, dx, cos["rodo"], cos["re0"])
     T["species_sort"] = time.perf_counter() - t0
     t0 = time.perf_counter()
-    u1, u11 = backend.density(nx, lado0, dx, cos["rote"], cos["rete"], npe, mesh, interp_degree)
-    u1, u11 = backend.renorm_density(nx, mesh, np.float32(cfg.fdm), u1, u11)
+    if hasattr(backend, "density_renorm"):  # one transfer of the grids
+        u1, u11 = backend.density_renorm(nx, lado0, dx, cos["rote"], cos["rete"], npe, mesh, interp_degree,
+                                         np.float32(cfg.fdm))
+    else:
+        u1, u11 = backend.density(nx, lado0, dx, cos["rote"], cos["rete"], npe, mesh, interp_degree)
+        u1, u11 = backend.renorm_density(nx, mesh, np.float32(cfg.fdm), u1, u11)
     T["density"] = time.perf_counter() - t0
     t0 = time.perf_counter()
     nd = backend.sort_x(nx, lado0)
     T["sort_x"] = time.perf_counter() - t0
-    cat = abi.Catalogue(plan.capacity)
+    cat = abi.Catalogue(plan.capacity, pinned=getattr(backend, "pinned_host", False))
     n_id_cap = max(snap.x.shape[0], 1)
     pph = np.zeros(n_id_cap, np.int32)
     nhallev = np.zeros(mesh.nl + 1, np.int32)

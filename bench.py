@@ -267,8 +267,9 @@ def main():
     ms_e2e = float(t.item())
     ncat = re.cat.nclus
     cat_bytes = ncat * 4 * (45 + 2 * 20 + 3 + 3 + 6 + 2)
-    h2d = n * 32
-    d2h = int(re.pph.shape[0]) * 4 + cat_bytes
+    h2d = n * 32 + cat_bytes  # particles; the catalogue windows go both ways
+    grid_bytes = 4 * (cfg.nx ** 3 + plan.mesh.total * 32 ** 3)  # U1 and U11 after RENORM_DENSITY
+    d2h = int(re.pph.shape[0]) * 4 + cat_bytes + grid_bytes
     e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "particles/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
 
