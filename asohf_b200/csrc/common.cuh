@@ -94,6 +94,10 @@ int ktime_begin(asohf_ctx* c, const char* name, cudaStream_t s);
 void ktime_end(asohf_ctx* c, int slot, cudaStream_t s);
 inline int ktime_begin(asohf_ctx* c, const char* name) { return ktime_begin(c, name, c->stream); }
 inline void ktime_end(asohf_ctx* c, int slot) { ktime_end(c, slot, c->stream); }
+// Host wall time (ms) of a phase of an entry point, added to the same
+// statistics as the kernels when profiling is on.
+double htime_now();
+void htime_end(asohf_ctx* c, const char* name, double t0);
 
 // Scratch: reserve() may grow the arena only when nothing is allocated from it.
 int arena_reserve(asohf_ctx* c, size_t bytes);

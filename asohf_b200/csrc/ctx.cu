@@ -1,6 +1,7 @@
 // ctx.cu -- context lifetime, scratch arena, device particle store.
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "common.cuh"
 
@@ -231,6 +232,31 @@ int ktime_begin(asohf_ctx* c, const char* name, cudaStream_t s) {
 void ktime_end(asohf_ctx* c, int slot, cudaStream_t s) {
   if (slot < 0) return;
   cudaEventRecord(c->krec[slot].b, s);
+}
+
+static void ksum_add(asohf_ctx* c, const char* name, double ms) {
+  int k;
+  for (k = 0; k < c->nksum; k++)
+    if (strcmp(c->ksum[k].name, name) == 0) break;
+  if (k == c->nksum) {
+    if (c->nksum >= 64) return;
+    c->ksum[k].name = name;
+    c->ksum[k].ms = 0.0;
+    c->ksum[k].n = 0;
+    c->nksum++;
+  }
+  c->ksum[k].ms += ms;
+  c->ksum[k].n++;
+}
+
+double htime_now() {
+  timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec * 1e3 + (double)t.tv_nsec * 1e-6;
+}
+
+void htime_end(asohf_ctx* c, const char* name, double t0) {
+  if (c->profiling) ksum_add(c, name, htime_now() - t0);
 }
 
 static void ktime_flush(asohf_ctx* c) {

@@ -198,6 +198,7 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
   if (low2 < low1) return ASOHF_OK;
   if (do_need_to_count == 1 && c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
   ASOHF_CUDA(cudaSetDevice(c->device));
+  double ht = htime_now();
   arena_reset(c);
   ASOHF_CHECK(arena_reserve(c, cat_bytes(low2) + 4096));
   CatMirror m;
@@ -215,6 +216,7 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
   ASOHF_CUDA(cudaGetLastError());
   ASOHF_CHECK(cat_mirror_out(c, &m));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  htime_end(c, "host:prune", ht);
   return ASOHF_OK;
 }
 
@@ -1177,7 +1179,7 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
 
 // UNBINDING8 (haloes_particles.f:1828-1983) on the staged list.
 template <int C>
-__device__ void unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int fac, float ref_max,
+__device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int fac, float ref_max,
                              const SegView& v, uint8_t* flag, double* pot, int64_t k2, int64_t idx_vir,
                              HaloState& h, GShared& sh) {
   float cm[3] = {0, 0, 0}, vcm[3] = {0, 0, 0}, mmm = 0.0f;
@@ -1187,6 +1189,27 @@ __device__ void unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int
     float lim = __fmul_rn(0.01f, ref_max);
     // first J with DISTA(J) > lim (the list is sorted by distance); K2+1 if none
     int64_t a = 0, b = k2;
+    if (k2 > 4096) {  // narrow the range with one parallel probe per thread of the CTA
+      const int64_t step = (k2 + blockDim.x - 1) / blockDim.x;
+      const int64_t jp = (int64_t)threadIdx.x * step;
+      bool above = jp < k2 && v.d[jp] > lim;
+      __syncthreads();
+      unsigned m = __ballot_sync(0xffffffffu, above);
+      if ((threadIdx.x & 31) == 0) sh.wcnt[threadIdx.x >> 5] = m ? (long long)((threadIdx.x & ~31) + __ffs(m) - 1) : LLONG_MAX;
+      __syncthreads();
+      long long fp = LLONG_MAX;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) fp = sh.wcnt[w] < fp ? sh.wcnt[w] : fp;
+      __syncthreads();
+      // probes are sorted: the answer lies in (probe fp-1, probe fp]
+      if (fp == LLONG_MAX) {  // after the last probe inside the list
+        int64_t lastp = (k2 - 1) / step;
+        if (lastp > (int64_t)blockDim.x - 1) lastp = (int64_t)blockDim.x - 1;
+        a = lastp * step + 1;
+      } else {
+        b = fp * step;
+        a = fp > 0 ? (fp - 1) * step + 1 : 0;
+      }
+    }
     while (a < b) {
       int64_t mid = (a + b) >> 1;
       if (v.d[mid] > lim) b = mid; else a = mid + 1;
@@ -1250,11 +1273,12 @@ __device__ void unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int
     }
   }
   unbind_result(h, konta3, cm, vcm, mmm, H.um);
+  return konta3;
 }
 
 // UNBINDING_SIGMA (haloes_particles.f:1987-2095) on the staged list.
 template <int C>
-__device__ void unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, const SegView& v, uint8_t* flag,
+__device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, const SegView& v, uint8_t* flag,
                                   int64_t k2, int64_t idx_vir, HaloState& h, GShared& sh) {
   float bb = fmaxf(__fsub_rn(6.0f, __fmul_rn(1.0f, (float)(fac - 1))), 3.0f);
   bb = __fmul_rn(bb, bb);
@@ -1306,6 +1330,7 @@ __device__ void unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, con
     }
   }
   unbind_result(h, konta3, cm, vcm, mmm, H.um);
+  return konta3;
 }
 
 // Bound-particle properties (haloes_particles.f:1187-1353) over j < konta of
@@ -1469,11 +1494,13 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     fac++;
     int64_t prev = k2;
     ep += (unsigned long long)k2;
-    unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, idx_vir, h, sh);
-    int64_t nk2;
-    compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
-    SegView t = cur; cur = nxt; nxt = t; which ^= 1;
-    k2 = nk2;
+    long long kept = unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, idx_vir, h, sh);
+    if (kept != k2) {  // nothing removed: the list, IDX_VIR and the tail stay as they are
+      int64_t nk2;
+      compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
+      SegView t = cur; cur = nxt; nxt = t; which ^= 1;
+      k2 = nk2;
+    }
     ref_max = k2 > 0 ? cur.d[k2 - 1] : 1.e10f;
     contaerr = prev - k2;
     if (fac > 100000) break;
@@ -1485,11 +1512,13 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     fac++;
     int64_t prev = k2;
     ep += (unsigned long long)k2;
-    unbinding_sigma_g(g, H, fac, cur, flag, k2, idx_vir, h, sh);
-    int64_t nk2;
-    compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
-    SegView t = cur; cur = nxt; nxt = t; which ^= 1;
-    k2 = nk2;
+    long long kept = unbinding_sigma_g(g, H, fac, cur, flag, k2, idx_vir, h, sh);
+    if (kept != k2) {
+      int64_t nk2;
+      compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
+      SegView t = cur; cur = nxt; nxt = t; which ^= 1;
+      k2 = nk2;
+    }
     ref_max = k2 > 0 ? cur.d[k2 - 1] : 1.e10f;
     contaerr = prev - k2;
     if (fac > 100000) break;
@@ -1933,6 +1962,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   if (c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
   if (k->do_compute_energies == 1) return ASOHF_ERR_UNSUPPORTED;
   ASOHF_CUDA(cudaSetDevice(c->device));
+  double ht = htime_now();
   arena_reset(c);
   int nh = lowh2 - lowh1 + 1;
   size_t need = cat_bytes(lowh2) + (size_t)nh * 96 + 65536;
@@ -1942,6 +1972,8 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   int32_t *hw, *hdm;
   int ns;
   ASOHF_CHECK(make_work(c, m, lowh1, lowh2, &hw, &ns, &hdm));
+  htime_end(c, "host:halo_mirror_in+work", ht);
+  ht = htime_now();
   Store S = store_of(c);
   ColIdx ci = col_idx(c, k);
   HConst H = hconst(k, mesh);
@@ -2004,6 +2036,8 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     }
     free(hesc);
     free(kesc);
+    htime_end(c, "host:halo_grow", ht);
+    ht = htime_now();
     hoff[0] = 0;
     bool left = false;  // haloes no group size could finish (not expected)
     for (int s = 0; s < ns; s++) {
@@ -2071,6 +2105,9 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     }
     sg.keys = k1;
     sg.vals = v1;
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    htime_end(c, "host:halo_gather_sort", ht);
+    ht = htime_now();
     {
       int kt_ = ktime_begin(c, "halo_main");
       LAUNCH_TIERS(k_halo_main, CB, tm, S, H, m.d, d_work, g, sg);
@@ -2081,6 +2118,8 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
     for (int s = 0; s < ns; s++)
       if (hst[s] && !rc) rc = hst[s];
+    htime_end(c, "host:halo_main", ht);
+    ht = htime_now();
     if (H.want_ids && rc == ASOHF_OK) {
       int64_t total;
       ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, ns, d_nbound, d_ids_off, &total));
@@ -2102,8 +2141,11 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   }
   free(hw);
   free(hdm);
+  htime_end(c, "host:halo_ids", ht);
+  ht = htime_now();
   ASOHF_CHECK(cat_mirror_out(c, &m));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  htime_end(c, "host:halo_mirror_out", ht);
   return rc;
 }
 
@@ -2719,6 +2761,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   if (lowh2 > cat->nclus) return ASOHF_ERR_INVALID;
   if (lowh2 < lowh1) return ASOHF_OK;
   ASOHF_CUDA(cudaSetDevice(c->device));
+  double ht = htime_now();
   arena_reset(c);
   int nh = lowh2 - lowh1 + 1;
   size_t need = cat_bytes(cat->nclus) + (size_t)nh * 160 + 65536;
@@ -2728,6 +2771,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   int32_t* hw;
   int ns;
   ASOHF_CHECK(make_sub_work(c, m, lowh1, lowh2, &hw, &ns));
+  htime_end(c, "host:sub_mirror_in+work", ht);
+  ht = htime_now();
   Store S = store_of(c);
   ColIdx ci = col_idx(c, k);
   HConst H = hconst(k, mesh);
@@ -2777,6 +2822,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       if (h_st[s]) rc = h_st[s];
       else h_act[na++] = s;
     }
+    htime_end(c, "host:sub_prep", ht);
+    ht = htime_now();
     // Jacobi radius, growing the unresolved ones
     int32_t* d_pos = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     if (!d_pos) rc = ASOHF_ERR_CAPACITY;
@@ -2811,6 +2858,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
         if (!h_done[q]) h_act[nn++] = h_act[q];
       na = nn;
     }
+    htime_end(c, "host:sub_jacobi_loop", ht);
+    ht = htime_now();
     if (rc == ASOHF_OK) {
       // last gather of every subhalo at its final radius, then the main pass
       unsigned long long* keys;
@@ -2818,6 +2867,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       int64_t T;
       ASOHF_CHECK(gather_sorted(c, S, ci, ns, d_pos, pr.cx, pr.cy, pr.cz, f_rlast, d_konta, d_off, h_off, &keys,
                                 &vals, &T, true));
+      htime_end(c, "host:sub_final_gather", ht);
+      ht = htime_now();
       Seg sg;
       sg.konta = d_konta;
       sg.off = d_off;
@@ -2849,6 +2900,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
       for (int s = 0; s < ns; s++)
         if (h_st[s] && !rc) rc = h_st[s];
+      htime_end(c, "host:sub_main", ht);
+      ht = htime_now();
       if (H.want_ids && rc == ASOHF_OK) {
         int64_t total;
         ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, ns, d_nbound, d_ids_off, &total));
@@ -2870,7 +2923,10 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
     c->pph_len = total;
   }
   free(hw);
+  htime_end(c, "host:sub_ids", ht);
+  ht = htime_now();
   ASOHF_CHECK(cat_mirror_out(c, &m));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  htime_end(c, "host:sub_mirror_out", ht);
   return rc;
 }
