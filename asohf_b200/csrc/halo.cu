@@ -962,19 +962,19 @@ k_sub_write_ids(const int32_t* __restrict__ nscan, const int64_t* __restrict__ o
 // length are copied from the old list, so both sets hold what the in-place
 // compaction would leave there (DISTA(K2+1) is read by the next UNBINDING8).
 struct SegBuf {
-  float* d;
+  float2* dm;  // (distance, mass): what the cumulative-mass scans read
   float4* mv;  // (m, vx, vy, vz)
   float4* px;  // (x, y, z, x-sorted position as int bits)
 };
 
 struct SegView {
-  float* d;
+  float2* dm;
   float4* mv;
   float4* px;
 };
 
 __device__ __forceinline__ SegView view_at(const SegBuf& b, int64_t base) {
-  return SegView{b.d + base, b.mv + base, b.px + base};
+  return SegView{b.dm + base, b.mv + base, b.px + base};
 }
 
 struct SegG {
@@ -1004,6 +1004,7 @@ struct GShared {
   long long bc_l[2];
   double at[16];
   double wsum[32];  // per-warp totals of the scans
+  double wsum3[96];
   long long wcnt[32];
   GX x;
 };
@@ -1084,13 +1085,14 @@ __device__ void load_segment(const Grp<C>& g, const Store& S, const unsigned lon
   for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
     unsigned long long kk = keys[j];
     int p = vals[j];
-    a.d[j] = __uint_as_float((uint32_t)(kk & 0xffffffffull));
-    a.mv[j] = make_float4(S.m[p], S.vx[p], S.vy[p], S.vz[p]);
+    float mp = S.m[p];
+    a.dm[j] = make_float2(__uint_as_float((uint32_t)(kk & 0xffffffffull)), mp);
+    a.mv[j] = make_float4(mp, S.vx[p], S.vy[p], S.vz[p]);
     a.px[j] = make_float4(S.x[p], S.y[p], S.z[p], __int_as_float(p));
     flag[j] = 1;
   }
   if (g.rank() == 0 && threadIdx.x == 0) {  // DISTA(K+1) of the sorted list
-    a.d[K] = 1.e10f; b.d[K] = 1.e10f;
+    a.dm[K] = make_float2(1.e10f, 0.f); b.dm[K] = a.dm[K];
     a.mv[K] = make_float4(0.f, 0.f, 0.f, 0.f); b.mv[K] = a.mv[K];
     a.px[K] = make_float4(0.f, 0.f, 0.f, 0.f); b.px[K] = a.px[K];
   }
@@ -1157,7 +1159,7 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     if (keep) {
       const int64_t d = d0 + __popc(m & below);
-      dst.d[d] = src.d[j];
+      dst.dm[d] = src.dm[j];
       dst.mv[d] = src.mv[j];
       dst.px[d] = src.px[j];
       if (j + 1 >= iv && d + 1 < reloc) reloc = d + 1;
@@ -1167,7 +1169,7 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
   const int64_t nn = tot;
   g.chunk(nn, k2, &lo, &hi);
   for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-    dst.d[j] = src.d[j];
+    dst.dm[j] = src.dm[j];
     dst.mv[j] = src.mv[j];
     dst.px[j] = src.px[j];
   }
@@ -1192,7 +1194,7 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
     if (k2 > 4096) {  // narrow the range with one parallel probe per thread of the CTA
       const int64_t step = (k2 + blockDim.x - 1) / blockDim.x;
       const int64_t jp = (int64_t)threadIdx.x * step;
-      bool above = jp < k2 && v.d[jp] > lim;
+      bool above = jp < k2 && v.dm[jp].x > lim;
       __syncthreads();
       unsigned m = __ballot_sync(0xffffffffu, above);
       if ((threadIdx.x & 31) == 0) sh.wcnt[threadIdx.x >> 5] = m ? (long long)((threadIdx.x & ~31) + __ffs(m) - 1) : LLONG_MAX;
@@ -1212,30 +1214,35 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
     }
     while (a < b) {
       int64_t mid = (a + b) >> 1;
-      if (v.d[mid] > lim) b = mid; else a = mid + 1;
+      if (v.dm[mid].x > lim) b = mid; else a = mid + 1;
     }
     int64_t jj = a + 1;
-    // cumulative mass MASA8 (kept in pot for now)
-    gscan_d(g, 0, k2, 0.0, [&](int64_t j) { return (double)v.mv[j].x / norma; },
-              [&](int64_t j, double s) { pot[j] = s; }, sh.wsum, sh.x);
-    g.sync();
-    double mk2 = pot[k2 - 1];
-    double mjj = (jj == k2 + 1) ? mk2 : pot[jj - 1];
-    double pot_jj = mjj / (double)v.d[jj - 1];
-    // POT(J) for J > JJ: POT(J-1) + MASA8*BAS8/DISTA(J)^2
-    gscan_d(g, jj, k2, pot_jj,
-              [&](int64_t j) {
-                float dj = v.d[j], dm = v.d[j - 1];
-                double bas8 = (dj != dm) ? (double)__fsub_rn(dj, dm) : 0.0;
-                double djd = (double)dj;
-                return pot[j] * bas8 / (djd * djd);
-              },
-              [&](int64_t j, double s) { pot[j] = s; }, sh.wsum, sh.x);
+    // MASA8 and the POT recurrence of haloes_particles.f:1870-1893 in one
+    // scan: POT(J) = POT(JJ) + Q(J), Q(J) = sum over JJ < I <= J of
+    // MASA8(I) * BAS8(I) / DISTA(I)^2; pot[] receives Q
+    double mk2, qk2, mjj_part = 0.0;
+    gscan_aff(
+        g, 0, k2, [&](int64_t j) { return (double)v.dm[j].y / norma; },
+        [&](int64_t j) {
+          if (j < jj) return 0.0;
+          float dj = v.dm[j].x, dm1 = v.dm[j - 1].x;
+          double bas8 = (dj != dm1) ? (double)__fsub_rn(dj, dm1) : 0.0;
+          double djd = (double)dj;
+          return bas8 / (djd * djd);
+        },
+        [&](int64_t j, double M, double Q) {
+          pot[j] = Q;
+          if (j == jj - 1) mjj_part = M;
+        },
+        sh.wsum3, sh.x, &mk2, &qk2);
+    double mjj = mk2;
+    if (jj <= k2) {
+      gsum_dv<1>(g, &mjj_part, sh.x);
+      mjj = mjj_part;
+    }
+    double pot_jj = mjj / (double)v.dm[jj - 1].x;
+    double pot1 = (pot_jj + qk2) + mk2 / (double)ref_max;
     int64_t lo, hi;
-    g.chunk(0, jj < k2 ? jj : k2, &lo, &hi);
-    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) pot[j] = pot_jj;
-    g.sync();
-    double pot1 = pot[k2 - 1] + mk2 / (double)ref_max;
     double aa8 = norma * (double)__fdiv_rn(H.cgr, H.rete);
     float bb = 2.0f;
     if (fac == 1) bb = 8.0f;
@@ -1245,7 +1252,7 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
     g.chunk(0, k2, &lo, &hi);
 #pragma unroll 4
     for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      float potok = (float)((pot[j] - pot1) * aa8);
+      float potok = (float)(((pot_jj + pot[j]) - pot1) * aa8);
       float vesc2 = __fmul_rn(2.0f, fabsf(potok));
       float4 q = v.mv[j];
       float ax = __fsub_rn(q.y, h.v[0]), ay = __fsub_rn(q.z, h.v[1]), az = __fsub_rn(q.w, h.v[2]);
@@ -1455,7 +1462,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   const float pi = H.pi, rote = H.rote, rete = H.rete, fdm = H.fdm, um = H.um;
   const float norma = S.norma;
   int64_t k2 = K, idx_vir = K;
-  float ref_max = cur.d[K - 1];
+  float ref_max = cur.dm[K - 1].x;
   HaloState h;
   h.radio = go.rclus[slot];
   h.masa = (float)(go.masadm[slot] * (double)um);
@@ -1467,10 +1474,10 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                            __fdiv_rn(__fmul_rn(4.0f, pi), 3.0f));
     float cvir = __fmul_rn(H.contrastec, fdm);
     long long best = LLONG_MAX;
-    gscan_d(g, 0, idx_vir, 0.0, [&](int64_t j) { return (double)cur.mv[j].x; },
+    gscan_d(g, 0, idx_vir, 0.0, [&](int64_t j) { return (double)cur.dm[j].y; },
               [&](int64_t j, double menc) {
                 if (j + 1 <= jjcore) return;
-                float d = cur.d[j];
+                float d = cur.dm[j].x;
                 float den = __fmul_rn(den0, __fmul_rn(__fmul_rn(d, d), d));
                 float delta = (float)(menc / (double)den);
                 if (delta < cvir && (long long)(j + 1) < best) best = j + 1;
@@ -1501,7 +1508,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
     }
-    ref_max = k2 > 0 ? cur.d[k2 - 1] : 1.e10f;
+    ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
     if (fac > 100000) break;
   }
@@ -1519,7 +1526,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
     }
-    ref_max = k2 > 0 ? cur.d[k2 - 1] : 1.e10f;
+    ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
     if (fac > 100000) break;
   }
@@ -1545,7 +1552,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                   __fmul_rn(500.0f, fdm), __fmul_rn(200.0f, fdm)};
   float cvir = __fmul_rn(H.contrastec, fdm);
   int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
-  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(cur.mv[j].x, norma); };
+  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(cur.dm[j].y, norma); };
   // pass A: virial crossing and the crossings at or before it
   long long jt[7];
   for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
@@ -1553,7 +1560,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
             [&](int64_t j, double bas8) {
               int64_t J = j + 1;
               if (J <= jjcore) return;
-              float vol = so_den(cur.d[j], rete, pi);
+              float vol = so_den(cur.dm[j].x, rete, pi);
               float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
               for (int q = 0; q < 6; q++)
                 if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
@@ -1574,7 +1581,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                   int64_t J = j + 1;
                   if (J <= jvir) return;
                   double b8 = bas8 - mvir;
-                  float vol = so_den(cur.d[j], rete, pi);
+                  float vol = so_den(cur.dm[j].x, rete, pi);
                   float delta2 = (float)((double)norma * b8 / (double)vol / (double)rote);
                   for (int q = 0; q < 6; q++)
                     if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
@@ -1601,7 +1608,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
                 if (J == jt[q]) sh.at[q] = (q == 6) ? bas8 : b8;
               if (J == jv) sh.at[7] = bas8;
               if (J <= jjcore) return;
-              float bas2 = (float)(b8 / (double)cur.d[j]);
+              float bas2 = (float)(b8 / (double)cur.dm[j].x);
               if (best_before((double)bas2, J, best_v, best_j)) {
                 best_v = bas2;
                 best_j = J;
@@ -1634,7 +1641,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     if (best_j != LLONG_MAX) {
       cat.vcmax[i0] = (float)best_v;
       cat.mcmax[i0] = (float)best_b;
-      cat.rcmax[i0] = cur.d[best_j - 1];
+      cat.rcmax[i0] = cur.dm[best_j - 1].x;
     }
     float* mo[6] = {cat.m2500c, cat.m500c, cat.m200c, cat.m2500m, cat.m500m, cat.m200m};
     float* ro[6] = {cat.r2500c, cat.r500c, cat.r200c, cat.r2500m, cat.r500m, cat.r200m};
@@ -1642,7 +1649,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     for (int q = 0; q < 6; q++) {
       if (jt[q] != LLONG_MAX && jt[q] <= jend) {
         int64_t J = jt[q];
-        float d = cur.d[J - 1];
+        float d = cur.dm[J - 1].x;
         float vol = so_den(d, rete, pi);
         float delta2 = (float)((double)norma * s_at[q] / (double)vol / (double)rote);
         mo[q][i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
@@ -2057,7 +2064,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                     (int32_t*)nullptr, (int32_t*)nullptr, (int)(T > 0 ? T : 1), 0, 32 + bits);
     size_t E = (size_t)T + ns;
-    size_t elem = (size_t)T * (8 + 8 + 4 + 4) + tb + E * (2 * (4 + 16 + 16) + 8 + 1) + 32768;
+    size_t elem = (size_t)T * (8 + 8 + 4 + 4) + tb + E * (2 * (8 + 16 + 16) + 8 + 1) + 32768;
     ASOHF_CHECK(seg_reserve(c, elem));
     unsigned long long* k0 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
     unsigned long long* k1 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
@@ -2067,10 +2074,10 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     SegG sg;
     sg.konta = g.konta;
     sg.off = d_off;
-    sg.a.d = (float*)seg_alloc(c, 4 * E);
+    sg.a.dm = (float2*)seg_alloc(c, 8 * E);
     sg.a.mv = (float4*)seg_alloc(c, 16 * E);
     sg.a.px = (float4*)seg_alloc(c, 16 * E);
-    sg.b.d = (float*)seg_alloc(c, 4 * E);
+    sg.b.dm = (float2*)seg_alloc(c, 8 * E);
     sg.b.mv = (float4*)seg_alloc(c, 16 * E);
     sg.b.px = (float4*)seg_alloc(c, 16 * E);
     sg.pot = (double*)seg_alloc(c, 8 * E);
@@ -2080,7 +2087,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.nscan = d_nscan;
     sg.work = c->d_work;
     sg.status = g.status;
-    if (!k0 || !k1 || !v0 || !v1 || !t || !sg.a.d || !sg.a.mv || !sg.a.px || !sg.b.d || !sg.b.mv || !sg.b.px ||
+    if (!k0 || !k1 || !v0 || !v1 || !t || !sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px ||
         !sg.pot || !sg.flag) {
       free(hk); free(hst); free(hoff); free(hw); free(hdm);
       return ASOHF_ERR_CAPACITY;

@@ -625,3 +625,106 @@ __device__ __forceinline__ double gscan_d(const Grp<C>& g, int64_t a, int64_t b,
   g.sync();
   return carry + tot;
 }
+
+// Prefix of the recurrence M_j = M_{j-1} + m_j, Q_j = Q_{j-1} + M_j * w_j
+// (a cumulative mass and a sum weighted by it) in one scan.  A run of
+// entries is summarised by (sum m, sum w, its own Q from zero); runs combine
+// left to right as (m1+m2, w1+w2, q1 + m1*w2 + q2).  Same run layout and
+// passes as gscan_d; use(j, M_j, Q_j) consumes the prefixes.  Returns the
+// totals (M, Q) through *mt, *qt.
+struct Aff {
+  double m, w, q;
+};
+__device__ __forceinline__ Aff aff_cat(const Aff& a, const Aff& b) {
+  return Aff{a.m + b.m, a.w + b.w, a.q + a.m * b.w + b.q};
+}
+__device__ __forceinline__ Aff aff_shfl_up(const Aff& v, int o) {
+  return Aff{__shfl_up_sync(0xffffffffu, v.m, o), __shfl_up_sync(0xffffffffu, v.w, o),
+             __shfl_up_sync(0xffffffffu, v.q, o)};
+}
+__device__ __forceinline__ Aff aff_shfl(const Aff& v, int src) {
+  return Aff{__shfl_sync(0xffffffffu, v.m, src), __shfl_sync(0xffffffffu, v.w, src),
+             __shfl_sync(0xffffffffu, v.q, src)};
+}
+// inclusive warp scan of one entry per lane
+__device__ __forceinline__ Aff aff_warp_scan(Aff v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    Aff y = aff_shfl_up(v, o);
+    if (lane >= o) v = aff_cat(y, v);
+  }
+  return v;
+}
+
+template <int C, class VM, class VW, class U>
+__device__ __forceinline__ void gscan_aff(const Grp<C>& g, int64_t a, int64_t b, VM valm, VW valw, U use,
+                                          double* wbuf /* 3 * 32 */, GX& x, double* mt, double* qt) {
+  int64_t lo, hi, wlo, whi;
+  g.chunk(a, b, &lo, &hi);
+  warp_run(lo, hi, &wlo, &whi);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // pass 1: summary of this warp's run
+  Aff run{0.0, 0.0, 0.0};
+#pragma unroll 2
+  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
+    const int64_t j = j0 + lane;
+    Aff e{0.0, 0.0, 0.0};
+    if (j < whi) {
+      e.m = valm(j);
+      e.w = valw(j);
+      e.q = e.m * e.w;
+    }
+    run = aff_cat(run, aff_shfl(aff_warp_scan(e), 31));
+  }
+  if (lane == 0) { wbuf[3 * w] = run.m; wbuf[3 * w + 1] = run.w; wbuf[3 * w + 2] = run.q; }
+  __syncthreads();
+  Aff pre{0.0, 0.0, 0.0}, tot{0.0, 0.0, 0.0};
+  for (int q = 0; q < nw; q++) {  // warps in order (every lane computes the same)
+    Aff s{wbuf[3 * q], wbuf[3 * q + 1], wbuf[3 * q + 2]};
+    if (q < w) pre = aff_cat(pre, s);
+    tot = aff_cat(tot, s);
+  }
+  if constexpr (C > 1) {  // CTAs of the cluster in rank order
+    if (threadIdx.x == 0) { x.d[0] = tot.m; x.d[1] = tot.w; x.d[2] = tot.q; }
+    g.sync();
+    if (threadIdx.x == 0) {
+      cg::cluster_group cl = cg::this_cluster();
+      Aff o{0.0, 0.0, 0.0}, t{0.0, 0.0, 0.0};
+      const unsigned me = g.rank();
+#pragma unroll 1
+      for (unsigned r = 0; r < (unsigned)C; r++) {
+        Aff s{*cl.map_shared_rank(&x.d[0], r), *cl.map_shared_rank(&x.d[1], r), *cl.map_shared_rank(&x.d[2], r)};
+        if (r == me) o = t;
+        t = aff_cat(t, s);
+      }
+      x.dres[0] = o.m; x.dres[1] = o.w; x.dres[2] = o.q;
+      x.dres[3] = t.m; x.dres[4] = t.w; x.dres[5] = t.q;
+    }
+    g.sync();
+    Aff o{x.dres[0], x.dres[1], x.dres[2]};
+    pre = aff_cat(o, pre);
+    tot = Aff{x.dres[3], x.dres[4], x.dres[5]};
+  }
+  // pass 2: prefixes
+  run = pre;
+#pragma unroll 2
+  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
+    const int64_t j = j0 + lane;
+    Aff e{0.0, 0.0, 0.0};
+    if (j < whi) {
+      e.m = valm(j);
+      e.w = valw(j);
+      e.q = e.m * e.w;
+    }
+    Aff s = aff_warp_scan(e);
+    if (j < whi) {
+      Aff p = aff_cat(run, s);
+      use(j, p.m, p.q);
+    }
+    run = aff_cat(run, aff_shfl(s, 31));
+  }
+  g.sync();
+  *mt = tot.m;
+  *qt = tot.q;
+}
