@@ -380,7 +380,7 @@ k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, aso
     long long c = 0;
     double ms = 0.0;
     float bas = -1.0f;
-    gquery_box(G, ci, cx, cy, cz, rclus, [&](const float4& e) {
+    gquery_box(G, ci, cx, cy, cz, rclus, sh.qb, [&](const float4& e) {
       int p = ppos(e);
       if (p < lo || p >= hi) return;
       float a = dist3(e.x, e.y, e.z, cx, cy, cz);
@@ -433,6 +433,7 @@ k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32
               const int64_t* __restrict__ off, const float* __restrict__ hcx, const float* __restrict__ hcy,
               const float* __restrict__ hcz, const float* __restrict__ rg, int32_t* __restrict__ fill,
               unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
+  __shared__ QBuf qb;
   Grp<C> G;
   int slot = group_slot<C>(slots);
   int kmax = konta[slot];
@@ -442,7 +443,7 @@ k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32
   slab_range(ci, cx, r, &lo, &hi);
   int64_t base = off[slot];
   unsigned long long hk = (unsigned long long)slot << 32;
-  gquery_box(G, ci, cx, cy, cz, r, [&](const float4& e) {
+  gquery_box(G, ci, cx, cy, cz, r, qb, [&](const float4& e) {
     int p = ppos(e);
     float a = dist3(e.x, e.y, e.z, cx, cy, cz);
     bool hit = p >= lo && p < hi && a < r;

@@ -349,10 +349,85 @@ __device__ __forceinline__ void query_box(const ColIdx& ci, float cx, float cy, 
   query_box_w(ci, cx, cy, cz, r, threadIdx.x >> 5, blockDim.x >> 5, f);
 }
 
+// Group query balanced by entries: every CTA finds the x ranges of all the
+// query's columns (up to QMAX) into shared memory, then the group's warps
+// take equal contiguous shares of the concatenated ranges, so a few dense
+// columns no longer keep one warp busy while the others wait.  More columns
+// than QMAX: the per-column distribution of query_box_w.
+#define QMAX 512
+struct QBuf {
+  long long s[QMAX];         // first entry of each column's x range
+  long long pre[QMAX + 1];   // prefix of the range lengths
+};
+
 template <int C, class F>
 __device__ __forceinline__ void gquery_box(const Grp<C>& g, const ColIdx& ci, float cx, float cy, float cz,
-                                           float r, F&& f) {
-  query_box_w(ci, cx, cy, cz, r, g.warp0(), g.nwarps(), f);
+                                           float r, QBuf& qb, F&& f) {
+  float rr = r * 1.0001f + 1e-6f;
+  int iy0 = col_index(cy - rr, ci.xl, ci.cdx, ci.ncol), iy1 = col_index(cy + rr, ci.xl, ci.cdx, ci.ncol);
+  int iz0 = col_index(cz - rr, ci.xl, ci.cdx, ci.ncol), iz1 = col_index(cz + rr, ci.xl, ci.cdx, ci.ncol);
+  int ny = iy1 - iy0 + 1;
+  int ncols = ny * (iz1 - iz0 + 1);
+  if (ncols > QMAX) {
+    query_box_w(ci, cx, cy, cz, r, g.warp0(), g.nwarps(), f);
+    return;
+  }
+  float xlo = cx - rr, xhi = cx + rr;
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    int64_t cid = (int64_t)(iz0 + c / ny) * ci.ncol + iy0 + c % ny;
+    int64_t a = ci.start[cid], b = ci.start[cid + 1];
+    int64_t lo = a, hi = b;
+    while (lo < hi) {  // first x >= xlo
+      int64_t mid = (lo + hi) >> 1;
+      if (ci.cp[mid].x < xlo) lo = mid + 1; else hi = mid;
+    }
+    int64_t s0 = lo;
+    hi = b;
+    while (lo < hi) {  // first x > xhi
+      int64_t mid = (lo + hi) >> 1;
+      if (ci.cp[mid].x <= xhi) lo = mid + 1; else hi = mid;
+    }
+    qb.s[c] = s0;
+    qb.pre[c + 1] = lo - s0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32) {  // prefix of the lengths, 32 columns per step
+    long long carry = 0;
+    for (int c0 = 0; c0 < ncols; c0 += 32) {
+      int c = c0 + lane;
+      long long v = c < ncols ? qb.pre[c + 1] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+      }
+      if (c < ncols) qb.pre[c + 1] = carry + v;
+      carry += __shfl_sync(0xffffffffu, v, 31);
+    }
+    if (lane == 0) qb.pre[0] = 0;
+  }
+  __syncthreads();
+  const long long E = qb.pre[ncols];
+  const int W = g.warp0(), NW = g.nwarps();
+  const long long per = (E + NW - 1) / NW;
+  long long lo = per * W < E ? per * W : E;
+  const long long hi = lo + per < E ? lo + per : E;
+  if (lo < hi) {
+    int a = 0, b = ncols - 1;  // last column with pre[c] <= lo
+    while (a < b) {
+      int mid = (a + b + 1) >> 1;
+      if (qb.pre[mid] <= lo) a = mid; else b = mid - 1;
+    }
+    for (int c = a; lo < hi && c < ncols; c++) {
+      const long long cend = qb.pre[c + 1] < hi ? qb.pre[c + 1] : hi;
+      const long long base = qb.s[c] - qb.pre[c];
+#pragma unroll 4
+      for (long long v = lo + lane; v < cend; v += 32) f(ci.cp[base + v]);
+      if (cend > lo) lo = cend;
+    }
+  }
+  __syncthreads();
 }
 
 __device__ __forceinline__ int ppos(const float4& e) { return __float_as_int(e.w); }
@@ -370,6 +445,7 @@ __device__ __forceinline__ float dist3(float x, float y, float z, float cx, floa
 }
 
 struct RecShared {
+  QBuf qb;
   double dens[64];
   float hist[MAX_HIST][4];
   double dred[32];
@@ -395,7 +471,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     slab_range(ci, cx, radio, &lo, &hi);
     long long c = 0;
     float mx = -1.e30f, mn = 1.e30f;
-    gquery_box(g, ci, cx, cy, cz, radio, [&](const float4& e) {
+    gquery_box(g, ci, cx, cy, cz, radio, sh.qb, [&](const float4& e) {
       int p = ppos(e);
       if (p >= lo && p < hi && in_cube(e.x, e.y, e.z, cx, cy, cz, radio)) {
         c++;
@@ -428,7 +504,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     for (int q = threadIdx.x; q < 64; q += blockDim.x) sh.dens[q] = 0.0;
     __syncthreads();
     bool ngp = __fdiv_rn(maxm, minm) < 8.0f;
-    gquery_box(g, ci, c0x, c0y, c0z, r0, [&](const float4& e) {
+    gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
       if (!member(e, nh)) return;
       int p = ppos(e);
       float mp = S.m[p];
@@ -506,7 +582,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     nh++;
     long long c = 0;
     float mx = -1.e30f, mn = 1.e30f;
-    gquery_box(g, ci, c0x, c0y, c0z, r0, [&](const float4& e) {
+    gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
       if (member(e, nh)) {
         c++;
         float mp = S.m[ppos(e)];
@@ -520,7 +596,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     if (cnt < 32) break;
   }
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  gquery_box(g, ci, c0x, c0y, c0z, r0, [&](const float4& e) {
+  gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
     if (member(e, nh)) {
       float mp = S.m[ppos(e)];
       v[0] += (double)mp;
