@@ -54,6 +54,8 @@ struct asohf_ctx {
   int64_t tier2_k = 4096, tier1_k = 512;
   DevParticles p;      // current store
   DevParticles alt;    // second buffer set for permutations
+  float4* rows = nullptr;  // row-packed copy of the store for permutations (2 float4 per particle)
+  int64_t rows_cap = 0;
   float norma = 0.f;   // MAXVAL(MASAP), refreshed on upload
   float mmin = 0.f;
   // x-slab index (SORT_DM_PARTICLES_X) and the column index built from it

@@ -179,6 +179,7 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaStreamSynchronize(c->stream);
   free_particles(c->p);
   free_particles(c->alt);
+  cudaFree(c->rows);
   cudaFree(c->d_ndmpart_x);
   cudaFree(c->d_colstart);
   cudaFree(c->d_colpart);

@@ -167,13 +167,27 @@ __global__ void k_species_scatter(const uint8_t* __restrict__ spec, int64_t n, i
   }
 }
 
-__global__ void k_gather8(const int64_t* __restrict__ perm, int64_t n, DevParticles s, DevParticles d) {
+// Store permutation in two passes: the store is packed row-wise (one
+// 32-byte row per particle, read and written in order), then each output
+// particle reads its whole source row with one random 32-byte access; a
+// gather straight from the eight arrays would touch eight sectors per
+// particle.
+__global__ void k_pack_rows(int64_t n, DevParticles s, float4* __restrict__ rows) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    rows[2 * i] = make_float4(s.x[i], s.y[i], s.z[i], s.m[i]);
+    rows[2 * i + 1] = make_float4(s.vx[i], s.vy[i], s.vz[i], __int_as_float(s.id[i]));
+  }
+}
+
+__global__ void k_gather_rows(const int64_t* __restrict__ perm, int64_t n, const float4* __restrict__ rows,
+                              DevParticles d) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int64_t j = perm[i];
-    d.x[i] = s.x[j]; d.y[i] = s.y[j]; d.z[i] = s.z[j];
-    d.vx[i] = s.vx[j]; d.vy[i] = s.vy[j]; d.vz[i] = s.vz[j];
-    d.m[i] = s.m[j]; d.id[i] = s.id[j];
+    float4 a = rows[2 * j], b = rows[2 * j + 1];
+    d.x[i] = a.x; d.y[i] = a.y; d.z[i] = a.z; d.m[i] = a.w;
+    d.vx[i] = b.x; d.vy[i] = b.y; d.vz[i] = b.z; d.id[i] = __float_as_int(b.w);
   }
 }
 
@@ -184,12 +198,22 @@ __global__ void k_iota(int32_t* __restrict__ a, int64_t n) {
 }
 
 int permute_store(asohf_ctx* c, const int64_t* perm) {
+  int64_t n = c->p.n;
+  if (c->rows_cap < n) {
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(c->rows);
+    c->rows = nullptr;
+    c->rows_cap = 0;
+    ASOHF_CUDA(cudaMalloc(&c->rows, 32 * (size_t)(n > 0 ? n : 1)));
+    c->rows_cap = n;
+  }
   {
     int kt_ = ktime_begin(c, "store_permute");
-    k_gather8<<<grid_for(c->p.n, 256), 256, 0, c->stream>>>(perm, c->p.n, c->p, c->alt);
+    k_pack_rows<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(n, c->p, c->rows);
+    k_gather_rows<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(perm, n, c->rows, c->alt);
     ktime_end(c, kt_);
   }
-  c->launches++;
+  c->launches += 2;
   ASOHF_CUDA(cudaGetLastError());
   ctx_swap_particles(c);
   return ASOHF_OK;
