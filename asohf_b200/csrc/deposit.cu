@@ -573,15 +573,18 @@ __global__ void k_base_stencil(const int32_t* __restrict__ cnt, int nx, Terms27 
 // slab.  Inside a CTA all warps stride over the unit's candidates as one
 // flat range.  A hit whose kernel level is 0 (27-cell cloud) is counted in
 // a host-cell grid when all masses are equal and spread by the 27-point
-// stencil at the end; every other hit deposits its clipped cloud with all 32
-// lanes of the warp, hits with the same host cell, level and mass once with
-// the group size as factor.
+// stencil at the end; every other hit deposits its clipped cloud with the
+// 32 lanes of the warp, hits with the same host cell, level and mass once
+// with the group size as factor.
 #define PZ 4              // z planes per unit
 #define PZ_BLOCK 256
 #define NSLAB (NA / PZ)
 #define PSLICE 8192       // candidates per work item
 #define PROWS 128         // bin rows staged in shared memory at a time
 #define CGX (NA + 2)      // host-cell count grid: x, y in [0, NA+1]
+#define AROW (NA + 5)     // accumulator row stride (doubles): rows shifted by 5 banks pairs
+#define APLANE (NA * AROW)
+#define ACC_N (PZ * APLANE)
 #define CGZ (PZ + 2)      //                       z in [zlo-1, zhi+1]
 
 // Offset of the centre of level l in the compact kernel table that stores
@@ -654,8 +657,8 @@ __global__ void __launch_bounds__(PZ_BLOCK, 3)
 k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t* __restrict__ S,
                   const int32_t* __restrict__ order, PatchWork W, float dx, const float* __restrict__ kernels,
                   int eqmass, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
-  extern __shared__ double acc[];  // NA*NA*PZ doubles, count grid, kernel table
-  int32_t* scnt = (int32_t*)(acc + NA * NA * PZ);
+  extern __shared__ double acc[];  // ACC_N doubles (padded rows), count grid, kernel table
+  int32_t* scnt = (int32_t*)(acc + ACC_N);
   float* ktab = (float*)(scnt + CGX * CGX * CGZ);
   __shared__ int s_lo[PROWS], s_pre[PROWS + 1];
   __shared__ double s_t27[27];
@@ -667,7 +670,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
     for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) out[q] = 0.0f;
     return;
   }
-  for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) acc[q] = 0.0;
+  for (int q = threadIdx.x; q < ACC_N; q += blockDim.x) acc[q] = 0.0;
   for (int q = threadIdx.x; q < CGX * CGX * CGZ; q += blockDim.x) scnt[q] = 0;
   for (int l = 0; l <= g.ir; l++) {
     int nk = 1 << l, c0 = ktab_center(l);
@@ -705,7 +708,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
       int64_t v = cbase + lane;
       bool hit = false;
       float mp = 0.f;
-      int ix = 0, jy = 0, kz = 0, lev = 0, i1 = 0, j1 = 0, k1 = 0, di = 0, dj = 0, vol = 0;
+      int ix = 0, jy = 0, kz = 0, lev = 0, i1 = 0, j1 = 0, k1 = 0, di = 0, dj = 0, dk = 0;
       if (v < b) {
         int lo2 = 0, hi2 = nr - 1;  // row of v: last r with s_pre[r] <= v
         while (lo2 < hi2) {
@@ -736,7 +739,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
                 hit = true;
                 di = i2 - i1 + 1;
                 dj = j2 - j1 + 1;
-                vol = di * dj * (k2 - k1 + 1);
+                dk = k2 - k1 + 1;
               }
             }
           }
@@ -764,19 +767,25 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
         int wkz = __shfl_sync(0xffffffffu, kz, src), wlev = __shfl_sync(0xffffffffu, lev, src);
         int wi1 = __shfl_sync(0xffffffffu, i1, src), wj1 = __shfl_sync(0xffffffffu, j1, src);
         int wk1 = __shfl_sync(0xffffffffu, k1, src), wdi = __shfl_sync(0xffffffffu, di, src);
-        int wdj = __shfl_sync(0xffffffffu, dj, src), wvol = __shfl_sync(0xffffffffu, vol, src);
+        int wdj = __shfl_sync(0xffffffffu, dj, src), wdk = __shfl_sync(0xffffffffu, dk, src);
         const float* kc = ktab + ktab_center(wlev);
-        // cell f of the clipped cloud: f = (kk-k1)*di*dj + (jj-j1)*di + (ii-i1); the
-        // quotients are exact in float (f < 2^13, divisors <= 32)
-        float rdi = 1.0f / (float)wdi, rdj = 1.0f / (float)wdj;
-        for (int f = lane; f < wvol; f += 32) {
-          int qa = (int)(((float)f + 0.5f) * rdi);
-          int ii = wi1 + (f - qa * wdi);
-          int qb = (int)(((float)qa + 0.5f) * rdj);
-          int jj = wj1 + (qa - qb * wdj);
-          int kk = wk1 + qb;
-          float tt = __fmul_rn(__fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]), kc[kk - wkz]);
-          atomicAdd(&acc[((kk - g.zlo) * NA + (jj - 1)) * NA + (ii - 1)], (double)tt * wc);
+        // lanes take the cloud's (ii, jj) pairs and walk its kk planes:
+        // each lane forms (m*W(ii))*W(jj) once and the plane loop reads W(kk)
+        // as a broadcast.  The pair quotient is exact in float (pairs < 2^11,
+        // divisor <= 33).
+        const int npair = wdi * wdj;
+        const float rdi = 1.0f / (float)wdi;
+        const float* wzk = kc + (wk1 - wkz);  // W(kk) of the cloud's planes
+        for (int pq = lane; pq < npair; pq += 32) {
+          int qj = (int)(((float)pq + 0.5f) * rdi);
+          int ii = wi1 + (pq - qj * wdi);
+          int jj = wj1 + qj;
+          float b = __fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]);
+          double* col = acc + (wk1 - g.zlo) * APLANE + (jj - 1) * AROW + (ii - 1);
+          for (int q = 0; q < wdk; q++) {
+            float tt = __fmul_rn(b, wzk[q]);
+            atomicAdd(col + q * APLANE, (double)tt * wc);
+          }
         }
       }
     }
@@ -795,7 +804,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
             int c = scnt[((k - kk - g.zlo + 1) * CGX + (j - jj)) * CGX + (i - ii)];
             if (c) s += (double)c * s_t27[(kk + 1) * 9 + (jj + 1) * 3 + (ii + 1)];
           }
-      acc[q] += s;
+      acc[(k - g.zlo) * APLANE + (j - 1) * AROW + (i - 1)] += s;
     }
   }
   const int sidx = W.scratch_of[it.x];
@@ -805,14 +814,16 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
     for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
       int i = q % NA, j = (q / NA) % NA, k = g.slab * PZ + q / (NA * NA);
       float v = 0.0f;
-      if (i < g.n1 && j < g.n2 && k < g.n3) v = (float)acc[q] / den;
+      if (i < g.n1 && j < g.n2 && k < g.n3) v = (float)acc[(q / (NA * NA)) * APLANE + j * AROW + i] / den;
       out[q] = v;
     }
   } else {  // one slice of a shared unit
     __syncthreads();
     double* sc = W.scratch + (size_t)sidx * NA * NA * PZ;
-    for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x)
-      if (acc[q] != 0.0) atomicAdd(&sc[q], acc[q]);
+    for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
+      double a = acc[(q / (NA * NA)) * APLANE + ((q / NA) % NA) * AROW + q % NA];
+      if (a != 0.0) atomicAdd(&sc[q], a);
+    }
   }
 }
 
@@ -1013,7 +1024,7 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
       free(hc); free(hs); free(ord); free(hitems); free(hmulti);
       PatchWork W{ditems, sof, scratch};
-      size_t smem = sizeof(double) * NA * NA * PZ + sizeof(int32_t) * CGX * CGX * CGZ + sizeof(float) * ktab_size(nl);
+      size_t smem = sizeof(double) * ACC_N + sizeof(int32_t) * CGX * CGX * CGZ + sizeof(float) * ktab_size(nl);
       ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       int kt_ = ktime_begin(c, "density_patches");
       k_density_patches<<<(unsigned)nitems, PZ_BLOCK, smem, c->stream>>>(M, B, bp, bs, order, W, dx, dk,
