@@ -776,16 +776,26 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
         const int npair = wdi * wdj;
         const float rdi = 1.0f / (float)wdi;
         const float* wzk = kc + (wk1 - wkz);  // W(kk) of the cloud's planes
+        // pair p = (jj-j1)*di + (ii-i1): the lane's first pair by division,
+        // the next ones (p += 32) by adding 32 = sj*di + si
+        int ci = lane, cj = 0;
+        {
+          int q0 = (int)(((float)lane + 0.5f) * rdi);
+          ci = lane - q0 * wdi;
+          cj = q0;
+        }
+        const int sj = (int)((32.0f + 0.5f) * rdi), si = 32 - sj * wdi;
         for (int pq = lane; pq < npair; pq += 32) {
-          int qj = (int)(((float)pq + 0.5f) * rdi);
-          int ii = wi1 + (pq - qj * wdi);
-          int jj = wj1 + qj;
+          const int ii = wi1 + ci, jj = wj1 + cj;
           float b = __fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]);
           double* col = acc + (wk1 - g.zlo) * APLANE + (jj - 1) * AROW + (ii - 1);
           for (int q = 0; q < wdk; q++) {
             float tt = __fmul_rn(b, wzk[q]);
             atomicAdd(col + q * APLANE, (double)tt * wc);
           }
+          ci += si;
+          cj += sj;
+          if (ci >= wdi) { ci -= wdi; cj++; }
         }
       }
     }
