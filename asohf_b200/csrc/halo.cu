@@ -989,9 +989,16 @@ struct SegG {
   uint8_t* final_b;         // 1: the final member list is in set b
   int32_t* nbound;          // IDs to write per slot (KONTA2 of the property loop)
   int32_t* nscan;           // entries the property loop scanned (NCAPAS)
-  unsigned long long* work; // element-pass counter
+  unsigned long long* work; // element-pass counter; with timing, [4..7] halo times
   int32_t* status;
+  int timing;               // record per-halo durations (profiling)
 };
+
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 struct GShared {
   double dred[32];
@@ -1449,6 +1456,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   const bool lead = leader(g.rank());
   const int i0 = work[slot];
   const int64_t K = go.konta[slot];
+  const unsigned long long t_start = sg.timing ? gtimer_ns() : 0ull;
   if (lead) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; sg.final_b[slot] = 0; }
   if (K == 0) return;
   const int64_t base = sg.off[slot] + slot;
@@ -1513,6 +1521,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     contaerr = prev - k2;
     if (fac > 100000) break;
   }
+  const int fac8 = fac;
   // sigma clipping (haloes_particles.f:918-933)
   fac = 0;
   contaerr = k2;
@@ -1720,6 +1729,14 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   ep += (unsigned long long)(k2 + ncapas);  // SO walk and property loop
   if (lead) {
     atomicAdd(&sg.work[0], ep);
+    if (sg.timing) {  // unbinding iterations in [2..3]; duration of this halo: max and sum,
+                      // clusters in [4..5], single CTAs in [6..7]
+      atomicAdd(&sg.work[2], (unsigned long long)fac8);
+      atomicAdd(&sg.work[3], (unsigned long long)fac);
+      unsigned long long dt = gtimer_ns() - t_start;
+      atomicMax(&sg.work[C > 1 ? 4 : 6], dt);
+      atomicAdd(&sg.work[C > 1 ? 5 : 7], dt);
+    }
     bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
@@ -2088,6 +2105,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.nscan = d_nscan;
     sg.work = c->d_work;
     sg.status = g.status;
+    sg.timing = c->profiling;
     if (!k0 || !k1 || !v0 || !v1 || !t || !sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px ||
         !sg.pot || !sg.flag) {
       free(hk); free(hst); free(hoff); free(hw); free(hdm);
