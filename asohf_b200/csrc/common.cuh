@@ -133,6 +133,10 @@ __device__ __forceinline__ int warp_sum_i(int v) {
 
 // Block-wide sum of a double, result valid in every thread.  sbuf >= 32 doubles.
 __device__ __forceinline__ double block_sum_d(double v, double* sbuf) {
+  if (blockDim.x == 32) {  // one warp: butterfly, no shared memory
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  }
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   v = warp_sum_d(v);
   __syncthreads();
@@ -151,6 +155,10 @@ __device__ __forceinline__ double block_sum_d(double v, double* sbuf) {
 }
 
 __device__ __forceinline__ long long block_sum_ll(long long v, long long* sbuf) {
+  if (blockDim.x == 32) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  }
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   __syncthreads();
@@ -169,6 +177,13 @@ __device__ __forceinline__ long long block_sum_ll(long long v, long long* sbuf) 
 }
 
 __device__ __forceinline__ long long block_min_ll(long long v, long long* sbuf) {
+  if (blockDim.x == 32) {
+    for (int o = 16; o > 0; o >>= 1) {
+      long long w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = w < v ? w : v;
+    }
+    return v;
+  }
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   for (int o = 16; o > 0; o >>= 1) {
     long long w = __shfl_down_sync(0xffffffffu, v, o);
@@ -193,6 +208,10 @@ __device__ __forceinline__ long long block_min_ll(long long v, long long* sbuf) 
 }
 
 __device__ __forceinline__ float block_max_f(float v, float* sbuf) {
+  if (blockDim.x == 32) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+  }
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
   __syncthreads();

@@ -64,6 +64,12 @@ struct GX {
 template <int K>
 __device__ __forceinline__ void block_sum_dv(double* v, GX& x) {
   static_assert(K <= 16, "at most 16 sums");
+  if (blockDim.x == 32) {  // one warp: butterflies, no shared memory
+#pragma unroll
+    for (int q = 0; q < K; q++)
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    return;
+  }
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int q = 0; q < K; q++) v[q] = warp_sum_d(v[q]);
