@@ -228,8 +228,8 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
 // passes are short and bound by latency.  The tiers run concurrently on four
 // streams.
 #define BIG_K 32768
-#define TIER2_K 4096
-#define TIER1_K 512
+#define TIER2_K 2048
+#define TIER1_K 256
 static const int kTierThreads[3] = {32, 128, 256};
 
 template <typename... P, typename... A>
@@ -434,10 +434,15 @@ k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32
               const float* __restrict__ hcz, const float* __restrict__ rg, int32_t* __restrict__ fill,
               unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
   __shared__ QBuf qb;
+  __shared__ int s_fill;  // the group's fill counter lives in rank 0's shared memory
   Grp<C> G;
   int slot = group_slot<C>(slots);
   int kmax = konta[slot];
   if (kmax == 0) return;
+  if (threadIdx.x == 0) s_fill = 0;
+  G.sync();
+  int* cnt = &s_fill;
+  if constexpr (C > 1) cnt = cg::this_cluster().map_shared_rank(&s_fill, 0);
   float cx = hcx[slot], cy = hcy[slot], cz = hcz[slot], r = rg[slot];
   int64_t lo, hi;
   slab_range(ci, cx, r, &lo, &hi);
@@ -453,7 +458,7 @@ k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32
     if (hm == 0u) return;
     int lead = __ffs(hm) - 1;
     int q0 = 0;
-    if ((int)act.thread_rank() == lead) q0 = atomicAdd(&fill[slot], __popc(hm));
+    if ((int)act.thread_rank() == lead) q0 = atomicAdd(cnt, __popc(hm));
     q0 = act.shfl(q0, lead);
     if (hit) {
       int q = q0 + __popc(hm & ((1u << act.thread_rank()) - 1u));
@@ -463,6 +468,8 @@ k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32
       }
     }
   });
+  G.sync();  // every CTA is done with rank 0's counter
+  if (G.rank() == 0 && threadIdx.x == 0) fill[slot] = s_fill;  // members written (diagnostic)
 }
 
 // Members of sphere (cx, r) of active entry blockIdx.x (substructure search).
@@ -1350,7 +1357,7 @@ __device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac
 
 // Bound-particle properties (haloes_particles.f:1187-1353) over j < konta of
 // the staged list; flag[j] receives the ID mask.  Returns KONTA2.
-template <int C>
+template <int C, bool SYM = true>
 __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
                                   const SegView& v, uint8_t* flag, int64_t konta, float rshell, float cx, float cy,
                                   float cz, const float* cmv, GShared& sh) {
@@ -1406,11 +1413,13 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
               acc[15] += (double)__fdiv_rn(mp, norma);
             },
             sh.wsum, sh.x);
-  // the inertia tensor is symmetric by construction of its entries; only the
-  // six distinct sums are reduced
-  double r[13] = {acc[0], acc[2], acc[3], acc[4], acc[5], acc[6], acc[7], acc[9], acc[10], acc[13],
-                  acc[14], acc[15], acc[16]};
-  gsum_dv<13>(g, r, sh.x);
+  // SYM (haloes_particles.f:1322-1324): the lower triangle of the inertia
+  // tensor is copied from the upper one, so only six sums are reduced; the
+  // subhalo loop (substructure.f:1620-1626) keeps all nine
+  double r[16] = {acc[0], acc[2], acc[3], acc[4], acc[5], acc[6], acc[7], acc[9], acc[10], acc[13],
+                  acc[14], acc[15], acc[16], acc[8], acc[11], acc[12]};
+  if constexpr (SYM) gsum_dv<13>(g, r, sh.x);
+  else gsum_dv<16>(g, r, sh.x);
   const double* r2 = r + 10;
   vmax = gmax_f(g, vmax, sh.fred, sh.x);
   long long cnt = (long long)r2[2];
@@ -1429,11 +1438,18 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
       cat.angularm[i0 * 3 + 2] = (float)(r[3] * (double)H.uv / den);
       cat.mean_vr[i0] = (float)(r2[0] / den * (double)H.uv);
       // in(ix, jy) column-major from the sums of bc(ix)*bc(jy) (jy <= ix kept)
+      // in(jy*3+ix) = sum m*bc(ix)*bc(jy) / den; r[4..9] hold (0,0) (0,1) (0,2)
+      // (1,1) (1,2) (2,2) as (jy,ix), r[13..15] the lower (1,0) (2,0) (2,1)
       float xx = (float)(r[4] / den), yx = (float)(r[5] / den), zx = (float)(r[6] / den);
       float yy = (float)(r[7] / den), zy = (float)(r[8] / den), zz = (float)(r[9] / den);
       float in[9] = {xx, yx, zx, yx, yy, zy, zx, zy, zz};
+      if constexpr (!SYM) {
+        in[3] = (float)(r[13] / den);
+        in[6] = (float)(r[14] / den);
+        in[7] = (float)(r[15] / den);
+      }
       float* it = cat.inertia_tensor + (size_t)i0 * 6;
-      it[0] = xx; it[1] = yx; it[2] = zx; it[3] = yy; it[4] = zy; it[5] = zz;
+      it[0] = in[0]; it[1] = in[3]; it[2] = in[6]; it[3] = in[4]; it[4] = in[7]; it[5] = in[8];
       cat.velocity_dispersion[i0] = (float)(sqrt(r[0] / (double)(float)cnt) * (double)H.uv);
       cat.vmaxclus[i0] = __fmul_rn(__fsqrt_rn(vmax), H.uv);
       float be[3] = {0.0f, 0.0f, 0.0f};
@@ -1964,6 +1980,20 @@ static int big_cluster(asohf_ctx* c) {
     for (int t_ = 0; t_ < 4; t_++) c->launches += (T).n[t_] > 0;                                    \
   } while (0)
 
+// The same tiers for kernels that run on single CTAs only: the cluster tier
+// becomes 256-thread CTAs on the context stream.
+#define LAUNCH_TIERS_CTA(KERN, T, ...)                                                               \
+  do {                                                                                              \
+    ASOHF_CHECK(fork_all(c));                                                                       \
+    if ((T).n[3] > 0) ASOHF_CUDA(launch_grp(KERN<1>, 1, (T).n[3], 256, c->stream, (T).slots[3], __VA_ARGS__)); \
+    for (int t_ = 2; t_ >= 0; t_--)                                                                 \
+      if ((T).n[t_] > 0)                                                                            \
+        ASOHF_CUDA(launch_grp(KERN<1>, 1, (T).n[t_], kTierThreads[t_], c->side[2 - t_], (T).slots[t_], \
+                              __VA_ARGS__));                                                        \
+    ASOHF_CHECK(join_all(c));                                                                       \
+    for (int t_ = 0; t_ < 4; t_++) c->launches += (T).n[t_] > 0;                                    \
+  } while (0)
+
 extern "C" int asohf_set_cluster_threshold(asohf_ctx* c, int64_t min_members) {
   if (!c || min_members < 0) return ASOHF_ERR_INVALID;
   c->cluster_min = min_members == 0 ? BIG_K : min_members;
@@ -2253,12 +2283,13 @@ k_sphere_count(ColIdx ci, const int32_t* __restrict__ act, const float* __restri
                const float* __restrict__ hcy, const float* __restrict__ hcz, const float* __restrict__ r,
                int32_t* __restrict__ konta) {
   __shared__ long long lred[32];
+  __shared__ QBuf qb;
   int s = act[blockIdx.x];
   float cx = hcx[s], cy = hcy[s], cz = hcz[s], rr = r[s];
   int64_t lo, hi;
   slab_range(ci, cx, rr, &lo, &hi);
   long long c = 0;
-  query_box(ci, cx, cy, cz, rr, [&](const float4& e) {
+  gquery_box(Grp<1>(), ci, cx, cy, cz, rr, qb, [&](const float4& e) {
     int p = ppos(e);
     if (p >= lo && p < hi && dist3(e.x, e.y, e.z, cx, cy, cz) < rr) c++;
   });
@@ -2281,14 +2312,17 @@ struct JacOut {
 
 // Jacobi radius on the sorted members (substructure.f:1016-1112).  Slot s of
 // the active list; segment [off[b], off[b]+konta[b]).
+template <int C>
 __global__ void __launch_bounds__(HB)
-k_sub_jacobi(Store S, HConst H, const int32_t* __restrict__ act, const int32_t* __restrict__ konta,
+k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t* __restrict__ act,
+             const int32_t* __restrict__ konta,
              const int64_t* __restrict__ off, const unsigned long long* __restrict__ keys,
              const int32_t* __restrict__ vals, const float* __restrict__ mhost_a,
              const float* __restrict__ disthost_a, float* __restrict__ r, JacOut o) {
+  static_assert(C == 1, "one CTA per subhalo");
   __shared__ MainShared sh;
   __shared__ double s_m[4];
-  int b = blockIdx.x, s = act[b];
+  int b = slots[blockIdx.x], s = act[b];
   int64_t K = konta[b];
   const unsigned long long* kk = keys + off[b];
   const int32_t* lip = vals + off[b];
@@ -2676,6 +2710,286 @@ k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ w
 }
 
 // Work list of a substructure level: REALCLUS != 0, largest RSUB first.
+// ---------------------------------------------------------------- subhalo main (staged)
+// The members kept by the Jacobi search, staged like the halo lists; the
+// subhalo list is the radially sorted list sorted a second time, which
+// reverses each run of equal distances (substructure.f:1161-1162): the
+// staging reads entry j from the mirror of j inside its run.
+template <int C>
+__device__ void load_segment_rev(const Grp<C>& g, const Store& S, const unsigned long long* keys,
+                                 const int32_t* vals, int64_t K, const SegView& a, const SegView& b,
+                                 uint8_t* flag) {
+  int64_t lo, hi;
+  g.chunk(0, K, &lo, &hi);
+  for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    const unsigned long long kj = keys[j];
+    int64_t rs = j, re = j + 1;
+    while (rs > 0 && keys[rs - 1] == kj) rs--;
+    while (re < K && keys[re] == kj) re++;
+    const int p = vals[rs + re - 1 - j];
+    const float mp = S.m[p];
+    a.dm[j] = make_float2(__uint_as_float((uint32_t)(kj & 0xffffffffull)), mp);
+    a.mv[j] = make_float4(mp, S.vx[p], S.vy[p], S.vz[p]);
+    a.px[j] = make_float4(S.x[p], S.y[p], S.z[p], __int_as_float(p));
+    flag[j] = 1;
+  }
+  if (g.rank() == 0 && threadIdx.x == 0) {  // DISTA(KONTA+1) of the sorted list
+    a.dm[K] = make_float2(1.e10f, 0.f); b.dm[K] = a.dm[K];
+    a.mv[K] = make_float4(0.f, 0.f, 0.f, 0.f); b.mv[K] = a.mv[K];
+    a.px[K] = make_float4(0.f, 0.f, 0.f, 0.f); b.px[K] = a.px[K];
+  }
+  g.sync();
+}
+
+// SUBSTRUCTURE_PARTICLES after the Jacobi radius (substructure.f:1115-1660):
+// unbinding, Jacobi trim, SO walk without early exit, properties.
+template <int C>
+__global__ void __launch_bounds__(HB, 3)
+k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogue cat,
+             const int32_t* __restrict__ work, SubMainIn in, SegG sg) {
+  __shared__ GShared sh;
+  Grp<C> g;
+  const int slot = group_slot<C>(slots);
+  const bool lead = leader(g.rank());
+  const int i0 = work[slot];
+  if (lead) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; sg.final_b[slot] = 0; }
+  const int64_t Kg = in.konta[slot];
+  const int64_t konta = in.jjac[slot];
+  const double masadm = in.masadm[slot];
+  const float um = H.um;
+  if (masadm <= 0.0 || konta < H.min_num_part || konta > Kg) {
+    // RSUB/MSUB were set when the Jacobi radius was fixed (substructure.f:1115-1117)
+    if (lead) {
+      cat.rsub[i0] = in.rclus[slot];
+      cat.msub[i0] = (float)(masadm * (double)um);
+      cat.realclus[i0] = 0;
+      sg.status[slot] = 0;
+    }
+    return;
+  }
+  const int64_t base = sg.off[slot] + slot;
+  SegView va = view_at(sg.a, base), vb = view_at(sg.b, base);
+  double* pot = sg.pot + base;
+  uint8_t* flag = sg.flag + base;
+  const float cx = in.cx[slot], cy = in.cy[slot], cz = in.cz[slot];
+  const float mhost = in.mhost[slot], disthost = in.disthost[slot];
+  load_segment_rev(g, S, sg.keys + sg.off[slot], sg.vals + sg.off[slot], konta, va, vb, flag);
+  SegView cur = va, nxt = vb;
+  int which = 0;
+  float cm0[3], v0[3], m2;
+  centromasas_g(g, cur, konta, cm0, v0, &m2, sh);
+  HaloState h;
+  for (int q = 0; q < 3; q++) { h.cm[q] = cm0[q]; h.v[q] = v0[q]; }
+  h.radio = in.rclus[slot];                 // RSUB
+  h.masa = (float)(masadm * (double)um);    // MSUB
+  h.realclus = cat.realclus[i0];
+  unsigned long long ep = 2ull * (unsigned long long)konta;
+  int64_t k2 = konta;
+  float ref_max = cur.dm[k2 - 1].x;
+  const float norma = S.norma;
+  auto write_back = [&]() {
+    if (lead) {
+      cat.clusrxcm[i0] = h.cm[0]; cat.clusrycm[i0] = h.cm[1]; cat.clusrzcm[i0] = h.cm[2];
+      cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2];
+      cat.rsub[i0] = h.radio; cat.msub[i0] = h.masa;
+      cat.dmpclus[i0] = (int32_t)konta;
+    }
+  };
+  auto finish_empty = [&]() {
+    write_back();
+    if (lead) {
+      cat.realclus[i0] = 0;
+      sg.final_b[slot] = (uint8_t)which;
+      sg.status[slot] = 0;
+    }
+  };
+  // escape-velocity unbinding with IDX_VIR = K2 (substructure.f:1172-1190)
+  int64_t contaerr = konta;
+  int fac = 0;
+  while (contaerr > 0 || fac < 3) {
+    fac++;
+    int64_t prev = k2, iv = k2;
+    ep += (unsigned long long)k2;
+    long long kept = unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, iv, h, sh);
+    if (kept != k2) {
+      int64_t nk2;
+      compact_g(g, cur, nxt, flag, k2, &iv, &nk2, sh);
+      SegView t = cur; cur = nxt; nxt = t; which ^= 1;
+      k2 = nk2;
+    }
+    ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
+    contaerr = prev - k2;
+    if (fac > 100000) break;
+  }
+  if (k2 < H.min_num_part) { finish_empty(); return; }
+  fac = 0;
+  contaerr = k2;
+  while (contaerr > 0 || fac < 4) {
+    fac++;
+    int64_t prev = k2, iv = k2;
+    ep += (unsigned long long)k2;
+    long long kept = unbinding_sigma_g(g, H, fac, cur, flag, k2, iv, h, sh);
+    if (kept != k2) {
+      int64_t nk2;
+      compact_g(g, cur, nxt, flag, k2, &iv, &nk2, sh);
+      SegView t = cur; cur = nxt; nxt = t; which ^= 1;
+      k2 = nk2;
+    }
+    ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
+    contaerr = prev - k2;
+    if (fac > 100000) break;
+  }
+  if (k2 < H.min_num_part) { finish_empty(); return; }
+  // Jacobi trim after unbinding (substructure.f:1241-1264)
+  int64_t ncapas = 0;
+  float rshell = 0.0f;
+  {
+    const double m0 = (double)__fdiv_rn(h.masa, um);
+    const double bx = (double)__fdiv_rn(cur.dm[k2 - 1].x, disthost);
+    const double e0 = eq_jacobi_dev(bx, m0 * (double)um / (double)mhost);
+    if (e0 > 0.0) {
+      // M(J) = MASADM - sum_{i >= J} m_i ; largest J in [1, k2] with EQ < 0
+      double tot = 0.0;
+      {
+        int64_t lo, hi;
+        g.chunk(0, k2, &lo, &hi);
+        for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) tot += (double)cur.dm[j].y;
+        gsum_dv<1>(g, &tot, sh.x);
+      }
+      long long f = -1;
+      double mf = 0.0;
+      gscan_d(g, 0, k2, 0.0, [&](int64_t j) { return (double)cur.dm[j].y; },
+              [&](int64_t j, double pre) {
+                const int64_t J = j + 1;
+                const double mj = m0 - (tot - pre + (double)cur.dm[j].y);  // after subtracting m(J..K2)
+                const double bxj = (double)__fdiv_rn(cur.dm[j].x, disthost);
+                const double e2 = eq_jacobi_dev(bxj, mj * (double)um / (double)mhost);
+                if (e2 < 0.0 && J > f) { f = J; mf = mj; }
+              },
+              sh.wsum, sh.x);
+      long long nf = f > 0 ? -f : LLONG_MAX;
+      gmin_llv<1>(g, &nf, sh.lred, sh.x);
+      const long long fmax = nf == LLONG_MAX ? -1 : -nf;
+      double mfv = (f == fmax && f > 0) ? mf : 0.0;  // one entry holds it
+      gsum_dv<1>(g, &mfv, sh.x);
+      int64_t J;
+      double mj;
+      if (fmax <= 0) {
+        J = 0;
+        mj = m0 - tot;
+      } else {
+        J = fmax;
+        mj = mfv;
+      }
+      h.radio = J + 1 <= k2 ? cur.dm[J].x : (J + 1 == k2 + 1 ? cur.dm[k2].x : 1.e10f);
+      h.masa = (float)(mj * (double)um);
+      k2 = J;
+      ncapas = J;
+      rshell = J >= 1 ? cur.dm[J - 1].x : 1.e10f;
+    }
+  }
+  if (k2 < H.min_num_part) { finish_empty(); return; }
+  // SO walk without early exit (substructure.f:1293-1463)
+  const float pi = H.pi, rote = H.rote, rete = H.rete;
+  const int64_t jjcore = (int64_t)fmaxf(10.0f, __fdiv_rn((float)k2, 100.0f));
+  const float thr[6] = {__fdiv_rn(2500.0f, H.omegaz), __fdiv_rn(500.0f, H.omegaz), __fdiv_rn(200.0f, H.omegaz),
+                        2500.0f, 500.0f, 200.0f};
+  const int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
+  long long jt[7];
+  for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
+  double best_v = -1.0;
+  long long best_j = LLONG_MAX;
+  double best_b = 0.0;
+  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(cur.dm[j].y, norma); };
+  const double btot = gscan_d(g, 0, k2, 0.0, mn_of,
+                              [&](int64_t j, double bas8) {
+                                const int64_t J = j + 1;
+                                if (J <= jjcore) return;
+                                const float d = cur.dm[j].x;
+                                const float vol = so_den(d, rete, pi);
+                                const float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
+                                for (int q = 0; q < 6; q++)
+                                  if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+                                if (delta2 <= H.contrastec && J > jvir_min && J < jt[6]) jt[6] = J;
+                                const float bas2 = (float)(bas8 / (double)d);
+                                if (best_before((double)bas2, J, best_v, best_j)) {
+                                  best_v = bas2; best_j = J; best_b = bas8;
+                                }
+                              },
+                              sh.wsum, sh.x);
+  gmin_llv<7>(g, jt, sh.lred, sh.x);
+  // BAS8 at the crossings and the momentum sums, in one more pass
+  double sv[10];
+  for (int q = 0; q < 10; q++) sv[q] = 0.0;
+  gscan_d(g, 0, k2, 0.0, mn_of,
+          [&](int64_t j, double bas8) {
+            for (int q = 0; q < 7; q++)
+              if (j + 1 == jt[q]) sv[q] = bas8;
+            const float4 qv = cur.mv[j];
+            const float mn = __fdiv_rn(qv.x, norma);
+            sv[7] += (double)__fmul_rn(mn, qv.y);
+            sv[8] += (double)__fmul_rn(mn, qv.z);
+            sv[9] += (double)__fmul_rn(mn, qv.w);
+          },
+          sh.wsum, sh.x);
+  gsum_dv<10>(g, sv, sh.x);
+  gbest(g, &best_v, &best_j, &best_b, sh);
+  if (lead) {
+    if (best_j != LLONG_MAX) {
+      cat.vcmax[i0] = (float)best_v;
+      cat.mcmax[i0] = (float)best_b;
+      cat.rcmax[i0] = cur.dm[best_j - 1].x;
+    }
+    float* mo[6] = {cat.m2500c, cat.m500c, cat.m200c, cat.m2500m, cat.m500m, cat.m200m};
+    float* ro[6] = {cat.r2500c, cat.r500c, cat.r200c, cat.r2500m, cat.r500m, cat.r200m};
+    for (int q = 0; q < 6; q++) {
+      if (jt[q] != LLONG_MAX) {
+        const int64_t J = jt[q];
+        const float d = cur.dm[J - 1].x;
+        const float vol = so_den(d, rete, pi);
+        const float delta2 = (float)((double)norma * sv[q] / (double)vol / (double)rote);
+        mo[q][i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
+        ro[q][i0] = d;
+        if (J == jjcore + 1) { mo[q][i0] = -1.0f; ro[q][i0] = -1.0f; }
+      } else {
+        mo[q][i0] = 0.0f;
+        ro[q][i0] = 0.0f;
+      }
+    }
+    if (jt[6] != LLONG_MAX) {
+      const int64_t J = jt[6];
+      const float d = cur.dm[J - 1].x;
+      const float vol = so_den(d, rete, pi);
+      const float delta2 = (float)((double)norma * sv[6] / (double)vol / (double)rote);
+      cat.masa[i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
+      cat.radio[i0] = d;
+    } else {
+      cat.masa[i0] = 0.0f;
+      cat.radio[i0] = 0.0f;
+    }
+    h.v[0] = (float)(sv[7] / btot);
+    h.v[1] = (float)(sv[8] / btot);
+    h.v[2] = (float)(sv[9] / btot);
+    const float bas = __fdiv_rn(__fmul_rn(__fmul_rn(cat.vcmax[i0], norma), H.cgr), rete);
+    cat.vcmax[i0] = __fmul_rn(__fsqrt_rn(bas), H.uv);
+    cat.mcmax[i0] = __fmul_rn(__fmul_rn(cat.mcmax[i0], norma), um);
+    sg.final_b[slot] = (uint8_t)which;
+  }
+  // the velocity the leader computed reaches every CTA through the catalogue
+  // (the properties read VX(I) from it, as the Fortran does)
+  write_back();
+  g.sync();
+  long long nb = properties_g<C, false>(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh);
+  ep += (unsigned long long)(k2 + ncapas);
+  if (lead) {
+    atomicAdd(&sg.work[1], ep);
+    const bool ok = nb >= H.min_num_part && H.want_ids;
+    sg.nbound[slot] = ok ? (int32_t)nb : 0;
+    sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
+    sg.status[slot] = 0;
+  }
+}
+
 static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots) {
   int nh = low2 - low1 + 1;
   int32_t* rc = (int32_t*)malloc(4 * (size_t)nh);
@@ -2702,10 +3016,13 @@ static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t
 
 // gather + segmented sort of the members of `na` spheres (active list act);
 // keys/vals sorted in segments at offsets off (device).
+// Counts, tiers (by count) of the spheres, gathers into segments and sorts
+// them; d_tslots and d_fill hold na entries.
 static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na, const int32_t* d_act,
                          const float* cx, const float* cy, const float* cz, const float* r,
                          int32_t* d_konta, int64_t* d_off, int64_t* h_off, unsigned long long** keys,
-                         int32_t** vals, int64_t* total, bool with_work) {
+                         int32_t** vals, int64_t* total, bool with_work, Tiers* tiers, int32_t* d_tslots,
+                         int32_t* d_fill) {
   {
     int kt_ = ktime_begin(c, "sub_sphere_count");
     k_sphere_count<<<na, HB, 0, c->stream>>>(ci, d_act, cx, cy, cz, r, d_konta);
@@ -2717,7 +3034,17 @@ static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na,
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   h_off[0] = 0;
   for (int s = 0; s < na; s++) h_off[s + 1] = h_off[s] + hk[s];
+  // few subhaloes per call, each in a dense region: 256-thread CTAs (tier 2)
+  // keep more of the GPU busy than the small tiers
+  for (int s = 0; s < na; s++) hk[s] = 0;
+  int64_t keep_t1 = c->tier1_k, keep_t2 = c->tier2_k;
+  c->tier1_k = 0;
+  c->tier2_k = 0;
+  int rt = split_tiers(c, hk, na, d_tslots, tiers);
+  c->tier1_k = keep_t1;
+  c->tier2_k = keep_t2;
   free(hk);
+  ASOHF_CHECK(rt);
   int64_t T = h_off[na];
   ASOHF_CUDA(cudaMemcpyAsync(d_off, h_off, 8 * (size_t)(na + 1), cudaMemcpyHostToDevice, c->stream));
   int bits = 1;
@@ -2725,7 +3052,7 @@ static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na,
   size_t tb = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                   (int32_t*)nullptr, (int32_t*)nullptr, (int)(T > 0 ? T : 1), 0, 32 + bits);
-  size_t work = with_work ? ((size_t)T + na) * (4 + 4 + 8 + 1) + 4096 : 0;
+  size_t work = with_work ? ((size_t)T + na) * (2 * (8 + 16 + 16) + 8 + 1) + 16384 : 0;
   ASOHF_CHECK(seg_reserve(c, (size_t)T * 24 + tb + work + 16384));
   unsigned long long* k0 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
   unsigned long long* k1 = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
@@ -2734,18 +3061,18 @@ static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na,
   void* t = seg_alloc(c, tb);
   if (!k0 || !k1 || !v0 || !v1 || !t) return ASOHF_ERR_CAPACITY;
   if (T > 0) {
-    // k_sub_gather reads per-slot arrays through the active list order: it
-    // indexes by blockIdx (slot in the active list), so pass compacted views
+    // the per-sphere arrays are indexed by position in the active list
+    ASOHF_CUDA(cudaMemsetAsync(d_fill, 0, 4 * (size_t)na, c->stream));
     {
       int kt_ = ktime_begin(c, "sub_gather");
-      k_sub_gather<<<na, HB, 0, c->stream>>>(S, ci, d_konta, d_off, cx, cy, cz, r, k0, v0);
+      LAUNCH_TIERS_CTA(k_halo_gather, *tiers, S, ci, d_konta, d_off, cx, cy, cz, r, d_fill, k0, v0);
       ktime_end(c, kt_);
     }
     int kt_ = ktime_begin(c, "sub_radix_sort");
     ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)T, 0, 32 + bits, c->stream));
     ktime_end(c, kt_);
     k_tiefix<<<grid_for(T, 256), 256, 0, c->stream>>>(k1, v1, T, 1);
-    c->launches += 2;
+    c->launches++;
   }
   *keys = k1;
   *vals = v1;
@@ -2790,7 +3117,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   double ht = htime_now();
   arena_reset(c);
   int nh = lowh2 - lowh1 + 1;
-  size_t need = cat_bytes(cat->nclus) + (size_t)nh * 160 + 65536;
+  size_t need = cat_bytes(cat->nclus) + (size_t)nh * 192 + 65536;
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
   ASOHF_CHECK(cat_mirror_in(c, cat, cat->nclus, on_device, &m, lowh1 - 1, true));
@@ -2852,7 +3179,9 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
     ht = htime_now();
     // Jacobi radius, growing the unresolved ones
     int32_t* d_pos = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
-    if (!d_pos) rc = ASOHF_ERR_CAPACITY;
+    int32_t* d_tsl = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    int32_t* d_fill = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+    if (!d_pos || !d_tsl || !d_fill) rc = ASOHF_ERR_CAPACITY;
     else k_iota32<<<(ns + 255) / 256, 256, 0, c->stream>>>(d_pos, ns);
     for (int iter = 0; na > 0 && rc == ASOHF_OK; iter++) {
       if (iter > 200) { rc = ASOHF_ERR_TIMEOUT; break; }
@@ -2865,17 +3194,18 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       unsigned long long* keys;
       int32_t* vals;
       int64_t T;
+      Tiers tj;
       ASOHF_CHECK(gather_sorted(c, S, ci, na, d_pos, t_cx, t_cy, t_cz, t_r, d_konta, d_off, h_off, &keys, &vals,
-                                &T, false));
+                                &T, false, &tj, d_tsl, d_fill));
       {
         int kt_ = ktime_begin(c, "sub_jacobi");
-        k_sub_jacobi<<<na, HB, 0, c->stream>>>(S, H, d_act, d_konta, d_off, keys, vals, pr.mhost, pr.disthost,
-                                               pr.r, jo);
+        LAUNCH_TIERS_CTA(k_sub_jacobi, tj, S, H, d_act, d_konta, d_off, keys, vals, pr.mhost, pr.disthost, pr.r,
+                         jo);
         ktime_end(c, kt_);
       }
       k_jacobi_scatter<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, jo, t_r, f_jjac, f_masadm, f_rclus,
                                                                 f_rlast);
-      c->launches += 2;
+      c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       ASOHF_CUDA(cudaMemcpyAsync(h_done, jo.done, 4 * (size_t)na, cudaMemcpyDeviceToHost, c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
@@ -2891,36 +3221,50 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       unsigned long long* keys;
       int32_t* vals;
       int64_t T;
+      Tiers tf;
       ASOHF_CHECK(gather_sorted(c, S, ci, ns, d_pos, pr.cx, pr.cy, pr.cz, f_rlast, d_konta, d_off, h_off, &keys,
-                                &vals, &T, true));
+                                &vals, &T, true, &tf, d_tsl, d_fill));
       htime_end(c, "host:sub_final_gather", ht);
       ht = htime_now();
-      Seg sg;
+      // staged lists of the kept members, tiers by that count
+      const size_t E = (size_t)T + ns;
+      SegG sg;
       sg.konta = d_konta;
       sg.off = d_off;
       sg.keys = keys;
       sg.vals = vals;
-      sg.dista = (float*)seg_alloc(c, 4 * ((size_t)T + ns));
-      sg.lip = (int32_t*)seg_alloc(c, 4 * ((size_t)T + ns));
-      sg.pot = (double*)seg_alloc(c, 8 * ((size_t)T + ns));
-      sg.flag = (uint8_t*)seg_alloc(c, (size_t)T + ns);
+      sg.a.dm = (float2*)seg_alloc(c, 8 * E);
+      sg.a.mv = (float4*)seg_alloc(c, 16 * E);
+      sg.a.px = (float4*)seg_alloc(c, 16 * E);
+      sg.b.dm = (float2*)seg_alloc(c, 8 * E);
+      sg.b.mv = (float4*)seg_alloc(c, 16 * E);
+      sg.b.px = (float4*)seg_alloc(c, 16 * E);
+      sg.pot = (double*)seg_alloc(c, 8 * E);
+      sg.flag = (uint8_t*)seg_alloc(c, E);
+      sg.final_b = (uint8_t*)arena_alloc(c, (size_t)ns);
       sg.nbound = d_nbound;
       sg.nscan = d_nscan;
       sg.work = c->d_work;
       sg.status = pr.status;
-      if (!sg.dista || !sg.lip || !sg.pot || !sg.flag) {
+      sg.timing = 0;
+      int32_t* d_ts = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
+      if (!sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px || !sg.pot || !sg.flag ||
+          !sg.final_b || !d_ts) {
         free(hw); free(h_off); free(h_act); free(h_done); free(h_st);
         return ASOHF_ERR_CAPACITY;
       }
       SubMainIn in;
       in.konta = d_konta; in.jjac = f_jjac; in.masadm = f_masadm; in.rclus = f_rclus;
       in.cx = pr.cx; in.cy = pr.cy; in.cz = pr.cz; in.mhost = pr.mhost; in.disthost = pr.disthost;
+      Tiers ts;
+      ASOHF_CUDA(cudaMemcpyAsync(h_st, f_jjac, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      ASOHF_CHECK(split_tiers(c, h_st, ns, d_ts, &ts));
       {
         int kt_ = ktime_begin(c, "sub_main");
-        k_sub_main<<<ns, HB, 0, c->stream>>>(S, H, m.d, d_work, in, sg);
+        LAUNCH_TIERS_CTA(k_sub_main_g, ts, S, H, m.d, d_work, in, sg);
         ktime_end(c, kt_);
       }
-      c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       ASOHF_CUDA(cudaMemcpyAsync(h_st, pr.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
@@ -2934,10 +3278,10 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
         ASOHF_CHECK(ensure_pph(c, total));
         {
           int kt_ = ktime_begin(c, "sub_write_ids");
-          k_sub_write_ids<<<ns, HB, 0, c->stream>>>(d_nscan, d_off, d_ids_off, sg.lip, sg.flag, c->p.id, c->d_pph);
+          LAUNCH_TIERS_CTA(k_write_ids, ts, d_nscan, d_off, d_ids_off, sg.final_b, sg.a.px, sg.b.px, sg.flag,
+                           c->p.id, c->d_pph);
           ktime_end(c, kt_);
         }
-        c->launches++;
         ASOHF_CUDA(cudaGetLastError());
         c->pph_len = total;
       }

@@ -59,7 +59,7 @@ int asohf_set_cluster_threshold(asohf_ctx *ctx, int64_t min_members);
  * threshold are refined by one CTA of 256 threads from tier2_members
  * members, of 128 threads from tier1_members, else of 32 threads; a halo
  * whose growth sphere outgrows its CTA moves to a larger one.  0 restores
- * a default (512, 4096). */
+ * a default (256, 2048). */
 int asohf_set_group_tiers(asohf_ctx *ctx, int64_t tier1_members, int64_t tier2_members);
 
 /* MODULE PARTICLES (particles.f:1-14) / READ_AND_ALLOC_PARTICLES
