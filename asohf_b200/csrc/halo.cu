@@ -472,35 +472,6 @@ k_halo_gather(const int32_t* __restrict__ slots, Store S, ColIdx ci, const int32
   if (G.rank() == 0 && threadIdx.x == 0) fill[slot] = s_fill;  // members written (diagnostic)
 }
 
-// Members of sphere (cx, r) of active entry blockIdx.x (substructure search).
-__global__ void __launch_bounds__(HB)
-k_sub_gather(Store S, ColIdx ci, const int32_t* __restrict__ konta, const int64_t* __restrict__ off,
-              const float* __restrict__ hcx, const float* __restrict__ hcy, const float* __restrict__ hcz,
-              const float* __restrict__ rg, unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
-  __shared__ int fill;
-  int slot = blockIdx.x;
-  if (konta[slot] == 0) return;
-  if (threadIdx.x == 0) fill = 0;
-  __syncthreads();
-  float cx = hcx[slot], cy = hcy[slot], cz = hcz[slot], r = rg[slot];
-  int64_t lo, hi;
-  slab_range(ci, cx, r, &lo, &hi);
-  int64_t base = off[slot];
-  unsigned long long hk = (unsigned long long)slot << 32;
-  query_box(ci, cx, cy, cz, r, [&](const float4& e) {
-    int p = ppos(e);
-    if (p < lo || p >= hi) return;
-    float a = dist3(e.x, e.y, e.z, cx, cy, cz);
-    if (a < r) {
-      int q = atomicAdd(&fill, 1);
-      if (q < konta[slot]) {
-        keys[base + q] = hk | __float_as_uint(a);
-        vals[base + q] = p;
-      }
-    }
-  });
-}
-
 // Runs of equal (halo, distance) get their positions in descending (desc=1)
 // or ascending order.
 __global__ void k_tiefix(const unsigned long long* __restrict__ keys, int32_t* __restrict__ vals,
@@ -524,21 +495,6 @@ __global__ void k_tiefix(const unsigned long long* __restrict__ keys, int32_t* _
 }
 
 // ---------------------------------------------------------------- main
-struct Seg {
-  const int32_t* konta;
-  const int64_t* off;      // element offset of the segment (segments padded by 1)
-  const unsigned long long* keys;
-  const int32_t* vals;
-  float* dista;            // DISTA(1..K) at [off], DISTA(K+1) pad
-  int32_t* lip;
-  double* pot;
-  uint8_t* flag;
-  int32_t* nbound;         // IDs to write per slot (KONTA2 of the property loop)
-  int32_t* nscan;          // entries the property loop scanned (NCAPAS)
-  unsigned long long* work;  // element-pass counter of this kernel
-  int32_t* status;
-};
-
 struct MainShared {
   double dred[32];
   float fred[32];
@@ -554,63 +510,6 @@ struct MainShared {
 
 // Block-wide minimum of an index (LLONG_MAX when none).
 __device__ __forceinline__ long long bmin(long long v, MainShared& sh) { return block_min_ll(v, sh.lred); }
-
-// CENTROMASAS_PART (haloes_particles.f:1731-1824) over j <= n with flag=1.
-__device__ void centromasas_block(const Store& S, const float* dista_unused, const int32_t* lip,
-                                  const uint8_t* flag, bool all_kept, int64_t n, float* cm, float* vcm,
-                                  float* masa, MainShared& sh) {
-  double a[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
-    if (!all_kept && !flag[j]) continue;
-    int p = lip[j];
-    double bas = (double)S.m[p];
-    a[0] += (double)S.x[p] * bas;
-    a[1] += (double)S.y[p] * bas;
-    a[2] += (double)S.z[p] * bas;
-    a[3] += (double)S.vx[p] * bas;
-    a[4] += (double)S.vy[p] * bas;
-    a[5] += (double)S.vz[p] * bas;
-    a[6] += bas;
-  }
-  for (int q = 0; q < 7; q++) a[q] = block_sum_d(a[q], sh.dred);
-  if (a[6] > 0.0) {
-    for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
-    *masa = (float)a[6];
-  } else {
-    for (int q = 0; q < 3; q++) { cm[q] = 0.0f; vcm[q] = 0.0f; }
-    *masa = 0.0f;
-  }
-}
-
-// REORDENAR(...,0,...) (haloes_particles.f:1696-1722): stable in-place
-// compaction of the kept entries of j <= k2, IDX_VIR relocated to the first
-// kept entry at or after it.  Entries past the new length keep their values.
-__device__ void reordenar_compact(float* dista, int32_t* lip, const uint8_t* flag, int64_t k2,
-                                  int64_t* idx_vir, int64_t* k2new, MainShared& sh) {
-  int64_t carry = 0;
-  long long reloc = LLONG_MAX;
-  int64_t iv = *idx_vir;  // 1-based
-  __shared__ int sb[33];
-  for (int64_t t0 = 0; t0 < k2; t0 += HB) {
-    int64_t j = t0 + threadIdx.x;
-    bool keep = j < k2 && flag[j];
-    float d = keep ? dista[j] : 0.0f;
-    int32_t l = keep ? lip[j] : 0;
-    int tot;
-    int inc = block_scan_i(keep ? 1 : 0, sb, &tot);
-    int64_t dst = carry + inc - 1;
-    if (keep) {
-      dista[dst] = d;
-      lip[dst] = l;
-      if (j + 1 >= iv && dst + 1 < reloc) reloc = dst + 1;
-    }
-    carry += tot;
-    __syncthreads();
-  }
-  reloc = bmin(reloc, sh);
-  *k2new = carry;
-  *idx_vir = reloc == LLONG_MAX ? carry : reloc;
-}
 
 struct HaloState {
   float cm[3], v[3], masa, radio;
@@ -628,137 +527,6 @@ __device__ __forceinline__ void unbind_result(HaloState& h, long long konta3, co
     for (int q = 0; q < 3; q++) { h.cm[q] = cm[q]; h.v[q] = vcm[q]; }
     h.masa = __fmul_rn(mmm, um);
   }
-}
-
-// UNBINDING8 (haloes_particles.f:1828-1983).  dista/lip/flag/pot are the
-// 0-based views of the segment (element j-1 = Fortran J).
-__device__ void unbinding8_block(const Store& S, const HConst& H, int fac, float ref_max, float* dista,
-                                 int32_t* lip, uint8_t* flag, double* pot, int64_t k2, int64_t idx_vir,
-                                 HaloState& h, MainShared& sh) {
-  float cm[3] = {0, 0, 0}, vcm[3] = {0, 0, 0}, mmm = 0.0f;
-  long long konta3 = 0;
-  if (k2 > 0) {
-    double norma = (double)S.norma;
-    float lim = __fmul_rn(0.01f, ref_max);
-    long long jj = LLONG_MAX;
-    for (int64_t t0 = 0; t0 < k2 && jj == LLONG_MAX; t0 += HB) {
-      int64_t j = t0 + threadIdx.x;
-      long long cand = (j < k2 && dista[j] > lim) ? (long long)(j + 1) : LLONG_MAX;
-      jj = bmin(cand, sh);
-    }
-    if (jj == LLONG_MAX) jj = k2 + 1;
-    // cumulative mass MASA8 (stored in pot for now)
-    double mjj = 0.0, mk2 = 0.0;
-    __shared__ double s_m[2];
-    tile_prefix_d(0, k2, 0.0, [&](int64_t j) { return (double)S.m[lip[j]] / norma; },
-                  [&](int64_t j, double v) {
-                    pot[j] = v;
-                    if (j + 1 == jj) s_m[0] = v;
-                    if (j + 1 == k2) s_m[1] = v;
-                  },
-                  sh.dred);
-    __syncthreads();
-    mk2 = s_m[1];
-    if (jj == k2 + 1) mjj = mk2; else mjj = s_m[0];
-    double pot_jj = mjj / (double)dista[jj - 1];
-    // POT(J) for J > JJ: POT(J-1) + MASA8*BAS8/DISTA(J)^2
-    tile_prefix_d(jj, k2, pot_jj,
-                  [&](int64_t j) {
-                    float dj = dista[j], dm = dista[j - 1];
-                    double bas8 = (dj != dm) ? (double)__fsub_rn(dj, dm) : 0.0;
-                    double djd = (double)dj;
-                    return pot[j] * bas8 / (djd * djd);
-                  },
-                  [&](int64_t j, double v) { pot[j] = v; }, sh.dred);
-    __syncthreads();
-    for (int64_t j = threadIdx.x; j < jj && j < k2; j += blockDim.x) pot[j] = pot_jj;
-    __syncthreads();
-    double pot1 = pot[k2 - 1] + mk2 / (double)ref_max;
-    double aa8 = norma * (double)__fdiv_rn(H.cgr, H.rete);
-    float bb = 2.0f;
-    if (fac == 1) bb = 8.0f;
-    if (fac == 2) bb = 4.0f;
-    bb = __fmul_rn(bb, bb);
-    double a[7] = {0, 0, 0, 0, 0, 0, 0};
-    long long kept = 0;
-    for (int64_t j = threadIdx.x; j < k2; j += blockDim.x) {
-      float potok = (float)((pot[j] - pot1) * aa8);
-      float vesc2 = __fmul_rn(2.0f, fabsf(potok));
-      int p = lip[j];
-      float ax = __fsub_rn(S.vx[p], h.v[0]), ay = __fsub_rn(S.vy[p], h.v[1]), az = __fsub_rn(S.vz[p], h.v[2]);
-      float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
-      bool keep = !(vvv2 > __fmul_rn(bb, vesc2));
-      flag[j] = keep;
-      kept += keep;
-      if (keep && j < idx_vir) {
-        double bas = (double)S.m[p];
-        a[0] += (double)S.x[p] * bas;
-        a[1] += (double)S.y[p] * bas;
-        a[2] += (double)S.z[p] * bas;
-        a[3] += (double)S.vx[p] * bas;
-        a[4] += (double)S.vy[p] * bas;
-        a[5] += (double)S.vz[p] * bas;
-        a[6] += bas;
-      }
-    }
-    konta3 = block_sum_ll(kept, sh.lred);
-    for (int q = 0; q < 7; q++) a[q] = block_sum_d(a[q], sh.dred);
-    if (a[6] > 0.0) {
-      for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
-      mmm = (float)a[6];
-    }
-  }
-  unbind_result(h, konta3, cm, vcm, mmm, H.um);
-}
-
-// UNBINDING_SIGMA (haloes_particles.f:1987-2095).
-__device__ void unbinding_sigma_block(const Store& S, const HConst& H, int fac, int32_t* lip, uint8_t* flag,
-                                      int64_t k2, int64_t idx_vir, HaloState& h, MainShared& sh) {
-  float bb = fmaxf(__fsub_rn(6.0f, __fmul_rn(1.0f, (float)(fac - 1))), 3.0f);
-  bb = __fmul_rn(bb, bb);
-  float cm[3] = {h.cm[0], h.cm[1], h.cm[2]}, vcm[3] = {h.v[0], h.v[1], h.v[2]}, mmm = 0.0f;
-  long long konta3 = 0;
-  if (k2 > 0) {
-    double s2 = 0.0;
-    for (int64_t j = threadIdx.x; j < idx_vir && j < k2; j += blockDim.x) {
-      int p = lip[j];
-      float ax = __fsub_rn(S.vx[p], vcm[0]), ay = __fsub_rn(S.vy[p], vcm[1]), az = __fsub_rn(S.vz[p], vcm[2]);
-      s2 += (double)__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
-    }
-    double sigma2 = block_sum_d(s2, sh.dred);
-    if (idx_vir > 1) sigma2 = sigma2 / (double)(idx_vir - 1);
-    double thr = (double)bb * sigma2;
-    double a[7] = {0, 0, 0, 0, 0, 0, 0};
-    long long kept = 0;
-    for (int64_t j = threadIdx.x; j < k2; j += blockDim.x) {
-      int p = lip[j];
-      float ax = __fsub_rn(S.vx[p], vcm[0]), ay = __fsub_rn(S.vy[p], vcm[1]), az = __fsub_rn(S.vz[p], vcm[2]);
-      float bas = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
-      bool keep = !((double)bas > thr);
-      flag[j] = keep;
-      kept += keep;
-      if (keep && j < idx_vir) {
-        double w = (double)S.m[p];
-        a[0] += (double)S.x[p] * w;
-        a[1] += (double)S.y[p] * w;
-        a[2] += (double)S.z[p] * w;
-        a[3] += (double)S.vx[p] * w;
-        a[4] += (double)S.vy[p] * w;
-        a[5] += (double)S.vz[p] * w;
-        a[6] += w;
-      }
-    }
-    konta3 = block_sum_ll(kept, sh.lred);
-    for (int q = 0; q < 7; q++) a[q] = block_sum_d(a[q], sh.dred);
-    if (a[6] > 0.0) {
-      for (int q = 0; q < 3; q++) { cm[q] = (float)(a[q] / a[6]); vcm[q] = (float)(a[3 + q] / a[6]); }
-      mmm = (float)a[6];
-    } else {
-      for (int q = 0; q < 3; q++) { cm[q] = 0.0f; vcm[q] = 0.0f; }
-      mmm = 0.0f;
-    }
-  }
-  unbind_result(h, konta3, cm, vcm, mmm, H.um);
 }
 
 // DIAGONALISE (num.f:2-116), REAL*8 Jacobi; `in` is column-major REAL*4.
@@ -833,133 +601,9 @@ __device__ void sort_eigen_dev(float* e) {
   }
 }
 
-// Bound-particle properties (haloes_particles.f:1187-1353 and
-// substructure.f:1478-1660) over j <= konta; flag[j] receives the ID mask.
-// Returns the number of bound particles (KONTA2).
-__device__ long long properties_block(const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
-                                      float* dista, int32_t* lip, uint8_t* flag, int64_t konta, float rshell,
-                                      float cx, float cy, float cz, const float* cmv, bool sym,
-                                      MainShared& sh) {
-  float norma = S.norma;
-  float vc[3] = {cat.vx[i0], cat.vy[i0], cat.vz[i0]};
-  int64_t each_prof = konta / ASOHF_NBINS;
-  if (each_prof == 0) each_prof = 1;
-  double acc[16];
-  for (int q = 0; q < 16; q++) acc[q] = 0.0;
-  float vmax = -1.0f;
-  long long cnt = 0;
-  // masked cumulative mass for the profile entries, then the sums
-  tile_prefix_d(0, konta,
-                0.0,
-                [&](int64_t j) {
-                  int p = lip[j];
-                  float a = dist3(S.x[p], S.y[p], S.z[p], cx, cy, cz);
-                  bool in = a <= rshell;
-                  flag[j] = in;
-                  return in ? (double)__fdiv_rn(S.m[p], norma) : 0.0;
-                },
-                [&](int64_t j, double basmas) {
-                  int64_t J = j + 1;
-                  if (!flag[j]) return;
-                  int p = lip[j];
-                  float bv[3] = {__fsub_rn(S.x[p], cx), __fsub_rn(S.y[p], cy), __fsub_rn(S.z[p], cz)};
-                  float aadm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(bv[0], bv[0]), __fmul_rn(bv[1], bv[1])),
-                                                    __fmul_rn(bv[2], bv[2])));
-                  cnt++;
-                  if (J % each_prof == 0 && J / each_prof <= ASOHF_NBINS) {
-                    int64_t b = J / each_prof;
-                    cat.profiles[(size_t)i0 * 2 * ASOHF_NBINS + (b - 1)] = aadm;
-                    cat.profiles[(size_t)i0 * 2 * ASOHF_NBINS + ASOHF_NBINS + (b - 1)] =
-                        (float)(basmas * (double)norma * (double)H.um);
-                  }
-                  float bc[3] = {__fsub_rn(S.x[p], cmv[0]), __fsub_rn(S.y[p], cmv[1]), __fsub_rn(S.z[p], cmv[2])};
-                  float bvc[3] = {__fsub_rn(S.vx[p], vc[0]), __fsub_rn(S.vy[p], vc[1]), __fsub_rn(S.vz[p], vc[2])};
-                  float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(bvc[0], bvc[0]), __fmul_rn(bvc[1], bvc[1])),
-                                         __fmul_rn(bvc[2], bvc[2]));
-                  float mp = S.m[p];
-                  acc[0] += (double)vvv2;
-                  acc[1] += (double)__fmul_rn(mp, vvv2);
-                  acc[2] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[1], bvc[2]), __fmul_rn(bc[2], bvc[1])));
-                  acc[3] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[2], bvc[0]), __fmul_rn(bc[0], bvc[2])));
-                  acc[4] += (double)__fmul_rn(mp, __fsub_rn(__fmul_rn(bc[0], bvc[1]), __fmul_rn(bc[1], bvc[0])));
-                  for (int jy = 0; jy < 3; jy++)
-                    for (int ix = 0; ix < 3; ix++)
-                      acc[5 + jy * 3 + ix] += (double)__fmul_rn(__fmul_rn(mp, bc[ix]), bc[jy]);
-                  vmax = fmaxf(vmax, vvv2);
-                  if (aadm != 0.0f) {
-                    float aa = __fadd_rn(__fadd_rn(__fmul_rn(__fdiv_rn(bv[0], aadm), bvc[0]),
-                                                   __fmul_rn(__fdiv_rn(bv[1], aadm), bvc[1])),
-                                         __fmul_rn(__fdiv_rn(bv[2], aadm), bvc[2]));
-                    acc[14] += (double)__fmul_rn(aa, mp);
-                  }
-                  acc[15] += (double)__fdiv_rn(mp, norma);
-                },
-                sh.dred);
-  for (int q = 0; q < 16; q++) acc[q] = block_sum_d(acc[q], sh.dred);
-  cnt = block_sum_ll(cnt, sh.lred);
-  vmax = block_max_f(vmax, sh.fred);
-  if (threadIdx.x == 0) {
-    cat.dmpclus[i0] = (int32_t)cnt;
-    if (cnt < H.min_num_part) {
-      cat.realclus[i0] = 0;
-      cat.vmaxclus[i0] = vmax;  // the running maximum of |v|^2 (-1 if none) stays
-    } else {
-      cat.potential_e[i0] = 0.0f;
-      cat.iplip[i0] = S.id[lip[0]];
-      double basmas = acc[15];
-      double den = basmas * (double)norma;
-      cat.angularm[i0 * 3 + 0] = (float)(acc[2] * (double)H.uv / den);
-      cat.angularm[i0 * 3 + 1] = (float)(acc[3] * (double)H.uv / den);
-      cat.angularm[i0 * 3 + 2] = (float)(acc[4] * (double)H.uv / den);
-      cat.mean_vr[i0] = (float)(acc[14] / den * (double)H.uv);
-      float in[9];
-      for (int jy = 0; jy < 3; jy++)
-        for (int ix = 0; ix < 3; ix++) in[jy * 3 + ix] = (float)(acc[5 + jy * 3 + ix] / den);
-      if (sym) {
-        in[3] = in[1];
-        in[6] = in[2];
-        in[7] = in[5];
-      }
-      float* it = cat.inertia_tensor + (size_t)i0 * 6;
-      it[0] = in[0]; it[1] = in[3]; it[2] = in[6]; it[3] = in[4]; it[4] = in[7]; it[5] = in[8];
-      cat.velocity_dispersion[i0] = (float)(sqrt(acc[0] / (double)(float)cnt) * (double)H.uv);
-      cat.vmaxclus[i0] = __fmul_rn(__fsqrt_rn(vmax), H.uv);
-      float be[3] = {0.0f, 0.0f, 0.0f};
-      diagonalise_dev(in, be);
-      sort_eigen_dev(be);
-      for (int q = 0; q < 3; q++) cat.eigenval[(size_t)i0 * 3 + q] = __fsqrt_rn(__fmul_rn(5.0f, be[q]));
-    }
-  }
-  __syncthreads();
-  return cnt;
-}
-
 __device__ __forceinline__ float so_den(float d, float rete, float pi) {
   float dr = __fmul_rn(d, rete);
   return __fmul_rn(__fmul_rn(pi, 1.3333334f), __fmul_rn(__fmul_rn(dr, dr), dr));
-}
-
-// IDs of the bound subhalo particles, in radial order, at ids_off[slot].
-__global__ void __launch_bounds__(HB)
-k_sub_write_ids(const int32_t* __restrict__ nscan, const int64_t* __restrict__ off, const int64_t* __restrict__ ids_off,
-            const int32_t* __restrict__ lip_all, const uint8_t* __restrict__ flag_all, const int32_t* __restrict__ id,
-            int32_t* __restrict__ out) {
-  __shared__ int sb[33];
-  int slot = blockIdx.x;
-  int64_t n = nscan[slot];
-  if (n == 0) return;
-  int64_t base = off[slot] + slot;
-  const int32_t* lip = lip_all + base;
-  const uint8_t* flag = flag_all + base;
-  int64_t carry = ids_off[slot];
-  for (int64_t t0 = 0; t0 < n; t0 += HB) {
-    int64_t j = t0 + threadIdx.x;
-    bool k = j < n && flag[j];
-    int tot;
-    int inc = block_scan_i(k ? 1 : 0, sb, &tot);
-    if (k) out[carry + inc - 1] = id[lip[j]];
-    carry += tot;
-  }
 }
 
 // ================================================================ main (group)
@@ -2223,7 +1867,9 @@ extern "C" int asohf_get_particles_per_halo(asohf_ctx* c, int32_t* out, int64_t 
 // one level): recentering and the host's enclosed mass (k_sub_prep); the
 // Jacobi-radius search (gather, sort, k_sub_jacobi) repeated for the
 // subhaloes whose radius must grow x1.5; a last gather at the final radius;
-// then k_sub_main: unbinding, Jacobi trim, SO walk, properties.
+// then k_sub_main_g on the staged lists: unbinding, Jacobi trim, SO walk,
+// properties.  The per-subhalo kernels run in the size tiers of the halo
+// path, single CTAs only.
 
 struct SubPrep {
   float *cx, *cy, *cz;
@@ -2423,22 +2069,6 @@ k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t
   }
 }
 
-// Reverses runs of equal distance in the first n entries (the tie order of
-// ARGSORT applied to an already sorted list, substructure.f:1161-1162).
-__device__ void reverse_tie_runs(float* dista, int32_t* lip, int64_t n) {
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    if (i > 0 && dista[i] == dista[i - 1]) continue;
-    int64_t e = i + 1;
-    while (e < n && dista[e] == dista[i]) e++;
-    for (int64_t a = i, z = e - 1; a < z; a++, z--) {
-      int32_t t = lip[a];
-      lip[a] = lip[z];
-      lip[z] = t;
-    }
-  }
-  __syncthreads();
-}
-
 struct SubMainIn {
   const int32_t* konta;   // gathered members
   const int32_t* jjac;    // members kept (J_JACOBI)
@@ -2446,268 +2076,6 @@ struct SubMainIn {
   const float* rclus;
   const float *cx, *cy, *cz, *mhost, *disthost;
 };
-
-__global__ void __launch_bounds__(HB)
-k_sub_main(Store S, HConst H, asohf_catalogue cat, const int32_t* __restrict__ work, SubMainIn in, Seg sg) {
-  __shared__ MainShared sh;
-  int slot = blockIdx.x;
-  int i0 = work[slot];
-  if (threadIdx.x == 0) { sg.nbound[slot] = 0; sg.nscan[slot] = 0; }
-  int64_t Kg = in.konta[slot];
-  int64_t konta = in.jjac[slot];
-  double masadm = in.masadm[slot];
-  float um = H.um;
-  if (masadm <= 0.0 || konta < H.min_num_part || konta > Kg) {
-    // RSUB/MSUB were set when the Jacobi radius was fixed (substructure.f:1115-1117)
-    if (threadIdx.x == 0) {
-      cat.rsub[i0] = in.rclus[slot];
-      cat.msub[i0] = (float)(masadm * (double)um);
-      cat.realclus[i0] = 0;
-    }
-    return;
-  }
-  int64_t base = sg.off[slot] + slot;
-  float* dista = sg.dista + base;
-  int32_t* lip = sg.lip + base;
-  double* pot = sg.pot + base;
-  uint8_t* flag = sg.flag + base;
-  int64_t kbase = sg.off[slot];
-  for (int64_t j = threadIdx.x; j < konta; j += blockDim.x) {
-    dista[j] = __uint_as_float((uint32_t)(sg.keys[kbase + j] & 0xffffffffull));
-    lip[j] = sg.vals[kbase + j];
-    flag[j] = 1;
-  }
-  if (threadIdx.x == 0) dista[konta] = 1.e10f;
-  __syncthreads();
-  float cx = in.cx[slot], cy = in.cy[slot], cz = in.cz[slot];
-  float mhost = in.mhost[slot], disthost = in.disthost[slot];
-  float cm0[3], v0[3], m2;
-  centromasas_block(S, dista, lip, flag, true, konta, cm0, v0, &m2, sh);
-  HaloState h;
-  for (int q = 0; q < 3; q++) { h.cm[q] = cm0[q]; h.v[q] = v0[q]; }
-  h.radio = in.rclus[slot];                 // RSUB
-  h.masa = (float)(masadm * (double)um);    // MSUB
-  h.realclus = cat.realclus[i0];
-  reverse_tie_runs(dista, lip, konta);
-  unsigned long long ep = 2ull * (unsigned long long)konta;
-  int64_t k2 = konta, iv;
-  float ref_max = dista[k2 - 1];
-  int64_t contaerr = konta;
-  int fac = 0;
-  auto write_back = [&]() {
-    if (threadIdx.x == 0) {
-      cat.clusrxcm[i0] = h.cm[0]; cat.clusrycm[i0] = h.cm[1]; cat.clusrzcm[i0] = h.cm[2];
-      cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2];
-      cat.rsub[i0] = h.radio; cat.msub[i0] = h.masa;
-      cat.dmpclus[i0] = (int32_t)konta;
-    }
-  };
-  while (contaerr > 0 || fac < 3) {
-    fac++;
-    int64_t prev = k2;
-    iv = k2;
-    ep += (unsigned long long)k2;
-    unbinding8_block(S, H, fac, ref_max, dista, lip, flag, pot, k2, iv, h, sh);
-    int64_t nk2;
-    reordenar_compact(dista, lip, flag, k2, &iv, &nk2, sh);
-    k2 = nk2;
-    __syncthreads();
-    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
-    contaerr = prev - k2;
-    if (fac > 100000) break;
-  }
-  if (k2 < H.min_num_part) {
-    write_back();
-    if (threadIdx.x == 0) cat.realclus[i0] = 0;
-    return;
-  }
-  fac = 0;
-  contaerr = k2;
-  while (contaerr > 0 || fac < 4) {
-    fac++;
-    int64_t prev = k2;
-    iv = k2;
-    ep += (unsigned long long)k2;
-    unbinding_sigma_block(S, H, fac, lip, flag, k2, iv, h, sh);
-    int64_t nk2;
-    reordenar_compact(dista, lip, flag, k2, &iv, &nk2, sh);
-    k2 = nk2;
-    __syncthreads();
-    ref_max = k2 > 0 ? dista[k2 - 1] : 1.e10f;
-    contaerr = prev - k2;
-    if (fac > 100000) break;
-  }
-  if (k2 < H.min_num_part) {
-    write_back();
-    if (threadIdx.x == 0) cat.realclus[i0] = 0;
-    return;
-  }
-  // Jacobi trim after unbinding (substructure.f:1241-1264)
-  int64_t ncapas = 0;
-  float rshell = 0.0f;
-  {
-    double m0 = (double)__fdiv_rn(h.masa, um);
-    double bx = (double)__fdiv_rn(dista[k2 - 1], disthost);
-    double e0 = eq_jacobi_dev(bx, m0 * (double)um / (double)mhost);
-    if (e0 > 0.0) {
-      // M(J) = MASADM - sum_{i >= J} m_i ; largest J in [1, k2] with EQ < 0
-      __shared__ double s_tot;
-      double tot = tile_prefix_d(0, k2, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
-                                 [&](int64_t, double) {}, sh.dred);
-      if (threadIdx.x == 0) s_tot = tot;
-      __syncthreads();
-      tot = s_tot;
-      long long f = -1;
-      double mf = 0.0;
-      tile_prefix_d(0, k2, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
-                    [&](int64_t j, double pre) {
-                      int64_t J = j + 1;
-                      double mj = m0 - (tot - pre + (double)S.m[lip[j]]);  // after subtracting m(J..K2)
-                      double bxj = (double)__fdiv_rn(dista[j], disthost);
-                      double e2 = eq_jacobi_dev(bxj, mj * (double)um / (double)mhost);
-                      if (e2 < 0.0 && J > f) { f = J; mf = mj; }
-                    },
-                    sh.dred);
-      long long fmax = -bmin(-f, sh);  // -1: none
-      __shared__ double s_mf;
-      if (f == fmax && f > 0) s_mf = mf;
-      __syncthreads();
-      int64_t J;
-      double mj;
-      if (fmax <= 0) {
-        J = 0;
-        mj = m0 - tot;
-      } else {
-        J = fmax;
-        mj = s_mf;
-      }
-      h.radio = J + 1 <= k2 ? dista[J] : (J + 1 == k2 + 1 ? dista[k2] : 1.e10f);
-      h.masa = (float)(mj * (double)um);
-      k2 = J;
-      ncapas = J;
-      rshell = J >= 1 ? dista[J - 1] : 1.e10f;
-      __syncthreads();
-    }
-  }
-  if (k2 < H.min_num_part) {
-    write_back();
-    if (threadIdx.x == 0) cat.realclus[i0] = 0;
-    return;
-  }
-  // SO walk without early exit (substructure.f:1293-1463)
-  float pi = H.pi, rote = H.rote, rete = H.rete;
-  float norma = S.norma;
-  int64_t jjcore = (int64_t)fmaxf(10.0f, __fdiv_rn((float)k2, 100.0f));
-  float thr[6] = {__fdiv_rn(2500.0f, H.omegaz), __fdiv_rn(500.0f, H.omegaz), __fdiv_rn(200.0f, H.omegaz),
-                  2500.0f, 500.0f, 200.0f};
-  int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
-  long long jt[7];
-  for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
-  double best_v = -1.0;
-  long long best_j = LLONG_MAX;
-  double best_b = 0.0;
-  auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(S.m[lip[j]], norma); };
-  double btot = tile_prefix_d(0, k2, 0.0, mn_of,
-                              [&](int64_t j, double bas8) {
-                                int64_t J = j + 1;
-                                if (J <= jjcore) return;
-                                float d = dista[j];
-                                float vol = so_den(d, rete, pi);
-                                float delta2 = (float)((double)norma * bas8 / (double)vol / (double)rote);
-                                for (int q = 0; q < 6; q++)
-                                  if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
-                                if (delta2 <= H.contrastec && J > jvir_min && J < jt[6]) jt[6] = J;
-                                float bas2 = (float)(bas8 / (double)d);
-                                if ((double)bas2 > best_v || ((double)bas2 == best_v && J < best_j)) {
-                                  best_v = bas2; best_j = J; best_b = bas8;
-                                }
-                              },
-                              sh.dred);
-  for (int q = 0; q < 7; q++) jt[q] = bmin(jt[q], sh);
-  __shared__ double s_at[7];
-  tile_prefix_d(0, k2, 0.0, mn_of,
-                [&](int64_t j, double bas8) {
-                  for (int q = 0; q < 7; q++)
-                    if (j + 1 == jt[q]) s_at[q] = bas8;
-                },
-                sh.dred);
-  double vacc[3];
-  for (int ax = 0; ax < 3; ax++) {
-    const float* vv = ax == 0 ? S.vx : (ax == 1 ? S.vy : S.vz);
-    vacc[ax] = tile_prefix_d(0, k2, 0.0, [&](int64_t j) {
-                               int p = lip[j];
-                               return (double)__fmul_rn(__fdiv_rn(S.m[p], norma), vv[p]);
-                             },
-                             [&](int64_t, double) {}, sh.dred);
-  }
-  sh.bestv[threadIdx.x] = best_v;
-  sh.bestj[threadIdx.x] = best_j;
-  sh.bestb[threadIdx.x] = best_b;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double bv = -1.0;
-    long long bj = LLONG_MAX;
-    double bb = 0.0;
-    for (int t = 0; t < HB; t++) {
-      if (sh.bestj[t] == LLONG_MAX) continue;
-      if (sh.bestv[t] > bv || (sh.bestv[t] == bv && sh.bestj[t] < bj)) {
-        bv = sh.bestv[t]; bj = sh.bestj[t]; bb = sh.bestb[t];
-      }
-    }
-    if (bj != LLONG_MAX) {
-      cat.vcmax[i0] = (float)bv;
-      cat.mcmax[i0] = (float)bb;
-      cat.rcmax[i0] = dista[bj - 1];
-    }
-    float* mo[6] = {cat.m2500c, cat.m500c, cat.m200c, cat.m2500m, cat.m500m, cat.m200m};
-    float* ro[6] = {cat.r2500c, cat.r500c, cat.r200c, cat.r2500m, cat.r500m, cat.r200m};
-    for (int q = 0; q < 6; q++) {
-      if (jt[q] != LLONG_MAX) {
-        int64_t J = jt[q];
-        float d = dista[J - 1];
-        float vol = so_den(d, rete, pi);
-        float delta2 = (float)((double)norma * s_at[q] / (double)vol / (double)rote);
-        mo[q][i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
-        ro[q][i0] = d;
-        if (J == jjcore + 1) { mo[q][i0] = -1.0f; ro[q][i0] = -1.0f; }
-      } else {
-        mo[q][i0] = 0.0f;
-        ro[q][i0] = 0.0f;
-      }
-    }
-    if (jt[6] != LLONG_MAX) {
-      int64_t J = jt[6];
-      float d = dista[J - 1];
-      float vol = so_den(d, rete, pi);
-      float delta2 = (float)((double)norma * s_at[6] / (double)vol / (double)rote);
-      cat.masa[i0] = __fmul_rn(__fmul_rn(__fmul_rn(delta2, vol), rote), um);
-      cat.radio[i0] = d;
-    } else {
-      cat.masa[i0] = 0.0f;
-      cat.radio[i0] = 0.0f;
-    }
-    h.v[0] = (float)(vacc[0] / btot);
-    h.v[1] = (float)(vacc[1] / btot);
-    h.v[2] = (float)(vacc[2] / btot);
-    float bas = __fdiv_rn(__fmul_rn(__fmul_rn(cat.vcmax[i0], norma), H.cgr), rete);
-    cat.vcmax[i0] = __fmul_rn(__fsqrt_rn(bas), H.uv);
-    cat.mcmax[i0] = __fmul_rn(__fmul_rn(cat.mcmax[i0], norma), um);
-  }
-  __syncthreads();
-  write_back();
-  // the properties read VX(I) from the catalogue
-  if (threadIdx.x == 0) { cat.vx[i0] = h.v[0]; cat.vy[i0] = h.v[1]; cat.vz[i0] = h.v[2]; }
-  __syncthreads();
-  long long nb = properties_block(S, H, cat, i0, dista, lip, flag, ncapas, rshell, cx, cy, cz, cm0, false, sh);
-  ep += (unsigned long long)(k2 + ncapas);
-  if (threadIdx.x == 0) {
-    atomicAdd(&sg.work[1], ep);
-    bool ok = nb >= H.min_num_part && H.want_ids;
-    sg.nbound[slot] = ok ? (int32_t)nb : 0;
-    sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
-    sg.status[slot] = 0;
-  }
-}
 
 // Work list of a substructure level: REALCLUS != 0, largest RSUB first.
 // ---------------------------------------------------------------- subhalo main (staged)
