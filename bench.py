@@ -35,6 +35,9 @@ sys.path.insert(0, ROOT)
 
 CPU_SAMPLE = "cfg4s"
 BYTES_PER_ELEMENT_PASS = 32  # d, m, |v| 12, position index read + dist/index written
+# DRAM bytes (read + write) per element-pass of k_halo_main: 9.06 GB over
+# 136.4M element-passes in one ncu capture of the 256^3 workload's launches
+DRAM_BYTES_PER_ELEMENT_PASS = 66.4
 
 
 def peaks():
@@ -273,18 +276,25 @@ def main():
     e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "particles/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel (kernel names only: "host:" entries are
+    # host phases, "k_x/tier" entries split a kernel's launches by size tier)
     hbm, src = peaks()
-    top = max(kstats.items(), key=lambda kv: kv[1][0]) if kstats else ("none", (0.0, 1))
+    kern = {k: v for k, v in kstats.items() if not k.startswith("host:") and "/" not in k}
+    top = max(kern.items(), key=lambda kv: kv[1][0]) if kern else ("none", (0.0, 1))
     name, (tot_ms, nl) = top
     roofline = None
     if name == "halo_main" and tot_ms > 0:
         alg = float(work[0]) * BYTES_PER_ELEMENT_PASS
         ach = alg / (tot_ms * 1e-3) / 1e9
         roofline = {"kernel": name, "bound": "hbm", "achieved": round(ach, 2), "peak": hbm, "unit": "GB/s",
-                    "frac": round(ach / hbm, 5), "traffic": None, "peak_source": src,
+                    "frac": round(ach / hbm, 5),
+                    "traffic": round(float(work[0]) / nl * DRAM_BYTES_PER_ELEMENT_PASS),
+                    "peak_source": src,
                     "algorithmic_bytes_per_launch": alg / nl, "avg_launch_ms": tot_ms / nl,
-                    "note": f"{BYTES_PER_ELEMENT_PASS} B per element-pass, element-passes counted on device"}
+                    "note": (f"{BYTES_PER_ELEMENT_PASS} B per element-pass, element-passes counted on the device; "
+                             f"traffic: {DRAM_BYTES_PER_ELEMENT_PASS} DRAM bytes per element-pass from an ncu "
+                             "capture of every k_halo_main launch of the 256^3 workload, times this launch's "
+                             "element-passes")}
     out = {
         "metric": metric, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -296,7 +306,11 @@ def main():
                    "l2": "inputs > L2 (4.3 GB of particles per step)"},
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches),
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in
-                                sorted(kstats.items(), key=lambda kv: -kv[1][0])[:40]},
+                                sorted(kstats.items(), key=lambda kv: -kv[1][0])
+                                if not k.startswith("host:")},
+        "host_phases_ms_per_step": {k[5:]: round(v[0] / args.steps, 3) for k, v in
+                                    sorted(kstats.items(), key=lambda kv: -kv[1][0])
+                                    if k.startswith("host:")},
         "stage_s": {k: round(v, 4) for k, v in r.stage_s.items()},
         "catalogue": {"haloes": int((r.cat.realclus[: r.cat.nclus] == -1).sum()),
                       "subhaloes": int((r.cat.realclus[: r.cat.nclus] > 0).sum()),
