@@ -77,6 +77,13 @@ struct asohf_ctx {
   // kernel phases of one call, when the stream is idle
   char* seg = nullptr;
   size_t seg_size = 0, seg_used = 0;
+  // device copies kept between calls: MOMENTO's sin^2 table for s2_nx, and
+  // the last RADX(0:NX+1) the layer was given (h_radx: its host copy)
+  float* d_s2 = nullptr;
+  int s2_nx = 0;
+  float* d_radx = nullptr;
+  float* h_radx = nullptr;
+  int radx_n = 0;
   // counters of kernels launched by this context (reported by the bench)
   int64_t launches = 0;
   // work counters written by kernels (element-passes of the per-halo kernels)

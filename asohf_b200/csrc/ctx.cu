@@ -180,6 +180,9 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   free_particles(c->p);
   free_particles(c->alt);
   cudaFree(c->rows);
+  cudaFree(c->d_s2);
+  cudaFree(c->d_radx);
+  free(c->h_radx);
   cudaFree(c->d_ndmpart_x);
   cudaFree(c->d_colstart);
   cudaFree(c->d_colpart);

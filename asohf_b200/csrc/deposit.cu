@@ -1139,7 +1139,7 @@ template <typename T>
 __global__ void k_tsc_base(const float* __restrict__ x, const float* __restrict__ y,
                            const float* __restrict__ z, const float* __restrict__ m, int64_t n_per,
                            int batch, int nx, float xl, float dx, const float* __restrict__ radx,
-                           T* __restrict__ acc) {
+                           float mdiv, T* __restrict__ acc) {
   int64_t ntot = n_per * batch;
   size_t g = (size_t)nx * nx * nx;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < ntot;
@@ -1151,7 +1151,7 @@ __global__ void k_tsc_base(const float* __restrict__ x, const float* __restrict_
     tsc_weights(xp, radx[ix - 1], radx[ix], radx[ix + 1], dx, wx);
     tsc_weights(yp, radx[jy - 1], radx[jy], radx[jy + 1], dx, wy);
     tsc_weights(zp, radx[kz - 1], radx[kz], radx[kz + 1], dx, wz);
-    float mp = m[q];
+    float mp = mdiv == 1.0f ? m[q] : __fdiv_rn(m[q], mdiv);  // mass, or mass / DENBAS
     T* a = acc + (size_t)b * g;
 #pragma unroll
     for (int kk = -1; kk <= 1; kk++) {
@@ -1293,7 +1293,7 @@ extern "C" int asohf_interpolate_density_tsc(asohf_ctx* c, int nx, float lado0, 
     {
       int kt_ = ktime_begin(c, "tsc_base");
       k_tsc_base<double><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-        c->p.x, c->p.y, c->p.z, c->p.m, n, 1, nx, xl, dx, dradx, acc);
+        c->p.x, c->p.y, c->p.z, c->p.m, n, 1, nx, xl, dx, dradx, 1.0f, acc);
       ktime_end(c, kt_);
     }
     c->launches++;
@@ -1341,16 +1341,16 @@ extern "C" int asohf_interpolate_density_tsc(asohf_ctx* c, int nx, float lado0, 
   return ASOHF_OK;
 }
 
-// exported for poisson.cu (batched forward deposit)
+// exported for poisson.cu (batched forward deposit of m / denbas)
 int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* dradx, int batch,
                          int64_t n_per, const float* x, const float* y, const float* z,
-                         const float* m, float* acc) {
+                         const float* m, float denbas, float* acc) {
   int64_t n = n_per * batch;
   if (n > 0) {
     {
       int kt_ = ktime_begin(c, "tsc_base_batched");
       k_tsc_base<float><<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(x, y, z, m, n_per, batch,
-                                                                              nx, xl, dx, dradx, acc);
+                                                                              nx, xl, dx, dradx, denbas, acc);
       ktime_end(c, kt_);
     }
     c->launches++;

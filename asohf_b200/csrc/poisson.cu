@@ -17,7 +17,7 @@
 
 int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* dradx, int batch,
                          int64_t n_per, const float* x, const float* y, const float* z,
-                         const float* m, float* acc);
+                         const float* m, float denbas, float* acc);
 
 #define ASOHF_CUFFT(call)                                                        \
   do {                                                                           \
@@ -82,38 +82,79 @@ static void momento_axis(int nx, float* s2) {
 }
 
 // Half-spectrum multiply: spec[(k*N + j)*(N/2+1) + i] *= KKK(i,j,k) / N^3.
+// One warp per (batch, k, j) row of N/2+1 values, lanes along i.
 __global__ void k_green(cufftComplex* __restrict__ spec, int nx, int batch, const float* __restrict__ s2,
                         float del2, float inv_n3) {
-  int nh = nx / 2 + 1;
-  int64_t per = (int64_t)nx * nx * nh;
-  int64_t tot = per * batch;
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot;
-       q += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = q % per;
-    int i = (int)(r % nh);
-    int j = (int)((r / nh) % nx);
-    int k = (int)(r / ((int64_t)nh * nx));
-    float den = (i == 0 && j == 0 && k == 0) ? 1.0e30f : __fadd_rn(__fadd_rn(s2[i], s2[j]), s2[k]);
-    float kkk = -del2 / den;
-    float f = __fmul_rn(kkk, inv_n3);
-    cufftComplex v = spec[q];
-    v.x = __fmul_rn(v.x, f);
-    v.y = __fmul_rn(v.y, f);
-    spec[q] = v;
+  const int nh = nx / 2 + 1;
+  const int64_t rows = (int64_t)batch * nx * nx;
+  const int lane = threadIdx.x & 31;
+  for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < rows;
+       row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int j = (int)(row % nx), k = (int)((row / nx) % nx);
+    cufftComplex* r = spec + row * nh;
+#pragma unroll 5
+    for (int i = lane; i < nh; i += 32) {
+      float den = (i == 0 && j == 0 && k == 0) ? 1.0e30f : __fadd_rn(__fadd_rn(s2[i], s2[j]), s2[k]);
+      float kkk = -del2 / den;
+      float f = __fmul_rn(kkk, inv_n3);
+      cufftComplex v = r[i];
+      v.x = __fmul_rn(v.x, f);
+      v.y = __fmul_rn(v.y, f);
+      r[i] = v;
+    }
   }
 }
 
+// MOMENTO's table on the device, computed once per NX.
+static int green_table(asohf_ctx* c, int nx, const float** out) {
+  if (c->s2_nx != nx) {
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(c->d_s2);
+    c->d_s2 = nullptr;
+    c->s2_nx = 0;
+    float* hs2 = (float*)malloc(4 * (size_t)nx);
+    momento_axis(nx, hs2);
+    cudaError_t e = cudaMalloc(&c->d_s2, 4 * (size_t)nx);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_s2, hs2, 4 * (size_t)nx, cudaMemcpyHostToDevice);
+    free(hs2);
+    ASOHF_CUDA(e);
+    c->s2_nx = nx;
+  }
+  *out = c->d_s2;
+  return ASOHF_OK;
+}
+
+// RADX(0:NX+1) on the device; re-uploaded only when its contents change.
+int radx_device(asohf_ctx* c, int nx, const float* radx, const float** out) {
+  const int n = nx + 2;
+  if (c->radx_n != n || memcmp(c->h_radx, radx, 4 * (size_t)n) != 0) {
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->radx_n != n) {
+      cudaFree(c->d_radx);
+      free(c->h_radx);
+      c->d_radx = nullptr;
+      c->h_radx = (float*)malloc(4 * (size_t)n);
+      c->radx_n = 0;
+      if (!c->h_radx) return ASOHF_ERR_CAPACITY;
+      ASOHF_CUDA(cudaMalloc(&c->d_radx, 4 * (size_t)n));
+      c->radx_n = n;
+    }
+    memcpy(c->h_radx, radx, 4 * (size_t)n);
+    ASOHF_CUDA(cudaMemcpy(c->d_radx, radx, 4 * (size_t)n, cudaMemcpyHostToDevice));
+  }
+  *out = c->d_radx;
+  return ASOHF_OK;
+}
+
+// FFT solve on the context stream; returns once enqueued.
 static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* rho, float* pot) {
   int64_t gc = (int64_t)nx * nx * (nx / 2 + 1) * batch;
   cufftComplex* spec = (cufftComplex*)arena_alloc(c, sizeof(cufftComplex) * gc);
-  float* ds2 = (float*)arena_alloc(c, 4 * (size_t)nx);
-  if (!spec || !ds2) return ASOHF_ERR_CAPACITY;
-  float* hs2 = (float*)malloc(4 * (size_t)nx);
-  momento_axis(nx, hs2);
-  ASOHF_CUDA(cudaMemcpyAsync(ds2, hs2, 4 * (size_t)nx, cudaMemcpyHostToDevice, c->stream));
+  if (!spec) return ASOHF_ERR_CAPACITY;
+  const float* ds2;
+  ASOHF_CHECK(green_table(c, nx, &ds2));
   FftPlan* P;
-  int rc = get_plan(c, nx, batch, &P);
-  if (rc) { free(hs2); return rc; }
+  ASOHF_CHECK(get_plan(c, nx, batch, &P));
   int kt_ = ktime_begin(c, "fft_r2c");
   ASOHF_CUFFT(cufftExecR2C(P->r2c, (cufftReal*)rho, spec));
   ktime_end(c, kt_);
@@ -121,7 +162,9 @@ static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* r
   float inv_n3 = 1.0f / ((float)nx * (float)nx * (float)nx);
   {
     int kt_ = ktime_begin(c, "green_multiply");
-    k_green<<<grid_for(gc, 256, c->num_sms * 8), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2, inv_n3);
+    int64_t rows = (int64_t)batch * nx * nx;
+    k_green<<<grid_for(rows * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2,
+                                                                             inv_n3);
     ktime_end(c, kt_);
   }
   c->launches++;
@@ -129,13 +172,11 @@ static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* r
   ASOHF_CUFFT(cufftExecC2R(P->c2r, spec, (cufftReal*)pot));
   ktime_end(c, kt_);
   ASOHF_CUDA(cudaGetLastError());
-  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(hs2);
   return ASOHF_OK;
 }
 
 static size_t poisson_bytes(int nx, int batch) {
-  return sizeof(cufftComplex) * (size_t)nx * nx * (nx / 2 + 1) * batch + 4 * (size_t)nx + 4096;
+  return sizeof(cufftComplex) * (size_t)nx * nx * (nx / 2 + 1) * batch + 4096;
 }
 
 extern "C" int asohf_poisson_fft(asohf_ctx* c, int nx, float dx, int batch, const float* rho,
@@ -162,12 +203,6 @@ extern "C" int asohf_poisson_fft(asohf_ctx* c, int nx, float dx, int batch, cons
 }
 
 // ------------------------------------------------------------ layer
-__global__ void k_scale_inv(float* __restrict__ a, int64_t n, float d) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    a[i] = a[i] / d;
-}
-
 extern "C" int asohf_tsc_poisson_forward(asohf_ctx* c, int nx, float lado0, float dx,
                                          const float* radx, float rote, float rete, int batch,
                                          int64_t n_per, const float* x, const float* y,
@@ -176,14 +211,14 @@ extern "C" int asohf_tsc_poisson_forward(asohf_ctx* c, int nx, float lado0, floa
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
   int64_t g = (int64_t)nx * nx * nx * batch;
-  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * (size_t)(nx + 2) + 1024));
-  float* dradx = (float*)arena_alloc(c, 4 * (size_t)(nx + 2));
-  ASOHF_CUDA(cudaMemcpyAsync(dradx, radx, 4 * (size_t)(nx + 2), cudaMemcpyHostToDevice, c->stream));
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 1024));
+  const float* dradx;
+  ASOHF_CHECK(radx_device(c, nx, radx, &dradx));
   ASOHF_CUDA(cudaMemsetAsync(rho, 0, 4 * g, c->stream));
-  ASOHF_CHECK(tsc_base_batched_f32(c, nx, -lado0 / 2.0f, dx, dradx, batch, n_per, x, y, z, m, rho));
+  // each particle deposits m / (DX^3 ROTE RETE^3): the division of the cell
+  // sums (grids.f:1236-1238) moved onto the terms, so rho needs no extra pass
   float denbas = dx * dx * dx * rote * (rete * rete * rete);
-  k_scale_inv<<<grid_for(g, 256, c->num_sms * 8), 256, 0, c->stream>>>(rho, g, denbas);
-  c->launches++;
+  ASOHF_CHECK(tsc_base_batched_f32(c, nx, -lado0 / 2.0f, dx, dradx, batch, n_per, x, y, z, m, denbas, rho));
   return poisson_dev(c, nx, dx, batch, rho, pot);
 }
 
@@ -261,11 +296,11 @@ extern "C" int asohf_tsc_poisson_adjoint(asohf_ctx* c, int nx, float lado0, floa
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
   int64_t g = (int64_t)nx * nx * nx * batch;
-  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * g + 4 * (size_t)(nx + 2) + 2048));
-  float* dradx = (float*)arena_alloc(c, 4 * (size_t)(nx + 2));
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * g + 2048));
+  const float* dradx;
+  ASOHF_CHECK(radx_device(c, nx, radx, &dradx));
   float* gfield = (float*)arena_alloc(c, 4 * g);
-  if (!dradx || !gfield) return ASOHF_ERR_CAPACITY;
-  ASOHF_CUDA(cudaMemcpyAsync(dradx, radx, 4 * (size_t)(nx + 2), cudaMemcpyHostToDevice, c->stream));
+  if (!gfield) return ASOHF_ERR_CAPACITY;
   // the Green's operator is real and symmetric: its adjoint is itself
   ASOHF_CHECK(poisson_dev(c, nx, dx, batch, w, gfield));
   float denbas = dx * dx * dx * rote * (rete * rete * rete);
@@ -281,6 +316,5 @@ extern "C" int asohf_tsc_poisson_adjoint(asohf_ctx* c, int nx, float lado0, floa
     c->launches++;
   }
   ASOHF_CUDA(cudaGetLastError());
-  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  return ASOHF_OK;
+  return ASOHF_OK;  // device outputs: enqueued on the context stream
 }
