@@ -37,6 +37,7 @@ CPU_SAMPLE = "cfg4s"
 BYTES_PER_ELEMENT_PASS = 32  # d, m, |v| 12, position index read + dist/index written
 # DRAM bytes (read + write) per element-pass of k_halo_main: 9.06 GB over
 # 136.4M element-passes in one ncu capture of the 256^3 workload's launches
+# (`--config cfg2 --steps 1 --warmup 0 --no-cpu --no-layer --no-e2e`)
 DRAM_BYTES_PER_ELEMENT_PASS = 66.4
 
 
@@ -167,6 +168,8 @@ def main():
     ap.add_argument("--no-subs", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-layer", action="store_true", help="skip the deposit+Poisson layer leg")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end leg (profiling runs: only the device-timed steps)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -243,38 +246,40 @@ def main():
     n = cfg.n
     value = world * n / (ms_max * 1e-3)
 
-    # e2e: pinned host particles in, catalogue and IDs out, through the API
-    host = [a.cpu().pin_memory() for a in (snap.x, snap.y, snap.z, snap.vx, snap.vy, snap.vz, snap.m, snap.id)]
-    parts_h = SimpleNamespace(x=host[0].numpy(), y=host[1].numpy(), z=host[2].numpy(), vx=host[3].numpy(),
-                              vy=host[4].numpy(), vz=host[5].numpy(), m=host[6].numpy(), id=host[7].numpy(), n=n)
-    be = api.GpuBackend(local)
-    be.a.set_stream(torch.cuda.current_stream().cuda_stream)
+    e2e = None
+    if not args.no_e2e:
+        # e2e: pinned host particles in, catalogue and IDs out, through the API
+        host = [a.cpu().pin_memory() for a in (snap.x, snap.y, snap.z, snap.vx, snap.vy, snap.vz, snap.m, snap.id)]
+        parts_h = SimpleNamespace(x=host[0].numpy(), y=host[1].numpy(), z=host[2].numpy(), vx=host[3].numpy(),
+                                  vy=host[4].numpy(), vz=host[5].numpy(), m=host[6].numpy(), id=host[7].numpy(), n=n)
+        be = api.GpuBackend(local)
+        be.a.set_stream(torch.cuda.current_stream().cuda_stream)
 
-    def step_e2e():
-        return driver.execute(plan, be, with_subs=with_subs, particles=parts_h, download=False)
+        def step_e2e():
+            return driver.execute(plan, be, with_subs=with_subs, particles=parts_h, download=False)
 
-    re = step_e2e()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0.record(st)
-    for _ in range(args.steps):
         re = step_e2e()
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms_e2e = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / args.steps
-    t = torch.tensor([ms_e2e], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_e2e = float(t.item())
-    ncat = re.cat.nclus
-    cat_bytes = ncat * 4 * (45 + 2 * 20 + 3 + 3 + 6 + 2)
-    h2d = n * 32 + cat_bytes  # particles; the catalogue windows go both ways
-    grid_bytes = 4 * (cfg.nx ** 3 + plan.mesh.total * 32 ** 3)  # U1 and U11 after RENORM_DENSITY
-    d2h = int(re.pph.shape[0]) * 4 + cat_bytes + grid_bytes
-    e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "particles/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(st)
+        for _ in range(args.steps):
+            re = step_e2e()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_e2e = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / args.steps
+        t = torch.tensor([ms_e2e], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+        ncat = re.cat.nclus
+        cat_bytes = ncat * 4 * (45 + 2 * 20 + 3 + 3 + 6 + 2)
+        h2d = n * 32 + cat_bytes  # particles; the catalogue windows go both ways
+        grid_bytes = 4 * (cfg.nx ** 3 + plan.mesh.total * 32 ** 3)  # U1 and U11 after RENORM_DENSITY
+        d2h = int(re.pph.shape[0]) * 4 + cat_bytes + grid_bytes
+        e2e = {"value": world * n / (ms_e2e * 1e-3), "unit": "particles/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
 
     # roofline of the dominant kernel (kernel names only: "host:" entries are
     # host phases, "k_x/tier" entries split a kernel's launches by size tier)
@@ -312,6 +317,7 @@ def main():
                                     sorted(kstats.items(), key=lambda kv: -kv[1][0])
                                     if k.startswith("host:")},
         "stage_s": {k: round(v, 4) for k, v in r.stage_s.items()},
+        "halo_element_passes_per_step": int(work[0]) // args.steps,
         "catalogue": {"haloes": int((r.cat.realclus[: r.cat.nclus] == -1).sum()),
                       "subhaloes": int((r.cat.realclus[: r.cat.nclus] > 0).sum()),
                       "bound_ids": int(r.pph.shape[0])},
