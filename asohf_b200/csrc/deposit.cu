@@ -660,8 +660,9 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
   extern __shared__ double acc[];  // ACC_N doubles (padded rows), count grid, kernel table
   int32_t* scnt = (int32_t*)(acc + ACC_N);
   float* ktab = (float*)(scnt + CGX * CGX * CGZ);
-  __shared__ int s_lo[PROWS], s_pre[PROWS + 1];
+  __shared__ int s_lo[PROWS], s_pre[PROWS + 1], s_next;
   __shared__ double s_t27[27];
+  __shared__ float s_rcp[NA + 1];  // 1/n for the clipped cloud widths n <= NA
   const int2 it = W.items[blockIdx.x];
   UnitGeo g;
   unit_geo(M, B, order, it.x, dx, g);
@@ -677,6 +678,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
     for (int i = threadIdx.x - nk; i <= nk; i += blockDim.x)
       ktab[c0 + i] = kernels[(size_t)l * KW + ASOHF_NMAX_KERNELS + i];
   }
+  if (threadIdx.x >= 1 && threadIdx.x <= NA) s_rcp[threadIdx.x] = 1.0f / (float)threadIdx.x;
   __syncthreads();
   if (eqmass && threadIdx.x < 27) {  // level-0 terms of the common mass
     const float* kc = ktab + ktab_center(0);
@@ -697,25 +699,52 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
       s_pre[threadIdx.x + 1] = len;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      s_pre[0] = 0;
-      for (int r = 1; r <= nr; r++) s_pre[r] += s_pre[r - 1];
+    if (warp == 0) {  // inclusive prefix of the row lengths in place, 32 rows at a time
+      int run = 0;
+      for (int r = 1 + lane; r - lane <= nr; r += 32) {
+        int sc = r <= nr ? s_pre[r] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+          int y = __shfl_up_sync(0xffffffffu, sc, o);
+          if (lane >= o) sc += y;
+        }
+        if (r <= nr) s_pre[r] = run + sc;
+        run += __shfl_sync(0xffffffffu, sc, 31);
+      }
+      if (lane == 0) {
+        s_pre[0] = 0;
+        s_next = (int)(max(v0, vbase) - vbase);  // first candidate of this slice in these rows
+      }
     }
     __syncthreads();
-    const int64_t tot = s_pre[nr];
-    const int64_t a = max(v0, vbase) - vbase, b = min(v1, vbase + tot) - vbase;
-    for (int64_t cbase = a + (int64_t)warp * 32; cbase < b; cbase += (int64_t)nwarp * 32) {
-      int64_t v = cbase + lane;
+    const int tot = s_pre[nr];
+    const int b = (int)(min(v1, vbase + tot) - vbase);
+    // warps take 32 candidates at a time from a shared counter: a warp that
+    // met wide clouds takes fewer
+    for (;;) {
+      int cbase = 0;
+      if (lane == 0) cbase = atomicAdd(&s_next, 32);
+      cbase = __shfl_sync(0xffffffffu, cbase, 0);
+      if (cbase >= b) break;
+      const int v = cbase + lane, vlast = min(cbase + 31, b - 1);
+      // rows of the warp's first and last candidates (rows whose start is
+      // not above them), then each lane's row between the two
+      int c0 = 0, c1 = 0;
+      for (int r = 1 + lane; r <= nr; r += 32) {
+        int sp = s_pre[r];
+        c0 += sp <= cbase;
+        c1 += sp <= vlast;
+      }
+      int row = (int)__reduce_add_sync(0xffffffffu, (unsigned)c0);
+      int rhi = (int)__reduce_add_sync(0xffffffffu, (unsigned)c1);
+      while (row < rhi) {
+        int mid = (row + rhi + 1) >> 1;
+        if (s_pre[mid] <= v) row = mid; else rhi = mid - 1;
+      }
       bool hit = false;
       float mp = 0.f;
-      int ix = 0, jy = 0, kz = 0, lev = 0, i1 = 0, j1 = 0, k1 = 0, di = 0, dj = 0, dk = 0;
+      int ix = 0, jy = 0, kz = 0, lev = 0;
       if (v < b) {
-        int lo2 = 0, hi2 = nr - 1;  // row of v: last r with s_pre[r] <= v
-        while (lo2 < hi2) {
-          int mid = (lo2 + hi2 + 1) >> 1;
-          if (s_pre[mid] <= v) lo2 = mid; else hi2 = mid - 1;
-        }
-        int e = s_lo[lo2] + (int)(v - s_pre[lo2]);
+        int e = s_lo[row] + (v - s_pre[row]);
         int s = S[e];
         float4 q = P[e];
         if (s != 255 && g.pxl < q.x && q.x < g.pxr && g.pyl < q.y && q.y < g.pyr && g.pzl < q.z && q.z < g.pzr) {
@@ -725,22 +754,13 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
           ix = (int)floorf((q.x - g.xlfix) / g.dxpa) + 1;
           jy = (int)floorf((q.y - g.ylfix) / g.dxpa) + 1;
           kz = (int)floorf((q.z - g.zlfix) / g.dxpa) + 1;
-          int i2 = ix + nk, j2 = jy + nk, k2 = kz + nk;
-          i1 = ix - nk; j1 = jy - nk; k1 = kz - nk;
-          if (!(i1 > g.n1 || i2 < 1 || j1 > g.n2 || j2 < 1 || k1 > g.n3 || k2 < 1)) {
-            i1 = max(i1, 1); i2 = min(i2, g.n1);
-            j1 = max(j1, 1); j2 = min(j2, g.n2);
-            k1 = max(max(k1, 1), g.zlo); k2 = min(min(k2, g.n3), g.zhi);
-            if (k1 <= k2) {
-              mp = q.w;
-              if (eqmass && lev == 0) {  // host cell count (ix in [0, n1+1], kz in [zlo-1, zhi+1])
-                atomicAdd(&scnt[((kz - g.zlo + 1) * CGX + jy) * CGX + ix], 1);
-              } else {
-                hit = true;
-                di = i2 - i1 + 1;
-                dj = j2 - j1 + 1;
-                dk = k2 - k1 + 1;
-              }
+          if (!(ix - nk > g.n1 || ix + nk < 1 || jy - nk > g.n2 || jy + nk < 1 || kz - nk > g.n3 || kz + nk < 1) &&
+              max(max(kz - nk, 1), g.zlo) <= min(min(kz + nk, g.n3), g.zhi)) {
+            mp = q.w;
+            if (eqmass && lev == 0) {  // host cell count (ix in [0, n1+1], kz in [zlo-1, zhi+1])
+              atomicAdd(&scnt[((kz - g.zlo + 1) * CGX + jy) * CGX + ix], 1);
+            } else {
+              hit = true;
             }
           }
         }
@@ -750,35 +770,41 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
                     ((unsigned long long)(kz + 1024) << 30) | ((unsigned long long)lev << 26) |
                     (unsigned long long)(__float_as_uint(mp) >> 6)
               : ~0ull - (unsigned long long)lane;
-      unsigned grp = __match_any_sync(0xffffffffu, key);
-      if (hit) {  // the key keeps 26 bits of the mass: confirm equal masses inside the group
+      // hits of one host cell, level and mass deposit once with the group size as factor
+      unsigned grp = 1u << lane;
+      if (__popc(__ballot_sync(0xffffffffu, hit)) > 1) grp = __match_any_sync(0xffffffffu, key);
+      if (hit && (grp & (grp - 1))) {  // the key keeps 26 bits of the mass: confirm equal masses
         float m0 = __shfl_sync(grp, mp, __ffs(grp) - 1);
         unsigned same = __ballot_sync(grp, mp == m0);
         if (same != grp) grp = 1u << lane;
       }
-      float gcnt = (float)__popc(grp);
+      // host cell (11 bits per axis, offset 1024), level and group size of each hit
+      const int pxy = (ix + 1024) | ((jy + 1024) << 16);
+      const int pzl = (kz + 1024) | (lev << 16) | (__popc(grp) << 24);
       unsigned hm = __ballot_sync(0xffffffffu, hit && lane == __ffs(grp) - 1);
       while (hm) {
         int src = __ffs(hm) - 1;
         hm &= hm - 1;
-        float wm = __shfl_sync(0xffffffffu, mp, src);
-        double wc = (double)__shfl_sync(0xffffffffu, gcnt, src);
-        int wix = __shfl_sync(0xffffffffu, ix, src), wjy = __shfl_sync(0xffffffffu, jy, src);
-        int wkz = __shfl_sync(0xffffffffu, kz, src), wlev = __shfl_sync(0xffffffffu, lev, src);
-        int wi1 = __shfl_sync(0xffffffffu, i1, src), wj1 = __shfl_sync(0xffffffffu, j1, src);
-        int wk1 = __shfl_sync(0xffffffffu, k1, src), wdi = __shfl_sync(0xffffffffu, di, src);
-        int wdj = __shfl_sync(0xffffffffu, dj, src), wdk = __shfl_sync(0xffffffffu, dk, src);
+        const float wm = __shfl_sync(0xffffffffu, mp, src);
+        const int wxy = __shfl_sync(0xffffffffu, pxy, src), wzl = __shfl_sync(0xffffffffu, pzl, src);
+        const int wix = (wxy & 0xffff) - 1024, wjy = (wxy >> 16) - 1024, wkz = (wzl & 0xffff) - 1024;
+        const int wlev = (wzl >> 16) & 0xff, nk = 1 << wlev;
+        const double wc = (double)(wzl >> 24);
+        // the cloud clipped to the patch and to the unit's planes
+        const int wi1 = max(wix - nk, 1), wj1 = max(wjy - nk, 1), wk1 = max(max(wkz - nk, 1), g.zlo);
+        const int wdi = min(wix + nk, g.n1) - wi1 + 1, wdj = min(wjy + nk, g.n2) - wj1 + 1;
+        const int wdk = min(min(wkz + nk, g.n3), g.zhi) - wk1 + 1;
         const float* kc = ktab + ktab_center(wlev);
         // lanes take the cloud's (ii, jj) pairs and walk its kk planes:
         // each lane forms (m*W(ii))*W(jj) once and the plane loop reads W(kk)
         // as a broadcast.  The pair quotient is exact in float (pairs < 2^11,
-        // divisor <= 33).
+        // divisor <= 32).
         const int npair = wdi * wdj;
-        const float rdi = 1.0f / (float)wdi;
+        const float rdi = s_rcp[wdi];
         const float* wzk = kc + (wk1 - wkz);  // W(kk) of the cloud's planes
         // pair p = (jj-j1)*di + (ii-i1): the lane's first pair by division,
         // the next ones (p += 32) by adding 32 = sj*di + si
-        int ci = lane, cj = 0;
+        int ci, cj;
         {
           int q0 = (int)(((float)lane + 0.5f) * rdi);
           ci = lane - q0 * wdi;
@@ -787,12 +813,11 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
         const int sj = (int)((32.0f + 0.5f) * rdi), si = 32 - sj * wdi;
         for (int pq = lane; pq < npair; pq += 32) {
           const int ii = wi1 + ci, jj = wj1 + cj;
-          float b = __fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]);
+          float bw = __fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]);
           double* col = acc + (wk1 - g.zlo) * APLANE + (jj - 1) * AROW + (ii - 1);
-          for (int q = 0; q < wdk; q++) {
-            float tt = __fmul_rn(b, wzk[q]);
-            atomicAdd(col + q * APLANE, (double)tt * wc);
-          }
+#pragma unroll
+          for (int q = 0; q < PZ; q++)
+            if (q < wdk) atomicAdd(col + q * APLANE, __dmul_rn((double)__fmul_rn(bw, wzk[q]), wc));
           ci += si;
           cj += sj;
           if (ci >= wdi) { ci -= wdi; cj++; }
