@@ -651,20 +651,19 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
   return t;
 }
 
-struct GShared {
-  double dred[32];
-  float fred[32];
-  long long lred[32];
-  int sb[33];
-  double wv[32];
-  long long wj[32];
-  double wb[32];
+struct GShared {  // per-warp slots: HW warps at most
+  double dred[HW];
+  float fred[HW];
+  long long lred[HW];
+  double wv[HW];
+  long long wj[HW];
+  double wb[HW];
   double bc_d[2];
   long long bc_l[2];
   double at[16];
-  double wsum[32];  // per-warp totals of the scans
-  double wsum3[96];
-  long long wcnt[32];
+  double wsum[HW];  // per-warp totals of the scans
+  double wsum3[3 * HW];
+  long long wcnt[HW];
   GX x;
 };
 
@@ -793,6 +792,41 @@ __device__ void centromasas_g(const Grp<C>& g, const SegView& v, int64_t n, floa
 template <int C>
 __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& dst, const uint8_t* flag,
                           int64_t k2, int64_t* idx_vir, int64_t* k2new, GShared& sh) {
+  if constexpr (C == 1) {
+    if (blockDim.x == 32) {  // one warp: offsets from the ballots as it goes
+      const int lane = threadIdx.x;
+      const unsigned below = (1u << lane) - 1u;
+      const int64_t iv = *idx_vir;  // 1-based
+      long long reloc = LLONG_MAX;
+      int64_t d0 = 0;
+      for (int64_t j0 = 0; j0 < k2; j0 += 32) {
+        const int64_t j = j0 + lane;
+        const bool keep = j < k2 && flag[j];
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int64_t d = d0 + __popc(m & below);
+          dst.dm[d] = src.dm[j];
+          dst.mv[d] = src.mv[j];
+          dst.px[d] = src.px[j];
+          if (j + 1 >= iv && d + 1 < reloc) reloc = d + 1;
+        }
+        d0 += __popc(m);
+      }
+      for (int64_t j = d0 + lane; j < k2; j += 32) {
+        dst.dm[j] = src.dm[j];
+        dst.mv[j] = src.mv[j];
+        dst.px[j] = src.px[j];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        long long y = __shfl_xor_sync(0xffffffffu, reloc, o);
+        reloc = y < reloc ? y : reloc;
+      }
+      *k2new = d0;
+      *idx_vir = reloc == LLONG_MAX ? d0 : reloc;
+      __syncthreads();
+      return;
+    }
+  }
   int64_t lo, hi, wlo, whi;
   g.chunk(0, k2, &lo, &hi);
   warp_run(lo, hi, &wlo, &whi);

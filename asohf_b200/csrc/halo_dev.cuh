@@ -13,6 +13,7 @@
 namespace cg = cooperative_groups;
 
 #define HB 256          // threads per CTA of the per-halo kernels (at most)
+#define HW (HB / 32)    // warps per CTA (at most)
 #define IPT 4           // items per thread per tile of the block scans
 #define MAX_HIST 48     // recentering shrink steps kept in shared memory
 
@@ -50,7 +51,7 @@ struct Grp {
 // a few threads combine the C published values in rank order, so results are
 // identical on every CTA and do not depend on scheduling.
 struct GX {
-  double vred[16][32];  // per-warp partials of vector sums
+  double vred[16][HW];  // per-warp partials of vector sums
   double bres[16];      // CTA totals
   double d[16];         // published CTA values
   double dres[16];      // group totals
@@ -677,6 +678,26 @@ __device__ __forceinline__ void warp_run(int64_t lo, int64_t hi, int64_t* wlo, i
 template <int C, class V, class U>
 __device__ __forceinline__ double gscan_d(const Grp<C>& g, int64_t a, int64_t b, double carry, V val, U use,
                                           double* wbuf, GX& x) {
+  if constexpr (C == 1) {
+    if (blockDim.x == 32) {  // one warp: the walk alone, val evaluated once
+      const int lane = threadIdx.x;
+      double run = carry;
+#pragma unroll 2
+      for (int64_t j0 = a; j0 < b; j0 += 32) {
+        const int64_t j = j0 + lane;
+        double s = j < b ? val(j) : 0.0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          double y = __shfl_up_sync(0xffffffffu, s, o);
+          if (lane >= o) s += y;
+        }
+        if (j < b) use(j, run + s);
+        run += __shfl_sync(0xffffffffu, s, 31);
+      }
+      __syncthreads();
+      return run;
+    }
+  }
   int64_t lo, hi, wlo, whi;
   g.chunk(a, b, &lo, &hi);
   warp_run(lo, hi, &wlo, &whi);
@@ -742,6 +763,32 @@ __device__ __forceinline__ Aff aff_warp_scan(Aff v) {
 template <int C, class VM, class VW, class U>
 __device__ __forceinline__ void gscan_aff(const Grp<C>& g, int64_t a, int64_t b, VM valm, VW valw, U use,
                                           double* wbuf /* 3 * 32 */, GX& x, double* mt, double* qt) {
+  if constexpr (C == 1) {
+    if (blockDim.x == 32) {  // one warp: the walk alone (its final run is the pass-1 summary)
+      const int lane = threadIdx.x;
+      Aff run{0.0, 0.0, 0.0};
+#pragma unroll 2
+      for (int64_t j0 = a; j0 < b; j0 += 32) {
+        const int64_t j = j0 + lane;
+        Aff e{0.0, 0.0, 0.0};
+        if (j < b) {
+          e.m = valm(j);
+          e.w = valw(j);
+          e.q = e.m * e.w;
+        }
+        Aff s = aff_warp_scan(e);
+        if (j < b) {
+          Aff p = aff_cat(run, s);
+          use(j, p.m, p.q);
+        }
+        run = aff_cat(run, aff_shfl(s, 31));
+      }
+      __syncthreads();
+      *mt = run.m;
+      *qt = run.q;
+      return;
+    }
+  }
   int64_t lo, hi, wlo, whi;
   g.chunk(a, b, &lo, &hi);
   warp_run(lo, hi, &wlo, &whi);
