@@ -740,14 +740,36 @@ __device__ void load_segment(const Grp<C>& g, const Store& S, const unsigned lon
                              const int32_t* vals, int64_t K, const SegView& a, const SegView& b, uint8_t* flag) {
   int64_t lo, hi;
   g.chunk(0, K, &lo, &hi);
-  for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-    unsigned long long kk = keys[j];
-    int p = vals[j];
-    float mp = S.m[p];
-    a.dm[j] = make_float2(__uint_as_float((uint32_t)(kk & 0xffffffffull)), mp);
-    a.mv[j] = make_float4(mp, S.vx[p], S.vy[p], S.vz[p]);
-    a.px[j] = make_float4(S.x[p], S.y[p], S.z[p], __int_as_float(p));
-    flag[j] = 1;
+  const int bd = blockDim.x;
+  // four entries per thread: keys, then the store's fields, then the writes
+#pragma unroll 1
+  for (int64_t jb = lo + threadIdx.x; jb < hi; jb += 4 * bd) {
+    unsigned long long kk[4];
+    int p[4];
+    float f[4][7];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int64_t j = jb + u * bd;
+      kk[u] = j < hi ? keys[j] : 0ull;
+      p[u] = j < hi ? vals[j] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (jb + u * bd < hi) {
+        const int q = p[u];
+        f[u][0] = S.m[q]; f[u][1] = S.vx[q]; f[u][2] = S.vy[q]; f[u][3] = S.vz[q];
+        f[u][4] = S.x[q]; f[u][5] = S.y[q]; f[u][6] = S.z[q];
+      }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int64_t j = jb + u * bd;
+      if (j < hi) {
+        a.dm[j] = make_float2(__uint_as_float((uint32_t)(kk[u] & 0xffffffffull)), f[u][0]);
+        a.mv[j] = make_float4(f[u][0], f[u][1], f[u][2], f[u][3]);
+        a.px[j] = make_float4(f[u][4], f[u][5], f[u][6], __int_as_float(p[u]));
+        flag[j] = 1;
+      }
+    }
   }
   if (g.rank() == 0 && threadIdx.x == 0) {  // DISTA(K+1) of the sorted list
     a.dm[K] = make_float2(1.e10f, 0.f); b.dm[K] = a.dm[K];
@@ -786,6 +808,73 @@ __device__ void centromasas_g(const Grp<C>& g, const SegView& v, int64_t n, floa
   }
 }
 
+// One warp's stable compaction of [j0, j1) into dst from position d0: steps
+// of 32 entries in pairs, both steps read before either is written.
+// Returns the next free position; *reloc gets the lowest 1-based
+// destination of a kept entry at or after 1-based position iv.
+__device__ __forceinline__ int64_t compact_run(const SegView& src, const SegView& dst, const uint8_t* flag,
+                                               int64_t j0, int64_t j1, int64_t iv, int64_t d0, long long* reloc) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+#pragma unroll 1
+  for (int64_t jb = j0; jb < j1; jb += 64) {
+    bool keep[2];
+    float2 e0[2];
+    float4 e1[2], e2[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      keep[u] = j < j1 && flag[j];
+      if (j < j1) {
+        e0[u] = src.dm[j];
+        e1[u] = src.mv[j];
+        e2[u] = src.px[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      const unsigned m = __ballot_sync(0xffffffffu, keep[u]);
+      if (keep[u]) {
+        const int64_t d = d0 + __popc(m & below);
+        dst.dm[d] = e0[u];
+        dst.mv[d] = e1[u];
+        dst.px[d] = e2[u];
+        if (j + 1 >= iv && d + 1 < *reloc) *reloc = d + 1;
+      }
+      d0 += __popc(m);
+    }
+  }
+  return d0;
+}
+
+// dst[j] = src[j] for j = j0, j0 + step, ... < j1, two entries read at a time.
+__device__ __forceinline__ void copy_run(const SegView& src, const SegView& dst, int64_t j0, int64_t j1, int step) {
+#pragma unroll 1
+  for (int64_t jb = j0; jb < j1; jb += 2 * (int64_t)step) {
+    float2 e0[2];
+    float4 e1[2], e2[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int64_t j = jb + (int64_t)u * step;
+      if (j < j1) {
+        e0[u] = src.dm[j];
+        e1[u] = src.mv[j];
+        e2[u] = src.px[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int64_t j = jb + (int64_t)u * step;
+      if (j < j1) {
+        dst.dm[j] = e0[u];
+        dst.mv[j] = e1[u];
+        dst.px[j] = e2[u];
+      }
+    }
+  }
+}
+
 // REORDENAR(...,0,...) (haloes_particles.f:1696-1722): the kept entries of
 // j < k2 in order into dst, IDX_VIR relocated to the first kept entry at or
 // after it; dst[k2new, k2) = src[k2new, k2).
@@ -795,28 +884,10 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
   if constexpr (C == 1) {
     if (blockDim.x == 32) {  // one warp: offsets from the ballots as it goes
       const int lane = threadIdx.x;
-      const unsigned below = (1u << lane) - 1u;
       const int64_t iv = *idx_vir;  // 1-based
       long long reloc = LLONG_MAX;
-      int64_t d0 = 0;
-      for (int64_t j0 = 0; j0 < k2; j0 += 32) {
-        const int64_t j = j0 + lane;
-        const bool keep = j < k2 && flag[j];
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (keep) {
-          const int64_t d = d0 + __popc(m & below);
-          dst.dm[d] = src.dm[j];
-          dst.mv[d] = src.mv[j];
-          dst.px[d] = src.px[j];
-          if (j + 1 >= iv && d + 1 < reloc) reloc = d + 1;
-        }
-        d0 += __popc(m);
-      }
-      for (int64_t j = d0 + lane; j < k2; j += 32) {
-        dst.dm[j] = src.dm[j];
-        dst.mv[j] = src.mv[j];
-        dst.px[j] = src.px[j];
-      }
+      const int64_t d0 = compact_run(src, dst, flag, 0, k2, iv, 0, &reloc);
+      copy_run(src, dst, d0 + lane, k2, 32);
       for (int o = 16; o > 0; o >>= 1) {
         long long y = __shfl_xor_sync(0xffffffffu, reloc, o);
         reloc = y < reloc ? y : reloc;
@@ -844,28 +915,10 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
   int64_t d0 = off + woff;
   long long reloc = LLONG_MAX;
   const int64_t iv = *idx_vir;  // 1-based
-  const unsigned below = (1u << lane) - 1u;
-#pragma unroll 2
-  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
-    const int64_t j = j0 + lane;
-    const bool keep = j < whi && flag[j];
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (keep) {
-      const int64_t d = d0 + __popc(m & below);
-      dst.dm[d] = src.dm[j];
-      dst.mv[d] = src.mv[j];
-      dst.px[d] = src.px[j];
-      if (j + 1 >= iv && d + 1 < reloc) reloc = d + 1;
-    }
-    d0 += __popc(m);
-  }
+  compact_run(src, dst, flag, wlo, whi, iv, d0, &reloc);
   const int64_t nn = tot;
   g.chunk(nn, k2, &lo, &hi);
-  for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-    dst.dm[j] = src.dm[j];
-    dst.mv[j] = src.mv[j];
-    dst.px[j] = src.px[j];
-  }
+  copy_run(src, dst, lo + threadIdx.x, hi, blockDim.x);
   gmin_llv<1>(g, &reloc, sh.lred, sh.x);
   *k2new = nn;
   *idx_vir = reloc == LLONG_MAX ? nn : reloc;
@@ -943,26 +996,44 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
     bb = __fmul_rn(bb, bb);
     double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // 7 sums and the kept count
     g.chunk(0, k2, &lo, &hi);
-#pragma unroll 4
-    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      float potok = (float)(((pot_jj + pot[j]) - pot1) * aa8);
-      float vesc2 = __fmul_rn(2.0f, fabsf(potok));
-      float4 q = v.mv[j];
-      float ax = __fsub_rn(q.y, h.v[0]), ay = __fsub_rn(q.z, h.v[1]), az = __fsub_rn(q.w, h.v[2]);
-      float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
-      bool keep = !(vvv2 > __fmul_rn(bb, vesc2));
-      flag[j] = keep;
-      s[7] += keep ? 1.0 : 0.0;
-      if (keep && j < idx_vir) {
-        float4 p = v.px[j];
-        double bas = (double)q.x;
-        s[0] += (double)p.x * bas;
-        s[1] += (double)p.y * bas;
-        s[2] += (double)p.z * bas;
-        s[3] += (double)q.y * bas;
-        s[4] += (double)q.z * bas;
-        s[5] += (double)q.w * bas;
-        s[6] += bas;
+    const int bd = blockDim.x;
+    // pairs of entries per thread, both read before either flag is stored
+#pragma unroll 1
+    for (int64_t jb = lo + threadIdx.x; jb < hi; jb += 2 * bd) {
+      double pt[2];
+      float4 qv[2], pv[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int64_t j = jb + u * bd;
+        if (j < hi) {
+          pt[u] = pot[j];
+          qv[u] = v.mv[j];
+          if (j < idx_vir) pv[u] = v.px[j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int64_t j = jb + u * bd;
+        if (j >= hi) break;
+        float potok = (float)(((pot_jj + pt[u]) - pot1) * aa8);
+        float vesc2 = __fmul_rn(2.0f, fabsf(potok));
+        const float4 q = qv[u];
+        float ax = __fsub_rn(q.y, h.v[0]), ay = __fsub_rn(q.z, h.v[1]), az = __fsub_rn(q.w, h.v[2]);
+        float vvv2 = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+        bool keep = !(vvv2 > __fmul_rn(bb, vesc2));
+        flag[j] = keep;
+        s[7] += keep ? 1.0 : 0.0;
+        if (keep && j < idx_vir) {
+          const float4 p = pv[u];
+          double bas = (double)q.x;
+          s[0] += (double)p.x * bas;
+          s[1] += (double)p.y * bas;
+          s[2] += (double)p.z * bas;
+          s[3] += (double)q.y * bas;
+          s[4] += (double)q.z * bas;
+          s[5] += (double)q.w * bas;
+          s[6] += bas;
+        }
       }
     }
     gsum_dv<8>(g, s, sh.x);
@@ -999,24 +1070,39 @@ __device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac
     double thr = (double)bb * sigma2;
     double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     g.chunk(0, k2, &lo, &hi);
-#pragma unroll 4
-    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      float4 q = v.mv[j];
-      float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
-      float bas = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
-      bool keep = !((double)bas > thr);
-      flag[j] = keep;
-      s[7] += keep ? 1.0 : 0.0;
-      if (keep && j < idx_vir) {
-        float4 p = v.px[j];
-        double w = (double)q.x;
-        s[0] += (double)p.x * w;
-        s[1] += (double)p.y * w;
-        s[2] += (double)p.z * w;
-        s[3] += (double)q.y * w;
-        s[4] += (double)q.z * w;
-        s[5] += (double)q.w * w;
-        s[6] += w;
+    const int bd = blockDim.x;
+#pragma unroll 1
+    for (int64_t jb = lo + threadIdx.x; jb < hi; jb += 2 * bd) {
+      float4 qv[2], pv[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int64_t j = jb + u * bd;
+        if (j < hi) {
+          qv[u] = v.mv[j];
+          if (j < idx_vir) pv[u] = v.px[j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int64_t j = jb + u * bd;
+        if (j >= hi) break;
+        const float4 q = qv[u];
+        float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
+        float bas = __fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+        bool keep = !((double)bas > thr);
+        flag[j] = keep;
+        s[7] += keep ? 1.0 : 0.0;
+        if (keep && j < idx_vir) {
+          const float4 p = pv[u];
+          double w = (double)q.x;
+          s[0] += (double)p.x * w;
+          s[1] += (double)p.y * w;
+          s[2] += (double)p.z * w;
+          s[3] += (double)q.y * w;
+          s[4] += (double)q.z * w;
+          s[5] += (double)q.w * w;
+          s[6] += w;
+        }
       }
     }
     gsum_dv<8>(g, s, sh.x);
@@ -1049,15 +1135,15 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
   gscan_d(g, 0, konta, 0.0,
             [&](int64_t j) {
               float4 p = v.px[j];
-              float a = dist3(p.x, p.y, p.z, cx, cy, cz);
-              bool in = a <= rshell;
-              flag[j] = in;
+              bool in = dist3(p.x, p.y, p.z, cx, cy, cz) <= rshell;
               return in ? (double)__fdiv_rn(v.mv[j].x, norma) : 0.0;
             },
             [&](int64_t j, double basmas) {
               int64_t J = j + 1;
-              if (!flag[j]) return;
               float4 p = v.px[j], q = v.mv[j];
+              const bool in = dist3(p.x, p.y, p.z, cx, cy, cz) <= rshell;
+              flag[j] = in;
+              if (!in) return;
               float bv[3] = {__fsub_rn(p.x, cx), __fsub_rn(p.y, cy), __fsub_rn(p.z, cz)};
               float aadm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(bv[0], bv[0]), __fmul_rn(bv[1], bv[1])),
                                                 __fmul_rn(bv[2], bv[2])));

@@ -668,32 +668,58 @@ __device__ __forceinline__ void warp_run(int64_t lo, int64_t hi, int64_t* wlo, i
   *whi = lo + (per * (w + 1) < n ? per * (w + 1) : n);
 }
 
+// Steps of 32 entries are walked in batches of SB: the terms of a batch are
+// all read before its first consumer runs, so a warp has SB steps of loads
+// in flight although the consumers store to memory (which the compiler
+// cannot move loads across).
+#define SB 2
+
+// One warp's inclusive walk of [j0, j1) from *run: val(j) gives the term,
+// use(j, prefix) consumes it; *run receives the total.
+template <class V, class U>
+__device__ __forceinline__ void warp_walk_d(int64_t j0, int64_t j1, double* run_io, V val, U use) {
+  const int lane = threadIdx.x & 31;
+  double run = *run_io;
+#pragma unroll 1
+  for (int64_t jb = j0; jb < j1; jb += 32 * SB) {
+    double t[SB];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      t[u] = j < j1 ? val(j) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      double s = t[u];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        double y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      if (j < j1) use(j, run + s);
+      run += __shfl_sync(0xffffffffu, s, 31);
+    }
+  }
+  *run_io = run;
+}
+
 // Inclusive prefix over [a, b) in index order: val(j) gives the term,
 // use(j, prefix) consumes it.  The range is split into the group's CTA
 // chunks and each chunk into one contiguous run per warp; a first pass sums
 // the runs, a second walks each run 32 entries at a time with a warp scan,
 // starting from the totals of everything before it, so a CTA synchronises a
 // fixed number of times per call whatever the length.  val is evaluated
-// twice per entry.  Returns carry + the group total; ends synchronised.
+// twice per entry (once for a one-warp group, which walks directly) and
+// must not read what use stores.  Returns carry + the group total; ends
+// synchronised.
 template <int C, class V, class U>
 __device__ __forceinline__ double gscan_d(const Grp<C>& g, int64_t a, int64_t b, double carry, V val, U use,
                                           double* wbuf, GX& x) {
   if constexpr (C == 1) {
-    if (blockDim.x == 32) {  // one warp: the walk alone, val evaluated once
-      const int lane = threadIdx.x;
+    if (blockDim.x == 32) {  // one warp: the walk alone
       double run = carry;
-#pragma unroll 2
-      for (int64_t j0 = a; j0 < b; j0 += 32) {
-        const int64_t j = j0 + lane;
-        double s = j < b ? val(j) : 0.0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          double y = __shfl_up_sync(0xffffffffu, s, o);
-          if (lane >= o) s += y;
-        }
-        if (j < b) use(j, run + s);
-        run += __shfl_sync(0xffffffffu, s, 31);
-      }
+      warp_walk_d(a, b, &run, val, use);
       __syncthreads();
       return run;
     }
@@ -713,18 +739,7 @@ __device__ __forceinline__ double gscan_d(const Grp<C>& g, int64_t a, int64_t b,
   double off = 0.0, tot = ctot;
   if constexpr (C > 1) gexcl_d(g, ctot, &off, &tot, x);
   double run = carry + off + woff;
-#pragma unroll 2
-  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
-    const int64_t j = j0 + lane;
-    double s = j < whi ? val(j) : 0.0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      double y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
-    }
-    if (j < whi) use(j, run + s);
-    run += __shfl_sync(0xffffffffu, s, 31);
-  }
+  warp_walk_d(wlo, whi, &run, val, use);
   g.sync();
   return carry + tot;
 }
@@ -760,29 +775,43 @@ __device__ __forceinline__ Aff aff_warp_scan(Aff v) {
   return v;
 }
 
+// One warp's walk of [j0, j1) from *run (batches of SB steps, terms read
+// first); *run receives the summary of everything walked.
+template <class VM, class VW, class U>
+__device__ __forceinline__ void warp_walk_aff(int64_t j0, int64_t j1, Aff* run_io, VM valm, VW valw, U use) {
+  const int lane = threadIdx.x & 31;
+  Aff run = *run_io;
+#pragma unroll 1
+  for (int64_t jb = j0; jb < j1; jb += 32 * SB) {
+    double tm[SB], tw[SB];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      tm[u] = j < j1 ? valm(j) : 0.0;
+      tw[u] = j < j1 ? valw(j) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      Aff e{tm[u], tw[u], tm[u] * tw[u]};
+      Aff s = aff_warp_scan(e);
+      if (j < j1) {
+        Aff p = aff_cat(run, s);
+        use(j, p.m, p.q);
+      }
+      run = aff_cat(run, aff_shfl(s, 31));
+    }
+  }
+  *run_io = run;
+}
+
 template <int C, class VM, class VW, class U>
 __device__ __forceinline__ void gscan_aff(const Grp<C>& g, int64_t a, int64_t b, VM valm, VW valw, U use,
-                                          double* wbuf /* 3 * 32 */, GX& x, double* mt, double* qt) {
+                                          double* wbuf /* 3 * HW */, GX& x, double* mt, double* qt) {
   if constexpr (C == 1) {
     if (blockDim.x == 32) {  // one warp: the walk alone (its final run is the pass-1 summary)
-      const int lane = threadIdx.x;
       Aff run{0.0, 0.0, 0.0};
-#pragma unroll 2
-      for (int64_t j0 = a; j0 < b; j0 += 32) {
-        const int64_t j = j0 + lane;
-        Aff e{0.0, 0.0, 0.0};
-        if (j < b) {
-          e.m = valm(j);
-          e.w = valw(j);
-          e.q = e.m * e.w;
-        }
-        Aff s = aff_warp_scan(e);
-        if (j < b) {
-          Aff p = aff_cat(run, s);
-          use(j, p.m, p.q);
-        }
-        run = aff_cat(run, aff_shfl(s, 31));
-      }
+      warp_walk_aff(a, b, &run, valm, valw, use);
       __syncthreads();
       *mt = run.m;
       *qt = run.q;
@@ -795,16 +824,20 @@ __device__ __forceinline__ void gscan_aff(const Grp<C>& g, int64_t a, int64_t b,
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // pass 1: summary of this warp's run
   Aff run{0.0, 0.0, 0.0};
-#pragma unroll 2
-  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
-    const int64_t j = j0 + lane;
-    Aff e{0.0, 0.0, 0.0};
-    if (j < whi) {
-      e.m = valm(j);
-      e.w = valw(j);
-      e.q = e.m * e.w;
+#pragma unroll 1
+  for (int64_t jb = wlo; jb < whi; jb += 32 * SB) {
+    double tm[SB], tw[SB];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int64_t j = jb + 32 * u + lane;
+      tm[u] = j < whi ? valm(j) : 0.0;
+      tw[u] = j < whi ? valw(j) : 0.0;
     }
-    run = aff_cat(run, aff_shfl(aff_warp_scan(e), 31));
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      Aff e{tm[u], tw[u], tm[u] * tw[u]};
+      run = aff_cat(run, aff_shfl(aff_warp_scan(e), 31));
+    }
   }
   if (lane == 0) { wbuf[3 * w] = run.m; wbuf[3 * w + 1] = run.w; wbuf[3 * w + 2] = run.q; }
   __syncthreads();
@@ -837,22 +870,7 @@ __device__ __forceinline__ void gscan_aff(const Grp<C>& g, int64_t a, int64_t b,
   }
   // pass 2: prefixes
   run = pre;
-#pragma unroll 2
-  for (int64_t j0 = wlo; j0 < whi; j0 += 32) {
-    const int64_t j = j0 + lane;
-    Aff e{0.0, 0.0, 0.0};
-    if (j < whi) {
-      e.m = valm(j);
-      e.w = valw(j);
-      e.q = e.m * e.w;
-    }
-    Aff s = aff_warp_scan(e);
-    if (j < whi) {
-      Aff p = aff_cat(run, s);
-      use(j, p.m, p.q);
-    }
-    run = aff_cat(run, aff_shfl(s, 31));
-  }
+  warp_walk_aff(wlo, whi, &run, valm, valw, use);
   g.sync();
   *mt = tot.m;
   *qt = tot.q;
