@@ -59,7 +59,8 @@ def load():
                      "asohf_sort_dm_particles_x", "asohf_prune_poor_haloes",
                      "asohf_halofind_particles", "asohf_substructure_particles",
                      "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
-                     "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers"]:
+                     "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers",
+                     "asohf_copy_to_host_sm"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -129,6 +130,24 @@ class Asohf:
     def set_profiling(self, on: bool):
         """Brackets the main kernels with CUDA events (diagnostics)."""
         _check(self.L.asohf_set_profiling(self.h, C.c_int(int(on))), "asohf_set_profiling")
+
+    def copy_to_host_sm(self, dst, src, stream=None):
+        """Enqueues dst[:] = src[:] (page-locked host tensor <- device tensor
+        of this context's GPU, same byte size, a multiple of 16) as SM
+        stores on `stream` (a torch stream; the context stream when None)."""
+        import torch
+        nb = src.numel() * src.element_size()
+        if not dst.is_pinned() or dst.numel() * dst.element_size() != nb or not dst.is_contiguous() \
+                or not src.is_contiguous() or not src.is_cuda or dst.dtype != src.dtype:
+            raise ValueError("copy_to_host_sm: a contiguous page-locked tensor of the device tensor's size")
+        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        head = nb - nb % 16 if dst.data_ptr() % 16 == 0 and src.data_ptr() % 16 == 0 else 0
+        _check(self.L.asohf_copy_to_host_sm(self.h, C.c_void_p(dst.data_ptr()), C.c_void_p(src.data_ptr()),
+                                            C.c_int64(head), s), "asohf_copy_to_host_sm")
+        if head < nb:  # the last few bytes (or an unaligned buffer) by an ordinary copy on the same stream
+            e = head // src.element_size()
+            with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+                dst.view(-1)[e:].copy_(src.view(-1)[e:], non_blocking=True)
 
     def work_counters(self, reset: bool = False):
         """Element-passes of the halo (entry 0) and subhalo (entry 1) kernels."""
@@ -327,32 +346,63 @@ class GpuBackend:
     def density_renorm(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, fdm):
         """DENSITY then RENORM_DENSITY with the grids kept on the device
         between the two calls and copied once into page-locked host arrays
-        owned by the backend (valid until its next density_renorm)."""
+        owned by the backend (valid until its next density_renorm).  The copy
+        runs on a stream of its own while the caller goes on with the halo
+        finder: the arrays hold the grids once sync_outputs() has returned
+        (driver.execute calls it before it returns)."""
         import torch
         n11 = max(mesh.total, 1) * abi.NAMRX ** 3
         dev = f"cuda:{self.a.device}"
+        self.sync_outputs()  # the previous copy reads the device grids rewritten below
         if getattr(self, "_g1", None) is None or self._g1.numel() != nx ** 3:
             self._g1 = torch.empty(nx ** 3, dtype=torch.float32, device=dev)
             self._h1 = torch.empty(nx ** 3, dtype=torch.float32).pin_memory()
         if getattr(self, "_g11", None) is None or self._g11.numel() < n11:
             self._g11 = torch.empty(n11, dtype=torch.float32, device=dev)
             self._h11 = torch.empty(n11, dtype=torch.float32).pin_memory()
+        # both calls return with their work complete on the device
         self.a.density(nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, self._g1, self._g11)
         self.a.renorm_density(nx, mesh, fdm, self._g1, self._g11)
-        self._h1.copy_(self._g1)
-        self._h11[:n11].copy_(self._g11[:n11])
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream(device=dev)
+        self._grids_pending = n11  # issued after SORT_DM_PARTICLES_X (see sort_x)
         u1 = self._h1.numpy().reshape(nx, nx, nx)
         u11 = self._h11[:n11].numpy().reshape(-1, abi.NAMRX ** 3)[: mesh.total]
         return u1, u11
+
+    def _issue_grid_copy(self):
+        # SM stores, not a copy engine, so the halo finder's short copies on
+        # the context stream do not queue behind this one; issued once the
+        # x-sort (whose store permutation it would slow down) is done
+        import torch
+        n11 = getattr(self, "_grids_pending", None)
+        if n11 is None:
+            return
+        self._grids_pending = None
+        self.a.copy_to_host_sm(self._h1, self._g1, self._copy_stream)
+        self.a.copy_to_host_sm(self._h11[:n11], self._g11[:n11], self._copy_stream)
+        self._grids_done = torch.cuda.Event()
+        self._grids_done.record(self._copy_stream)
+
+    def sort_x(self, nx, lado0):
+        nd = self.a.sort_dm_particles_x(nx, lado0)
+        self._issue_grid_copy()
+        return nd
+
+    def sync_outputs(self):
+        """Waits for the host copies of the grids left in flight by
+        density_renorm (issued after the next sort_x, or here)."""
+        self._issue_grid_copy()
+        ev = getattr(self, "_grids_done", None)
+        if ev is not None:
+            ev.synchronize()
+            self._grids_done = None
 
     def tsc_deposit(self, nx, lado0, dx, radx, rote, rete, mesh, fp64=True):
         u1 = np.zeros(nx ** 3, np.float32)
         u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)
         self.a.interpolate_density_tsc(nx, lado0, dx, radx, rote, rete, mesh, u1, u11)
         return u1.reshape(nx, nx, nx), u11[: mesh.total]
-
-    def sort_x(self, nx, lado0):
-        return self.a.sort_dm_particles_x(nx, lado0)
 
     def prune_poor_haloes(self, consts, cat, low1, low2, facrad, do_need_to_count):
         self.a.prune_poor_haloes(consts, cat, low1, low2, facrad, do_need_to_count)

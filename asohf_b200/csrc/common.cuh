@@ -60,6 +60,7 @@ struct asohf_ctx {
   float mmin = 0.f;
   // x-slab index (SORT_DM_PARTICLES_X) and the column index built from it
   int nx_sorted = 0;
+  int ndmpart_cap = 0;               // entries of d_ndmpart_x
   int32_t* d_ndmpart_x = nullptr;   // NX+1 entries
   int64_t ncols = 0;                // columns of the (y,z) index
   float col_xl = 0.f, col_dx = 0.f;

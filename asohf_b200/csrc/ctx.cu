@@ -350,3 +350,34 @@ extern "C" int asohf_work_counters(asohf_ctx* c, int64_t* out, int reset) {
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return ASOHF_OK;
 }
+
+// ------------------------------------------------------------ host copies
+// Device -> page-locked host copy made by SM stores through the host
+// buffer's device mapping instead of a copy engine: a large copy issued this
+// way on a stream of its own does not queue ahead of the short copies the
+// context's host phases make meanwhile.
+__global__ void k_store_to_host(const uint4* __restrict__ src, uint4* __restrict__ dst, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+extern "C" int asohf_copy_to_host_sm(asohf_ctx* c, void* host_dst, const void* dev_src, int64_t bytes,
+                                     void* stream) {
+  if (!c || bytes < 0 || (bytes && (!host_dst || !dev_src))) return ASOHF_ERR_INVALID;
+  if (bytes % 16 || (uintptr_t)host_dst % 16 || (uintptr_t)dev_src % 16) return ASOHF_ERR_INVALID;
+  if (bytes == 0) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  cudaPointerAttributes ha, da;
+  ASOHF_CUDA(cudaPointerGetAttributes(&ha, host_dst));
+  ASOHF_CUDA(cudaPointerGetAttributes(&da, dev_src));
+  if (ha.type != cudaMemoryTypeHost || !ha.devicePointer || da.type != cudaMemoryTypeDevice ||
+      da.device != c->device)
+    return ASOHF_ERR_INVALID;  // page-locked host memory and this context's device memory only
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int64_t n = bytes / 16;
+  int grid = c->num_sms / 4 > 0 ? c->num_sms / 4 : 1;
+  k_store_to_host<<<grid, 256, 0, s>>>((const uint4*)dev_src, (uint4*)ha.devicePointer, n);
+  ASOHF_CUDA(cudaGetLastError());
+  c->launches++;
+  return ASOHF_OK;
+}

@@ -160,9 +160,12 @@ extern "C" int asohf_sort_dm_particles_x(asohf_ctx* c, int nx, float lado0, int3
   size_t need = 16 * (size_t)n + 8 * (size_t)n + tb + 4096;
   size_t need2 = column_index_bytes(n, nx);
   ASOHF_CHECK(arena_reserve(c, need > need2 ? need : need2));
-  if (!c->d_ndmpart_x || c->nx_sorted < nx) {
+  if (!c->d_ndmpart_x || c->ndmpart_cap < nx + 1) {  // grows only (cudaFree waits for the whole device)
     cudaFree(c->d_ndmpart_x);
+    c->d_ndmpart_x = nullptr;
+    c->ndmpart_cap = 0;
     ASOHF_CUDA(cudaMalloc(&c->d_ndmpart_x, sizeof(int32_t) * (size_t)(nx + 1)));
+    c->ndmpart_cap = nx + 1;
   }
   if (n > 0) {
     uint32_t* k0 = (uint32_t*)arena_alloc(c, 4 * n);

@@ -124,7 +124,7 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
     pph = np.zeros(n_id_cap, np.int32)
     nhallev = np.zeros(mesh.nl + 1, np.int32)
     base_of_level = np.concatenate([[0], np.cumsum(cand.nhallev)])
-    slot_of_truth = {}
+    slot_of_truth = np.zeros(max(int(snap.halo_pos.shape[0]), 1), np.int64)  # generator halo -> slot
     t0 = time.perf_counter()
     for ir in range(mesh.nl + 1):
         lo, hi = int(base_of_level[ir]), int(base_of_level[ir + 1])
@@ -151,9 +151,8 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
         truth = truth[re_sort_haloes(cat, nhallev, ir)]
         low1 = int(nhallev[:ir].sum()) + 1
         low2 = int(nhallev[: ir + 1].sum())
-        for q, t in enumerate(truth):
-            if t >= 0:
-                slot_of_truth[int(t)] = low1 + q
+        known = truth >= 0
+        slot_of_truth[truth[known]] = low1 + np.nonzero(known)[0]
         if nhallev[ir] == 0:
             continue
         backend.halofind_particles(consts, mesh, cat, low1, low2, pph)
@@ -188,6 +187,8 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
     live = cat.realclus[: cat.nclus] != 0
     n_ids = int(cat.indcs[: cat.nclus][live][:, 1].max()) if live.any() else 0
     ids = backend.final_ids(pph, n_ids)
+    if hasattr(backend, "sync_outputs"):  # host grids copied while the halo finder ran
+        backend.sync_outputs()
     return RunResult(npe, u1, u11, nd, cat, ids, nhallev, subs_lev,
                      backend.download() if download else None, T, mesh)
 

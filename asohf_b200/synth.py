@@ -356,33 +356,43 @@ def build_candidates(snap: Snapshot, mesh: Mesh, dx: float, seed: int = 99,
 def build_sub_candidates(snap: Snapshot, host_slot: dict, host_ok, dx: float, nl: int,
                          seed: int = 98):
     """Stand-in for SEARCH_SUBSTRUCTURE_GRID: one candidate per generated
-    subhalo whose host survived the halo stage.  host_slot maps a generator
-    halo index to its 1-based catalogue slot; host_ok(slot) says whether the
-    host is a confirmed halo.  Returns per-candidate arrays and SUBS_LEV."""
+    subhalo whose host survived the halo stage.  host_slot[h] is the 1-based
+    catalogue slot of generator halo h (0: none); host_ok(slots) says, for an
+    array of slots, which hosts are confirmed haloes.  The centre offsets and
+    radius factors are drawn for every generated subhalo (one seeded stream),
+    so a candidate's values do not depend on which others are kept.  Returns
+    per-candidate arrays, ordered by level (stable), and SUBS_LEV."""
     cfg = snap.cfg
     rng = np.random.Generator(np.random.PCG64(seed))
     H = cfg.n_haloes
-    rows = []
-    for s in range(H, snap.halo_pos.shape[0]):
-        host = int(snap.halo_host[s])
-        slot = host_slot.get(host)
-        if slot is None or not host_ok(slot):
-            continue
-        r = snap.halo_r200[s]
-        c = snap.halo_pos[s] + rng.standard_normal(3) * 0.05 * r
-        lev = int(np.clip(math.floor(math.log2(max(dx / max(r / 2.0, 1e-9), 1.0))), 1, nl))
-        rows.append((lev, c, r * rng.uniform(0.8, 1.2), slot, s))
-    rows.sort(key=lambda t: t[0])
+    ns = snap.halo_pos.shape[0] - H
     subs_lev = np.zeros(nl + 1, np.int32)
-    for t in rows:
-        subs_lev[t[0]] += 1
-    if not rows:
-        z = np.zeros(0, np.float32)
-        return z, z, z, z, np.zeros(0, np.int32), np.zeros(0, np.int64), subs_lev
-    c = np.array([t[1] for t in rows])
+    z = np.zeros(0, np.float32)
+    empty = (z, z, z, z, np.zeros(0, np.int32), np.zeros(0, np.int64), subs_lev)
+    if ns <= 0:
+        return empty
+    off = rng.standard_normal((ns, 3))
+    fac = rng.uniform(0.8, 1.2, ns)
+    idx = np.arange(H, H + ns)
+    hosts = np.asarray(snap.halo_host[H:], np.int64)
+    hs = np.asarray(host_slot, np.int64)
+    inside = (hosts >= 0) & (hosts < hs.shape[0])
+    slot = np.zeros(ns, np.int64)
+    slot[inside] = hs[hosts[inside]]
+    keep = slot > 0
+    keep[keep] = np.asarray(host_ok(slot[keep]), bool)
+    if not keep.any():
+        return empty
+    idx, slot, off, fac = idx[keep], slot[keep], off[keep], fac[keep]
+    r = np.asarray(snap.halo_r200[idx], np.float64)
+    c = np.asarray(snap.halo_pos[idx], np.float64) + off * (0.05 * r)[:, None]
+    ratio = np.maximum(dx / np.maximum(r / 2.0, 1e-9), 1.0)
+    lev = np.clip(np.floor(np.log2(ratio)).astype(np.int64), 1, nl)
+    o = np.argsort(lev, kind="stable")
+    lev, c, rad, slot, idx = lev[o], c[o], (r * fac)[o], slot[o], idx[o]
+    np.add.at(subs_lev, lev, 1)
     return (c[:, 0].astype(np.float32), c[:, 1].astype(np.float32), c[:, 2].astype(np.float32),
-            np.array([t[2] for t in rows], np.float32), np.array([t[3] for t in rows], np.int32),
-            np.array([t[4] for t in rows], np.int64), subs_lev)
+            rad.astype(np.float32), slot.astype(np.int32), idx.astype(np.int64), subs_lev)
 
 
 def _halo_table(cfg: SnapshotConfig, rng):

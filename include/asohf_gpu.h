@@ -50,6 +50,14 @@ int asohf_kernel_stats(asohf_ctx *ctx, int i, const char **name, double *total_m
  * element-passes of the halo kernel, 1: of the subhalo kernel), optionally
  * reset after reading. */
 int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
+/* Host I/O, no counterpart in the reference: enqueues on `cuda_stream`
+ * (the context stream when NULL) a copy of `bytes` bytes from device memory
+ * of this context's GPU to page-locked host memory, made by SM stores
+ * rather than a copy engine so that it overlaps the context's own host
+ * copies.  Both pointers and bytes must be multiples of 16 and host_dst must
+ * hold `bytes` bytes; the copy is complete when the stream reaches it. */
+int asohf_copy_to_host_sm(asohf_ctx *ctx, void *host_dst, const void *dev_src, int64_t bytes,
+                          void *cuda_stream);
 /* Tuning, no counterpart in the reference: haloes with at least
  * min_members members are refined by a thread-block cluster, the others by
  * one CTA each (results are the same either way).  0 restores the default
