@@ -40,6 +40,7 @@ struct CatMirror {
   int n;              // entries 0..n-1 addressable
   int w0;             // first entry of the call's window
   bool host;
+  bool prune;         // only the fields PRUNE_POOR_HALOES reads and writes move
 };
 
 #define CAT_F1(X) X(masa) X(radio) X(clusrx) X(clusry) X(clusrz) X(clusrxcm) X(clusrycm) X(clusrzcm) \
@@ -48,6 +49,9 @@ struct CatMirror {
   X(m2500m) X(r2500m) X(velocity_dispersion) X(kinetic_e) X(potential_e)
 #define CAT_I1(X) X(patchclus) X(realclus) X(levhal) X(dmpclus) X(iplip)
 #define CAT_FM(X) X(angularm, 3) X(profiles, 2 * ASOHF_NBINS) X(eigenval, 3) X(inertia_tensor, 6)
+// fields PRUNE_POOR_HALOES reads, and writes
+#define CAT_PRUNE_IN(X) X(clusrx) X(clusry) X(clusrz) X(radio) X(realclus) X(dmpclus)
+#define CAT_PRUNE_OUT(X) X(realclus) X(dmpclus)
 // fields of host entries the subhalo kernels read
 #define CAT_HOST(X) X(realclus, 1) X(masa, 1) X(msub, 1) X(clusrx, 1) X(clusry, 1) X(clusrz, 1) \
   X(profiles, 2 * ASOHF_NBINS)
@@ -65,14 +69,24 @@ static size_t cat_bytes(int n) {
 }
 
 static int cat_mirror_in(asohf_ctx* c, asohf_catalogue* h, int n, int on_device, CatMirror* m, int w0,
-                         bool hosts = false) {
+                         bool hosts = false, bool prune = false) {
   m->h = *h;
   m->n = n;
   m->w0 = w0 < 0 ? 0 : (w0 > n ? n : w0);
   m->host = !on_device;
+  m->prune = prune;
   if (on_device) { m->d = *h; return ASOHF_OK; }
   m->d = *h;
   const size_t a = (size_t)m->w0, cnt = (size_t)(n - m->w0);
+  if (prune) {  // the prune kernels touch six fields of the window
+#define P(f)                                                                                        \
+  m->d.f = (decltype(m->d.f))arena_alloc(c, 4 * (size_t)n + 4);                                    \
+  if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                           \
+  if (cnt) ASOHF_CUDA(cudaMemcpyAsync(m->d.f + a, h->f + a, 4 * cnt, cudaMemcpyHostToDevice, c->stream));
+    CAT_PRUNE_IN(P)
+#undef P
+    return ASOHF_OK;
+  }
 #define F(f)                                                                                        \
   m->d.f = (decltype(m->d.f))arena_alloc(c, 4 * (size_t)n + 4);                                    \
   if (!m->d.f) return ASOHF_ERR_CAPACITY;                                                           \
@@ -100,6 +114,13 @@ static int cat_mirror_in(asohf_ctx* c, asohf_catalogue* h, int n, int on_device,
 static int cat_mirror_out(asohf_ctx* c, CatMirror* m) {
   if (!m->host || m->n == m->w0) return ASOHF_OK;
   const size_t a = (size_t)m->w0, cnt = (size_t)(m->n - m->w0);
+  if (m->prune) {
+#define P(f) ASOHF_CUDA(cudaMemcpyAsync(m->h.f + a, m->d.f + a, 4 * cnt, cudaMemcpyDeviceToHost, c->stream));
+    CAT_PRUNE_OUT(P)
+#undef P
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+    return ASOHF_OK;
+  }
 #define F(f) ASOHF_CUDA(cudaMemcpyAsync(m->h.f + a, m->d.f + a, 4 * cnt, cudaMemcpyDeviceToHost, c->stream));
   CAT_F1(F) CAT_I1(F)
 #undef F
@@ -202,7 +223,7 @@ extern "C" int asohf_prune_poor_haloes(asohf_ctx* c, const asohf_consts* k, asoh
   arena_reset(c);
   ASOHF_CHECK(arena_reserve(c, cat_bytes(low2) + 4096));
   CatMirror m;
-  ASOHF_CHECK(cat_mirror_in(c, cat, low2, on_device, &m, low1 - 1));
+  ASOHF_CHECK(cat_mirror_in(c, cat, low2, on_device, &m, low1 - 1, false, true));
   int nh = low2 - low1 + 1;
   if (do_need_to_count == 1)
     {
