@@ -44,9 +44,9 @@ struct asohf_ctx {
   cudaStream_t stream = 0;
   // streams for per-halo launches that run beside the cluster launch,
   // forked from and joined back into `stream` with the events
-  static const int NSIDE = 3;
-  cudaStream_t side[NSIDE] = {nullptr, nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join[NSIDE] = {nullptr, nullptr, nullptr};
+  static const int NSIDE = 5;
+  cudaStream_t side[NSIDE] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[NSIDE] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int num_sms = 148;
   // size tiers of the per-halo launches (members): >= cluster_min a CTA
   // cluster, >= tier2_k 256 threads, >= tier1_k 128 threads, else 32

@@ -322,9 +322,37 @@ static int split_tiers(asohf_ctx* c, const int32_t* hcount, int n, int32_t* dbuf
   return ASOHF_OK;
 }
 
+// Reorders the cluster tier's slot list (tier 3, at the front of its
+// device buffer) into runs for clusters of cb (at most 16), 8 and 4 CTAs by
+// member count: a CTA's share stays near CLUSTER_SHARE entries.
+#define CLUSTER_SHARE 32768
+static int split_cluster_tier(asohf_ctx* c, const int32_t* hcount, int n, int cb, Tiers* T, int nsub[3],
+                              int32_t* sub[3]) {
+  auto pick = [&](int32_t k) {
+    if (cb < 8) return 0;                                 // no clusters: one CTA each
+    if (cb < 16) return k > 4 * CLUSTER_SHARE ? 0 : 2;  // 8 CTAs at most
+    return k > 8 * CLUSTER_SHARE ? 0 : (k > 4 * CLUSTER_SHARE ? 1 : 2);
+  };
+  int32_t* h = (int32_t*)malloc(4 * (size_t)(T->n[3] > 0 ? T->n[3] : 1));
+  int cnt[3] = {0, 0, 0};
+  for (int i = 0; i < n; i++)
+    if (hcount[i] >= c->cluster_min) cnt[pick(hcount[i])]++;
+  int fill[3] = {0, cnt[0], cnt[0] + cnt[1]};
+  for (int i = 0; i < n; i++)
+    if (hcount[i] >= c->cluster_min) h[fill[pick(hcount[i])]++] = i;
+  if (T->n[3]) ASOHF_CUDA(cudaMemcpyAsync(T->slots[3], h, 4 * (size_t)T->n[3], cudaMemcpyHostToDevice, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  free(h);
+  for (int q = 0; q < 3; q++) {
+    nsub[q] = cnt[q];
+    sub[q] = T->slots[3] + (q == 0 ? 0 : (q == 1 ? cnt[0] : cnt[0] + cnt[1]));
+  }
+  return ASOHF_OK;
+}
+
 template <int C>
 __device__ __forceinline__ int group_slot(const int32_t* slots) {
-  if constexpr (C == 1) return slots[blockIdx.x];
+  if constexpr (C <= 1) return slots[blockIdx.x];
   else return slots[blockIdx.x / C];
 }
 
@@ -691,7 +719,7 @@ struct GShared {  // per-warp slots: HW warps at most
 // Values the leader (rank 0, thread 0) stored in sh.bc_* , seen by the group.
 template <int C>
 __device__ __forceinline__ void gbcast(const Grp<C>& g, double* d, long long* l, GShared& sh) {
-  if constexpr (C == 1) {
+  if constexpr (C <= 1) {
     __syncthreads();
     *d = sh.bc_d[0];
     *l = sh.bc_l[0];
@@ -902,8 +930,8 @@ __device__ __forceinline__ void copy_run(const SegView& src, const SegView& dst,
 template <int C>
 __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& dst, const uint8_t* flag,
                           int64_t k2, int64_t* idx_vir, int64_t* k2new, GShared& sh) {
-  if constexpr (C == 1) {
-    if (blockDim.x == 32) {  // one warp: offsets from the ballots as it goes
+  if constexpr (C <= 1) {
+    if (C == 0 || blockDim.x == 32) {  // one warp: offsets from the ballots as it goes
       const int lane = threadIdx.x;
       const int64_t iv = *idx_vir;  // 1-based
       long long reloc = LLONG_MAX;
@@ -1248,7 +1276,7 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
 }
 
 template <int C>
-__global__ void __launch_bounds__(HB, 3)
+__global__ void __launch_bounds__(C == 0 ? 32 : HB, C == 0 ? 24 : 3)
 k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogue cat,
             const int32_t* __restrict__ work, GrowOut go, SegG sg) {
   __shared__ GShared sh;
@@ -1745,7 +1773,9 @@ static int big_cluster(asohf_ctx* c) {
 
 // The cluster tier on the context stream, the CTA tiers on the side streams,
 // the context stream waiting for all.
-#define LAUNCH_TIERS(KERN, CB, T, ...)                                                              \
+#define LAUNCH_TIERS(KERN, CB, T, ...) LAUNCH_TIERS_W(KERN, CB, 1, T, __VA_ARGS__)
+// W0: group template argument of the 32-thread tier (0: the one-warp build)
+#define LAUNCH_TIERS_W(KERN, CB, W0, T, ...)                                                        \
   do {                                                                                              \
     ASOHF_CHECK(fork_all(c));                                                                       \
     if ((T).n[3] > 0) {                                                                             \
@@ -1758,7 +1788,10 @@ static int big_cluster(asohf_ctx* c) {
         static const char* const nm_[3] = {#KERN "/cta32", #KERN "/cta128", #KERN "/cta256"};       \
         cudaStream_t s_ = c->side[2 - t_];                                                          \
         int k_ = ktime_begin(c, nm_[t_], s_);                                                       \
-        ASOHF_CUDA(launch_grp(KERN<1>, 1, (T).n[t_], kTierThreads[t_], s_, (T).slots[t_], __VA_ARGS__)); \
+        if (t_ == 0)                                                                                \
+          ASOHF_CUDA(launch_grp(KERN<W0>, 1, (T).n[0], 32, s_, (T).slots[0], __VA_ARGS__));         \
+        else                                                                                        \
+          ASOHF_CUDA(launch_grp(KERN<1>, 1, (T).n[t_], kTierThreads[t_], s_, (T).slots[t_], __VA_ARGS__)); \
         ktime_end(c, k_, s_);                                                                       \
       }                                                                                             \
     ASOHF_CHECK(join_all(c));                                                                       \
@@ -1950,8 +1983,40 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     htime_end(c, "host:halo_gather_sort", ht);
     ht = htime_now();
     {
+      // the cluster tier by size: every cluster synchronisation costs the
+      // same whatever the list length, so a halo gets the smallest cluster
+      // that keeps its CTAs' shares near CLUSTER_SHARE entries
+      int nsub[3] = {0, 0, 0};  // clusters of CB, 8, 4 CTAs
+      int32_t* sub[3] = {tm.slots[3], tm.slots[3], tm.slots[3]};
+      if (tm.n[3] > 0) ASOHF_CHECK(split_cluster_tier(c, hk, ns, CB, &tm, nsub, sub));
       int kt_ = ktime_begin(c, "halo_main");
-      LAUNCH_TIERS(k_halo_main, CB, tm, S, H, m.d, d_work, g, sg);
+      ASOHF_CHECK(fork_all(c));
+      static const int subC[3] = {16, 8, 4};
+      static const char* const subn[3] = {"k_halo_main/cluster", "k_halo_main/cluster8", "k_halo_main/cluster4"};
+      for (int q = 0; q < 3; q++) {
+        if (nsub[q] == 0) continue;
+        cudaStream_t s_ = q == 0 ? c->stream : c->side[2 + q];
+        int k_ = ktime_begin(c, subn[q], s_);
+        const int cs = q == 0 ? CB : subC[q];
+        if (cs == 16) ASOHF_CUDA(launch_grp(k_halo_main<16>, 16, nsub[q], HB, s_, sub[q], S, H, m.d, d_work, g, sg));
+        else if (cs == 8) ASOHF_CUDA(launch_grp(k_halo_main<8>, 8, nsub[q], HB, s_, sub[q], S, H, m.d, d_work, g, sg));
+        else if (cs == 4) ASOHF_CUDA(launch_grp(k_halo_main<4>, 4, nsub[q], HB, s_, sub[q], S, H, m.d, d_work, g, sg));
+        else ASOHF_CUDA(launch_grp(k_halo_main<1>, 1, nsub[q], HB, s_, sub[q], S, H, m.d, d_work, g, sg));
+        ktime_end(c, k_, s_);
+        c->launches++;
+      }
+      for (int t_ = 2; t_ >= 0; t_--)
+        if (tm.n[t_] > 0) {
+          static const char* const nm_[3] = {"k_halo_main/cta32", "k_halo_main/cta128", "k_halo_main/cta256"};
+          cudaStream_t s_ = c->side[2 - t_];
+          int k_ = ktime_begin(c, nm_[t_], s_);
+          if (t_ == 0) ASOHF_CUDA(launch_grp(k_halo_main<0>, 1, tm.n[0], 32, s_, tm.slots[0], S, H, m.d, d_work, g, sg));
+          else ASOHF_CUDA(launch_grp(k_halo_main<1>, 1, tm.n[t_], kTierThreads[t_], s_, tm.slots[t_], S, H, m.d,
+                                     d_work, g, sg));
+          ktime_end(c, k_, s_);
+          c->launches++;
+        }
+      ASOHF_CHECK(join_all(c));
       ktime_end(c, kt_);
     }
     ASOHF_CUDA(cudaGetLastError());

@@ -17,22 +17,23 @@ namespace cg = cooperative_groups;
 #define IPT 4           // items per thread per tile of the block scans
 #define MAX_HIST 48     // recentering shrink steps kept in shared memory
 
-// A halo is refined by a group of C CTAs: one CTA (C = 1) or a thread-block
-// cluster whose CTAs split every element loop into contiguous chunks and
-// combine partial results through distributed shared memory.
+// A halo is refined by a group of C CTAs: one CTA (C = 1; C = 0 marks a
+// CTA of one warp, whose code keeps only the one-warp paths) or a
+// thread-block cluster whose CTAs split every element loop into contiguous
+// chunks and combine partial results through distributed shared memory.
 template <int C>
 struct Grp {
   __device__ __forceinline__ unsigned rank() const {
-    if constexpr (C == 1) return 0;
+    if constexpr (C <= 1) return 0;
     else return cg::this_cluster().block_rank();
   }
   __device__ __forceinline__ void sync() const {
-    if constexpr (C == 1) __syncthreads();
+    if constexpr (C <= 1) __syncthreads();
     else cg::this_cluster().sync();
   }
   // this CTA's contiguous part of [a, b)
   __device__ __forceinline__ void chunk(int64_t a, int64_t b, int64_t* lo, int64_t* hi) const {
-    if constexpr (C == 1) {
+    if constexpr (C <= 1) {
       *lo = a;
       *hi = b;
     } else {
@@ -43,7 +44,7 @@ struct Grp {
   }
   // first global warp and warp stride for warp-strided loops
   __device__ __forceinline__ int warp0() const { return (int)rank() * (blockDim.x >> 5) + (threadIdx.x >> 5); }
-  __device__ __forceinline__ int nwarps() const { return C * (blockDim.x >> 5); }
+  __device__ __forceinline__ int nwarps() const { return (C > 1 ? C : 1) * (blockDim.x >> 5); }
 };
 
 // Per-CTA exchange slots for group reductions.  A group reduction first
@@ -201,7 +202,7 @@ __device__ __forceinline__ float gmin_f(const Grp<C>& g, float v, float* fred, G
 // CTA (v: the CTA's value, the same in all its threads).
 template <int C>
 __device__ __forceinline__ void gexcl_d(const Grp<C>& g, double v, double* off, double* tot, GX& x) {
-  if constexpr (C == 1) {
+  if constexpr (C <= 1) {
     *off = 0.0;
     *tot = v;
   } else {
@@ -228,7 +229,7 @@ __device__ __forceinline__ void gexcl_d(const Grp<C>& g, double v, double* off, 
 
 template <int C>
 __device__ __forceinline__ void gexcl_ll(const Grp<C>& g, long long v, long long* off, long long* tot, GX& x) {
-  if constexpr (C == 1) {
+  if constexpr (C <= 1) {
     *off = 0;
     *tot = v;
   } else {
@@ -716,8 +717,8 @@ __device__ __forceinline__ void warp_walk_d(int64_t j0, int64_t j1, double* run_
 template <int C, class V, class U>
 __device__ __forceinline__ double gscan_d(const Grp<C>& g, int64_t a, int64_t b, double carry, V val, U use,
                                           double* wbuf, GX& x) {
-  if constexpr (C == 1) {
-    if (blockDim.x == 32) {  // one warp: the walk alone
+  if constexpr (C <= 1) {
+    if (C == 0 || blockDim.x == 32) {  // one warp: the walk alone
       double run = carry;
       warp_walk_d(a, b, &run, val, use);
       __syncthreads();
@@ -808,8 +809,8 @@ __device__ __forceinline__ void warp_walk_aff(int64_t j0, int64_t j1, Aff* run_i
 template <int C, class VM, class VW, class U>
 __device__ __forceinline__ void gscan_aff(const Grp<C>& g, int64_t a, int64_t b, VM valm, VW valw, U use,
                                           double* wbuf /* 3 * HW */, GX& x, double* mt, double* qt) {
-  if constexpr (C == 1) {
-    if (blockDim.x == 32) {  // one warp: the walk alone (its final run is the pass-1 summary)
+  if constexpr (C <= 1) {
+    if (C == 0 || blockDim.x == 32) {  // one warp: the walk alone (its final run is the pass-1 summary)
       Aff run{0.0, 0.0, 0.0};
       warp_walk_aff(a, b, &run, valm, valw, use);
       __syncthreads();
