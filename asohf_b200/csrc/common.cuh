@@ -54,8 +54,14 @@ struct asohf_ctx {
   int64_t tier2_k = 2048, tier1_k = 256;
   DevParticles p;      // current store
   DevParticles alt;    // second buffer set for permutations
-  float4* rows = nullptr;  // row-packed copy of the store for permutations (2 float4 per particle)
+  // The store as rows (x, y, z, m | vx, vy, vz, id bits), 2 float4 per
+  // particle, in two buffers: rows[rows_cur] holds the current order after
+  // a permutation (-1: none since the upload), the other is the target of
+  // the next one.  Gathers of one particle read one or two 16-byte rows
+  // instead of one sector per field.
+  float4* rows[2] = {nullptr, nullptr};
   int64_t rows_cap = 0;
+  int rows_cur = -1;
   float norma = 0.f;   // MAXVAL(MASAP), refreshed on upload
   float mmin = 0.f;
   // x-slab index (SORT_DM_PARTICLES_X) and the column index built from it

@@ -179,7 +179,8 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaStreamSynchronize(c->stream);
   free_particles(c->p);
   free_particles(c->alt);
-  cudaFree(c->rows);
+  cudaFree(c->rows[0]);
+  cudaFree(c->rows[1]);
   cudaFree(c->d_s2);
   cudaFree(c->d_radx);
   free(c->h_radx);
@@ -322,6 +323,7 @@ extern "C" int asohf_upload_particles(asohf_ctx* c, const asohf_particles* s, in
   ASOHF_CUDA(cudaMemcpyAsync(c->p.m, s->m, fb, k, c->stream));
   ASOHF_CUDA(cudaMemcpyAsync(c->p.id, s->id, sizeof(int32_t) * (size_t)s->n, k, c->stream));
   c->nx_sorted = 0;  // slab table and column index are stale
+  c->rows_cur = -1;  // and so is the row copy
   if (s->n > 0) ASOHF_CHECK(ctx_refresh_mass_range(c));
   return ASOHF_OK;
 }

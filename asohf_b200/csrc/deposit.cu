@@ -180,14 +180,17 @@ __global__ void k_pack_rows(int64_t n, DevParticles s, float4* __restrict__ rows
   }
 }
 
+// New store (fields and rows) in the order perm gives: d[i] = old[perm[i]].
 __global__ void k_gather_rows(const int64_t* __restrict__ perm, int64_t n, const float4* __restrict__ rows,
-                              DevParticles d) {
+                              DevParticles d, float4* __restrict__ out_rows) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int64_t j = perm[i];
     float4 a = rows[2 * j], b = rows[2 * j + 1];
     d.x[i] = a.x; d.y[i] = a.y; d.z[i] = a.z; d.m[i] = a.w;
     d.vx[i] = b.x; d.vy[i] = b.y; d.vz[i] = b.z; d.id[i] = __float_as_int(b.w);
+    out_rows[2 * i] = a;
+    out_rows[2 * i + 1] = b;
   }
 }
 
@@ -201,19 +204,29 @@ int permute_store(asohf_ctx* c, const int64_t* perm) {
   int64_t n = c->p.n;
   if (c->rows_cap < n) {
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-    cudaFree(c->rows);
-    c->rows = nullptr;
+    cudaFree(c->rows[0]);
+    cudaFree(c->rows[1]);
+    c->rows[0] = c->rows[1] = nullptr;
     c->rows_cap = 0;
-    ASOHF_CUDA(cudaMalloc(&c->rows, 32 * (size_t)(n > 0 ? n : 1)));
+    c->rows_cur = -1;
+    ASOHF_CUDA(cudaMalloc(&c->rows[0], 32 * (size_t)(n > 0 ? n : 1)));
+    ASOHF_CUDA(cudaMalloc(&c->rows[1], 32 * (size_t)(n > 0 ? n : 1)));
     c->rows_cap = n;
   }
   {
     int kt_ = ktime_begin(c, "store_permute");
-    k_pack_rows<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(n, c->p, c->rows);
-    k_gather_rows<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(perm, n, c->rows, c->alt);
+    int src = c->rows_cur;
+    if (src < 0) {  // no row copy of the current order yet
+      src = 0;
+      k_pack_rows<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(n, c->p, c->rows[0]);
+      c->launches++;
+    }
+    k_gather_rows<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(perm, n, c->rows[src], c->alt,
+                                                                          c->rows[1 - src]);
+    c->rows_cur = 1 - src;
     ktime_end(c, kt_);
   }
-  c->launches += 2;
+  c->launches++;
   ASOHF_CUDA(cudaGetLastError());
   ctx_swap_particles(c);
   return ASOHF_OK;
@@ -508,10 +521,11 @@ static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d) {
 
 __global__ void k_bin_stage(const int32_t* __restrict__ idx, int64_t n, int64_t ndep, const float* __restrict__ x,
                             const float* __restrict__ y, const float* __restrict__ z, const float* __restrict__ m,
-                            const int64_t* __restrict__ esp_end, float4* __restrict__ P, uint8_t* __restrict__ S) {
+                            const float4* __restrict__ rows, const int64_t* __restrict__ esp_end,
+                            float4* __restrict__ P, uint8_t* __restrict__ S) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
     int p = idx[t];
-    P[t] = make_float4(x[p], y[p], z[p], m[p]);
+    P[t] = rows ? rows[2 * (int64_t)p] : make_float4(x[p], y[p], z[p], m[p]);
     int s = 0;
     while (s < ASOHF_N_ESP - 1 && (int64_t)p >= esp_end[s]) s++;
     S[t] = (int64_t)p < ndep ? (uint8_t)s : (uint8_t)255;  // 255: not deposited
@@ -1011,8 +1025,9 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       if (!bp || !bs || !ucnt || !sof) return ASOHF_ERR_CAPACITY;
       {
         int kt_ = ktime_begin(c, "density_bin_stage");
-        k_bin_stage<<<grid_for(nall, 256, c->num_sms * 16), 256, 0, c->stream>>>(B.idx, nall, n, c->p.x, c->p.y,
-                                                                               c->p.z, c->p.m, dend, bp, bs);
+        k_bin_stage<<<grid_for(nall, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+            B.idx, nall, n, c->p.x, c->p.y, c->p.z, c->p.m, c->rows_cur >= 0 ? c->rows[c->rows_cur] : nullptr,
+            dend, bp, bs);
         k_patch_unit_counts<<<(nunits + 7) / 8, 256, 0, c->stream>>>(M, B, order, nunits, dx, ucnt);
         ktime_end(c, kt_);
         c->launches += 2;

@@ -152,6 +152,7 @@ static Store store_of(asohf_ctx* c) {
   S.x = c->p.x; S.y = c->p.y; S.z = c->p.z;
   S.vx = c->p.vx; S.vy = c->p.vy; S.vz = c->p.vz;
   S.m = c->p.m; S.id = c->p.id;
+  S.rows = c->rows_cur >= 0 ? c->rows[c->rows_cur] : nullptr;
   S.norma = c->norma;
   S.eqmass_lt8 = c->norma / c->mmin < 8.0f;
   return S;
@@ -806,8 +807,14 @@ __device__ void load_segment(const Grp<C>& g, const Store& S, const unsigned lon
     for (int u = 0; u < 4; u++)
       if (jb + u * bd < hi) {
         const int q = p[u];
-        f[u][0] = S.m[q]; f[u][1] = S.vx[q]; f[u][2] = S.vy[q]; f[u][3] = S.vz[q];
-        f[u][4] = S.x[q]; f[u][5] = S.y[q]; f[u][6] = S.z[q];
+        if (S.rows) {
+          const float4 r0 = S.rows[2 * (int64_t)q], r1 = S.rows[2 * (int64_t)q + 1];
+          f[u][0] = r0.w; f[u][1] = r1.x; f[u][2] = r1.y; f[u][3] = r1.z;
+          f[u][4] = r0.x; f[u][5] = r0.y; f[u][6] = r0.z;
+        } else {
+          f[u][0] = S.m[q]; f[u][1] = S.vx[q]; f[u][2] = S.vy[q]; f[u][3] = S.vz[q];
+          f[u][4] = S.x[q]; f[u][5] = S.y[q]; f[u][6] = S.z[q];
+        }
       }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -2301,10 +2308,17 @@ __device__ void load_segment_rev(const Grp<C>& g, const Store& S, const unsigned
     while (rs > 0 && keys[rs - 1] == kj) rs--;
     while (re < K && keys[re] == kj) re++;
     const int p = vals[rs + re - 1 - j];
-    const float mp = S.m[p];
-    a.dm[j] = make_float2(__uint_as_float((uint32_t)(kj & 0xffffffffull)), mp);
-    a.mv[j] = make_float4(mp, S.vx[p], S.vy[p], S.vz[p]);
-    a.px[j] = make_float4(S.x[p], S.y[p], S.z[p], __int_as_float(p));
+    float4 r0, r1;
+    if (S.rows) {
+      r0 = S.rows[2 * (int64_t)p];
+      r1 = S.rows[2 * (int64_t)p + 1];
+    } else {
+      r0 = make_float4(S.x[p], S.y[p], S.z[p], S.m[p]);
+      r1 = make_float4(S.vx[p], S.vy[p], S.vz[p], 0.f);
+    }
+    a.dm[j] = make_float2(__uint_as_float((uint32_t)(kj & 0xffffffffull)), r0.w);
+    a.mv[j] = make_float4(r0.w, r1.x, r1.y, r1.z);
+    a.px[j] = make_float4(r0.x, r0.y, r0.z, __int_as_float(p));
     flag[j] = 1;
   }
   if (g.rank() == 0 && threadIdx.x == 0) {  // DISTA(KONTA+1) of the sorted list

@@ -257,6 +257,7 @@ __device__ __forceinline__ void gexcl_ll(const Grp<C>& g, long long v, long long
 struct Store {
   const float *x, *y, *z, *vx, *vy, *vz, *m;
   const int32_t* id;
+  const float4* rows;  // the same store as rows (x, y, z, m | vx, vy, vz, id), or null
   float norma;        // MAXVAL(MASAP)
   int eqmass_lt8;     // max/min mass < 8 over the whole store
 };

@@ -73,12 +73,17 @@ __global__ void k_colkeys(const float* __restrict__ y, const float* __restrict__
 
 __global__ void k_colfill(const int32_t* __restrict__ order, const uint32_t* __restrict__ keys, int64_t n,
                           const float* __restrict__ x, const float* __restrict__ y,
-                          const float* __restrict__ z, float4* __restrict__ cp, int64_t* __restrict__ colstart,
-                          int64_t ncols) {
+                          const float* __restrict__ z, const float4* __restrict__ rows, float4* __restrict__ cp,
+                          int64_t* __restrict__ colstart, int64_t ncols) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
        q += (int64_t)gridDim.x * blockDim.x) {
     int32_t p = order[q];
-    cp[q] = make_float4(x[p], y[p], z[p], __int_as_float(p));
+    if (rows) {
+      const float4 r = rows[2 * (int64_t)p];
+      cp[q] = make_float4(r.x, r.y, r.z, __int_as_float(p));
+    } else {
+      cp[q] = make_float4(x[p], y[p], z[p], __int_as_float(p));
+    }
     uint32_t k = keys[q];
     uint32_t kp = q > 0 ? keys[q - 1] : 0xffffffffu;
     if (q == 0) {
@@ -130,8 +135,9 @@ int build_column_index(asohf_ctx* c, int nx, float lado0) {
   ktime_end(c, kt_);
   {
     int kt_ = ktime_begin(c, "column_index_fill");
-    k_colfill<<<grid_for(n, 256), 256, 0, c->stream>>>(v1, k1, n, c->p.x, c->p.y, c->p.z, c->d_colpart,
-                                                     c->d_colstart, ncols);
+    k_colfill<<<grid_for(n, 256), 256, 0, c->stream>>>(
+        v1, k1, n, c->p.x, c->p.y, c->p.z, c->rows_cur >= 0 ? c->rows[c->rows_cur] : nullptr, c->d_colpart,
+        c->d_colstart, ncols);
     ktime_end(c, kt_);
   }
   c->launches += 2;
