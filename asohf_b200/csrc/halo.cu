@@ -153,6 +153,7 @@ static Store store_of(asohf_ctx* c) {
   S.vx = c->p.vx; S.vy = c->p.vy; S.vz = c->p.vz;
   S.m = c->p.m; S.id = c->p.id;
   S.rows = c->rows_cur >= 0 ? c->rows[c->rows_cur] : nullptr;
+  S.meq = (c->p.n > 0 && c->mmin == c->norma) ? c->norma : 0.0f;  // no gather of equal masses
   S.norma = c->norma;
   S.eqmass_lt8 = c->norma / c->mmin < 8.0f;
   return S;
@@ -436,7 +437,7 @@ k_halo_grow(const int32_t* __restrict__ slots, Store S, ColIdx ci, HConst H, aso
       float a = dist3(e.x, e.y, e.z, cx, cy, cz);
       if (a < rclus) {
         c++;
-        ms += (double)S.m[p];
+        ms += (double)S.mass(p);
         bas = fmaxf(bas, a);
       }
     });
@@ -2195,7 +2196,7 @@ k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t
   double expo = (double)(1.0f / 3.0f);
   // estimation: first J > MINJ with r/D - (m/(m+3M))^(1/3) > 0
   long long jest = LLONG_MAX;
-  tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+  tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.mass(lip[j]); },
                 [&](int64_t j, double mas) {
                   int64_t J = j + 1;
                   if (J <= minj) return;
@@ -2210,7 +2211,7 @@ k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t
   double mjj = 0.0;
   if (threadIdx.x == 0) s_m[0] = 0.0;
   __syncthreads();
-  tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+  tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.mass(lip[j]); },
                 [&](int64_t j, double mas) { if (j + 1 == jj) s_m[0] = mas; }, sh.dred);
   __syncthreads();
   mjj = s_m[0];
@@ -2224,7 +2225,7 @@ k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t
   if (eq < 0.0) {
     dir = 1;  // forward: first J > jj with EQ > 0
     long long f = LLONG_MAX;
-    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.mass(lip[j]); },
                   [&](int64_t j, double mas) {
                     int64_t J = j + 1;
                     if (J <= jj) return;
@@ -2238,7 +2239,7 @@ k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t
   } else {
     // backward: largest J in [MINJ, jj-1] with EQ(prefix(J)) < 0
     long long f = -1;
-    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.mass(lip[j]); },
                   [&](int64_t j, double mas) {
                     int64_t J = j + 1;
                     if (J < minj || J > jj - 1) return;
@@ -2265,7 +2266,7 @@ k_sub_jacobi(const int32_t* __restrict__ slots, Store S, HConst H, const int32_t
     __syncthreads();
     int64_t jm = jj2;
     if (dir == -1 && jfound == LLONG_MAX && jj - 1 < minj) jm = jj;
-    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.m[lip[j]]; },
+    tile_prefix_d(0, K, 0.0, [&](int64_t j) { return (double)S.mass(lip[j]); },
                   [&](int64_t j, double mas) { if (j + 1 == jm) s_m[1] = mas; }, sh.dred);
     __syncthreads();
     masadm = (jm >= 1 && jm <= K) ? s_m[1] : (jm > K ? mjj : 0.0);

@@ -258,6 +258,8 @@ struct Store {
   const float *x, *y, *z, *vx, *vy, *vz, *m;
   const int32_t* id;
   const float4* rows;  // the same store as rows (x, y, z, m | vx, vy, vz, id), or null
+  float meq;           // the common particle mass when all are equal, else 0
+  __device__ __forceinline__ float mass(int p) const { return meq != 0.0f ? meq : m[p]; }
   float norma;        // MAXVAL(MASAP)
   int eqmass_lt8;     // max/min mass < 8 over the whole store
 };
@@ -484,7 +486,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
       int p = ppos(e);
       if (p >= lo && p < hi && in_cube(e.x, e.y, e.z, cx, cy, cz, radio)) {
         c++;
-        float mp = S.m[p];
+        float mp = S.mass(p);
         mx = fmaxf(mx, mp);
         mn = fminf(mn, mp);
       }
@@ -516,7 +518,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
       if (!member(e, nh)) return;
       int p = ppos(e);
-      float mp = S.m[p];
+      float mp = S.mass(p);
       if (ngp) {
         int ix = (int)__fdiv_rn(__fsub_rn(e.x, xl), ddxx) + 1;
         int jy = (int)__fdiv_rn(__fsub_rn(e.y, yl), ddxx) + 1;
@@ -594,7 +596,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
       if (member(e, nh)) {
         c++;
-        float mp = S.m[ppos(e)];
+        float mp = S.mass(ppos(e));
         mx = fmaxf(mx, mp);
         mn = fminf(mn, mp);
       }
@@ -607,7 +609,7 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
     if (member(e, nh)) {
-      float mp = S.m[ppos(e)];
+      float mp = S.mass(ppos(e));
       v[0] += (double)mp;
       v[1] += (double)__fmul_rn(e.x, mp);
       v[2] += (double)__fmul_rn(e.y, mp);
