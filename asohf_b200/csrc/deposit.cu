@@ -677,6 +677,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
   __shared__ int s_lo[PROWS], s_pre[PROWS + 1], s_next;
   __shared__ double s_t27[27];
   __shared__ float s_rcp[NA + 1];  // 1/n for the clipped cloud widths n <= NA
+  __shared__ int s_any;            // some level-0 host was counted
   const int2 it = W.items[blockIdx.x];
   UnitGeo g;
   unit_geo(M, B, order, it.x, dx, g);
@@ -693,6 +694,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
       ktab[c0 + i] = kernels[(size_t)l * KW + ASOHF_NMAX_KERNELS + i];
   }
   if (threadIdx.x >= 1 && threadIdx.x <= NA) s_rcp[threadIdx.x] = 1.0f / (float)threadIdx.x;
+  if (threadIdx.x == 0) s_any = 0;
   __syncthreads();
   if (eqmass && threadIdx.x < 27) {  // level-0 terms of the common mass
     const float* kc = ktab + ktab_center(0);
@@ -773,6 +775,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
             mp = q.w;
             if (eqmass && lev == 0) {  // host cell count (ix in [0, n1+1], kz in [zlo-1, zhi+1])
               atomicAdd(&scnt[((kz - g.zlo + 1) * CGX + jy) * CGX + ix], 1);
+              s_any = 1;
             } else {
               hit = true;
             }
@@ -842,7 +845,40 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
   }
   __syncthreads();
   // level-0 hosts: 27-point stencil of the counts (cells inside the patch)
-  if (eqmass) {
+  if (eqmass && s_any && ktab[ktab_center(0) - 1] == ktab[ktab_center(0) + 1]) {
+    // a symmetric level-0 kernel leaves 8 distinct terms, t(|di|, |dj|, |dk|):
+    // a thread takes a column of cells, sums the counts of each neighbour
+    // pattern plane by plane (integers) and forms 8 products per cell
+    double tp[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) tp[q] = s_t27[((q >> 2) + 1) * 9 + (((q >> 1) & 1) + 1) * 3 + ((q & 1) + 1)];
+    for (int col = threadIdx.x; col < NA * NA; col += blockDim.x) {
+      const int i = col % NA + 1, j = col / NA + 1;
+      if (i > g.n1 || j > g.n2) continue;
+      int a0[CGZ], ax[CGZ], ay[CGZ], axy[CGZ];  // per count plane: centre, x pair, y pair, corners
+#pragma unroll
+      for (int pz = 0; pz < CGZ; pz++) {
+        const int32_t* r0 = scnt + (pz * CGX + j) * CGX + i;
+        const int32_t* rm = r0 - CGX;
+        const int32_t* rp = r0 + CGX;
+        a0[pz] = r0[0];
+        ax[pz] = r0[-1] + r0[1];
+        ay[pz] = rm[0] + rp[0];
+        axy[pz] = (rm[-1] + rm[1]) + (rp[-1] + rp[1]);
+      }
+#pragma unroll
+      for (int pz = 1; pz <= PZ; pz++) {  // output plane k = zlo + pz - 1
+        if (g.zlo + pz - 1 > g.zhi) break;
+        const int c0 = a0[pz], c1 = ax[pz], c2 = ay[pz], c3 = axy[pz];
+        const int c4 = a0[pz - 1] + a0[pz + 1], c5 = ax[pz - 1] + ax[pz + 1];
+        const int c6 = ay[pz - 1] + ay[pz + 1], c7 = axy[pz - 1] + axy[pz + 1];
+        if ((c0 | c1 | c2 | c3 | c4 | c5 | c6 | c7) == 0) continue;
+        double s = (double)c0 * tp[0] + (double)c1 * tp[1] + (double)c2 * tp[2] + (double)c3 * tp[3] +
+                   (double)c4 * tp[4] + (double)c5 * tp[5] + (double)c6 * tp[6] + (double)c7 * tp[7];
+        acc[(pz - 1) * APLANE + (j - 1) * AROW + (i - 1)] += s;
+      }
+    }
+  } else if (eqmass && s_any) {
     for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
       int i = q % NA + 1, j = (q / NA) % NA + 1, k = g.zlo + q / (NA * NA);
       if (i > g.n1 || j > g.n2 || k > g.zhi) continue;
