@@ -115,6 +115,16 @@ class Catalogue:
     def fields(self):
         return CAT_SCALAR_FLOAT + CAT_SCALAR_INT + list(CAT_MULTI)
 
+    def reset(self):
+        """Back to the initial state (zeros, nclus = 0).  Entries past nclus
+        are never written, so only the first nclus are cleared."""
+        n = self.nclus
+        if n:
+            for f in self.fields():
+                getattr(self, f)[:n] = 0
+        self.nclus = 0
+        return self
+
     def copy(self) -> "Catalogue":
         c = Catalogue.__new__(Catalogue)
         c.capacity, c.nclus = self.capacity, self.nclus

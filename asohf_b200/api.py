@@ -329,6 +329,19 @@ class GpuBackend:
     def species_sort(self, nx, dx, rodo, re0):
         return self.a.sort_dm_particles_localdensity(nx, dx, rodo, re0)
 
+    def catalogue(self, capacity):
+        """A zeroed page-locked catalogue from a ring of two owned by the
+        backend: the one returned by a run stays valid through the next run
+        (page-locking fresh memory every run would cost more than the run's
+        catalogue copies)."""
+        ring = getattr(self, "_cat_ring", None)
+        if ring is None or ring[0].capacity != capacity:
+            ring = self._cat_ring = [abi.Catalogue(capacity, pinned=True), abi.Catalogue(capacity, pinned=True)]
+            self._cat_next = 0
+        c = ring[self._cat_next]
+        self._cat_next ^= 1
+        return c.reset()
+
     def density(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree=2, fp64=True):
         u1 = np.zeros(nx ** 3, np.float32)
         u11 = np.zeros((max(mesh.total, 1), abi.NAMRX ** 3), np.float32)

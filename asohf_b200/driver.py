@@ -119,7 +119,10 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
     t0 = time.perf_counter()
     nd = backend.sort_x(nx, lado0)
     T["sort_x"] = time.perf_counter() - t0
-    cat = abi.Catalogue(plan.capacity, pinned=getattr(backend, "pinned_host", False))
+    if hasattr(backend, "catalogue"):  # backend-owned page-locked catalogues, reused
+        cat = backend.catalogue(plan.capacity)
+    else:
+        cat = abi.Catalogue(plan.capacity, pinned=getattr(backend, "pinned_host", False))
     n_id_cap = max(snap.x.shape[0], 1)
     pph = np.zeros(n_id_cap, np.int32)
     nhallev = np.zeros(mesh.nl + 1, np.int32)
