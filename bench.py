@@ -35,10 +35,10 @@ sys.path.insert(0, ROOT)
 
 CPU_SAMPLE = "cfg4s"
 BYTES_PER_ELEMENT_PASS = 32  # d, m, |v| 12, position index read + dist/index written
-# DRAM bytes (read + write) per element-pass of k_halo_main: 9.06 GB over
+# DRAM bytes (read + write) per element-pass of k_halo_main: 3.53 GB over
 # 136.4M element-passes in one ncu capture of the 256^3 workload's launches
 # (`--config cfg2 --steps 1 --warmup 0 --no-cpu --no-layer --no-e2e`)
-DRAM_BYTES_PER_ELEMENT_PASS = 66.4
+DRAM_BYTES_PER_ELEMENT_PASS = 25.9
 
 
 def peaks():
