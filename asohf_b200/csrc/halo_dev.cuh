@@ -468,8 +468,10 @@ struct RecShared {
 
 // RECENTER_DENSITY_PEAK_PARTICLES (haloes_particles.f:367-574).  The member
 // list of each shrink step is the first cube intersected with every later
-// cube, so each step re-reads the first cube from the column index instead
-// of storing the list.  Returns false if the shrink history overflows.
+// cube; instead of storing the list, each step re-reads the column index
+// over the latest cube (which holds the intersection; the radius halves
+// every step) and tests membership against all of them.  Returns false if
+// the shrink history overflows.
 template <int C>
 __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci, float* pcx, float* pcy,
                                float* pcz, float R, float dxpamin, RecShared& sh) {
@@ -511,11 +513,18 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
       if (!in_cube(e.x, e.y, e.z, sh.hist[hh][0], sh.hist[hh][1], sh.hist[hh][2], sh.hist[hh][3])) return false;
     return true;
   };
+  // the latest cube of the history (the first cube before any shrink)
+  auto qcube = [&](int upto, float* qx, float* qy, float* qz, float* qr) {
+    if (upto == 0) { *qx = c0x; *qy = c0y; *qz = c0z; *qr = r0; }
+    else { *qx = sh.hist[upto - 1][0]; *qy = sh.hist[upto - 1][1]; *qz = sh.hist[upto - 1][2]; *qr = sh.hist[upto - 1][3]; }
+  };
+  float qx, qy, qz, qr;
   for (;;) {
     for (int q = threadIdx.x; q < 64; q += blockDim.x) sh.dens[q] = 0.0;
     __syncthreads();
     bool ngp = __fdiv_rn(maxm, minm) < 8.0f;
-    gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
+    qcube(nh, &qx, &qy, &qz, &qr);
+    gquery_box(g, ci, qx, qy, qz, qr, sh.qb, [&](const float4& e) {
       if (!member(e, nh)) return;
       int p = ppos(e);
       float mp = S.mass(p);
@@ -593,7 +602,8 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     nh++;
     long long c = 0;
     float mx = -1.e30f, mn = 1.e30f;
-    gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
+    qcube(nh, &qx, &qy, &qz, &qr);
+    gquery_box(g, ci, qx, qy, qz, qr, sh.qb, [&](const float4& e) {
       if (member(e, nh)) {
         c++;
         float mp = S.mass(ppos(e));
@@ -607,7 +617,8 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
     if (cnt < 32) break;
   }
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  gquery_box(g, ci, c0x, c0y, c0z, r0, sh.qb, [&](const float4& e) {
+  qcube(nh, &qx, &qy, &qz, &qr);
+  gquery_box(g, ci, qx, qy, qz, qr, sh.qb, [&](const float4& e) {
     if (member(e, nh)) {
       float mp = S.mass(ppos(e));
       v[0] += (double)mp;
