@@ -60,7 +60,7 @@ def load():
                      "asohf_halofind_particles", "asohf_substructure_particles",
                      "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
                      "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers",
-                     "asohf_copy_to_host_sm"]:
+                     "asohf_copy_to_host_sm", "asohf_set_cluster_share"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -121,6 +121,10 @@ class Asohf:
         (0: default)."""
         _check(self.L.asohf_set_cluster_threshold(self.h, C.c_int64(int(min_members))),
                "asohf_set_cluster_threshold")
+
+    def set_cluster_share(self, members_per_cta: int):
+        """Entries per CTA from which the halo kernel widens its clusters (0: default)."""
+        _check(self.L.asohf_set_cluster_share(self.h, C.c_int64(int(members_per_cta))), "asohf_set_cluster_share")
 
     def set_group_tiers(self, tier1: int, tier2: int):
         """Member counts from which a halo gets 128 / 256 threads (0: default)."""
@@ -309,11 +313,13 @@ class GpuBackend:
 
     pinned_host = True  # host catalogue in page-locked memory
 
-    def __init__(self, device: int = 0, cluster_threshold: int = 0, tiers=(0, 0)):
+    def __init__(self, device: int = 0, cluster_threshold: int = 0, tiers=(0, 0), cluster_share: int = 0):
         self.a = Asohf(device)
         self._ids = None
         if cluster_threshold:
             self.a.set_cluster_threshold(cluster_threshold)
+        if cluster_share:
+            self.a.set_cluster_share(cluster_share)
         if tiers != (0, 0):
             self.a.set_group_tiers(*tiers)
 

@@ -51,6 +51,7 @@ struct asohf_ctx {
   // size tiers of the per-halo launches (members): >= cluster_min a CTA
   // cluster, >= tier2_k 256 threads, >= tier1_k 128 threads, else 32
   int64_t cluster_min = 32768;
+  int64_t cluster_share = 32768;  // entries per CTA that set the halo kernel's cluster width
   int64_t tier2_k = 2048, tier1_k = 256;
   DevParticles p;      // current store
   DevParticles alt;    // second buffer set for permutations

@@ -326,14 +326,14 @@ static int split_tiers(asohf_ctx* c, const int32_t* hcount, int n, int32_t* dbuf
 
 // Reorders the cluster tier's slot list (tier 3, at the front of its
 // device buffer) into runs for clusters of cb (at most 16), 8 and 4 CTAs by
-// member count: a CTA's share stays near CLUSTER_SHARE entries.
-#define CLUSTER_SHARE 32768
+// member count: a CTA's share stays near ctx->cluster_share entries.
 static int split_cluster_tier(asohf_ctx* c, const int32_t* hcount, int n, int cb, Tiers* T, int nsub[3],
                               int32_t* sub[3]) {
+  const int64_t sh = c->cluster_share;
   auto pick = [&](int32_t k) {
-    if (cb < 8) return 0;                                 // no clusters: one CTA each
-    if (cb < 16) return k > 4 * CLUSTER_SHARE ? 0 : 2;  // 8 CTAs at most
-    return k > 8 * CLUSTER_SHARE ? 0 : (k > 4 * CLUSTER_SHARE ? 1 : 2);
+    if (cb < 8) return 0;                      // no clusters: one CTA each
+    if (cb < 16) return k > 4 * sh ? 0 : 2;  // 8 CTAs at most
+    return k > 8 * sh ? 0 : (k > 4 * sh ? 1 : 2);
   };
   int32_t* h = (int32_t*)malloc(4 * (size_t)(T->n[3] > 0 ? T->n[3] : 1));
   int cnt[3] = {0, 0, 0};
@@ -1823,6 +1823,12 @@ static int big_cluster(asohf_ctx* c) {
 extern "C" int asohf_set_cluster_threshold(asohf_ctx* c, int64_t min_members) {
   if (!c || min_members < 0) return ASOHF_ERR_INVALID;
   c->cluster_min = min_members == 0 ? BIG_K : min_members;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_set_cluster_share(asohf_ctx* c, int64_t members_per_cta) {
+  if (!c || members_per_cta < 0) return ASOHF_ERR_INVALID;
+  c->cluster_share = members_per_cta == 0 ? 32768 : members_per_cta;
   return ASOHF_OK;
 }
 

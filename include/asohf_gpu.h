@@ -63,6 +63,11 @@ int asohf_copy_to_host_sm(asohf_ctx *ctx, void *host_dst, const void *dev_src, i
  * one CTA each (results are the same either way).  0 restores the default
  * (32768); 1 sends every halo to the cluster path. */
 int asohf_set_cluster_threshold(asohf_ctx *ctx, int64_t min_members);
+/* Tuning, no counterpart in the reference: the halo kernel gives a
+ * cluster-tier halo 16 CTAs above 8 x members_per_cta members, 8 above
+ * 4 x, else 4 (results are the same for every width).  0 restores the
+ * default (32768). */
+int asohf_set_cluster_share(asohf_ctx *ctx, int64_t members_per_cta);
 /* Tuning, no counterpart in the reference: haloes below the cluster
  * threshold are refined by one CTA of 256 threads from tier2_members
  * members, of 128 threads from tier1_members, else of 32 threads; a halo

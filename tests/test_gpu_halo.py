@@ -15,17 +15,20 @@ from tests.catalogue_compare import compare
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,cluster_min,tiers", [("tiny", 0, (0, 0)), ("small", 0, (0, 0)),
-                                                    ("tiny", 1, (0, 0)), ("small", 1, (0, 0)),
-                                                    ("small", 300, (0, 0)), ("tiny", 0, (16, 64)),
-                                                    ("small", 2000, (16, 64))])
-def test_halofind_matches_oracle(gpu_lib, name, cluster_min, tiers):
+@pytest.mark.parametrize("name,cluster_min,tiers,share", [("tiny", 0, (0, 0), 0), ("small", 0, (0, 0), 0),
+                                                          ("tiny", 1, (0, 0), 0), ("small", 1, (0, 0), 0),
+                                                          ("small", 300, (0, 0), 0), ("tiny", 0, (16, 64), 0),
+                                                          ("small", 2000, (16, 64), 0), ("tiny", 1, (0, 0), 1),
+                                                          ("small", 1, (0, 0), 64), ("small", 300, (0, 0), 100)])
+def test_halofind_matches_oracle(gpu_lib, name, cluster_min, tiers, share):
     """cluster_min 1 sends every halo through the thread-block-cluster
     kernels, 300 splits the haloes between clusters and single CTAs; the
     small tier bounds (16, 64) put haloes in all four launch shapes and make
-    growing haloes move to larger groups mid-growth."""
+    growing haloes move to larger groups mid-growth; a small per-CTA share
+    gives cluster haloes the 16- and 8-CTA widths of the halo kernel."""
     s = synth.generate(name)
-    rg = driver.run(s, api.GpuBackend(cluster_threshold=cluster_min, tiers=tiers), with_subs=False)
+    rg = driver.run(s, api.GpuBackend(cluster_threshold=cluster_min, tiers=tiers, cluster_share=share),
+                    with_subs=False)
     ro = driver.run(s, O.OracleBackend(), with_subs=False)
     assert (ro.cat.realclus[: ro.cat.nclus] != 0).sum() > 0
     compare(rg, ro)
