@@ -181,16 +181,35 @@ __global__ void k_pack_rows(int64_t n, DevParticles s, float4* __restrict__ rows
 }
 
 // New store (fields and rows) in the order perm gives: d[i] = old[perm[i]].
+// Four particles per thread and step: their rows are all requested before
+// any is written.
 __global__ void k_gather_rows(const int64_t* __restrict__ perm, int64_t n, const float4* __restrict__ rows,
                               DevParticles d, float4* __restrict__ out_rows) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t j = perm[i];
-    float4 a = rows[2 * j], b = rows[2 * j + 1];
-    d.x[i] = a.x; d.y[i] = a.y; d.z[i] = a.z; d.m[i] = a.w;
-    d.vx[i] = b.x; d.vy[i] = b.y; d.vz[i] = b.z; d.id[i] = __float_as_int(b.w);
-    out_rows[2 * i] = a;
-    out_rows[2 * i + 1] = b;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+    int64_t j[4];
+    float4 a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int64_t i = i0 + u * stride;
+      j[u] = i < n ? perm[i] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (i0 + u * stride < n) {
+        a[u] = rows[2 * j[u]];
+        b[u] = rows[2 * j[u] + 1];
+      }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int64_t i = i0 + u * stride;
+      if (i < n) {
+        d.x[i] = a[u].x; d.y[i] = a[u].y; d.z[i] = a[u].z; d.m[i] = a[u].w;
+        d.vx[i] = b[u].x; d.vy[i] = b[u].y; d.vz[i] = b[u].z; d.id[i] = __float_as_int(b[u].w);
+        out_rows[2 * i] = a[u];
+        out_rows[2 * i + 1] = b[u];
+      }
+    }
   }
 }
 
@@ -552,6 +571,42 @@ __global__ void k_base_counts(const float* __restrict__ x, const float* __restri
 struct Terms27 {
   double t[27];  // t[(kk+1)*9 + (jj+1)*3 + (ii+1)] = ((m*W(ii))*W(jj))*W(kk) in REAL*4
 };
+
+// Symmetric level-0 kernel (W(-1) = W(1)): the 27 terms take 8 values
+// t(|di|, |dj|, |dk|), so a cell needs the count sums of 8 neighbour
+// patterns (integers) and 8 products.
+__global__ void k_base_stencil_sym(const int32_t* __restrict__ cnt, int nx, Terms27 T, double* __restrict__ acc) {
+  int64_t g = (int64_t)nx * nx * nx;
+  double tp[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) tp[q] = T.t[((q >> 2) + 1) * 9 + (((q >> 1) & 1) + 1) * 3 + ((q & 1) + 1)];
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(c % nx) + 1, j = (int)((c / nx) % nx) + 1, k = (int)(c / ((int64_t)nx * nx)) + 1;
+    const int im = wrap_once(i - 1, nx) - 1, ip = wrap_once(i + 1, nx) - 1;
+    const int jm = wrap_once(j - 1, nx) - 1, jp = wrap_once(j + 1, nx) - 1;
+    int a0[3], ax[3], ay[3], axy[3];
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      const int hk = wrap_once(k + kk, nx) - 1;
+      const int32_t* pl = cnt + (int64_t)hk * nx * nx;
+      const int32_t* r0 = pl + (int64_t)(j - 1) * nx;
+      const int32_t* rm = pl + (int64_t)jm * nx;
+      const int32_t* rp = pl + (int64_t)jp * nx;
+      a0[kk + 1] = r0[i - 1];
+      ax[kk + 1] = r0[im] + r0[ip];
+      ay[kk + 1] = rm[i - 1] + rp[i - 1];
+      axy[kk + 1] = (rm[im] + rm[ip]) + (rp[im] + rp[ip]);
+    }
+    const int c0 = a0[1], c1 = ax[1], c2 = ay[1], c3 = axy[1];
+    const int c4 = a0[0] + a0[2], c5 = ax[0] + ax[2], c6 = ay[0] + ay[2], c7 = axy[0] + axy[2];
+    double s = 0.0;
+    if ((c0 | c1 | c2 | c3 | c4 | c5 | c6 | c7) != 0)
+      s = (double)c0 * tp[0] + (double)c1 * tp[1] + (double)c2 * tp[2] + (double)c3 * tp[3] +
+          (double)c4 * tp[4] + (double)c5 * tp[5] + (double)c6 * tp[6] + (double)c7 * tp[7];
+    acc[c] = s;
+  }
+}
 
 __global__ void k_base_stencil(const int32_t* __restrict__ cnt, int nx, Terms27 T, double* __restrict__ acc) {
   int64_t g = (int64_t)nx * nx * nx;
@@ -997,6 +1052,12 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         t = t * h0[kk];
         T27.t[(kk + 1) * 9 + (jj + 1) * 3 + (ii + 1)] = (double)t;
       }
+  bool sym27 = true;  // each term equals the one of its mirrored offsets
+  for (int q = 0; q < 27; q++) {
+    const int ii = q % 3 - 1, jj = (q / 3) % 3 - 1, kk = q / 9 - 1;
+    const int m = (abs(kk) + 1) * 9 + (abs(jj) + 1) * 3 + (abs(ii) + 1);
+    if (T27.t[q] != T27.t[m]) sym27 = false;
+  }
   free(hk);
   float* du1;
   ASOHF_CHECK(stage_out(c, u1, 4 * g, on_device, &du1));
@@ -1017,7 +1078,10 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
     int kt_ = ktime_begin(c, "density_base");
     k_base_counts<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, nx, xl,
                                                                           dx, cnt);
-    k_base_stencil<<<grid_for(g, 256, c->num_sms * 16), 256, 0, c->stream>>>(cnt, nx, T27, acc);
+    if (sym27)  // 8 distinct terms
+      k_base_stencil_sym<<<grid_for(g, 256, c->num_sms * 16), 256, 0, c->stream>>>(cnt, nx, T27, acc);
+    else
+      k_base_stencil<<<grid_for(g, 256, c->num_sms * 16), 256, 0, c->stream>>>(cnt, nx, T27, acc);
     k_density_base_outliers<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
       c->p.x, c->p.y, c->p.z, c->p.m, n, nx, xl, dx, k0, acc);
     ktime_end(c, kt_);

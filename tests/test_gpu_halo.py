@@ -43,3 +43,16 @@ def test_substructure_matches_oracle(gpu_lib, name):
     sub = ro.cat.realclus[ro.subs_lev[0]: ro.cat.nclus]
     assert (sub > 0).sum() > 0
     compare(rg, ro)
+
+
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_pipeline_unequal_masses_matches_oracle(gpu_lib, name):
+    """Unequal particle masses: no common mass to use, so the growth,
+    recentering and subhalo kernels read each member's mass."""
+    s = synth.generate(name)
+    rng = np.random.default_rng(7)
+    s.m = (s.m * (1.0 + 0.5 * rng.random(s.m.shape[0]))).astype(np.float32)
+    rg = driver.run(s, api.GpuBackend(), with_subs=True)
+    ro = driver.run(s, O.OracleBackend(), with_subs=True)
+    assert (ro.cat.realclus[: ro.cat.nclus] != 0).sum() > 0
+    compare(rg, ro)
