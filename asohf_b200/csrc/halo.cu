@@ -165,6 +165,8 @@ static HConst hconst(const asohf_consts* k, const asohf_mesh* mesh) {
   h.contrastec = k->contrastec; h.omegaz = k->omegaz; h.fdm = k->fdm; h.zeta = k->zeta;
   h.min_num_part = k->min_num_part;
   h.want_ids = (k->flag_wdm == 1 || k->var > 1);
+  h.energies = k->do_compute_energies == 1;
+  h.max_part_dsum = k->max_part_dsum;
   h.nl = mesh ? mesh->nl : 0;
   int acc = mesh ? mesh->npatch[0] : 0;
   for (int ir = 0; ir <= ASOHF_NLEVELS + 1; ir++) { h.lev_lo[ir] = 0; h.lev_hi[ir] = -1; }
@@ -1178,10 +1180,72 @@ __device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac
 
 // Bound-particle properties (haloes_particles.f:1187-1353) over j < konta of
 // the staged list; flag[j] receives the ID mask.  Returns KONTA2.
+// COMPUTE_EPOT (haloes_particles.f:1494-1628), direct summation over the
+// konta entries whose flag is set: every pair's REAL*4 -m1*m2/r in float64.
+// A thread sums the row of each of its entries against all entries (tiles
+// of the list in shared memory; both members of a pair compute the same
+// term, so the total is half the rows' sum), and the most bound entry is
+// the first minimum of row / m (100000 for entries not in).  Returns the
+// total through *epot8 and the entry through *jbest.
+template <int C>
+__device__ void epot_direct_g(const Grp<C>& g, const SegView& v, const uint8_t* flag, int64_t konta,
+                              double* epot8, long long* jbest, GShared& sh) {
+  __shared__ float4 tile[HB];
+  int64_t lo, hi;
+  g.chunk(0, konta, &lo, &hi);
+  double rows = 0.0, best_v = -INFINITY, best_b = 0.0;  // best_v: -(row / m), the largest wins
+  long long best_j = LLONG_MAX;
+#pragma unroll 1
+  for (int64_t j0 = lo; j0 < hi; j0 += blockDim.x) {  // the same trip count in every thread of the CTA
+    const int64_t j = j0 + threadIdx.x;
+    const bool act = j < hi && flag[j];
+    float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (act) {
+      const float4 p = v.px[j];
+      pj = make_float4(p.x, p.y, p.z, v.mv[j].x);
+    }
+    double e = 0.0;
+#pragma unroll 1
+    for (int64_t q0 = 0; q0 < konta; q0 += HB) {
+      __syncthreads();
+      for (int t = threadIdx.x; t < HB; t += blockDim.x) {
+        const int64_t q = q0 + t;
+        float4 w = make_float4(0.f, 0.f, 0.f, -1.f);  // m < 0: not in
+        if (q < konta && flag[q]) {
+          const float4 p = v.px[q];
+          w = make_float4(p.x, p.y, p.z, v.mv[q].x);
+        }
+        tile[t] = w;
+      }
+      __syncthreads();
+      if (act) {
+        const int nt = konta - q0 < HB ? (int)(konta - q0) : HB;
+        for (int t = 0; t < nt; t++) {
+          const float4 w = tile[t];
+          if (w.w < 0.f || q0 + t == j) continue;
+          const float ax = __fsub_rn(pj.x, w.x), ay = __fsub_rn(pj.y, w.y), az = __fsub_rn(pj.z, w.z);
+          const float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az)));
+          e += (double)__fdiv_rn(-__fmul_rn(pj.w, w.w), r);
+        }
+      }
+    }
+    if (j < hi) {
+      const double ev = act ? e / (double)pj.w : 100000.0;
+      if (act) rows += e;
+      if (best_before(-ev, j, best_v, best_j)) { best_v = -ev; best_j = j; }
+    }
+  }
+  double t = rows;
+  gsum_dv<1>(g, &t, sh.x);
+  gbest(g, &best_v, &best_j, &best_b, sh);
+  *epot8 = 0.5 * t;
+  *jbest = best_j;
+}
+
 template <int C, bool SYM = true>
 __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
                                   const SegView& v, uint8_t* flag, int64_t konta, float rshell, float cx, float cy,
-                                  float cz, const float* cmv, GShared& sh) {
+                                  float cz, const float* cmv, GShared& sh, int* unsupported) {
   float norma = S.norma;
   float vc[3] = {cat.vx[i0], cat.vy[i0], cat.vz[i0]};
   int64_t each_prof = konta / ASOHF_NBINS;
@@ -1244,14 +1308,38 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
   const double* r2 = r + 10;
   vmax = gmax_f(g, vmax, sh.fred, sh.x);
   long long cnt = (long long)r2[2];
+  // energies (haloes_particles.f:1297-1316): kinetic sum of the bound
+  // entries, potential by direct summation below MAX_PART_DSUM entries (the
+  // reference samples above it with an unseeded generator: not reproduced,
+  // reported as unsupported)
+  double ekin = acc[1], epot8 = 0.0;
+  long long jmb = 0;
+  *unsupported = 0;
+  if (H.energies && cnt >= H.min_num_part) {
+    if (cnt >= H.max_part_dsum) {
+      *unsupported = 1;
+    } else {
+      gsum_dv<1>(g, &ekin, sh.x);
+      epot_direct_g(g, v, flag, konta, &epot8, &jmb, sh);
+    }
+  }
   if (g.rank() == 0 && threadIdx.x == 0) {
     cat.dmpclus[i0] = (int32_t)cnt;
     if (cnt < H.min_num_part) {
       cat.realclus[i0] = 0;
       cat.vmaxclus[i0] = vmax;  // the running maximum of |v|^2 (-1 if none) stays
+    } else if (H.energies) {
+      const double gcons = (double)4.301e-9f;
+      float epot = (float)epot8;
+      epot = (float)((double)epot * (double)__fmul_rn(H.um, H.um) * gcons);
+      cat.kinetic_e[i0] = (float)(0.5 * ekin * (double)H.um * (double)__fmul_rn(H.uv, H.uv));
+      cat.potential_e[i0] = __fmul_rn(epot, __fadd_rn(1.0f, H.zeta));
+      cat.iplip[i0] = S.id[__float_as_int(v.px[jmb].w)];
     } else {
       cat.potential_e[i0] = 0.0f;
       cat.iplip[i0] = S.id[__float_as_int(v.px[0].w)];
+    }
+    if (cnt >= H.min_num_part) {
       double basmas = r2[1];
       double den = basmas * (double)norma;
       cat.angularm[i0 * 3 + 0] = (float)(r[1] * (double)H.uv / den);
@@ -1562,7 +1650,8 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     if (lead) cat.realclus[i0] = 0;
     return;
   }
-  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh);
+  int unsup = 0;
+  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup);
   ep += (unsigned long long)(k2 + ncapas);  // SO walk and property loop
   if (lead) {
     atomicAdd(&sg.work[0], ep);
@@ -1577,7 +1666,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
-    sg.status[slot] = 0;
+    sg.status[slot] = unsup ? ASOHF_ERR_UNSUPPORTED : 0;
   }
 }
 
@@ -1847,7 +1936,6 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   if (!c || !k || !cat || lowh1 < 1 || lowh2 > cat->nclus) return ASOHF_ERR_INVALID;
   if (lowh2 < lowh1) return ASOHF_OK;
   if (c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
-  if (k->do_compute_energies == 1) return ASOHF_ERR_UNSUPPORTED;
   ASOHF_CUDA(cudaSetDevice(c->device));
   double ht = htime_now();
   arena_reset(c);
@@ -2574,14 +2662,15 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
   // (the properties read VX(I) from it, as the Fortran does)
   write_back();
   g.sync();
-  long long nb = properties_g<C, false>(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh);
+  int unsup = 0;
+  long long nb = properties_g<C, false>(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup);
   ep += (unsigned long long)(k2 + ncapas);
   if (lead) {
     atomicAdd(&sg.work[1], ep);
     const bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
-    sg.status[slot] = 0;
+    sg.status[slot] = unsup ? ASOHF_ERR_UNSUPPORTED : 0;
   }
 }
 
@@ -2702,7 +2791,6 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
                                             int on_device) {
   if (!c || !k || !cat || !subs_lev || !mesh || ir < 1 || ir > mesh->nl) return ASOHF_ERR_INVALID;
   if (c->nx_sorted != k->nx) return ASOHF_ERR_INVALID;
-  if (k->do_compute_energies == 1) return ASOHF_ERR_UNSUPPORTED;
   int lowh1 = 1, lowh2 = 0;
   for (int q = 0; q < ir; q++) lowh1 += subs_lev[q];
   for (int q = 0; q <= ir; q++) lowh2 += subs_lev[q];

@@ -56,3 +56,40 @@ def test_pipeline_unequal_masses_matches_oracle(gpu_lib, name):
     ro = driver.run(s, O.OracleBackend(), with_subs=True)
     assert (ro.cat.realclus[: ro.cat.nclus] != 0).sum() > 0
     compare(rg, ro)
+
+
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_energies_match_oracle(gpu_lib, name):
+    """DO_COMPUTE_ENERGIES=1 with every halo below MAX_PART_DSUM: the direct
+    pair sum (COMPUTE_EPOT), the kinetic energy and the most bound particle
+    as IPLIP, haloes and subhaloes."""
+    s = synth.generate(name)
+    plans = []
+    for _ in range(2):
+        p = driver.prepare(s)
+        p.consts.do_compute_energies = 1
+        p.consts.max_part_dsum = 1 << 30
+        plans.append(p)
+    rg = driver.execute(plans[0], api.GpuBackend(), with_subs=True)
+    ro = driver.execute(plans[1], O.OracleBackend(), with_subs=True)
+    live = ro.cat.realclus[: ro.cat.nclus] != 0
+    assert live.sum() > 0
+    compare(rg, ro)
+    n = ro.cat.nclus
+    for f in ("kinetic_e", "potential_e"):
+        a = getattr(rg.cat, f)[:n].astype(np.float64)
+        b = getattr(ro.cat, f)[:n].astype(np.float64)
+        assert np.all(np.abs(a - b) <= 1e-5 * np.maximum(np.abs(b), 1e-30)), f
+    assert np.all(ro.cat.potential_e[:n][live] < 0)
+
+
+def test_energies_above_dsum_limit_are_unsupported(gpu_lib):
+    """Above MAX_PART_DSUM the reference samples pairs with an unseeded
+    generator; the library reports that case as unsupported, like the
+    oracle."""
+    s = synth.generate("tiny")
+    p = driver.prepare(s)
+    p.consts.do_compute_energies = 1
+    p.consts.max_part_dsum = 10
+    with pytest.raises(RuntimeError):
+        driver.execute(p, api.GpuBackend(), with_subs=False)
