@@ -60,7 +60,8 @@ def load():
                      "asohf_halofind_particles", "asohf_substructure_particles",
                      "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
                      "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers",
-                     "asohf_copy_to_host_sm", "asohf_set_cluster_share"]:
+                     "asohf_copy_to_host_sm", "asohf_set_cluster_share",
+                     "asohf_check_rubish", "asohf_accidental_substructure"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -275,6 +276,22 @@ class Asohf:
                                               C.c_int(do_need_to_count), C.c_int(0)),
                "PRUNE_POOR_HALOES")
 
+    def check_rubish(self, cat, low1, low2):
+        """CHECK_RUBISH over the window low1..low2; returns KONTA."""
+        cc = cat.as_c()
+        n = C.c_int32()
+        _check(self.L.asohf_check_rubish(self.h, C.byref(cc), C.c_int(cat.nclus), C.c_int(low1), C.c_int(low2),
+                                         C.c_int(0), C.byref(n)), "CHECK_RUBISH")
+        return n.value
+
+    def accidental_substructure(self, cat):
+        """ACCIDENTAL_SUBSTRUCTURE over the catalogue; returns KONTA."""
+        cc = cat.as_c()
+        n = C.c_int32()
+        _check(self.L.asohf_accidental_substructure(self.h, C.byref(cc), C.c_int(cat.nclus), C.c_int(0),
+                                                    C.byref(n)), "ACCIDENTAL_SUBSTRUCTURE")
+        return n.value
+
     def halofind_particles(self, consts, mesh, cat, low1, low2):
         mh = abi.MeshHolder(mesh)
         cc = cat.as_c()
@@ -428,6 +445,12 @@ class GpuBackend:
 
     def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
         self.a.halofind_particles(consts, mesh, cat, low1, low2)
+
+    def check_rubish(self, cat, low1, low2):
+        return self.a.check_rubish(cat, low1, low2)
+
+    def accidental_substructure(self, cat):
+        return self.a.accidental_substructure(cat)
 
     def substructure_particles(self, consts, mesh, cat, ir, subs_lev, pph):
         self.a.substructure_particles(consts, mesh, cat, ir, subs_lev)

@@ -1,0 +1,397 @@
+// clean.cu -- catalogue cleaning after each level's particle refinement:
+// CHECK_RUBISH (haloes_particles.f:259-318) and ACCIDENTAL_SUBSTRUCTURE
+// (haloes_particles.f:321-364), both called from asohf.f:672-675.
+//
+// Both remove (REALCLUS = 0) a halo because of a halo of a LOWER level, and
+// the driver appends each level's haloes after the previous levels', so in
+// a catalogue whose levels never decrease with the index the Fortran's
+// sequential loops reduce to: a halo of level l is removed iff some halo of
+// a level below l that is still alive once its own level is settled meets
+// the test.  The device settles one level at a time, one thread per halo of
+// that level against all lower haloes (tiles in shared memory).  A catalogue
+// out of level order is refused (ASOHF_ERR_INVALID).
+//
+// CHECK_RUBISH's speed ratio A2 is assigned only when both speeds are
+// nonzero; otherwise the Fortran reuses the value of the pair before, an
+// order-dependent quantity.  Such a pair can only add a removal, so the
+// result is known unless a halo no regular pair removes has a zero-speed
+// pair passing the distance and mass tests: that case is reported as
+// ASOHF_ERR_UNSUPPORTED instead of guessed.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "common.cuh"
+
+namespace {
+
+struct CleanCat {
+  const float *x, *y, *z, *vx, *vy, *vz, *m, *r;
+  const int32_t* lev;
+  int32_t* rc;
+};
+
+#define CT 256  // threads per CTA and lower haloes per shared-memory tile
+
+__device__ __forceinline__ float dist_f(float x1, float y1, float z1, float x2, float y2, float z2) {
+  const float dx = __fsub_rn(x1, x2), dy = __fsub_rn(y1, y2), dz = __fsub_rn(z1, z2);
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+}
+
+__device__ __forceinline__ float speed_f(float vx, float vy, float vz) {
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+}
+
+// Every entry sorted by x (sidx: entries in x order, sx: their x).  A CTA
+// takes 256 consecutive sorted entries; those of the level run [j0, j1)
+// are its haloes, and only the lower haloes whose x lies within reach of
+// theirs (a binary search of sx) are tested: a removal needs DIS below
+// 1.01 R(J) (CHECK_RUBISH) or below R(I) (ACCIDENTAL_SUBSTRUCTURE), hence
+// |dx| below the reach, padded for rounding.
+// First sorted position whose x is not below v (UPPER: not at or below v);
+// NaN x sort last and count as neither.
+template <bool UPPER>
+__device__ __forceinline__ int search_x(const float* sx, int n, float v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (UPPER ? sx[mid] <= v : sx[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// The sorted positions [*q0, *q1) whose x lies within w of the x of some
+// active halo of the CTA.  DIS never falls below |dx| once the squares are
+// normal numbers, so w is kept at least 1e-18; a NaN bound widens to the
+// whole axis.  Called by every thread of the CTA.
+__device__ __forceinline__ void cta_window(const float* sx, int n, bool act, float xj, float w, int* q0, int* q1) {
+  __shared__ float s_red[2][CT / 32];
+  __shared__ int s_q[2];
+  float lo = INFINITY, hi = -INFINITY;
+  if (act) {
+    w = w == w ? fmaxf(w, 1e-18f) : INFINITY;
+    lo = __fsub_rn(xj, w);
+    hi = __fadd_rn(xj, w);
+    if (lo != lo) lo = -INFINITY;
+    if (hi != hi) hi = INFINITY;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) { s_red[0][threadIdx.x >> 5] = lo; s_red[1][threadIdx.x >> 5] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float l = INFINITY, h = -INFINITY;
+    for (int k = 0; k < CT / 32; k++) { l = fminf(l, s_red[0][k]); h = fmaxf(h, s_red[1][k]); }
+    s_q[0] = l > h ? 0 : search_x<false>(sx, n, l);
+    s_q[1] = l > h ? 0 : h == INFINITY ? n : search_x<true>(sx, n, h);
+  }
+  __syncthreads();
+  *q0 = s_q[0];
+  *q1 = s_q[1];
+}
+
+// Haloes j0..j1-1 (one level, the window's) against the lower haloes
+// 0..i1-1: DIS < 1.01 MIN(R), MIN(M)/MAX(M) > 0.2, |V1-V2|/MAX(V) < 3.
+__global__ void __launch_bounds__(CT) k_check_rubish(CleanCat c, const int32_t* __restrict__ sidx,
+                                                     const float* __restrict__ sx, int n, int j0, int j1, int i1,
+                                                     int* zero_speed, int* removed) {
+  __shared__ float4 tp[CT];   // x, y, z, m
+  __shared__ float2 tr[CT];   // radius, speed (< 0: not a candidate)
+  __shared__ int tl[CT];
+  const int ps = blockIdx.x * CT + threadIdx.x;
+  const int j = ps < n ? sidx[ps] : -1;
+  const bool act = j >= j0 && j < j1 && c.rc[j] != 0;
+  float xj = 0.f, yj = 0.f, zj = 0.f, mj = 0.f, rj = 0.f, vj = 0.f;
+  int lj = 0;
+  if (act) {
+    xj = c.x[j]; yj = c.y[j]; zj = c.z[j]; mj = c.m[j]; rj = c.r[j]; lj = c.lev[j];
+    vj = speed_f(c.vx[j], c.vy[j], c.vz[j]);
+  }
+  int q0, q1;  // DIS < 1.01 MIN(R) <= 1.01 R(J)
+  cta_window(sx, n, act, xj, __fmul_rn(1.02f, rj), &q0, &q1);
+  bool kill = false, zero = false;
+  for (int t0 = q0; t0 < q1; t0 += CT) {
+    __syncthreads();
+    const int q = t0 + threadIdx.x;
+    if (q < q1) {
+      const int i = sidx[q];
+      const bool cand = i < i1 && c.rc[i] != 0;
+      tp[threadIdx.x] = make_float4(c.x[i], c.y[i], c.z[i], c.m[i]);
+      tr[threadIdx.x] = make_float2(c.r[i], cand ? speed_f(c.vx[i], c.vy[i], c.vz[i]) : -1.f);
+      tl[threadIdx.x] = c.lev[i];
+    }
+    __syncthreads();
+    if (!act || kill) continue;
+    const int nt = q1 - t0 < CT ? q1 - t0 : CT;
+    for (int t = 0; t < nt; t++) {
+      const float2 rv = tr[t];
+      if (rv.y < 0.f || !(lj > tl[t])) continue;
+      const float4 p = tp[t];
+      const float dis = dist_f(p.x, p.y, p.z, xj, yj, zj);
+      const float a1 = __fdiv_rn(fminf(p.w, mj), fmaxf(p.w, mj));
+      const float a3 = fminf(rv.x, rj);
+      if (!(dis < __fmul_rn(1.01f, a3) && a1 > 0.2f)) continue;
+      if (fminf(rv.y, vj) == 0.0f) { zero = true; continue; }  // A2 not assigned for this pair
+      const float a2 = __fdiv_rn(fabsf(__fsub_rn(rv.y, vj)), fmaxf(rv.y, vj));
+      if (a2 < 3.0f) { kill = true; break; }
+    }
+  }
+  if (act && zero && !kill) atomicOr(zero_speed, 1);
+  if (act && kill) {
+    c.rc[j] = 0;
+    atomicAdd(removed, 1);
+  }
+}
+
+// Confirmed haloes j0..j1-1 (one level) inside a confirmed lower halo of
+// 0..i1-1: DIS + R(J) <= 1.0 R(I); rmax bounds R(I).
+__global__ void __launch_bounds__(CT) k_accidental(CleanCat c, const int32_t* __restrict__ sidx,
+                                                   const float* __restrict__ sx, int n, int j0, int j1, int i1,
+                                                   const float* __restrict__ rmax, int* removed) {
+  __shared__ float4 tp[CT];  // x, y, z, radius (NaN: not a confirmed lower halo, fails every test)
+  __shared__ int tl[CT];
+  const int ps = blockIdx.x * CT + threadIdx.x;
+  const int j = ps < n ? sidx[ps] : -1;
+  const bool act = j >= j0 && j < j1 && c.rc[j] == -1;
+  float xj = 0.f, yj = 0.f, zj = 0.f, rj = 0.f;
+  int lj = 0;
+  if (act) { xj = c.x[j]; yj = c.y[j]; zj = c.z[j]; rj = c.r[j]; lj = c.lev[j]; }
+  int q0, q1;  // DIS <= R(I) - R(J) <= rmax + MAX(-R(J), 0)
+  cta_window(sx, n, act, xj, __fmul_rn(1.02f, __fadd_rn(*rmax, fmaxf(-rj, 0.f))), &q0, &q1);
+  bool kill = false;
+  for (int t0 = q0; t0 < q1; t0 += CT) {
+    __syncthreads();
+    const int q = t0 + threadIdx.x;
+    if (q < q1) {
+      const int i = sidx[q];
+      tp[threadIdx.x] = make_float4(c.x[i], c.y[i], c.z[i], i < i1 && c.rc[i] == -1 ? c.r[i] : __int_as_float(0x7fffffff));
+      tl[threadIdx.x] = c.lev[i];
+    }
+    __syncthreads();
+    if (!act || kill) continue;
+    const int nt = q1 - t0 < CT ? q1 - t0 : CT;
+    for (int t = 0; t < nt; t++) {
+      const float4 p = tp[t];
+      if (!(lj > tl[t])) continue;
+      const float dis = dist_f(p.x, p.y, p.z, xj, yj, zj);
+      if (__fadd_rn(dis, rj) <= __fmul_rn(1.0f, p.w)) { kill = true; break; }
+    }
+  }
+  if (act && kill) {
+    c.rc[j] = 0;
+    atomicAdd(removed, 1);
+  }
+}
+
+__global__ void k_x_keys(const float* __restrict__ x, int n, uint32_t* __restrict__ key, int32_t* __restrict__ val) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t u = __float_as_uint(x[i]);
+  if (u == 0x80000000u) u = 0u;  // -0 beside +0
+  key[i] = x[i] != x[i] ? 0xffffffffu : (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // NaN last
+  val[i] = i;
+}
+
+__global__ void k_sorted_x(const int32_t* __restrict__ sidx, const float* __restrict__ x, int n,
+                           float* __restrict__ sx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) sx[i] = x[sidx[i]];
+}
+
+// Largest radius of a confirmed halo among entries 0..n-1 (radii >= 0 compare as their bits).
+__global__ void k_rmax(const float* __restrict__ r, const int32_t* __restrict__ rc, int n, int* out) {
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (rc[i] == -1 && r[i] > 0.f) m = max(m, __float_as_int(r[i]));
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+size_t x_order_bytes(int n) {
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
+                                  (int32_t*)nullptr, n > 0 ? n : 1);
+  return tb + 20 * (size_t)n + 6 * 256;
+}
+
+// Entries in x order: sidx (entry per sorted position) and sx (its x).
+int x_order(asohf_ctx* c, const float* dx, int n, int32_t** sidx, float** sx) {
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
+                                  (int32_t*)nullptr, n > 0 ? n : 1);
+  uint32_t* k0 = (uint32_t*)arena_alloc(c, 4 * (size_t)n + 4);
+  uint32_t* k1 = (uint32_t*)arena_alloc(c, 4 * (size_t)n + 4);
+  int32_t* v0 = (int32_t*)arena_alloc(c, 4 * (size_t)n + 4);
+  int32_t* v1 = (int32_t*)arena_alloc(c, 4 * (size_t)n + 4);
+  float* s = (float*)arena_alloc(c, 4 * (size_t)n + 4);
+  void* t = arena_alloc(c, tb);
+  if (!k0 || !k1 || !v0 || !v1 || !s || !t) return ASOHF_ERR_CAPACITY;
+  if (n > 0) {
+    k_x_keys<<<(n + 255) / 256, 256, 0, c->stream>>>(dx, n, k0, v0);
+    ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, n, 0, 32, c->stream));
+    k_sorted_x<<<(n + 255) / 256, 256, 0, c->stream>>>(v1, dx, n, s);
+    c->launches += 2;
+  }
+  *sidx = v1;
+  *sx = s;
+  return ASOHF_OK;
+}
+
+// Device copies of the fields both routines read (entries 0..n-1), REALCLUS
+// read back by the caller; with on_device the caller's arrays are used.
+struct CleanIo {
+  CleanCat d;
+  int32_t* h_rc = nullptr;
+  int n = 0;
+  bool host = false;
+};
+
+int clean_in(asohf_ctx* c, const asohf_catalogue* cat, int n, int on_device, CleanIo* io) {
+  io->n = n;
+  io->host = !on_device;
+  io->h_rc = cat->realclus;
+  ASOHF_CHECK(arena_reserve(c, (on_device ? 0 : (size_t)n * 40 + 10 * 256) + x_order_bytes(n) + 4096));
+  if (on_device) {
+    io->d = CleanCat{cat->clusrx, cat->clusry, cat->clusrz, cat->vx, cat->vy, cat->vz, cat->masa, cat->radio,
+                     cat->levhal, cat->realclus};
+    return ASOHF_OK;
+  }
+  const float* hf[8] = {cat->clusrx, cat->clusry, cat->clusrz, cat->vx, cat->vy, cat->vz, cat->masa, cat->radio};
+  float* df[8];
+  for (int q = 0; q < 8; q++) {
+    df[q] = (float*)arena_alloc(c, 4 * (size_t)n + 4);
+    if (!df[q]) return ASOHF_ERR_CAPACITY;
+    if (n) ASOHF_CUDA(cudaMemcpyAsync(df[q], hf[q], 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  }
+  int32_t* dl = (int32_t*)arena_alloc(c, 4 * (size_t)n + 4);
+  int32_t* dr = (int32_t*)arena_alloc(c, 4 * (size_t)n + 4);
+  if (!dl || !dr) return ASOHF_ERR_CAPACITY;
+  if (n) {
+    ASOHF_CUDA(cudaMemcpyAsync(dl, cat->levhal, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(dr, cat->realclus, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  }
+  io->d = CleanCat{df[0], df[1], df[2], df[3], df[4], df[5], df[6], df[7], dl, dr};
+  return ASOHF_OK;
+}
+
+// Level of every entry 0..n-1 on the host (a copy when the catalogue is on
+// the device); ASOHF_ERR_INVALID unless the levels never decrease.
+int level_runs(asohf_ctx* c, const asohf_catalogue* cat, int n, int on_device, int32_t** lev_out) {
+  int32_t* lev = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
+  if (!lev) return ASOHF_ERR_CAPACITY;
+  if (on_device) {
+    if (n) ASOHF_CUDA(cudaMemcpyAsync(lev, cat->levhal, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  } else if (n) {
+    memcpy(lev, cat->levhal, 4 * (size_t)n);
+  }
+  for (int i = 1; i < n; i++)
+    if (lev[i] < lev[i - 1]) {
+      free(lev);
+      return ASOHF_ERR_INVALID;
+    }
+  *lev_out = lev;
+  return ASOHF_OK;
+}
+
+}  // namespace
+
+extern "C" int asohf_check_rubish(asohf_ctx* c, asohf_catalogue* cat, int nclus, int low1, int low2,
+                                  int on_device, int32_t* removed) {
+  if (!c || !cat || nclus < 0 || nclus > cat->capacity || low1 < 1 || low2 > nclus) return ASOHF_ERR_INVALID;
+  if (removed) *removed = 0;
+  if (low2 < low1) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int32_t* lev = nullptr;
+  ASOHF_CHECK(level_runs(c, cat, nclus, on_device, &lev));
+  CleanIo io;
+  int rc = clean_in(c, cat, nclus, on_device, &io);
+  int* dflags = rc == ASOHF_OK ? (int*)arena_alloc(c, 8) : nullptr;
+  if (rc != ASOHF_OK || !dflags) {
+    free(lev);
+    return rc != ASOHF_OK ? rc : ASOHF_ERR_CAPACITY;
+  }
+  ASOHF_CUDA(cudaMemsetAsync(dflags, 0, 8, c->stream));
+  int kt_ = ktime_begin(c, "check_rubish");
+  int32_t* sidx = nullptr;
+  float* sx = nullptr;
+  rc = x_order(c, io.d.x, nclus, &sidx, &sx);
+  if (rc != ASOHF_OK) {
+    free(lev);
+    return rc;
+  }
+  // the window's levels in increasing order; each against everything before it
+  for (int a = low1 - 1; a < low2;) {
+    int b = a;
+    while (b < low2 && lev[b] == lev[a]) b++;
+    k_check_rubish<<<(nclus + CT - 1) / CT, CT, 0, c->stream>>>(io.d, sidx, sx, nclus, a, b, a, dflags,
+                                                                 dflags + 1);
+    c->launches++;
+    a = b;
+  }
+  ktime_end(c, kt_);
+  free(lev);
+  ASOHF_CUDA(cudaGetLastError());
+  int hflags[2];
+  ASOHF_CUDA(cudaMemcpyAsync(hflags, dflags, 8, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  if (hflags[0]) return ASOHF_ERR_UNSUPPORTED;  // a live pair with a zero speed (see the top of the file)
+  if (io.host && low2 >= low1)
+    ASOHF_CUDA(cudaMemcpyAsync(cat->realclus + low1 - 1, io.d.rc + low1 - 1, 4 * (size_t)(low2 - low1 + 1),
+                               cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  if (removed) *removed = hflags[1];
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_accidental_substructure(asohf_ctx* c, asohf_catalogue* cat, int nclus, int on_device,
+                                             int32_t* removed) {
+  if (!c || !cat || nclus < 0 || nclus > cat->capacity) return ASOHF_ERR_INVALID;
+  if (removed) *removed = 0;
+  if (nclus == 0) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  int32_t* lev = nullptr;
+  ASOHF_CHECK(level_runs(c, cat, nclus, on_device, &lev));
+  CleanIo io;
+  int rc = clean_in(c, cat, nclus, on_device, &io);
+  int* dcount = rc == ASOHF_OK ? (int*)arena_alloc(c, 8) : nullptr;
+  if (rc != ASOHF_OK || !dcount) {
+    free(lev);
+    return rc != ASOHF_OK ? rc : ASOHF_ERR_CAPACITY;
+  }
+  ASOHF_CUDA(cudaMemsetAsync(dcount, 0, 8, c->stream));  // removals, largest confirmed radius
+  int kt_ = ktime_begin(c, "accidental_substructure");
+  int32_t* sidx = nullptr;
+  float* sx = nullptr;
+  rc = x_order(c, io.d.x, nclus, &sidx, &sx);
+  if (rc != ASOHF_OK) {
+    free(lev);
+    return rc;
+  }
+  k_rmax<<<148, 256, 0, c->stream>>>(io.d.r, io.d.rc, nclus, dcount + 1);
+  c->launches++;
+  // level by level: the lowest level is never removed, each next one is
+  // settled against the survivors of all levels before it
+  int a = 0;
+  while (a < nclus && lev[a] == lev[0]) a++;
+  while (a < nclus) {
+    int b = a;
+    while (b < nclus && lev[b] == lev[a]) b++;
+    k_accidental<<<(nclus + CT - 1) / CT, CT, 0, c->stream>>>(io.d, sidx, sx, nclus, a, b, a,
+                                                              (const float*)(dcount + 1), dcount);
+    c->launches++;
+    a = b;
+  }
+  ktime_end(c, kt_);
+  free(lev);
+  ASOHF_CUDA(cudaGetLastError());
+  int hcount = 0;
+  ASOHF_CUDA(cudaMemcpyAsync(&hcount, dcount, 4, cudaMemcpyDeviceToHost, c->stream));
+  if (io.host)
+    ASOHF_CUDA(cudaMemcpyAsync(cat->realclus, io.d.rc, 4 * (size_t)nclus, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  if (removed) *removed = hcount;
+  return ASOHF_OK;
+}

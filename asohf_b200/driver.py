@@ -160,6 +160,9 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
             continue
         backend.halofind_particles(consts, mesh, cat, low1, low2, pph)
         backend.prune_poor_haloes(consts, cat, low1, low2, np.float32(1.0), 0)
+        # catalogue cleaning (asohf.f:672-675)
+        backend.check_rubish(cat, low1, low2)
+        backend.accidental_substructure(cat)
     T["halofind"] = time.perf_counter() - t0
     subs_lev = np.zeros(mesh.nl + 1, np.int32)
     subs_lev[0] = cat.nclus

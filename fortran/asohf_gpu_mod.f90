@@ -3,10 +3,12 @@
 !
 ! Include from asohf.f under `#if gpu == 1` in place of the Fortran bodies of
 ! DENSITY, RENORM_DENSITY, SORT_DM_PARTICLES_LOCALDENSITY,
-! SORT_DM_PARTICLES_X, PRUNE_POOR_HALOES, HALOFIND_PARTICLES and
-! SUBSTRUCTURE_PARTICLES.  The dummy argument lists are the reference's
-! (grids.f:710, grids.f:2668, reader.f:140, grids.f:2726,
-! haloes_particles.f:185, haloes_particles.f:578, substructure.f:756).
+! SORT_DM_PARTICLES_X, PRUNE_POOR_HALOES, CHECK_RUBISH,
+! ACCIDENTAL_SUBSTRUCTURE, HALOFIND_PARTICLES and SUBSTRUCTURE_PARTICLES.
+! The dummy argument lists are the reference's (grids.f:710, grids.f:2668,
+! reader.f:140, grids.f:2726, haloes_particles.f:185,
+! haloes_particles.f:259, haloes_particles.f:321, haloes_particles.f:578,
+! substructure.f:756).
 ! Written against those declarations; not compiled in this repository (no
 ! Fortran compiler is available where it was written).
 
@@ -152,6 +154,22 @@
          INTEGER(C_INT64_T) :: N
          INTEGER(C_INT), VALUE :: ONDEV
         END FUNCTION
+        INTEGER(C_INT) FUNCTION ASOHF_CHECK_RUBISH_C(C, CAT, NCLUS, LOW1,
+     &   LOW2, ONDEV, KONTA) BIND(C, NAME='asohf_check_rubish')
+         IMPORT :: C_INT, C_PTR, ASOHF_CATALOGUE_T
+         TYPE(C_PTR), VALUE :: C
+         TYPE(ASOHF_CATALOGUE_T) :: CAT
+         INTEGER(C_INT), VALUE :: NCLUS, LOW1, LOW2, ONDEV
+         INTEGER(C_INT) :: KONTA
+        END FUNCTION
+        INTEGER(C_INT) FUNCTION ASOHF_ACCIDENTAL_C(C, CAT, NCLUS, ONDEV,
+     &   KONTA) BIND(C, NAME='asohf_accidental_substructure')
+         IMPORT :: C_INT, C_PTR, ASOHF_CATALOGUE_T
+         TYPE(C_PTR), VALUE :: C
+         TYPE(ASOHF_CATALOGUE_T) :: CAT
+         INTEGER(C_INT), VALUE :: NCLUS, ONDEV
+         INTEGER(C_INT) :: KONTA
+        END FUNCTION
        END INTERFACE
 
       CONTAINS
@@ -194,6 +212,56 @@
      &                  'SORT_DM_PARTICLES_X')
        CALL ASOHF_CHECK(ASOHF_DOWNLOAD_PARTICLES(CTX, P, 0_C_INT),
      &                  'download')
+      END SUBROUTINE
+
+! Replacement of CHECK_RUBISH (haloes_particles.f:259-318): same dummies.
+! Only the fields the test reads are bound; the rest stay C_NULL_PTR.
+      SUBROUTINE CHECK_RUBISH(NCLUS,REALCLUS,CLUSRX,CLUSRY,CLUSRZ,VX,
+     &                        VY,VZ,MASA,RADIO,LEVHAL,LOWH1,LOWH2)
+       USE ASOHF_GPU
+       IMPLICIT NONE
+       INCLUDE 'input_files/asohf_parameters.dat'
+       INTEGER NCLUS,LOWH1,LOWH2
+       INTEGER, TARGET :: REALCLUS(MAXNCLUS),LEVHAL(MAXNCLUS)
+       REAL*4, TARGET :: CLUSRX(MAXNCLUS),CLUSRY(MAXNCLUS),
+     &                   CLUSRZ(MAXNCLUS),RADIO(MAXNCLUS),MASA(MAXNCLUS)
+       REAL*4, TARGET :: VX(NMAXNCLUS),VY(NMAXNCLUS),VZ(NMAXNCLUS)
+       TYPE(ASOHF_CATALOGUE_T) :: CAT
+       INTEGER(C_INT) :: KONTA
+       CALL ASOHF_ENSURE_CTX()
+       CAT%NCLUS=NCLUS; CAT%CAPACITY=MAXNCLUS
+       CAT%CLUSRX=C_LOC(CLUSRX); CAT%CLUSRY=C_LOC(CLUSRY)
+       CAT%CLUSRZ=C_LOC(CLUSRZ); CAT%VX=C_LOC(VX); CAT%VY=C_LOC(VY)
+       CAT%VZ=C_LOC(VZ); CAT%MASA=C_LOC(MASA); CAT%RADIO=C_LOC(RADIO)
+       CAT%LEVHAL=C_LOC(LEVHAL); CAT%REALCLUS=C_LOC(REALCLUS)
+       CALL ASOHF_CHECK(ASOHF_CHECK_RUBISH_C(CTX, CAT, NCLUS, LOWH1,
+     &                  LOWH2, 0_C_INT, KONTA), 'CHECK_RUBISH')
+       WRITE(*,*)'... Checking rubbish ----->', KONTA
+      END SUBROUTINE
+
+! Replacement of ACCIDENTAL_SUBSTRUCTURE (haloes_particles.f:321-364).
+      SUBROUTINE ACCIDENTAL_SUBSTRUCTURE(NCLUS,REALCLUS,CLUSRX,CLUSRY,
+     &                                   CLUSRZ,VX,VY,VZ,MASA,RADIO,
+     &                                   LEVHAL)
+       USE ASOHF_GPU
+       IMPLICIT NONE
+       INCLUDE 'input_files/asohf_parameters.dat'
+       INTEGER NCLUS
+       INTEGER, TARGET :: REALCLUS(MAXNCLUS),LEVHAL(MAXNCLUS)
+       REAL*4, TARGET :: CLUSRX(MAXNCLUS),CLUSRY(MAXNCLUS),
+     &                   CLUSRZ(MAXNCLUS),RADIO(MAXNCLUS),MASA(MAXNCLUS)
+       REAL*4, TARGET :: VX(NMAXNCLUS),VY(NMAXNCLUS),VZ(NMAXNCLUS)
+       TYPE(ASOHF_CATALOGUE_T) :: CAT
+       INTEGER(C_INT) :: KONTA
+       CALL ASOHF_ENSURE_CTX()
+       CAT%NCLUS=NCLUS; CAT%CAPACITY=MAXNCLUS
+       CAT%CLUSRX=C_LOC(CLUSRX); CAT%CLUSRY=C_LOC(CLUSRY)
+       CAT%CLUSRZ=C_LOC(CLUSRZ); CAT%VX=C_LOC(VX); CAT%VY=C_LOC(VY)
+       CAT%VZ=C_LOC(VZ); CAT%MASA=C_LOC(MASA); CAT%RADIO=C_LOC(RADIO)
+       CAT%LEVHAL=C_LOC(LEVHAL); CAT%REALCLUS=C_LOC(REALCLUS)
+       CALL ASOHF_CHECK(ASOHF_ACCIDENTAL_C(CTX, CAT, NCLUS, 0_C_INT,
+     &                  KONTA), 'ACCIDENTAL_SUBSTRUCTURE')
+       WRITE(*,*)'... Checking accidental substructure ----->', KONTA
       END SUBROUTINE
 
 ! The other replacements (DENSITY, RENORM_DENSITY,

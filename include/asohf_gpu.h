@@ -145,6 +145,24 @@ int asohf_prune_poor_haloes(asohf_ctx *ctx, const asohf_consts *k, asohf_catalog
                             int low1, int low2, float facrad, int do_need_to_count,
                             int on_device);
 
+/* CHECK_RUBISH (haloes_particles.f:259-318), called after each level's
+ * refinement (asohf.f:672-673): a halo of the window low1..low2 (1-based,
+ * inclusive) is removed (REALCLUS=0) when a live halo of a lower level lies
+ * within 1.01 times the smaller radius, with mass ratio above 0.2 and
+ * relative speed difference below 3.  Requires levels that never decrease
+ * with the catalogue index (the driver's order; ASOHF_ERR_INVALID
+ * otherwise).  A zero speed leaves the Fortran's speed ratio at the
+ * previous pair's value; when that alone would decide a removal the call
+ * returns ASOHF_ERR_UNSUPPORTED.  *removed (may be NULL) receives KONTA. */
+int asohf_check_rubish(asohf_ctx *ctx, asohf_catalogue *cat, int nclus, int low1, int low2, int on_device,
+                       int32_t *removed);
+/* ACCIDENTAL_SUBSTRUCTURE (haloes_particles.f:321-364), asohf.f:674-675: a
+ * confirmed halo (REALCLUS=-1) wholly inside a confirmed halo of a lower
+ * level (DIS + R <= R of the other) is removed.  Same level-order
+ * requirement.  *removed (may be NULL) receives KONTA. */
+int asohf_accidental_substructure(asohf_ctx *ctx, asohf_catalogue *cat, int nclus, int on_device,
+                                  int32_t *removed);
+
 /* HALOFIND_PARTICLES (haloes_particles.f:578-1411) over haloes
  * lowh1..lowh2: recentering, SO growth, radial sort, unbinding, SO walk,
  * properties and bound-particle IDs (appended to the context's

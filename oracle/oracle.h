@@ -63,6 +63,15 @@ void orc_find_particle_indices(float cx, float r, float xldom, float dx, int nma
 void orc_prune_poor_haloes(const orc_store *st, const asohf_consts *k,
                            asohf_catalogue *cat, int low1, int low2,
                            float facrad, int do_need_to_count);
+/* CHECK_RUBISH (haloes_particles.f:259-318): a halo of the window
+ * low1..low2 is removed (REALCLUS=0) when a live halo of a lower level is
+ * closer than 1.01 times the smaller radius, with mass ratio above 0.2 and
+ * relative speed difference below 3.  Returns the number removed. */
+int orc_check_rubish(asohf_catalogue *cat, int nclus, int low1, int low2);
+/* ACCIDENTAL_SUBSTRUCTURE (haloes_particles.f:321-364): a confirmed halo
+ * (REALCLUS=-1) lying wholly inside a confirmed halo of a lower level is
+ * removed.  Returns the number removed. */
+int orc_accidental_substructure(asohf_catalogue *cat, int nclus);
 /* HALOFIND_PARTICLES for haloes low1..low2 (Fortran 1-based, inclusive).
  * The bound-particle ID stream is written to pph (capacity pph_cap) and the
  * total used length returned in *pph_len.  Returns a status code. */

@@ -208,6 +208,14 @@ class OracleBackend:
         lib().orc_prune_poor_haloes(C.byref(s), C.byref(consts), C.byref(cc), C.c_int(low1),
                                     C.c_int(low2), C.c_float(facrad), C.c_int(do_need_to_count))
 
+    def check_rubish(self, cat, low1, low2):
+        cc = cat.as_c()
+        return lib().orc_check_rubish(C.byref(cc), C.c_int(cat.nclus), C.c_int(low1), C.c_int(low2))
+
+    def accidental_substructure(self, cat):
+        cc = cat.as_c()
+        return lib().orc_accidental_substructure(C.byref(cc), C.c_int(cat.nclus))
+
     def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
         s = self._store()
         cc = cat.as_c()

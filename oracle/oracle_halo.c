@@ -63,6 +63,61 @@ static int count_particles_halo(const orc_store *st, const asohf_consts *k,
 }
 
 /* PRUNE_POOR_HALOES (haloes_particles.f:185-256). low1/low2 Fortran 1-based. */
+/* CHECK_RUBISH (haloes_particles.f:259-318), the Fortran loops in order.
+ * A2 keeps its last value when one of the two speeds is zero (the Fortran
+ * assigns it only otherwise); before any assignment it is taken as 0. */
+int orc_check_rubish(asohf_catalogue *cat, int nclus, int low1, int low2)
+{
+  int konta = 0;
+  float a2 = 0.0f;
+  for (int i = 1; i <= nclus; i++) {
+    if (cat->realclus[i - 1] == 0) continue;
+    for (int j = low1; j <= low2; j++) {
+      if (!(cat->realclus[j - 1] != 0 && cat->levhal[j - 1] > cat->levhal[i - 1])) continue;
+      float dx = cat->clusrx[i - 1] - cat->clusrx[j - 1];
+      float dy = cat->clusry[i - 1] - cat->clusry[j - 1];
+      float dz = cat->clusrz[i - 1] - cat->clusrz[j - 1];
+      float dis = sqrtf(dx * dx + dy * dy + dz * dz);
+      float mi = cat->masa[i - 1], mj = cat->masa[j - 1];
+      float a1 = (mi < mj ? mi : mj) / (mi > mj ? mi : mj);
+      float v1 = sqrtf(cat->vx[i - 1] * cat->vx[i - 1] + cat->vy[i - 1] * cat->vy[i - 1] +
+                       cat->vz[i - 1] * cat->vz[i - 1]);
+      float v2 = sqrtf(cat->vx[j - 1] * cat->vx[j - 1] + cat->vy[j - 1] * cat->vy[j - 1] +
+                       cat->vz[j - 1] * cat->vz[j - 1]);
+      if ((v1 < v2 ? v1 : v2) != 0.0f) a2 = fabsf(v1 - v2) / (v1 > v2 ? v1 : v2);
+      float ri = cat->radio[i - 1], rj = cat->radio[j - 1];
+      float a3 = ri < rj ? ri : rj;
+      if (dis < 1.01f * a3 && a1 > 0.2f && a2 < 3.0f) {
+        cat->realclus[j - 1] = 0;
+        konta++;
+      }
+    }
+  }
+  return konta;
+}
+
+/* ACCIDENTAL_SUBSTRUCTURE (haloes_particles.f:321-364), the Fortran loops in
+ * order. */
+int orc_accidental_substructure(asohf_catalogue *cat, int nclus)
+{
+  int konta = 0;
+  for (int i = 1; i <= nclus; i++) {
+    if (cat->realclus[i - 1] != -1) continue;
+    for (int j = 1; j <= nclus; j++) {
+      if (cat->realclus[j - 1] != -1) continue;
+      float dx = cat->clusrx[i - 1] - cat->clusrx[j - 1];
+      float dy = cat->clusry[i - 1] - cat->clusry[j - 1];
+      float dz = cat->clusrz[i - 1] - cat->clusrz[j - 1];
+      float dis = sqrtf(dx * dx + dy * dy + dz * dz);
+      if (cat->levhal[j - 1] > cat->levhal[i - 1] && dis + cat->radio[j - 1] <= 1.0f * cat->radio[i - 1]) {
+        cat->realclus[j - 1] = 0;
+        konta++;
+      }
+    }
+  }
+  return konta;
+}
+
 void orc_prune_poor_haloes(const orc_store *st, const asohf_consts *k,
                            asohf_catalogue *cat, int low1, int low2,
                            float facrad, int do_need_to_count)

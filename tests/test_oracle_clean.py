@@ -1,0 +1,39 @@
+"""Known answers of the oracle's CHECK_RUBISH and ACCIDENTAL_SUBSTRUCTURE
+(haloes_particles.f:259-364) on hand-built catalogues."""
+import numpy as np
+
+from asohf_b200 import abi
+from oracle import oracle as O
+
+
+def cat_of(rows):
+    """rows: (level, x, y, z, radius, mass, speed, realclus)"""
+    c = abi.Catalogue(len(rows) + 2)
+    for i, (l, x, y, z, r, m, v, rc) in enumerate(rows):
+        c.levhal[i], c.clusrx[i], c.clusry[i], c.clusrz[i] = l, x, y, z
+        c.radio[i], c.masa[i], c.vx[i], c.realclus[i] = r, m, v, rc
+    c.nclus = len(rows)
+    return c
+
+
+def test_check_rubish_known_answers():
+    rows = [(0, 0.0, 0.0, 0.0, 1.0, 1e12, 100.0, -1),   # host
+            (1, 0.5, 0.0, 0.0, 0.6, 5e11, 120.0, -1),   # inside 1.01*0.6, mass ratio 0.5: removed
+            (1, 0.5, 0.0, 0.0, 0.6, 1e11, 120.0, -1),   # mass ratio 0.1: kept
+            (1, 3.0, 0.0, 0.0, 0.6, 5e11, 120.0, -1),   # too far: kept
+            (1, 0.2, 0.0, 0.0, 0.6, 5e11, 500.0, -1)]   # |dv|/v = 0.8 < 3: removed
+    c = cat_of(rows)
+    k = O.OracleBackend().check_rubish(c, 2, 5)
+    assert k == 2
+    assert list(c.realclus[:5]) == [-1, 0, -1, -1, 0]
+
+
+def test_accidental_substructure_known_answers():
+    rows = [(0, 0.0, 0.0, 0.0, 1.0, 1e12, 100.0, -1),
+            (1, 0.3, 0.0, 0.0, 0.5, 1e11, 100.0, -1),   # 0.3 + 0.5 <= 1: removed
+            (1, 0.6, 0.0, 0.0, 0.5, 1e11, 100.0, -1),   # 1.1 > 1: kept
+            (2, 0.6, 0.0, 0.0, 0.3, 1e10, 100.0, -1)]   # inside the kept level-1 halo: removed
+    c = cat_of(rows)
+    k = O.OracleBackend().accidental_substructure(c)
+    assert k == 2
+    assert list(c.realclus[:4]) == [-1, 0, -1, 0]
