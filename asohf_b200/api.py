@@ -292,6 +292,16 @@ class Asohf:
                                                     C.byref(n)), "ACCIDENTAL_SUBSTRUCTURE")
         return n.value
 
+    def overlapping(self, cat, ir, nhallev, vol_solap_low):
+        """OVERLAPPING at level ir (nhallev[l]: haloes of level l); returns
+        the number of removed haloes among level ir's."""
+        nh = np.ascontiguousarray(nhallev[:ir + 1], dtype=np.int32)
+        cc = cat.as_c()
+        n = C.c_int32()
+        _check(self.L.asohf_overlapping(self.h, C.byref(cc), C.c_int(ir), nh.ctypes.data_as(C.c_void_p),
+                                        C.c_float(vol_solap_low), C.c_int(0), C.byref(n)), "OVERLAPPING")
+        return n.value
+
     def halofind_particles(self, consts, mesh, cat, low1, low2):
         mh = abi.MeshHolder(mesh)
         cc = cat.as_c()
@@ -451,6 +461,9 @@ class GpuBackend:
 
     def accidental_substructure(self, cat):
         return self.a.accidental_substructure(cat)
+
+    def overlapping(self, cat, ir, nhallev, vol_solap_low):
+        return self.a.overlapping(cat, ir, nhallev, vol_solap_low)
 
     def substructure_particles(self, consts, mesh, cat, ir, subs_lev, pph):
         self.a.substructure_particles(consts, mesh, cat, ir, subs_lev)

@@ -162,6 +162,18 @@ int asohf_check_rubish(asohf_ctx *ctx, asohf_catalogue *cat, int nclus, int low1
  * requirement.  *removed (may be NULL) receives KONTA. */
 int asohf_accidental_substructure(asohf_ctx *ctx, asohf_catalogue *cat, int nclus, int on_device,
                                   int32_t *removed);
+/* OVERLAPPING (haloes_grids.f:27-201), called by the grid finder at the end
+ * of each level (haloes_grids.f:577, 1081): over the haloes 1..lowh2, with
+ * the new level lowh3..lowh2 (lowh3 = SUM(NHALLEV(0:ir-1))+1, lowh2 =
+ * SUM(NHALLEV(0:ir)); nhallev: host array of ir+1 counts), pass 1 removes
+ * the smaller of two nested spheres, pass 2 the smaller of two spheres
+ * whose lens overlap exceeds vol_solap_low of the smaller volume, with the
+ * Fortran's sequential order reproduced.  The reference's mesh, SOLAP,
+ * CR0AMR and density arguments are not read by the routine and are not
+ * taken.  *removed (may be NULL) receives COUNT(REALCLUS(lowh3:lowh2)==0),
+ * the figure the routine prints. */
+int asohf_overlapping(asohf_ctx *ctx, asohf_catalogue *cat, int ir, const int32_t *nhallev,
+                      float vol_solap_low, int on_device, int32_t *removed);
 
 /* HALOFIND_PARTICLES (haloes_particles.f:578-1411) over haloes
  * lowh1..lowh2: recentering, SO growth, radial sort, unbinding, SO walk,

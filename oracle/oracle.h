@@ -68,6 +68,8 @@ void orc_prune_poor_haloes(const orc_store *st, const asohf_consts *k,
  * closer than 1.01 times the smaller radius, with mass ratio above 0.2 and
  * relative speed difference below 3.  Returns the number removed. */
 int orc_check_rubish(asohf_catalogue *cat, int nclus, int low1, int low2);
+/* OVERLAPPING (haloes_grids.f:27-201) over halo indices 1..lowh2, the new level lowh3..lowh2. */
+int orc_overlapping(asohf_catalogue *cat, int lowh3, int lowh2, float vol_solap_low);
 /* ACCIDENTAL_SUBSTRUCTURE (haloes_particles.f:321-364): a confirmed halo
  * (REALCLUS=-1) lying wholly inside a confirmed halo of a lower level is
  * removed.  Returns the number removed. */

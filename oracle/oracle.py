@@ -216,6 +216,13 @@ class OracleBackend:
         cc = cat.as_c()
         return lib().orc_accidental_substructure(C.byref(cc), C.c_int(cat.nclus))
 
+    def overlapping(self, cat, ir, nhallev, vol_solap_low):
+        """OVERLAPPING at level ir; nhallev[l] = haloes found at level l."""
+        lowh3 = int(sum(nhallev[:ir])) + 1
+        lowh2 = int(sum(nhallev[:ir + 1]))
+        cc = cat.as_c()
+        return lib().orc_overlapping(C.byref(cc), C.c_int(lowh3), C.c_int(lowh2), C.c_float(vol_solap_low))
+
     def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
         s = self._store()
         cc = cat.as_c()

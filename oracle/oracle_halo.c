@@ -118,6 +118,50 @@ int orc_accidental_substructure(asohf_catalogue *cat, int nclus)
   return konta;
 }
 
+/* OVERLAPPING (haloes_grids.f:27-201), the grid finder's overlap removal at
+ * the end of level IR: lowh3 = SUM(NHALLEV(0:IR-1))+1, lowh2 =
+ * SUM(NHALLEV(0:IR)).  Pass 1 removes the smaller of two spheres when one
+ * lies inside the other (|R1-R2| >= DIST); pass 2 when the overlap volume
+ * (two-sphere lens, in units of the smaller sphere) exceeds vol_solap_low.
+ * The row halo's REALCLUS is read once per row (BASINT), so a removed row
+ * halo still removes later partners.  Returns COUNT(REALCLUS(lowh3:lowh2)
+ * == 0), the figure the routine prints. */
+int orc_overlapping(asohf_catalogue *cat, int lowh3, int lowh2, float vol_solap_low)
+{
+  const float pi = (float)acos(-1.0);
+  for (int pass = 1; pass <= 2; pass++) {
+    for (int i = 1; i <= lowh2; i++) {
+      if (cat->realclus[i - 1] == 0) continue;
+      const float r1 = cat->radio[i - 1], x1 = cat->clusrx[i - 1], y1 = cat->clusry[i - 1],
+                  z1 = cat->clusrz[i - 1];
+      for (int j = (i + 1 > lowh3 ? i + 1 : lowh3); j <= lowh2; j++) {
+        if (cat->realclus[j - 1] == 0) continue;
+        const float r2 = cat->radio[j - 1];
+        const float dx = x1 - cat->clusrx[j - 1], dy = y1 - cat->clusry[j - 1], dz = z1 - cat->clusrz[j - 1];
+        const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+        int imin = j;
+        if (pass == 1) {
+          if (!(fabsf(r1 - r2) >= dist)) continue;
+          if (r2 > r1 && cat->levhal[j - 1] <= cat->levhal[i - 1]) imin = i;
+        } else {
+          const float s = r1 + r2, d = r1 - r2;
+          const float bas = dist / s;
+          if (!(bas < 1.0f)) continue;
+          const float xi = bas, u = 1.0f - xi, m = fminf(r1, r2);
+          float vint = pi / 12.0f * (s * s * s) * (u * u / xi) * (xi * xi + 2.0f * xi - 3.0f * (d * d) / (s * s));
+          vint = vint / (4.0f * pi / 3.0f * (m * m * m));
+          if (!(vint > vol_solap_low)) continue;
+          if (r2 > 1.5f * r1 && cat->levhal[j - 1] <= cat->levhal[i - 1]) imin = i;
+        }
+        cat->realclus[imin - 1] = 0;
+      }
+    }
+  }
+  int n0 = 0;
+  for (int j = lowh3; j <= lowh2; j++) n0 += cat->realclus[j - 1] == 0;
+  return n0;
+}
+
 void orc_prune_poor_haloes(const orc_store *st, const asohf_consts *k,
                            asohf_catalogue *cat, int low1, int low2,
                            float facrad, int do_need_to_count)

@@ -37,3 +37,21 @@ def test_accidental_substructure_known_answers():
     k = O.OracleBackend().accidental_substructure(c)
     assert k == 2
     assert list(c.realclus[:4]) == [-1, 0, -1, 0]
+
+
+def test_overlapping_known_answers():
+    """OVERLAPPING (haloes_grids.f:27-201) at level 1 of a two-level list."""
+    rows = [(0, 0.0, 0.0, 0.0, 1.0, 1e12, 100.0, -1),   # level 0
+            (0, 5.0, 0.0, 0.0, 1.0, 1e12, 100.0, -1),   # level 0
+            (1, 0.2, 0.0, 0.0, 0.5, 1e11, 100.0, -1),   # nested in halo 1 (|1-0.5| >= 0.2): removed
+            (1, 6.1, 0.0, 0.0, 1.0, 1e11, 100.0, -1),   # equal radii 1.1 apart: lens 0.26 of a sphere
+            (1, 9.0, 0.0, 0.0, 0.3, 1e11, 100.0, -1),   # alone: kept
+            (1, 9.0, 0.0, 0.1, 2.0, 1e11, 100.0, -1)]   # contains the one before, larger, same level:
+                                                         # the smaller (row 5) is removed
+    c = cat_of(rows)
+    k = O.OracleBackend().overlapping(c, 1, [2, 4], 0.2)
+    assert list(c.realclus[:6]) == [-1, -1, 0, 0, 0, -1]
+    assert k == 3
+    c = cat_of(rows)
+    O.OracleBackend().overlapping(c, 1, [2, 4], 0.3)   # above the lens fraction: row 4 kept
+    assert list(c.realclus[:6]) == [-1, -1, 0, -1, 0, -1]
