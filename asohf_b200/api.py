@@ -237,6 +237,35 @@ class Asohf:
             C.c_float(rote), C.c_float(rete), C.byref(mh.c), _ptr(u1), _ptr(u11),
             C.c_int(int(_is_torch(u1)))), "INTERPOLATE_DENSITY_TSC")
 
+    def mesh_base_counts(self, nx, dx, refine_thr, bor, npart_esp, out=None):
+        """CREATE_MESH base-grid counts CR0 (grids.f:107-143), flat nx^3, IX fastest."""
+        esp = np.zeros(abi.N_ESP, np.int32)
+        esp[:len(npart_esp)] = npart_esp
+        if out is None:
+            out = np.empty(nx ** 3, np.int32)
+        _check(self.L.asohf_mesh_base_counts(self.h, C.c_int(nx), C.c_float(dx), C.c_int(refine_thr), C.c_int(bor),
+                                             esp.ctypes.data_as(C.c_void_p), _ptr(out),
+                                             C.c_int(int(_is_torch(out)))), "CREATE_MESH counts")
+        return out
+
+    def mesh_patch_counts(self, nx, lado0, dx, irpa, refine_thr, boramr, npart_esp, pnx, pny, pnz, prx, pry, prz,
+                          out=None):
+        """CREATE_MESH counts CR01 on the patches of level irpa (grids.f:341-380),
+        (npatch, NAMRX^3) int32, IX fastest."""
+        esp = np.zeros(abi.N_ESP, np.int32)
+        esp[:len(npart_esp)] = npart_esp
+        ai = [np.ascontiguousarray(a, np.int32) for a in (pnx, pny, pnz)]
+        af = [np.ascontiguousarray(a, np.float32) for a in (prx, pry, prz)]
+        npatch = int(ai[0].shape[0])
+        if out is None:
+            out = np.empty((npatch, abi.NAMRX ** 3), np.int32)
+        _check(self.L.asohf_mesh_patch_counts(
+            self.h, C.c_int(nx), C.c_float(lado0), C.c_float(dx), C.c_int(irpa), C.c_int(refine_thr),
+            C.c_int(boramr), esp.ctypes.data_as(C.c_void_p), C.c_int(npatch),
+            *[a.ctypes.data_as(C.c_void_p) for a in ai], *[a.ctypes.data_as(C.c_void_p) for a in af],
+            _ptr(out), C.c_int(int(_is_torch(out)))), "CREATE_MESH patch counts")
+        return out
+
     def poisson_fft(self, nx, dx, rho, pot, batch=1):
         """MOMENTO + POFFT3D (poisson.f:98-249)."""
         _check(self.L.asohf_poisson_fft(self.h, C.c_int(nx), C.c_float(dx), C.c_int(batch),

@@ -1498,3 +1498,177 @@ int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* 
   ASOHF_CUDA(cudaGetLastError());
   return ASOHF_OK;
 }
+
+// ------------------------------------------------------------ CREATE_MESH particle counts
+// The two counting loops of CREATE_MESH (grids.f:107-143 for the base grid,
+// grids.f:357-380 for the patches of one level): NGP cell counts in which a
+// particle weighs 1 when its species level PLEV is at most the level being
+// refined (0 for the base grid) and REFINE_THR otherwise, then zero within
+// BOR (BORAMR) cells of the faces.  PLEV(I) is the species whose index range
+// (NPART_ESP, store order) holds I, and 0 past the last range (grids.f:83-91).
+// The patch placement that consumes the counts is sequential and stays with
+// the caller.
+
+struct EspEnds {
+  int64_t e[ASOHF_N_ESP];  // cumulative ends of the species ranges
+};
+
+__device__ __forceinline__ int plev_of(int64_t i, const EspEnds& E) {
+  for (int s = 0; s < ASOHF_N_ESP; s++)
+    if (i < E.e[s]) return s;
+  return 0;
+}
+
+__global__ void k_mesh_base_counts(const float* __restrict__ x, const float* __restrict__ y,
+                                   const float* __restrict__ z, int64_t n, int nx, float xl, float dx,
+                                   int refine_thr, EspEnds E, int32_t* __restrict__ cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    // IX = INT((RXPA-XL)/DX)+1 clamped to 1..NX (a NaN offset counts as below)
+    int c3[3];
+    const float v3[3] = {x[i], y[i], z[i]};
+    for (int a = 0; a < 3; a++) {
+      const float v = __fdiv_rn(__fsub_rn(v3[a], xl), dx);
+      c3[a] = v >= (float)nx ? nx : (v >= 1.0f ? (int)v + 1 : 1);
+    }
+    const int w = plev_of(i, E) == 0 ? 1 : refine_thr;
+    atomicAdd(&cnt[((int64_t)(c3[2] - 1) * nx + (c3[1] - 1)) * nx + (c3[0] - 1)], w);
+  }
+}
+
+__global__ void k_mesh_border(int32_t* __restrict__ cnt, int nx, int bor) {
+  const int64_t g = (int64_t)nx * nx * nx;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < g; q += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(q % nx) + 1, jy = (int)((q / nx) % nx) + 1, kz = (int)(q / ((int64_t)nx * nx)) + 1;
+    if (ix <= bor || ix >= nx - bor + 1 || jy <= bor || jy >= nx - bor + 1 || kz <= bor || kz >= nx - bor + 1)
+      cnt[q] = 0;
+  }
+}
+
+// One CTA per patch of the level: counts in shared memory (NAMRX^3 ints),
+// candidates from the bins covering the patch widened by two fine cells
+// (a superset of the particles the FLOOR test keeps, for cells wider than
+// the float spacing of the coordinates).
+__global__ void __launch_bounds__(PD_BLOCK)
+k_mesh_patch_counts(const int32_t* __restrict__ pn, const float* __restrict__ pr, int np, Bins B,
+                    const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                    int irpa, float dxpa, int refine_thr, int boramr, EspEnds E, int32_t* __restrict__ out) {
+  extern __shared__ int32_t s_cnt[];
+  const int ip = blockIdx.x;
+  const int n1 = pn[ip], n2 = pn[np + ip], n3 = pn[2 * np + ip];
+  for (int q = threadIdx.x; q < NA * NA * NA; q += blockDim.x) s_cnt[q] = 0;
+  __syncthreads();
+  // XL = PATCHRX - DXPA (grids.f:358-360)
+  const float xl = __fsub_rn(pr[ip], dxpa), yl = __fsub_rn(pr[np + ip], dxpa), zl = __fsub_rn(pr[2 * np + ip], dxpa);
+  const float pad = 2.0f * dxpa;
+  const int bx0 = bin_of(xl - pad, B.xl, B.bsz, B.nb), bx1 = bin_of(xl + (float)(n1 + 2) * dxpa, B.xl, B.bsz, B.nb);
+  const int by0 = bin_of(yl - pad, B.xl, B.bsz, B.nb), by1 = bin_of(yl + (float)(n2 + 2) * dxpa, B.xl, B.bsz, B.nb);
+  const int bz0 = bin_of(zl - pad, B.xl, B.bsz, B.nb), bz1 = bin_of(zl + (float)(n3 + 2) * dxpa, B.xl, B.bsz, B.nb);
+  for (int bz = bz0; bz <= bz1; bz++)
+    for (int by = by0; by <= by1; by++) {
+      const int lo = B.start[(bz * B.nb + by) * B.nb + bx0], hi = B.start[(bz * B.nb + by) * B.nb + bx1 + 1];
+      for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+        const int p = B.idx[t];
+        // IX = FLOOR((RXPA-XL)/DXPA)+1 kept when 1 <= IX <= N1
+        const float vx = __fdiv_rn(__fsub_rn(x[p], xl), dxpa);
+        if (!(vx >= 0.0f && vx < (float)n1)) continue;
+        const float vy = __fdiv_rn(__fsub_rn(y[p], yl), dxpa);
+        if (!(vy >= 0.0f && vy < (float)n2)) continue;
+        const float vz = __fdiv_rn(__fsub_rn(z[p], zl), dxpa);
+        if (!(vz >= 0.0f && vz < (float)n3)) continue;
+        const int w = plev_of(p, E) <= irpa ? 1 : refine_thr;
+        atomicAdd(&s_cnt[((int)vz * NA + (int)vy) * NA + (int)vx], w);
+      }
+    }
+  __syncthreads();
+  int32_t* o = out + (size_t)ip * NA * NA * NA;
+  for (int q = threadIdx.x; q < NA * NA * NA; q += blockDim.x) {
+    const int ix = q % NA + 1, jy = (q / NA) % NA + 1, kz = q / (NA * NA) + 1;
+    int v = s_cnt[q];
+    if (ix > n1 || jy > n2 || kz > n3 || ix <= boramr || ix >= n1 - boramr + 1 || jy <= boramr ||
+        jy >= n2 - boramr + 1 || kz <= boramr || kz >= n3 - boramr + 1)
+      v = 0;
+    o[q] = v;
+  }
+}
+
+static int esp_ends(const int32_t* npart_esp, EspEnds* E) {
+  int64_t acc = 0;
+  for (int s = 0; s < ASOHF_N_ESP; s++) {
+    if (npart_esp[s] < 0) return ASOHF_ERR_INVALID;
+    acc += npart_esp[s];
+    E->e[s] = acc;
+  }
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_mesh_base_counts(asohf_ctx* c, int nx, float dx, int refine_thr, int bor,
+                                      const int32_t* npart_esp, int32_t* cr0, int on_device) {
+  if (!c || nx <= 0 || !npart_esp || !cr0) return ASOHF_ERR_INVALID;
+  EspEnds E;
+  ASOHF_CHECK(esp_ends(npart_esp, &E));
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  const int64_t g = (int64_t)nx * nx * nx, n = c->p.n;
+  ASOHF_CHECK(arena_reserve(c, 4 * (size_t)g + 4096));
+  int32_t* d = on_device ? cr0 : (int32_t*)arena_alloc(c, 4 * (size_t)g);
+  if (!d) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaMemsetAsync(d, 0, 4 * (size_t)g, c->stream));
+  const float xl = -((float)nx * dx / 2.0f);  // XL = -NX*DX/2.
+  int kt_ = ktime_begin(c, "mesh_base_counts");
+  if (n > 0) {
+    k_mesh_base_counts<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, nx, xl,
+                                                                                  dx, refine_thr, E, d);
+    c->launches++;
+  }
+  k_mesh_border<<<grid_for(g, 256), 256, 0, c->stream>>>(d, nx, bor);
+  c->launches++;
+  ktime_end(c, kt_);
+  ASOHF_CUDA(cudaGetLastError());
+  if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(cr0, d, 4 * (size_t)g, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_mesh_patch_counts(asohf_ctx* c, int nx, float lado0, float dx, int irpa, int refine_thr,
+                                       int boramr, const int32_t* npart_esp, int npatch, const int32_t* patchnx,
+                                       const int32_t* patchny, const int32_t* patchnz, const float* patchrx,
+                                       const float* patchry, const float* patchrz, int32_t* cr01, int on_device) {
+  if (!c || nx <= 0 || irpa < 1 || npatch < 0 || !npart_esp || (npatch > 0 && (!patchnx || !patchny || !patchnz ||
+      !patchrx || !patchry || !patchrz || !cr01)))
+    return ASOHF_ERR_INVALID;
+  EspEnds E;
+  ASOHF_CHECK(esp_ends(npart_esp, &E));
+  for (int q = 0; q < npatch; q++)
+    if (patchnx[q] < 1 || patchnx[q] > NA || patchny[q] < 1 || patchny[q] > NA || patchnz[q] < 1 || patchnz[q] > NA)
+      return ASOHF_ERR_INVALID;
+  if (npatch == 0) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  const int64_t n = c->p.n;
+  const size_t outb = 4 * (size_t)npatch * NA * NA * NA;
+  ASOHF_CHECK(arena_reserve(c, (on_device ? 0 : outb) + 24 * (size_t)npatch + bins_bytes(n, lado0, dx, 2) + 8192));
+  int32_t* pn = (int32_t*)arena_alloc(c, 12 * (size_t)npatch);
+  float* pr = (float*)arena_alloc(c, 12 * (size_t)npatch);
+  int32_t* d = on_device ? cr01 : (int32_t*)arena_alloc(c, outb);
+  if (!pn || !pr || !d) return ASOHF_ERR_CAPACITY;
+  const int32_t* hn[3] = {patchnx, patchny, patchnz};
+  const float* hr[3] = {patchrx, patchry, patchrz};
+  for (int a = 0; a < 3; a++) {
+    ASOHF_CUDA(cudaMemcpyAsync(pn + (size_t)a * npatch, hn[a], 4 * (size_t)npatch, cudaMemcpyHostToDevice, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(pr + (size_t)a * npatch, hr[a], 4 * (size_t)npatch, cudaMemcpyHostToDevice, c->stream));
+  }
+  Bins B;
+  ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B));
+  const float dxpa = ldexpf(dx, -irpa);  // DX/(2.0**IRPA), exact
+  const size_t smem = sizeof(int32_t) * NA * NA * NA;
+  ASOHF_CUDA(cudaFuncSetAttribute(k_mesh_patch_counts, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int kt_ = ktime_begin(c, "mesh_patch_counts");
+  k_mesh_patch_counts<<<npatch, PD_BLOCK, smem, c->stream>>>(pn, pr, npatch, B, c->p.x, c->p.y, c->p.z, irpa, dxpa,
+                                                             refine_thr, boramr, E, d);
+  c->launches++;
+  ktime_end(c, kt_);
+  ASOHF_CUDA(cudaGetLastError());
+  if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(cr01, d, outb, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}

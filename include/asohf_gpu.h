@@ -145,6 +145,29 @@ int asohf_prune_poor_haloes(asohf_ctx *ctx, const asohf_consts *k, asohf_catalog
                             int low1, int low2, float facrad, int do_need_to_count,
                             int on_device);
 
+/* CREATE_MESH particle counts of the base grid (grids.f:107-143), on the
+ * uploaded store in species order: cr0[(kz*nx + jy)*nx + ix] (IX fastest,
+ * nx^3 int32) = particles of species 0 plus refine_thr per particle of a
+ * heavier species in each cell, IX = INT((x - XL)/DX)+1 clamped to 1..nx
+ * with XL = -nx*dx/2, then zero within bor cells of the faces.  The species
+ * of store index i is the range of npart_esp (N_ESP counts) holding it, 0
+ * past the last.  The greedy patch placement that reads CR0 stays with the
+ * caller. */
+int asohf_mesh_base_counts(asohf_ctx *ctx, int nx, float dx, int refine_thr, int bor, const int32_t *npart_esp,
+                           int32_t *cr0, int on_device);
+/* CREATE_MESH particle counts on the npatch patches of level irpa
+ * (grids.f:341-380): per patch NAMRX^3 int32 (IX fastest), IX =
+ * FLOOR((x - XL)/DXPA)+1 kept when 1 <= IX <= PATCHNX, XL = PATCHRX - DXPA,
+ * DXPA = dx/2^irpa; 1 per particle of species <= irpa, refine_thr otherwise;
+ * zero within boramr cells of the patch faces and outside the patch.
+ * patchnx..patchrz: host arrays of the level's patches (the slice
+ * LOW1..LOW2 of the reference's patch table); nx, lado0 size the particle
+ * bins. */
+int asohf_mesh_patch_counts(asohf_ctx *ctx, int nx, float lado0, float dx, int irpa, int refine_thr, int boramr,
+                            const int32_t *npart_esp, int npatch, const int32_t *patchnx, const int32_t *patchny,
+                            const int32_t *patchnz, const float *patchrx, const float *patchry,
+                            const float *patchrz, int32_t *cr01, int on_device);
+
 /* CHECK_RUBISH (haloes_particles.f:259-318), called after each level's
  * refinement (asohf.f:672-673): a halo of the window low1..low2 (1-based,
  * inclusive) is removed (REALCLUS=0) when a live halo of a lower level lies

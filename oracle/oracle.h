@@ -43,6 +43,13 @@ void orc_tsc_deposit(int nx, float lado0, float dx, const float *radx, float rot
                      const float *z, const float *m, const asohf_mesh *mesh,
                      int mode, float *u1, float *u11);
 void orc_momento(int nx, float dx, float *kkk);
+/* CREATE_MESH particle counts (grids.f:94-143, grids.f:341-380). */
+void orc_mesh_base_counts(int64_t n, const float *x, const float *y, const float *z, int nx, float dx,
+                          int refine_thr, int bor, const int32_t *npart_esp, int32_t *cr0);
+void orc_mesh_patch_counts(int64_t n, const float *x, const float *y, const float *z, int irpa, float dx,
+                           int refine_thr, int boramr, const int32_t *npart_esp, int npatch,
+                           const int32_t *pnx, const int32_t *pny, const int32_t *pnz, const float *prx,
+                           const float *pry, const float *prz, int32_t *cr01);
 void orc_poisson_fft(int nx, float dx, const float *u1, float *pot);
 void orc_argsort(int64_t n, const float *a, int64_t *indx);
 void orc_sort_x(int64_t n, float *x, float *y, float *z, float *vx, float *vy,

@@ -250,6 +250,30 @@ class OracleBackend:
             raise RuntimeError(abi.ERRORS[rc])
         return n.value
 
+    def mesh_base_counts(self, nx, dx, refine_thr, bor, npart_esp):
+        """CREATE_MESH base-grid counts CR0 (grids.f:94-143), flat, IX fastest."""
+        p = self.p
+        esp = np.zeros(abi.N_ESP, np.int32)
+        esp[:len(npart_esp)] = npart_esp
+        out = np.empty(nx ** 3, np.int32)
+        lib().orc_mesh_base_counts(C.c_int64(p.n), P(p.x), P(p.y), P(p.z), C.c_int(nx), C.c_float(dx),
+                                   C.c_int(refine_thr), C.c_int(bor), P(esp, _ip), P(out, _ip))
+        return out
+
+    def mesh_patch_counts(self, irpa, dx, refine_thr, boramr, npart_esp, pnx, pny, pnz, prx, pry, prz):
+        """CREATE_MESH counts on the patches of level irpa (grids.f:341-380)."""
+        p = self.p
+        esp = np.zeros(abi.N_ESP, np.int32)
+        esp[:len(npart_esp)] = npart_esp
+        ai = [np.ascontiguousarray(a, np.int32) for a in (pnx, pny, pnz)]
+        af = [np.ascontiguousarray(a, np.float32) for a in (prx, pry, prz)]
+        npatch = ai[0].shape[0]
+        out = np.empty((npatch, abi.NAMRX ** 3), np.int32)
+        lib().orc_mesh_patch_counts(C.c_int64(p.n), P(p.x), P(p.y), P(p.z), C.c_int(irpa), C.c_float(dx),
+                                    C.c_int(refine_thr), C.c_int(boramr), P(esp, _ip), C.c_int(npatch),
+                                    *[P(a, _ip) for a in ai], *[P(a) for a in af], P(out, _ip))
+        return out
+
     def poisson_fft(self, u1, dx):
         return poisson_fft(u1, dx)
 

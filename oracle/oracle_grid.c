@@ -681,3 +681,86 @@ void orc_sort_x(int64_t n, float *x, float *y, float *z, float *vx, float *vy,
   for (int q = ix; q <= nx; q++) ndmpart_x[q] = (int32_t)(i - 1);
   free(radxr);
 }
+
+
+/* PLEV(I) of CREATE_MESH (grids.f:83-91): the species whose NPART_ESP range
+ * holds the 0-based store index i, 0 past the last range. */
+static int mesh_plev(int64_t i, const int32_t *npart_esp)
+{
+  int64_t acc = 0;
+  for (int s = 0; s < ASOHF_N_ESP; s++) {
+    acc += npart_esp[s];
+    if (i < acc) return s;
+  }
+  return 0;
+}
+
+/* CREATE_MESH base-grid counts (grids.f:94-143): CONTA1 by NGP with
+ * IX = INT((RXPA-XL)/DX)+1 clamped to 1..NX, weight 1 for PLEV 0 and
+ * REFINE_THR otherwise, then zero within BOR cells of the faces; CR0 =
+ * CONTA1, IX fastest.  A NaN offset takes the lower clamp. */
+void orc_mesh_base_counts(int64_t n, const float *x, const float *y, const float *z, int nx, float dx,
+                          int refine_thr, int bor, const int32_t *npart_esp, int32_t *cr0)
+{
+  const float xl = -((float)nx * dx / 2.0f);
+  const int64_t g = (int64_t)nx * nx * nx;
+  memset(cr0, 0, sizeof(int32_t) * (size_t)g);
+  for (int64_t i = 0; i < n; i++) {
+    const float v3[3] = {x[i], y[i], z[i]};
+    int c3[3];
+    for (int a = 0; a < 3; a++) {
+      const float v = (v3[a] - xl) / dx;
+      int ic;
+      if (v >= (float)nx) ic = nx;            /* INT(v)+1 > NX */
+      else if (v >= 1.0f) ic = (int)v + 1;    /* INT truncates toward zero */
+      else ic = 1;                            /* INT(v)+1 <= 1, or NaN */
+      c3[a] = ic;
+    }
+    const int w = mesh_plev(i, npart_esp) == 0 ? 1 : refine_thr;
+    int64_t q = ((int64_t)(c3[2] - 1) * nx + (c3[1] - 1)) * nx + (c3[0] - 1);
+    cr0[q] = (int32_t)((uint32_t)cr0[q] + (uint32_t)w);
+  }
+  for (int kz = 1; kz <= nx; kz++)
+    for (int jy = 1; jy <= nx; jy++)
+      for (int ix = 1; ix <= nx; ix++)
+        if (ix <= bor || ix >= nx - bor + 1 || jy <= bor || jy >= nx - bor + 1 || kz <= bor || kz >= nx - bor + 1)
+          cr0[((int64_t)(kz - 1) * nx + (jy - 1)) * nx + (ix - 1)] = 0;
+}
+
+/* CREATE_MESH counts on the patches of level IRPA (grids.f:341-380): per
+ * patch, XL = PATCHRX - DXPA, IX = FLOOR((RXPA-XL)/DXPA)+1 kept when
+ * 1 <= IX <= N1 (and the same in y, z), weight 1 for PLEV <= IRPA and
+ * REFINE_THR otherwise, zero within BORAMR cells of the faces; each patch
+ * NAMRX^3 cells, IX fastest, zero outside N1 x N2 x N3. */
+void orc_mesh_patch_counts(int64_t n, const float *x, const float *y, const float *z, int irpa, float dx,
+                           int refine_thr, int boramr, const int32_t *npart_esp, int npatch,
+                           const int32_t *pnx, const int32_t *pny, const int32_t *pnz, const float *prx,
+                           const float *pry, const float *prz, int32_t *cr01)
+{
+  const int na = ASOHF_NAMRX;
+  const float dxpa = dx / powf(2.0f, (float)irpa);
+#pragma omp parallel for schedule(dynamic)
+  for (int ip = 0; ip < npatch; ip++) {
+    int32_t *o = cr01 + (size_t)ip * na * na * na;
+    memset(o, 0, sizeof(int32_t) * (size_t)na * na * na);
+    const float xl = prx[ip] - dxpa, yl = pry[ip] - dxpa, zl = prz[ip] - dxpa;
+    const int n1 = pnx[ip], n2 = pny[ip], n3 = pnz[ip];
+    for (int64_t i = 0; i < n; i++) {
+      const float vx = floorf((x[i] - xl) / dxpa);
+      if (!(vx >= 0.0f && vx <= (float)(n1 - 1))) continue;
+      const float vy = floorf((y[i] - yl) / dxpa);
+      if (!(vy >= 0.0f && vy <= (float)(n2 - 1))) continue;
+      const float vz = floorf((z[i] - zl) / dxpa);
+      if (!(vz >= 0.0f && vz <= (float)(n3 - 1))) continue;
+      const int w = mesh_plev(i, npart_esp) <= irpa ? 1 : refine_thr;
+      const size_t q = ((size_t)vz * na + (size_t)vy) * na + (size_t)vx;
+      o[q] = (int32_t)((uint32_t)o[q] + (uint32_t)w);
+    }
+    for (int kz = 1; kz <= n3; kz++)
+      for (int jy = 1; jy <= n2; jy++)
+        for (int ix = 1; ix <= n1; ix++)
+          if (ix <= boramr || ix >= n1 - boramr + 1 || jy <= boramr || jy >= n2 - boramr + 1 || kz <= boramr ||
+              kz >= n3 - boramr + 1)
+            o[((size_t)(kz - 1) * na + (jy - 1)) * na + (ix - 1)] = 0;
+  }
+}

@@ -187,3 +187,21 @@ def test_halo_oracle_finds_generated_haloes():
     ind = r.cat.indcs[: r.cat.nclus][real]
     assert np.all(ind[:, 1] - ind[:, 0] + 1 == r.cat.dmpclus[: r.cat.nclus][real])
     assert len(np.unique(r.pph)) == len(r.pph)
+
+
+def test_mesh_base_counts_known_answer():
+    """CREATE_MESH base counts (grids.f:94-143) on four particles in a 4^3
+    grid of side 4: species weights, clamping, border zeroing."""
+    from types import SimpleNamespace
+    x = np.array([0.5, 0.6, -0.4, 9.0], np.float32)   # cells (3,3,3), (3,3,3), (2,3,3), clamped (4,3,3)
+    yz = np.array([0.5, 0.5, 0.5, 0.5], np.float32)
+    z0 = np.zeros(4, np.float32)
+    o = O.OracleBackend()
+    o.upload(SimpleNamespace(x=x, y=yz, z=yz, vx=z0, vy=z0, vz=z0, m=z0 + 1, id=np.arange(4, dtype=np.int32)))
+    c = o.mesh_base_counts(4, 1.0, 8, 0, [1, 2]).reshape(4, 4, 4)   # [kz, jy, ix]
+    assert c[2, 2, 2] == 1 + 8      # species 0 and species 1
+    assert c[2, 2, 1] == 8          # species 1
+    assert c[2, 2, 3] == 1          # past the ranges: species 0, clamped to IX = NX
+    assert c.sum() == 18
+    c = o.mesh_base_counts(4, 1.0, 8, 1, [1, 2]).reshape(4, 4, 4)
+    assert c[2, 2, 3] == 0 and c[2, 2, 2] == 9   # IX = NX is a border cell
