@@ -158,6 +158,23 @@ def layer_bench(iters=10, warmup=3):
             "fwd_adj_GBps": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4), "peak_source": src}
 
 
+def replica_config(cfg, rank):
+    """The snapshot recipe of one replica: the same sizes, seed + rank (the
+    ranks share nothing, so each runs the hot path on its own snapshot)."""
+    from asohf_b200 import synth
+    return synth.SnapshotConfig(**{**cfg.__dict__, "seed": cfg.seed + rank})
+
+
+def max_over_ranks(ms, world, dist, device):
+    """The slowest rank's step time (all ranks take this collective in the
+    same order); whole-job throughput is world * particles / this time."""
+    import torch
+    t = torch.tensor([float(ms)], device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -204,8 +221,7 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    cfg = synth.CONFIGS[args.config]
-    cfg = synth.SnapshotConfig(**{**cfg.__dict__, "seed": cfg.seed + rank})
+    cfg = replica_config(synth.CONFIGS[args.config], rank)
     snap = synth.generate_fast(cfg, device=f"cuda:{local}", keep_on_device=True)
     plan = driver.prepare(snap)
     with_subs = not args.no_subs
@@ -239,10 +255,7 @@ def main():
     kstats = b.a.kernel_stats()
     work = b.a.work_counters()
     b.a.set_profiling(False)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, dist, "cuda")
     n = cfg.n
     value = world * n / (ms_max * 1e-3)
 
@@ -269,10 +282,7 @@ def main():
         e1.record(st)
         torch.cuda.synchronize()
         ms_e2e = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / args.steps
-        t = torch.tensor([ms_e2e], device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+        ms_e2e = max_over_ranks(ms_e2e, world, dist, "cuda")
         ncat = re.cat.nclus
         cat_bytes = ncat * 4 * (45 + 2 * 20 + 3 + 3 + 6 + 2)
         h2d = n * 32 + cat_bytes  # particles; the catalogue windows go both ways
