@@ -46,6 +46,10 @@ void orc_momento(int nx, float dx, float *kkk);
 /* CREATE_MESH particle counts (grids.f:94-143, grids.f:341-380). */
 void orc_mesh_base_counts(int64_t n, const float *x, const float *y, const float *z, int nx, float dx,
                           int refine_thr, int bor, const int32_t *npart_esp, int32_t *cr0);
+/* VEINSGRID_REDUCED (grids.f:1771-2073) on one level's patches. */
+int orc_veinsgrid_reduced(int ir, float dx, float radx1, int npatch, const int32_t *pnx, const int32_t *pny,
+                          const int32_t *pnz, const float *prx, const float *pry, const float *prz, int max_nb,
+                          int32_t *cr01, int32_t *conta11);
 void orc_mesh_patch_counts(int64_t n, const float *x, const float *y, const float *z, int irpa, float dx,
                            int refine_thr, int boramr, const int32_t *npart_esp, int npatch,
                            const int32_t *pnx, const int32_t *pny, const int32_t *pnz, const float *prx,

@@ -274,6 +274,18 @@ class OracleBackend:
                                     *[P(a, _ip) for a in ai], *[P(a) for a in af], P(out, _ip))
         return out
 
+    def veinsgrid_reduced(self, ir, dx, radx1, pnx, pny, pnz, prx, pry, prz, max_nb, cr01, conta11=None):
+        """VEINSGRID_REDUCED (grids.f:1771-2073) on one level's patches; cr01
+        and conta11 ((npatch, NAMRX^3) int32) are modified in place."""
+        ai = [np.ascontiguousarray(a, np.int32) for a in (pnx, pny, pnz)]
+        af = [np.ascontiguousarray(a, np.float32) for a in (prx, pry, prz)]
+        assert cr01.dtype == np.int32 and cr01.flags.c_contiguous
+        rc = lib().orc_veinsgrid_reduced(C.c_int(ir), C.c_float(dx), C.c_float(radx1), C.c_int(ai[0].shape[0]),
+                                         *[P(a, _ip) for a in ai], *[P(a) for a in af], C.c_int(max_nb),
+                                         P(cr01, _ip), P(conta11, _ip) if conta11 is not None else None)
+        if rc:
+            raise RuntimeError("VEINSGRID_REDUCED: too many neighbours" if rc == -1 else "out of memory")
+
     def poisson_fft(self, u1, dx):
         return poisson_fft(u1, dx)
 

@@ -764,3 +764,119 @@ void orc_mesh_patch_counts(int64_t n, const float *x, const float *y, const floa
             o[((size_t)(kz - 1) * na + (jy - 1)) * na + (ix - 1)] = 0;
   }
 }
+
+
+/* One axis of VEINSGRID_REDUCED's overlap corners (grids.f:1965-2026, the X
+ * block; Y and Z are the same): the cells CORN1..CORN2 of patch I and
+ * CORNN1..CORNN2 of patch J that face each other.  INT truncates toward
+ * zero. */
+static void veins_axis(float r1, float r2, float rr1, float rr2, float dxpa, int n, int nn, int *c1, int *c2,
+                       int *cc1, int *cc2)
+{
+  if (rr1 >= r1 && rr2 <= r2) {
+    *c1 = (int)(((rr1 - r1) / dxpa) + 0.5f) + 1;
+    *c2 = (int)(((rr2 - r1) / dxpa) + 0.5f) + 1;
+    *cc1 = 1;
+    *cc2 = nn;
+  }
+  if (rr1 >= r1 && rr2 > r2) {
+    *c1 = (int)(((rr1 - r1) / dxpa) + 0.5f) + 1;
+    *c2 = n;
+    *cc1 = 1;
+    *cc2 = (int)(((r2 - rr1) / dxpa) + 0.5f) + 1;
+  }
+  if (rr2 <= r2 && rr1 < r1) {
+    *c1 = 1;
+    *c2 = (int)(((rr2 - r1) / dxpa) + 0.5f) + 1;
+    *cc1 = (int)(((r1 - rr1) / dxpa) + 0.5f) + 1;
+    *cc2 = nn;
+  }
+  if (rr1 < r1 && rr2 > r2) {
+    *c1 = 1;
+    *c2 = n;
+    *cc1 = (int)(((r1 - rr1) / dxpa) + 0.5f) + 1;
+    *cc2 = (int)(((r2 - rr1) / dxpa) + 0.5f) + 1;
+  }
+}
+
+/* VEINSGRID_REDUCED (grids.f:1771-2073) on the npatch patches of level ir
+ * (the slice LOW1..LOW2): neighbours are the other patches whose cell boxes
+ * on the level's grid (origin RXFIX = RADX(1) - DX/2 + DXPA/2) intersect;
+ * then, patch I in order and its neighbours J in order, when the overlap
+ * covers more than 0.1 of J, every cell of J facing a cell of I not yet
+ * marked is marked and its CR01 / CONTA11 zeroed.  Returns 0, or -1 when a
+ * patch has more than max_nb neighbours (the reference's STOP).  Cells
+ * outside the NAMRX^3 arrays are skipped. */
+int orc_veinsgrid_reduced(int ir, float dx, float radx1, int npatch, const int32_t *pnx, const int32_t *pny,
+                          const int32_t *pnz, const float *prx, const float *pry, const float *prz, int max_nb,
+                          int32_t *cr01, int32_t *conta11)
+{
+  const int na = ASOHF_NAMRX;
+  const size_t pc = (size_t)na * na * na;
+  const float dxpa = dx / powf(2.0f, (float)ir);
+  const float fix = radx1 - dx * 0.5f + 0.5f * dxpa;
+  int *g1 = malloc(sizeof(int) * 3 * (size_t)(npatch > 0 ? npatch : 1));
+  uint8_t *solap = calloc((size_t)(npatch > 0 ? npatch : 1), pc);
+  int *nb = malloc(sizeof(int) * (size_t)(npatch > 0 ? npatch : 1));
+  if (!g1 || !solap || !nb) { free(g1); free(solap); free(nb); return -2; }
+  const float *pr[3] = {prx, pry, prz};
+  const int32_t *pn[3] = {pnx, pny, pnz};
+  for (int i = 0; i < npatch; i++)
+    for (int a = 0; a < 3; a++)
+      g1[3 * i + a] = (int)(((pr[a][i] - 0.5f * dxpa - fix) / dxpa) + 0.5f) + 1;
+  int rc = 0;
+  for (int i = 0; i < npatch && rc == 0; i++) {
+    int nv = 0;
+    for (int j = 0; j < npatch; j++) {
+      if (j == i) continue;
+      int ok = 1;
+      for (int a = 0; a < 3; a++)
+        ok &= g1[3 * i + a] <= g1[3 * j + a] + pn[a][j] - 1 && g1[3 * j + a] <= g1[3 * i + a] + pn[a][i] - 1;
+      nv += ok;
+    }
+    if (nv > max_nb) rc = -1;
+  }
+  for (int i = 0; i < npatch && rc == 0; i++) {
+    float r1[3], r2[3];
+    for (int a = 0; a < 3; a++) {
+      r1[a] = pr[a][i] - 0.5f * dxpa;
+      r2[a] = pr[a][i] - 0.5f * dxpa + (float)(pn[a][i] - 1) * dxpa;
+    }
+    for (int j = 0; j < npatch; j++) {
+      if (j == i) continue;
+      int ok = 1;
+      for (int a = 0; a < 3; a++)
+        ok &= g1[3 * i + a] <= g1[3 * j + a] + pn[a][j] - 1 && g1[3 * j + a] <= g1[3 * i + a] + pn[a][i] - 1;
+      if (!ok) continue;
+      int c1[3], c2[3], cc1[3], cc2[3];
+      for (int a = 0; a < 3; a++) {
+        const float rr1 = pr[a][j] - 0.5f * dxpa;
+        const float rr2 = pr[a][j] - 0.5f * dxpa + (float)(pn[a][j] - 1) * dxpa;
+        c1[a] = c2[a] = cc1[a] = cc2[a] = 0;
+        veins_axis(r1[a], r2[a], rr1, rr2, dxpa, pn[a][i], pn[a][j], &c1[a], &c2[a], &cc1[a], &cc2[a]);
+      }
+      int prod = (cc2[2] - cc1[2] + 1) * (cc2[1] - cc1[1] + 1) * (cc2[0] - cc1[0] + 1);
+      float ov = fabsf((float)prod) / (float)pnx[j] / (float)pny[j] / (float)pnz[j];
+      if (!(ov > 0.1f)) continue;
+      for (int kk = cc1[2]; kk <= cc2[2]; kk++)
+        for (int jj = cc1[1]; jj <= cc2[1]; jj++)
+          for (int ii = cc1[0]; ii <= cc2[0]; ii++) {
+            const int ix = ii - cc1[0] + c1[0], jy = jj - cc1[1] + c1[1], kz = kk - cc1[2] + c1[2];
+            if (ii < 1 || ii > na || jj < 1 || jj > na || kk < 1 || kk > na || ix < 1 || ix > na || jy < 1 ||
+                jy > na || kz < 1 || kz > na)
+              continue;
+            const size_t qi = (size_t)i * pc + ((size_t)(kz - 1) * na + (jy - 1)) * na + (ix - 1);
+            const size_t qj = (size_t)j * pc + ((size_t)(kk - 1) * na + (jj - 1)) * na + (ii - 1);
+            if (solap[qi] == 0) {
+              solap[qj] = 1;
+              cr01[qj] = 0;
+              if (conta11) conta11[qj] = 0;
+            }
+          }
+    }
+  }
+  free(g1);
+  free(solap);
+  free(nb);
+  return rc;
+}

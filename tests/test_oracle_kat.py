@@ -205,3 +205,26 @@ def test_mesh_base_counts_known_answer():
     assert c.sum() == 18
     c = o.mesh_base_counts(4, 1.0, 8, 1, [1, 2]).reshape(4, 4, 4)
     assert c[2, 2, 3] == 0 and c[2, 2, 2] == 9   # IX = NX is a border cell
+
+
+def test_veinsgrid_reduced_known_answer():
+    """VEINSGRID_REDUCED (grids.f:1771-2073): two 8^3 patches of level 1
+    overlapping by half in x.  The first marks the half of the second that
+    faces it; the second then finds those cells marked and leaves the first
+    alone."""
+    na = 32
+    dx, radx1 = 1.0, -7.5                     # 16 base cells of side 1 from -8
+    n = np.array([8, 8], np.int32)
+    prx = np.array([-3.5, -1.5], np.float32)  # cell centres of level 0, 4 level-1 cells apart
+    pry = prz = np.array([-3.5, -3.5], np.float32)
+    cr = np.zeros((2, na, na, na), np.int32)   # [patch, kz, jy, ix]
+    cr[:, :8, :8, :8] = 1
+    c11 = cr.copy()
+    O.OracleBackend().veinsgrid_reduced(1, dx, radx1, n, n, n, prx, pry, prz, 100, cr.reshape(2, -1),
+                                        c11.reshape(2, -1))
+    assert cr[0, :8, :8, :8].all()              # the first patch is untouched
+    assert not cr[1, :8, :8, :4].any()          # the half of the second facing it is zeroed
+    assert cr[1, :8, :8, 4:8].all()
+    assert np.array_equal(cr, c11)
+    with pytest.raises(RuntimeError):            # more neighbours than allowed
+        O.OracleBackend().veinsgrid_reduced(1, dx, radx1, n, n, n, prx, pry, prz, 0, cr.reshape(2, -1))
