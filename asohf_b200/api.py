@@ -266,6 +266,17 @@ class Asohf:
             _ptr(out), C.c_int(int(_is_torch(out)))), "CREATE_MESH patch counts")
         return out
 
+    def veinsgrid_reduced(self, ir, dx, radx1, pnx, pny, pnz, prx, pry, prz, max_neighbours, cr01, conta11=None):
+        """VEINSGRID_REDUCED (grids.f:1771-2073) on one level's patches; cr01 and
+        conta11 ((npatch, NAMRX^3) int32, numpy or CUDA tensors) in place."""
+        ai = [np.ascontiguousarray(a, np.int32) for a in (pnx, pny, pnz)]
+        af = [np.ascontiguousarray(a, np.float32) for a in (prx, pry, prz)]
+        _check(self.L.asohf_veinsgrid_reduced(
+            self.h, C.c_int(ir), C.c_float(dx), C.c_float(radx1), C.c_int(int(ai[0].shape[0])),
+            *[a.ctypes.data_as(C.c_void_p) for a in ai], *[a.ctypes.data_as(C.c_void_p) for a in af],
+            C.c_int(max_neighbours), _ptr(cr01), _ptr(conta11) if conta11 is not None else None,
+            C.c_int(int(_is_torch(cr01)))), "VEINSGRID_REDUCED")
+
     def poisson_fft(self, nx, dx, rho, pot, batch=1):
         """MOMENTO + POFFT3D (poisson.f:98-249)."""
         _check(self.L.asohf_poisson_fft(self.h, C.c_int(nx), C.c_float(dx), C.c_int(batch),

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -1669,6 +1670,233 @@ extern "C" int asohf_mesh_patch_counts(asohf_ctx* c, int nx, float lado0, float 
   ktime_end(c, kt_);
   ASOHF_CUDA(cudaGetLastError());
   if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(cr01, d, outb, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  return ASOHF_OK;
+}
+
+// ------------------------------------------------------------ VEINSGRID_REDUCED
+// grids.f:1771-2073.  Patch I (in order) marks the cells of each neighbour J
+// that face an unmarked cell of I; a row reads only I's marks and writes
+// only its neighbours', and the neighbour relation (intersecting cell boxes
+// on the level's grid) is symmetric.  So rows whose patches do not
+// intersect commute, and the rows are replayed in waves: a row's wave is
+// one past the latest wave of its lower-index neighbours, and one launch
+// takes a wave with one CTA per row.  The result equals the sequential one.
+
+__device__ __forceinline__ int veins_int(float v) { return (int)__fadd_rn(v, 0.5f); }  // INT(v+0.5)
+
+// Lower cell of each patch on the level's grid (IG1, JG1, KG1).
+__global__ void k_veins_box(const int32_t* __restrict__ pn, const float* __restrict__ pr, int np, float dxpa,
+                            float fix, int32_t* __restrict__ g1) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 3 * np) return;
+  const float r1 = __fsub_rn(pr[q], __fmul_rn(0.5f, dxpa));
+  g1[q] = veins_int(__fdiv_rn(__fsub_rn(r1, fix), dxpa)) + 1;
+}
+
+__device__ __forceinline__ bool veins_meet(const int32_t* g1, const int32_t* pn, int np, int i, int j) {
+  bool ok = true;
+  for (int a = 0; a < 3; a++) {
+    const int gi = g1[a * np + i], gj = g1[a * np + j];
+    ok = ok && gi <= gj + pn[a * np + j] - 1 && gj <= gi + pn[a * np + i] - 1;
+  }
+  return ok;
+}
+
+// Neighbours of each patch, in index order: counts (fill == nullptr) or the list.
+__global__ void k_veins_neighbours(const int32_t* __restrict__ g1, const int32_t* __restrict__ pn, int np,
+                                   int32_t* __restrict__ cnt, const int32_t* __restrict__ off,
+                                   int32_t* __restrict__ fill) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  int k = 0;
+  for (int j = 0; j < np; j++) {
+    if (j == i || !veins_meet(g1, pn, np, i, j)) continue;
+    if (fill) fill[off[i] + k] = j;
+    k++;
+  }
+  if (!fill) cnt[i] = k;
+}
+
+// The overlap corners of one axis (the four cases of grids.f:1965-2026).
+__device__ __forceinline__ void veins_axis_d(float r1, float r2, float rr1, float rr2, float dxpa, int n, int nn,
+                                             int* c1, int* c2, int* cc1, int* cc2) {
+  if (rr1 >= r1 && rr2 <= r2) {
+    *c1 = veins_int(__fdiv_rn(__fsub_rn(rr1, r1), dxpa)) + 1;
+    *c2 = veins_int(__fdiv_rn(__fsub_rn(rr2, r1), dxpa)) + 1;
+    *cc1 = 1;
+    *cc2 = nn;
+  }
+  if (rr1 >= r1 && rr2 > r2) {
+    *c1 = veins_int(__fdiv_rn(__fsub_rn(rr1, r1), dxpa)) + 1;
+    *c2 = n;
+    *cc1 = 1;
+    *cc2 = veins_int(__fdiv_rn(__fsub_rn(r2, rr1), dxpa)) + 1;
+  }
+  if (rr2 <= r2 && rr1 < r1) {
+    *c1 = 1;
+    *c2 = veins_int(__fdiv_rn(__fsub_rn(rr2, r1), dxpa)) + 1;
+    *cc1 = veins_int(__fdiv_rn(__fsub_rn(r1, rr1), dxpa)) + 1;
+    *cc2 = nn;
+  }
+  if (rr1 < r1 && rr2 > r2) {
+    *c1 = 1;
+    *c2 = n;
+    *cc1 = veins_int(__fdiv_rn(__fsub_rn(r1, rr1), dxpa)) + 1;
+    *cc2 = veins_int(__fdiv_rn(__fsub_rn(r2, rr1), dxpa)) + 1;
+  }
+}
+
+// One CTA per row of the wave: patch I against each neighbour J.
+__global__ void __launch_bounds__(256) k_veins_rows(const int32_t* __restrict__ rows, const int32_t* __restrict__ off,
+                                                    const int32_t* __restrict__ nb, const int32_t* __restrict__ pn,
+                                                    const float* __restrict__ pr, int np, float dxpa,
+                                                    uint8_t* __restrict__ solap, int32_t* __restrict__ cr01,
+                                                    int32_t* __restrict__ conta11) {
+  const int i = rows[blockIdx.x];
+  const size_t pc = (size_t)NA * NA * NA;
+  float r1[3], r2[3];
+  int n[3];
+  for (int a = 0; a < 3; a++) {
+    n[a] = pn[a * np + i];
+    r1[a] = __fsub_rn(pr[a * np + i], __fmul_rn(0.5f, dxpa));
+    r2[a] = __fadd_rn(r1[a], __fmul_rn((float)(n[a] - 1), dxpa));
+  }
+  for (int k = off[i]; k < off[i + 1]; k++) {
+    const int j = nb[k];
+    int c1[3], c2[3], cc1[3], cc2[3], e[3];
+    for (int a = 0; a < 3; a++) {
+      const int nn = pn[a * np + j];
+      const float rr1 = __fsub_rn(pr[a * np + j], __fmul_rn(0.5f, dxpa));
+      const float rr2 = __fadd_rn(rr1, __fmul_rn((float)(nn - 1), dxpa));
+      c1[a] = c2[a] = cc1[a] = cc2[a] = 0;
+      veins_axis_d(r1[a], r2[a], rr1, rr2, dxpa, n[a], nn, &c1[a], &c2[a], &cc1[a], &cc2[a]);
+      e[a] = cc2[a] - cc1[a] + 1;
+    }
+    const int prod = e[2] * e[1] * e[0];
+    const float ov = __fdiv_rn(__fdiv_rn(__fdiv_rn(fabsf((float)prod), (float)pn[j]), (float)pn[np + j]),
+                               (float)pn[2 * np + j]);
+    if (!(ov > 0.1f) || e[0] <= 0 || e[1] <= 0 || e[2] <= 0) continue;
+    const int ncell = e[0] * e[1] * e[2];
+    for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
+      const int ii = cc1[0] + q % e[0], jj = cc1[1] + (q / e[0]) % e[1], kk = cc1[2] + q / (e[0] * e[1]);
+      const int ix = ii - cc1[0] + c1[0], jy = jj - cc1[1] + c1[1], kz = kk - cc1[2] + c1[2];
+      if (ii < 1 || ii > NA || jj < 1 || jj > NA || kk < 1 || kk > NA || ix < 1 || ix > NA || jy < 1 || jy > NA ||
+          kz < 1 || kz > NA)
+        continue;  // outside the NAMRX^3 arrays
+      const size_t qi = (size_t)i * pc + ((size_t)(kz - 1) * NA + (jy - 1)) * NA + (ix - 1);
+      const size_t qj = (size_t)j * pc + ((size_t)(kk - 1) * NA + (jj - 1)) * NA + (ii - 1);
+      if (solap[qi] == 0) {
+        solap[qj] = 1;
+        cr01[qj] = 0;
+        if (conta11) conta11[qj] = 0;
+      }
+    }
+  }
+}
+
+extern "C" int asohf_veinsgrid_reduced(asohf_ctx* c, int ir, float dx, float radx1, int npatch,
+                                       const int32_t* patchnx, const int32_t* patchny, const int32_t* patchnz,
+                                       const float* patchrx, const float* patchry, const float* patchrz,
+                                       int max_neighbours, int32_t* cr01, int32_t* conta11, int on_device) {
+  if (!c || ir < 1 || npatch < 0 || max_neighbours < 0 ||
+      (npatch > 0 && (!patchnx || !patchny || !patchnz || !patchrx || !patchry || !patchrz || !cr01)))
+    return ASOHF_ERR_INVALID;
+  for (int q = 0; q < npatch; q++)
+    if (patchnx[q] < 1 || patchnx[q] > NA || patchny[q] < 1 || patchny[q] > NA || patchnz[q] < 1 || patchnz[q] > NA)
+      return ASOHF_ERR_INVALID;
+  if (npatch == 0) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  arena_reset(c);
+  const int np = npatch;
+  const size_t pc = (size_t)NA * NA * NA;
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, (int32_t*)nullptr, (int32_t*)nullptr, np + 1);
+  const size_t host_b = on_device ? 0 : 4 * pc * (size_t)np * (conta11 ? 2 : 1);
+  ASOHF_CHECK(arena_reserve(c, host_b + pc * (size_t)np + 48 * (size_t)np + tb + 16 * 256 + 4096));
+  int32_t* pn = (int32_t*)arena_alloc(c, 12 * (size_t)np);
+  float* pr = (float*)arena_alloc(c, 12 * (size_t)np);
+  int32_t* g1 = (int32_t*)arena_alloc(c, 12 * (size_t)np);
+  int32_t* cnt = (int32_t*)arena_alloc(c, 4 * (size_t)np + 4);
+  int32_t* off = (int32_t*)arena_alloc(c, 4 * (size_t)np + 4);
+  int32_t* rows = (int32_t*)arena_alloc(c, 4 * (size_t)np);
+  void* tmp = arena_alloc(c, tb);
+  uint8_t* solap = (uint8_t*)arena_alloc(c, pc * (size_t)np);
+  int32_t* dcr = on_device ? cr01 : (int32_t*)arena_alloc(c, 4 * pc * (size_t)np);
+  int32_t* dct = (!conta11 || on_device) ? conta11 : (int32_t*)arena_alloc(c, 4 * pc * (size_t)np);
+  if (!pn || !pr || !g1 || !cnt || !off || !rows || !tmp || !solap || !dcr || (conta11 && !dct))
+    return ASOHF_ERR_CAPACITY;
+  const int32_t* hn[3] = {patchnx, patchny, patchnz};
+  const float* hr[3] = {patchrx, patchry, patchrz};
+  for (int a = 0; a < 3; a++) {
+    ASOHF_CUDA(cudaMemcpyAsync(pn + (size_t)a * np, hn[a], 4 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(pr + (size_t)a * np, hr[a], 4 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+  }
+  if (!on_device) {
+    ASOHF_CUDA(cudaMemcpyAsync(dcr, cr01, 4 * pc * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+    if (conta11) ASOHF_CUDA(cudaMemcpyAsync(dct, conta11, 4 * pc * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+  }
+  ASOHF_CUDA(cudaMemsetAsync(solap, 0, pc * (size_t)np, c->stream));
+  ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (size_t)np + 4, c->stream));
+  const float dxpa = ldexpf(dx, -ir);                       // DX/(2.**IR)
+  const float fix = radx1 - dx * 0.5f + 0.5f * dxpa;        // RXFIX
+  int kt_ = ktime_begin(c, "veinsgrid_reduced");
+  k_veins_box<<<(3 * np + 255) / 256, 256, 0, c->stream>>>(pn, pr, np, dxpa, fix, g1);
+  k_veins_neighbours<<<(np + 127) / 128, 128, 0, c->stream>>>(g1, pn, np, cnt, nullptr, nullptr);
+  ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, np + 1, c->stream));
+  c->launches += 3;
+  std::vector<int32_t> hoff(np + 1);
+  ASOHF_CUDA(cudaMemcpyAsync(hoff.data(), off, 4 * (size_t)(np + 1), cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  const int ne = hoff[np];
+  int maxnv = 0;
+  for (int i = 0; i < np; i++) maxnv = std::max(maxnv, hoff[i + 1] - hoff[i]);
+  if (maxnv > max_neighbours) {
+    ktime_end(c, kt_);
+    return ASOHF_ERR_CAPACITY;  // the reference stops: more neighbours than NPALEV2
+  }
+  int32_t* nb = nullptr;
+  if (ne > 0) {
+    // the list lives in the segment buffer (the arena is sized before the count is known)
+    ASOHF_CHECK(seg_reserve(c, 4 * (size_t)ne + 256));
+    nb = (int32_t*)seg_alloc(c, 4 * (size_t)ne);
+    if (!nb) return ASOHF_ERR_CAPACITY;
+    k_veins_neighbours<<<(np + 127) / 128, 128, 0, c->stream>>>(g1, pn, np, nullptr, off, nb);
+    c->launches++;
+  }
+  std::vector<int32_t> hnb(ne > 0 ? ne : 1);
+  if (ne > 0) ASOHF_CUDA(cudaMemcpyAsync(hnb.data(), nb, 4 * (size_t)ne, cudaMemcpyDeviceToHost, c->stream));
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  // waves: one past the latest wave of the lower-index neighbours
+  std::vector<int32_t> wave(np, 0);
+  int nwave = 0;
+  for (int i = 0; i < np; i++) {
+    int w = 0;
+    for (int k = hoff[i]; k < hoff[i + 1]; k++)
+      if (hnb[k] < i) w = std::max(w, wave[hnb[k]] + 1);
+    wave[i] = w;
+    nwave = std::max(nwave, w + 1);
+  }
+  std::vector<int32_t> wstart(nwave + 1, 0), horder(np);
+  for (int i = 0; i < np; i++) wstart[wave[i] + 1]++;
+  for (int w = 0; w < nwave; w++) wstart[w + 1] += wstart[w];
+  {
+    std::vector<int32_t> fillp(wstart.begin(), wstart.end() - 1);
+    for (int i = 0; i < np; i++) horder[fillp[wave[i]]++] = i;
+  }
+  ASOHF_CUDA(cudaMemcpyAsync(rows, horder.data(), 4 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+  for (int w = 0; w < nwave; w++) {
+    const int nr = wstart[w + 1] - wstart[w];
+    if (nr <= 0) continue;
+    k_veins_rows<<<nr, 256, 0, c->stream>>>(rows + wstart[w], off, nb, pn, pr, np, dxpa, solap, dcr, dct);
+    c->launches++;
+  }
+  ktime_end(c, kt_);
+  ASOHF_CUDA(cudaGetLastError());
+  if (!on_device) {
+    ASOHF_CUDA(cudaMemcpyAsync(cr01, dcr, 4 * pc * (size_t)np, cudaMemcpyDeviceToHost, c->stream));
+    if (conta11) ASOHF_CUDA(cudaMemcpyAsync(conta11, dct, 4 * pc * (size_t)np, cudaMemcpyDeviceToHost, c->stream));
+  }
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return ASOHF_OK;
 }

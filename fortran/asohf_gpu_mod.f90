@@ -201,6 +201,16 @@
          INTEGER(C_INT) :: NPART_ESP(*), PNX(*), PNY(*), PNZ(*), CR01(*)
          REAL(C_FLOAT) :: PRX(*), PRY(*), PRZ(*)
         END FUNCTION
+        INTEGER(C_INT) FUNCTION ASOHF_VEINSGRID_REDUCED_C(C, IR, DX,
+     &   RADX1, NPATCH, PNX, PNY, PNZ, PRX, PRY, PRZ, MAXNB, CR01,
+     &   CONTA11, ONDEV) BIND(C, NAME='asohf_veinsgrid_reduced')
+         IMPORT :: C_INT, C_PTR, C_FLOAT
+         TYPE(C_PTR), VALUE :: C
+         INTEGER(C_INT), VALUE :: IR, NPATCH, MAXNB, ONDEV
+         REAL(C_FLOAT), VALUE :: DX, RADX1
+         INTEGER(C_INT) :: PNX(*), PNY(*), PNZ(*), CR01(*), CONTA11(*)
+         REAL(C_FLOAT) :: PRX(*), PRY(*), PRZ(*)
+        END FUNCTION
        END INTERFACE
 
       CONTAINS

@@ -168,6 +168,21 @@ int asohf_mesh_patch_counts(asohf_ctx *ctx, int nx, float lado0, float dx, int i
                             const int32_t *patchnz, const float *patchrx, const float *patchry,
                             const float *patchrz, int32_t *cr01, int on_device);
 
+/* VEINSGRID_REDUCED (grids.f:1771-2073), called by CREATE_MESH after the
+ * patch counts of level ir: on the npatch patches of the level (host arrays,
+ * the slice LOW1..LOW2), patch I in order marks every cell of each
+ * neighbour J (intersecting cell boxes on the level's grid, origin RADX(1) -
+ * DX/2 + DXPA/2 with radx1 = RADX(1)) that faces an unmarked cell of I,
+ * when the overlap covers more than 0.1 of J, and zeroes CR01 and CONTA11
+ * there (NAMRX^3 int32 per patch, IX fastest; conta11 may be NULL).  The
+ * sequential order is reproduced exactly.  ASOHF_ERR_CAPACITY when a patch
+ * has more than max_neighbours neighbours (NPALEV2; the reference stops).
+ * Cells outside the NAMRX^3 arrays are skipped. */
+int asohf_veinsgrid_reduced(asohf_ctx *ctx, int ir, float dx, float radx1, int npatch, const int32_t *patchnx,
+                            const int32_t *patchny, const int32_t *patchnz, const float *patchrx,
+                            const float *patchry, const float *patchrz, int max_neighbours, int32_t *cr01,
+                            int32_t *conta11, int on_device);
+
 /* CHECK_RUBISH (haloes_particles.f:259-318), called after each level's
  * refinement (asohf.f:672-673): a halo of the window low1..low2 (1-based,
  * inclusive) is removed (REALCLUS=0) when a live halo of a lower level lies
