@@ -35,3 +35,35 @@ def test_status_strings():
     L = api.load()
     for code in range(9):
         assert L.asohf_strerror(code).decode()
+
+
+def test_no_device_fails_loudly():
+    """Without a GPU the library refuses to start (ASOHF_ERR_NO_DEVICE): it
+    has no CPU fallback."""
+    L = api.load()
+    ctx = ctypes.c_void_p()
+    rc = L.asohf_create(0, ctypes.byref(ctx))
+    import torch
+    if torch.cuda.is_available():
+        assert rc == 0
+        L.asohf_destroy(ctx)
+    else:
+        assert rc == 7  # ASOHF_ERR_NO_DEVICE
+        assert "device" in L.asohf_strerror(rc).decode().lower()
+
+
+def test_cleaning_and_mesh_entry_points_reject_a_null_context():
+    """Argument checks of the catalogue cleaning and mesh entry points come
+    before any device work (ASOHF_ERR_INVALID = 1)."""
+    L = api.load()
+    p = ctypes.c_void_p()
+    i32 = ctypes.c_int32()
+    nh = (ctypes.c_int32 * 2)(1, 1)
+    assert L.asohf_check_rubish(None, p, 0, 1, 1, 0, ctypes.byref(i32)) == 1
+    assert L.asohf_accidental_substructure(None, p, 0, 0, ctypes.byref(i32)) == 1
+    assert L.asohf_overlapping(None, p, 1, nh, ctypes.c_float(0.2), 0, ctypes.byref(i32)) == 1
+    assert L.asohf_mesh_base_counts(None, 8, ctypes.c_float(1.0), 8, 1, nh, p, 0) == 1
+    assert L.asohf_mesh_patch_counts(None, 8, ctypes.c_float(8.0), ctypes.c_float(1.0), 1, 8, 1, nh, 0,
+                                     None, None, None, None, None, None, None, 0) == 1
+    assert L.asohf_veinsgrid_reduced(None, 1, ctypes.c_float(1.0), ctypes.c_float(-3.5), 0, None, None, None,
+                                     None, None, None, 100, None, None, 0) == 1
