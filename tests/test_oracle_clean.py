@@ -55,3 +55,15 @@ def test_overlapping_known_answers():
     c = cat_of(rows)
     O.OracleBackend().overlapping(c, 1, [2, 4], 0.3)   # above the lens fraction: row 4 kept
     assert list(c.realclus[:6]) == [-1, -1, 0, -1, 0, -1]
+
+
+def test_overlapping_row_flag_read_once():
+    """OVERLAPPING reads the row halo's REALCLUS once per row (BASINT,
+    haloes_grids.f:106-107): a row halo removed by its first partner still
+    removes its later partners."""
+    rows = [(0, 0.0, 0.0, 0.0, 1.0, 1e12, 100.0, -1),   # I: radius 1
+            (0, 0.1, 0.0, 0.0, 3.0, 1e12, 100.0, -1),   # contains I, larger, same level: I removed
+            (0, -0.2, 0.0, 0.0, 0.3, 1e12, 100.0, -1)]  # inside I: removed by I although I is gone
+    c = cat_of(rows)
+    O.OracleBackend().overlapping(c, 0, [3], 0.2)
+    assert list(c.realclus[:3]) == [0, -1, 0]
