@@ -216,6 +216,20 @@ class OracleBackend:
         cc = cat.as_c()
         return lib().orc_accidental_substructure(C.byref(cc), C.c_int(cat.nclus))
 
+    def halofind_grid_base(self, nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low, cat):
+        """HALOFIND_GRID at the base level for a run without AMR levels
+        (haloes_grids.f:287-582): fills cat, returns NHALLEV(0)."""
+        u = np.ascontiguousarray(u1, np.float32).reshape(-1)
+        r = np.ascontiguousarray(radx, np.float32)
+        cc = cat.as_c()
+        rc = lib().orc_halofind_grid_base(C.c_int(nx), C.c_float(dx), P(u), P(r), C.c_float(contrastec),
+                                          C.c_float(rote), C.c_float(rete), C.c_float(rodo), C.c_float(re0),
+                                          C.c_float(bound), C.c_float(vol_solap_low), C.byref(cc))
+        cat.nclus = cc.nclus
+        if rc < 0:
+            raise RuntimeError("HALOFIND_GRID: growing not converged" if rc == -1 else "catalogue full")
+        return rc
+
     def overlapping(self, cat, ir, nhallev, vol_solap_low):
         """OVERLAPPING at level ir; nhallev[l] = haloes found at level l."""
         lowh3 = int(sum(nhallev[:ir])) + 1

@@ -1311,3 +1311,150 @@ int orc_substructure_particles(const orc_store *st, const asohf_consts *k,
   free(ids);
   return rc ? rc : rc2;
 }
+
+
+/* HALOFIND_GRID at the base level (haloes_grids.f:287-582) for a run without
+ * AMR levels (NL = 0: no RECENTER_DENSITY_PEAK, no duplicate test).  U1
+ * (nx^3, IX fastest) is rho/rho_B; radx holds RADX(0..NX+1).  Peaks: cells
+ * at least BOR=1 from the faces with U1 >= CONTRASTEC/6 that exceed their
+ * six neighbours, taken in decreasing density (SORT_CELLS: ARGSORT of
+ * 1/U1).  A peak not yet inside a halo (CONTA = 1) starts one and grows it
+ * in spherical shells (R_EXT = 0.8 DX, then MAX(R_EXT + 0.2 DX, 1.05
+ * R_EXT)) while its mean density exceeds CONTRASTEC*ROTE, zeroing CONTA
+ * over its cells.  The shell sums are the sequential (K, J, I) order of the
+ * reference's OpenMP reductions.  As in the reference, the centre-of-mass
+ * numerators restart each shell from the box bound held in the same
+ * variable (BASX = XCEN + R_EXT) while the denominator BASDELTA runs over
+ * all shells.  OVERLAPPING (vol_solap_low) follows.  Returns the haloes
+ * appended (NHALLEV(0)), -1 when a halo grows past BOUND (the reference
+ * stops), -2 when the catalogue is full. */
+int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx, float contrastec, float rote,
+                           float rete, float rodo, float re0, float bound, float vol_solap_low,
+                           asohf_catalogue *cat)
+{
+  const int bor = 1;
+  const float esp = 0.2f * dx, esp_log = 1.05f;
+  const float peak_thr = contrastec / 6.0f;
+  const size_t g = (size_t)nx * nx * nx;
+#define U(i, j, k) u1[((size_t)((k) - 1) * nx + ((j) - 1)) * nx + ((i) - 1)]
+  int32_t *conta = (int32_t *)calloc(g, sizeof(int32_t));
+  if (!conta) return -2;
+#define CONTA(i, j, k) conta[((size_t)((k) - 1) * nx + ((j) - 1)) * nx + ((i) - 1)]
+  for (int k = 1 + bor; k <= nx - bor; k++)
+    for (int j = 1 + bor; j <= nx - bor; j++)
+      for (int i = 1 + bor; i <= nx - bor; i++) CONTA(i, j, k) = 1;
+  /* candidates in (KZ, JY, IX) order */
+  int64_t cap = 1024, ncand = 0;
+  float *ddd = malloc(sizeof(float) * cap);
+  int *dx3 = malloc(sizeof(int) * 3 * cap);
+  for (int k = 1 + bor; k <= nx - bor; k++)
+    for (int j = 1 + bor; j <= nx - bor; j++)
+      for (int i = 1 + bor; i <= nx - bor; i++) {
+        const float b = U(i, j, k);
+        if (!(b >= peak_thr)) continue;
+        if (!(U(i + 1, j, k) - b < 0.0f)) continue;
+        if (!(U(i, j + 1, k) - b < 0.0f)) continue;
+        if (!(U(i, j, k + 1) - b < 0.0f)) continue;
+        if (!(b - U(i - 1, j, k) > 0.0f)) continue;
+        if (!(b - U(i, j - 1, k) > 0.0f)) continue;
+        if (!(b - U(i, j, k - 1) > 0.0f)) continue;
+        if (ncand == cap) {
+          cap *= 2;
+          ddd = realloc(ddd, sizeof(float) * cap);
+          dx3 = realloc(dx3, sizeof(int) * 3 * cap);
+        }
+        ddd[ncand] = b;
+        dx3[3 * ncand] = i;
+        dx3[3 * ncand + 1] = j;
+        dx3[3 * ncand + 2] = k;
+        ncand++;
+      }
+  /* SORT_CELLS: ARGSORT of 1/DDD */
+  float *inv = calloc((size_t)(ncand > 0 ? ncand : 1), sizeof(float));
+  int64_t *order = malloc(sizeof(int64_t) * (ncand > 0 ? ncand : 1));
+  for (int64_t q = 0; q < ncand; q++) inv[q] = 1.0f / ddd[q];
+  orc_argsort(ncand, inv, order);
+  cat->nclus = 0;  /* IF (IR.EQ.0) NCLUS=0 */
+  int rc = 0, added = 0;
+  const float volcell = dx * dx * dx;
+  for (int64_t l = 0; l < ncand && rc == 0; l++) {
+    const int64_t q = order[l] - 1;
+    const int ic = dx3[3 * q], jc = dx3[3 * q + 1], kc = dx3[3 * q + 2];
+    if (CONTA(ic, jc, kc) != 1) continue;
+    if (cat->nclus >= cat->capacity) { rc = -2; break; }
+    const int h = cat->nclus++;
+    added++;
+    cat->realclus[h] = -1;
+    cat->levhal[h] = 0;
+    cat->patchclus[h] = 0;
+    const float xc = radx[ic], yc = radx[jc], zc = radx[kc];
+    cat->clusrx[h] = xc;
+    cat->clusry[h] = yc;
+    cat->clusrz[h] = zc;
+    float basx = 0.0f, basy = 0.0f, basz = 0.0f, basdelta = 0.0f, basmass = 0.0f, basvol = 0.0f;
+    float r_int = 0.0f, r_ext = 0.8f * dx;
+    float delta = 10.0f * contrastec * rote;
+    int iter = 0;
+    while (delta > contrastec * rote) {
+      iter++;
+      if (iter > 1) {
+        if (r_ext <= bound) {
+          r_int = r_ext;
+          const float a = r_ext + esp, b = r_ext * esp_log;
+          r_ext = a > b ? a : b;
+        } else {
+          rc = -1;
+          break;
+        }
+      }
+      int lo[3], hi[3];
+      const float c3[3] = {xc, yc, zc};
+      for (int a = 0; a < 3; a++) {
+        float bb = c3[a] - r_ext;
+        lo[a] = (int)(((bb - radx[1]) / dx) + 0.5f) + 1;
+        if (lo[a] < 1) lo[a] = 1;
+        bb = c3[a] + r_ext;
+        hi[a] = (int)(((bb - radx[1]) / dx) + 0.5f) + 1;
+        if (hi[a] > nx) hi[a] = nx;
+      }
+      /* BASX..BASZ hold the upper box bounds when the shell sums start */
+      basx = xc + r_ext;
+      basy = yc + r_ext;
+      basz = zc + r_ext;
+      float shell = 0.0f;
+      for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+          for (int i = lo[0]; i <= hi[0]; i++) {
+            const float ddx = radx[i] - xc, ddy = radx[j] - yc, ddz = radx[k] - zc;
+            const float aa = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
+            if (!(aa >= r_int && aa < r_ext)) continue;
+            CONTA(i, j, k) = 0;
+            basvol = basvol + volcell;
+            const float b = U(i, j, k) * volcell;
+            shell = shell + b;
+            basx = basx + radx[i] * b;
+            basy = basy + radx[j] * b;
+            basz = basz + radx[k] * b;
+            basdelta = basdelta + b;
+          }
+      basmass = basmass + shell * rodo * (re0 * re0 * re0);
+      if (basvol > 0.0f) delta = basmass / (basvol * (rete * rete * rete));
+    }
+    cat->radio[h] = r_ext;
+    cat->masa[h] = basmass;
+    cat->clusrxcm[h] = basx / basdelta;
+    cat->clusrycm[h] = basy / basdelta;
+    cat->clusrzcm[h] = basz / basdelta;
+  }
+  free(ddd);
+  free(dx3);
+  free(inv);
+  free(order);
+  free(conta);
+#undef U
+#undef CONTA
+  if (rc) return rc;
+  /* OVERLAPPING at IR = 0: LOWH3 = 1, LOWH2 = NHALLEV(0) */
+  orc_overlapping(cat, 1, cat->nclus, vol_solap_low);
+  return added;
+}

@@ -228,3 +228,38 @@ def test_veinsgrid_reduced_known_answer():
     assert np.array_equal(cr, c11)
     with pytest.raises(RuntimeError):            # more neighbours than allowed
         O.OracleBackend().veinsgrid_reduced(1, dx, radx1, n, n, n, prx, pry, prz, 0, cr.reshape(2, -1))
+
+
+def _tophat_field(nx, spheres):
+    """rho/rho_B = 1 with top-hat spheres (centre cell, radius in cells,
+    value) whose centre cell is raised by 10 % (a strict peak)."""
+    u = np.ones((nx, nx, nx), np.float32)          # [kz, jy, ix]
+    k, j, i = np.meshgrid(np.arange(nx), np.arange(nx), np.arange(nx), indexing="ij")
+    for (ci, cj, ck), r, v in spheres:
+        inside = (i - ci) ** 2 + (j - cj) ** 2 + (k - ck) ** 2 <= r * r
+        u[inside] = v
+        u[ck, cj, ci] = 1.1 * v
+    return u
+
+
+def test_halofind_grid_base_known_answer():
+    """HALOFIND_GRID base level (haloes_grids.f:287-582, no AMR levels): two
+    top-hat overdensities give two haloes, the denser first, centred on the
+    peak cells; each grows until its mean density falls below CONTRASTEC
+    (1 + A (R0/R)^3 = CONTRASTEC gives R = R0 (A/(CONTRASTEC-1))^(1/3))."""
+    nx, lado0 = 48, 48.0
+    radx, dx = grid.malla(nx, lado0)
+    spheres = [((12, 14, 20), 3.0, 400.0), ((34, 30, 26), 4.0, 300.0)]
+    u = _tophat_field(nx, spheres)
+    cat = abi.Catalogue(64)
+    contrastec, rodo, re0 = 200.0, 1.0, 1.0
+    n = O.OracleBackend().halofind_grid_base(nx, float(dx), u, radx, contrastec, rodo, re0, rodo, re0,
+                                              10.0, 0.2, cat)
+    assert n == 2 and cat.nclus == 2
+    assert list(cat.realclus[:2]) == [-1, -1] and list(cat.levhal[:2]) == [0, 0]
+    for h, ((ci, cj, ck), r0, a) in enumerate(spheres):   # denser sphere first
+        assert (cat.clusrx[h], cat.clusry[h], cat.clusrz[h]) == (radx[ci + 1], radx[cj + 1], radx[ck + 1])
+        r_pred = r0 * dx * (a / (contrastec - 1.0)) ** (1.0 / 3.0)
+        assert 0.85 * r_pred < cat.radio[h] < 1.2 * r_pred
+        # mass: the cells inside the final radius, rho_B = 1
+        assert cat.masa[h] > a * (4.0 / 3.0) * math.pi * (0.8 * r0) ** 3
