@@ -85,10 +85,10 @@ int orc_overlapping(asohf_catalogue *cat, int lowh3, int lowh2, float vol_solap_
  * (REALCLUS=-1) lying wholly inside a confirmed halo of a lower level is
  * removed.  Returns the number removed. */
 int orc_accidental_substructure(asohf_catalogue *cat, int nclus);
-/* HALOFIND_GRID at the base level without AMR levels (haloes_grids.f:287-582). */
+/* HALOFIND_GRID at the base level (haloes_grids.f:287-582); mesh/u11 may be NULL (no AMR levels). */
 int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx, float contrastec, float rote,
                            float rete, float rodo, float re0, float bound, float vol_solap_low,
-                           asohf_catalogue *cat);
+                           const asohf_mesh *mesh, const float *u11, asohf_catalogue *cat);
 /* HALOFIND_PARTICLES for haloes low1..low2 (Fortran 1-based, inclusive).
  * The bound-particle ID stream is written to pph (capacity pph_cap) and the
  * total used length returned in *pph_len.  Returns a status code. */

@@ -216,15 +216,21 @@ class OracleBackend:
         cc = cat.as_c()
         return lib().orc_accidental_substructure(C.byref(cc), C.c_int(cat.nclus))
 
-    def halofind_grid_base(self, nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low, cat):
-        """HALOFIND_GRID at the base level for a run without AMR levels
-        (haloes_grids.f:287-582): fills cat, returns NHALLEV(0)."""
+    def halofind_grid_base(self, nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low, cat,
+                           mesh=None, u11=None):
+        """HALOFIND_GRID at the base level (haloes_grids.f:287-582), with the
+        recentering on the AMR levels when mesh and u11 are given: fills
+        cat, returns NHALLEV(0)."""
         u = np.ascontiguousarray(u1, np.float32).reshape(-1)
         r = np.ascontiguousarray(radx, np.float32)
         cc = cat.as_c()
+        mh = abi.MeshHolder(mesh) if mesh is not None else None
+        v11 = np.ascontiguousarray(u11, np.float32).reshape(-1) if u11 is not None else None
         rc = lib().orc_halofind_grid_base(C.c_int(nx), C.c_float(dx), P(u), P(r), C.c_float(contrastec),
                                           C.c_float(rote), C.c_float(rete), C.c_float(rodo), C.c_float(re0),
-                                          C.c_float(bound), C.c_float(vol_solap_low), C.byref(cc))
+                                          C.c_float(bound), C.c_float(vol_solap_low),
+                                          C.byref(mh.c) if mh else None, P(v11) if v11 is not None else None,
+                                          C.byref(cc))
         cat.nclus = cc.nclus
         if rc < 0:
             raise RuntimeError("HALOFIND_GRID: growing not converged" if rc == -1 else "catalogue full")

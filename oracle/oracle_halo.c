@@ -1313,8 +1313,93 @@ int orc_substructure_particles(const orc_store *st, const asohf_consts *k,
 }
 
 
-/* HALOFIND_GRID at the base level (haloes_grids.f:287-582) for a run without
- * AMR levels (NL = 0: no RECENTER_DENSITY_PEAK, no duplicate test).  U1
+/* Strict local maximum test of UBAS(ii, jj, kk) (1-based in the 6^3 block). */
+static int ubas_peak(const float ub[6][6][6], int ii, int jj, int kk)
+{
+#define UB(i, j, k) ub[(k) - 1][(j) - 1][(i) - 1]
+  const float c = UB(ii, jj, kk);
+  const float dxp = UB(ii + 1, jj, kk) - c, dxm = c - UB(ii - 1, jj, kk);
+  const float dyp = UB(ii, jj + 1, kk) - c, dym = c - UB(ii, jj - 1, kk);
+  const float dzp = UB(ii, jj, kk + 1) - c, dzm = c - UB(ii, jj, kk - 1);
+#undef UB
+  return dxp < 0.0f && dyp < 0.0f && dzp < 0.0f && dxm > 0.0f && dym > 0.0f && dzm > 0.0f;
+}
+
+/* RECENTER_DENSITY_PEAK (haloes_grids.f:1099-1259): from level hlev+1 down,
+ * the first patch of the level that strictly encloses the 6-cell box
+ * around the current centre; in its 6^3 block the highest strict local
+ * maximum among the inner 2^3 cells, then among the inner 4^3 (the second
+ * scan always runs); the centre moves to that cell's RX/RY/RZ.  Stops at the
+ * first level with no enclosing patch or no maximum.  *pipatch receives the
+ * last patch used (1-based).  A block reaching outside the NAMRX^3 array
+ * ends the descent (the Fortran would read past the patch there). */
+static void recenter_grid_peak(float *c3, int hlev, const asohf_mesh *m, const float *u11, float dx, int *pipatch)
+{
+  const int bor = 2, na = ASOHF_NAMRX;
+  const size_t pc = (size_t)na * na * na;
+  const int32_t *pn[3] = {m->patchnx, m->patchny, m->patchnz};
+  const float *pr[3] = {m->patchrx, m->patchry, m->patchrz};
+  for (int ir = hlev + 1; ir <= m->nl; ir++) {
+    const float dxpa = dx / powf(2.0f, (float)ir);
+    float x1[3], x2[3], x3[3];
+    for (int a = 0; a < 3; a++) {
+      x1[a] = c3[a] - (1.0f + (float)bor) * dxpa;
+      x2[a] = c3[a] + (1.0f + (float)bor) * dxpa;
+    }
+    int low1 = 0;
+    for (int l = 0; l < ir; l++) low1 += m->npatch[l];
+    const int low2 = low1 + m->npatch[ir];
+    int found = -1;
+    for (int i = low1; i < low2 && found < 0; i++) {
+      int ok = 1;
+      for (int a = 0; a < 3; a++) {
+        const float lo = pr[a][i] - dxpa, hi = lo + (float)pn[a][i] * dxpa;
+        ok &= lo < x1[a] && x2[a] < hi;
+      }
+      if (ok) found = i;
+    }
+    if (found < 0) break;
+    int i1[3];
+    int inside = 1;
+    for (int a = 0; a < 3; a++) {
+      x3[a] = pr[a][found] - dxpa;
+      i1[a] = (int)((x1[a] - x3[a]) / dxpa + 0.5f) + 1;
+      inside &= i1[a] >= 1 && i1[a] + 1 + 2 * bor <= na;
+    }
+    if (!inside) break;
+    float ub[6][6][6];
+    const float *u = u11 + (size_t)found * pc;
+    for (int kk = 0; kk < 6; kk++)
+      for (int jj = 0; jj < 6; jj++)
+        for (int ii = 0; ii < 6; ii++)
+          ub[kk][jj][ii] = u[((size_t)(i1[2] - 1 + kk) * na + (i1[1] - 1 + jj)) * na + (i1[0] - 1 + ii)];
+    float cur = -100000.0f;
+    int inmax[3] = {0, 0, 0};
+    for (int pass = 0; pass < 2; pass++) {
+      const int lo = pass == 0 ? 3 : 2, hi = pass == 0 ? 4 : 5;
+      for (int kk = lo; kk <= hi; kk++)
+        for (int jj = lo; jj <= hi; jj++)
+          for (int ii = lo; ii <= hi; ii++)
+            if (ubas_peak((const float(*)[6][6])ub, ii, jj, kk) && ub[kk - 1][jj - 1][ii - 1] > cur) {
+              cur = ub[kk - 1][jj - 1][ii - 1];
+              inmax[0] = ii;
+              inmax[1] = jj;
+              inmax[2] = kk;
+            }
+    }
+    if (cur < 0.0f) break;
+    for (int a = 0; a < 3; a++) {
+      const int ix = i1[a] + inmax[a] - 1;
+      c3[a] = (pr[a][found] - 0.5f * dxpa) + (float)(ix - 1) * dxpa;  /* RX(IX, I) */
+    }
+    *pipatch = found + 1;
+  }
+}
+
+/* HALOFIND_GRID at the base level (haloes_grids.f:287-582).  With AMR levels
+ * (mesh->nl > 0 and u11: NAMRX^3 per patch, patches in mesh order) each new
+ * peak is first recentred on the finer levels (RECENTER_DENSITY_PEAK) and
+ * dropped when the new centre lies inside a halo already found.  U1
  * (nx^3, IX fastest) is rho/rho_B; radx holds RADX(0..NX+1).  Peaks: cells
  * at least BOR=1 from the faces with U1 >= CONTRASTEC/6 that exceed their
  * six neighbours, taken in decreasing density (SORT_CELLS: ARGSORT of
@@ -1330,8 +1415,9 @@ int orc_substructure_particles(const orc_store *st, const asohf_consts *k,
  * stops), -2 when the catalogue is full. */
 int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx, float contrastec, float rote,
                            float rete, float rodo, float re0, float bound, float vol_solap_low,
-                           asohf_catalogue *cat)
+                           const asohf_mesh *mesh, const float *u11, asohf_catalogue *cat)
 {
+  const int amr = mesh && mesh->nl > 0 && u11;
   const int bor = 1;
   const float esp = 0.2f * dx, esp_log = 1.05f;
   const float peak_thr = contrastec / 6.0f;
@@ -1382,12 +1468,23 @@ int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx,
     const int ic = dx3[3 * q], jc = dx3[3 * q + 1], kc = dx3[3 * q + 2];
     if (CONTA(ic, jc, kc) != 1) continue;
     if (cat->nclus >= cat->capacity) { rc = -2; break; }
+    float c3[3] = {radx[ic], radx[jc], radx[kc]};
+    int ipatch = 0;
+    if (amr) {
+      recenter_grid_peak(c3, 0, mesh, u11, dx, &ipatch);
+      int dup = 0;  /* the same halo found again after recentering */
+      for (int q2 = 0; q2 < cat->nclus && !dup; q2++) {
+        const float ex = c3[0] - cat->clusrx[q2], ey = c3[1] - cat->clusry[q2], ez = c3[2] - cat->clusrz[q2];
+        dup = ex * ex + ey * ey + ez * ez < cat->radio[q2] * cat->radio[q2];
+      }
+      if (dup) continue;
+    }
     const int h = cat->nclus++;
     added++;
     cat->realclus[h] = -1;
     cat->levhal[h] = 0;
-    cat->patchclus[h] = 0;
-    const float xc = radx[ic], yc = radx[jc], zc = radx[kc];
+    cat->patchclus[h] = ipatch;
+    const float xc = c3[0], yc = c3[1], zc = c3[2];
     cat->clusrx[h] = xc;
     cat->clusry[h] = yc;
     cat->clusrz[h] = zc;

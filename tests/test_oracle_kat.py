@@ -263,3 +263,26 @@ def test_halofind_grid_base_known_answer():
         assert 0.85 * r_pred < cat.radio[h] < 1.2 * r_pred
         # mass: the cells inside the final radius, rho_B = 1
         assert cat.masa[h] > a * (4.0 / 3.0) * math.pi * (0.8 * r0) ** 3
+
+
+def test_halofind_grid_base_recenters_on_a_patch():
+    """With an AMR level the new peak moves to the finer level's maximum
+    (RECENTER_DENSITY_PEAK, haloes_grids.f:1099-1259): the centre becomes
+    that fine cell's RX/RY/RZ and PATCHCLUS the patch."""
+    nx, lado0 = 32, 32.0
+    radx, dx = grid.malla(nx, lado0)
+    u = _tophat_field(nx, [((15, 15, 15), 3.0, 400.0)])     # base peak at RADX(16) = -0.5 on each axis
+    na = abi.NAMRX
+    # one level-1 patch of 16^3 cells from base cell 12 (PATCHRX = RADX(12) = -4.5)
+    mesh = synth.Mesh(1, np.array([0, 1], np.int32), *(np.array([16], np.int32) for _ in range(3)),
+                      *(np.array([12], np.int32) for _ in range(3)),
+                      *(np.array([radx[12]], np.float32) for _ in range(3)), np.array([0], np.int32))
+    k, j, i = np.meshgrid(np.arange(1, na + 1), np.arange(1, na + 1), np.arange(1, na + 1), indexing="ij")
+    u11 = (900.0 - 10.0 * ((i - 10) ** 2 + (j - 9) ** 2 + (k - 10) ** 2)).astype(np.float32)[None]
+    cat = abi.Catalogue(16)
+    n = O.OracleBackend().halofind_grid_base(nx, float(dx), u, radx, 200.0, 1.0, 1.0, 1.0, 1.0, 10.0, 0.2, cat,
+                                              mesh=mesh, u11=u11)
+    assert n == 1
+    # RX(IX) = PATCHRX - DXPA/2 + (IX-1) DXPA with DXPA = 0.5: IX = 10, 9, 10
+    assert (cat.clusrx[0], cat.clusry[0], cat.clusrz[0]) == (-0.25, -0.75, -0.25)
+    assert cat.patchclus[0] == 1
