@@ -36,7 +36,33 @@ def make():
            "u1_sample": r.u1.ravel()[::97].copy(), "indcs": r.cat.indcs[:n].copy()}
     for f in SCALARS:
         out["cat_" + f] = getattr(r.cat, f)[:n].copy()
+    out.update(make_mesh_and_grid_finder(s, r))
     return out
+
+
+def make_mesh_and_grid_finder(s, r):
+    """The mesh builder's counts and VEINSGRID_REDUCED on the snapshot's
+    level-1 patches, and the base level of the grid finder on its density."""
+    from asohf_b200 import abi
+    cfg = s.cfg
+    plan = driver.prepare(s)
+    dx = float(plan.dx)
+    ob = O.OracleBackend(nthreads=1)
+    ob.upload(s)
+    npe = ob.species_sort(cfg.nx, plan.dx, plan.cos["rodo"], plan.cos["re0"])
+    cr0 = ob.mesh_base_counts(cfg.nx, dx, 8, 2, npe)
+    m = plan.mesh
+    n1 = int(m.npatch[1])
+    pat = (m.patchnx[:n1], m.patchny[:n1], m.patchnz[:n1], m.patchrx[:n1], m.patchry[:n1], m.patchrz[:n1])
+    cr01 = ob.mesh_patch_counts(1, dx, 8, 1, npe, *pat)
+    ob.veinsgrid_reduced(1, dx, float(plan.radx[1]), *pat, 1000, cr01)
+    cat = abi.Catalogue(4096)
+    nh = ob.halofind_grid_base(cfg.nx, dx, r.u1, plan.radx, 200.0, 1.0, 1.0, 1.0, 1.0, 10.0 * dx, 0.2, cat,
+                               mesh=m, u11=r.u11)
+    return {"mesh_cr0_sha256": np.array([digest(cr0)]), "mesh_cr01_sha256": np.array([digest(cr01)]),
+            "mesh_cr01_nonzero": np.array([int((cr01 > 0).sum())]),
+            "grid_nhallev0": np.array([nh]), "grid_radio": cat.radio[:cat.nclus].copy(),
+            "grid_clusrx": cat.clusrx[:cat.nclus].copy(), "grid_realclus": cat.realclus[:cat.nclus].copy()}
 
 
 if __name__ == "__main__":
