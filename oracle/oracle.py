@@ -236,6 +236,24 @@ class OracleBackend:
             raise RuntimeError("HALOFIND_GRID: growing not converged" if rc == -1 else "catalogue full")
         return rc
 
+    def halofind_grid_amr(self, ir, nx, dx, u1, radx, mesh, u11, cr0amr, cr0amr11, solap, contrastec, rote, rete,
+                          rodo, re0, bound, vol_solap_low, cat):
+        """HALOFIND_GRID on AMR level ir (haloes_grids.f:586-1097), appending to
+        cat; returns NHALLEV(ir)."""
+        f = lambda a, t=np.float32: np.ascontiguousarray(a, t).reshape(-1)
+        u, r, v11 = f(u1), f(radx), f(u11)
+        c0, c11, so = f(cr0amr, np.int32), f(cr0amr11, np.int32), f(solap, np.int32)
+        mh = abi.MeshHolder(mesh)
+        cc = cat.as_c()
+        rc = lib().orc_halofind_grid_amr(C.c_int(ir), C.c_int(nx), C.c_float(dx), P(u), P(r), C.byref(mh.c), P(v11),
+                                         P(c0, _ip), P(c11, _ip), P(so, _ip), C.c_float(contrastec),
+                                         C.c_float(rote), C.c_float(rete), C.c_float(rodo), C.c_float(re0),
+                                         C.c_float(bound), C.c_float(vol_solap_low), C.byref(cc))
+        cat.nclus = cc.nclus
+        if rc < 0:
+            raise RuntimeError("HALOFIND_GRID: growing not converged" if rc == -1 else "catalogue full")
+        return rc
+
     def overlapping(self, cat, ir, nhallev, vol_solap_low):
         """OVERLAPPING at level ir; nhallev[l] = haloes found at level l."""
         lowh3 = int(sum(nhallev[:ir])) + 1

@@ -1555,3 +1555,238 @@ int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx,
   orc_overlapping(cat, 1, cat->nclus, vol_solap_low);
   return added;
 }
+
+
+/* HALOFIND_GRID on the AMR level ir >= 1 (haloes_grids.f:586-1097).  The
+ * catalogue holds the haloes of the levels below (appended to).  cr0amr
+ * (nx^3), cr0amr11 and solap (NAMRX^3 per patch, mesh order) are the
+ * caller's refinement and overlap masks, 1 where a cell is not refined
+ * further (CR0AMR, CR0AMR11) or is the master copy (SOLAP).  Steps:
+ * CONTA1 = 1 on the level's patches, 0 inside any halo already found
+ * (AA <= RADIO) and where SOLAP = 0 (CLEAN_OVERLAPS_INT); peaks as on the
+ * base grid but inside BORAMR = 1 of the patch faces and with CONTA1 = 1,
+ * in decreasing density (SORT_CELLS_AMR); a peak still at CONTA1 = 1 is
+ * recentred on the finer levels when ir < NL (and dropped when inside a
+ * halo found before), then grown from R_EXT = 0.87 DXPA by MAX(R_EXT + 0.2
+ * DXPA, 1.05 R_EXT) up to MAX(BOUND/1.5^ir, 3): each shell sums the base
+ * cells with CR0AMR = 1, the cells of the levels 1..ir-1 with CR0AMR11 = 1
+ * and SOLAP = 1 and the level-ir cells with SOLAP = 1 (zeroing CONTA1
+ * there), on the patches whose boxes meet the sphere's (PATCHES_SPHERE).
+ * OVERLAPPING follows.  Returns NHALLEV(ir), -1 when a halo grows past the
+ * bound, -2 when the catalogue is full. */
+int orc_halofind_grid_amr(int ir, int nx, float dx, const float *u1, const float *radx, const asohf_mesh *m,
+                          const float *u11, const int32_t *cr0amr, const int32_t *cr0amr11, const int32_t *solap,
+                          float contrastec, float rote, float rete, float rodo, float re0, float bound,
+                          float vol_solap_low, asohf_catalogue *cat)
+{
+  const int na = ASOHF_NAMRX, boramr = 1;
+  const size_t pc = (size_t)na * na * na;
+  const int32_t *pn[3] = {m->patchnx, m->patchny, m->patchnz};
+  const float *pr[3] = {m->patchrx, m->patchry, m->patchrz};
+  const float peak_thr = contrastec / 6.0f;
+  int *lev_lo = malloc(sizeof(int) * (size_t)(m->nl + 2));
+  {
+    int acc = 0;
+    for (int l = 0; l <= m->nl; l++) {
+      lev_lo[l] = acc;  /* 0-based first patch of level l */
+      acc += m->npatch[l];
+    }
+    lev_lo[m->nl + 1] = acc;
+  }
+  const int low1 = lev_lo[ir], low2 = lev_lo[ir + 1];
+  const float dxpa = dx / powf(2.0f, (float)ir);
+  /* RX(IX, I) = PATCHRX(I) - DXPA/2 + (IX-1) DXPA on level l */
+#define RXL(a, ix, i, d) ((pr[a][i] - 0.5f * (d)) + (float)((ix) - 1) * (d))
+  int32_t *conta1 = calloc((size_t)(low2 > low1 ? low2 - low1 : 1), pc * sizeof(int32_t));
+#define C1(i, j, k, p) conta1[(size_t)((p) - low1) * pc + ((size_t)((k) - 1) * na + ((j) - 1)) * na + ((i) - 1)]
+#define U11(i, j, k, p) u11[(size_t)(p) * pc + ((size_t)((k) - 1) * na + ((j) - 1)) * na + ((i) - 1)]
+#define MASK(a, i, j, k, p) (a)[(size_t)(p) * pc + ((size_t)((k) - 1) * na + ((j) - 1)) * na + ((i) - 1)]
+  for (int p = low1; p < low2; p++)
+    for (int k = 1; k <= pn[2][p]; k++)
+      for (int j = 1; j <= pn[1][p]; j++)
+        for (int i = 1; i <= pn[0][p]; i++) C1(i, j, k, p) = 1;
+  for (int p = low1; p < low2; p++) {
+    float x1[3], x2[3];
+    for (int a = 0; a < 3; a++) {
+      x1[a] = pr[a][p] - dxpa;
+      x2[a] = x1[a] + (float)pn[a][p] * dxpa;
+    }
+    for (int h = 0; h < cat->nclus; h++) {
+      const float c3[3] = {cat->clusrx[h], cat->clusry[h], cat->clusrz[h]}, b = cat->radio[h];
+      int meet = 1;
+      for (int a = 0; a < 3; a++) meet &= x1[a] <= c3[a] + b && c3[a] - b <= x2[a];
+      if (!meet) continue;
+      for (int k = 1; k <= pn[2][p]; k++)
+        for (int j = 1; j <= pn[1][p]; j++)
+          for (int i = 1; i <= pn[0][p]; i++) {
+            const float ex = RXL(0, i, p, dxpa) - c3[0], ey = RXL(1, j, p, dxpa) - c3[1],
+                        ez = RXL(2, k, p, dxpa) - c3[2];
+            if (sqrtf(ex * ex + ey * ey + ez * ez) <= b) C1(i, j, k, p) = 0;
+          }
+    }
+    for (int k = 1; k <= pn[2][p]; k++)  /* CLEAN_OVERLAPS_INT */
+      for (int j = 1; j <= pn[1][p]; j++)
+        for (int i = 1; i <= pn[0][p]; i++) C1(i, j, k, p) = C1(i, j, k, p) * MASK(solap, i, j, k, p);
+  }
+  /* peaks, in (patch, KZ, JY, IX) order, then SORT_CELLS_AMR */
+  int64_t cap = 1024, ncand = 0;
+  float *ddd = malloc(sizeof(float) * cap);
+  int *d4 = malloc(sizeof(int) * 4 * cap);
+  for (int p = low1; p < low2; p++)
+    for (int k = 1 + boramr; k <= pn[2][p] - boramr; k++)
+      for (int j = 1 + boramr; j <= pn[1][p] - boramr; j++)
+        for (int i = 1 + boramr; i <= pn[0][p] - boramr; i++) {
+          const float b = U11(i, j, k, p);
+          if (!(b >= peak_thr && C1(i, j, k, p) == 1)) continue;
+          if (!(U11(i + 1, j, k, p) - b < 0.0f)) continue;
+          if (!(U11(i, j + 1, k, p) - b < 0.0f)) continue;
+          if (!(U11(i, j, k + 1, p) - b < 0.0f)) continue;
+          if (!(b - U11(i - 1, j, k, p) > 0.0f)) continue;
+          if (!(b - U11(i, j - 1, k, p) > 0.0f)) continue;
+          if (!(b - U11(i, j, k - 1, p) > 0.0f)) continue;
+          if (ncand == cap) {
+            cap *= 2;
+            ddd = realloc(ddd, sizeof(float) * cap);
+            d4 = realloc(d4, sizeof(int) * 4 * cap);
+          }
+          ddd[ncand] = b;
+          d4[4 * ncand] = i;
+          d4[4 * ncand + 1] = j;
+          d4[4 * ncand + 2] = k;
+          d4[4 * ncand + 3] = p;
+          ncand++;
+        }
+  float *inv = calloc((size_t)(ncand > 0 ? ncand : 1), sizeof(float));
+  int64_t *order = malloc(sizeof(int64_t) * (size_t)(ncand > 0 ? ncand : 1));
+  for (int64_t q = 0; q < ncand; q++) inv[q] = 1.0f / ddd[q];
+  orc_argsort(ncand, inv, order);
+  const int lowh3 = cat->nclus + 1;
+  const float esp = 0.2f * dxpa, esp_log = 1.05f;
+  const float b15 = bound / powf(1.5f, (float)ir);
+  const float boundir = b15 > 3.0f ? b15 : 3.0f;
+  int rc = 0, added = 0;
+  for (int64_t l = 0; l < ncand && rc == 0; l++) {
+    const int64_t q = order[l] - 1;
+    const int ic = d4[4 * q], jc = d4[4 * q + 1], kc = d4[4 * q + 2];
+    int ipatch = d4[4 * q + 3];
+    if (C1(ic, jc, kc, ipatch) != 1) continue;
+    float c3[3] = {RXL(0, ic, ipatch, dxpa), RXL(1, jc, ipatch, dxpa), RXL(2, kc, ipatch, dxpa)};
+    int ipf = ipatch + 1;  /* 1-based, as PATCHCLUS */
+    if (ir != m->nl) {
+      recenter_grid_peak(c3, ir, m, u11, dx, &ipf);
+      int dup = 0;
+      for (int q2 = 0; q2 < cat->nclus; q2++) {
+        const float ex = c3[0] - cat->clusrx[q2], ey = c3[1] - cat->clusry[q2], ez = c3[2] - cat->clusrz[q2];
+        if (ex * ex + ey * ey + ez * ez < cat->radio[q2] * cat->radio[q2]) dup = 1;
+      }
+      if (dup) continue;
+    }
+    if (cat->nclus >= cat->capacity) { rc = -2; break; }
+    const int h = cat->nclus++;
+    added++;
+    cat->realclus[h] = -1;
+    cat->levhal[h] = ir;
+    cat->patchclus[h] = ipf;
+    cat->clusrx[h] = c3[0];
+    cat->clusry[h] = c3[1];
+    cat->clusrz[h] = c3[2];
+    float bx = 0.0f, by = 0.0f, bz = 0.0f, basdelta = 0.0f, basmass = 0.0f, basvol = 0.0f;
+    float r_int = 0.0f, r_ext = 0.87f * dxpa;
+    float delta = 10.0f * contrastec * rote;
+    int iter = 0;
+    while (delta > contrastec * rote) {
+      iter++;
+      if (iter > 1) {
+        if (r_ext <= boundir) {
+          r_int = r_ext;
+          const float a1 = r_ext + esp, a2 = r_ext * esp_log;
+          r_ext = a1 > a2 ? a1 : a2;
+        } else {
+          rc = -1;
+          break;
+        }
+      }
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; a++) {
+        float bb = c3[a] - r_ext;
+        lo[a] = (int)(((bb - radx[1]) / dx) + 0.5f) + 1;
+        if (lo[a] < 1) lo[a] = 1;
+        bb = c3[a] + r_ext;
+        hi[a] = (int)(((bb - radx[1]) / dx) + 0.5f) + 1;
+        if (hi[a] > nx) hi[a] = nx;
+      }
+      /* BASX..BASZ hold the upper box bounds when the shell sums start */
+      bx = c3[0] + r_ext;
+      by = c3[1] + r_ext;
+      bz = c3[2] + r_ext;
+      float shell = 0.0f;
+      float volcell = dx * dx * dx;
+      for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+          for (int i = lo[0]; i <= hi[0]; i++) {
+            if (cr0amr[((size_t)(k - 1) * nx + (j - 1)) * nx + (i - 1)] != 1) continue;
+            const float ex = radx[i] - c3[0], ey = radx[j] - c3[1], ez = radx[k] - c3[2];
+            const float aa = sqrtf(ex * ex + ey * ey + ez * ez);
+            if (!(aa >= r_int && aa < r_ext)) continue;
+            basvol = basvol + volcell;
+            const float b = u1[((size_t)(k - 1) * nx + (j - 1)) * nx + (i - 1)] * volcell;
+            shell = shell + b;
+            bx = bx + radx[i] * b;
+            by = by + radx[j] * b;
+            bz = bz + radx[k] * b;
+            basdelta = basdelta + b;
+          }
+      /* PATCHES_SPHERE: the patches of levels 1..ir whose boxes meet the sphere's */
+      for (int irr = 1; irr <= ir; irr++) {
+        const float d = dx / powf(2.0f, (float)irr);
+        volcell = d * d * d;
+        for (int p = lev_lo[irr]; p < lev_lo[irr + 1]; p++) {
+          int meet = 1;
+          for (int a = 0; a < 3; a++) {
+            const float x3 = pr[a][p] - d, x4 = x3 + (float)pn[a][p] * d;
+            meet &= c3[a] - r_ext <= x4 && x3 <= c3[a] + r_ext;
+          }
+          if (!meet) continue;
+          for (int k = 1; k <= pn[2][p]; k++)
+            for (int j = 1; j <= pn[1][p]; j++)
+              for (int i = 1; i <= pn[0][p]; i++) {
+                if (irr < ir && MASK(cr0amr11, i, j, k, p) != 1) continue;
+                if (MASK(solap, i, j, k, p) != 1) continue;
+                const float rx = RXL(0, i, p, d), ry = RXL(1, j, p, d), rz = RXL(2, k, p, d);
+                const float ex = rx - c3[0], ey = ry - c3[1], ez = rz - c3[2];
+                const float aa = sqrtf(ex * ex + ey * ey + ez * ez);
+                if (!(aa >= r_int && aa < r_ext)) continue;
+                if (irr == ir) C1(i, j, k, p) = 0;
+                basvol = basvol + volcell;
+                const float b = U11(i, j, k, p) * volcell;
+                shell = shell + b;
+                bx = bx + rx * b;
+                by = by + ry * b;
+                bz = bz + rz * b;
+                basdelta = basdelta + b;
+              }
+        }
+      }
+      basmass = basmass + shell * rodo * (re0 * re0 * re0);
+      if (basvol > 0.0f) delta = basmass / (basvol * (rete * rete * rete));
+    }
+    cat->radio[h] = r_ext;
+    cat->masa[h] = basmass;
+    cat->clusrxcm[h] = bx / basdelta;
+    cat->clusrycm[h] = by / basdelta;
+    cat->clusrzcm[h] = bz / basdelta;
+  }
+#undef RXL
+#undef C1
+#undef U11
+#undef MASK
+  free(ddd);
+  free(d4);
+  free(inv);
+  free(order);
+  free(conta1);
+  free(lev_lo);
+  if (rc) return rc;
+  orc_overlapping(cat, lowh3, cat->nclus, vol_solap_low);
+  return added;
+}

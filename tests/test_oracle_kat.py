@@ -286,3 +286,36 @@ def test_halofind_grid_base_recenters_on_a_patch():
     # RX(IX) = PATCHRX - DXPA/2 + (IX-1) DXPA with DXPA = 0.5: IX = 10, 9, 10
     assert (cat.clusrx[0], cat.clusry[0], cat.clusrz[0]) == (-0.25, -0.75, -0.25)
     assert cat.patchclus[0] == 1
+
+
+def test_halofind_grid_amr_known_answer():
+    """HALOFIND_GRID on AMR level 1 (haloes_grids.f:586-1097): a top-hat
+    overdensity resolved only on a level-1 patch gives one halo of level 1
+    on that patch's peak cell, grown over the patch cells (the base cells
+    under the patch are masked by CR0AMR) to the top-hat radius."""
+    nx, lado0, na = 32, 32.0, abi.NAMRX
+    radx, dx = grid.malla(nx, lado0)
+    mesh = synth.Mesh(1, np.array([0, 1], np.int32), *(np.array([32], np.int32) for _ in range(3)),
+                      *(np.array([9], np.int32) for _ in range(3)),
+                      *(np.array([radx[9]], np.float32) for _ in range(3)), np.array([0], np.int32))
+    u1 = np.ones((nx, nx, nx), np.float32)
+    cr0amr = np.ones((nx, nx, nx), np.int32)
+    cr0amr[8:24, 8:24, 8:24] = 0                     # base cells 9..24 lie under the patch
+    u11 = _tophat_field(na, [((16, 16, 16), 3.0, 400.0)])[None]   # fine cell 17: RX = 0.25
+    ones = np.ones((1, na, na, na), np.int32)
+    cat = abi.Catalogue(16)
+    n = O.OracleBackend().halofind_grid_amr(1, nx, float(dx), u1, radx, mesh, u11, cr0amr, ones, ones, 200.0,
+                                             1.0, 1.0, 1.0, 1.0, 10.0, 0.2, cat)
+    assert n == 1 and cat.nclus == 1
+    assert (cat.levhal[0], cat.patchclus[0], cat.realclus[0]) == (1, 1, -1)
+    assert (cat.clusrx[0], cat.clusry[0], cat.clusrz[0]) == (0.25, 0.25, 0.25)
+    r_pred = 3 * 0.5 * (400.0 / 199.0) ** (1.0 / 3.0)
+    assert 0.85 * r_pred < cat.radio[0] < 1.2 * r_pred
+    # a second call at the same level finds the peak inside the halo: nothing new
+    cat2 = abi.Catalogue(16)
+    cat2.nclus = 1
+    for f in ("clusrx", "clusry", "clusrz", "radio"):
+        getattr(cat2, f)[0] = getattr(cat, f)[0]
+    cat2.realclus[0] = -1
+    assert O.OracleBackend().halofind_grid_amr(1, nx, float(dx), u1, radx, mesh, u11, cr0amr, ones, ones, 200.0,
+                                               1.0, 1.0, 1.0, 1.0, 10.0, 0.2, cat2) == 0
