@@ -46,6 +46,9 @@ void orc_momento(int nx, float dx, float *kkk);
 /* CREATE_MESH particle counts (grids.f:94-143, grids.f:341-380). */
 void orc_mesh_base_counts(int64_t n, const float *x, const float *y, const float *z, int nx, float dx,
                           int refine_thr, int bor, const int32_t *npart_esp, int32_t *cr0);
+/* COMPUTE_CR0AMR (grids.f:2076-2226) and VEINSGRID (grids.f:2229-2500): refinement and overlap masks. */
+void orc_compute_cr0amr(int nx, float lado0, const asohf_mesh *m, int32_t *cr0amr, int32_t *cr0amr1);
+void orc_veinsgrid(int ir, float dx, float radx1, const asohf_mesh *m, int32_t *solap);
 /* VEINSGRID_REDUCED (grids.f:1771-2073) on one level's patches. */
 int orc_veinsgrid_reduced(int ir, float dx, float radx1, int npatch, const int32_t *pnx, const int32_t *pny,
                           const int32_t *pnz, const float *prx, const float *pry, const float *prz, int max_nb,

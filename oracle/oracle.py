@@ -312,6 +312,22 @@ class OracleBackend:
                                     *[P(a, _ip) for a in ai], *[P(a) for a in af], P(out, _ip))
         return out
 
+    def compute_cr0amr(self, nx, lado0, mesh):
+        """COMPUTE_CR0AMR (grids.f:2076-2226): (CR0AMR nx^3, CR0AMR1 per patch)."""
+        mh = abi.MeshHolder(mesh)
+        ntot = int(np.asarray(mesh.npatch).sum())
+        c0 = np.empty(nx ** 3, np.int32)
+        c1 = np.empty((max(ntot, 1), abi.NAMRX ** 3), np.int32)
+        lib().orc_compute_cr0amr(C.c_int(nx), C.c_float(lado0), C.byref(mh.c), P(c0, _ip), P(c1, _ip))
+        return c0, c1[:ntot]
+
+    def veinsgrid(self, ir, dx, radx1, mesh, solap):
+        """VEINSGRID (grids.f:2229-2500) on level ir; solap ((npatch total,
+        NAMRX^3) int32) written for the level's patches."""
+        mh = abi.MeshHolder(mesh)
+        assert solap.dtype == np.int32 and solap.flags.c_contiguous
+        lib().orc_veinsgrid(C.c_int(ir), C.c_float(dx), C.c_float(radx1), C.byref(mh.c), P(solap, _ip))
+
     def veinsgrid_reduced(self, ir, dx, radx1, pnx, pny, pnz, prx, pry, prz, max_nb, cr01, conta11=None):
         """VEINSGRID_REDUCED (grids.f:1771-2073) on one level's patches; cr01
         and conta11 ((npatch, NAMRX^3) int32) are modified in place."""

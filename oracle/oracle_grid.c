@@ -880,3 +880,139 @@ int orc_veinsgrid_reduced(int ir, float dx, float radx1, int npatch, const int32
   free(nb);
   return rc;
 }
+
+
+/* COMPUTE_CR0AMR (grids.f:2076-2226): CR0AMR(IX,JY,KZ) = 0 for the base
+ * cells under a level-1 patch (its odd cells' parents from PATCHX..Z),
+ * CR0AMR1 = 0 for the cells of a patch under one of its children (parent
+ * cells from PATCHX..Z in the parent's grid, PARE) and, on levels 1..NL-1,
+ * for cells inside the cell-centre box of a next-level patch that is not
+ * their child; 1 elsewhere.  cr0amr: nx^3; cr0amr1: NAMRX^3 per patch in
+ * mesh order (patch q = Fortran index q+1).  Parent cells outside the
+ * arrays are skipped. */
+void orc_compute_cr0amr(int nx, float lado0, const asohf_mesh *m, int32_t *cr0amr, int32_t *cr0amr1)
+{
+  const int na = ASOHF_NAMRX;
+  const size_t pc = (size_t)na * na * na;
+  int ntot = 0;
+  for (int l = 0; l <= m->nl; l++) ntot += m->npatch[l];
+  for (size_t q = 0; q < (size_t)nx * nx * nx; q++) cr0amr[q] = 1;
+  for (size_t q = 0; q < (size_t)ntot * pc; q++) cr0amr1[q] = 1;
+  int *lo = malloc(sizeof(int) * (size_t)(m->nl + 2));
+  int acc = 0;
+  for (int l = 0; l <= m->nl; l++) { lo[l] = acc; acc += m->npatch[l]; }
+  lo[m->nl + 1] = acc;
+  if (m->nl >= 1)
+    for (int i = lo[1]; i < lo[2]; i++)
+      for (int kz = 1; kz <= m->patchnz[i]; kz += 2)
+        for (int jy = 1; jy <= m->patchny[i]; jy += 2)
+          for (int ix = 1; ix <= m->patchnx[i]; ix += 2) {
+            const int c1 = m->patchx[i] - 1 + (ix + 1) / 2, c2 = m->patchy[i] - 1 + (jy + 1) / 2,
+                      c3 = m->patchz[i] - 1 + (kz + 1) / 2;
+            if (c1 < 1 || c1 > nx || c2 < 1 || c2 > nx || c3 < 1 || c3 > nx) continue;
+            cr0amr[((size_t)(c3 - 1) * nx + (c2 - 1)) * nx + (c1 - 1)] = 0;
+          }
+  for (int ir = 2; ir <= m->nl; ir++)
+    for (int i = lo[ir]; i < lo[ir + 1]; i++) {
+      const int par = m->pare[i] - 1;
+      if (par < 0 || par >= ntot) continue;
+      for (int kz = 1; kz <= m->patchnz[i]; kz++)
+        for (int jy = 1; jy <= m->patchny[i]; jy++)
+          for (int ix = 1; ix <= m->patchnx[i]; ix++) {
+            const int c1 = m->patchx[i] - 1 + (ix + 1) / 2, c2 = m->patchy[i] - 1 + (jy + 1) / 2,
+                      c3 = m->patchz[i] - 1 + (kz + 1) / 2;
+            if (c1 < 1 || c1 > na || c2 < 1 || c2 > na || c3 < 1 || c3 > na) continue;
+            cr0amr1[(size_t)par * pc + ((size_t)(c3 - 1) * na + (c2 - 1)) * na + (c1 - 1)] = 0;
+          }
+    }
+  const float dx = lado0 / (float)nx;
+  for (int ir = 1; ir <= m->nl - 1; ir++) {
+    const float dxpa = dx / powf(2.0f, (float)ir);
+    for (int i = lo[ir]; i < lo[ir + 1]; i++)
+      for (int kz = 1; kz <= m->patchnz[i]; kz++)
+        for (int jy = 1; jy <= m->patchny[i]; jy++)
+          for (int ix = 1; ix <= m->patchnx[i]; ix++) {
+            int32_t *c = &cr0amr1[(size_t)i * pc + ((size_t)(kz - 1) * na + (jy - 1)) * na + (ix - 1)];
+            if (*c != 1) continue;
+            const float xx = m->patchrx[i] - 0.5f * dxpa + (float)(ix - 1) * dxpa;
+            const float yy = m->patchry[i] - 0.5f * dxpa + (float)(jy - 1) * dxpa;
+            const float zz = m->patchrz[i] - 0.5f * dxpa + (float)(kz - 1) * dxpa;
+            for (int ii = lo[ir + 1]; ii < lo[ir + 2]; ii++) {
+              if (m->pare[ii] == i + 1) continue;
+              const float xx1 = m->patchrx[ii] - 0.5f * (dxpa * 0.5f);
+              const float yy1 = m->patchry[ii] - 0.5f * (dxpa * 0.5f);
+              const float zz1 = m->patchrz[ii] - 0.5f * (dxpa * 0.5f);
+              const float xx2 = xx1 + (float)(m->patchnx[ii] - 1) * dxpa * 0.5f;
+              const float yy2 = yy1 + (float)(m->patchny[ii] - 1) * dxpa * 0.5f;
+              const float zz2 = zz1 + (float)(m->patchnz[ii] - 1) * dxpa * 0.5f;
+              const float b1 = (xx - xx1) * (xx2 - xx), b2 = (yy - yy1) * (yy2 - yy), b3 = (zz - zz1) * (zz2 - zz);
+              if (b1 >= 0.0f && b2 >= 0.0f && b3 >= 0.0f) {
+                *c = 0;
+                break;
+              }
+            }
+          }
+  }
+  free(lo);
+}
+
+/* VEINSGRID (grids.f:2229-2500): SOLAP = 1 on the level's patches; then,
+ * patch I in order and each neighbour J in order (the intersecting cell
+ * boxes of VEINSGRID_REDUCED), for each pair of facing cells both still 1,
+ * the cell of I is cleared when it lies on I's faces (IX = 1 or N1, ...),
+ * else the cell of J.  solap: NAMRX^3 per patch in mesh order; only the
+ * level's patches are written.  Cells outside the arrays are skipped. */
+void orc_veinsgrid(int ir, float dx, float radx1, const asohf_mesh *m, int32_t *solap)
+{
+  const int na = ASOHF_NAMRX;
+  const size_t pc = (size_t)na * na * na;
+  int low1 = 0;
+  for (int l = 0; l < ir; l++) low1 += m->npatch[l];
+  const int low2 = low1 + m->npatch[ir];
+  const float dxpa = dx / powf(2.0f, (float)ir);
+  const float fix = radx1 - dx * 0.5f + 0.5f * dxpa;
+  const int32_t *pn[3] = {m->patchnx, m->patchny, m->patchnz};
+  const float *pr[3] = {m->patchrx, m->patchry, m->patchrz};
+  for (int i = low1; i < low2; i++)
+    for (size_t q = 0; q < pc; q++) solap[(size_t)i * pc + q] = 1;
+  for (int i = low1; i < low2; i++) {
+    int g1[3], n[3];
+    float r1[3], r2[3];
+    for (int a = 0; a < 3; a++) {
+      n[a] = pn[a][i];
+      g1[a] = (int)(((pr[a][i] - 0.5f * dxpa - fix) / dxpa) + 0.5f) + 1;
+      r1[a] = pr[a][i] - 0.5f * dxpa;
+      r2[a] = pr[a][i] - 0.5f * dxpa + (float)(n[a] - 1) * dxpa;
+    }
+    for (int j = low1; j < low2; j++) {
+      if (j == i) continue;
+      int ok = 1;
+      for (int a = 0; a < 3; a++) {
+        const int gj = (int)(((pr[a][j] - 0.5f * dxpa - fix) / dxpa) + 0.5f) + 1;
+        ok &= g1[a] <= gj + pn[a][j] - 1 && gj <= g1[a] + n[a] - 1;
+      }
+      if (!ok) continue;
+      int c1[3], c2[3], cc1[3], cc2[3];
+      for (int a = 0; a < 3; a++) {
+        const float rr1 = pr[a][j] - 0.5f * dxpa;
+        const float rr2 = pr[a][j] - 0.5f * dxpa + (float)(pn[a][j] - 1) * dxpa;
+        c1[a] = c2[a] = cc1[a] = cc2[a] = 0;
+        veins_axis(r1[a], r2[a], rr1, rr2, dxpa, n[a], pn[a][j], &c1[a], &c2[a], &cc1[a], &cc2[a]);
+      }
+      for (int kk = cc1[2]; kk <= cc2[2]; kk++)
+        for (int jj = cc1[1]; jj <= cc2[1]; jj++)
+          for (int ii = cc1[0]; ii <= cc2[0]; ii++) {
+            const int ix = ii - cc1[0] + c1[0], jy = jj - cc1[1] + c1[1], kz = kk - cc1[2] + c1[2];
+            if (ii < 1 || ii > na || jj < 1 || jj > na || kk < 1 || kk > na || ix < 1 || ix > na || jy < 1 ||
+                jy > na || kz < 1 || kz > na)
+              continue;
+            int32_t *si = &solap[(size_t)i * pc + ((size_t)(kz - 1) * na + (jy - 1)) * na + (ix - 1)];
+            int32_t *sj = &solap[(size_t)j * pc + ((size_t)(kk - 1) * na + (jj - 1)) * na + (ii - 1)];
+            if (*si == 1 && *sj == 1) {
+              if (ix == 1 || ix == n[0] || jy == 1 || jy == n[1] || kz == 1 || kz == n[2]) *si = 0;
+              else *sj = 0;
+            }
+          }
+    }
+  }
+}

@@ -59,7 +59,25 @@ def make_mesh_and_grid_finder(s, r):
     cat = abi.Catalogue(4096)
     nh = ob.halofind_grid_base(cfg.nx, dx, r.u1, plan.radx, 200.0, 1.0, 1.0, 1.0, 1.0, 10.0 * dx, 0.2, cat,
                                mesh=m, u11=r.u11)
-    return {"mesh_cr0_sha256": np.array([digest(cr0)]), "mesh_cr01_sha256": np.array([digest(cr01)]),
+    # the whole grid finder on the level-1 mesh: masks, base level, level 1
+    m1 = synth.Mesh(1, np.array([0, n1], np.int32), *(np.ascontiguousarray(a[:n1]) for a in (
+        m.patchnx, m.patchny, m.patchnz, m.patchx, m.patchy, m.patchz, m.patchrx, m.patchry, m.patchrz)),
+        np.zeros(n1, np.int32))
+    c0, c11 = ob.compute_cr0amr(cfg.nx, float(cfg.lado0), m1)
+    so = np.zeros((n1, abi.NAMRX ** 3), np.int32)
+    ob.veinsgrid(1, dx, float(plan.radx[1]), m1, so)
+    u11_1 = np.ascontiguousarray(r.u11[:n1])
+    g = abi.Catalogue(4096)
+    n0 = ob.halofind_grid_base(cfg.nx, dx, r.u1, plan.radx, 200.0, 1.0, 1.0, 1.0, 1.0, 10.0 * dx, 0.2, g,
+                               mesh=m1, u11=u11_1)
+    na1 = ob.halofind_grid_amr(1, cfg.nx, dx, r.u1, plan.radx, m1, u11_1, c0, c11, so, 200.0, 1.0, 1.0, 1.0, 1.0,
+                               10.0 * dx, 0.2, g)
+    k = g.nclus
+    amr = {"gridamr_cr0amr_sha256": np.array([digest(c0)]), "gridamr_solap_sha256": np.array([digest(so)]),
+           "gridamr_nhallev": np.array([n0, na1]), "gridamr_levhal": g.levhal[:k].copy(),
+           "gridamr_realclus": g.realclus[:k].copy(), "gridamr_radio": g.radio[:k].copy(),
+           "gridamr_clusrx": g.clusrx[:k].copy(), "gridamr_patchclus": g.patchclus[:k].copy()}
+    return {**amr, "mesh_cr0_sha256": np.array([digest(cr0)]), "mesh_cr01_sha256": np.array([digest(cr01)]),
             "mesh_cr01_nonzero": np.array([int((cr01 > 0).sum())]),
             "grid_nhallev0": np.array([nh]), "grid_radio": cat.radio[:cat.nclus].copy(),
             "grid_clusrx": cat.clusrx[:cat.nclus].copy(), "grid_realclus": cat.realclus[:cat.nclus].copy()}

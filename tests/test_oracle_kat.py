@@ -319,3 +319,42 @@ def test_halofind_grid_amr_known_answer():
     cat2.realclus[0] = -1
     assert O.OracleBackend().halofind_grid_amr(1, nx, float(dx), u1, radx, mesh, u11, cr0amr, ones, ones, 200.0,
                                                1.0, 1.0, 1.0, 1.0, 10.0, 0.2, cat2) == 0
+
+
+def _mesh(nl, npatch, n, px, pr, pare):
+    a = lambda v, t=np.int32: np.asarray(v, t)
+    return synth.Mesh(nl, a(npatch), a(n[0]), a(n[1]), a(n[2]), a(px[0]), a(px[1]), a(px[2]),
+                      a(pr[0], np.float32), a(pr[1], np.float32), a(pr[2], np.float32), a(pare))
+
+
+def test_compute_cr0amr_known_answer():
+    """COMPUTE_CR0AMR (grids.f:2076-2226): base cells under a level-1 patch
+    and parent cells under a level-2 child are 0, the rest 1."""
+    nx = 16
+    radx, dx = grid.malla(nx, 16.0)
+    # level 1: 8^3 cells from base cell 3 (covers base 3..6); level 2: 4^3 cells from its cell 2 (covers 2..3)
+    r1 = radx[3]
+    r2 = r1 - 0.25 + 1 * 0.5          # centre of the parent's cell 2 on level 1 (RX(2) = PATCHRX - DXPA/2 + DXPA)
+    m = _mesh(2, [0, 1, 1], ([8, 4], [8, 4], [8, 4]), ([3, 2], [3, 2], [3, 2]), ([r1, r2],) * 3, [0, 1])
+    c0, c1 = O.OracleBackend().compute_cr0amr(nx, 16.0, m)
+    c0 = c0.reshape(nx, nx, nx)
+    assert (c0[2:6, 2:6, 2:6] == 0).all() and c0.sum() == nx ** 3 - 64
+    p1 = c1[0].reshape(abi.NAMRX, abi.NAMRX, abi.NAMRX)
+    assert (p1[1:3, 1:3, 1:3] == 0).all() and (p1 == 0).sum() == 8
+    assert (c1[1] == 1).all()
+
+
+def test_veinsgrid_known_answer():
+    """VEINSGRID (grids.f:2229-2500): two 8^3 patches overlapping by half in
+    x; each facing pair keeps one master, the first patch's cell when it is
+    not on that patch's faces."""
+    na = abi.NAMRX
+    m = _mesh(1, [0, 2], ([8, 8], [8, 8], [8, 8]), ([5, 7], [5, 5], [5, 5]),
+              ([-3.5, -1.5], [-3.5, -3.5], [-3.5, -3.5]), [0, 0])
+    so = np.zeros((2, na ** 3), np.int32)
+    O.OracleBackend().veinsgrid(1, 1.0, -7.5, m, so)
+    a = so[0].reshape(na, na, na)[:8, :8, :8]
+    b = so[1].reshape(na, na, na)[:8, :8, :8]
+    assert (a == 0).sum() == 64 + 3 * 28    # A's face cells among the facing ones (ix = 8, or on a y/z face)
+    assert (b == 0).sum() == 256 - 148      # the other facing pairs drop B's cell
+    assert (a[:, :, :4] == 1).all() and (b[:, :, 4:] == 1).all()
