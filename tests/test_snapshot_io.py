@@ -60,3 +60,42 @@ def test_pipeline_from_a_file_equals_the_run_from_memory(tmp_path):
     n = a.cat.nclus
     assert np.array_equal(a.u1, b.u1)
     assert np.array_equal(a.cat.realclus[:n], b.cat.realclus[:n]) and np.array_equal(a.pph, b.pph)
+
+
+def gadget_case(npp, header_dm_mass, seed):
+    rng = np.random.default_rng(seed)
+    ntot = sum(npp)
+    pos = rng.uniform(0, 100, (ntot, 3)).astype(np.float32)
+    vel = rng.normal(0, 300, (ntot, 3)).astype(np.float32)
+    ids = rng.permutation(ntot).astype(np.int32) + 1000
+    m_all = rng.uniform(1, 2, ntot).astype(np.float32)
+    mass_arr = [0.0] * 6
+    if header_dm_mass:
+        mass_arr[1] = 0.75
+        keep = np.r_[0:npp[0], sum(npp[:4]):ntot]   # the block skips types 1-3
+        masses = m_all[keep]
+    else:
+        masses = m_all
+    return pos, vel, ids, m_all, mass_arr, masses
+
+
+@pytest.mark.parametrize("header_dm_mass", [True, False])
+def test_gadget_format2(tmp_path, header_dm_mass):
+    npp = [30, 200, 10, 5, 40, 2]          # gas, dm (three types), stars, black holes
+    pos, vel, ids, m_all, mass_arr, masses = gadget_case(npp, header_dm_mass, 3)
+    p = str(tmp_path / "snap_001")
+    sio.write_gadget_format2(p, npp, mass_arr, 0.5, pos, vel, ids, masses, boxsize=100.0)
+    r = sio.read_gadget_unformatted(p, var=2, cio_length=0.5, cio_xc=50.0, cio_yc=50.0, cio_zc=50.0)
+    dm = slice(30, 245)
+    st = slice(245, 285)
+    assert (r.n_dm, r.n_st, r.n) == (215, 40, 255) and r.zeta == 0.5
+    assert np.array_equal(r.x[:215], ((pos[dm, 0] - np.float32(50)) * np.float32(0.5)).astype(np.float32))
+    assert np.array_equal(r.vz[215:], vel[st, 2])
+    assert np.array_equal(r.id, np.r_[31:246, 246:286].astype(np.int32))    # numbered by file position
+    if header_dm_mass:
+        assert (r.m[:215] == np.float32(0.75)).all()
+    else:
+        assert np.array_equal(r.m[:215], m_all[dm])
+    assert np.array_equal(r.m[215:], m_all[st])
+    r1 = sio.read_gadget_unformatted(p, var=1)
+    assert r1.n == 215 and r1.n_st == 0
