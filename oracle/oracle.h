@@ -88,6 +88,12 @@ int orc_overlapping(asohf_catalogue *cat, int lowh3, int lowh2, float vol_solap_
  * (REALCLUS=-1) lying wholly inside a confirmed halo of a lower level is
  * removed.  Returns the number removed. */
 int orc_accidental_substructure(asohf_catalogue *cat, int nclus);
+/* SEARCH_SUBSTRUCTURE_GRID (substructure.f:2-697) on AMR level ir; subs_lev[0..ir] in/out. */
+int orc_search_substructure_grid(int ir, int nx, float dx, const float *u1, const float *radx,
+                                 const asohf_mesh *m, const float *u11, const int32_t *cr0amr,
+                                 const int32_t *cr0amr11, const int32_t *solap, float contrastec, float rote,
+                                 float rete, float rodo, float re0, float um, int32_t *subs_lev,
+                                 asohf_catalogue *cat);
 /* HALOFIND_GRID on AMR level ir >= 1 (haloes_grids.f:586-1097), given the refinement and overlap masks. */
 int orc_halofind_grid_amr(int ir, int nx, float dx, const float *u1, const float *radx, const asohf_mesh *m,
                           const float *u11, const int32_t *cr0amr, const int32_t *cr0amr11, const int32_t *solap,

@@ -254,6 +254,25 @@ class OracleBackend:
             raise RuntimeError("HALOFIND_GRID: growing not converged" if rc == -1 else "catalogue full")
         return rc
 
+    def search_substructure_grid(self, ir, nx, dx, u1, radx, mesh, u11, cr0amr, cr0amr11, solap, contrastec, rote,
+                                 rete, rodo, re0, um, subs_lev, cat):
+        """SEARCH_SUBSTRUCTURE_GRID on level ir (substructure.f:2-697); subs_lev
+        (int32, NL+1 entries) is updated in place; returns SUBS_LEV(ir)."""
+        f = lambda a, t=np.float32: np.ascontiguousarray(a, t).reshape(-1)
+        u, r, v11 = f(u1), f(radx), f(u11)
+        c0, c11, so = f(cr0amr, np.int32), f(cr0amr11, np.int32), f(solap, np.int32)
+        assert subs_lev.dtype == np.int32 and subs_lev.flags.c_contiguous
+        mh = abi.MeshHolder(mesh)
+        cc = cat.as_c()
+        rc = lib().orc_search_substructure_grid(C.c_int(ir), C.c_int(nx), C.c_float(dx), P(u), P(r), C.byref(mh.c),
+                                                P(v11), P(c0, _ip), P(c11, _ip), P(so, _ip), C.c_float(contrastec),
+                                                C.c_float(rote), C.c_float(rete), C.c_float(rodo), C.c_float(re0),
+                                                C.c_float(um), P(subs_lev, _ip), C.byref(cc))
+        cat.nclus = cc.nclus
+        if rc < 0:
+            raise RuntimeError({-2: "catalogue full", -3: "growth counts no cell"}.get(rc, str(rc)))
+        return rc
+
     def overlapping(self, cat, ir, nhallev, vol_solap_low):
         """OVERLAPPING at level ir; nhallev[l] = haloes found at level l."""
         lowh3 = int(sum(nhallev[:ir])) + 1

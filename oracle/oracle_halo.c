@@ -1790,3 +1790,295 @@ int orc_halofind_grid_amr(int ir, int nx, float dx, const float *u1, const float
   orc_overlapping(cat, lowh3, cat->nclus, vol_solap_low);
   return added;
 }
+
+
+/* FIND_HOST_HALO (substructure.f:1699-1747): from level ir-1 down to 0, the
+ * entries of that level's range (SUBS_LEV) still alive whose sphere (RADIO
+ * for haloes, RSUB for subhaloes) holds the point; the closest in units of
+ * that radius at the first level with any.  0-based index, or -1. */
+static int find_host_halo(const float *c3, int ir, const int32_t *subs_lev, const asohf_catalogue *cat)
+{
+  int host = -1;
+  float mind = 100000.0f;
+  for (int irr = ir - 1; irr >= 0; irr--) {
+    int low1 = 0;
+    for (int l = 0; l < irr; l++) low1 += subs_lev[l];
+    const int low2 = low1 + subs_lev[irr];
+    int flag = 0;
+    for (int ii = low1; ii < low2; ii++) {
+      if (cat->realclus[ii] == 0) continue;
+      const float bas = cat->realclus[ii] == -1 ? cat->radio[ii] : cat->rsub[ii];
+      const float ex = c3[0] - cat->clusrx[ii], ey = c3[1] - cat->clusry[ii], ez = c3[2] - cat->clusrz[ii];
+      const float d = sqrtf(ex * ex + ey * ey + ez * ez) / bas;
+      if (d < 1.0f) {
+        flag = 1;
+        if (d < mind) {
+          mind = d;
+          host = ii;
+        }
+      }
+    }
+    if (flag) break;
+  }
+  return host;
+}
+
+/* SEARCH_SUBSTRUCTURE_GRID (substructure.f:2-697) on AMR level ir: seeds
+ * subhaloes at density peaks of the level's patches that lie inside a halo
+ * or subhalo already found (CONTA1 = 1 within RADIO / RSUB, 0 within 2 DXPA
+ * of any centre and where SOLAP = 0).  A peak is a cell at least BORAMR = 1
+ * from the faces, with U11 >= CONTRASTEC/6 (CONTRASTEC from level 2 on) and
+ * no lower than any of its 26 neighbours, taken in decreasing density.  It
+ * is recentred on the finer levels when ir < NL (and dropped when inside a
+ * subhalo of this call), given a host by FIND_HOST_HALO (none: dropped;
+ * closer than 2 DXPA: dropped) and grown in shells as in HALOFIND_GRID
+ * (base cells with CR0AMR = 1, patch cells of levels 1..ir with CR0AMR11 =
+ * 1 and SOLAP = 1) until the Jacobi radius test R/DISTHOST >
+ * (M/(M + 3 MHOST))^(1/3) holds with more than 15 cells; MHOST is the
+ * host's profile mass interpolated at DISTHOST in r^3.  MASA and RADIO
+ * take the first shell below the virial contrast, scaled by UM (RADIO too,
+ * as in the reference), RSUB/MSUB the Jacobi shell.  subs_lev[ir] receives
+ * the subhaloes found.  Returns that count, -2 when the catalogue is full,
+ * -3 when a growth counts no cell in 100000 shells (the reference would
+ * loop for ever). */
+int orc_search_substructure_grid(int ir, int nx, float dx, const float *u1, const float *radx,
+                                 const asohf_mesh *m, const float *u11, const int32_t *cr0amr,
+                                 const int32_t *cr0amr11, const int32_t *solap, float contrastec, float rote,
+                                 float rete, float rodo, float re0, float um, int32_t *subs_lev,
+                                 asohf_catalogue *cat)
+{
+  const int na = ASOHF_NAMRX, boramr = 1, nb = ASOHF_NBINS;
+  const size_t pc = (size_t)na * na * na;
+  const int32_t *pn[3] = {m->patchnx, m->patchny, m->patchnz};
+  const float *pr[3] = {m->patchrx, m->patchry, m->patchrz};
+  float peak_thr = contrastec / 6.0f;
+  if (ir >= 2) peak_thr = contrastec;
+  const int nclus_ini = cat->nclus;
+  int *lev_lo = malloc(sizeof(int) * (size_t)(m->nl + 2));
+  {
+    int acc = 0;
+    for (int l = 0; l <= m->nl; l++) { lev_lo[l] = acc; acc += m->npatch[l]; }
+    lev_lo[m->nl + 1] = acc;
+  }
+  const int ntot = lev_lo[m->nl + 1];
+  const int low1 = lev_lo[ir], low2 = lev_lo[ir + 1];
+  const float dxpa = dx / powf(2.0f, (float)ir);
+#define RXL(a, ix, i, d) ((pr[a][i] - 0.5f * (d)) + (float)((ix) - 1) * (d))
+#define U11(i, j, k, p) u11[(size_t)(p) * pc + ((size_t)((k) - 1) * na + ((j) - 1)) * na + ((i) - 1)]
+#define MASK(a, i, j, k, p) (a)[(size_t)(p) * pc + ((size_t)((k) - 1) * na + ((j) - 1)) * na + ((i) - 1)]
+  int32_t *conta1 = calloc((size_t)(ntot > 0 ? ntot : 1), pc * sizeof(int32_t));
+#define C1(i, j, k, p) MASK(conta1, i, j, k, p)
+  for (int p = low1; p < low2; p++) {
+    float x1[3], x2[3];
+    for (int a = 0; a < 3; a++) {
+      x1[a] = pr[a][p] - dxpa;
+      x2[a] = x1[a] + (float)pn[a][p] * dxpa;
+    }
+    for (int pass = 0; pass < 2; pass++)   /* inside a halo: 1; near a centre: 0 */
+      for (int h = 0; h < cat->nclus; h++) {
+        if (cat->realclus[h] == 0) continue;
+        const float c3[3] = {cat->clusrx[h], cat->clusry[h], cat->clusrz[h]};
+        const float b = pass == 0 ? (cat->realclus[h] == -1 ? cat->radio[h] : cat->rsub[h]) : 2.0f * dxpa;
+        int meet = 1;
+        for (int a = 0; a < 3; a++) meet &= x1[a] <= c3[a] + b && c3[a] - b <= x2[a];
+        if (!meet) continue;
+        for (int k = 1; k <= pn[2][p]; k++)
+          for (int j = 1; j <= pn[1][p]; j++)
+            for (int i = 1; i <= pn[0][p]; i++) {
+              const float ex = RXL(0, i, p, dxpa) - c3[0], ey = RXL(1, j, p, dxpa) - c3[1],
+                          ez = RXL(2, k, p, dxpa) - c3[2];
+              if (sqrtf(ex * ex + ey * ey + ez * ez) <= b) C1(i, j, k, p) = pass == 0 ? 1 : 0;
+            }
+      }
+  }
+  for (int p = 0; p < ntot; p++)   /* CLEAN_OVERLAPS_INT over all levels */
+    for (int k = 1; k <= pn[2][p]; k++)
+      for (int j = 1; j <= pn[1][p]; j++)
+        for (int i = 1; i <= pn[0][p]; i++) C1(i, j, k, p) = C1(i, j, k, p) * MASK(solap, i, j, k, p);
+  /* peaks: no lower than the 3^3 neighbourhood */
+  int64_t cap = 1024, ncand = 0;
+  float *ddd = malloc(sizeof(float) * cap);
+  int *d4 = malloc(sizeof(int) * 4 * cap);
+  for (int p = low1; p < low2; p++)
+    for (int k = 1 + boramr; k <= pn[2][p] - boramr; k++)
+      for (int j = 1 + boramr; j <= pn[1][p] - boramr; j++)
+        for (int i = 1 + boramr; i <= pn[0][p] - boramr; i++) {
+          const float b = U11(i, j, k, p);
+          if (!(b >= peak_thr && C1(i, j, k, p) == 1)) continue;
+          float mx = -INFINITY;
+          for (int kk = k - 1; kk <= k + 1; kk++)
+            for (int jj = j - 1; jj <= j + 1; jj++)
+              for (int ii = i - 1; ii <= i + 1; ii++) {
+                const float v = U11(ii, jj, kk, p);
+                if (v > mx || mx != mx) mx = v;
+              }
+          if (!(b >= mx)) continue;
+          if (ncand == cap) {
+            cap *= 2;
+            ddd = realloc(ddd, sizeof(float) * cap);
+            d4 = realloc(d4, sizeof(int) * 4 * cap);
+          }
+          ddd[ncand] = b;
+          d4[4 * ncand] = i;
+          d4[4 * ncand + 1] = j;
+          d4[4 * ncand + 2] = k;
+          d4[4 * ncand + 3] = p;
+          ncand++;
+        }
+  float *inv = calloc((size_t)(ncand > 0 ? ncand : 1), sizeof(float));
+  int64_t *order = malloc(sizeof(int64_t) * (size_t)(ncand > 0 ? ncand : 1));
+  for (int64_t q = 0; q < ncand; q++) inv[q] = 1.0f / ddd[q];
+  orc_argsort(ncand, inv, order);
+  const float esp = 0.2f * dxpa, esp_log = 1.05f;
+  int rc = 0;
+  for (int64_t l = 0; l < ncand && rc == 0; l++) {
+    const int64_t q = order[l] - 1;
+    const int ic = d4[4 * q], jc = d4[4 * q + 1], kc = d4[4 * q + 2];
+    const int ipatch = d4[4 * q + 3];
+    if (C1(ic, jc, kc, ipatch) == 0) continue;
+    float c3[3] = {RXL(0, ic, ipatch, dxpa), RXL(1, jc, ipatch, dxpa), RXL(2, kc, ipatch, dxpa)};
+    int ipf = ipatch + 1;
+    if (ir != m->nl) {
+      recenter_grid_peak(c3, ir, m, u11, dx, &ipf);
+      int dup = 0;
+      for (int q2 = nclus_ini; q2 < cat->nclus && !dup; q2++) {
+        const float ex = c3[0] - cat->clusrx[q2], ey = c3[1] - cat->clusry[q2], ez = c3[2] - cat->clusrz[q2];
+        dup = ex * ex + ey * ey + ez * ez < cat->rsub[q2] * cat->rsub[q2];
+      }
+      if (dup) continue;
+    }
+    const int host = find_host_halo(c3, ir, subs_lev, cat);
+    if (host < 0) continue;
+    const float hx = c3[0] - cat->clusrx[host], hy = c3[1] - cat->clusry[host], hz = c3[2] - cat->clusrz[host];
+    const float disthost = sqrtf(hx * hx + hy * hy + hz * hz);
+    if (disthost < 2.0f * dxpa) continue;
+    /* MHOST: the host's profile mass interpolated at DISTHOST in r^3 */
+    const float *pr1 = cat->profiles + (size_t)host * 2 * nb, *pm = pr1 + nb;
+    int nbp = nb;
+    for (int jj = 1; jj <= nb; jj++)
+      if (pr1[jj - 1] == 0.0f) { nbp = jj - 1; break; }
+    int jj = 1;
+    while (jj <= nbp && !(pr1[jj - 1] > disthost)) jj++;
+    float mhost;
+    if (jj == 1) {
+      const float t = disthost / pr1[0];
+      mhost = pm[0] * (t * t * t);
+    } else if (jj <= nbp) {
+      const float r1 = pr1[jj - 2], r2 = pr1[jj - 1];
+      mhost = pm[jj - 2] + (pm[jj - 1] - pm[jj - 2]) * (disthost * disthost * disthost - r1 * r1 * r1) /
+                               (r2 * r2 * r2 - r1 * r1 * r1);
+    } else {
+      mhost = pm[nbp - 1];
+    }
+    if (cat->nclus >= cat->capacity) { rc = -2; break; }
+    const int h = cat->nclus++;
+    cat->realclus[h] = host + 1;
+    cat->levhal[h] = ir;
+    cat->patchclus[h] = ipf;
+    cat->clusrx[h] = c3[0];
+    cat->clusry[h] = c3[1];
+    cat->clusrz[h] = c3[2];
+    float bx = 0.0f, by = 0.0f, bz = 0.0f, basdelta = 0.0f, basmass = 0.0f, basvol = 0.0f;
+    float r_int = 0.0f, r_ext = 0.8f * dxpa;
+    float delta = 10.0f * contrastec * rote;
+    int iter = 0, cells = 0, flag_vir = 0;
+    for (;;) {
+      iter++;
+      if (iter > 100000) { rc = -3; break; }  /* no cell ever counted: the reference loops for ever */
+      if (iter > 1) {
+        r_int = r_ext;
+        const float a1 = r_ext + esp, a2 = r_ext * esp_log;
+        r_ext = a1 > a2 ? a1 : a2;
+      }
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; a++) {
+        float bb = c3[a] - r_ext;
+        lo[a] = (int)(((bb - radx[1]) / dx) + 0.5f) + 1;
+        if (lo[a] < 1) lo[a] = 1;
+        bb = c3[a] + r_ext;
+        hi[a] = (int)(((bb - radx[1]) / dx) + 0.5f) + 1;
+        if (hi[a] > nx) hi[a] = nx;
+      }
+      bx = c3[0] + r_ext;  /* BASX..BASZ hold the upper box bounds when the sums start */
+      by = c3[1] + r_ext;
+      bz = c3[2] + r_ext;
+      float shell = 0.0f, volcell = dx * dx * dx;
+      for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+          for (int i = lo[0]; i <= hi[0]; i++) {
+            if (cr0amr[((size_t)(k - 1) * nx + (j - 1)) * nx + (i - 1)] != 1) continue;
+            const float ex = radx[i] - c3[0], ey = radx[j] - c3[1], ez = radx[k] - c3[2];
+            const float aa = sqrtf(ex * ex + ey * ey + ez * ez);
+            if (!(aa >= r_int && aa < r_ext)) continue;
+            cells++;
+            basvol = basvol + volcell;
+            const float b = u1[((size_t)(k - 1) * nx + (j - 1)) * nx + (i - 1)] * volcell;
+            shell = shell + b;
+            bx = bx + radx[i] * b;
+            by = by + radx[j] * b;
+            bz = bz + radx[k] * b;
+            basdelta = basdelta + b;
+          }
+      for (int irr = 1; irr <= ir; irr++) {   /* PATCHES_SPHERE up to level ir */
+        const float d = dx / powf(2.0f, (float)irr);
+        volcell = d * d * d;
+        for (int p = lev_lo[irr]; p < lev_lo[irr + 1]; p++) {
+          int meet = 1;
+          for (int a = 0; a < 3; a++) {
+            const float x3 = pr[a][p] - d, x4 = x3 + (float)pn[a][p] * d;
+            meet &= c3[a] - r_ext <= x4 && x3 <= c3[a] + r_ext;
+          }
+          if (!meet) continue;
+          for (int k = 1; k <= pn[2][p]; k++)
+            for (int j = 1; j <= pn[1][p]; j++)
+              for (int i = 1; i <= pn[0][p]; i++) {
+                if (MASK(cr0amr11, i, j, k, p) != 1 || MASK(solap, i, j, k, p) != 1) continue;
+                const float rx = RXL(0, i, p, d), ry = RXL(1, j, p, d), rz = RXL(2, k, p, d);
+                const float ex = rx - c3[0], ey = ry - c3[1], ez = rz - c3[2];
+                const float aa = sqrtf(ex * ex + ey * ey + ez * ez);
+                if (!(aa >= r_int && aa < r_ext)) continue;
+                cells++;
+                basvol = basvol + volcell;
+                const float b = U11(i, j, k, p) * volcell;
+                shell = shell + b;
+                bx = bx + rx * b;
+                by = by + ry * b;
+                bz = bz + rz * b;
+                basdelta = basdelta + b;
+                C1(i, j, k, p) = 0;
+              }
+        }
+      }
+      basmass = basmass + shell * rodo * (re0 * re0 * re0);
+      if (basvol > 0.0f) delta = basmass / (basvol * (rete * rete * rete));
+      if (flag_vir == 0 && delta < contrastec * rote) {
+        flag_vir = 1;
+        cat->masa[h] = basmass * um;
+        cat->radio[h] = r_ext * um;
+      }
+      const float mm = basmass * um;
+      const float eq = r_ext / disthost - powf(mm / (mm + 3.0f * mhost), 1.0f / 3.0f);
+      if (eq > 0.0f && cells > 15) {
+        cat->rsub[h] = r_ext;
+        cat->msub[h] = basmass * um;
+        break;
+      }
+    }
+    cat->clusrxcm[h] = bx / basdelta;
+    cat->clusrycm[h] = by / basdelta;
+    cat->clusrzcm[h] = bz / basdelta;
+  }
+#undef RXL
+#undef U11
+#undef MASK
+#undef C1
+  free(ddd);
+  free(d4);
+  free(inv);
+  free(order);
+  free(conta1);
+  free(lev_lo);
+  if (rc) return rc;
+  subs_lev[ir] = cat->nclus - nclus_ini;
+  return subs_lev[ir];
+}

@@ -358,3 +358,35 @@ def test_veinsgrid_known_answer():
     assert (a == 0).sum() == 64 + 3 * 28    # A's face cells among the facing ones (ix = 8, or on a y/z face)
     assert (b == 0).sum() == 256 - 148      # the other facing pairs drop B's cell
     assert (a[:, :, :4] == 1).all() and (b[:, :, 4:] == 1).all()
+
+
+def test_search_substructure_grid_known_answer():
+    """SEARCH_SUBSTRUCTURE_GRID (substructure.f:2-697): a top-hat peak on a
+    level-1 patch inside a base-level halo becomes one subhalo of that host,
+    grown until the Jacobi test R/d > (M/(M + 3 M_host(d)))^(1/3) holds."""
+    nx, lado0, na, nb = 32, 32.0, abi.NAMRX, abi.NBINS
+    radx, dx = grid.malla(nx, lado0)
+    mesh = synth.Mesh(1, np.array([0, 1], np.int32), *(np.array([32], np.int32) for _ in range(3)),
+                      *(np.array([9], np.int32) for _ in range(3)),
+                      *(np.array([radx[9]], np.float32) for _ in range(3)), np.array([0], np.int32))
+    u1 = np.ones((nx, nx, nx), np.float32)
+    cr0amr = np.ones((nx, nx, nx), np.int32)
+    cr0amr[8:24, 8:24, 8:24] = 0
+    u11 = _tophat_field(na, [((24, 16, 16), 3.0, 400.0)])[None]   # fine cell (25, 17, 17): (4.25, 0.25, 0.25)
+    ones = np.ones((1, na, na, na), np.int32)
+    cat = abi.Catalogue(16)
+    cat.nclus = 1                                   # the host, found at level 0
+    cat.realclus[0], cat.levhal[0] = -1, 0
+    cat.clusrx[0], cat.clusry[0], cat.clusrz[0], cat.radio[0] = -3.75, 0.25, 0.25, 10.0
+    r = 0.5 * np.arange(1, nb + 1, dtype=np.float32)
+    cat.profiles[0, :nb], cat.profiles[0, nb:] = r, 1000.0 * r   # M_host(r) = 1000 r
+    subs_lev = np.array([1, 0], np.int32)
+    n = O.OracleBackend().search_substructure_grid(1, nx, float(dx), u1, radx, mesh, u11, cr0amr, ones, ones, 200.0,
+                                                    1.0, 1.0, 1.0, 1.0, 1.0, subs_lev, cat)
+    assert n == 1 and cat.nclus == 2 and list(subs_lev) == [1, 1]
+    assert (cat.realclus[1], cat.levhal[1], cat.patchclus[1]) == (1, 1, 1)
+    assert (cat.clusrx[1], cat.clusry[1], cat.clusrz[1]) == (4.25, 0.25, 0.25)
+    d, rs, ms = 8.0, float(cat.rsub[1]), float(cat.msub[1])
+    assert 1.5 < rs < d
+    assert rs / d > (ms / (ms + 3 * 8000.0)) ** (1 / 3)     # the Jacobi test holds at R_SUB
+    assert 0 < cat.radio[1] < rs                              # the virial radius comes first
