@@ -73,7 +73,19 @@ def make_mesh_and_grid_finder(s, r):
     na1 = ob.halofind_grid_amr(1, cfg.nx, dx, r.u1, plan.radx, m1, u11_1, c0, c11, so, 200.0, 1.0, 1.0, 1.0, 1.0,
                                10.0 * dx, 0.2, g)
     k = g.nclus
-    amr = {"gridamr_cr0amr_sha256": np.array([digest(c0)]), "gridamr_solap_sha256": np.array([digest(so)]),
+    # subhalo seeding on level 1 inside the haloes of the particle pipeline's catalogue
+    sc = abi.Catalogue(r.cat.capacity + 4096)
+    nh = int(r.subs_lev[0]) if len(r.subs_lev) else r.cat.nclus
+    sc.nclus = nh
+    for f in ("realclus", "levhal", "clusrx", "clusry", "clusrz", "radio", "rsub", "masa", "msub", "profiles"):
+        getattr(sc, f)[:nh] = getattr(r.cat, f)[:nh]
+    sl = np.zeros(2, np.int32)
+    sl[0] = nh
+    ns = ob.search_substructure_grid(1, cfg.nx, dx, r.u1, plan.radx, m1, u11_1, c0, c11, so, 200.0, 1.0, 1.0, 1.0,
+                                     1.0, 1.0, sl, sc)
+    sub = {"gridsub_n": np.array([ns]), "gridsub_realclus": sc.realclus[nh:sc.nclus].copy(),
+           "gridsub_rsub": sc.rsub[nh:sc.nclus].copy(), "gridsub_clusrx": sc.clusrx[nh:sc.nclus].copy()}
+    amr = {**sub, "gridamr_cr0amr_sha256": np.array([digest(c0)]), "gridamr_solap_sha256": np.array([digest(so)]),
            "gridamr_nhallev": np.array([n0, na1]), "gridamr_levhal": g.levhal[:k].copy(),
            "gridamr_realclus": g.realclus[:k].copy(), "gridamr_radio": g.radio[:k].copy(),
            "gridamr_clusrx": g.clusrx[:k].copy(), "gridamr_patchclus": g.patchclus[:k].copy()}
