@@ -6,17 +6,35 @@
 // later cudaMalloc, or code that must not trigger the device-wide
 // synchronisation that cudaMalloc/cudaFree can cause.  For them the float64
 // accumulator this deposit needs lives in a fixed file-scope device array of
-// ASOHF_NOALLOC_MAX_CELLS cells (16 MiB, held by every GPU that loads the
-// library until the process exits), and the entry point neither allocates
-// nor frees anything.
+// ASOHF_NOALLOC_MAX_CELLS cells (16 MiB), and the entry point neither
+// allocates nor frees anything.
+//
+// With CUDA's lazy module loading (the default since CUDA 12.2) the array and
+// the two kernels are placed on a device when this module is first used
+// there, not when the library is loaded.  The first call on each device
+// therefore does that set-up (symbol lookup plus a load of both kernels); it
+// is the one call that can need device memory, and must come before the
+// application reserves its memory and before any stream capture.  A call with
+// n = 0 is enough.  From then on the array is held on that device until the
+// process exits.
+#include <atomic>
+#include <mutex>
+
 #include "common.cuh"
 
 static __device__ __align__(256) double g_noalloc_acc[ASOHF_NOALLOC_MAX_CELLS];
 
-// Per-device address of g_noalloc_acc (host code may not use the symbol's
-// host-side stand-in as a device address).
-static double* g_acc_addr[64];
-static bool g_acc_ready[64];
+// Per-device set-up results.  Host code may not use the array's host-side
+// stand-in as a device address, so the address comes from
+// cudaGetSymbolAddress, looked up once per device with that device current.
+// Readers take the published pointer with acquire ordering; the set-up runs
+// under a mutex and publishes with release ordering, after the SM count.
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+std::atomic<double*> g_acc_addr[kMaxDevices];
+int g_sm_count[kMaxDevices];
+}  // namespace
 
 struct Level0Kernel {
   float w[3];  // W(-1), W(0), W(1) of COMPUTE_KERNELS level 0
@@ -91,6 +109,21 @@ __global__ void k_finish_noalloc(const double* __restrict__ acc, int64_t g, floa
     u1[c] = (float)acc[c] / denbas;
 }
 
+// Loads the array and both kernels on device `dev` (current) and records the
+// array's device address and the SM count.  Called under g_setup_mutex.
+static int noalloc_setup(int dev) {
+  double* addr = nullptr;
+  ASOHF_CUDA(cudaGetSymbolAddress((void**)&addr, g_noalloc_acc));
+  cudaFuncAttributes fa;
+  ASOHF_CUDA(cudaFuncGetAttributes(&fa, k_density_base_noalloc));
+  ASOHF_CUDA(cudaFuncGetAttributes(&fa, k_finish_noalloc));
+  int sms = 0;
+  ASOHF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  g_sm_count[dev] = sms > 0 ? sms : 1;
+  g_acc_addr[dev].store(addr, std::memory_order_release);
+  return ASOHF_OK;
+}
+
 extern "C" int asohf_density_base_noalloc(int nx, float lado0, float dx, float rote, float rete,
                                           int interp_degree, int64_t n, const float* x,
                                           const float* y, const float* z, const float* m,
@@ -101,28 +134,43 @@ extern "C" int asohf_density_base_noalloc(int nx, float lado0, float dx, float r
   int64_t g = (int64_t)nx * nx * nx;
   if (g > (int64_t)ASOHF_NOALLOC_MAX_CELLS) return ASOHF_ERR_CAPACITY;
   int dev = 0;
-  ASOHF_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return ASOHF_ERR_INVALID;
-  if (!g_acc_ready[dev]) {
-    // once per device, with that device current
-    ASOHF_CUDA(cudaGetSymbolAddress((void**)&g_acc_addr[dev], g_noalloc_acc));
-    g_acc_ready[dev] = true;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) {
+    cudaGetLastError();
+    return ASOHF_ERR_NO_DEVICE;
   }
-  double* acc = g_acc_addr[dev];
+  ASOHF_CUDA(e);
+  if (dev < 0 || dev >= kMaxDevices) return ASOHF_ERR_INVALID;
   cudaStream_t s = (cudaStream_t)cuda_stream;
+  if (s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread) {
+    // the array's address is per device: the stream must run on the current one
+    int sdev = -1;
+    ASOHF_CUDA(cudaStreamGetDevice(s, &sdev));
+    if (sdev != dev) return ASOHF_ERR_INVALID;
+  }
+  double* acc = g_acc_addr[dev].load(std::memory_order_acquire);
+  if (!acc) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    acc = g_acc_addr[dev].load(std::memory_order_acquire);
+    if (!acc) {
+      ASOHF_CHECK(noalloc_setup(dev));
+      acc = g_acc_addr[dev].load(std::memory_order_acquire);
+    }
+  }
+  const int max_blocks = g_sm_count[dev] * 16;
   // the array keeps the previous call's sums: clear the cells this grid uses
   ASOHF_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * (size_t)g, s));
   if (n > 0) {
-    int blocks = (int)((n + 255) / 256);
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    k_density_base_noalloc<<<blocks, 256, 0, s>>>(x, y, z, m, n, nx, -lado0 / 2.0f, dx,
-                                                  level0_kernel(interp_degree), acc);
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > max_blocks) blocks = max_blocks;
+    k_density_base_noalloc<<<(int)blocks, 256, 0, s>>>(x, y, z, m, n, nx, -lado0 / 2.0f, dx,
+                                                       level0_kernel(interp_degree), acc);
     ASOHF_CUDA(cudaGetLastError());
   }
   float denbas = dx * dx * dx * rote * (rete * rete * rete);
-  int fb = (int)((g + 255) / 256);
-  if (fb > 148 * 16) fb = 148 * 16;
-  k_finish_noalloc<<<fb, 256, 0, s>>>(acc, g, denbas, u1);
+  int64_t fb = (g + 255) / 256;
+  if (fb > max_blocks) fb = max_blocks;
+  k_finish_noalloc<<<(int)fb, 256, 0, s>>>(acc, g, denbas, u1);
   ASOHF_CUDA(cudaGetLastError());
   return ASOHF_OK;
 }

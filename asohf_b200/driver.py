@@ -7,8 +7,9 @@ prepared before the hot path runs (``prepare``): the patch table
 (CREATE_MESH) and the halo candidates (HALOFIND_GRID).  Subhalo candidates
 (SEARCH_SUBSTRUCTURE_GRID) are listed during the run, once the host haloes
 are known.  The catalogue cleaning passes CHECK_RUBISH and
-ACCIDENTAL_SUBSTRUCTURE are not run.  RE_SORT_HALOES (haloes_particles.f:
-2-56), a compaction of the candidate list, is done here on the host.
+ACCIDENTAL_SUBSTRUCTURE run on the backend after each level's refinement,
+as asohf.f:669-675 calls them.  RE_SORT_HALOES (haloes_particles.f:2-56),
+a compaction of the candidate list, is done here on the host.
 """
 from __future__ import annotations
 

@@ -233,14 +233,19 @@ int asohf_substructure_particles(asohf_ctx *ctx, const asohf_consts *k, const as
  * code that must avoid the device synchronisation cudaMalloc/cudaFree can
  * cause.  It allocates nothing and needs no context: x, y, z, m (n
  * particles) and u1 (nx^3, column-major) are the caller's device pointers,
- * cuda_stream the stream to run on.  Its float64 scratch is a fixed
- * file-scope device array of ASOHF_NOALLOC_MAX_CELLS cells (16 MiB on every
- * GPU that loads the library, until exit); grids with more cells are refused
- * with ASOHF_ERR_CAPACITY.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture.  Every call shares the array and
- * clears the part it uses: calls that overlap on the GPU (other streams,
- * other host threads) race. */
+ * cuda_stream a stream of the current device (0 for the default stream;
+ * another device's stream is refused with ASOHF_ERR_INVALID).  Its float64
+ * scratch is a fixed file-scope device array of ASOHF_NOALLOC_MAX_CELLS
+ * cells (16 MiB); grids with more cells are refused with
+ * ASOHF_ERR_CAPACITY.  Under CUDA's default lazy module loading that array
+ * and the two kernels are placed on a device at the first call there, not
+ * at library load: the first call on each device (n = 0 is enough) does this
+ * set-up and is the only one that may need device memory, so make it before
+ * the application reserves its device memory and before any stream capture.
+ * The array then stays on that device until the process exits.  Every call
+ * shares the array and clears the part it uses: calls that overlap on the
+ * GPU (other streams, other host threads) race.  Without a usable device it
+ * returns ASOHF_ERR_NO_DEVICE. */
 #define ASOHF_NOALLOC_MAX_CELLS (128 * 128 * 128)
 int asohf_density_base_noalloc(int nx, float lado0, float dx, float rote, float rete,
                                int interp_degree, int64_t n, const float *x, const float *y,

@@ -106,6 +106,12 @@ int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx,
 /* HALOFIND_PARTICLES for haloes low1..low2 (Fortran 1-based, inclusive).
  * The bound-particle ID stream is written to pph (capacity pph_cap) and the
  * total used length returned in *pph_len.  Returns a status code. */
+/* Decision-margin counts (test instrumentation): rows4 receives, per
+ * catalogue row, 4 counts of particle tests within a relative 1e-6 of their
+ * threshold (sphere membership, overdensity, escape energy, velocity
+ * dispersion), added by orc_halofind_particles and
+ * orc_substructure_particles; NULL switches the counting off. */
+void orc_set_margin_counts(int32_t *rows4, int64_t cap);
 int orc_halofind_particles(const orc_store *st, const asohf_consts *k,
                            const asohf_mesh *mesh, asohf_catalogue *cat,
                            int low1, int low2, int32_t *pph, int64_t pph_cap,

@@ -126,6 +126,33 @@ class Particles:
         return cls(s.x, s.y, s.z, s.vx, s.vy, s.vz, s.m, s.id)
 
 
+class MarginCounts:
+    """Decision-margin counts of the oracle's halo and subhalo refinement
+    (orc_set_margin_counts): per catalogue row, the particle tests within a
+    relative 1e-6 of their threshold -- [0] growth-sphere membership,
+    [1] overdensity (virial index, SO walk, subhalo Jacobi estimate),
+    [2] escape energy (UNBINDING8), [3] velocity dispersion
+    (UNBINDING_SIGMA).  Use as a context manager around the oracle calls."""
+
+    KINDS = ("membership", "overdensity", "escape_energy", "dispersion")
+
+    def __init__(self, capacity: int):
+        self.rows = np.zeros((int(capacity), 4), np.int32)
+
+    def __enter__(self):
+        lib().orc_set_margin_counts(P(self.rows, _ip), C.c_int64(self.rows.shape[0]))
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_margin_counts(None, C.c_int64(0))
+        return False
+
+    def totals(self, rows=None) -> dict:
+        r = self.rows if rows is None else self.rows[rows]
+        t = r.sum(axis=0)
+        return {k: int(v) for k, v in zip(self.KINDS, t)}
+
+
 class OracleBackend:
     """Runs each hot-path routine on the CPU oracle.  Methods mirror the
     reference subroutines; arrays are numpy, Fortran layouts."""

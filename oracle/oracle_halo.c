@@ -21,6 +21,36 @@
 
 #define NB ASOHF_NBINS
 
+/* Decision margins (test instrumentation, off unless a buffer is set):
+ * for each catalogue row, the number of particle tests whose two sides lie
+ * within a relative 1e-6 of each other -- the particles whose decision a
+ * last-bit difference in the arithmetic could flip.  Four counts per row:
+ * [0] membership of the growth sphere (distance vs radius, final iteration),
+ * [1] overdensity thresholds (FIND_IDX_VIR, the SO walk, the subhalo Jacobi
+ *     estimate), [2] UNBINDING8's escape-energy test, [3] UNBINDING_SIGMA's
+ * velocity-dispersion test.  Each row is refined by one thread, so the
+ * counts need no atomics. */
+#define MARGIN_REL 1e-6
+static int32_t *g_margin = NULL;
+static int64_t g_margin_cap = 0;
+static _Thread_local int64_t g_row = -1;
+
+void orc_set_margin_counts(int32_t *rows4, int64_t cap)
+{
+  g_margin = rows4;
+  g_margin_cap = rows4 ? cap : 0;
+}
+
+static inline void margin_add(int kind, int64_t n)
+{
+  if (g_margin && g_row >= 0 && g_row < g_margin_cap && n) g_margin[g_row * 4 + kind] += (int32_t)n;
+}
+
+static inline int near_thr(double a, double thr)
+{
+  return fabs(a - thr) <= MARGIN_REL * fabs(thr);
+}
+
 /* FIND_PARTICLE_INDICES (haloes_particles.f:117-143).  lowp1/lowp2 are
  * 1-based inclusive positions in the x-sorted store. */
 void orc_find_particle_indices(float cx, float r, float xldom, float dx, int nmax,
@@ -413,6 +443,7 @@ static int64_t find_idx_vir(const orc_store *st, const hwork *w, float rote, flo
     float d = w->dista[j];
     float den = rote * (rete * rete * rete) * (4.0f * pi / 3.0f) * (d * d * d);
     float delta = (float)(menc / (double)den);
+    margin_add(1, near_thr(delta, contrastec));
     if (delta < contrastec) break;
   }
   if (j == idx_vir + 1) return -1;
@@ -503,6 +534,7 @@ static void unbinding8(const orc_store *st, const asohf_consts *k, int fac, floa
       int64_t p = w->lip[j];
       float ax = st->vx[p] - *h->vx, ay = st->vy[p] - *h->vy, az = st->vz[p] - *h->vz;
       float vvv2 = ax * ax + ay * ay + az * az;
+      margin_add(2, near_thr(vvv2, bb * vesc2));
       if (vvv2 > bb * vesc2) w->contadm[j] = 1;
     }
     free(pot);
@@ -533,8 +565,10 @@ static void unbinding_sigma(const orc_store *st, const asohf_consts *k, int fac,
       if (j <= idx_vir) sigma2 = sigma2 + (double)bas;
     }
     if (idx_vir > 1) sigma2 = sigma2 / (double)(idx_vir - 1);
-    for (int64_t j = 1; j <= konta2; j++)
+    for (int64_t j = 1; j <= konta2; j++) {
+      margin_add(3, near_thr((double)desv2[j], (double)bb * sigma2));
       if ((double)desv2[j] > (double)bb * sigma2) w->contadm[j] = 1;
+    }
     free(desv2);
     centromasas(st, idx_vir, w, cm, vcm, &mmm);
   }
@@ -765,6 +799,7 @@ static int properties(const orc_store *st, const asohf_consts *k, asohf_catalogu
 static inline void so_hit(int *flag, float delta2, float thr, float vol, float rote, float um,
                           float d, int64_t j, int64_t jjcore, float *mo, float *ro)
 {
+  if (*flag == 0) margin_add(1, near_thr(delta2, thr));
   if (*flag == 0 && delta2 <= thr) {
     *mo = delta2 * vol * rote * um;
     *ro = d;
@@ -778,6 +813,7 @@ static int halofind_one(const orc_store *st, const asohf_consts *k, const asohf_
                         asohf_catalogue *cat, int I, ilist *ids)
 {
   int i0 = I - 1;
+  g_row = i0;
   int kk_entero = cat->realclus[i0];
   if (kk_entero == 0) return 0;
   float pi = k->pi, rote = k->rote, rete = k->rete, fdm = k->fdm, um = k->um;
@@ -804,14 +840,17 @@ static int halofind_one(const orc_store *st, const asohf_consts *k, const asohf_
   float delta2 = 100.0f * minoverdens;
   double masadm = 0.0;
   ilist lip = {0};
+  int64_t near_r = 0;
   while (delta2 > 0.99f * minoverdens) {
     lip.n = 0;
     masadm = 0.0;
+    near_r = 0;
     float bas = -1.0f;
     int64_t lo, hi;
     orc_find_particle_indices(cx, rclus, xldom, k->dx, k->nx, st->ndmpart_x, &lo, &hi);
     for (int64_t j = lo; j <= hi; j++) {
       float aadm = dist3(st, j - 1, cx, cy, cz);
+      near_r += near_thr(aadm, rclus);
       if (aadm < rclus) {
         il_push(&lip, j - 1);
         masadm = masadm + (double)st->m[j - 1];
@@ -822,6 +861,7 @@ static int halofind_one(const orc_store *st, const asohf_consts *k, const asohf_
     delta2 = (float)(masadm / (double)den);
     if (delta2 > 0.9f * minoverdens) rclus = 1.25f * rclus;
   }
+  margin_add(0, near_r);
   int64_t konta = lip.n;
   if (masadm <= 0.0 || konta == 0) {
     cat->realclus[i0] = 0;
@@ -917,6 +957,7 @@ static int halofind_one(const orc_store *st, const asohf_consts *k, const asohf_
     so_hit(&f2500m, delta2, m2500, vol, rote, um, d, j, jjcore, &cat->m2500m[i0], &cat->r2500m[i0]);
     so_hit(&f500m, delta2, m500, vol, rote, um, d, j, jjcore, &cat->m500m[i0], &cat->r500m[i0]);
     so_hit(&f200m, delta2, m200, vol, rote, um, d, j, jjcore, &cat->m200m[i0], &cat->r200m[i0]);
+    if (fvir == 0 && j > jvir_min) margin_add(1, near_thr(delta2, cvir));
     if (fvir == 0 && delta2 <= cvir && j > jvir_min) {
       salida = 1;
       fvir = 1;
@@ -1036,6 +1077,7 @@ static int substructure_one(const orc_store *st, const asohf_consts *k, const as
                             asohf_catalogue *cat, int I, ilist *ids)
 {
   int i0 = I - 1;
+  g_row = i0;
   int kk_entero = cat->realclus[i0];
   if (kk_entero == 0) return 0;
   float pi = k->pi, rote = k->rote, rete = k->rete, um = k->um;
@@ -1084,12 +1126,18 @@ static int substructure_one(const orc_store *st, const asohf_consts *k, const as
   int64_t konta = 0, konta2 = 0, useless = 0;
   int flag_jacobi = 0;
   float rclus = 2.0f * cat->rsub[i0];
+  int64_t near_r = 0, near_jac = 0;
   while (flag_jacobi == 0) {
     ilist lip = {0};
     int64_t lo, hi;
+    near_r = 0;
+    near_jac = 0;
     orc_find_particle_indices(cx, rclus, xldom, k->dx, k->nx, st->ndmpart_x, &lo, &hi);
-    for (int64_t j = lo; j <= hi; j++)
-      if (dist3(st, j - 1, cx, cy, cz) < rclus) il_push(&lip, j - 1);
+    for (int64_t j = lo; j <= hi; j++) {
+      float aadm = dist3(st, j - 1, cx, cy, cz);
+      near_r += near_thr(aadm, rclus);
+      if (aadm < rclus) il_push(&lip, j - 1);
+    }
     konta = lip.n;
     if (w.lip) hw_free(&w);
     int64_t cap = konta;
@@ -1106,7 +1154,9 @@ static int substructure_one(const orc_store *st, const asohf_consts *k, const as
     for (j = 1; j <= konta; j++) {
       masadm = masadm + (double)st->m[w.lip[j]];
       double mu = masadm * (double)um;
-      double eq = (double)(w.dista[j] / disthost) - pow(mu / (mu + (double)(3.0f * mhost)), (double)(1.0f / 3.0f));
+      double tid = pow(mu / (mu + (double)(3.0f * mhost)), (double)(1.0f / 3.0f));
+      double eq = (double)(w.dista[j] / disthost) - tid;
+      if (j > minj) near_jac += near_thr(tid + eq, tid);
       if (eq > 0.0 && j > minj) { j_jacobi = j; break; }
     }
     if (j_jacobi == -1) j_jacobi = konta;
@@ -1151,6 +1201,8 @@ static int substructure_one(const orc_store *st, const asohf_consts *k, const as
       konta = j_jacobi;
     }
   }
+  margin_add(0, near_r);
+  margin_add(1, near_jac);
   if (masadm <= 0.0 || konta < k->min_num_part) {
     cat->realclus[i0] = 0;
     hw_free(&w);
@@ -1258,6 +1310,7 @@ static int substructure_one(const orc_store *st, const asohf_consts *k, const as
     so_hit(&f2500m, delta2, 2500.0f, vol, rote, um, d, j, jjcore, &cat->m2500m[i0], &cat->r2500m[i0]);
     so_hit(&f500m, delta2, 500.0f, vol, rote, um, d, j, jjcore, &cat->m500m[i0], &cat->r500m[i0]);
     so_hit(&f200m, delta2, 200.0f, vol, rote, um, d, j, jjcore, &cat->m200m[i0], &cat->r200m[i0]);
+    if (fvir == 0 && j > jvir_min) margin_add(1, near_thr(delta2, k->contrastec));
     if (fvir == 0 && delta2 <= k->contrastec && j > jvir_min) {
       fvir = 1;
       cat->masa[i0] = delta2 * vol * rote * um;

@@ -50,6 +50,12 @@ def test_no_device_fails_loudly():
     else:
         assert rc == 7  # ASOHF_ERR_NO_DEVICE
         assert "device" in L.asohf_strerror(rc).decode().lower()
+        # the context-free entry point reports the same status
+        dummy = ctypes.c_float()
+        fn = L.asohf_density_base_noalloc
+        rc = fn(1, ctypes.c_float(1.0), ctypes.c_float(1.0), ctypes.c_float(1.0), ctypes.c_float(1.0), 2,
+                ctypes.c_int64(0), None, None, None, None, ctypes.byref(dummy), None)
+        assert rc == 7
 
 
 def test_cleaning_and_mesh_entry_points_reject_a_null_context():

@@ -1,15 +1,26 @@
-"""Size-independent checks of the hot path at the benchmark size: the
-512^3-particle snapshot (250 Mpc/h, 6 AMR levels, 2e5 haloes and their
-subhaloes) run through the device-resident path, where the CPU oracle would
-take minutes.  Checked: mass conservation of the base-grid deposit, the
+"""The hot path at the benchmark size: the 512^3-particle snapshot (250
+Mpc/h, 6 AMR levels, 2e5 haloes and their subhaloes) run through the
+device-resident path.
+
+Size-independent checks: mass conservation of the base-grid deposit, the
 x-slab sort (sorted store, consistent NDMPART_X), and the catalogue
 (consistent INDCS ranges over the ID stream, IDs valid and unique within
 each halo, bound counts above MIN_NUM_PART, positive masses and radii,
-centres in the box)."""
+centres in the box).
+
+Parity on a window: the oracle would take too long on every halo, so it
+reruns, on the same x-sorted store, a seeded window of rows from every
+HALOFIND_PARTICLES and SUBSTRUCTURE_PARTICLES call of the run -- the 20
+largest of each call, every halo of the thread-block-cluster tier (32768
+members and more) and 200 others drawn at random -- and each row must equal
+the device's (integer fields and ID lists identical, floats within 1e-5),
+unless the oracle counted a particle test within a relative 1e-6 of its
+threshold in that row.  The margin counts are printed with the result."""
 import numpy as np
 import pytest
 
 from asohf_b200 import api, driver, grid, synth
+from tests import window_parity as W
 
 pytestmark = pytest.mark.gpu
 
@@ -22,8 +33,10 @@ def run512(gpu_lib):
     plan = driver.prepare(snap)
     b = api.DeviceBackend(0)
     b.a.set_stream(torch.cuda.current_stream().cuda_stream)
-    r = driver.execute(plan, b, with_subs=True, download=False)
+    rec = W.Recorder(b)
+    r = driver.execute(plan, rec, with_subs=True, download=False)
     torch.cuda.synchronize()
+    b.calls = rec.calls
     return cfg, snap, plan, b, r
 
 
@@ -103,3 +116,37 @@ def test_catalogue_and_id_stream(run512):
     assert bool((vals >= 1).all()) and bool((vals <= snap.x.shape[0]).all())
     key = torch.sort(owner * (1 << 32) + vals).values
     assert bool((key[1:] != key[:-1]).all())
+
+
+def test_window_matches_oracle(run512):
+    import json
+    import torch
+    cfg, snap, plan, b, r = run512
+    n = snap.x.shape[0]
+    out = [torch.empty(n, dtype=torch.float32, device="cuda:0") for _ in range(7)] + \
+          [torch.empty(n, dtype=torch.int32, device="cuda:0")]
+    b.a.download_particles(out)
+    torch.cuda.synchronize()
+    store = W.OracleStore(*(t.cpu().numpy() for t in out), r.ndmpart_x)
+    del out
+    rng = np.random.default_rng(20261203)
+    reports = []
+    for call in b.calls:
+        rows = W.choose_rows(call, rng)
+        if rows.size == 0:
+            continue
+        ocat, opph, margins = W.run_oracle_rows(call, rows, store, plan.consts, plan.mesh)
+        reports.append(W.compare_rows(call, rows, ocat, opph, margins))
+    tot = {k: sum(rep["margins"][k] for rep in reports) for k in reports[0]["margins"]}
+    summary = {"calls": len(reports), "rows": sum(rep["rows"] for rep in reports),
+               "bound_ids": sum(rep["bound_ids"] for rep in reports),
+               "largest_rows_members": int(max(int(c.post.dmpclus[c.low1 - 1:c.low2].max(initial=0))
+                                               for c in b.calls)),
+               "margins_1e-6": tot,
+               "rows_with_margin": sum(rep["rows_with_margin"] for rep in reports),
+               "explained_mismatches": {f"{rep['kind']}{rep['low1']}": rep["explained"] for rep in reports
+                                        if rep["explained"]}}
+    print("parity-512-window", json.dumps(summary))
+    unexplained = {f"{rep['kind']}{rep['low1']}": rep["unexplained"] for rep in reports if rep["unexplained"]}
+    assert not unexplained, unexplained
+    assert summary["rows"] > 1000
