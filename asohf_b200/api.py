@@ -117,6 +117,10 @@ class Asohf:
     def launch_count(self) -> int:
         return int(self.L.asohf_launch_count(self.h))
 
+    def set_epot_seed(self, seed: int):
+        """Seed of COMPUTE_EPOT's sampling estimator (default 1)."""
+        _check(self.L.asohf_set_epot_seed(self.h, C.c_uint32(int(seed))), "asohf_set_epot_seed")
+
     def set_cluster_threshold(self, min_members: int):
         """Haloes with at least min_members members go to the cluster path
         (0: default)."""

@@ -53,6 +53,8 @@ struct asohf_ctx {
   int64_t cluster_min = 32768;
   int64_t cluster_share = 32768;  // entries per CTA that set the halo kernel's cluster width
   int64_t tier2_k = 2048, tier1_k = 256;
+  // seed of COMPUTE_EPOT's sampling estimator (asohf_set_epot_seed)
+  uint32_t epot_seed = 1;
   DevParticles p;      // current store
   DevParticles alt;    // second buffer set for permutations
   // The store as rows (x, y, z, m | vx, vy, vz, id bits), 2 float4 per

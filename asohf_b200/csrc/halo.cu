@@ -1242,10 +1242,122 @@ __device__ void epot_direct_g(const Grp<C>& g, const SegView& v, const uint8_t* 
   *jbest = best_j;
 }
 
+// COMPUTE_EPOT's sampling branch (haloes_particles.f:1568-1626), for bound
+// lists of MAX_PART_DSUM entries or more.  NSAMPLE = MAX(INT(MAX_PART_DSUM
+// /1.4), INT(0.01*KONTA2)) draws of a bound entry J, each paired with
+// NSAMPLE draws of a bound entry K != J, all uniform over the KONTA scanned
+// entries with rejection of the unbound ones (J = 1 + FLOOR(U*KONTA)).
+// Per draw J the REAL*8 sum BAS of the REAL*4 terms -m_J m_K / r_JK; EPOT8
+// is the sum of the BAS in draw order scaled by FLOAT(KONTA(KONTA-1)/2) /
+// FLOAT(NSAMPLE^2); the most bound entry is the J whose BAS/m_J first beats
+// the running minimum, that minimum being kept in REAL*4 as the reference
+// keeps LARGEST_ENERGY.
+//
+// The reference's U comes from RANDOM_NUMBER after an unseeded RANDOM_SEED
+// (irreproducible).  Here U is counter-based: bits = mix(key_outer, inner +
+// 0x9E3779B9 * attempt) with key_outer = mix(key_row, outer), key_row =
+// mix(seed, row), mix(a, b) = fmix32(a ^ fmix32(b)) and fmix32 the
+// MurmurHash3 32-bit finaliser, and U = (bits >> 8) * 2^-24 (24 bits, exact
+// in REAL*4).  outer is the 1-based draw of J, inner 0 for J itself and
+// 1..NSAMPLE for its partners, attempt counts the rejections.  Every draw J
+// is summed by one thread in the reference's order and the final sum and
+// minimum are taken by one thread in draw order, so the result equals the
+// oracle's sequential loop bit for bit.  The BAS, BAS/m and J of each draw
+// are kept in the halo's potential array and in its spare member-list set
+// (free once the member list is final).  A draw that finds no bound entry
+// after EPOT_MAX_ATTEMPTS tries makes the call return 1 (the caller reports
+// ASOHF_ERR_TIMEOUT); the reference would loop on.
+#define EPOT_MAX_ATTEMPTS 4096u
+
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+__device__ __forceinline__ uint32_t mix2(uint32_t a, uint32_t b) { return fmix32(a ^ fmix32(b)); }
+
+// 0-based entry J-1 of one draw (clamped to the list: U*KONTA can round up
+// to KONTA in REAL*4)
+__device__ __forceinline__ int64_t epot_draw(uint32_t key_outer, uint32_t inner, uint32_t attempt, int64_t konta) {
+  const uint32_t bits = mix2(key_outer, inner + 0x9E3779B9u * attempt);
+  const float u = __fmul_rn((float)(bits >> 8), 5.9604644775390625e-8f);
+  const int64_t j = (int64_t)floorf(__fmul_rn(u, (float)konta));
+  return j < konta ? j : konta - 1;
+}
+
+template <int C>
+__device__ int epot_sample_g(const Grp<C>& g, const SegView& v, const SegView& spare, double* pot,
+                             const uint8_t* flag, int64_t konta, long long konta2, int max_part_dsum,
+                             uint32_t key_row, double* epot8, long long* jbest, GShared& sh) {
+  const int64_t ns_a = (int64_t)__fdiv_rn((float)max_part_dsum, 1.4f);
+  const int64_t ns_b = (int64_t)__fmul_rn(0.01f, (float)konta2);
+  const int64_t nsample = ns_a > ns_b ? ns_a : ns_b;
+  double* bas_m = reinterpret_cast<double*>(spare.dm);   // 8 B per entry
+  int32_t* jsel = reinterpret_cast<int32_t*>(spare.mv);   // 16 B per entry
+  const int64_t tid = (int64_t)g.rank() * blockDim.x + threadIdx.x;
+  const int64_t nth = (int64_t)(C > 1 ? C : 1) * blockDim.x;
+  int bad = 0;
+#pragma unroll 1
+  for (int64_t o = tid; o < nsample && !bad; o += nth) {
+    const uint32_t ko = mix2(key_row, (uint32_t)(o + 1));
+    int64_t j = -1;
+    for (uint32_t a = 0; a < EPOT_MAX_ATTEMPTS; a++) {
+      const int64_t c = epot_draw(ko, 0u, a, konta);
+      if (flag[c]) { j = c; break; }
+    }
+    if (j < 0) { bad = 1; break; }
+    const float4 pj = v.px[j];
+    const float m1 = v.mv[j].x;
+    double bas = 0.0;
+#pragma unroll 1
+    for (int64_t q = 1; q <= nsample; q++) {
+      int64_t kq = -1;
+      for (uint32_t a = 0; a < EPOT_MAX_ATTEMPTS; a++) {
+        const int64_t c = epot_draw(ko, (uint32_t)q, a, konta);
+        if (flag[c] && c != j) { kq = c; break; }
+      }
+      if (kq < 0) { bad = 1; break; }
+      const float4 pk = v.px[kq];
+      const float m2 = v.mv[kq].x;
+      const float ax = __fsub_rn(pj.x, pk.x), ay = __fsub_rn(pj.y, pk.y), az = __fsub_rn(pj.z, pk.z);
+      const float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az)));
+      bas = bas - (double)__fdiv_rn(__fmul_rn(m1, m2), r);
+    }
+    pot[o] = bas;
+    bas_m[o] = bas / (double)m1;
+    jsel[o] = (int32_t)j;
+  }
+  double anybad = (double)bad;
+  gsum_dv<1>(g, &anybad, sh.x);
+  __threadfence();
+  g.sync();
+  if (anybad != 0.0) return 1;
+  if (g.rank() == 0 && threadIdx.x == 0) {
+    double e = 0.0;
+    float lmin = 1000000.0f;
+    long long best = 0;
+    for (int64_t o = 0; o < nsample; o++) {
+      e = e + pot[o];
+      const double b = bas_m[o];
+      if (b < (double)lmin) { lmin = (float)b; best = jsel[o]; }
+    }
+    const long long npt = (long long)konta * (long long)(konta - 1) / 2;
+    const long long npr = (long long)nsample * (long long)nsample;
+    *epot8 = e * (double)__fdiv_rn((float)npt, (float)npr);
+    *jbest = best;
+  }
+  return 0;
+}
+
 template <int C, bool SYM = true>
 __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
                                   const SegView& v, uint8_t* flag, int64_t konta, float rshell, float cx, float cy,
-                                  float cz, const float* cmv, GShared& sh, int* unsupported) {
+                                  float cz, const float* cmv, GShared& sh, int* unsupported, const SegView& spare,
+                                  double* pot) {
   float norma = S.norma;
   float vc[3] = {cat.vx[i0], cat.vy[i0], cat.vz[i0]};
   int64_t each_prof = konta / ASOHF_NBINS;
@@ -1309,17 +1421,18 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
   vmax = gmax_f(g, vmax, sh.fred, sh.x);
   long long cnt = (long long)r2[2];
   // energies (haloes_particles.f:1297-1316): kinetic sum of the bound
-  // entries, potential by direct summation below MAX_PART_DSUM entries (the
-  // reference samples above it with an unseeded generator: not reproduced,
-  // reported as unsupported)
+  // entries, potential by direct summation below MAX_PART_DSUM entries and
+  // by the seeded sampling estimator from there on
   double ekin = acc[1], epot8 = 0.0;
   long long jmb = 0;
   *unsupported = 0;
   if (H.energies && cnt >= H.min_num_part) {
+    gsum_dv<1>(g, &ekin, sh.x);
     if (cnt >= H.max_part_dsum) {
-      *unsupported = 1;
+      const uint32_t key_row = mix2(H.epot_seed, (uint32_t)i0);
+      if (epot_sample_g(g, v, spare, pot, flag, konta, cnt, H.max_part_dsum, key_row, &epot8, &jmb, sh))
+        *unsupported = 2;
     } else {
-      gsum_dv<1>(g, &ekin, sh.x);
       epot_direct_g(g, v, flag, konta, &epot8, &jmb, sh);
     }
   }
@@ -1651,7 +1764,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     return;
   }
   int unsup = 0;
-  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup);
+  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup, nxt, pot);
   ep += (unsigned long long)(k2 + ncapas);  // SO walk and property loop
   if (lead) {
     atomicAdd(&sg.work[0], ep);
@@ -1666,7 +1779,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
-    sg.status[slot] = unsup ? ASOHF_ERR_UNSUPPORTED : 0;
+    sg.status[slot] = unsup == 1 ? ASOHF_ERR_UNSUPPORTED : unsup == 2 ? ASOHF_ERR_TIMEOUT : 0;
   }
 }
 
@@ -1909,6 +2022,12 @@ static int big_cluster(asohf_ctx* c) {
     for (int t_ = 0; t_ < 4; t_++) c->launches += (T).n[t_] > 0;                                    \
   } while (0)
 
+extern "C" int asohf_set_epot_seed(asohf_ctx* c, uint32_t seed) {
+  if (!c) return ASOHF_ERR_INVALID;
+  c->epot_seed = seed;
+  return ASOHF_OK;
+}
+
 extern "C" int asohf_set_cluster_threshold(asohf_ctx* c, int64_t min_members) {
   if (!c || min_members < 0) return ASOHF_ERR_INVALID;
   c->cluster_min = min_members == 0 ? BIG_K : min_members;
@@ -1952,6 +2071,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   Store S = store_of(c);
   ColIdx ci = col_idx(c, k);
   HConst H = hconst(k, mesh);
+  H.epot_seed = c->epot_seed;
   const int CB = big_cluster(c);
   int rc = ASOHF_OK;
   if (ns > 0) {
@@ -2663,14 +2783,15 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
   write_back();
   g.sync();
   int unsup = 0;
-  long long nb = properties_g<C, false>(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup);
+  long long nb = properties_g<C, false>(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup,
+                                        nxt, pot);
   ep += (unsigned long long)(k2 + ncapas);
   if (lead) {
     atomicAdd(&sg.work[1], ep);
     const bool ok = nb >= H.min_num_part && H.want_ids;
     sg.nbound[slot] = ok ? (int32_t)nb : 0;
     sg.nscan[slot] = ok ? (int32_t)ncapas : 0;
-    sg.status[slot] = unsup ? ASOHF_ERR_UNSUPPORTED : 0;
+    sg.status[slot] = unsup == 1 ? ASOHF_ERR_UNSUPPORTED : unsup == 2 ? ASOHF_ERR_TIMEOUT : 0;
   }
 }
 
@@ -2812,6 +2933,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   Store S = store_of(c);
   ColIdx ci = col_idx(c, k);
   HConst H = hconst(k, mesh);
+  H.epot_seed = c->epot_seed;
   int rc = ASOHF_OK;
   if (ns > 0) {
     int32_t* d_work = (int32_t*)arena_alloc(c, 4 * (size_t)ns);

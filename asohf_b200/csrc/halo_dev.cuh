@@ -281,6 +281,7 @@ struct HConst {
   int want_ids;            // FLAG_WDM.EQ.1 .OR. VAR.GT.1
   int energies;            // DO_COMPUTE_ENERGIES.EQ.1
   int max_part_dsum;       // MAX_PART_DSUM: direct pair sums below it
+  uint32_t epot_seed;      // seed of the sampling estimator at or above it
   int nl;
   int lev_lo[ASOHF_NLEVELS + 2], lev_hi[ASOHF_NLEVELS + 2];  // 1-based patch ranges per level
 };

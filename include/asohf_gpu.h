@@ -58,6 +58,14 @@ int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
  * hold `bytes` bytes; the copy is complete when the stream reaches it. */
 int asohf_copy_to_host_sm(asohf_ctx *ctx, void *host_dst, const void *dev_src, int64_t bytes,
                           void *cuda_stream);
+/* Seed of COMPUTE_EPOT's sampling estimator (haloes_particles.f:1568-1626),
+ * used for bound lists of MAX_PART_DSUM entries or more when energies are
+ * on.  The reference draws its particle pairs from RANDOM_NUMBER after an
+ * unseeded RANDOM_SEED(), so its estimate changes from run to run; here the
+ * draws come from a counter-based generator keyed by (seed, catalogue row,
+ * draw), so a run is reproducible and equals the oracle's bit for bit.
+ * Default 1. */
+int asohf_set_epot_seed(asohf_ctx *ctx, uint32_t seed);
 /* Tuning, no counterpart in the reference: haloes with at least
  * min_members members are refined by a thread-block cluster, the others by
  * one CTA each (results are the same either way).  0 restores the default

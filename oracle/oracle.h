@@ -112,6 +112,9 @@ int orc_halofind_grid_base(int nx, float dx, const float *u1, const float *radx,
  * dispersion), added by orc_halofind_particles and
  * orc_substructure_particles; NULL switches the counting off. */
 void orc_set_margin_counts(int32_t *rows4, int64_t cap);
+/* Seed of COMPUTE_EPOT's sampling estimator (default 1); the draws are
+ * keyed by (seed, catalogue row, draw), as in the library. */
+void orc_set_epot_seed(uint32_t seed);
 int orc_halofind_particles(const orc_store *st, const asohf_consts *k,
                            const asohf_mesh *mesh, asohf_catalogue *cat,
                            int low1, int low2, int32_t *pph, int64_t pph_cap,

@@ -577,13 +577,101 @@ static void unbinding_sigma(const orc_store *st, const asohf_consts *k, int fac,
   unbind_result(h, konta3, cm, vcm, mmm, k->um);
 }
 
-/* COMPUTE_EPOT (haloes_particles.f:1494-1628), direct-summation branch.
- * The sampling branch draws from an unseeded RANDOM_SEED() in the
- * reference (irreproducible); here it is reported as unsupported. */
+/* Seed of the sampling estimator (orc_set_epot_seed; default 1). */
+static uint32_t g_epot_seed = 1;
+
+void orc_set_epot_seed(uint32_t seed) { g_epot_seed = seed; }
+
+/* MurmurHash3's 32-bit finaliser and the chained mix of the draws. */
+static inline uint32_t fmix32(uint32_t h)
+{
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+static inline uint32_t mix2(uint32_t a, uint32_t b) { return fmix32(a ^ fmix32(b)); }
+
+/* One draw J = 1 + FLOOR(U*KONTA) of the sampling branch, with U a REAL*4
+ * of 24 random bits: U = (bits >> 8) * 2^-24, bits = mix(key_outer, inner +
+ * 0x9E3779B9 * attempt).  Clamped to KONTA (U*KONTA can round up to KONTA
+ * in REAL*4, where the reference would read past the list). */
+static inline int64_t epot_draw(uint32_t key_outer, uint32_t inner, uint32_t attempt, int64_t konta)
+{
+  uint32_t bits = mix2(key_outer, inner + 0x9E3779B9u * attempt);
+  float u = (float)(bits >> 8) * 5.9604644775390625e-8f;
+  int64_t j = 1 + (int64_t)floorf(u * (float)konta);
+  return j <= konta ? j : konta;
+}
+
+#define EPOT_MAX_ATTEMPTS 4096u
+
+/* The sampling branch of COMPUTE_EPOT (haloes_particles.f:1568-1626),
+ * statement by statement, with the reference's RANDOM_NUMBER stream (after
+ * an unseeded RANDOM_SEED: irreproducible) replaced by epot_draw keyed by
+ * (seed, catalogue row, outer draw): the draws of J and, for each J, of its
+ * NSAMPLE partners K != J, rejecting unbound entries.  A draw that finds no
+ * bound entry in EPOT_MAX_ATTEMPTS tries returns ASOHF_ERR_TIMEOUT (the
+ * reference would loop on). */
+static int compute_epot_sampled(const orc_store *st, int64_t konta, int64_t konta2, const hwork *w,
+                                int max_part_dsum, float *epot, int64_t *most_bound)
+{
+  int64_t nsa = (int64_t)((float)max_part_dsum / 1.4f);
+  int64_t nsb = (int64_t)(0.01f * (float)konta2);
+  int64_t nsample = nsa > nsb ? nsa : nsb;
+  int64_t npairs = 0;
+  double epot8 = 0.0;
+  float largest_energy = 1000000.0f;
+  int64_t mb = w->lip[1];
+  uint32_t key_row = mix2(g_epot_seed, (uint32_t)g_row);
+  for (int64_t jjj = 1; jjj <= nsample; jjj++) {
+    uint32_t ko = mix2(key_row, (uint32_t)jjj);
+    int64_t j = -1;
+    for (uint32_t a = 0; a < EPOT_MAX_ATTEMPTS; a++) {
+      int64_t c = epot_draw(ko, 0u, a, konta);
+      if (w->contadm[c] == 0) { j = c; break; }
+    }
+    if (j < 0) return ASOHF_ERR_TIMEOUT;
+    int64_t jj = w->lip[j];
+    float x1 = st->x[jj], y1 = st->y[jj], z1 = st->z[jj], m1 = st->m[jj];
+    double bas = 0.0;
+    for (int64_t kkk = 1; kkk <= nsample; kkk++) {
+      int64_t kq = -1;
+      for (uint32_t a = 0; a < EPOT_MAX_ATTEMPTS; a++) {
+        int64_t c = epot_draw(ko, (uint32_t)kkk, a, konta);
+        if (w->contadm[c] == 0 && c != j) { kq = c; break; }
+      }
+      if (kq < 0) return ASOHF_ERR_TIMEOUT;
+      int64_t kk = w->lip[kq];
+      float ax = x1 - st->x[kk], ay = y1 - st->y[kk], az = z1 - st->z[kk];
+      float m2 = st->m[kk];
+      npairs++;
+      bas = bas - (double)(m1 * m2 / sqrtf(ax * ax + ay * ay + az * az));
+    }
+    epot8 = epot8 + bas;
+    bas = bas / (double)m1;
+    if (bas < (double)largest_energy) {
+      largest_energy = (float)bas;
+      mb = jj;
+    }
+  }
+  int64_t npairs_total = konta * (konta - 1) / 2;
+  epot8 = epot8 * (double)((float)npairs_total / (float)npairs);
+  *epot = (float)epot8;
+  *most_bound = mb;
+  return 0;
+}
+
+/* COMPUTE_EPOT (haloes_particles.f:1494-1628): direct summation below
+ * MAX_PART_DSUM bound entries, the seeded sampling estimator from there on. */
 static int compute_epot(const orc_store *st, int64_t konta, int64_t konta2, const hwork *w,
                         int max_part_dsum, float *epot, int64_t *most_bound)
 {
-  if (!(konta2 < max_part_dsum)) return ASOHF_ERR_UNSUPPORTED;
+  if (!(konta2 < max_part_dsum))
+    return compute_epot_sampled(st, konta, konta2, w, max_part_dsum, epot, most_bound);
   double epot8 = 0.0;
   double *ep = (double *)calloc((size_t)(konta + 1), sizeof(double));
   for (int64_t j = 1; j <= konta; j++) {
