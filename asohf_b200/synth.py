@@ -82,6 +82,10 @@ CONFIGS = {
     # the bounded sample the CPU oracle is timed on
     "cfg4s": SnapshotConfig("cfg4s", 128, 62.5, 128, 6, 3125, 1e10, 1e15, 0.70,
                             sub_host_min=1e12),
+    # the 512^3 workload at 1/8 of its volume: the second point of the CPU
+    # oracle's scaling trend
+    "cfg4m": SnapshotConfig("cfg4m", 256, 125.0, 256, 6, 25000, 1e10, 1e15, 0.70,
+                            sub_host_min=1e12),
     # small cases for tests
     "tiny": SnapshotConfig("tiny", 32, 10.0, 32, 2, 6, 1e11, 1e12, 0.70,
                            sub_host_min=3e11, seed=7),

@@ -17,7 +17,13 @@ on its own snapshot (weak scaling).
 
 --impl reference times the CPU restatement of the reference routines (the
 reference is Fortran and no Fortran compiler exists here) on a bounded
-sample of the same workload (the 512^3 recipe at 1/64 of the volume).
+sample of the same workload (the 512^3 recipe at 1/64 of the volume: 128^3
+particles), then once on the recipe at 1/8 of the volume (256^3 particles).
+From the two measured points each stage's cost is fitted as a power of the
+particle count and extrapolated to 512^3; the extrapolation is labelled as
+such.  The CPU's particles/s falls as the snapshot grows (the patch deposit
+scans every particle once per patch, the halo queries scan x-slabs that
+span the box), so the measured 256^3 rate bounds the 512^3 rate from above.
 """
 import argparse
 import json
@@ -34,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CPU_SAMPLE = "cfg4s"
+CPU_TREND = "cfg4m"   # the second point of the CPU scaling trend
 BYTES_PER_ELEMENT_PASS = 32  # d, m, |v| 12, position index read + dist/index written
 # DRAM bytes (read + write) per element-pass of k_halo_main: 3.53 GB over
 # 136.4M element-passes in one ncu capture of the 256^3 workload's launches
@@ -93,7 +100,8 @@ def clock_summary(proc, path):
 
 
 def cpu_oracle_run(name, steps, warmup, nthreads):
-    """The oracle pipeline (CPU restatement of the reference routines)."""
+    """The oracle pipeline (CPU restatement of the reference routines):
+    particles, seconds per step and seconds per stage (mean over steps)."""
     from asohf_b200 import driver, synth
     from oracle import oracle as O
     snap = synth.generate(name)
@@ -101,11 +109,43 @@ def cpu_oracle_run(name, steps, warmup, nthreads):
     b = O.OracleBackend(nthreads=nthreads)
     for _ in range(warmup):
         driver.execute(plan, b, download=False)
+    stages = {}
     t0 = time.perf_counter()
     for _ in range(steps):
-        driver.execute(plan, b, download=False)
+        r = driver.execute(plan, b, download=False)
+        for k, v in r.stage_s.items():
+            stages[k] = stages.get(k, 0.0) + v / steps
     dt = (time.perf_counter() - t0) / steps
-    return snap.cfg.n, dt
+    return snap.cfg.n, dt, stages
+
+
+def cpu_trend(small, nthreads, target_n):
+    """Measured CPU points at 128^3 (`small` = (n, dt, stages)) and 256^3
+    particles of the 512^3 recipe, and each stage fitted as t = a n^k through
+    the two points and extrapolated to target_n particles."""
+    from asohf_b200 import synth
+    n1, dt1, st1 = small
+    n2, dt2, st2 = cpu_oracle_run(CPU_TREND, 1, 0, nthreads)
+    pts = []
+    for name, n, dt, st in ((CPU_SAMPLE, n1, dt1, st1), (CPU_TREND, n2, dt2, st2)):
+        c = synth.CONFIGS[name]
+        pts.append({"workload": f"{name}: {c.npart_side}^3 particles, {c.box_mpc_h} Mpc/h, NX={c.nx}",
+                    "particles": n, "s_per_step": round(dt, 3), "particles_per_s": n / dt,
+                    "stage_s": {k: round(v, 4) for k, v in st.items()}})
+    ratio = n2 / n1
+    ext, exps = {}, {}
+    for k in st2:
+        a, b = max(st1.get(k, 0.0), 1e-9), max(st2[k], 1e-9)
+        kexp = math.log(b / a) / math.log(ratio)
+        exps[k] = round(kexp, 3)
+        ext[k] = b * (target_n / n2) ** kexp
+    t_ext = sum(ext.values())
+    return {"points": pts,
+            "extrapolated": {"particles": target_n, "s_per_step": round(t_ext, 1),
+                             "particles_per_s": target_n / t_ext, "stage_exponents": exps,
+                             "stage_s": {k: round(v, 1) for k, v in ext.items()},
+                             "note": "extrapolated, not measured: each stage fitted as a power of the particle "
+                                     "count through the two measured points"}}
 
 
 def layer_bench(iters=10, warmup=3):
@@ -184,6 +224,8 @@ def main():
     ap.add_argument("--config", default="cfg4")
     ap.add_argument("--no-subs", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-cpu-trend", action="store_true",
+                    help="skip the CPU run of the 256^3 sample and the extrapolation to the full size")
     ap.add_argument("--no-layer", action="store_true", help="skip the deposit+Poisson layer leg")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs: only the device-timed steps)")
@@ -196,9 +238,16 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        from asohf_b200 import synth
         nth = os.cpu_count() or 1
-        n, dt = cpu_oracle_run(CPU_SAMPLE, args.steps, args.warmup, nth)
+        small = cpu_oracle_run(CPU_SAMPLE, args.steps, args.warmup, nth)
+        n, dt, _ = small
         v = n / dt
+        cb = {"value": v, "unit": "particles/s", "cores": nth, "kind": "port",
+              "sample": "full hot path on the 128^3 sample of the 512^3 recipe (C restatement of the Fortran), "
+                        f"{args.steps} steps"}
+        if not args.no_cpu_trend:
+            cb["trend"] = cpu_trend(small, nth, synth.CONFIGS[args.config].n)
         print(json.dumps({
             "impl": "reference", "metric": metric, "value": v, "unit": "particles/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -206,8 +255,7 @@ def main():
             "dtype": "f32/f64", "data": "synthetic",
             "config": {"workload": f"{CPU_SAMPLE}: 128^3 particles, 62.5 Mpc/h, the 512^3 recipe at 1/64 volume",
                        "parallelism": "cpu"},
-            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": nth, "kind": "port",
-                             "sample": "full hot path on the 128^3 sample of the 512^3 recipe (C restatement of the Fortran)"},
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
         return
@@ -336,10 +384,13 @@ def main():
         out["deposit_poisson"] = layer_bench()
     if rank == 0 and not args.no_cpu:
         nth = os.cpu_count() or 1
-        n_s, dt = cpu_oracle_run(CPU_SAMPLE, 1, 0, nth)
+        small = cpu_oracle_run(CPU_SAMPLE, 1, 0, nth)
+        n_s, dt, _ = small
         out["cpu_baseline"] = {"value": n_s / dt, "unit": "particles/s", "cores": nth, "kind": "port",
                                "sample": f"{CPU_SAMPLE}: 128^3 particles, the 512^3 recipe at 1/64 volume, "
                                          "full hot path, 1 step"}
+        if not args.no_cpu_trend:
+            out["cpu_baseline"]["trend"] = cpu_trend(small, nth, n)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -83,13 +83,25 @@ def test_energies_match_oracle(gpu_lib, name):
     assert np.all(ro.cat.potential_e[:n][live] < 0)
 
 
-def test_energies_above_dsum_limit_are_unsupported(gpu_lib):
-    """Above MAX_PART_DSUM the reference samples pairs with an unseeded
-    generator; the library reports that case as unsupported, like the
-    oracle."""
+def test_energies_above_dsum_limit_use_the_seeded_estimator(gpu_lib):
+    """Above MAX_PART_DSUM the reference estimates the potential energy from
+    sampled pairs (with an unseeded generator); the library and the oracle
+    run the same estimator from a seeded counter-based generator, so the
+    sampled haloes' POTENTIAL_E and IPLIP are identical."""
+    import ctypes as C
     s = synth.generate("tiny")
-    p = driver.prepare(s)
-    p.consts.do_compute_energies = 1
-    p.consts.max_part_dsum = 10
-    with pytest.raises(RuntimeError):
-        driver.execute(p, api.GpuBackend(), with_subs=False)
+    plans = []
+    for _ in range(2):
+        p = driver.prepare(s)
+        p.consts.do_compute_energies = 1
+        p.consts.max_part_dsum = 10
+        plans.append(p)
+    rg = driver.execute(plans[0], api.GpuBackend(), with_subs=True)
+    O.lib().orc_set_epot_seed(C.c_uint32(1))
+    ro = driver.execute(plans[1], O.OracleBackend(), with_subs=True)
+    n = ro.cat.nclus
+    live = ro.cat.realclus[:n] != 0
+    assert live.sum() > 0
+    compare(rg, ro)
+    assert np.array_equal(rg.cat.potential_e[:n][live], ro.cat.potential_e[:n][live])
+    assert np.array_equal(rg.cat.iplip[:n], ro.cat.iplip[:n])
