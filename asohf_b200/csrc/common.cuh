@@ -304,3 +304,20 @@ __device__ __forceinline__ double block_scan_d(double v, double* sbuf, double* t
   if (total) *total = tot;
   return x + off;
 }
+
+// TSC weights of grids.f:1194-1213: BAS=|x-r|/d, 0.5(1.5-BAS)^2, 0.75-BAS^2.
+__device__ __forceinline__ void tsc_weights(float xp, float rm, float r0, float rp, float d, float* v) {
+  float b = fabsf(__fsub_rn(xp, rm)) / d;
+  float t = __fsub_rn(1.5f, b);
+  v[0] = __fmul_rn(0.5f, __fmul_rn(t, t));
+  b = fabsf(__fsub_rn(xp, r0)) / d;
+  v[1] = __fsub_rn(0.75f, __fmul_rn(b, b));
+  b = fabsf(__fsub_rn(xp, rp)) / d;
+  t = __fsub_rn(1.5f, b);
+  v[2] = __fmul_rn(0.5f, __fmul_rn(t, t));
+}
+
+__device__ __forceinline__ int tsc_cell(float v, float xl, float dx, int nx) {
+  int i = (int)((v - xl) / dx) + 1;
+  return i < 1 ? 1 : (i > nx ? nx : i);
+}

@@ -1258,23 +1258,6 @@ extern "C" int asohf_renorm_density(asohf_ctx* c, int nx, const asohf_mesh* mesh
 }
 
 // ------------------------------------------------------------ TSC deposit
-// TSC weights of grids.f:1194-1213: BAS=|x-r|/d, 0.5(1.5-BAS)^2, 0.75-BAS^2.
-__device__ __forceinline__ void tsc_weights(float xp, float rm, float r0, float rp, float d, float* v) {
-  float b = fabsf(__fsub_rn(xp, rm)) / d;
-  float t = __fsub_rn(1.5f, b);
-  v[0] = __fmul_rn(0.5f, __fmul_rn(t, t));
-  b = fabsf(__fsub_rn(xp, r0)) / d;
-  v[1] = __fsub_rn(0.75f, __fmul_rn(b, b));
-  b = fabsf(__fsub_rn(xp, rp)) / d;
-  t = __fsub_rn(1.5f, b);
-  v[2] = __fmul_rn(0.5f, __fmul_rn(t, t));
-}
-
-__device__ __forceinline__ int tsc_cell(float v, float xl, float dx, int nx) {
-  int i = (int)((v - xl) / dx) + 1;
-  return i < 1 ? 1 : (i > nx ? nx : i);
-}
-
 // Base grid TSC for a batch of particle sets; acc has batch*nx^3 doubles or floats.
 template <typename T>
 __global__ void k_tsc_base(const float* __restrict__ x, const float* __restrict__ y,

@@ -13,6 +13,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "common.cuh"
 
 int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* dradx, int batch,
@@ -203,6 +205,175 @@ extern "C" int asohf_poisson_fft(asohf_ctx* c, int nx, float dx, int batch, cons
 }
 
 // ------------------------------------------------------------ layer
+// The layer's particles are sorted once per call by a key of (copy, Morton
+// code of the host cell), so a warp reads 32 particles of neighbouring cells
+// and the grid cells it touches are close together.  Particles that share a
+// host cell share all 27 target cells: a warp adds each run of equal keys
+// as one segmented sum (shuffles) and issues one atomic per run and target.
+// In a halo core, where hundreds of particles share a cell, this replaces
+// 27 contended atomics per particle by 27 per run (warp-aggregated atomics).
+// The sums are float32; a cell's terms are added in a different order than
+// the sequential loop of grids.f:1163-1239, which changes the result within
+// float32 rounding.
+
+// bits 0..9 of v spread to every third bit (Morton interleave)
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+struct LayerSort {
+  uint32_t* keys;  // sorted keys: copy << cbits | Morton(ix-1, jy-1, kz-1)
+  int32_t* idx;    // sorted particle indices
+  float4* pm;      // (x, y, z, m) in input order
+  int cbits;
+};
+
+static int ceil_log2(int64_t v) {
+  int b = 0;
+  while ((1ll << b) < v) b++;
+  return b;
+}
+
+// whether the sorted path applies: keys fit in 31 bits, indices in int32
+static bool layer_sortable(int nx, int batch, int64_t ntot) {
+  return nx <= 1024 && 3 * ceil_log2(nx) + ceil_log2(batch) <= 31 && ntot < (1ll << 31);
+}
+
+static size_t layer_sort_bytes(int nx, int batch, int64_t ntot) {
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
+                                  (int32_t*)nullptr, (int)(ntot > 0 ? ntot : 1), 0,
+                                  3 * ceil_log2(nx) + ceil_log2(batch));
+  return 32 * (size_t)ntot + tb + 2048;
+}
+
+__global__ void k_layer_keys(const float* __restrict__ x, const float* __restrict__ y,
+                             const float* __restrict__ z, const float* __restrict__ m, int64_t ntot,
+                             int64_t n_per, int nx, float xl, float dx, int cbits, uint32_t* __restrict__ keys,
+                             int32_t* __restrict__ idx, float4* __restrict__ pm) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < ntot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const float xp = x[q], yp = y[q], zp = z[q];
+    const int ix = tsc_cell(xp, xl, dx, nx), jy = tsc_cell(yp, xl, dx, nx), kz = tsc_cell(zp, xl, dx, nx);
+    const uint32_t mort = spread3((uint32_t)(ix - 1)) | (spread3((uint32_t)(jy - 1)) << 1) |
+                          (spread3((uint32_t)(kz - 1)) << 2);
+    keys[q] = ((uint32_t)(q / n_per) << cbits) | mort;
+    idx[q] = (int32_t)q;
+    pm[q] = make_float4(xp, yp, zp, m[q]);
+  }
+}
+
+static int layer_sort(asohf_ctx* c, int nx, float xl, float dx, int batch, int64_t n_per, const float* x,
+                      const float* y, const float* z, const float* m, LayerSort* s) {
+  const int64_t ntot = n_per * batch;
+  const int bits = 3 * ceil_log2(nx) + ceil_log2(batch);
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
+                                  (int32_t*)nullptr, (int)ntot, 0, bits);
+  uint32_t* k0 = (uint32_t*)arena_alloc(c, 4 * (size_t)ntot);
+  uint32_t* k1 = (uint32_t*)arena_alloc(c, 4 * (size_t)ntot);
+  int32_t* v0 = (int32_t*)arena_alloc(c, 4 * (size_t)ntot);
+  int32_t* v1 = (int32_t*)arena_alloc(c, 4 * (size_t)ntot);
+  float4* pm = (float4*)arena_alloc(c, 16 * (size_t)ntot);
+  void* t = arena_alloc(c, tb);
+  if (!k0 || !k1 || !v0 || !v1 || !pm || !t) return ASOHF_ERR_CAPACITY;
+  s->cbits = 3 * ceil_log2(nx);
+  {
+    int kt_ = ktime_begin(c, "layer_keys");
+    k_layer_keys<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(x, y, z, m, ntot, n_per, nx, xl, dx,
+                                                                             s->cbits, k0, v0, pm);
+    ktime_end(c, kt_);
+  }
+  c->launches++;
+  {
+    int kt_ = ktime_begin(c, "layer_sort");
+    ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)ntot, 0, bits, c->stream));
+    ktime_end(c, kt_);
+  }
+  s->keys = k1;
+  s->idx = v1;
+  s->pm = pm;
+  ASOHF_CUDA(cudaGetLastError());
+  return ASOHF_OK;
+}
+
+// TSC deposit (grids.f:1163-1239, periodic base grid) of the sorted
+// particles, m / DENBAS per particle; one warp per 32 sorted particles.
+__global__ void __launch_bounds__(256) k_layer_deposit(const uint32_t* __restrict__ keys,
+                                                       const int32_t* __restrict__ idx,
+                                                       const float4* __restrict__ pm, int64_t ntot, int nx,
+                                                       int cbits, float xl, float dx,
+                                                       const float* __restrict__ radx, float denbas,
+                                                       float* __restrict__ rho) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const size_t G = (size_t)nx * nx * nx;
+  for (int64_t base = warp * 32; base < ntot; base += nwarps * 32) {
+    const int64_t i = base + lane;
+    const bool valid = i < ntot;
+    const uint32_t key = valid ? keys[i] : 0xffffffffu;  // past the end: one run of its own
+    const float4 p = valid ? pm[idx[i]] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t prev = __shfl_up_sync(FULL, key, 1);
+    const bool head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(FULL, head);
+    const bool runs = __ballot_sync(FULL, !head) != 0u;  // some run is longer than one particle
+    const int rs = 31 - __clz(heads & (FULL >> (31 - lane)));  // first lane of my run
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    const int ix = tsc_cell(p.x, xl, dx, nx), jy = tsc_cell(p.y, xl, dx, nx), kz = tsc_cell(p.z, xl, dx, nx);
+    float wx[3], wy[3], wz[3];
+    tsc_weights(p.x, radx[ix - 1], radx[ix], radx[ix + 1], dx, wx);
+    tsc_weights(p.y, radx[jy - 1], radx[jy], radx[jy + 1], dx, wy);
+    tsc_weights(p.z, radx[kz - 1], radx[kz], radx[kz + 1], dx, wz);
+    const float mp = __fdiv_rn(p.w, denbas);
+    float* a = rho + (size_t)(valid ? (key >> cbits) : 0u) * G;
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      int k1 = kz + kk;
+      if (k1 == nx + 1) k1 = 1;
+      if (k1 == 0) k1 = nx;
+#pragma unroll
+      for (int jj = -1; jj <= 1; jj++) {
+        int j1 = jy + jj;
+        if (j1 == nx + 1) j1 = 1;
+        if (j1 == 0) j1 = nx;
+#pragma unroll
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = ix + ii;
+          if (i1 == nx + 1) i1 = 1;
+          if (i1 == 0) i1 = nx;
+          float t = valid ? __fmul_rn(__fmul_rn(__fmul_rn(mp, wx[ii + 1]), wy[jj + 1]), wz[kk + 1]) : 0.f;
+          const size_t cell = ((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1);
+          if (runs) {
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+              const float v = __shfl_up_sync(FULL, t, d);
+              if (lane - d >= rs) t = __fadd_rn(t, v);
+            }
+            if (valid && tail) atomicAdd(&a[cell], t);
+          } else if (valid) {
+            atomicAdd(&a[cell], t);
+          }
+        }
+      }
+    }
+  }
+}
+
+// dL/dx_p = m_p/DENBAS * sum_c d(Wx Wy Wz)/dx_p * g_c,  g = G * w, over the
+// sorted particles (neighbouring warps read neighbouring cells of g).
+__global__ void k_layer_adjoint(const uint32_t* __restrict__ keys, const int32_t* __restrict__ idx,
+                                const float4* __restrict__ pm, int64_t ntot, int nx, int cbits, float xl,
+                                float dx, const float* __restrict__ radx, const float* __restrict__ gfield,
+                                float inv_denbas, float* __restrict__ gx, float* __restrict__ gy,
+                                float* __restrict__ gz, float* __restrict__ gm);
+
 extern "C" int asohf_tsc_poisson_forward(asohf_ctx* c, int nx, float lado0, float dx,
                                          const float* radx, float rote, float rete, int batch,
                                          int64_t n_per, const float* x, const float* y,
@@ -211,14 +382,28 @@ extern "C" int asohf_tsc_poisson_forward(asohf_ctx* c, int nx, float lado0, floa
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
   int64_t g = (int64_t)nx * nx * nx * batch;
-  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 1024));
+  const int64_t ntot = n_per * batch;
+  const bool sorted = ntot > 0 && layer_sortable(nx, batch, ntot);
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + (sorted ? layer_sort_bytes(nx, batch, ntot) : 0) + 1024));
   const float* dradx;
   ASOHF_CHECK(radx_device(c, nx, radx, &dradx));
   ASOHF_CUDA(cudaMemsetAsync(rho, 0, 4 * g, c->stream));
   // each particle deposits m / (DX^3 ROTE RETE^3): the division of the cell
   // sums (grids.f:1236-1238) moved onto the terms, so rho needs no extra pass
   float denbas = dx * dx * dx * rote * (rete * rete * rete);
-  ASOHF_CHECK(tsc_base_batched_f32(c, nx, -lado0 / 2.0f, dx, dradx, batch, n_per, x, y, z, m, denbas, rho));
+  const float xl = -lado0 / 2.0f;
+  if (sorted) {
+    LayerSort s;
+    ASOHF_CHECK(layer_sort(c, nx, xl, dx, batch, n_per, x, y, z, m, &s));
+    int kt_ = ktime_begin(c, "layer_deposit");
+    k_layer_deposit<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.keys, s.idx, s.pm, ntot, nx, s.cbits, xl, dx, dradx, denbas, rho);
+    ktime_end(c, kt_);
+    c->launches++;
+    ASOHF_CUDA(cudaGetLastError());
+  } else {
+    ASOHF_CHECK(tsc_base_batched_f32(c, nx, xl, dx, dradx, batch, n_per, x, y, z, m, denbas, rho));
+  }
   return poisson_dev(c, nx, dx, batch, rho, pot);
 }
 
@@ -287,6 +472,54 @@ __global__ void k_tsc_adjoint(const float* __restrict__ x, const float* __restri
   }
 }
 
+__global__ void k_layer_adjoint(const uint32_t* __restrict__ keys, const int32_t* __restrict__ idx,
+                                const float4* __restrict__ pm, int64_t ntot, int nx, int cbits, float xl,
+                                float dx, const float* __restrict__ radx, const float* __restrict__ gfield,
+                                float inv_denbas, float* __restrict__ gx, float* __restrict__ gy,
+                                float* __restrict__ gz, float* __restrict__ gm) {
+  const size_t G = (size_t)nx * nx * nx;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ntot;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t q = idx[i];
+    const float4 p = pm[q];
+    const int ix = tsc_cell(p.x, xl, dx, nx), jy = tsc_cell(p.y, xl, dx, nx), kz = tsc_cell(p.z, xl, dx, nx);
+    float wx[3], wy[3], wz[3], dwx[3], dwy[3], dwz[3];
+    tsc_w_dw(p.x, radx[ix - 1], radx[ix], radx[ix + 1], dx, wx, dwx);
+    tsc_w_dw(p.y, radx[jy - 1], radx[jy], radx[jy + 1], dx, wy, dwy);
+    tsc_w_dw(p.z, radx[kz - 1], radx[kz], radx[kz + 1], dx, wz, dwz);
+    const float* g = gfield + (size_t)(keys[i] >> cbits) * G;
+    float ax = 0.f, ay = 0.f, az = 0.f, am = 0.f;
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      int k1 = kz + kk;
+      if (k1 == nx + 1) k1 = 1;
+      if (k1 == 0) k1 = nx;
+#pragma unroll
+      for (int jj = -1; jj <= 1; jj++) {
+        int j1 = jy + jj;
+        if (j1 == nx + 1) j1 = 1;
+        if (j1 == 0) j1 = nx;
+#pragma unroll
+        for (int ii = -1; ii <= 1; ii++) {
+          int i1 = ix + ii;
+          if (i1 == nx + 1) i1 = 1;
+          if (i1 == 0) i1 = nx;
+          float gv = g[((size_t)(k1 - 1) * nx + (j1 - 1)) * nx + (i1 - 1)];
+          ax += dwx[ii + 1] * wy[jj + 1] * wz[kk + 1] * gv;
+          ay += wx[ii + 1] * dwy[jj + 1] * wz[kk + 1] * gv;
+          az += wx[ii + 1] * wy[jj + 1] * dwz[kk + 1] * gv;
+          am += wx[ii + 1] * wy[jj + 1] * wz[kk + 1] * gv;
+        }
+      }
+    }
+    const float mp = p.w * inv_denbas;
+    gx[q] = mp * ax;
+    gy[q] = mp * ay;
+    gz[q] = mp * az;
+    if (gm) gm[q] = am * inv_denbas;
+  }
+}
+
 extern "C" int asohf_tsc_poisson_adjoint(asohf_ctx* c, int nx, float lado0, float dx,
                                          const float* radx, float rote, float rete, int batch,
                                          int64_t n_per, const float* x, const float* y,
@@ -296,16 +529,27 @@ extern "C" int asohf_tsc_poisson_adjoint(asohf_ctx* c, int nx, float lado0, floa
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
   int64_t g = (int64_t)nx * nx * nx * batch;
-  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * g + 2048));
+  int64_t ntot = n_per * batch;
+  const bool sorted = ntot > 0 && layer_sortable(nx, batch, ntot);
+  ASOHF_CHECK(arena_reserve(c, poisson_bytes(nx, batch) + 4 * g + (sorted ? layer_sort_bytes(nx, batch, ntot) : 0) +
+                                   2048));
   const float* dradx;
   ASOHF_CHECK(radx_device(c, nx, radx, &dradx));
   float* gfield = (float*)arena_alloc(c, 4 * g);
   if (!gfield) return ASOHF_ERR_CAPACITY;
+  float denbas = dx * dx * dx * rote * (rete * rete * rete);
+  const float xl = -lado0 / 2.0f;
+  LayerSort s;
+  if (sorted) ASOHF_CHECK(layer_sort(c, nx, xl, dx, batch, n_per, x, y, z, m, &s));
   // the Green's operator is real and symmetric: its adjoint is itself
   ASOHF_CHECK(poisson_dev(c, nx, dx, batch, w, gfield));
-  float denbas = dx * dx * dx * rote * (rete * rete * rete);
-  int64_t ntot = n_per * batch;
-  if (ntot > 0) {
+  if (sorted) {
+    int kt_ = ktime_begin(c, "layer_adjoint");
+    k_layer_adjoint<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.keys, s.idx, s.pm, ntot, nx, s.cbits, xl, dx, dradx, gfield, 1.0f / denbas, grad_x, grad_y, grad_z, grad_m);
+    ktime_end(c, kt_);
+    c->launches++;
+  } else if (ntot > 0) {
     {
       int kt_ = ktime_begin(c, "tsc_adjoint_gather");
       k_tsc_adjoint<<<grid_for(ntot, 256, c->num_sms * 16), 256, 0, c->stream>>>(
