@@ -41,7 +41,10 @@ sys.path.insert(0, ROOT)
 
 CPU_SAMPLE = "cfg4s"
 CPU_TREND = "cfg4m"   # the second point of the CPU scaling trend
-BYTES_PER_ELEMENT_PASS = 32  # d, m, |v| 12, position index read + dist/index written
+# algorithmic bytes of one (particle, pass) of the per-halo kernels: the
+# particle's position 12, velocity 12, mass 4 and ID 8 read, its distance and
+# flag 8 written
+BYTES_PER_ELEMENT_PASS = 44
 # DRAM bytes (read + write) per element-pass of k_halo_main: 3.53 GB over
 # 136.4M element-passes in one ncu capture of the 256^3 workload's launches
 # (`--config cfg2 --steps 1 --warmup 0 --no-cpu --no-layer --no-e2e`)
