@@ -26,6 +26,7 @@ ERRORS = {
     6: "wrong sorting, cannot continue",
     7: "no usable CUDA device",
     8: "unsupported option",
+    9: "growing not converged",
 }
 
 _fp = C.POINTER(C.c_float)

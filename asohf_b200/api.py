@@ -346,6 +346,20 @@ class Asohf:
                                         C.c_float(vol_solap_low), C.c_int(0), C.byref(n)), "OVERLAPPING")
         return n.value
 
+    def halofind_grid_base(self, nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low, cat):
+        """HALOFIND_GRID at the base level without AMR recentering; fills
+        cat (host), returns NHALLEV(0)."""
+        u = np.ascontiguousarray(u1, np.float32).reshape(-1)
+        r = np.ascontiguousarray(radx, np.float32)
+        cc = cat.as_c()
+        n = C.c_int32()
+        f = C.c_float
+        _check(self.L.asohf_halofind_grid_base(self.h, C.c_int(nx), f(dx), _ptr(u), _ptr(r), f(contrastec), f(rote),
+                                               f(rete), f(rodo), f(re0), f(bound), f(vol_solap_low), None,
+                                               C.byref(cc), C.c_int(0), C.byref(n)), "HALOFIND_GRID")
+        cat.nclus = cc.nclus
+        return n.value
+
     def halofind_particles(self, consts, mesh, cat, low1, low2):
         mh = abi.MeshHolder(mesh)
         cc = cat.as_c()
@@ -496,6 +510,16 @@ class GpuBackend:
 
     def prune_poor_haloes(self, consts, cat, low1, low2, facrad, do_need_to_count):
         self.a.prune_poor_haloes(consts, cat, low1, low2, facrad, do_need_to_count)
+
+    def halofind_grid_base(self, nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low, cat,
+                           mesh=None, u11=None):
+        """HALOFIND_GRID at the base level (haloes_grids.f:287-582); the
+        recentering on AMR levels is not on the device (a mesh with patches
+        raises)."""
+        if mesh is not None and int(np.asarray(mesh.npatch)[1:mesh.nl + 1].sum()) > 0:
+            raise AsohfError(8, "HALOFIND_GRID with AMR recentering")
+        return self.a.halofind_grid_base(nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low,
+                                         cat)
 
     def halofind_particles(self, consts, mesh, cat, low1, low2, pph):
         self.a.halofind_particles(consts, mesh, cat, low1, low2)

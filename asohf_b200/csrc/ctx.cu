@@ -25,6 +25,7 @@ extern "C" const char* asohf_strerror(int code) {
     case ASOHF_ERR_WRONG_SORTING: return "wrong sorting, cannot continue";
     case ASOHF_ERR_NO_DEVICE: return "no usable CUDA device";
     case ASOHF_ERR_UNSUPPORTED: return "unsupported option";
+    case ASOHF_ERR_NOT_CONVERGED: return "growing not converged";
     default: return "unknown status";
   }
 }

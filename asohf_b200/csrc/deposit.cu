@@ -717,39 +717,6 @@ __global__ void k_patch_unit_counts(DevMesh M, Bins B, const int32_t* __restrict
   if (lane == 0) cnt[u] = s;
 }
 
-// Compensated float32 accumulation of the patch cells: every cell keeps a
-// sum and a compensation in shared memory.  An atomic add returns the sum it
-// replaced, so the rounding error of that addition is known exactly (Knuth's
-// TwoSum of the old sum and the term) and goes to the compensation, together
-// with the exact rounding error of the term's product by the hit-group size
-// (an FMA).  sum + compensation is then the exact total up to the rounding of
-// the compensations themselves (second order), so the cell rounds to float32
-// like the float64 sum it replaces, at the cost of float32 atomics.
-__device__ __forceinline__ float two_sum_err(float a, float b, float s) {
-  const float bp = __fsub_rn(s, a);
-  return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
-}
-
-__device__ __forceinline__ void acc_add(float* __restrict__ sum, float* __restrict__ comp, int i, float t, float wc) {
-  float p = t, ep = 0.0f;
-  if (wc != 1.0f) {
-    p = __fmul_rn(t, wc);
-    ep = __fmaf_rn(t, wc, -p);  // t * wc - p, exact
-  }
-  const float old = atomicAdd(&sum[i], p);
-  const float c = __fadd_rn(two_sum_err(old, p, __fadd_rn(old, p)), ep);
-  if (c != 0.0f) atomicAdd(&comp[i], c);
-}
-
-// Non-atomic variant for a cell owned by one thread: adds a float64 value
-// as its float32 head and tail.
-__device__ __forceinline__ void acc_add_owned(float* __restrict__ sum, float* __restrict__ comp, int i, double v) {
-  const float hi = (float)v, lo = (float)(v - (double)hi);
-  const float old = sum[i], s = __fadd_rn(old, hi);
-  sum[i] = s;
-  comp[i] = __fadd_rn(comp[i], __fadd_rn(two_sum_err(old, hi, s), lo));
-}
-
 struct PatchWork {
   const int2* items;         // (unit, slice)
   const int32_t* scratch_of; // per unit: scratch slab index, -1 for single-slice units
@@ -760,10 +727,8 @@ __global__ void __launch_bounds__(PZ_BLOCK, 3)
 k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t* __restrict__ S,
                   const int32_t* __restrict__ order, PatchWork W, float dx, const float* __restrict__ kernels,
                   int eqmass, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
-  extern __shared__ double smem_d[];  // sums and compensations (padded rows), count grid, kernel table
-  float* accs = (float*)smem_d;
-  float* accc = accs + ACC_N;
-  int32_t* scnt = (int32_t*)(accc + ACC_N);
+  extern __shared__ double acc[];  // ACC_N doubles (padded rows), count grid, kernel table
+  int32_t* scnt = (int32_t*)(acc + ACC_N);
   float* ktab = (float*)(scnt + CGX * CGX * CGZ);
   __shared__ int s_lo[PROWS], s_pre[PROWS + 1], s_next;
   __shared__ double s_t27[27];
@@ -777,7 +742,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
     for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) out[q] = 0.0f;
     return;
   }
-  for (int q = threadIdx.x; q < ACC_N; q += blockDim.x) { accs[q] = 0.0f; accc[q] = 0.0f; }
+  for (int q = threadIdx.x; q < ACC_N; q += blockDim.x) acc[q] = 0.0;
   for (int q = threadIdx.x; q < CGX * CGX * CGZ; q += blockDim.x) scnt[q] = 0;
   for (int l = 0; l <= g.ir; l++) {
     int nk = 1 << l, c0 = ktab_center(l);
@@ -897,7 +862,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
         const int wxy = __shfl_sync(0xffffffffu, pxy, src), wzl = __shfl_sync(0xffffffffu, pzl, src);
         const int wix = (wxy & 0xffff) - 1024, wjy = (wxy >> 16) - 1024, wkz = (wzl & 0xffff) - 1024;
         const int wlev = (wzl >> 16) & 0xff, nk = 1 << wlev;
-        const float wc = (float)(wzl >> 24);
+        const double wc = (double)(wzl >> 24);
         // the cloud clipped to the patch and to the unit's planes
         const int wi1 = max(wix - nk, 1), wj1 = max(wjy - nk, 1), wk1 = max(max(wkz - nk, 1), g.zlo);
         const int wdi = min(wix + nk, g.n1) - wi1 + 1, wdj = min(wjy + nk, g.n2) - wj1 + 1;
@@ -922,10 +887,10 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
         for (int pq = lane; pq < npair; pq += 32) {
           const int ii = wi1 + ci, jj = wj1 + cj;
           float bw = __fmul_rn(__fmul_rn(wm, kc[ii - wix]), kc[jj - wjy]);
-          const int col = (wk1 - g.zlo) * APLANE + (jj - 1) * AROW + (ii - 1);
+          double* col = acc + (wk1 - g.zlo) * APLANE + (jj - 1) * AROW + (ii - 1);
 #pragma unroll
           for (int q = 0; q < PZ; q++)
-            if (q < wdk) acc_add(accs, accc, col + q * APLANE, __fmul_rn(bw, wzk[q]), wc);
+            if (q < wdk) atomicAdd(col + q * APLANE, __dmul_rn((double)__fmul_rn(bw, wzk[q]), wc));
           ci += si;
           cj += sj;
           if (ci >= wdi) { ci -= wdi; cj++; }
@@ -966,7 +931,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
         if ((c0 | c1 | c2 | c3 | c4 | c5 | c6 | c7) == 0) continue;
         double s = (double)c0 * tp[0] + (double)c1 * tp[1] + (double)c2 * tp[2] + (double)c3 * tp[3] +
                    (double)c4 * tp[4] + (double)c5 * tp[5] + (double)c6 * tp[6] + (double)c7 * tp[7];
-        acc_add_owned(accs, accc, (pz - 1) * APLANE + (j - 1) * AROW + (i - 1), s);
+        acc[(pz - 1) * APLANE + (j - 1) * AROW + (i - 1)] += s;
       }
     }
   } else if (eqmass && s_any) {
@@ -980,7 +945,7 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
             int c = scnt[((k - kk - g.zlo + 1) * CGX + (j - jj)) * CGX + (i - ii)];
             if (c) s += (double)c * s_t27[(kk + 1) * 9 + (jj + 1) * 3 + (ii + 1)];
           }
-      acc_add_owned(accs, accc, (k - g.zlo) * APLANE + (j - 1) * AROW + (i - 1), s);
+      acc[(k - g.zlo) * APLANE + (j - 1) * AROW + (i - 1)] += s;
     }
   }
   const int sidx = W.scratch_of[it.x];
@@ -990,18 +955,14 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
     for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
       int i = q % NA, j = (q / NA) % NA, k = g.slab * PZ + q / (NA * NA);
       float v = 0.0f;
-      if (i < g.n1 && j < g.n2 && k < g.n3) {
-        const int a = (q / (NA * NA)) * APLANE + j * AROW + i;
-        v = (float)((double)accs[a] + (double)accc[a]) / den;
-      }
+      if (i < g.n1 && j < g.n2 && k < g.n3) v = (float)acc[(q / (NA * NA)) * APLANE + j * AROW + i] / den;
       out[q] = v;
     }
   } else {  // one slice of a shared unit
     __syncthreads();
     double* sc = W.scratch + (size_t)sidx * NA * NA * PZ;
     for (int q = threadIdx.x; q < NA * NA * PZ; q += blockDim.x) {
-      const int ai = (q / (NA * NA)) * APLANE + ((q / NA) % NA) * AROW + q % NA;
-      double a = (double)accs[ai] + (double)accc[ai];
+      double a = acc[(q / (NA * NA)) * APLANE + ((q / NA) % NA) * AROW + q % NA];
       if (a != 0.0) atomicAdd(&sc[q], a);
     }
   }

@@ -41,7 +41,8 @@ enum {
   ASOHF_ERR_NOT_PREFOUND_VIRIAL = 5, /* haloes_particles.f:1483-1486 */
   ASOHF_ERR_WRONG_SORTING = 6,       /* reader.f:267-270 */
   ASOHF_ERR_NO_DEVICE = 7,    /* no usable CUDA device: the library never falls back to the CPU */
-  ASOHF_ERR_UNSUPPORTED = 8   /* option outside the implemented hot path */
+  ASOHF_ERR_UNSUPPORTED = 8,  /* option outside the implemented hot path */
+  ASOHF_ERR_NOT_CONVERGED = 9 /* haloes_grids.f:482-488: growing not converged */
 };
 
 /* AMR patch table (the arrays CREATE_MESH fills, asohf.f:51-62).  Host

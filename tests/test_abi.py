@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 def test_status_strings():
     build.build()
     L = api.load()
-    for code in range(9):
+    for code in range(10):
         assert L.asohf_strerror(code).decode()
 
 
