@@ -117,6 +117,15 @@ class Asohf:
     def launch_count(self) -> int:
         return int(self.L.asohf_launch_count(self.h))
 
+    def set_density_overlap(self, on: bool):
+        """Deferred AMR-patch deposit for device outputs (see
+        asohf_set_density_overlap); U11 is complete after density_wait."""
+        _check(self.L.asohf_set_density_overlap(self.h, C.c_int(int(on))), "asohf_set_density_overlap")
+
+    def density_wait(self, stream_ptr: int):
+        """Makes the CUDA stream `stream_ptr` wait for a deferred patch deposit."""
+        _check(self.L.asohf_density_wait(self.h, C.c_void_p(stream_ptr)), "asohf_density_wait")
+
     def set_epot_seed(self, seed: int):
         """Seed of COMPUTE_EPOT's sampling estimator (default 1)."""
         _check(self.L.asohf_set_epot_seed(self.h, C.c_uint32(int(seed))), "asohf_set_epot_seed")
@@ -401,6 +410,9 @@ class GpuBackend:
     def __init__(self, device: int = 0, cluster_threshold: int = 0, tiers=(0, 0), cluster_share: int = 0):
         self.a = Asohf(device)
         self._ids = None
+        # the patch deposit of density_renorm runs beside the x-sort and the
+        # halo finder; the grid copies and sync_outputs wait for it
+        self.a.set_density_overlap(True)
         if cluster_threshold:
             self.a.set_cluster_threshold(cluster_threshold)
         if cluster_share:
@@ -483,6 +495,7 @@ class GpuBackend:
         if n11 is None:
             return
         self._grids_pending = None
+        self.a.density_wait(self._copy_stream.cuda_stream)
         self.a.copy_to_host_sm(self._h1, self._g1, self._copy_stream)
         self.a.copy_to_host_sm(self._h11[:n11], self._g11[:n11], self._copy_stream)
         self._grids_done = torch.cuda.Event()
@@ -571,6 +584,12 @@ class DeviceBackend(GpuBackend):
 
     def download(self):
         return None
+
+    def sync_outputs(self):
+        """The caller's current stream waits for the deferred patch deposit
+        (U11 is complete for work issued on it afterwards)."""
+        import torch
+        self.a.density_wait(torch.cuda.current_stream(self.a.device).cuda_stream)
 
     def final_ids(self, pph, n):
         """PARTICLES_PER_HALO(1:n), left on the device (a torch tensor owned

@@ -87,6 +87,16 @@ struct asohf_ctx {
   // kernel phases of one call, when the stream is idle
   char* seg = nullptr;
   size_t seg_size = 0, seg_used = 0;
+  // Deferred patch deposit (asohf_set_density_overlap): with device outputs
+  // the patch kernels of asohf_density (and RENORM_DENSITY's patch scaling)
+  // run on dens_stream from the two density pools, which later calls do not
+  // reuse, and finish after the call returns; dens_done marks their end.
+  int density_overlap = 0;
+  cudaStream_t dens_stream = nullptr;
+  cudaEvent_t dens_fork = nullptr, dens_done = nullptr;
+  bool dens_pending = false;
+  struct Pool { char* base = nullptr; size_t size = 0, used = 0; };
+  Pool dpool[2];
   // device copies kept between calls: MOMENTO's sin^2 table for s2_nx, and
   // the last RADX(0:NX+1) the layer was given (h_radx: its host copy)
   float* d_s2 = nullptr;
@@ -125,6 +135,12 @@ inline void arena_reset(asohf_ctx* c) { c->arena_used = 0; }
 
 // Segment buffer: reserve() syncs the stream and regrows it (contents lost).
 int seg_reserve(asohf_ctx* c, size_t bytes);
+// Density pools 0 and 1 (bump allocators like the arena, reset by
+// dpool_reserve; the caller has waited for any deferred patch work).
+int dpool_reserve(asohf_ctx* c, int which, size_t bytes);
+void* dpool_alloc(asohf_ctx* c, int which, size_t bytes);
+// Waits (host) for a deferred patch deposit still in flight.
+int density_settle(asohf_ctx* c);
 void* seg_alloc(asohf_ctx* c, size_t bytes);
 
 int ctx_ensure_particles(asohf_ctx* c, int64_t n);

@@ -88,6 +88,54 @@ void* arena_alloc(asohf_ctx* c, size_t bytes) {
   return p;
 }
 
+int dpool_reserve(asohf_ctx* c, int which, size_t bytes) {
+  asohf_ctx::Pool& p = c->dpool[which];
+  p.used = 0;
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (p.size >= bytes) return ASOHF_OK;
+  cudaFree(p.base);
+  p.base = nullptr;
+  p.size = 0;
+  size_t want = bytes + bytes / 4;
+  ASOHF_CUDA(cudaMalloc(&p.base, want));
+  p.size = want;
+  return ASOHF_OK;
+}
+
+void* dpool_alloc(asohf_ctx* c, int which, size_t bytes) {
+  asohf_ctx::Pool& p = c->dpool[which];
+  size_t b = (bytes + 255) & ~(size_t)255;
+  if (p.used + b > p.size) return nullptr;
+  void* r = p.base + p.used;
+  p.used += b;
+  return r;
+}
+
+int density_settle(asohf_ctx* c) {
+  if (!c->dens_pending) return ASOHF_OK;
+  c->dens_pending = false;
+  ASOHF_CUDA(cudaEventSynchronize(c->dens_done));
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_set_density_overlap(asohf_ctx* c, int on) {
+  if (!c) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  if (on && !c->dens_stream) {
+    ASOHF_CUDA(cudaStreamCreateWithFlags(&c->dens_stream, cudaStreamNonBlocking));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->dens_fork, cudaEventDisableTiming));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->dens_done, cudaEventDisableTiming));
+  }
+  c->density_overlap = on ? 1 : 0;
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_density_wait(asohf_ctx* c, void* cuda_stream) {
+  if (!c) return ASOHF_ERR_INVALID;
+  if (c->dens_pending) ASOHF_CUDA(cudaStreamWaitEvent((cudaStream_t)cuda_stream, c->dens_done, 0));
+  return ASOHF_OK;
+}
+
 int seg_reserve(asohf_ctx* c, size_t bytes) {
   c->seg_used = 0;
   bytes = (bytes + 255) & ~(size_t)255;
@@ -178,6 +226,14 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   if (!c) return ASOHF_ERR_INVALID;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->dens_stream) {
+    cudaStreamSynchronize(c->dens_stream);
+    cudaStreamDestroy(c->dens_stream);
+    cudaEventDestroy(c->dens_fork);
+    cudaEventDestroy(c->dens_done);
+  }
+  cudaFree(c->dpool[0].base);
+  cudaFree(c->dpool[1].base);
   free_particles(c->p);
   free_particles(c->alt);
   cudaFree(c->rows[0]);
@@ -212,6 +268,7 @@ extern "C" int asohf_set_stream(asohf_ctx* c, void* s) {
 
 extern "C" int asohf_synchronize(asohf_ctx* c) {
   if (!c) return ASOHF_ERR_INVALID;
+  ASOHF_CHECK(density_settle(c));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   return ASOHF_OK;
 }

@@ -450,7 +450,15 @@ __global__ void k_bin_fill(const int32_t* __restrict__ binof, int64_t n, const i
   }
 }
 
-static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B) {
+// Where a density buffer lives: the call's arena, or density pool 0 when
+// the patch deposit is deferred (buffers the deferred kernels read).
+struct DAlloc {
+  asohf_ctx* c;
+  bool pool;
+  void* get(size_t bytes) const { return pool ? dpool_alloc(c, 0, bytes) : arena_alloc(c, bytes); }
+};
+
+static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B, DAlloc A = DAlloc{nullptr, false}) {
   int64_t n = c->p.n;
   int nx = (int)lrintf(lado0 / dx);
   int nb = (nx + bw - 1) / bw;
@@ -461,7 +469,7 @@ static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B) {
   B->bsz = lado0 / (float)nb;
   int32_t* binof = (int32_t*)arena_alloc(c, 4 * n);
   int32_t* cnt = (int32_t*)arena_alloc(c, 4 * (nbin + 1));
-  B->start = (int32_t*)arena_alloc(c, 4 * (nbin + 1));
+  B->start = (int32_t*)(A.pool ? A.get(4 * (nbin + 1)) : arena_alloc(c, 4 * (nbin + 1)));
   B->idx = (int32_t*)arena_alloc(c, 4 * n);
   size_t tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, B->start, (int)(nbin + 1));
@@ -492,7 +500,7 @@ struct DevMesh {
   float *rx, *ry, *rz;
 };
 
-static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d) {
+static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d, DAlloc A = DAlloc{nullptr, false}) {
   int np = 0;
   for (int ir = 1; ir <= mh->nl; ir++) np += mh->npatch[ir];
   d->np = np;
@@ -518,8 +526,8 @@ static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d) {
       hf[np + q] = mh->patchry[ip];
       hf[2 * np + q] = mh->patchrz[ip];
     }
-  int32_t* di = (int32_t*)arena_alloc(c, 16 * (size_t)np);
-  float* df = (float*)arena_alloc(c, 12 * (size_t)np);
+  int32_t* di = (int32_t*)(A.pool ? A.get(16 * (size_t)np) : arena_alloc(c, 16 * (size_t)np));
+  float* df = (float*)(A.pool ? A.get(12 * (size_t)np) : arena_alloc(c, 12 * (size_t)np));
   if (!di || !df) { free(hi); free(hf); return ASOHF_ERR_CAPACITY; }
   cudaMemcpyAsync(di, hi, 16 * (size_t)np, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(df, hf, 12 * (size_t)np, cudaMemcpyHostToDevice, c->stream);
@@ -987,26 +995,26 @@ __global__ void k_patch_finish(DevMesh M, const int32_t* __restrict__ order, con
 }
 
 // Patch order of the deposit: finest level first, table order within a level.
-static int patch_order(asohf_ctx* c, const asohf_mesh* mh, int32_t** d_order) {
+static int patch_order(asohf_ctx* c, const asohf_mesh* mh, int32_t** d_order, DAlloc A = DAlloc{nullptr, false}) {
   int np = 0;
   for (int ir = 1; ir <= mh->nl; ir++) np += mh->npatch[ir];
-  int32_t* h = (int32_t*)malloc(4 * (size_t)(np > 0 ? np : 1));
+  std::vector<int32_t> h((size_t)(np > 0 ? np : 1));
   int q = 0;
   for (int ir = mh->nl; ir >= 1; ir--) {
     int first = 0;
     for (int l = 1; l < ir; l++) first += mh->npatch[l];
     for (int p = 0; p < mh->npatch[ir]; p++) h[q++] = first + p;
   }
-  *d_order = (int32_t*)arena_alloc(c, 4 * (size_t)(np > 0 ? np : 1));
-  if (!*d_order) { free(h); return ASOHF_ERR_CAPACITY; }
-  ASOHF_CUDA(cudaMemcpyAsync(*d_order, h, 4 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+  const size_t bytes = 4 * (size_t)(np > 0 ? np : 1);
+  *d_order = (int32_t*)(A.pool ? A.get(bytes) : arena_alloc(c, bytes));
+  if (!*d_order) return ASOHF_ERR_CAPACITY;
+  ASOHF_CUDA(cudaMemcpyAsync(*d_order, h.data(), 4 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(h);
   return ASOHF_OK;
 }
 
-static float* upload_floats(asohf_ctx* c, const float* h, size_t n) {
-  float* d = (float*)arena_alloc(c, 4 * n);
+static float* upload_floats(asohf_ctx* c, const float* h, size_t n, DAlloc A = DAlloc{nullptr, false}) {
+  float* d = (float*)(A.pool ? A.get(4 * n) : arena_alloc(c, 4 * n));
   if (d) cudaMemcpyAsync(d, h, 4 * n, cudaMemcpyHostToDevice, c->stream);
   return d;
 }
@@ -1036,13 +1044,24 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
   if (np > 0 && !u11) return ASOHF_ERR_INVALID;
   const int64_t nall = c->p.n;
   const bool eqmass = c->mmin == c->norma;  // one particle mass in the store
+  // the previous call's deferred patch work reads the pools and writes U11
+  ASOHF_CHECK(density_settle(c));
+  const bool defer = c->density_overlap && on_device && np > 0 && n > 0 && c->dens_stream;
+  const DAlloc A{c, defer};
   size_t need = 12 * g + (on_device ? 0 : 4 * g + 4 * (size_t)np * NA * NA * NA) +
                 4 * KW * (ASOHF_NLEVELS + 1) + 96 * (size_t)np + 16384 +
                 (np ? bins_bytes(nall, lado0, dx, 2) + 17 * (size_t)nall : 0);
   ASOHF_CHECK(arena_reserve(c, need));
+  if (defer) {  // what the deferred kernels read: kernels, mesh, order, bins, staged particles, renorm dims
+    const int nbw = (int)lrintf(lado0 / dx);
+    const int64_t nb = (nbw + 1) / 2, nbin = nb * nb * nb;
+    ASOHF_CHECK(dpool_reserve(c, 0, 4 * KW * (ASOHF_NLEVELS + 1) + 4 * (ASOHF_NLEVELS + 1) + 48 * (size_t)np +
+                                        4 * (size_t)(nbin + 1) + 17 * (size_t)nall + 4 * NSLAB * (size_t)np +
+                                        16 * 256));
+  }
   float* hk = (float*)malloc(sizeof(float) * KW * (ASOHF_NLEVELS + 1));
   compute_kernels_host(nl, interp_degree, hk);
-  float* dk = upload_floats(c, hk, (size_t)KW * (ASOHF_NLEVELS + 1));
+  float* dk = upload_floats(c, hk, (size_t)KW * (ASOHF_NLEVELS + 1), A);
   const float* h0 = hk + ASOHF_NMAX_KERNELS;  // level 0: W(-1), W(0), W(1) at h0[-1..1]
   Terms27 T27;
   for (int kk = -1; kk <= 1; kk++)
@@ -1103,26 +1122,26 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
   if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(u1, du1, 4 * g, cudaMemcpyDeviceToHost, c->stream));
   if (np > 0) {
     DevMesh M;
-    ASOHF_CHECK(upload_mesh(c, mesh, &M));
+    ASOHF_CHECK(upload_mesh(c, mesh, &M, A));
     float hden[ASOHF_NLEVELS + 1];
     for (int ir = 0; ir <= ASOHF_NLEVELS; ir++) {
       float dxpa = dx / powf(2.0f, (float)ir);
       hden[ir] = dxpa * dxpa * dxpa * rote * (rete * rete * rete);
     }
-    float* dden = upload_floats(c, hden, ASOHF_NLEVELS + 1);
+    float* dden = upload_floats(c, hden, ASOHF_NLEVELS + 1, A);
     float* du11;
     ASOHF_CHECK(stage_out(c, u11, 4 * (size_t)np * NA * NA * NA, on_device, &du11));
     int32_t* order = nullptr;
     if (!dden) return ASOHF_ERR_CAPACITY;
-    ASOHF_CHECK(patch_order(c, mesh, &order));
+    ASOHF_CHECK(patch_order(c, mesh, &order, A));
     if (n > 0) {
       Bins B;
-      ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B));
-      float4* bp = (float4*)arena_alloc(c, 16 * (size_t)nall);
-      uint8_t* bs = (uint8_t*)arena_alloc(c, (size_t)nall);
+      ASOHF_CHECK(build_bins(c, lado0, dx, 2, &B, A));
+      float4* bp = (float4*)A.get(16 * (size_t)nall);
+      uint8_t* bs = (uint8_t*)A.get((size_t)nall);
       const int nunits = NSLAB * np;
       int64_t* ucnt = (int64_t*)arena_alloc(c, 8 * (size_t)nunits);
-      int32_t* sof = (int32_t*)arena_alloc(c, 4 * (size_t)nunits);
+      int32_t* sof = (int32_t*)A.get(4 * (size_t)nunits);
       if (!bp || !bs || !ucnt || !sof) return ASOHF_ERR_CAPACITY;
       {
         int kt_ = ktime_begin(c, "density_bin_stage");
@@ -1158,10 +1177,14 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         if (hs[u] >= 0) hmulti[hs[u]] = u;
       }
       size_t scratch_b = sizeof(double) * NA * NA * PZ * (size_t)nmulti;
-      int rcs = seg_reserve(c, sizeof(int2) * (size_t)nitems + 4 * (size_t)nmulti + scratch_b + 4096);
-      int2* ditems = rcs == ASOHF_OK ? (int2*)seg_alloc(c, sizeof(int2) * (size_t)nitems) : nullptr;
-      int32_t* dmulti = rcs == ASOHF_OK ? (int32_t*)seg_alloc(c, 4 * (size_t)(nmulti > 0 ? nmulti : 1)) : nullptr;
-      double* scratch = rcs == ASOHF_OK ? (double*)seg_alloc(c, scratch_b > 0 ? scratch_b : 8) : nullptr;
+      // work items, shared-unit list and scratch: the segment buffers, or
+      // density pool 1 when deferred
+      const size_t wbytes = sizeof(int2) * (size_t)nitems + 4 * (size_t)nmulti + scratch_b + 4096;
+      int rcs = defer ? dpool_reserve(c, 1, wbytes) : seg_reserve(c, wbytes);
+      auto walloc = [&](size_t b) { return defer ? dpool_alloc(c, 1, b) : seg_alloc(c, b); };
+      int2* ditems = rcs == ASOHF_OK ? (int2*)walloc(sizeof(int2) * (size_t)nitems) : nullptr;
+      int32_t* dmulti = rcs == ASOHF_OK ? (int32_t*)walloc(4 * (size_t)(nmulti > 0 ? nmulti : 1)) : nullptr;
+      double* scratch = rcs == ASOHF_OK ? (double*)walloc(scratch_b > 0 ? scratch_b : 8) : nullptr;
       if (!ditems || !dmulti || !scratch) {
         free(hc); free(hs); free(ord); free(hitems); free(hmulti);
         return rcs != ASOHF_OK ? rcs : ASOHF_ERR_CAPACITY;
@@ -1177,12 +1200,24 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       PatchWork W{ditems, sof, scratch};
       size_t smem = sizeof(double) * ACC_N + sizeof(int32_t) * CGX * CGX * CGZ + sizeof(float) * ktab_size(nl);
       ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      int kt_ = ktime_begin(c, "density_patches");
-      k_density_patches<<<(unsigned)nitems, PZ_BLOCK, smem, c->stream>>>(M, B, bp, bs, order, W, dx, dk,
-                                                                       eqmass ? 1 : 0, du11, dden);
-      if (nmulti) k_patch_finish<<<nmulti, 256, 0, c->stream>>>(M, order, dmulti, scratch, du11, dden);
-      ktime_end(c, kt_);
+      // deferred: the patch kernels run on the density stream after the
+      // staging above, and the call returns without waiting for them
+      cudaStream_t ps = c->stream;
+      if (defer) {
+        ASOHF_CUDA(cudaEventRecord(c->dens_fork, c->stream));
+        ASOHF_CUDA(cudaStreamWaitEvent(c->dens_stream, c->dens_fork, 0));
+        ps = c->dens_stream;
+      }
+      int kt_ = ktime_begin(c, "density_patches", ps);
+      k_density_patches<<<(unsigned)nitems, PZ_BLOCK, smem, ps>>>(M, B, bp, bs, order, W, dx, dk,
+                                                                eqmass ? 1 : 0, du11, dden);
+      if (nmulti) k_patch_finish<<<nmulti, 256, 0, ps>>>(M, order, dmulti, scratch, du11, dden);
+      ktime_end(c, kt_, ps);
       c->launches += 1 + (nmulti > 0);
+      if (defer) {
+        ASOHF_CUDA(cudaEventRecord(c->dens_done, ps));
+        c->dens_pending = true;
+      }
     } else {  // no particles: empty patches
       ASOHF_CUDA(cudaMemsetAsync(du11, 0, 4 * (size_t)np * NA * NA * NA, c->stream));
     }
@@ -1234,18 +1269,35 @@ extern "C" int asohf_renorm_density(asohf_ctx* c, int nx, const asohf_mesh* mesh
   c->launches++;
   if (np) {
     int base = mesh->npatch[0];
-    int32_t* hd = (int32_t*)malloc(12 * (size_t)np);
+    std::vector<int32_t> hd(3 * (size_t)np);
     for (int q = 0; q < np; q++) {
       hd[q] = mesh->patchnx[base + q];
       hd[np + q] = mesh->patchny[base + q];
       hd[2 * np + q] = mesh->patchnz[base + q];
     }
-    int32_t* dd = (int32_t*)arena_alloc(c, 12 * (size_t)np);
-    ASOHF_CUDA(cudaMemcpyAsync(dd, hd, 12 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
-    k_scale_patches<<<np, 256, 0, c->stream>>>(d11, dd, np, fdm);
+    // after a deferred patch deposit the scaling follows it on its stream,
+    // with the dimensions in its pool
+    const bool deferred = on_device && c->dens_pending;
+    int32_t* dd = (int32_t*)(deferred ? dpool_alloc(c, 0, 12 * (size_t)np) : arena_alloc(c, 12 * (size_t)np));
+    if (!dd) return ASOHF_ERR_CAPACITY;
+    // the dimensions go up on the context stream (a pageable copy on the
+    // density stream would make the host wait for the patch kernels)
+    ASOHF_CUDA(cudaMemcpyAsync(dd, hd.data(), 12 * (size_t)np, cudaMemcpyHostToDevice, c->stream));
+    cudaStream_t ps = c->stream;
+    if (deferred) {
+      ASOHF_CUDA(cudaEventRecord(c->dens_fork, c->stream));
+      ASOHF_CUDA(cudaStreamWaitEvent(c->dens_stream, c->dens_fork, 0));
+      ps = c->dens_stream;
+    }
+    k_scale_patches<<<np, 256, 0, ps>>>(d11, dd, np, fdm);
     c->launches++;
+    if (deferred) {
+      ASOHF_CUDA(cudaGetLastError());
+      ASOHF_CUDA(cudaEventRecord(c->dens_done, ps));
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));  // the base grid; the patches follow on their stream
+      return ASOHF_OK;
+    }
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-    free(hd);
   }
   ASOHF_CUDA(cudaGetLastError());
   if (!on_device) {

@@ -58,6 +58,17 @@ int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
  * hold `bytes` bytes; the copy is complete when the stream reaches it. */
 int asohf_copy_to_host_sm(asohf_ctx *ctx, void *host_dst, const void *dev_src, int64_t bytes,
                           void *cuda_stream);
+/* Tuning, no counterpart in the reference: with on = 1, asohf_density
+ * called with device outputs returns before its AMR-patch deposit is done:
+ * that work runs on a stream of the context's own, from buffers no other
+ * call reuses, beside whatever the caller issues next (the x-slab sort and
+ * the halo finder do not read U11), and asohf_renorm_density's patch scaling
+ * follows it there.  U11 is complete once asohf_density_wait has made a
+ * stream wait for it, or after asohf_synchronize.  U1 is complete on return
+ * as before. */
+int asohf_set_density_overlap(asohf_ctx *ctx, int on);
+/* Makes cuda_stream wait (device side) for a deferred patch deposit. */
+int asohf_density_wait(asohf_ctx *ctx, void *cuda_stream);
 /* Seed of COMPUTE_EPOT's sampling estimator (haloes_particles.f:1568-1626),
  * used for bound lists of MAX_PART_DSUM entries or more when energies are
  * on.  The reference draws its particle pairs from RANDOM_NUMBER after an
