@@ -356,16 +356,22 @@ class Asohf:
         return n.value
 
     def halofind_grid_base(self, nx, dx, u1, radx, contrastec, rote, rete, rodo, re0, bound, vol_solap_low, cat):
-        """HALOFIND_GRID at the base level without AMR recentering; fills
-        cat (host), returns NHALLEV(0)."""
-        u = np.ascontiguousarray(u1, np.float32).reshape(-1)
+        """HALOFIND_GRID at the base level without AMR recentering; u1 is a
+        host array or a torch CUDA tensor; fills cat (host), returns
+        NHALLEV(0)."""
+        if _is_torch(u1) and u1.is_cuda:
+            u, on_dev = u1.contiguous(), 1
+        else:
+            u, on_dev = np.ascontiguousarray(u1, np.float32).reshape(-1), 0
         r = np.ascontiguousarray(radx, np.float32)
         cc = cat.as_c()
         n = C.c_int32()
         f = C.c_float
+        # the catalogue stays on the host: the grid is read in place on the device
         _check(self.L.asohf_halofind_grid_base(self.h, C.c_int(nx), f(dx), _ptr(u), _ptr(r), f(contrastec), f(rote),
                                                f(rete), f(rodo), f(re0), f(bound), f(vol_solap_low), None,
-                                               C.byref(cc), C.c_int(0), C.byref(n)), "HALOFIND_GRID")
+                                               C.byref(cc), C.c_int(on_dev), C.c_int(0), C.byref(n)),
+               "HALOFIND_GRID")
         cat.nclus = cc.nclus
         return n.value
 

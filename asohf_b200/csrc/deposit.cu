@@ -731,10 +731,12 @@ struct PatchWork {
   double* scratch;           // NA*NA*PZ doubles per multi-slice unit
 };
 
-__global__ void __launch_bounds__(PZ_BLOCK, 3)
-k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t* __restrict__ S,
-                  const int32_t* __restrict__ order, PatchWork W, float dx, const float* __restrict__ kernels,
-                  int eqmass, float* __restrict__ u11, const float* __restrict__ denbas_lev) {
+// One work item (a slice of one 4-plane unit of a patch) of the patch deposit.
+__device__ __forceinline__ void density_patch_item(const int2 it, const DevMesh& M, const Bins& B,
+                                                   const float4* __restrict__ P, const uint8_t* __restrict__ S,
+                                                   const int32_t* __restrict__ order, const PatchWork& W, float dx,
+                                                   const float* __restrict__ kernels, int eqmass,
+                                                   float* __restrict__ u11, const float* __restrict__ denbas_lev) {
   extern __shared__ double acc[];  // ACC_N doubles (padded rows), count grid, kernel table
   int32_t* scnt = (int32_t*)(acc + ACC_N);
   float* ktab = (float*)(scnt + CGX * CGX * CGZ);
@@ -742,7 +744,6 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
   __shared__ double s_t27[27];
   __shared__ float s_rcp[NA + 1];  // 1/n for the clipped cloud widths n <= NA
   __shared__ int s_any;            // some level-0 host was counted
-  const int2 it = W.items[blockIdx.x];
   UnitGeo g;
   unit_geo(M, B, order, it.x, dx, g);
   float* out = u11 + (size_t)g.ip * NA * NA * NA + (size_t)g.slab * PZ * NA * NA;
@@ -976,6 +977,27 @@ k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t
   }
 }
 
+// The patch deposit over its work items: CTA b takes item b, and, with a
+// work counter (a grid smaller than the item count), the next free item
+// after each one -- the deferred deposit runs as one CTA per SM this way,
+// leaving the other slots of every SM to the kernels launched beside it.
+__global__ void __launch_bounds__(PZ_BLOCK, 3)
+k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t* __restrict__ S,
+                  const int32_t* __restrict__ order, PatchWork W, float dx, const float* __restrict__ kernels,
+                  int eqmass, float* __restrict__ u11, const float* __restrict__ denbas_lev, int nitems,
+                  int* __restrict__ next_item) {
+  __shared__ int s_item;
+  int item = blockIdx.x;
+  while (item < nitems) {
+    density_patch_item(W.items[item], M, B, P, S, order, W, dx, kernels, eqmass, u11, denbas_lev);
+    if (!next_item) break;
+    __syncthreads();  // the item's last reads of shared memory are done
+    if (threadIdx.x == 0) s_item = atomicAdd(next_item, 1) + (int)gridDim.x;
+    __syncthreads();
+    item = s_item;
+  }
+}
+
 // Units shared by several slices: the summed scratch slab to U11.
 __global__ void k_patch_finish(DevMesh M, const int32_t* __restrict__ order, const int32_t* __restrict__ multi,
                                const double* __restrict__ scratch, float* __restrict__ u11,
@@ -1179,13 +1201,14 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       size_t scratch_b = sizeof(double) * NA * NA * PZ * (size_t)nmulti;
       // work items, shared-unit list and scratch: the segment buffers, or
       // density pool 1 when deferred
-      const size_t wbytes = sizeof(int2) * (size_t)nitems + 4 * (size_t)nmulti + scratch_b + 4096;
+      const size_t wbytes = sizeof(int2) * (size_t)nitems + 4 * (size_t)nmulti + scratch_b + 4096 + 256;
       int rcs = defer ? dpool_reserve(c, 1, wbytes) : seg_reserve(c, wbytes);
       auto walloc = [&](size_t b) { return defer ? dpool_alloc(c, 1, b) : seg_alloc(c, b); };
       int2* ditems = rcs == ASOHF_OK ? (int2*)walloc(sizeof(int2) * (size_t)nitems) : nullptr;
       int32_t* dmulti = rcs == ASOHF_OK ? (int32_t*)walloc(4 * (size_t)(nmulti > 0 ? nmulti : 1)) : nullptr;
       double* scratch = rcs == ASOHF_OK ? (double*)walloc(scratch_b > 0 ? scratch_b : 8) : nullptr;
-      if (!ditems || !dmulti || !scratch) {
+      int* next_item = (rcs == ASOHF_OK && defer) ? (int*)walloc(sizeof(int)) : nullptr;
+      if (!ditems || !dmulti || !scratch || (defer && !next_item)) {
         free(hc); free(hs); free(ord); free(hitems); free(hmulti);
         return rcs != ASOHF_OK ? rcs : ASOHF_ERR_CAPACITY;
       }
@@ -1195,6 +1218,7 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         ASOHF_CUDA(cudaMemcpyAsync(dmulti, hmulti, 4 * (size_t)nmulti, cudaMemcpyHostToDevice, c->stream));
         ASOHF_CUDA(cudaMemsetAsync(scratch, 0, scratch_b, c->stream));
       }
+      if (next_item) ASOHF_CUDA(cudaMemsetAsync(next_item, 0, sizeof(int), c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
       free(hc); free(hs); free(ord); free(hitems); free(hmulti);
       PatchWork W{ditems, sof, scratch};
@@ -1209,8 +1233,10 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         ps = c->dens_stream;
       }
       int kt_ = ktime_begin(c, "density_patches", ps);
-      k_density_patches<<<(unsigned)nitems, PZ_BLOCK, smem, ps>>>(M, B, bp, bs, order, W, dx, dk,
-                                                                eqmass ? 1 : 0, du11, dden);
+      // deferred: one CTA per SM taking items from the counter; otherwise one CTA per item
+      const int64_t grid = defer ? (nitems < c->num_sms ? nitems : c->num_sms) : nitems;
+      k_density_patches<<<(unsigned)grid, PZ_BLOCK, smem, ps>>>(M, B, bp, bs, order, W, dx, dk, eqmass ? 1 : 0,
+                                                               du11, dden, (int)nitems, next_item);
       if (nmulti) k_patch_finish<<<nmulti, 256, 0, ps>>>(M, order, dmulti, scratch, du11, dden);
       ktime_end(c, kt_, ps);
       c->launches += 1 + (nmulti > 0);

@@ -346,7 +346,8 @@ __global__ void __launch_bounds__(256) k_grid_commit(GridIn G, GridChunk C, Grid
 extern "C" int asohf_halofind_grid_base(asohf_ctx* c, int nx, float dx, const float* u1, const float* radx,
                                         float contrastec, float rote, float rete, float rodo, float re0,
                                         float bound, float vol_solap_low, const asohf_mesh* mesh,
-                                        asohf_catalogue* cat, int on_device, int32_t* nhal) {
+                                        asohf_catalogue* cat, int u1_on_device, int cat_on_device,
+                                        int32_t* nhal) {
   if (!c || nx < 3 || nx > 1024 || !u1 || !radx || !cat || !nhal || cat->capacity < 0) return ASOHF_ERR_INVALID;
   if (mesh && mesh->nl > 0) {
     for (int ir = 1; ir <= mesh->nl; ir++)
@@ -367,10 +368,10 @@ extern "C" int asohf_halofind_grid_base(asohf_ctx* c, int nx, float dx, const fl
   // arena: the grid (when on the host), CONTA, RADX, the radii, counters and
   // the catalogue columns; segment arena: the candidates and chunk arrays
   const size_t cap = cat->capacity > 0 ? (size_t)cat->capacity : 1;
-  ASOHF_CHECK(arena_reserve(c, (on_device ? 0 : 4 * (size_t)g) + (size_t)g + 4 * (size_t)(nx + 2) +
+  ASOHF_CHECK(arena_reserve(c, (u1_on_device ? 0 : 4 * (size_t)g) + (size_t)g + 4 * (size_t)(nx + 2) +
                                    4 * GF_MAXSH + 64 + 64 + 44 * cap + 16 * 256));
   float* du = (float*)u1;
-  if (!on_device) {
+  if (!u1_on_device) {
     du = (float*)arena_alloc(c, 4 * (size_t)g);
     if (!du) return ASOHF_ERR_CAPACITY;
     ASOHF_CUDA(cudaMemcpyAsync(du, u1, 4 * (size_t)g, cudaMemcpyHostToDevice, c->stream));
@@ -465,7 +466,7 @@ extern "C" int asohf_halofind_grid_base(asohf_ctx* c, int nx, float dx, const fl
   if (st[1]) return st[1];
   const int nk = st[0];
   // the rows into the caller's catalogue (IF (IR.EQ.0) NCLUS=0)
-  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const cudaMemcpyKind kind = cat_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (nk > 0) {
     ASOHF_CUDA(cudaMemcpyAsync(cat->realclus, K.realclus, 4 * (size_t)nk, kind, c->stream));
     ASOHF_CUDA(cudaMemcpyAsync(cat->levhal, K.levhal, 4 * (size_t)nk, kind, c->stream));
@@ -485,7 +486,7 @@ extern "C" int asohf_halofind_grid_base(asohf_ctx* c, int nx, float dx, const fl
   int32_t nhallev[ASOHF_NLEVELS + 1] = {0};
   nhallev[0] = nk;
   int32_t nrem = 0;
-  if (nk > 0) ASOHF_CHECK(asohf_overlapping(c, cat, 0, nhallev, vol_solap_low, on_device, &nrem));
+  if (nk > 0) ASOHF_CHECK(asohf_overlapping(c, cat, 0, nhallev, vol_solap_low, cat_on_device, &nrem));
   *nhal = nk;
   return ASOHF_OK;
 }

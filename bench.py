@@ -201,6 +201,32 @@ def layer_bench(iters=10, warmup=3):
             "fwd_adj_GBps": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4), "peak_source": src}
 
 
+def grid_finder_bench(b, plan, iters=3):
+    """HALOFIND_GRID at the base level on the device, on the renormalised
+    base grid the benchmark step left on the device (512^3 cells), with the
+    snapshot's cosmology; device time per call (CUDA events)."""
+    import torch
+    from asohf_b200 import abi
+    cfg, cos = plan.snap.cfg, plan.cos
+    u1 = b._u1
+    args = (float(cos["contrastec"]), float(cos["rote"]), float(cos["rete"]), float(cos["rodo"]),
+            float(cos["re0"]), float(cfg.lado0) / 4, 0.2)
+    cat = abi.Catalogue(max(plan.capacity, 1 << 20))
+    st = torch.cuda.current_stream()
+    b.sync_outputs()
+    n = b.a.halofind_grid_base(cfg.nx, float(plan.dx), u1, plan.radx, *args, cat)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(iters):
+        n = b.a.halofind_grid_base(cfg.nx, float(plan.dx), u1, plan.radx, *args, cat)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return {"grid": f"{cfg.nx}^3 cells (the step's renormalised U1)", "haloes": int(n),
+            "ms": round(e0.elapsed_time(e1) / iters, 3),
+            "note": "HALOFIND_GRID base level (haloes_grids.f:287-582) and OVERLAPPING, catalogue to the host"}
+
+
 def replica_config(cfg, rank):
     """The snapshot recipe of one replica: the same sizes, seed + rank (the
     ranks share nothing, so each runs the hot path on its own snapshot)."""
@@ -232,6 +258,9 @@ def main():
     ap.add_argument("--no-layer", action="store_true", help="skip the deposit+Poisson layer leg")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs: only the device-timed steps)")
+    ap.add_argument("--no-grid", action="store_true", help="skip the grid halo finder leg")
+    ap.add_argument("--layer-only", action="store_true",
+                    help="only the deposit+Poisson layer leg (profiling runs of its kernels)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -269,6 +298,10 @@ def main():
     from asohf_b200 import api, driver, synth
 
     torch.cuda.set_device(local)
+    if args.layer_only:
+        if rank == 0:
+            print(json.dumps({"deposit_poisson": layer_bench()}))
+        return
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
@@ -385,6 +418,8 @@ def main():
     }
     if rank == 0 and not args.no_layer:
         out["deposit_poisson"] = layer_bench()
+    if rank == 0 and not args.no_grid:
+        out["grid_finder"] = grid_finder_bench(b, plan)
     if rank == 0 and not args.no_cpu:
         nth = os.cpu_count() or 1
         small = cpu_oracle_run(CPU_SAMPLE, 1, 0, nth)

@@ -233,10 +233,12 @@ int asohf_overlapping(asohf_ctx *ctx, asohf_catalogue *cat, int ir, const int32_
                       float vol_solap_low, int on_device, int32_t *removed);
 
 /* HALOFIND_GRID at the base level (haloes_grids.f:287-582): the candidate
- * peaks of u1 (NX^3 column-major, host or device by on_device) above
+ * peaks of u1 (NX^3 column-major; a device pointer when u1_on_device,
+ * else host) above
  * CONTRASTEC/6, taken from the densest, each grown in spherical shells to
  * the contrast CONTRASTEC unless a kept halo already covers its peak; then
- * OVERLAPPING at IR = 0.  radx: host RADX(0:NX+1).  The catalogue is reset
+ * OVERLAPPING at IR = 0.  radx: host RADX(0:NX+1).  cat's arrays are
+ * device pointers when cat_on_device, else host.  The catalogue is reset
  * (NCLUS = 0) and receives REALCLUS = -1, LEVHAL = 0, PATCHCLUS = 0,
  * CLUSRX..Z, RADIO, MASA and CLUSRXCM..ZCM of every halo; *nhal receives
  * NHALLEV(0).  A mesh with patches (the recentering on the AMR levels,
@@ -244,8 +246,8 @@ int asohf_overlapping(asohf_ctx *ctx, asohf_catalogue *cat, int ir, const int32_
  * BOUND returns ASOHF_ERR_NOT_CONVERGED (the reference's STOP 1). */
 int asohf_halofind_grid_base(asohf_ctx *ctx, int nx, float dx, const float *u1, const float *radx,
                              float contrastec, float rote, float rete, float rodo, float re0, float bound,
-                             float vol_solap_low, const asohf_mesh *mesh, asohf_catalogue *cat, int on_device,
-                             int32_t *nhal);
+                             float vol_solap_low, const asohf_mesh *mesh, asohf_catalogue *cat, int u1_on_device,
+                             int cat_on_device, int32_t *nhal);
 
 /* HALOFIND_PARTICLES (haloes_particles.f:578-1411) over haloes
  * lowh1..lowh2: recentering, SO growth, radial sort, unbinding, SO walk,
