@@ -979,8 +979,7 @@ __device__ __forceinline__ void density_patch_item(const int2 it, const DevMesh&
 
 // The patch deposit over its work items: CTA b takes item b, and, with a
 // work counter (a grid smaller than the item count), the next free item
-// after each one -- the deferred deposit runs as one CTA per SM this way,
-// leaving the other slots of every SM to the kernels launched beside it.
+// after each one.
 __global__ void __launch_bounds__(PZ_BLOCK, 3)
 k_density_patches(DevMesh M, Bins B, const float4* __restrict__ P, const uint8_t* __restrict__ S,
                   const int32_t* __restrict__ order, PatchWork W, float dx, const float* __restrict__ kernels,
@@ -1207,8 +1206,12 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       int2* ditems = rcs == ASOHF_OK ? (int2*)walloc(sizeof(int2) * (size_t)nitems) : nullptr;
       int32_t* dmulti = rcs == ASOHF_OK ? (int32_t*)walloc(4 * (size_t)(nmulti > 0 ? nmulti : 1)) : nullptr;
       double* scratch = rcs == ASOHF_OK ? (double*)walloc(scratch_b > 0 ? scratch_b : 8) : nullptr;
-      int* next_item = (rcs == ASOHF_OK && defer) ? (int*)walloc(sizeof(int)) : nullptr;
-      if (!ditems || !dmulti || !scratch || (defer && !next_item)) {
+      // one CTA per item; the kernel can also run as a smaller grid drawing
+      // items from a counter (next_item), which measured slower beside the
+      // halo finder (the patch deposit took 181 ms as one CTA per SM and
+      // slowed the halo kernels by 38 ms), so the full grid is launched
+      int* next_item = nullptr;
+      if (!ditems || !dmulti || !scratch) {
         free(hc); free(hs); free(ord); free(hitems); free(hmulti);
         return rcs != ASOHF_OK ? rcs : ASOHF_ERR_CAPACITY;
       }
@@ -1218,7 +1221,6 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         ASOHF_CUDA(cudaMemcpyAsync(dmulti, hmulti, 4 * (size_t)nmulti, cudaMemcpyHostToDevice, c->stream));
         ASOHF_CUDA(cudaMemsetAsync(scratch, 0, scratch_b, c->stream));
       }
-      if (next_item) ASOHF_CUDA(cudaMemsetAsync(next_item, 0, sizeof(int), c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
       free(hc); free(hs); free(ord); free(hitems); free(hmulti);
       PatchWork W{ditems, sof, scratch};
@@ -1233,9 +1235,7 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         ps = c->dens_stream;
       }
       int kt_ = ktime_begin(c, "density_patches", ps);
-      // deferred: one CTA per SM taking items from the counter; otherwise one CTA per item
-      const int64_t grid = defer ? (nitems < c->num_sms ? nitems : c->num_sms) : nitems;
-      k_density_patches<<<(unsigned)grid, PZ_BLOCK, smem, ps>>>(M, B, bp, bs, order, W, dx, dk, eqmass ? 1 : 0,
+      k_density_patches<<<(unsigned)nitems, PZ_BLOCK, smem, ps>>>(M, B, bp, bs, order, W, dx, dk, eqmass ? 1 : 0,
                                                                du11, dden, (int)nitems, next_item);
       if (nmulti) k_patch_finish<<<nmulti, 256, 0, ps>>>(M, order, dmulti, scratch, du11, dden);
       ktime_end(c, kt_, ps);
