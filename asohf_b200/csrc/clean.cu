@@ -18,6 +18,8 @@
 // result is known unless a halo no regular pair removes has a zero-speed
 // pair passing the distance and mass tests: that case is reported as
 // ASOHF_ERR_UNSUPPORTED instead of guessed.
+#include <vector>
+
 #include <cub/device/device_radix_sort.cuh>
 
 #include "common.cuh"
@@ -450,9 +452,9 @@ int clean_in(asohf_ctx* c, const asohf_catalogue* cat, int n, int on_device, Cle
 
 // Level of every entry 0..n-1 on the host (a copy when the catalogue is on
 // the device); ASOHF_ERR_INVALID unless the levels never decrease.
-int level_runs(asohf_ctx* c, const asohf_catalogue* cat, int n, int on_device, int32_t** lev_out) {
-  int32_t* lev = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
-  if (!lev) return ASOHF_ERR_CAPACITY;
+int level_runs(asohf_ctx* c, const asohf_catalogue* cat, int n, int on_device, std::vector<int32_t>& lev_v) {
+  lev_v.assign((size_t)(n > 0 ? n : 1), 0);
+  int32_t* lev = lev_v.data();
   if (on_device) {
     if (n) ASOHF_CUDA(cudaMemcpyAsync(lev, cat->levhal, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
@@ -460,11 +462,7 @@ int level_runs(asohf_ctx* c, const asohf_catalogue* cat, int n, int on_device, i
     memcpy(lev, cat->levhal, 4 * (size_t)n);
   }
   for (int i = 1; i < n; i++)
-    if (lev[i] < lev[i - 1]) {
-      free(lev);
-      return ASOHF_ERR_INVALID;
-    }
-  *lev_out = lev;
+    if (lev[i] < lev[i - 1]) return ASOHF_ERR_INVALID;
   return ASOHF_OK;
 }
 
@@ -477,24 +475,19 @@ extern "C" int asohf_check_rubish(asohf_ctx* c, asohf_catalogue* cat, int nclus,
   if (low2 < low1) return ASOHF_OK;
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
-  int32_t* lev = nullptr;
-  ASOHF_CHECK(level_runs(c, cat, nclus, on_device, &lev));
+  std::vector<int32_t> lev_v;
+  ASOHF_CHECK(level_runs(c, cat, nclus, on_device, lev_v));
+  const int32_t* lev = lev_v.data();
   CleanIo io;
   int rc = clean_in(c, cat, nclus, on_device, &io);
   int* dflags = rc == ASOHF_OK ? (int*)arena_alloc(c, 8) : nullptr;
-  if (rc != ASOHF_OK || !dflags) {
-    free(lev);
-    return rc != ASOHF_OK ? rc : ASOHF_ERR_CAPACITY;
-  }
+  if (rc != ASOHF_OK || !dflags) return rc != ASOHF_OK ? rc : ASOHF_ERR_CAPACITY;
   ASOHF_CUDA(cudaMemsetAsync(dflags, 0, 8, c->stream));
   int kt_ = ktime_begin(c, "check_rubish");
   int32_t* sidx = nullptr;
   float* sx = nullptr;
   rc = x_order(c, io.d.x, nclus, &sidx, &sx);
-  if (rc != ASOHF_OK) {
-    free(lev);
-    return rc;
-  }
+  if (rc != ASOHF_OK) return rc;
   // the window's levels in increasing order; each against everything before it
   for (int a = low1 - 1; a < low2;) {
     int b = a;
@@ -505,7 +498,6 @@ extern "C" int asohf_check_rubish(asohf_ctx* c, asohf_catalogue* cat, int nclus,
     a = b;
   }
   ktime_end(c, kt_);
-  free(lev);
   ASOHF_CUDA(cudaGetLastError());
   int hflags[2];
   ASOHF_CUDA(cudaMemcpyAsync(hflags, dflags, 8, cudaMemcpyDeviceToHost, c->stream));
@@ -526,24 +518,19 @@ extern "C" int asohf_accidental_substructure(asohf_ctx* c, asohf_catalogue* cat,
   if (nclus == 0) return ASOHF_OK;
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
-  int32_t* lev = nullptr;
-  ASOHF_CHECK(level_runs(c, cat, nclus, on_device, &lev));
+  std::vector<int32_t> lev_v;
+  ASOHF_CHECK(level_runs(c, cat, nclus, on_device, lev_v));
+  const int32_t* lev = lev_v.data();
   CleanIo io;
   int rc = clean_in(c, cat, nclus, on_device, &io);
   int* dcount = rc == ASOHF_OK ? (int*)arena_alloc(c, 8) : nullptr;
-  if (rc != ASOHF_OK || !dcount) {
-    free(lev);
-    return rc != ASOHF_OK ? rc : ASOHF_ERR_CAPACITY;
-  }
+  if (rc != ASOHF_OK || !dcount) return rc != ASOHF_OK ? rc : ASOHF_ERR_CAPACITY;
   ASOHF_CUDA(cudaMemsetAsync(dcount, 0, 8, c->stream));  // removals, largest confirmed radius
   int kt_ = ktime_begin(c, "accidental_substructure");
   int32_t* sidx = nullptr;
   float* sx = nullptr;
   rc = x_order(c, io.d.x, nclus, &sidx, &sx);
-  if (rc != ASOHF_OK) {
-    free(lev);
-    return rc;
-  }
+  if (rc != ASOHF_OK) return rc;
   k_rmax<<<148, 256, 0, c->stream>>>(io.d.r, io.d.rc, nclus, dcount + 1);
   c->launches++;
   // level by level: the lowest level is never removed, each next one is
@@ -559,7 +546,6 @@ extern "C" int asohf_accidental_substructure(asohf_ctx* c, asohf_catalogue* cat,
     a = b;
   }
   ktime_end(c, kt_);
-  free(lev);
   ASOHF_CUDA(cudaGetLastError());
   int hcount = 0;
   ASOHF_CUDA(cudaMemcpyAsync(&hcount, dcount, 4, cudaMemcpyDeviceToHost, c->stream));

@@ -512,8 +512,10 @@ static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d, DAlloc A 
         mh->patchnz[ip] < 1 || mh->patchnz[ip] > ASOHF_NAMRX)
       return ASOHF_ERR_INVALID;
   }
-  int32_t* hi = (int32_t*)malloc(4 * (size_t)np * 4);
-  float* hf = (float*)malloc(4 * (size_t)np * 3);
+  std::vector<int32_t> hi_v(4 * (size_t)np);
+  std::vector<float> hf_v(3 * (size_t)np);
+  int32_t* hi = hi_v.data();
+  float* hf = hf_v.data();
   int q = 0;
   for (int ir = 1; ir <= mh->nl; ir++)
     for (int p = 0; p < mh->npatch[ir]; p++, q++) {
@@ -528,12 +530,10 @@ static int upload_mesh(asohf_ctx* c, const asohf_mesh* mh, DevMesh* d, DAlloc A 
     }
   int32_t* di = (int32_t*)(A.pool ? A.get(16 * (size_t)np) : arena_alloc(c, 16 * (size_t)np));
   float* df = (float*)(A.pool ? A.get(12 * (size_t)np) : arena_alloc(c, 12 * (size_t)np));
-  if (!di || !df) { free(hi); free(hf); return ASOHF_ERR_CAPACITY; }
+  if (!di || !df) return ASOHF_ERR_CAPACITY;
   cudaMemcpyAsync(di, hi, 16 * (size_t)np, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(df, hf, 12 * (size_t)np, cudaMemcpyHostToDevice, c->stream);
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(hi);
-  free(hf);
   d->nx = di; d->ny = di + np; d->nz = di + 2 * np; d->level = di + 3 * np;
   d->rx = df; d->ry = df + np; d->rz = df + 2 * np;
   return ASOHF_OK;
@@ -1080,7 +1080,8 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
                                         4 * (size_t)(nbin + 1) + 17 * (size_t)nall + 4 * NSLAB * (size_t)np +
                                         16 * 256));
   }
-  float* hk = (float*)malloc(sizeof(float) * KW * (ASOHF_NLEVELS + 1));
+  std::vector<float> hk_v((size_t)KW * (ASOHF_NLEVELS + 1));
+  float* hk = hk_v.data();
   compute_kernels_host(nl, interp_degree, hk);
   float* dk = upload_floats(c, hk, (size_t)KW * (ASOHF_NLEVELS + 1), A);
   const float* h0 = hk + ASOHF_NMAX_KERNELS;  // level 0: W(-1), W(0), W(1) at h0[-1..1]
@@ -1099,7 +1100,6 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
     const int m = (abs(kk) + 1) * 9 + (abs(jj) + 1) * 3 + (abs(ii) + 1);
     if (T27.t[q] != T27.t[m]) sym27 = false;
   }
-  free(hk);
   float* du1;
   ASOHF_CHECK(stage_out(c, u1, 4 * g, on_device, &du1));
   const float xl = -lado0 / 2.0f;
@@ -1174,9 +1174,11 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         c->launches += 2;
       }
       // work list: slices of PSLICE candidates, the densest units first
-      int64_t* hc = (int64_t*)malloc(8 * (size_t)nunits);
-      int32_t* hs = (int32_t*)malloc(4 * (size_t)nunits);
-      int32_t* ord = (int32_t*)malloc(4 * (size_t)nunits);
+      std::vector<int64_t> hc_v((size_t)nunits);
+      std::vector<int32_t> hs_v((size_t)nunits), ord_v((size_t)nunits);
+      int64_t* hc = hc_v.data();
+      int32_t* hs = hs_v.data();
+      int32_t* ord = ord_v.data();
       ASOHF_CUDA(cudaMemcpyAsync(hc, ucnt, 8 * (size_t)nunits, cudaMemcpyDeviceToHost, c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
       int64_t nitems = 0;
@@ -1188,8 +1190,10 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         ord[u] = u;
       }
       std::sort(ord, ord + nunits, [&](int a2, int b2) { return hc[a2] > hc[b2] || (hc[a2] == hc[b2] && a2 < b2); });
-      int2* hitems = (int2*)malloc(sizeof(int2) * (size_t)nitems);
-      int32_t* hmulti = (int32_t*)malloc(4 * (size_t)(nmulti > 0 ? nmulti : 1));
+      std::vector<int2> hitems_v((size_t)nitems);
+      std::vector<int32_t> hmulti_v((size_t)(nmulti > 0 ? nmulti : 1));
+      int2* hitems = hitems_v.data();
+      int32_t* hmulti = hmulti_v.data();
       int64_t w = 0;
       for (int k = 0; k < nunits; k++) {
         int u = ord[k];
@@ -1211,10 +1215,7 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       // halo finder (the patch deposit took 181 ms as one CTA per SM and
       // slowed the halo kernels by 38 ms), so the full grid is launched
       int* next_item = nullptr;
-      if (!ditems || !dmulti || !scratch) {
-        free(hc); free(hs); free(ord); free(hitems); free(hmulti);
-        return rcs != ASOHF_OK ? rcs : ASOHF_ERR_CAPACITY;
-      }
+      if (!ditems || !dmulti || !scratch) return rcs != ASOHF_OK ? rcs : ASOHF_ERR_CAPACITY;
       ASOHF_CUDA(cudaMemcpyAsync(ditems, hitems, sizeof(int2) * (size_t)nitems, cudaMemcpyHostToDevice, c->stream));
       ASOHF_CUDA(cudaMemcpyAsync(sof, hs, 4 * (size_t)nunits, cudaMemcpyHostToDevice, c->stream));
       if (nmulti) {
@@ -1222,7 +1223,6 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         ASOHF_CUDA(cudaMemsetAsync(scratch, 0, scratch_b, c->stream));
       }
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-      free(hc); free(hs); free(ord); free(hitems); free(hmulti);
       PatchWork W{ditems, sof, scratch};
       size_t smem = sizeof(double) * ACC_N + sizeof(int32_t) * CGX * CGX * CGZ + sizeof(float) * ktab_size(nl);
       ASOHF_CUDA(cudaFuncSetAttribute(k_density_patches, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -21,6 +21,7 @@
 // The reference scans a full-(y,z) x-slab per query (haloes_particles.f:
 // 117-143); the column index returns the same member sets from the columns a
 // sphere overlaps.
+#include <vector>
 #include <stdlib.h>
 #include <string.h>
 
@@ -303,7 +304,8 @@ struct Tiers {
 // slot ids[i] (slot i when ids is null).  dbuf holds n entries.
 static int split_tiers(asohf_ctx* c, const int32_t* hcount, int n, int32_t* dbuf, Tiers* T,
                        const int32_t* ids = nullptr) {
-  int32_t* h = (int32_t*)malloc(4 * (size_t)(n > 0 ? n : 1));
+  std::vector<int32_t> h_v((size_t)(n > 0 ? n : 1));
+  int32_t* h = h_v.data();
   int cnt[4] = {0, 0, 0, 0};
   auto tier = [&](int32_t k) {
     return k >= c->cluster_min ? 3 : (k >= c->tier2_k ? 2 : (k >= c->tier1_k ? 1 : 0));
@@ -318,7 +320,6 @@ static int split_tiers(asohf_ctx* c, const int32_t* hcount, int n, int32_t* dbuf
   for (int i = 0; i < n; i++) h[fill[tier(hcount[i])]++] = ids ? ids[i] : i;
   if (n) ASOHF_CUDA(cudaMemcpyAsync(dbuf, h, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(h);
   for (int t = 0; t < 4; t++) {
     T->n[t] = cnt[t];
     T->slots[t] = dbuf + off[t];
@@ -337,7 +338,8 @@ static int split_cluster_tier(asohf_ctx* c, const int32_t* hcount, int n, int cb
     if (cb < 16) return k > 4 * sh ? 0 : 2;  // 8 CTAs at most
     return k > 8 * sh ? 0 : (k > 4 * sh ? 1 : 2);
   };
-  int32_t* h = (int32_t*)malloc(4 * (size_t)(T->n[3] > 0 ? T->n[3] : 1));
+  std::vector<int32_t> h_v((size_t)(T->n[3] > 0 ? T->n[3] : 1));
+  int32_t* h = h_v.data();
   int cnt[3] = {0, 0, 0};
   for (int i = 0; i < n; i++)
     if (hcount[i] >= c->cluster_min) cnt[pick(hcount[i])]++;
@@ -346,7 +348,6 @@ static int split_cluster_tier(asohf_ctx* c, const int32_t* hcount, int n, int cb
     if (hcount[i] >= c->cluster_min) h[fill[pick(hcount[i])]++] = i;
   if (T->n[3]) ASOHF_CUDA(cudaMemcpyAsync(T->slots[3], h, 4 * (size_t)T->n[3], cudaMemcpyHostToDevice, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  free(h);
   for (int q = 0; q < 3; q++) {
     nsub[q] = cnt[q];
     sub[q] = T->slots[3] + (q == 0 ? 0 : (q == 1 ? cnt[0] : cnt[0] + cnt[1]));
@@ -1841,11 +1842,16 @@ int ensure_pph(asohf_ctx* c, int64_t need) {
 int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int32_t* work, int nslots,
                       const int32_t* d_nbound, int64_t* d_ids_off, int64_t* total_out) {
   int n = low2;
-  int32_t* realclus = (int32_t*)malloc(4 * (size_t)n);
-  int32_t* indcs = (int32_t*)malloc(8 * (size_t)n);
-  int32_t* nbound = (int32_t*)malloc(4 * (size_t)(nslots > 0 ? nslots : 1));
-  int64_t* ids_off = (int64_t*)malloc(8 * (size_t)(nslots > 0 ? nslots : 1));
-  int32_t* slot_of = (int32_t*)malloc(4 * (size_t)(low2 - low1 + 1));
+  std::vector<int32_t> realclus_v((size_t)n);
+  int32_t* realclus = realclus_v.data();
+  std::vector<int32_t> indcs_v(2 * (size_t)n);
+  int32_t* indcs = indcs_v.data();
+  std::vector<int32_t> nbound_v((size_t)(nslots > 0 ? nslots : 1));
+  int32_t* nbound = nbound_v.data();
+  std::vector<int64_t> ids_off_v((size_t)(nslots > 0 ? nslots : 1));
+  int64_t* ids_off = ids_off_v.data();
+  std::vector<int32_t> slot_of_v((size_t)(low2 - low1 + 1));
+  int32_t* slot_of = slot_of_v.data();
   // entries before the window: from the caller's arrays when they are on the host
   int h0 = m.host ? m.w0 : 0;
   if (h0) {
@@ -1886,26 +1892,29 @@ int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int3
     ASOHF_CUDA(cudaMemcpyAsync(d_ids_off, ids_off, 8 * (size_t)nslots, cudaMemcpyHostToDevice, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   *total_out = j;
-  free(realclus); free(indcs); free(nbound); free(ids_off); free(slot_of);
   return ASOHF_OK;
 }
 
 // Work list: haloes of [low1, low2] with REALCLUS != 0, DMPCLUS descending
 // (largest first keeps the longest CTAs from finishing last).
-int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots,
-              int32_t** h_dm = nullptr) {
+int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, std::vector<int32_t>& h_work, int* nslots,
+              std::vector<int32_t>* h_dm = nullptr) {
   int nh = low2 - low1 + 1;
-  int32_t* rc = (int32_t*)malloc(4 * (size_t)nh);
-  int32_t* dm = (int32_t*)malloc(4 * (size_t)nh);
+  std::vector<int32_t> rc_v((size_t)nh);
+  int32_t* rc = rc_v.data();
+  std::vector<int32_t> dm_v((size_t)nh);
+  int32_t* dm = dm_v.data();
   ASOHF_CUDA(cudaMemcpyAsync(rc, m.d.realclus + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaMemcpyAsync(dm, m.d.dmpclus + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  int32_t* w = (int32_t*)malloc(4 * (size_t)(nh > 0 ? nh : 1));
+  h_work.assign(nh > 0 ? nh : 1, 0);
+  int32_t* w = h_work.data();
   int k = 0;
   for (int i = 0; i < nh; i++)
     if (rc[i] != 0) w[k++] = low1 - 1 + i;
   // sort by DMPCLUS descending (stable)
-  int32_t* tmp = (int32_t*)malloc(4 * (size_t)(k > 0 ? k : 1));
+  std::vector<int32_t> tmp_v((size_t)(k > 0 ? k : 1));
+  int32_t* tmp = tmp_v.data();
   for (int width = 1; width < k; width *= 2) {
     for (int i = 0; i < k; i += 2 * width) {
       int a = i, am = min(i + width, k), b = am, bm = min(i + 2 * width, k), o = i;
@@ -1918,15 +1927,10 @@ int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, 
     }
     memcpy(w, tmp, 4 * (size_t)k);
   }
-  free(tmp);
   if (h_dm) {  // DMPCLUS of each slot
-    int32_t* d = (int32_t*)malloc(4 * (size_t)(k > 0 ? k : 1));
-    for (int i = 0; i < k; i++) d[i] = dm[w[i] - (low1 - 1)];
-    *h_dm = d;
+    h_dm->assign(k > 0 ? k : 1, 0);
+    for (int i = 0; i < k; i++) (*h_dm)[i] = dm[w[i] - (low1 - 1)];
   }
-  free(rc);
-  free(dm);
-  *h_work = w;
   *nslots = k;
   return ASOHF_OK;
 }
@@ -2063,9 +2067,11 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
   ASOHF_CHECK(cat_mirror_in(c, cat, lowh2, on_device, &m, lowh1 - 1));
-  int32_t *hw, *hdm;
+  std::vector<int32_t> hw_v, hdm_v;
   int ns;
-  ASOHF_CHECK(make_work(c, m, lowh1, lowh2, &hw, &ns, &hdm));
+  ASOHF_CHECK(make_work(c, m, lowh1, lowh2, hw_v, &ns, &hdm_v));
+  int32_t* hw = hw_v.data();
+  int32_t* hdm = hdm_v.data();
   htime_end(c, "host:halo_mirror_in+work", ht);
   ht = htime_now();
   Store S = store_of(c);
@@ -2097,7 +2103,6 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     if (!d_work || !d_tg || !d_tm || !d_fill || !d_final || !g.cx || !g.cy || !g.cz ||
         !g.rgather || !g.rclus || !g.konta || !g.masadm || !g.status || !d_off || !d_nbound || !d_nscan ||
         !d_ids_off) {
-      free(hw); free(hdm);
       return ASOHF_ERR_CAPACITY;
     }
     ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
@@ -2105,11 +2110,16 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     // was pruned); haloes that outgrow their group size resume in a larger one
     Tiers tg, tm;
     GrowCaps caps{c->tier2_k, 4 * c->tier2_k, CB > 1 ? c->cluster_min : (int64_t)LLONG_MAX};
-    int32_t* hk = (int32_t*)malloc(4 * (size_t)ns);
-    int32_t* hst = (int32_t*)malloc(4 * (size_t)ns);
-    int64_t* hoff = (int64_t*)malloc(8 * (size_t)(ns + 1));
-    int32_t* hesc = (int32_t*)malloc(4 * (size_t)ns);
-    int32_t* kesc = (int32_t*)malloc(4 * (size_t)ns);
+    std::vector<int32_t> hk_v((size_t)ns);
+    int32_t* hk = hk_v.data();
+    std::vector<int32_t> hst_v((size_t)ns);
+    int32_t* hst = hst_v.data();
+    std::vector<int64_t> hoff_v((size_t)(ns + 1));
+    int64_t* hoff = hoff_v.data();
+    std::vector<int32_t> hesc_v((size_t)ns);
+    int32_t* hesc = hesc_v.data();
+    std::vector<int32_t> kesc_v((size_t)ns);
+    int32_t* kesc = kesc_v.data();
     ASOHF_CHECK(split_tiers(c, hdm, ns, d_tg, &tg));
     for (int round = 0;; round++) {
       {
@@ -2129,8 +2139,6 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       if (round >= 3) break;  // every tier was tried: reported below
       ASOHF_CHECK(split_tiers(c, kesc, ne, d_tg, &tg, hesc));
     }
-    free(hesc);
-    free(kesc);
     htime_end(c, "host:halo_grow", ht);
     ht = htime_now();
     hoff[0] = 0;
@@ -2178,7 +2186,6 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.timing = c->profiling;
     if (!k0 || !k1 || !v0 || !v1 || !t || !sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px ||
         !sg.pot || !sg.flag) {
-      free(hk); free(hst); free(hoff); free(hw); free(hdm);
       return ASOHF_ERR_CAPACITY;
     }
     if (T > 0) {
@@ -2261,14 +2268,11 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       ASOHF_CUDA(cudaGetLastError());
       c->pph_len = total;
     }
-    free(hk); free(hst); free(hoff);
   } else if (H.want_ids) {
     int64_t total;
     ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, 0, nullptr, nullptr, &total));
     c->pph_len = total;
   }
-  free(hw);
-  free(hdm);
   htime_end(c, "host:halo_ids", ht);
   ht = htime_now();
   ASOHF_CHECK(cat_mirror_out(c, &m));
@@ -2795,14 +2799,18 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
   }
 }
 
-static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t** h_work, int* nslots) {
+static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, std::vector<int32_t>& h_work,
+                         int* nslots) {
   int nh = low2 - low1 + 1;
-  int32_t* rc = (int32_t*)malloc(4 * (size_t)nh);
-  float* rs = (float*)malloc(4 * (size_t)nh);
+  std::vector<int32_t> rc_v((size_t)nh);
+  int32_t* rc = rc_v.data();
+  std::vector<float> rs_v((size_t)nh);
+  float* rs = rs_v.data();
   ASOHF_CUDA(cudaMemcpyAsync(rc, m.d.realclus + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaMemcpyAsync(rs, m.d.rsub + low1 - 1, 4 * (size_t)nh, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
-  int32_t* w = (int32_t*)malloc(4 * (size_t)(nh > 0 ? nh : 1));
+  h_work.assign(nh > 0 ? nh : 1, 0);
+  int32_t* w = h_work.data();
   int k = 0;
   for (int i = 0; i < nh; i++)
     if (rc[i] != 0) w[k++] = low1 - 1 + i;
@@ -2812,9 +2820,6 @@ static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, int32_t
     while (j >= 0 && rs[w[j] - (low1 - 1)] < rs[v - (low1 - 1)]) { w[j + 1] = w[j]; j--; }
     w[j + 1] = v;
   }
-  free(rc);
-  free(rs);
-  *h_work = w;
   *nslots = k;
   return ASOHF_OK;
 }
@@ -2834,7 +2839,8 @@ static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na,
     ktime_end(c, kt_);
   }
   c->launches++;
-  int32_t* hk = (int32_t*)malloc(4 * (size_t)na);
+  std::vector<int32_t> hk_v((size_t)na);
+  int32_t* hk = hk_v.data();
   ASOHF_CUDA(cudaMemcpyAsync(hk, d_konta, 4 * (size_t)na, cudaMemcpyDeviceToHost, c->stream));
   ASOHF_CUDA(cudaStreamSynchronize(c->stream));
   h_off[0] = 0;
@@ -2848,7 +2854,6 @@ static int gather_sorted(asohf_ctx* c, const Store& S, const ColIdx& ci, int na,
   int rt = split_tiers(c, hk, na, d_tslots, tiers);
   c->tier1_k = keep_t1;
   c->tier2_k = keep_t2;
-  free(hk);
   ASOHF_CHECK(rt);
   int64_t T = h_off[na];
   ASOHF_CUDA(cudaMemcpyAsync(d_off, h_off, 8 * (size_t)(na + 1), cudaMemcpyHostToDevice, c->stream));
@@ -2925,9 +2930,10 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
   ASOHF_CHECK(cat_mirror_in(c, cat, cat->nclus, on_device, &m, lowh1 - 1, true));
-  int32_t* hw;
+  std::vector<int32_t> hw_v;
   int ns;
-  ASOHF_CHECK(make_sub_work(c, m, lowh1, lowh2, &hw, &ns));
+  ASOHF_CHECK(make_sub_work(c, m, lowh1, lowh2, hw_v, &ns));
+  int32_t* hw = hw_v.data();
   htime_end(c, "host:sub_mirror_in+work", ht);
   ht = htime_now();
   Store S = store_of(c);
@@ -2957,13 +2963,16 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
     int32_t* d_nbound = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int32_t* d_nscan = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     int64_t* d_ids_off = (int64_t*)arena_alloc(c, 8 * (size_t)ns);
-    int64_t* h_off = (int64_t*)malloc(8 * (size_t)(ns + 1));
-    int32_t* h_act = (int32_t*)malloc(4 * (size_t)ns);
-    int32_t* h_done = (int32_t*)malloc(4 * (size_t)ns);
-    int32_t* h_st = (int32_t*)malloc(4 * (size_t)ns);
+    std::vector<int64_t> h_off_v((size_t)(ns + 1));
+    int64_t* h_off = h_off_v.data();
+    std::vector<int32_t> h_act_v((size_t)ns);
+    int32_t* h_act = h_act_v.data();
+    std::vector<int32_t> h_done_v((size_t)ns);
+    int32_t* h_done = h_done_v.data();
+    std::vector<int32_t> h_st_v((size_t)ns);
+    int32_t* h_st = h_st_v.data();
     if (!d_work || !pr.cx || !pr.status || !d_act || !d_konta || !d_off || !t_r || !jo.done || !jo.rclus ||
         !f_jjac || !f_masadm || !f_rclus || !f_rlast || !d_nbound || !d_nscan || !d_ids_off) {
-      free(hw); free(h_off); free(h_act); free(h_done); free(h_st);
       return ASOHF_ERR_CAPACITY;
     }
     ASOHF_CUDA(cudaMemcpyAsync(d_work, hw, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
@@ -3055,7 +3064,6 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       int32_t* d_ts = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
       if (!sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px || !sg.pot || !sg.flag ||
           !sg.final_b || !d_ts) {
-        free(hw); free(h_off); free(h_act); free(h_done); free(h_st);
         return ASOHF_ERR_CAPACITY;
       }
       SubMainIn in;
@@ -3091,13 +3099,11 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
         c->pph_len = total;
       }
     }
-    free(h_off); free(h_act); free(h_done); free(h_st);
   } else if (H.want_ids) {
     int64_t total;
     ASOHF_CHECK(assign_id_offsets(c, m, lowh1, lowh2, hw, 0, nullptr, nullptr, &total));
     c->pph_len = total;
   }
-  free(hw);
   htime_end(c, "host:sub_ids", ht);
   ht = htime_now();
   ASOHF_CHECK(cat_mirror_out(c, &m));

@@ -13,6 +13,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include <cub/device/device_radix_sort.cuh>
 
 #include "common.cuh"
@@ -84,26 +86,25 @@ static void momento_axis(int nx, float* s2) {
 }
 
 // Half-spectrum multiply: spec[(k*N + j)*(N/2+1) + i] *= KKK(i,j,k) / N^3.
-// One warp per (batch, k, j) row of N/2+1 values, lanes along i.
+// A flat grid-stride loop over the complex values (consecutive threads take
+// consecutive values, so every warp access is one contiguous 256-byte run);
+// the (i, j, k) of a value come from its index, s2 from the L1-resident table.
 __global__ void k_green(cufftComplex* __restrict__ spec, int nx, int batch, const float* __restrict__ s2,
                         float del2, float inv_n3) {
-  const int nh = nx / 2 + 1;
-  const int64_t rows = (int64_t)batch * nx * nx;
-  const int lane = threadIdx.x & 31;
-  for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < rows;
-       row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-    const int j = (int)(row % nx), k = (int)((row / nx) % nx);
-    cufftComplex* r = spec + row * nh;
-#pragma unroll 5
-    for (int i = lane; i < nh; i += 32) {
-      float den = (i == 0 && j == 0 && k == 0) ? 1.0e30f : __fadd_rn(__fadd_rn(s2[i], s2[j]), s2[k]);
-      float kkk = -del2 / den;
-      float f = __fmul_rn(kkk, inv_n3);
-      cufftComplex v = r[i];
-      v.x = __fmul_rn(v.x, f);
-      v.y = __fmul_rn(v.y, f);
-      r[i] = v;
-    }
+  const int64_t nh = nx / 2 + 1;
+  const int64_t total = (int64_t)batch * nx * nx * nh;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = q / nh;
+    const int i = (int)(q - row * nh), j = (int)(row % nx), k = (int)((row / nx) % nx);
+    const float den = (i == 0 && j == 0 && k == 0) ? 1.0e30f : __fadd_rn(__fadd_rn(__ldg(s2 + i), __ldg(s2 + j)),
+                                                                         __ldg(s2 + k));
+    const float kkk = -del2 / den;
+    const float f = __fmul_rn(kkk, inv_n3);
+    cufftComplex v = spec[q];
+    v.x = __fmul_rn(v.x, f);
+    v.y = __fmul_rn(v.y, f);
+    spec[q] = v;
   }
 }
 
@@ -114,11 +115,11 @@ static int green_table(asohf_ctx* c, int nx, const float** out) {
     cudaFree(c->d_s2);
     c->d_s2 = nullptr;
     c->s2_nx = 0;
-    float* hs2 = (float*)malloc(4 * (size_t)nx);
+    std::vector<float> hs2_v((size_t)nx);
+    float* hs2 = hs2_v.data();
     momento_axis(nx, hs2);
     cudaError_t e = cudaMalloc(&c->d_s2, 4 * (size_t)nx);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_s2, hs2, 4 * (size_t)nx, cudaMemcpyHostToDevice);
-    free(hs2);
     ASOHF_CUDA(e);
     c->s2_nx = nx;
   }
@@ -164,9 +165,8 @@ static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* r
   float inv_n3 = 1.0f / ((float)nx * (float)nx * (float)nx);
   {
     int kt_ = ktime_begin(c, "green_multiply");
-    int64_t rows = (int64_t)batch * nx * nx;
-    k_green<<<grid_for(rows * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2,
-                                                                             inv_n3);
+    const int64_t total = (int64_t)batch * nx * nx * (nx / 2 + 1);
+    k_green<<<grid_for(total, 256, c->num_sms * 16), 256, 0, c->stream>>>(spec, nx, batch, ds2, del2, inv_n3);
     ktime_end(c, kt_);
   }
   c->launches++;
