@@ -110,11 +110,12 @@ struct asohf_ctx {
   unsigned long long* d_work = nullptr;  // 8 counters
   // optional CUDA-event timing of named kernels (asohf_set_profiling)
   int profiling = 0;
-  struct KRec { const char* name; cudaEvent_t a, b; };  // events on the launch's stream
+  struct KRec { const char* name; cudaEvent_t a, b; cudaStream_t s; };  // events on the launch's stream
   KRec* krec = nullptr;
   int nkrec = 0, capkrec = 0;
   struct KSum { const char* name; double ms; int64_t n; };
-  KSum ksum[64];
+  static constexpr int KSUM_CAP = 160;
+  KSum ksum[KSUM_CAP];
   int nksum = 0;
 };
 

@@ -1,4 +1,7 @@
 // ctx.cu -- context lifetime, scratch arena, device particle store.
+#include <mutex>
+#include <set>
+#include <string>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -286,6 +289,7 @@ int ktime_begin(asohf_ctx* c, const char* name, cudaStream_t s) {
   }
   asohf_ctx::KRec& r = c->krec[c->nkrec];
   r.name = name;
+  r.s = s;
   if (cudaEventCreate(&r.a) != cudaSuccess) return -1;
   if (cudaEventCreate(&r.b) != cudaSuccess) { cudaEventDestroy(r.a); return -1; }
   cudaEventRecord(r.a, s);
@@ -302,7 +306,7 @@ static void ksum_add(asohf_ctx* c, const char* name, double ms) {
   for (k = 0; k < c->nksum; k++)
     if (strcmp(c->ksum[k].name, name) == 0) break;
   if (k == c->nksum) {
-    if (c->nksum >= 64) return;
+    if (c->nksum >= asohf_ctx::KSUM_CAP) return;
     c->ksum[k].name = name;
     c->ksum[k].ms = 0.0;
     c->ksum[k].n = 0;
@@ -322,27 +326,41 @@ void htime_end(asohf_ctx* c, const char* name, double t0) {
   if (c->profiling) ksum_add(c, name, htime_now() - t0);
 }
 
+// "idle:<name>" names, interned for the statistics table (a bounded set:
+// one per timed region name)
+static const char* idle_name(const char* name) {
+  static std::mutex mu;
+  static std::set<std::string> names;
+  std::lock_guard<std::mutex> lock(mu);
+  return names.insert(std::string("idle:") + name).first->c_str();
+}
+
+// Folds the recorded events into the statistics.  Besides each region's
+// time, the gaps of the context stream between consecutive top-level regions
+// on it (host work, synchronisations and untimed launches in between) are
+// added as "idle:<next region>"; the per-tier sub-regions ("name/tier") sit
+// inside their family's region and are left out of the gaps.
 static void ktime_flush(asohf_ctx* c) {
   cudaStreamSynchronize(c->stream);
+  int prev = -1;
   for (int i = 0; i < c->nkrec; i++) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->krec[i].a, c->krec[i].b);
-    int k;
-    for (k = 0; k < c->nksum; k++)
-      if (strcmp(c->ksum[k].name, c->krec[i].name) == 0) break;
-    if (k == c->nksum && c->nksum < 64) {
-      c->ksum[k].name = c->krec[i].name;
-      c->ksum[k].ms = 0.0;
-      c->ksum[k].n = 0;
-      c->nksum++;
+    ksum_add(c, c->krec[i].name, ms);
+    if (c->krec[i].s == c->stream && !strchr(c->krec[i].name, '/')) {  // top-level regions only
+      if (prev >= 0) {
+        float gap = 0.f;
+        if (cudaEventElapsedTime(&gap, c->krec[prev].b, c->krec[i].a) == cudaSuccess && gap > 0.f)
+          ksum_add(c, idle_name(c->krec[i].name), gap);
+      }
+      prev = i;
     }
-    if (k < 64) {
-      c->ksum[k].ms += ms;
-      c->ksum[k].n++;
-    }
+  }
+  for (int i = 0; i < c->nkrec; i++) {
     cudaEventDestroy(c->krec[i].a);
     cudaEventDestroy(c->krec[i].b);
   }
+  cudaGetLastError();
   c->nkrec = 0;
 }
 

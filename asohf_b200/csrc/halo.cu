@@ -1895,6 +1895,31 @@ int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int3
   return ASOHF_OK;
 }
 
+// Stable descending order of w[0..k) by key[] (an unsigned image of the
+// value that preserves its order): LSD radix sort on the complemented key,
+// 8 bits a pass, passes whose digit is the same for every entry skipped.
+// Equal values keep their order, as in a stable comparison sort.
+static void stable_desc(std::vector<uint32_t>& key, int32_t* w, int k) {
+  std::vector<uint32_t> key2((size_t)k);
+  std::vector<int32_t> tmp((size_t)k);
+  for (int i = 0; i < k; i++) key[i] = ~key[i];
+  for (int sh = 0; sh < 32; sh += 8) {
+    int64_t cnt[257] = {0};
+    for (int i = 0; i < k; i++) cnt[((key[i] >> sh) & 255u) + 1]++;
+    bool one = false;
+    for (int d = 0; d < 256; d++) one |= cnt[d + 1] == k;
+    if (one) continue;
+    for (int d = 0; d < 256; d++) cnt[d + 1] += cnt[d];
+    for (int i = 0; i < k; i++) {
+      const int64_t o = cnt[(key[i] >> sh) & 255u]++;
+      tmp[o] = w[i];
+      key2[o] = key[i];
+    }
+    memcpy(w, tmp.data(), 4 * (size_t)k);
+    key.swap(key2);
+  }
+}
+
 // Work list: haloes of [low1, low2] with REALCLUS != 0, DMPCLUS descending
 // (largest first keeps the longest CTAs from finishing last).
 int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, std::vector<int32_t>& h_work, int* nslots,
@@ -1912,21 +1937,11 @@ int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, std::vector<int32_
   int k = 0;
   for (int i = 0; i < nh; i++)
     if (rc[i] != 0) w[k++] = low1 - 1 + i;
-  // sort by DMPCLUS descending (stable)
-  std::vector<int32_t> tmp_v((size_t)(k > 0 ? k : 1));
-  int32_t* tmp = tmp_v.data();
-  for (int width = 1; width < k; width *= 2) {
-    for (int i = 0; i < k; i += 2 * width) {
-      int a = i, am = min(i + width, k), b = am, bm = min(i + 2 * width, k), o = i;
-      while (a < am && b < bm) {
-        if (dm[w[b] - (low1 - 1)] > dm[w[a] - (low1 - 1)]) tmp[o++] = w[b++];
-        else tmp[o++] = w[a++];
-      }
-      while (a < am) tmp[o++] = w[a++];
-      while (b < bm) tmp[o++] = w[b++];
-    }
-    memcpy(w, tmp, 4 * (size_t)k);
-  }
+  // sort by DMPCLUS descending (stable); the signed value biased to an
+  // unsigned key of the same order
+  std::vector<uint32_t> key((size_t)(k > 0 ? k : 1));
+  for (int i = 0; i < k; i++) key[i] = (uint32_t)dm[w[i] - (low1 - 1)] ^ 0x80000000u;
+  stable_desc(key, w, k);
   if (h_dm) {  // DMPCLUS of each slot
     h_dm->assign(k > 0 ? k : 1, 0);
     for (int i = 0; i < k; i++) (*h_dm)[i] = dm[w[i] - (low1 - 1)];
@@ -2814,12 +2829,16 @@ static int make_sub_work(asohf_ctx* c, CatMirror& m, int low1, int low2, std::ve
   int k = 0;
   for (int i = 0; i < nh; i++)
     if (rc[i] != 0) w[k++] = low1 - 1 + i;
-  for (int i = 1; i < k; i++) {  // insertion sort by RSUB descending (stable)
-    int32_t v = w[i];
-    int j = i - 1;
-    while (j >= 0 && rs[w[j] - (low1 - 1)] < rs[v - (low1 - 1)]) { w[j + 1] = w[j]; j--; }
-    w[j + 1] = v;
+  // sort by RSUB descending (stable): the float's bits mapped to an unsigned
+  // key of the same order, -0 taken as +0 (they compare equal)
+  std::vector<uint32_t> key((size_t)(k > 0 ? k : 1));
+  for (int i = 0; i < k; i++) {
+    const float v = rs[w[i] - (low1 - 1)];
+    uint32_t b = 0u;
+    if (v != 0.0f) memcpy(&b, &v, 4);
+    key[i] = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
   }
+  stable_desc(key, w, k);
   *nslots = k;
   return ASOHF_OK;
 }

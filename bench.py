@@ -376,9 +376,10 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}
 
     # roofline of the dominant kernel (kernel names only: "host:" entries are
-    # host phases, "k_x/tier" entries split a kernel's launches by size tier)
+    # host phases, "idle:" entries gaps of the stream, "k_x/tier" entries split
+    # a kernel's launches by size tier)
     hbm, src = peaks()
-    kern = {k: v for k, v in kstats.items() if not k.startswith("host:") and "/" not in k}
+    kern = {k: v for k, v in kstats.items() if not k.startswith(("host:", "idle:")) and "/" not in k}
     top = max(kern.items(), key=lambda kv: kv[1][0]) if kern else ("none", (0.0, 1))
     name, (tot_ms, nl) = top
     roofline = None
@@ -406,7 +407,10 @@ def main():
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches),
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in
                                 sorted(kstats.items(), key=lambda kv: -kv[1][0])
-                                if not k.startswith("host:")},
+                                if not k.startswith(("host:", "idle:"))},
+        "stream_idle_ms_per_step": {k[5:]: round(v[0] / args.steps, 3) for k, v in
+                                    sorted(kstats.items(), key=lambda kv: -kv[1][0])
+                                    if k.startswith("idle:") and v[0] / args.steps >= 0.1},
         "host_phases_ms_per_step": {k[5:]: round(v[0] / args.steps, 3) for k, v in
                                     sorted(kstats.items(), key=lambda kv: -kv[1][0])
                                     if k.startswith("host:")},
