@@ -469,15 +469,22 @@ struct RecShared {
   GX x;
 };
 
+template <int C>
+__device__ bool recenter_group_ngp(const Grp<C>& g, const Store& S, const ColIdx& ci, float* pcx, float* pcy,
+                                   float* pcz, float R, float dxpamin, RecShared& sh);
+
 // RECENTER_DENSITY_PEAK_PARTICLES (haloes_particles.f:367-574).  The member
 // list of each shrink step is the first cube intersected with every later
 // cube; instead of storing the list, each step re-reads the column index
 // over the latest cube (which holds the intersection; the radius halves
 // every step) and tests membership against all of them.  Returns false if
-// the shrink history overflows.
+// the shrink history overflows.  When no two masses of the store are 8 or
+// more apart every density step is the NGP one, and recenter_group_ngp
+// takes the same steps with one pass per step.
 template <int C>
 __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci, float* pcx, float* pcy,
                                float* pcz, float R, float dxpamin, RecShared& sh) {
+  if (S.eqmass_lt8) return recenter_group_ngp(g, S, ci, pcx, pcy, pcz, R, dxpamin, sh);
   float cx = *pcx, cy = *pcy, cz = *pcz;
   float radio = fmaxf(__fmul_rn(0.05f, R), dxpamin);
   int64_t lo, hi;
@@ -630,6 +637,126 @@ __device__ bool recenter_group(const Grp<C>& g, const Store& S, const ColIdx& ci
       v[3] += (double)__fmul_rn(e.z, mp);
     }
   });
+  gsum_dv<4>(g, v, sh.x);
+  *pcx = (float)(v[1] / v[0]);
+  *pcy = (float)(v[2] / v[0]);
+  *pcz = (float)(v[3] / v[0]);
+  return true;
+}
+
+// NGP cell (1..4 per axis, clamped) of the 4^3 grid from (xl, yl, zl), cell
+// size ddxx: the density step's own arithmetic.
+__device__ __forceinline__ int ngp_cell(const float4& e, float xl, float yl, float zl, float ddxx) {
+  int ix = (int)__fdiv_rn(__fsub_rn(e.x, xl), ddxx) + 1;
+  int jy = (int)__fdiv_rn(__fsub_rn(e.y, yl), ddxx) + 1;
+  int kz = (int)__fdiv_rn(__fsub_rn(e.z, zl), ddxx) + 1;
+  ix = ix < 1 ? 1 : (ix > 4 ? 4 : ix);
+  jy = jy < 1 ? 1 : (jy > 4 ? 4 : jy);
+  kz = kz < 1 ? 1 : (kz > 4 ? 4 : kz);
+  return ((kz - 1) * 4 + (jy - 1)) * 4 + (ix - 1);
+}
+
+// recenter_group with every density step NGP (all mass ratios under 8).
+// The steps and their arithmetic are recenter_group's; the passes are
+// merged: the pass that counts a step's members (the opening cube, then
+// each shrunk cube) also deposits them on the 4^3 grid of that cube, which
+// is the grid the next density step reads, and adds their centre-of-mass
+// sums, which the last step returns.  Each step's member set and the
+// entries every thread visits are the same as in the separate passes.
+template <int C>
+__device__ bool recenter_group_ngp(const Grp<C>& g, const Store& S, const ColIdx& ci, float* pcx, float* pcy,
+                                   float* pcz, float R, float dxpamin, RecShared& sh) {
+  float cx = *pcx, cy = *pcy, cz = *pcz;
+  float radio = fmaxf(__fmul_rn(0.05f, R), dxpamin);
+  float ddxx, xl, yl, zl;
+  int64_t lo, hi;
+  long long cnt;
+  // opening cube: grown x1.2 until it holds more than 32 members
+  for (int it = 0;; it++) {
+    slab_range(ci, cx, radio, &lo, &hi);
+    ddxx = __fdiv_rn(__fmul_rn(2.0f, radio), 4.0f);
+    xl = __fsub_rn(cx, radio); yl = __fsub_rn(cy, radio); zl = __fsub_rn(cz, radio);
+    for (int q = threadIdx.x; q < 64; q += blockDim.x) sh.dens[q] = 0.0;
+    __syncthreads();
+    long long c = 0;
+    gquery_box(g, ci, cx, cy, cz, radio, sh.qb, [&](const float4& e) {
+      int p = ppos(e);
+      if (p >= lo && p < hi && in_cube(e.x, e.y, e.z, cx, cy, cz, radio)) {
+        c++;
+        atomicAdd(&sh.dens[ngp_cell(e, xl, yl, zl, ddxx)], (double)S.mass(p));
+      }
+    });
+    cnt = gsum_ll(g, c, sh.lred, sh.x);
+    if (cnt > 32) break;
+    radio = __fmul_rn(radio, 1.2f);
+    if (it > 10000) return false;
+  }
+  const float c0x = cx, c0y = cy, c0z = cz, r0 = radio;
+  const int64_t lo0 = lo, hi0 = hi;
+  int nh = 0;
+  auto member = [&](const float4& e, int upto) -> bool {
+    int p = ppos(e);
+    if (!(p >= lo0 && p < hi0 && in_cube(e.x, e.y, e.z, c0x, c0y, c0z, r0))) return false;
+    for (int hh = 0; hh < upto; hh++)
+      if (!in_cube(e.x, e.y, e.z, sh.hist[hh][0], sh.hist[hh][1], sh.hist[hh][2], sh.hist[hh][3])) return false;
+    return true;
+  };
+  double v[4];
+  for (;;) {
+    // sh.dens holds the grid of the current members
+    __syncthreads();
+    if constexpr (C > 1) {  // sum the 4^3 grids of the cluster
+      g.sync();
+      cg::cluster_group cl = cg::this_cluster();
+      double t = 0.0;
+      if (threadIdx.x < 64)
+        for (int r = 0; r < C; r++) t += *cl.map_shared_rank(&sh.dens[threadIdx.x], r);
+      g.sync();
+      if (threadIdx.x < 64) sh.dens[threadIdx.x] = t;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {  // MAXLOC: first maximum, column-major
+      int b = 0;
+      for (int q = 1; q < 64; q++)
+        if (sh.dens[q] > sh.dens[b]) b = q;
+      sh.best = b;
+    }
+    __syncthreads();
+    int b = sh.best;
+    int ix = b % 4 + 1, jy = (b / 4) % 4 + 1, kz = b / 16 + 1;
+    cx = __fadd_rn(xl, __fmul_rn(__fsub_rn((float)ix, 0.5f), ddxx));
+    cy = __fadd_rn(yl, __fmul_rn(__fsub_rn((float)jy, 0.5f), ddxx));
+    cz = __fadd_rn(zl, __fmul_rn(__fsub_rn((float)kz, 0.5f), ddxx));
+    radio = __fdiv_rn(radio, 2.0f);
+    xl = __fsub_rn(cx, radio);
+    yl = __fsub_rn(cy, radio);
+    zl = __fsub_rn(cz, radio);
+    ddxx = __fdiv_rn(ddxx, 2.0f);
+    if (nh >= MAX_HIST) return false;
+    if (threadIdx.x == 0) {
+      sh.hist[nh][0] = cx; sh.hist[nh][1] = cy; sh.hist[nh][2] = cz; sh.hist[nh][3] = radio;
+    }
+    for (int q = threadIdx.x; q < 64; q += blockDim.x) sh.dens[q] = 0.0;
+    __syncthreads();
+    nh++;
+    // the shrunk cube's members: count, grid of the next step, centre of mass
+    long long c = 0;
+    v[0] = v[1] = v[2] = v[3] = 0.0;
+    gquery_box(g, ci, sh.hist[nh - 1][0], sh.hist[nh - 1][1], sh.hist[nh - 1][2], sh.hist[nh - 1][3], sh.qb,
+               [&](const float4& e) {
+                 if (member(e, nh)) {
+                   c++;
+                   float mp = S.mass(ppos(e));
+                   atomicAdd(&sh.dens[ngp_cell(e, xl, yl, zl, ddxx)], (double)mp);
+                   v[0] += (double)mp;
+                   v[1] += (double)__fmul_rn(e.x, mp);
+                   v[2] += (double)__fmul_rn(e.y, mp);
+                   v[3] += (double)__fmul_rn(e.z, mp);
+                 }
+               });
+    cnt = gsum_ll(g, c, sh.lred, sh.x);
+    if (cnt < 32) break;
+  }
   gsum_dv<4>(g, v, sh.x);
   *pcx = (float)(v[1] / v[0]);
   *pcy = (float)(v[2] / v[0]);
