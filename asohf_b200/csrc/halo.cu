@@ -985,69 +985,90 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
   g.sync();
 }
 
+// The potential part of an UNBINDING8 call: it depends only on the list, its
+// length and the outer radius, so a call on the list the previous call left
+// unchanged (nothing removed) reads it back instead of scanning again.
+struct PotCache {
+  bool valid = false;
+  int64_t k2 = 0;
+  float ref_max = 0.0f;
+  double pot_jj = 0.0, pot1 = 0.0;  // pot[] holds the scan's Q
+};
+
 // UNBINDING8 (haloes_particles.f:1828-1983) on the staged list.
 template <int C>
 __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H, int fac, float ref_max,
                              const SegView& v, uint8_t* flag, double* pot, int64_t k2, int64_t idx_vir,
-                             HaloState& h, GShared& sh) {
+                             HaloState& h, GShared& sh, PotCache& pc) {
   float cm[3] = {0, 0, 0}, vcm[3] = {0, 0, 0}, mmm = 0.0f;
   long long konta3 = 0;
   if (k2 > 0) {
     double norma = (double)normaf;
-    float lim = __fmul_rn(0.01f, ref_max);
-    // first J with DISTA(J) > lim (the list is sorted by distance); K2+1 if none
-    int64_t a = 0, b = k2;
-    if (k2 > 4096) {  // narrow the range with one parallel probe per thread of the CTA
-      const int64_t step = (k2 + blockDim.x - 1) / blockDim.x;
-      const int64_t jp = (int64_t)threadIdx.x * step;
-      bool above = jp < k2 && v.dm[jp].x > lim;
-      __syncthreads();
-      unsigned m = __ballot_sync(0xffffffffu, above);
-      if ((threadIdx.x & 31) == 0) sh.wcnt[threadIdx.x >> 5] = m ? (long long)((threadIdx.x & ~31) + __ffs(m) - 1) : LLONG_MAX;
-      __syncthreads();
-      long long fp = LLONG_MAX;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) fp = sh.wcnt[w] < fp ? sh.wcnt[w] : fp;
-      __syncthreads();
-      // probes are sorted: the answer lies in (probe fp-1, probe fp]
-      if (fp == LLONG_MAX) {  // after the last probe inside the list
-        int64_t lastp = (k2 - 1) / step;
-        if (lastp > (int64_t)blockDim.x - 1) lastp = (int64_t)blockDim.x - 1;
-        a = lastp * step + 1;
-      } else {
-        b = fp * step;
-        a = fp > 0 ? (fp - 1) * step + 1 : 0;
+    double pot_jj, pot1;
+    if (pc.valid && pc.k2 == k2 && pc.ref_max == ref_max) {
+      pot_jj = pc.pot_jj;
+      pot1 = pc.pot1;
+    } else {
+      float lim = __fmul_rn(0.01f, ref_max);
+      // first J with DISTA(J) > lim (the list is sorted by distance); K2+1 if none
+      int64_t a = 0, b = k2;
+      if (k2 > 4096) {  // narrow the range with one parallel probe per thread of the CTA
+        const int64_t step = (k2 + blockDim.x - 1) / blockDim.x;
+        const int64_t jp = (int64_t)threadIdx.x * step;
+        bool above = jp < k2 && v.dm[jp].x > lim;
+        __syncthreads();
+        unsigned m = __ballot_sync(0xffffffffu, above);
+        if ((threadIdx.x & 31) == 0) sh.wcnt[threadIdx.x >> 5] = m ? (long long)((threadIdx.x & ~31) + __ffs(m) - 1) : LLONG_MAX;
+        __syncthreads();
+        long long fp = LLONG_MAX;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) fp = sh.wcnt[w] < fp ? sh.wcnt[w] : fp;
+        __syncthreads();
+        // probes are sorted: the answer lies in (probe fp-1, probe fp]
+        if (fp == LLONG_MAX) {  // after the last probe inside the list
+          int64_t lastp = (k2 - 1) / step;
+          if (lastp > (int64_t)blockDim.x - 1) lastp = (int64_t)blockDim.x - 1;
+          a = lastp * step + 1;
+        } else {
+          b = fp * step;
+          a = fp > 0 ? (fp - 1) * step + 1 : 0;
+        }
       }
+      while (a < b) {
+        int64_t mid = (a + b) >> 1;
+        if (v.dm[mid].x > lim) b = mid; else a = mid + 1;
+      }
+      int64_t jj = a + 1;
+      // MASA8 and the POT recurrence of haloes_particles.f:1870-1893 in one
+      // scan: POT(J) = POT(JJ) + Q(J), Q(J) = sum over JJ < I <= J of
+      // MASA8(I) * BAS8(I) / DISTA(I)^2; pot[] receives Q
+      double mk2, qk2, mjj_part = 0.0;
+      gscan_aff(
+          g, 0, k2, [&](int64_t j) { return (double)v.dm[j].y / norma; },
+          [&](int64_t j) {
+            if (j < jj) return 0.0;
+            float dj = v.dm[j].x, dm1 = v.dm[j - 1].x;
+            double bas8 = (dj != dm1) ? (double)__fsub_rn(dj, dm1) : 0.0;
+            double djd = (double)dj;
+            return bas8 / (djd * djd);
+          },
+          [&](int64_t j, double M, double Q) {
+            pot[j] = Q;
+            if (j == jj - 1) mjj_part = M;
+          },
+          sh.wsum3, sh.x, &mk2, &qk2);
+      double mjj = mk2;
+      if (jj <= k2) {
+        gsum_dv<1>(g, &mjj_part, sh.x);
+        mjj = mjj_part;
+      }
+      pot_jj = mjj / (double)v.dm[jj - 1].x;
+      pot1 = (pot_jj + qk2) + mk2 / (double)ref_max;
+      pc.valid = true;
+      pc.k2 = k2;
+      pc.ref_max = ref_max;
+      pc.pot_jj = pot_jj;
+      pc.pot1 = pot1;
     }
-    while (a < b) {
-      int64_t mid = (a + b) >> 1;
-      if (v.dm[mid].x > lim) b = mid; else a = mid + 1;
-    }
-    int64_t jj = a + 1;
-    // MASA8 and the POT recurrence of haloes_particles.f:1870-1893 in one
-    // scan: POT(J) = POT(JJ) + Q(J), Q(J) = sum over JJ < I <= J of
-    // MASA8(I) * BAS8(I) / DISTA(I)^2; pot[] receives Q
-    double mk2, qk2, mjj_part = 0.0;
-    gscan_aff(
-        g, 0, k2, [&](int64_t j) { return (double)v.dm[j].y / norma; },
-        [&](int64_t j) {
-          if (j < jj) return 0.0;
-          float dj = v.dm[j].x, dm1 = v.dm[j - 1].x;
-          double bas8 = (dj != dm1) ? (double)__fsub_rn(dj, dm1) : 0.0;
-          double djd = (double)dj;
-          return bas8 / (djd * djd);
-        },
-        [&](int64_t j, double M, double Q) {
-          pot[j] = Q;
-          if (j == jj - 1) mjj_part = M;
-        },
-        sh.wsum3, sh.x, &mk2, &qk2);
-    double mjj = mk2;
-    if (jj <= k2) {
-      gsum_dv<1>(g, &mjj_part, sh.x);
-      mjj = mjj_part;
-    }
-    double pot_jj = mjj / (double)v.dm[jj - 1].x;
-    double pot1 = (pot_jj + qk2) + mk2 / (double)ref_max;
     int64_t lo, hi;
     double aa8 = norma * (double)__fdiv_rn(H.cgr, H.rete);
     float bb = 2.0f;
@@ -1545,16 +1566,18 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   // escape-velocity unbinding (haloes_particles.f:894-907)
   int64_t contaerr = K;
   int fac = 0;
+  PotCache pc;
   while (contaerr > 0 || fac < 3) {
     fac++;
     int64_t prev = k2;
     ep += (unsigned long long)k2;
-    long long kept = unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, idx_vir, h, sh);
+    long long kept = unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, idx_vir, h, sh, pc);
     if (kept != k2) {  // nothing removed: the list, IDX_VIR and the tail stay as they are
       int64_t nk2;
       compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
+      pc.valid = false;
     }
     ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
@@ -2628,16 +2651,18 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
   // escape-velocity unbinding with IDX_VIR = K2 (substructure.f:1172-1190)
   int64_t contaerr = konta;
   int fac = 0;
+  PotCache pc;
   while (contaerr > 0 || fac < 3) {
     fac++;
     int64_t prev = k2, iv = k2;
     ep += (unsigned long long)k2;
-    long long kept = unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, iv, h, sh);
+    long long kept = unbinding8_g(g, norma, H, fac, ref_max, cur, flag, pot, k2, iv, h, sh, pc);
     if (kept != k2) {
       int64_t nk2;
       compact_g(g, cur, nxt, flag, k2, &iv, &nk2, sh);
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
+      pc.valid = false;
     }
     ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
