@@ -985,14 +985,35 @@ __device__ void compact_g(const Grp<C>& g, const SegView& src, const SegView& ds
   g.sync();
 }
 
-// The potential part of an UNBINDING8 call: it depends only on the list, its
-// length and the outer radius, so a call on the list the previous call left
-// unchanged (nothing removed) reads it back instead of scanning again.
+// What an UNBINDING8 call leaves for the next call on the same list.  The
+// potential depends only on the list, its length and the outer radius, so a
+// call on the list the previous call left unchanged (nothing removed) reads
+// it back instead of scanning again.  When that previous call kept every
+// entry, and the velocity centre it returned is the one it was given, a later
+// call differs from it only in the factor BB: the previous call also counted
+// the entries the smaller factors (16, 4) would remove, and a call whose
+// factor removes none is known to return the same state, so it is skipped.
 struct PotCache {
   bool valid = false;
   int64_t k2 = 0;
   float ref_max = 0.0f;
   double pot_jj = 0.0, pot1 = 0.0;  // pot[] holds the scan's Q
+  bool flags_valid = false;         // the last flag pass kept every entry
+  float hv[3] = {0.0f, 0.0f, 0.0f}; // the velocity centre that pass used
+  double rm16 = 0.0, rm4 = 0.0;     // entries BB = 16 and BB = 4 would remove
+};
+
+// The same for UNBINDING_SIGMA: sigma depends on the list, IDX_VIR and the
+// velocity centre; a call with all three unchanged reuses it, and, when the
+// pass that computed it kept every entry, skips the flag pass too if its
+// factor (25, 16 or 9) removes none.
+struct SigCache {
+  bool valid = false;
+  int64_t k2 = 0, iv = 0;
+  float v[3] = {0.0f, 0.0f, 0.0f};
+  double sigma2 = 0.0;
+  bool flags_valid = false;
+  double rm[3] = {0.0, 0.0, 0.0};  // entries BB = 25, 16, 9 would remove
 };
 
 // UNBINDING8 (haloes_particles.f:1828-1983) on the staged list.
@@ -1006,6 +1027,9 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
     double norma = (double)normaf;
     double pot_jj, pot1;
     if (pc.valid && pc.k2 == k2 && pc.ref_max == ref_max) {
+      if (pc.flags_valid && fac >= 2 && h.v[0] == pc.hv[0] && h.v[1] == pc.hv[1] && h.v[2] == pc.hv[2] &&
+          (fac == 2 ? pc.rm16 : pc.rm4) == 0.0)
+        return k2;  // every entry kept again: the state stays as it is
       pot_jj = pc.pot_jj;
       pot1 = pc.pot1;
     } else {
@@ -1075,7 +1099,7 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
     if (fac == 1) bb = 8.0f;
     if (fac == 2) bb = 4.0f;
     bb = __fmul_rn(bb, bb);
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // 7 sums and the kept count
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // 7 sums, the kept count, removals at BB = 16, 4
     g.chunk(0, k2, &lo, &hi);
     const int bd = blockDim.x;
     // pairs of entries per thread, both read before either flag is stored
@@ -1104,6 +1128,8 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
         bool keep = !(vvv2 > __fmul_rn(bb, vesc2));
         flag[j] = keep;
         s[7] += keep ? 1.0 : 0.0;
+        s[8] += vvv2 > __fmul_rn(16.0f, vesc2) ? 1.0 : 0.0;
+        s[9] += vvv2 > __fmul_rn(4.0f, vesc2) ? 1.0 : 0.0;
         if (keep && j < idx_vir) {
           const float4 p = pv[u];
           double bas = (double)q.x;
@@ -1117,8 +1143,12 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
         }
       }
     }
-    gsum_dv<8>(g, s, sh.x);
+    gsum_dv<10>(g, s, sh.x);
     konta3 = (long long)s[7];
+    pc.flags_valid = konta3 == k2;
+    for (int q = 0; q < 3; q++) pc.hv[q] = h.v[q];
+    pc.rm16 = s[8];
+    pc.rm4 = s[9];
     if (s[6] > 0.0) {
       for (int q = 0; q < 3; q++) { cm[q] = (float)(s[q] / s[6]); vcm[q] = (float)(s[3 + q] / s[6]); }
       mmm = (float)s[6];
@@ -1131,25 +1161,40 @@ __device__ long long unbinding8_g(const Grp<C>& g, float normaf, const HConst& H
 // UNBINDING_SIGMA (haloes_particles.f:1987-2095) on the staged list.
 template <int C>
 __device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac, const SegView& v, uint8_t* flag,
-                                  int64_t k2, int64_t idx_vir, HaloState& h, GShared& sh) {
+                                  int64_t k2, int64_t idx_vir, HaloState& h, GShared& sh, SigCache& sc) {
   float bb = fmaxf(__fsub_rn(6.0f, __fmul_rn(1.0f, (float)(fac - 1))), 3.0f);
   bb = __fmul_rn(bb, bb);
   float cm[3] = {h.cm[0], h.cm[1], h.cm[2]}, vcm[3] = {h.v[0], h.v[1], h.v[2]}, mmm = 0.0f;
   long long konta3 = 0;
   if (k2 > 0) {
     int64_t lo, hi;
-    g.chunk(0, idx_vir < k2 ? idx_vir : k2, &lo, &hi);
-    double s2 = 0.0;
+    double sigma2;
+    if (sc.valid && sc.k2 == k2 && sc.iv == idx_vir && vcm[0] == sc.v[0] && vcm[1] == sc.v[1] &&
+        vcm[2] == sc.v[2]) {
+      if (sc.flags_valid && fac >= 2 && sc.rm[fac == 2 ? 0 : (fac == 3 ? 1 : 2)] == 0.0)
+        return k2;  // every entry kept again: the state stays as it is
+      sigma2 = sc.sigma2;
+    } else {
+      g.chunk(0, idx_vir < k2 ? idx_vir : k2, &lo, &hi);
+      double s2 = 0.0;
 #pragma unroll 4
-    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      float4 q = v.mv[j];
-      float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
-      s2 += (double)__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+      for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        float4 q = v.mv[j];
+        float ax = __fsub_rn(q.y, vcm[0]), ay = __fsub_rn(q.z, vcm[1]), az = __fsub_rn(q.w, vcm[2]);
+        s2 += (double)__fadd_rn(__fadd_rn(__fmul_rn(ax, ax), __fmul_rn(ay, ay)), __fmul_rn(az, az));
+      }
+      sigma2 = gsum_d(g, s2, sh.dred, sh.x);
+      if (idx_vir > 1) sigma2 = sigma2 / (double)(idx_vir - 1);
+      sc.valid = true;
+      sc.k2 = k2;
+      sc.iv = idx_vir;
+      for (int q = 0; q < 3; q++) sc.v[q] = vcm[q];
+      sc.sigma2 = sigma2;
+      sc.flags_valid = false;
     }
-    double sigma2 = gsum_d(g, s2, sh.dred, sh.x);
-    if (idx_vir > 1) sigma2 = sigma2 / (double)(idx_vir - 1);
     double thr = (double)bb * sigma2;
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const double thr25 = (double)25.0f * sigma2, thr16 = (double)16.0f * sigma2, thr9 = (double)9.0f * sigma2;
+    double s[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // 7 sums, the kept count, removals at BB = 25, 16, 9
     g.chunk(0, k2, &lo, &hi);
     const int bd = blockDim.x;
 #pragma unroll 1
@@ -1173,6 +1218,9 @@ __device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac
         bool keep = !((double)bas > thr);
         flag[j] = keep;
         s[7] += keep ? 1.0 : 0.0;
+        s[8] += (double)bas > thr25 ? 1.0 : 0.0;
+        s[9] += (double)bas > thr16 ? 1.0 : 0.0;
+        s[10] += (double)bas > thr9 ? 1.0 : 0.0;
         if (keep && j < idx_vir) {
           const float4 p = pv[u];
           double w = (double)q.x;
@@ -1186,8 +1234,10 @@ __device__ long long unbinding_sigma_g(const Grp<C>& g, const HConst& H, int fac
         }
       }
     }
-    gsum_dv<8>(g, s, sh.x);
+    gsum_dv<11>(g, s, sh.x);
     konta3 = (long long)s[7];
+    sc.flags_valid = konta3 == k2;
+    for (int q = 0; q < 3; q++) sc.rm[q] = s[8 + q];
     if (s[6] > 0.0) {
       for (int q = 0; q < 3; q++) { cm[q] = (float)(s[q] / s[6]); vcm[q] = (float)(s[3 + q] / s[6]); }
       mmm = (float)s[6];
@@ -1577,7 +1627,7 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
       compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
-      pc.valid = false;
+      pc.valid = pc.flags_valid = false;
     }
     ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
@@ -1587,16 +1637,18 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   // sigma clipping (haloes_particles.f:918-933)
   fac = 0;
   contaerr = k2;
+  SigCache sc;
   while (contaerr > 0 || fac < 4) {
     fac++;
     int64_t prev = k2;
     ep += (unsigned long long)k2;
-    long long kept = unbinding_sigma_g(g, H, fac, cur, flag, k2, idx_vir, h, sh);
+    long long kept = unbinding_sigma_g(g, H, fac, cur, flag, k2, idx_vir, h, sh, sc);
     if (kept != k2) {
       int64_t nk2;
       compact_g(g, cur, nxt, flag, k2, &idx_vir, &nk2, sh);
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
+      sc.valid = sc.flags_valid = false;
     }
     ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
@@ -2662,7 +2714,7 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
       compact_g(g, cur, nxt, flag, k2, &iv, &nk2, sh);
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
-      pc.valid = false;
+      pc.valid = pc.flags_valid = false;
     }
     ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
@@ -2671,16 +2723,18 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
   if (k2 < H.min_num_part) { finish_empty(); return; }
   fac = 0;
   contaerr = k2;
+  SigCache sc;
   while (contaerr > 0 || fac < 4) {
     fac++;
     int64_t prev = k2, iv = k2;
     ep += (unsigned long long)k2;
-    long long kept = unbinding_sigma_g(g, H, fac, cur, flag, k2, iv, h, sh);
+    long long kept = unbinding_sigma_g(g, H, fac, cur, flag, k2, iv, h, sh, sc);
     if (kept != k2) {
       int64_t nk2;
       compact_g(g, cur, nxt, flag, k2, &iv, &nk2, sh);
       SegView t = cur; cur = nxt; nxt = t; which ^= 1;
       k2 = nk2;
+      sc.valid = sc.flags_valid = false;
     }
     ref_max = k2 > 0 ? cur.dm[k2 - 1].x : 1.e10f;
     contaerr = prev - k2;
