@@ -714,7 +714,6 @@ struct GShared {  // per-warp slots: HW warps at most
   double wb[HW];
   double bc_d[2];
   long long bc_l[2];
-  double at[16];
   double wsum[HW];  // per-warp totals of the scans
   double wsum3[3 * HW];
   long long wcnt[HW];
@@ -1677,11 +1676,14 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
   float cvir = __fmul_rn(H.contrastec, fdm);
   int64_t jvir_min = (int64_t)__fmul_rn(0.1f, (float)k2);
   auto mn_of = [&](int64_t j) { return (double)__fdiv_rn(cur.dm[j].y, norma); };
-  // pass A: virial crossing and the crossings at or before it
+  // pass A: virial crossing and the crossings at or before it; BAS8 of
+  // every entry is kept in pot[] (free after the unbinding) for the later
+  // passes, which read it instead of scanning again
   long long jt[7];
   for (int q = 0; q < 7; q++) jt[q] = LLONG_MAX;
   gscan_d(g, 0, k2, 0.0, mn_of,
             [&](int64_t j, double bas8) {
+              pot[j] = bas8;
               int64_t J = j + 1;
               if (J <= jjcore) return;
               float vol = so_den(cur.dm[j].x, rete, pi);
@@ -1700,59 +1702,58 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     for (int q = 0; q < 6; q++)
       if (jt[q] > jvir) { jt[q] = LLONG_MAX; again = true; }
     if (again) {  // pass A2: crossings after the virial one, with BAS8 - m(J_vir)
-      gscan_d(g, 0, k2, 0.0, mn_of,
-                [&](int64_t j, double bas8) {
-                  int64_t J = j + 1;
-                  if (J <= jvir) return;
-                  double b8 = bas8 - mvir;
-                  float vol = so_den(cur.dm[j].x, rete, pi);
-                  float delta2 = (float)((double)norma * b8 / (double)vol / (double)rote);
-                  for (int q = 0; q < 6; q++)
-                    if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
-                },
-                sh.wsum, sh.x);
+      int64_t lo, hi;
+      g.chunk(jvir, k2, &lo, &hi);
+      for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        const int64_t J = j + 1;
+        double b8 = pot[j] - mvir;
+        float vol = so_den(cur.dm[j].x, rete, pi);
+        float delta2 = (float)((double)norma * b8 / (double)vol / (double)rote);
+        for (int q = 0; q < 6; q++)
+          if (delta2 <= thr[q] && J < jt[q]) jt[q] = J;
+      }
       gmin_llv<6>(g, jt, sh.lred, sh.x);
     }
   }
   bool exit_found = jvir != LLONG_MAX && jt[5] != LLONG_MAX;
   int64_t jend = exit_found ? max(jvir, jt[5]) : k2;
-  // pass B: BAS8 at the crossings, V_c max over the walked range, and the
-  // velocity sums up to the virial crossing (or the whole walk)
-  if (threadIdx.x < 16) sh.at[threadIdx.x] = 0.0;
-  __syncthreads();
+  // pass B: BAS8 at the crossings (read from pot[]), V_c max over the walked
+  // range, and the velocity sums up to the virial crossing (or the whole walk)
   double best_v = -1.0;
   long long best_j = LLONG_MAX;
   double best_b = 0.0;
   int64_t jv = jvir != LLONG_MAX ? jvir : jend;
-  gscan_d(g, 0, jend, 0.0, mn_of,
-            [&](int64_t j, double bas8) {
-              int64_t J = j + 1;
-              double b8 = (jvir != LLONG_MAX && J > jvir) ? bas8 - mvir : bas8;
-              for (int q = 0; q < 7; q++)
-                if (J == jt[q]) sh.at[q] = (q == 6) ? bas8 : b8;
-              if (J == jv) sh.at[7] = bas8;
-              if (J <= jjcore) return;
-              float bas2 = (float)(b8 / (double)cur.dm[j].x);
-              if (best_before((double)bas2, J, best_v, best_j)) {
-                best_v = bas2;
-                best_j = J;
-                best_b = b8;
-              }
-            },
-            sh.wsum, sh.x);
-  __syncthreads();
   double sv[11];
-  for (int q = 0; q < 8; q++) sv[q] = threadIdx.x == 0 ? sh.at[q] : 0.0;
-  sv[8] = sv[9] = sv[10] = 0.0;
+  for (int q = 0; q < 11; q++) sv[q] = 0.0;
+  if (lead) {  // one contribution per group
+    for (int q = 0; q < 7; q++)
+      if (jt[q] != LLONG_MAX && jt[q] <= jend) {
+        const double bas8 = pot[jt[q] - 1];
+        sv[q] = (q == 6 || jvir == LLONG_MAX || jt[q] <= jvir) ? bas8 : bas8 - mvir;
+      }
+    if (jv >= 1) sv[7] = pot[jv - 1];
+  }
   {
     int64_t lo, hi;
-    g.chunk(0, jv, &lo, &hi);
+    g.chunk(0, jend, &lo, &hi);
     for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      float4 q = cur.mv[j];
-      float mn = __fdiv_rn(q.x, norma);
-      sv[8] += (double)__fmul_rn(mn, q.y);
-      sv[9] += (double)__fmul_rn(mn, q.z);
-      sv[10] += (double)__fmul_rn(mn, q.w);
+      const int64_t J = j + 1;
+      if (j < jv) {
+        float4 q = cur.mv[j];
+        float mn = __fdiv_rn(q.x, norma);
+        sv[8] += (double)__fmul_rn(mn, q.y);
+        sv[9] += (double)__fmul_rn(mn, q.z);
+        sv[10] += (double)__fmul_rn(mn, q.w);
+      }
+      if (J <= jjcore) continue;
+      const double bas8 = pot[j];
+      double b8 = (jvir != LLONG_MAX && J > jvir) ? bas8 - mvir : bas8;
+      float bas2 = (float)(b8 / (double)cur.dm[j].x);
+      if (best_before((double)bas2, J, best_v, best_j)) {
+        best_v = bas2;
+        best_j = J;
+        best_b = b8;
+      }
     }
   }
   gsum_dv<11>(g, sv, sh.x);
