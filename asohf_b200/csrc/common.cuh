@@ -79,6 +79,11 @@ struct asohf_ctx {
   int64_t colpart_cap = 0;
   // bound-particle ID stream (PARTICLES_PER_HALO)
   int32_t* d_pph = nullptr;
+  // sorted member segments of the subhaloes whose Jacobi radius is fixed,
+  // in the order they were fixed (SUBSTRUCTURE_PARTICLES)
+  unsigned long long* sfin_k = nullptr;
+  int32_t* sfin_v = nullptr;
+  int64_t sfin_cap = 0;
   int64_t pph_len = 0, pph_cap = 0;
   // scratch arena (bump allocator, reset at the start of every entry point)
   char* arena = nullptr;

@@ -248,6 +248,8 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaFree(c->d_colstart);
   cudaFree(c->d_colpart);
   cudaFree(c->d_pph);
+  cudaFree(c->sfin_k);
+  cudaFree(c->sfin_v);
   cudaFree(c->arena);
   cudaFree(c->seg);
   cudaFree(c->d_work);

@@ -3011,6 +3011,47 @@ __global__ void k_gather_f(const int32_t* __restrict__ act, int na, const float*
   if (i < na) dst[i] = src[act[i]];
 }
 
+// Copies segment b of (keys, vals) at off[b] (cnt[b] entries) to dst[b] of
+// (dk, dv); dst[b] < 0: not copied.  One CTA per segment.
+__global__ void k_copy_segments(const unsigned long long* __restrict__ keys, const int32_t* __restrict__ vals,
+                                const int64_t* __restrict__ off, const int32_t* __restrict__ cnt,
+                                const int64_t* __restrict__ dst, unsigned long long* __restrict__ dk,
+                                int32_t* __restrict__ dv) {
+  const int b = blockIdx.x;
+  const int64_t d = dst[b];
+  if (d < 0) return;
+  const int64_t o = off[b], n = cnt[b];
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+    dk[d + j] = keys[o + j];
+    dv[d + j] = vals[o + j];
+  }
+}
+
+// Room for n entries in the store of fixed segments, keeping the first
+// `keep` entries.
+static int sfin_reserve(asohf_ctx* c, int64_t n, int64_t keep) {
+  if (n <= c->sfin_cap) return ASOHF_OK;
+  const int64_t cap = n + n / 2 + 4096;
+  unsigned long long* nk = nullptr;
+  int32_t* nv = nullptr;
+  ASOHF_CUDA(cudaMalloc(&nk, 8 * (size_t)cap));
+  if (cudaMalloc(&nv, 4 * (size_t)cap) != cudaSuccess) {
+    cudaFree(nk);
+    return ASOHF_ERR_CUDA;
+  }
+  if (keep > 0) {
+    ASOHF_CUDA(cudaMemcpyAsync(nk, c->sfin_k, 8 * (size_t)keep, cudaMemcpyDeviceToDevice, c->stream));
+    ASOHF_CUDA(cudaMemcpyAsync(nv, c->sfin_v, 4 * (size_t)keep, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(c->sfin_k);
+  cudaFree(c->sfin_v);
+  c->sfin_k = nk;
+  c->sfin_v = nv;
+  c->sfin_cap = cap;
+  return ASOHF_OK;
+}
+
 extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k, const asohf_mesh* mesh,
                                             asohf_catalogue* cat, int ir, const int32_t* subs_lev,
                                             int on_device) {
@@ -3096,6 +3137,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
     int32_t* d_fill = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
     if (!d_pos || !d_tsl || !d_fill) rc = ASOHF_ERR_CAPACITY;
     else k_iota32<<<(ns + 255) / 256, 256, 0, c->stream>>>(d_pos, ns);
+    std::vector<int64_t> fin_off((size_t)ns, 0), fin_cnt((size_t)ns, 0), h_dst((size_t)ns, -1);
+    int64_t fin_total = 0;
     for (int iter = 0; na > 0 && rc == ASOHF_OK; iter++) {
       if (iter > 200) { rc = ASOHF_ERR_TIMEOUT; break; }
       ASOHF_CUDA(cudaMemcpyAsync(d_act, h_act, 4 * (size_t)na, cudaMemcpyHostToDevice, c->stream));
@@ -3122,6 +3165,26 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       ASOHF_CUDA(cudaGetLastError());
       ASOHF_CUDA(cudaMemcpyAsync(h_done, jo.done, 4 * (size_t)na, cudaMemcpyDeviceToHost, c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
+      // the members of the subhaloes fixed in this round, gathered at their
+      // final radius, are kept: the main pass reads them from there
+      int64_t fin0 = fin_total;
+      for (int q = 0; q < na; q++) {
+        h_dst[q] = -1;
+        if (h_done[q]) {
+          const int s = h_act[q];
+          fin_off[s] = fin_total;
+          fin_cnt[s] = h_off[q + 1] - h_off[q];
+          h_dst[q] = fin_total;
+          fin_total += fin_cnt[s];
+        }
+      }
+      if (fin_total > fin0) {
+        ASOHF_CHECK(sfin_reserve(c, fin_total, fin0));
+        ASOHF_CUDA(cudaMemcpyAsync(d_ids_off, h_dst.data(), 8 * (size_t)na, cudaMemcpyHostToDevice, c->stream));
+        k_copy_segments<<<na, 256, 0, c->stream>>>(keys, vals, d_off, d_konta, d_ids_off, c->sfin_k, c->sfin_v);
+        c->launches++;
+        ASOHF_CUDA(cudaGetLastError());
+      }
       int nn = 0;
       for (int q = 0; q < na; q++)
         if (!h_done[q]) h_act[nn++] = h_act[q];
@@ -3130,13 +3193,28 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
     htime_end(c, "host:sub_jacobi_loop", ht);
     ht = htime_now();
     if (rc == ASOHF_OK) {
-      // last gather of every subhalo at its final radius, then the main pass
-      unsigned long long* keys;
-      int32_t* vals;
-      int64_t T;
-      Tiers tf;
-      ASOHF_CHECK(gather_sorted(c, S, ci, ns, d_pos, pr.cx, pr.cy, pr.cz, f_rlast, d_konta, d_off, h_off, &keys,
-                                &vals, &T, true, &tf, d_tsl, d_fill));
+      // every subhalo's members at its final radius, in slot order, from the
+      // segments kept as the radii were fixed
+      h_off[0] = 0;
+      for (int s = 0; s < ns; s++) h_off[s + 1] = h_off[s] + fin_cnt[s];
+      const int64_t T = h_off[ns];
+      const size_t work = ((size_t)T + ns) * (2 * (8 + 16 + 16) + 8 + 1) + 16384;
+      ASOHF_CHECK(seg_reserve(c, (size_t)T * 12 + work + 16384));
+      unsigned long long* keys = (unsigned long long*)seg_alloc(c, 8 * (size_t)T + 8);
+      int32_t* vals = (int32_t*)seg_alloc(c, 4 * (size_t)T + 4);
+      int64_t* d_src = (int64_t*)seg_alloc(c, 8 * (size_t)ns);
+      if (!keys || !vals || !d_src) return ASOHF_ERR_CAPACITY;
+      for (int s = 0; s < ns; s++) { h_dst[s] = h_off[s]; h_st[s] = (int32_t)fin_cnt[s]; }
+      ASOHF_CUDA(cudaMemcpyAsync(d_src, fin_off.data(), 8 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+      ASOHF_CUDA(cudaMemcpyAsync(d_ids_off, h_dst.data(), 8 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+      ASOHF_CUDA(cudaMemcpyAsync(d_konta, h_st, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+      ASOHF_CUDA(cudaMemcpyAsync(d_off, h_off, 8 * (size_t)(ns + 1), cudaMemcpyHostToDevice, c->stream));
+      if (T > 0) {
+        k_copy_segments<<<ns, 256, 0, c->stream>>>(c->sfin_k, c->sfin_v, d_src, d_konta, d_ids_off, keys, vals);
+        c->launches++;
+      }
+      ASOHF_CUDA(cudaGetLastError());
+      ASOHF_CUDA(cudaStreamSynchronize(c->stream));
       htime_end(c, "host:sub_final_gather", ht);
       ht = htime_now();
       // staged lists of the kept members, tiers by that count
