@@ -46,6 +46,7 @@ struct asohf_ctx {
   // forked from and joined back into `stream` with the events
   static const int NSIDE = 5;
   cudaStream_t side[NSIDE] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int side_prio = 0;  // the side streams take the context stream's priority
   cudaEvent_t ev_fork = nullptr, ev_join[NSIDE] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int num_sms = 148;
   // size tiers of the per-halo launches (members): >= cluster_min a CTA

@@ -125,7 +125,12 @@ extern "C" int asohf_set_density_overlap(asohf_ctx* c, int on) {
   if (!c) return ASOHF_ERR_INVALID;
   ASOHF_CUDA(cudaSetDevice(c->device));
   if (on && !c->dens_stream) {
-    ASOHF_CUDA(cudaStreamCreateWithFlags(&c->dens_stream, cudaStreamNonBlocking));
+    // the least priority: its CTAs are scheduled when the hot path's streams
+    // have none waiting, so the deferred deposit fills the gaps of the halo
+    // finder instead of holding the SMs ahead of it
+    int least = 0, greatest = 0;
+    ASOHF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    ASOHF_CUDA(cudaStreamCreateWithPriority(&c->dens_stream, cudaStreamNonBlocking, least));
     ASOHF_CUDA(cudaEventCreateWithFlags(&c->dens_fork, cudaEventDisableTiming));
     ASOHF_CUDA(cudaEventCreateWithFlags(&c->dens_done, cudaEventDisableTiming));
   }
@@ -265,8 +270,24 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   return ASOHF_OK;
 }
 
+// The side streams (size tiers) run at the context stream's priority, so a
+// caller that raises its stream's priority raises the whole hot path above
+// the deferred deposit (created at the least priority).
 extern "C" int asohf_set_stream(asohf_ctx* c, void* s) {
   if (!c) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  int prio = 0;
+  ASOHF_CUDA(cudaStreamGetPriority((cudaStream_t)s, &prio));
+  if (prio != c->side_prio) {
+    for (int i = 0; i < asohf_ctx::NSIDE; i++) {
+      cudaStream_t n = nullptr;
+      ASOHF_CUDA(cudaStreamCreateWithPriority(&n, cudaStreamNonBlocking, prio));
+      ASOHF_CUDA(cudaStreamSynchronize(c->side[i]));
+      cudaStreamDestroy(c->side[i]);
+      c->side[i] = n;
+    }
+    c->side_prio = prio;
+  }
   c->stream = (cudaStream_t)s;
   return ASOHF_OK;
 }

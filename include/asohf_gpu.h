@@ -35,6 +35,11 @@ const char *asohf_last_error_detail(void);
 /* Context: device, stream, device particle store and scratch arena. */
 int asohf_create(int device, asohf_ctx **out);
 int asohf_destroy(asohf_ctx *ctx);
+/* The stream the context's kernels run on.  The size tiers of the per-halo
+   kernels run on side streams created at this stream's priority; the
+   deferred patch deposit (asohf_set_density_overlap) runs at the least
+   priority, so a caller that runs the hot path on a high-priority stream
+   lets the deposit fill the gaps the halo finder leaves. */
 int asohf_set_stream(asohf_ctx *ctx, void *cuda_stream);
 int asohf_synchronize(asohf_ctx *ctx);
 /* Number of kernels this context has launched (diagnostics). */
@@ -60,9 +65,10 @@ int asohf_copy_to_host_sm(asohf_ctx *ctx, void *host_dst, const void *dev_src, i
                           void *cuda_stream);
 /* Tuning, no counterpart in the reference: with on = 1, asohf_density
  * called with device outputs returns before its AMR-patch deposit is done:
- * that work runs on a stream of the context's own, from buffers no other
- * call reuses, beside whatever the caller issues next (the x-slab sort and
- * the halo finder do not read U11), and asohf_renorm_density's patch scaling
+ * that work runs on a stream of the context's own (at the least priority),
+ * from buffers no other call reuses, beside whatever the caller issues next
+ * (the x-slab sort and the halo finder do not read U11), and
+ * asohf_renorm_density's patch scaling
  * follows it there.  U11 is complete once asohf_density_wait has made a
  * stream wait for it, or after asohf_synchronize.  U1 is complete on return
  * as before. */
