@@ -60,7 +60,8 @@ def load():
                      "asohf_halofind_particles", "asohf_substructure_particles",
                      "asohf_get_particles_per_halo", "asohf_set_profiling", "asohf_kernel_stats",
                      "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers",
-                     "asohf_copy_to_host_sm", "asohf_set_cluster_share",
+                     "asohf_copy_to_host_sm", "asohf_set_cluster_share", "asohf_prefetch_particles",
+                     "asohf_copy_to_host_async", "asohf_copy_wait",
                      "asohf_check_rubish", "asohf_accidental_substructure"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
@@ -199,6 +200,32 @@ class Asohf:
         _check(self.L.asohf_upload_particles(self.h, C.byref(p), C.c_int(int(dev))),
                "asohf_upload_particles")
         self.n = p.n
+
+    def copy_to_host_async(self, dst, src):
+        """Copy of device tensor src into page-locked host tensor dst (same
+        size) on a copy engine, chunk by chunk, after the work issued so far;
+        copy_wait() waits for every such copy."""
+        if dst.numel() * dst.element_size() != src.numel() * src.element_size() or not dst.is_pinned():
+            raise ValueError("copy_to_host_async: a page-locked tensor of the device tensor's size")
+        _check(self.L.asohf_copy_to_host_async(self.h, C.c_void_p(dst.data_ptr()), C.c_void_p(src.data_ptr()),
+                                               C.c_int64(src.numel() * src.element_size())),
+               "asohf_copy_to_host_async")
+
+    def copy_wait(self, stream=None):
+        """Makes `stream` (the host, when None) wait for the copies of
+        copy_to_host_async issued so far."""
+        s = C.c_void_p(stream.cuda_stream) if stream is not None else None
+        _check(self.L.asohf_copy_wait(self.h, s), "asohf_copy_wait")
+
+    def prefetch_particles(self, x, y, z, vx, vy, vz, m, ids):
+        """Starts copying these host arrays (page-locked) for the next
+        upload_particles of the same arrays, beside the work in flight."""
+        p = abi.ParticlesC()
+        p.n = int(x.shape[0])
+        for f, a in zip(["x", "y", "z", "vx", "vy", "vz", "m"], [x, y, z, vx, vy, vz, m]):
+            setattr(p, f, C.cast(_ptr(a), _fp))
+        p.id = C.cast(_ptr(ids), _ip)
+        _check(self.L.asohf_prefetch_particles(self.h, C.byref(p)), "asohf_prefetch_particles")
 
     def download_particles(self, out=None):
         """Returns (x, y, z, vx, vy, vz, m, id) numpy arrays in store order."""
@@ -426,9 +453,18 @@ class GpuBackend:
         if tiers != (0, 0):
             self.a.set_group_tiers(*tiers)
 
+    # host particles of the next run, copied while this run computes (set by
+    # a caller that runs snapshots back to back; None: no prefetch)
+    prefetch_next = None
+
+    def prefetch(self, parts):
+        self.a.prefetch_particles(parts.x, parts.y, parts.z, parts.vx, parts.vy, parts.vz, parts.m, parts.id)
+
     def upload(self, parts):
         self.a.upload_particles(parts.x, parts.y, parts.z, parts.vx, parts.vy, parts.vz, parts.m,
                                 parts.id)
+        if self.prefetch_next is not None:
+            self.prefetch(self.prefetch_next)
 
     def download(self):
         from types import SimpleNamespace
@@ -485,41 +521,34 @@ class GpuBackend:
         # both calls return with their work complete on the device
         self.a.density(nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree, self._g1, self._g11)
         self.a.renorm_density(nx, mesh, fdm, self._g1, self._g11)
-        if getattr(self, "_copy_stream", None) is None:
-            self._copy_stream = torch.cuda.Stream(device=dev)
-        self._grids_pending = n11  # issued after SORT_DM_PARTICLES_X (see sort_x)
+        self._grids_pending = n11
+        self._issue_grid_copy()
         u1 = self._h1.numpy().reshape(nx, nx, nx)
         u11 = self._h11[:n11].numpy().reshape(-1, abi.NAMRX ** 3)[: mesh.total]
         return u1, u11
 
     def _issue_grid_copy(self):
-        # SM stores, not a copy engine, so the halo finder's short copies on
-        # the context stream do not queue behind this one; issued once the
-        # x-sort (whose store permutation it would slow down) is done
-        import torch
+        # on a copy engine, chunk by chunk (the halo finder's short copies on
+        # the context stream wait for one chunk at most), after the deferred
+        # patch deposit; no SM time is taken from the halo finder
         n11 = getattr(self, "_grids_pending", None)
         if n11 is None:
             return
         self._grids_pending = None
-        self.a.density_wait(self._copy_stream.cuda_stream)
-        self.a.copy_to_host_sm(self._h1, self._g1, self._copy_stream)
-        self.a.copy_to_host_sm(self._h11[:n11], self._g11[:n11], self._copy_stream)
-        self._grids_done = torch.cuda.Event()
-        self._grids_done.record(self._copy_stream)
+        self.a.copy_to_host_async(self._h1, self._g1)
+        self.a.copy_to_host_async(self._h11[:n11], self._g11[:n11])
+        self._grids_copying = True
 
     def sort_x(self, nx, lado0):
-        nd = self.a.sort_dm_particles_x(nx, lado0)
-        self._issue_grid_copy()
-        return nd
+        return self.a.sort_dm_particles_x(nx, lado0)
 
     def sync_outputs(self):
         """Waits for the host copies of the grids left in flight by
-        density_renorm (issued after the next sort_x, or here)."""
+        density_renorm."""
         self._issue_grid_copy()
-        ev = getattr(self, "_grids_done", None)
-        if ev is not None:
-            ev.synchronize()
-            self._grids_done = None
+        if getattr(self, "_grids_copying", False):
+            self.a.copy_wait()
+            self._grids_copying = False
 
     def tsc_deposit(self, nx, lado0, dx, radx, rote, rete, mesh, fp64=True):
         u1 = np.zeros(nx ** 3, np.float32)

@@ -11,6 +11,10 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <mutex>
+#include <thread>
+#include <vector>
+
 #include "../../include/asohf_gpu.h"
 
 #define ASOHF_CUDA(call)                                                   \
@@ -82,6 +86,30 @@ struct asohf_ctx {
   int32_t* d_pph = nullptr;
   // sorted member segments of the subhaloes whose Jacobi radius is fixed,
   // in the order they were fixed (SUBSTRUCTURE_PARTICLES)
+  // staging store of asohf_prefetch_particles: copied on copy_stream while
+  // the context stream runs; taken by the matching asohf_upload_particles
+  DevParticles stage;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t stage_ready = nullptr, stage_free = nullptr, chunk_done = nullptr;
+  bool staged = false, stage_free_set = false;
+  std::thread stager;       // issues the staged copy chunk by chunk
+  int stage_status = 0;     // its status (read after join)
+  // device -> host copies of asohf_copy_to_host_async, issued chunk by chunk
+  // on out_stream by a helper thread
+  struct OutJob {
+    void* dst;
+    const void* src;
+    int64_t bytes;
+  };
+  cudaStream_t out_stream = nullptr;
+  cudaEvent_t out_fork = nullptr, out_chunk = nullptr, out_done = nullptr;
+  std::thread outer;
+  std::mutex out_mu;
+  std::vector<OutJob> out_jobs;
+  bool out_running = false, out_any = false;
+  int out_status = 0;
+  const void* staged_src[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int64_t staged_n = 0;
   unsigned long long* sfin_k = nullptr;
   int32_t* sfin_v = nullptr;
   int64_t sfin_cap = 0;

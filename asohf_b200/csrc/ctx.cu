@@ -33,6 +33,9 @@ extern "C" const char* asohf_strerror(int code) {
   }
 }
 
+static int stage_join(asohf_ctx* c);
+static int out_join(asohf_ctx* c);
+
 static void free_particles(DevParticles& p) {
   cudaFree(p.x); cudaFree(p.y); cudaFree(p.z);
   cudaFree(p.vx); cudaFree(p.vy); cudaFree(p.vz);
@@ -51,7 +54,8 @@ static int alloc_particles(DevParticles& p, int64_t cap) {
 }
 
 int ctx_ensure_particles(asohf_ctx* c, int64_t n) {
-  if (c->p.cap < n) {
+  // both sets: a prefetch can hand the store arrays of another capacity
+  if (c->p.cap < n || c->alt.cap < n) {
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
     free_particles(c->p);
     free_particles(c->alt);
@@ -242,8 +246,25 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   }
   cudaFree(c->dpool[0].base);
   cudaFree(c->dpool[1].base);
+  stage_join(c);
+  out_join(c);
+  if (c->out_stream) {
+    cudaStreamSynchronize(c->out_stream);
+    cudaStreamDestroy(c->out_stream);
+    cudaEventDestroy(c->out_fork);
+    cudaEventDestroy(c->out_chunk);
+    cudaEventDestroy(c->out_done);
+  }
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+    cudaEventDestroy(c->stage_ready);
+    cudaEventDestroy(c->stage_free);
+    cudaEventDestroy(c->chunk_done);
+  }
   free_particles(c->p);
   free_particles(c->alt);
+  free_particles(c->stage);
   cudaFree(c->rows[0]);
   cudaFree(c->rows[1]);
   cudaFree(c->d_s2);
@@ -406,10 +427,110 @@ extern "C" int asohf_kernel_stats(asohf_ctx* c, int i, const char** name, double
   return ASOHF_OK;
 }
 
+static void host_fields(const asohf_particles* s, const void* f[8]) {
+  f[0] = s->x; f[1] = s->y; f[2] = s->z; f[3] = s->vx; f[4] = s->vy; f[5] = s->vz; f[6] = s->m; f[7] = s->id;
+}
+
+// Copy of a prefetch, on the context's copy stream, in chunks of
+// STAGE_CHUNK bytes issued one at a time: the copy engine serves copies in
+// the order they were queued, so a 4 GB copy queued at once would hold every
+// short copy the context stream issues meanwhile (mesh, catalogue windows)
+// until it ends; chunk by chunk, such a copy waits for one chunk at most.
+#define STAGE_CHUNK (32ll << 20)
+
+static int stage_copy(asohf_ctx* c, const void* const src[8], int64_t n) {
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  void* dst[8] = {c->stage.x, c->stage.y, c->stage.z, c->stage.vx, c->stage.vy, c->stage.vz, c->stage.m,
+                  c->stage.id};
+  const int64_t bytes = 4 * n;  // every field is 4 bytes an entry
+  for (int64_t o = 0; o < bytes; o += STAGE_CHUNK) {
+    const int64_t b = bytes - o < STAGE_CHUNK ? bytes - o : STAGE_CHUNK;
+    for (int q = 0; q < 8; q++)
+      ASOHF_CUDA(cudaMemcpyAsync((char*)dst[q] + o, (const char*)src[q] + o, (size_t)b, cudaMemcpyHostToDevice,
+                                 c->copy_stream));
+    ASOHF_CUDA(cudaEventRecord(c->chunk_done, c->copy_stream));
+    ASOHF_CUDA(cudaEventSynchronize(c->chunk_done));
+  }
+  ASOHF_CUDA(cudaEventRecord(c->stage_ready, c->copy_stream));
+  return ASOHF_OK;
+}
+
+// Waits until the stager has issued every chunk of the staged copy.
+static int stage_join(asohf_ctx* c) {
+  if (c->stager.joinable()) c->stager.join();
+  int st = c->stage_status;
+  c->stage_status = ASOHF_OK;
+  return st;
+}
+
+extern "C" int asohf_prefetch_particles(asohf_ctx* c, const asohf_particles* s) {
+  if (!c || !s || s->n < 0) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  ASOHF_CHECK(stage_join(c));  // an earlier prefetch not taken: its chunks are all issued
+  c->staged = false;
+  if (!c->copy_stream) {
+    ASOHF_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->stage_ready, cudaEventDisableTiming));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->chunk_done, cudaEventDisableTiming | cudaEventBlockingSync));
+  }
+  if (c->stage.cap < s->n) {  // a larger staging store: nothing may still copy into the old one
+    ASOHF_CUDA(cudaStreamSynchronize(c->copy_stream));
+    if (c->stage_free_set) ASOHF_CUDA(cudaEventSynchronize(c->stage_free));
+    free_particles(c->stage);
+    ASOHF_CHECK(alloc_particles(c->stage, s->n));
+    c->stage_free_set = false;
+  }
+  c->stage.n = s->n;
+  // the staging arrays were the store of an earlier call: copy into them once
+  // the work issued before they were handed over is done
+  if (c->stage_free_set) ASOHF_CUDA(cudaStreamWaitEvent(c->copy_stream, c->stage_free, 0));
+  host_fields(s, c->staged_src);
+  c->staged_n = s->n;
+  c->staged = true;
+  const void* src[8];
+  for (int q = 0; q < 8; q++) src[q] = c->staged_src[q];
+  const int64_t n = s->n;
+  try {
+    c->stager = std::thread([c, src, n]() { c->stage_status = stage_copy(c, src, n); });
+  } catch (...) {  // no thread: the copy is issued from here, at once
+    c->stage_status = stage_copy(c, src, n);
+  }
+  return ASOHF_OK;
+}
+
+// A prefetch of exactly these host arrays: the context stream waits for its
+// copy and the staging store becomes the particle store; the store it
+// replaces becomes the staging store of the next prefetch.
+static bool take_staged(asohf_ctx* c, const asohf_particles* s) {
+  if (!c->staged || c->staged_n != s->n) return false;
+  const void* f[8];
+  host_fields(s, f);
+  for (int q = 0; q < 8; q++)
+    if (f[q] != c->staged_src[q]) return false;
+  return true;
+}
+
 extern "C" int asohf_upload_particles(asohf_ctx* c, const asohf_particles* s, int on_device) {
   if (!c || !s || s->n < 0) return ASOHF_ERR_INVALID;
   ASOHF_CUDA(cudaSetDevice(c->device));
   arena_reset(c);
+  if (!on_device && take_staged(c, s)) {
+    c->staged = false;
+    ASOHF_CHECK(stage_join(c));
+    ASOHF_CHECK(ctx_ensure_particles(c, s->n));
+    ASOHF_CUDA(cudaStreamWaitEvent(c->stream, c->stage_ready, 0));
+    DevParticles t = c->p;
+    c->p = c->stage;
+    c->stage = t;
+    c->p.n = s->n;
+    ASOHF_CUDA(cudaEventRecord(c->stage_free, c->stream));
+    c->stage_free_set = true;
+    c->nx_sorted = 0;
+    c->rows_cur = -1;
+    if (s->n > 0) ASOHF_CHECK(ctx_refresh_mass_range(c));
+    return ASOHF_OK;
+  }
   ASOHF_CHECK(ctx_ensure_particles(c, s->n));
   cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   size_t fb = sizeof(float) * (size_t)s->n;
@@ -453,6 +574,91 @@ extern "C" int asohf_work_counters(asohf_ctx* c, int64_t* out, int reset) {
 }
 
 // ------------------------------------------------------------ host copies
+// Device -> page-locked host copies on a copy engine, issued in chunks of
+// STAGE_CHUNK bytes one at a time by a helper thread (the copy engine serves
+// copies in the order they were queued: chunk by chunk, a short copy of the
+// context stream waits for one chunk at most).
+static void out_worker(asohf_ctx* c) {
+  int st = ASOHF_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) st = ASOHF_ERR_CUDA;
+  for (;;) {
+    asohf_ctx::OutJob j;
+    {
+      std::lock_guard<std::mutex> lock(c->out_mu);
+      if (c->out_jobs.empty()) {
+        c->out_running = false;
+        if (st != ASOHF_OK) c->out_status = st;
+        return;
+      }
+      j = c->out_jobs.front();
+      c->out_jobs.erase(c->out_jobs.begin());
+    }
+    for (int64_t o = 0; st == ASOHF_OK && o < j.bytes; o += STAGE_CHUNK) {
+      const int64_t b = j.bytes - o < STAGE_CHUNK ? j.bytes - o : STAGE_CHUNK;
+      if (cudaMemcpyAsync((char*)j.dst + o, (const char*)j.src + o, (size_t)b, cudaMemcpyDeviceToHost,
+                          c->out_stream) != cudaSuccess ||
+          cudaEventRecord(c->out_chunk, c->out_stream) != cudaSuccess ||
+          cudaEventSynchronize(c->out_chunk) != cudaSuccess)
+        st = ASOHF_ERR_CUDA;
+    }
+    if (st == ASOHF_OK && cudaEventRecord(c->out_done, c->out_stream) != cudaSuccess) st = ASOHF_ERR_CUDA;
+  }
+}
+
+static int out_join(asohf_ctx* c) {
+  if (c->outer.joinable()) c->outer.join();
+  int st = c->out_status;
+  c->out_status = ASOHF_OK;
+  return st;
+}
+
+extern "C" int asohf_copy_to_host_async(asohf_ctx* c, void* host_dst, const void* dev_src, int64_t bytes) {
+  if (!c || bytes < 0 || (bytes && (!host_dst || !dev_src))) return ASOHF_ERR_INVALID;
+  if (bytes == 0) return ASOHF_OK;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  cudaPointerAttributes ha, da;
+  ASOHF_CUDA(cudaPointerGetAttributes(&ha, host_dst));
+  ASOHF_CUDA(cudaPointerGetAttributes(&da, dev_src));
+  if (ha.type != cudaMemoryTypeHost || da.type != cudaMemoryTypeDevice || da.device != c->device)
+    return ASOHF_ERR_INVALID;  // page-locked host memory and this context's device memory only
+  if (!c->out_stream) {
+    ASOHF_CUDA(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->out_fork, cudaEventDisableTiming));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->out_chunk, cudaEventDisableTiming | cudaEventBlockingSync));
+    ASOHF_CUDA(cudaEventCreateWithFlags(&c->out_done, cudaEventDisableTiming));
+  }
+  // after the work issued so far: the context stream's and a deferred patch
+  // deposit's
+  ASOHF_CUDA(cudaEventRecord(c->out_fork, c->stream));
+  ASOHF_CUDA(cudaStreamWaitEvent(c->out_stream, c->out_fork, 0));
+  if (c->dens_pending) ASOHF_CUDA(cudaStreamWaitEvent(c->out_stream, c->dens_done, 0));
+  std::lock_guard<std::mutex> lock(c->out_mu);
+  c->out_jobs.push_back({host_dst, dev_src, bytes});
+  c->out_any = true;
+  if (!c->out_running) {
+    if (c->outer.joinable()) c->outer.join();
+    c->out_running = true;
+    try {
+      c->outer = std::thread(out_worker, c);
+    } catch (...) {
+      c->out_running = false;
+      c->out_jobs.pop_back();
+      return ASOHF_ERR_CAPACITY;
+    }
+  }
+  return ASOHF_OK;
+}
+
+extern "C" int asohf_copy_wait(asohf_ctx* c, void* cuda_stream) {
+  if (!c) return ASOHF_ERR_INVALID;
+  ASOHF_CUDA(cudaSetDevice(c->device));
+  ASOHF_CHECK(out_join(c));
+  if (!c->out_any) return ASOHF_OK;
+  if (cuda_stream) ASOHF_CUDA(cudaStreamWaitEvent((cudaStream_t)cuda_stream, c->out_done, 0));
+  else ASOHF_CUDA(cudaEventSynchronize(c->out_done));
+  return ASOHF_OK;
+}
+
 // Device -> page-locked host copy made by SM stores through the host
 // buffer's device mapping instead of a copy engine: a large copy issued this
 // way on a stream of its own does not queue ahead of the short copies the

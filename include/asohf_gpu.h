@@ -63,15 +63,24 @@ int asohf_work_counters(asohf_ctx *ctx, int64_t *out8, int reset);
  * hold `bytes` bytes; the copy is complete when the stream reaches it. */
 int asohf_copy_to_host_sm(asohf_ctx *ctx, void *host_dst, const void *dev_src, int64_t bytes,
                           void *cuda_stream);
+/* Host I/O, no counterpart in the reference: copies `bytes` bytes from
+ * device memory of this context's GPU to page-locked host memory on a copy
+ * engine, after the work the context has issued so far (a deferred patch
+ * deposit included), and returns at once.  A helper thread issues the copy
+ * in chunks, one at a time: the copy engine serves copies in the order they
+ * were queued, so the short copies the context makes meanwhile wait for one
+ * chunk at most.  asohf_copy_wait makes cuda_stream (the host, when NULL)
+ * wait for every such copy issued so far. */
+int asohf_copy_to_host_async(asohf_ctx *ctx, void *host_dst, const void *dev_src, int64_t bytes);
+int asohf_copy_wait(asohf_ctx *ctx, void *cuda_stream);
 /* Tuning, no counterpart in the reference: with on = 1, asohf_density
  * called with device outputs returns before its AMR-patch deposit is done:
  * that work runs on a stream of the context's own (at the least priority),
  * from buffers no other call reuses, beside whatever the caller issues next
  * (the x-slab sort and the halo finder do not read U11), and
- * asohf_renorm_density's patch scaling
- * follows it there.  U11 is complete once asohf_density_wait has made a
- * stream wait for it, or after asohf_synchronize.  U1 is complete on return
- * as before. */
+ * asohf_renorm_density's patch scaling follows it there.  U11 is complete
+ * once asohf_density_wait has made a stream wait for it, or after
+ * asohf_synchronize.  U1 is complete on return as before. */
 int asohf_set_density_overlap(asohf_ctx *ctx, int on);
 /* Makes cuda_stream wait (device side) for a deferred patch deposit. */
 int asohf_density_wait(asohf_ctx *ctx, void *cuda_stream);
@@ -107,6 +116,14 @@ int asohf_set_group_tiers(asohf_ctx *ctx, int64_t tier1_members, int64_t tier2_m
  * permutes RXPA.., ORIPA). */
 int asohf_upload_particles(asohf_ctx *ctx, const asohf_particles *src, int on_device);
 int asohf_download_particles(asohf_ctx *ctx, asohf_particles *dst, int on_device);
+/* Tuning, no counterpart in the reference: starts copying the host arrays
+ * of a coming asohf_upload_particles (page-locked, for the copy to overlap)
+ * on a copy stream of the context's own into a staging store, while the
+ * context stream runs what was issued before.  The next upload of exactly
+ * these arrays (same pointers and count, on_device = 0) takes the staged
+ * store: the context stream waits for the copy instead of copying again.
+ * The arrays must not change until that upload. */
+int asohf_prefetch_particles(asohf_ctx *ctx, const asohf_particles *src);
 
 /* SORT_DM_PARTICLES_LOCALDENSITY (reader.f:140-336): NGP density on the
  * NX^3 grid, species INT(LOG(rho)/LOG(8)) in [0, N_ESP-1], stable sort of
