@@ -340,6 +340,7 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     clocks = clock_summary(clk, clk_path)
     launches = (b.a.launch_count() - l0) // args.steps
+    free_b, total_b = torch.cuda.mem_get_info(local)  # the library keeps its stores and arenas
     kstats = b.a.kernel_stats()
     work = b.a.work_counters()
     b.a.set_profiling(False)
@@ -419,6 +420,7 @@ def main():
                    "global_batch": world * n, "parallelism": f"replicas x{world}",
                    "l2": "inputs > L2 (4.3 GB of particles per step)"},
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches),
+        "device_memory_in_use_gb": round((total_b - free_b) / 1e9, 2),
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in
                                 sorted(kstats.items(), key=lambda kv: -kv[1][0])
                                 if not k.startswith(("host:", "idle:"))},
