@@ -475,17 +475,31 @@ class GpuBackend:
         return self.a.sort_dm_particles_localdensity(nx, dx, rodo, re0)
 
     def catalogue(self, capacity):
-        """A zeroed page-locked catalogue from a ring of two owned by the
+        """A zeroed page-locked catalogue from a ring of three owned by the
         backend: the one returned by a run stays valid through the next run
         (page-locking fresh memory every run would cost more than the run's
-        catalogue copies)."""
+        catalogue copies).  The one after it is zeroed by a helper thread
+        while this run goes on: it was returned two runs ago, so its
+        validity has ended (numpy's fill releases the GIL)."""
+        import threading
         ring = getattr(self, "_cat_ring", None)
         if ring is None or ring[0].capacity != capacity:
-            ring = self._cat_ring = [abi.Catalogue(capacity, pinned=True), abi.Catalogue(capacity, pinned=True)]
+            self._cat_join()
+            ring = self._cat_ring = [abi.Catalogue(capacity, pinned=True) for _ in range(3)]
             self._cat_next = 0
+        self._cat_join()  # this run's catalogue was being zeroed
         c = ring[self._cat_next]
-        self._cat_next ^= 1
-        return c.reset()
+        self._cat_next = (self._cat_next + 1) % 3
+        c.reset()  # a no-op when the helper zeroed it
+        self._cat_thread = threading.Thread(target=ring[self._cat_next].reset, daemon=True)
+        self._cat_thread.start()
+        return c
+
+    def _cat_join(self):
+        t = getattr(self, "_cat_thread", None)
+        if t is not None:
+            t.join()
+            self._cat_thread = None
 
     def density(self, nx, lado0, dx, rote, rete, npart_esp, mesh, interp_degree=2, fp64=True):
         u1 = np.zeros(nx ** 3, np.float32)

@@ -1189,7 +1189,11 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
         nitems += ns;
         ord[u] = u;
       }
-      std::sort(ord, ord + nunits, [&](int a2, int b2) { return hc[a2] > hc[b2] || (hc[a2] == hc[b2] && a2 < b2); });
+      {  // counts descending, ties by unit index (stable radix sort of the counts)
+        std::vector<uint32_t> key((size_t)nunits);
+        for (int u = 0; u < nunits; u++) key[u] = (uint32_t)(hc[u] < 0xffffffffll ? hc[u] : 0xffffffffll);
+        stable_desc(key, ord, nunits);
+      }
       std::vector<int2> hitems_v((size_t)nitems);
       std::vector<int32_t> hmulti_v((size_t)(nmulti > 0 ? nmulti : 1));
       int2* hitems = hitems_v.data();

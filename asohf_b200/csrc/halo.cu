@@ -1971,31 +1971,6 @@ int assign_id_offsets(asohf_ctx* c, CatMirror& m, int low1, int low2, const int3
   return ASOHF_OK;
 }
 
-// Stable descending order of w[0..k) by key[] (an unsigned image of the
-// value that preserves its order): LSD radix sort on the complemented key,
-// 8 bits a pass, passes whose digit is the same for every entry skipped.
-// Equal values keep their order, as in a stable comparison sort.
-static void stable_desc(std::vector<uint32_t>& key, int32_t* w, int k) {
-  std::vector<uint32_t> key2((size_t)k);
-  std::vector<int32_t> tmp((size_t)k);
-  for (int i = 0; i < k; i++) key[i] = ~key[i];
-  for (int sh = 0; sh < 32; sh += 8) {
-    int64_t cnt[257] = {0};
-    for (int i = 0; i < k; i++) cnt[((key[i] >> sh) & 255u) + 1]++;
-    bool one = false;
-    for (int d = 0; d < 256; d++) one |= cnt[d + 1] == k;
-    if (one) continue;
-    for (int d = 0; d < 256; d++) cnt[d + 1] += cnt[d];
-    for (int i = 0; i < k; i++) {
-      const int64_t o = cnt[(key[i] >> sh) & 255u]++;
-      tmp[o] = w[i];
-      key2[o] = key[i];
-    }
-    memcpy(w, tmp.data(), 4 * (size_t)k);
-    key.swap(key2);
-  }
-}
-
 // Work list: haloes of [low1, low2] with REALCLUS != 0, DMPCLUS descending
 // (largest first keeps the longest CTAs from finishing last).
 int make_work(asohf_ctx* c, CatMirror& m, int low1, int low2, std::vector<int32_t>& h_work, int* nslots,

@@ -62,13 +62,18 @@ def re_sort_haloes(cat: abi.Catalogue, nhallev: np.ndarray, ir: int):
     sl = slice(low1 - 1, low2)
     rc = cat.realclus[sl].copy()
     keep = rc != 0
-    k = int(keep.sum())
+    idx = np.flatnonzero(keep)
+    k = int(idx.shape[0])
+    if k == low2 - low1 + 1:  # nothing dropped: order and numbering stay
+        nhallev[ir] = k
+        cat.nclus = low1 - 1 + k
+        return keep
     resort = np.zeros(low2 - low1 + 1, np.int64)
-    resort[keep] = np.arange(low1, low1 + k)
+    resort[idx] = np.arange(low1, low1 + k)
     for f in CAT_MOVE:
         a = getattr(cat, f)
-        a[low1 - 1: low1 - 1 + k] = a[sl][keep]
-    new = rc[keep]
+        a[low1 - 1: low1 - 1 + k] = np.take(a[sl], idx)
+    new = rc[idx]
     pos = new > 0
     inside = pos & (new >= low1) & (new <= low2)
     new[inside] = resort[new[inside] - low1]
