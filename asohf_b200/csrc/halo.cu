@@ -696,6 +696,7 @@ struct SegG {
   int32_t* nscan;           // entries the property loop scanned (NCAPAS)
   unsigned long long* work; // element-pass counter; with timing, [4..7] halo times
   int32_t* status;
+  float* eig;               // 9 per slot: inertia tensor for k_eigen (NaN: none)
   int timing;               // record per-halo durations (profiling)
 };
 
@@ -1428,7 +1429,7 @@ template <int C, bool SYM = true>
 __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst& H, asohf_catalogue& cat, int i0,
                                   const SegView& v, uint8_t* flag, int64_t konta, float rshell, float cx, float cy,
                                   float cz, const float* cmv, GShared& sh, int* unsupported, const SegView& spare,
-                                  double* pot) {
+                                  double* pot, float* eig_in) {
   float norma = S.norma;
   float vc[3] = {cat.vx[i0], cat.vy[i0], cat.vz[i0]};
   int64_t each_prof = konta / ASOHF_NBINS;
@@ -1545,14 +1546,30 @@ __device__ long long properties_g(const Grp<C>& g, const Store& S, const HConst&
       it[0] = in[0]; it[1] = in[3]; it[2] = in[6]; it[3] = in[4]; it[4] = in[7]; it[5] = in[8];
       cat.velocity_dispersion[i0] = (float)(sqrt(r[0] / (double)(float)cnt) * (double)H.uv);
       cat.vmaxclus[i0] = __fmul_rn(__fsqrt_rn(vmax), H.uv);
-      float be[3] = {0.0f, 0.0f, 0.0f};
-      diagonalise_dev(in, be);
-      sort_eigen_dev(be);
-      for (int q = 0; q < 3; q++) cat.eigenval[(size_t)i0 * 3 + q] = __fsqrt_rn(__fmul_rn(5.0f, be[q]));
+      // the eigenvalues (DIAGONALISE, a serial FP64 Jacobi loop) come from
+      // k_eigen, one thread per halo, instead of this group's lead thread
+      for (int q = 0; q < 9; q++) eig_in[q] = in[q];
     }
   }
   g.sync();
   return cnt;
+}
+
+// Eigenvalues of the inertia tensors the per-halo kernels left in eig_in
+// (9 entries per slot, NaN in the first: none): DIAGONALISE (num.f:2-116),
+// the descending sort and SQRT(5*eig), one thread per slot.
+__global__ void k_eigen(const float* __restrict__ eig_in, const int32_t* __restrict__ work, int ns,
+                        float* __restrict__ eigenval) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  float in[9];
+  for (int q = 0; q < 9; q++) in[q] = eig_in[(size_t)s * 9 + q];
+  if (in[0] != in[0]) return;
+  float be[3] = {0.0f, 0.0f, 0.0f};
+  diagonalise_dev(in, be);
+  sort_eigen_dev(be);
+  const int i0 = work[s];
+  for (int q = 0; q < 3; q++) eigenval[(size_t)i0 * 3 + q] = __fsqrt_rn(__fmul_rn(5.0f, be[q]));
 }
 
 template <int C>
@@ -1841,7 +1858,8 @@ k_halo_main(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalogu
     return;
   }
   int unsup = 0;
-  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup, nxt, pot);
+  long long nb = properties_g(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup, nxt, pot,
+                              sg.eig + (size_t)slot * 9);
   ep += (unsigned long long)(k2 + ncapas);  // SO walk and property loop
   if (lead) {
     atomicAdd(&sg.work[0], ep);
@@ -2129,7 +2147,7 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
   double ht = htime_now();
   arena_reset(c);
   int nh = lowh2 - lowh1 + 1;
-  size_t need = cat_bytes(lowh2) + (size_t)nh * 96 + 65536;
+  size_t need = cat_bytes(lowh2) + (size_t)nh * (96 + 40) + 65536;
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
   ASOHF_CHECK(cat_mirror_in(c, cat, lowh2, on_device, &m, lowh1 - 1));
@@ -2250,10 +2268,12 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
     sg.work = c->d_work;
     sg.status = g.status;
     sg.timing = c->profiling;
+    sg.eig = (float*)arena_alloc(c, 36 * (size_t)ns);
     if (!k0 || !k1 || !v0 || !v1 || !t || !sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px ||
-        !sg.pot || !sg.flag) {
+        !sg.pot || !sg.flag || !sg.eig) {
       return ASOHF_ERR_CAPACITY;
     }
+    ASOHF_CUDA(cudaMemsetAsync(sg.eig, 0xff, 36 * (size_t)ns, c->stream));  // NaN: no tensor
     if (T > 0) {
       ASOHF_CUDA(cudaMemsetAsync(d_fill, 0, 4 * (size_t)ns, c->stream));
       {
@@ -2314,6 +2334,8 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       ASOHF_CHECK(join_all(c));
       ktime_end(c, kt_);
     }
+    k_eigen<<<(ns + 127) / 128, 128, 0, c->stream>>>(sg.eig, d_work, ns, m.d.eigenval);
+    c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
     ASOHF_CUDA(cudaStreamSynchronize(c->stream));
@@ -2858,7 +2880,7 @@ k_sub_main_g(const int32_t* __restrict__ slots, Store S, HConst H, asohf_catalog
   g.sync();
   int unsup = 0;
   long long nb = properties_g<C, false>(g, S, H, cat, i0, cur, flag, ncapas, rshell, cx, cy, cz, cm0, sh, &unsup,
-                                        nxt, pot);
+                                        nxt, pot, sg.eig + (size_t)slot * 9);
   ep += (unsigned long long)(k2 + ncapas);
   if (lead) {
     atomicAdd(&sg.work[1], ep);
@@ -3041,7 +3063,7 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
   double ht = htime_now();
   arena_reset(c);
   int nh = lowh2 - lowh1 + 1;
-  size_t need = cat_bytes(cat->nclus) + (size_t)nh * 192 + 65536;
+  size_t need = cat_bytes(cat->nclus) + (size_t)nh * (192 + 40) + 65536;
   ASOHF_CHECK(arena_reserve(c, need));
   CatMirror m;
   ASOHF_CHECK(cat_mirror_in(c, cat, cat->nclus, on_device, &m, lowh1 - 1, true));
@@ -3213,11 +3235,13 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       sg.work = c->d_work;
       sg.status = pr.status;
       sg.timing = 0;
+      sg.eig = (float*)arena_alloc(c, 36 * (size_t)ns);
       int32_t* d_ts = (int32_t*)arena_alloc(c, 4 * (size_t)ns);
       if (!sg.a.dm || !sg.a.mv || !sg.a.px || !sg.b.dm || !sg.b.mv || !sg.b.px || !sg.pot || !sg.flag ||
-          !sg.final_b || !d_ts) {
+          !sg.final_b || !d_ts || !sg.eig) {
         return ASOHF_ERR_CAPACITY;
       }
+      ASOHF_CUDA(cudaMemsetAsync(sg.eig, 0xff, 36 * (size_t)ns, c->stream));  // NaN: no tensor
       SubMainIn in;
       in.konta = d_konta; in.jjac = f_jjac; in.masadm = f_masadm; in.rclus = f_rclus;
       in.cx = pr.cx; in.cy = pr.cy; in.cz = pr.cz; in.mhost = pr.mhost; in.disthost = pr.disthost;
@@ -3230,6 +3254,8 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
         LAUNCH_TIERS_CTA(k_sub_main_g, ts, S, H, m.d, d_work, in, sg);
         ktime_end(c, kt_);
       }
+      k_eigen<<<(ns + 127) / 128, 128, 0, c->stream>>>(sg.eig, d_work, ns, m.d.eigenval);
+      c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       ASOHF_CUDA(cudaMemcpyAsync(h_st, pr.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
       ASOHF_CUDA(cudaStreamSynchronize(c->stream));
