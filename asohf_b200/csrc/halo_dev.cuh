@@ -58,28 +58,104 @@ struct GX {
   double dres[16];      // group totals
   long long l[8];
   long long lres[8];
+  long long lw[8][HW];  // per-warp minima (gmin_llv)
   float f[2];
   float fres[2];
 };
+
+// Warp reduce-scatter of K doubles (K <= 16, padded to a power of two KP):
+// the pairings of the xor butterfly (distances 16, 8, 4, 2, 1), so every
+// total is the butterfly's bit for bit, but while a lane holds several
+// partial sums each level exchanges half of them (the lane keeps the upper
+// half when its bit of that distance is set).  Returns the total of the value
+// that lane holds; scatter_lane<K>(q) is a lane that holds value q.
+template <int K>
+struct Scatter {
+  static constexpr int KP = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : 16;
+  static constexpr int LOG = K <= 1 ? 0 : K <= 2 ? 1 : K <= 4 ? 2 : K <= 8 ? 3 : 4;
+};
+
+template <int K>
+__device__ __forceinline__ double warp_sum_scatter(const double* v) {
+  constexpr int KP = Scatter<K>::KP;
+  double w[KP];
+#pragma unroll
+  for (int q = 0; q < KP; q++) w[q] = q < K ? v[q] : 0.0;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int lv = 0; lv < 5; lv++) {
+    const int o = 16 >> lv;
+    const int n = KP >> lv;  // partial sums a lane holds before this level
+    if (n > 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int i = 0; i < n / 2; i++) {
+        const double send = up ? w[i] : w[i + n / 2];
+        const double keep = up ? w[i + n / 2] : w[i];
+        w[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    } else {
+      w[0] += __shfl_xor_sync(0xffffffffu, w[0], o);
+    }
+  }
+  return w[0];
+}
+
+// The same reduce-scatter for the minimum of K long longs (exact in any
+// order).
+template <int K>
+__device__ __forceinline__ long long warp_min_scatter(const long long* v) {
+  constexpr int KP = Scatter<K>::KP;
+  long long w[KP];
+#pragma unroll
+  for (int q = 0; q < KP; q++) w[q] = q < K ? v[q] : LLONG_MAX;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int lv = 0; lv < 5; lv++) {
+    const int o = 16 >> lv;
+    const int n = KP >> lv;
+    if (n > 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int i = 0; i < n / 2; i++) {
+        const long long send = up ? w[i] : w[i + n / 2];
+        const long long keep = up ? w[i + n / 2] : w[i];
+        const long long r = __shfl_xor_sync(0xffffffffu, send, o);
+        w[i] = r < keep ? r : keep;
+      }
+    } else {
+      const long long r = __shfl_xor_sync(0xffffffffu, w[0], o);
+      w[0] = r < w[0] ? r : w[0];
+    }
+  }
+  return w[0];
+}
+
+template <int K>
+__device__ __forceinline__ int scatter_lane(int q) {
+  constexpr int LOG = Scatter<K>::LOG;
+  int l = 0;
+#pragma unroll
+  for (int lv = 0; lv < LOG; lv++) l |= ((q >> (LOG - 1 - lv)) & 1) << (4 - lv);
+  return l;
+}
 
 // Sum of K doubles over the CTA; every thread receives the totals.
 template <int K>
 __device__ __forceinline__ void block_sum_dv(double* v, GX& x) {
   static_assert(K <= 16, "at most 16 sums");
-  if (blockDim.x == 32) {  // one warp: butterflies, no shared memory
+  const int lane = threadIdx.x & 31;
+  const double mine = warp_sum_scatter<K>(v);
+  if (blockDim.x == 32) {  // one warp: no shared memory
 #pragma unroll
-    for (int q = 0; q < K; q++)
-      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    for (int q = 0; q < K; q++) v[q] = __shfl_sync(0xffffffffu, mine, scatter_lane<K>(q));
     return;
   }
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-  for (int q = 0; q < K; q++) v[q] = warp_sum_d(v[q]);
+  int wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   __syncthreads();
-  if (lane == 0) {
 #pragma unroll
-    for (int q = 0; q < K; q++) x.vred[q][wid] = v[q];
-  }
+  for (int q = 0; q < K; q++)
+    if (lane == scatter_lane<K>(q)) x.vred[q][wid] = mine;
   __syncthreads();
   for (int q = wid; q < K; q += nw) {
     double t = lane < nw ? x.vred[q][lane] : 0.0;
@@ -142,10 +218,28 @@ __device__ __forceinline__ long long gsum_ll(const Grp<C>& g, long long v, long 
 
 // Minimum of K indices over the group (K <= 8).
 template <int K, int C>
-__device__ __forceinline__ void gmin_llv(const Grp<C>& g, long long* v, long long* lred, GX& x) {
+__device__ __forceinline__ void gmin_llv(const Grp<C>& g, long long* v, long long* /*lred*/, GX& x) {
   static_assert(K <= 8, "at most 8 minima");
+  const int lane = threadIdx.x & 31;
+  const long long mine = warp_min_scatter<K>(v);
+  if (blockDim.x == 32) {
 #pragma unroll
-  for (int q = 0; q < K; q++) v[q] = block_min_ll(v[q], lred);
+    for (int q = 0; q < K; q++) v[q] = __shfl_sync(0xffffffffu, mine, scatter_lane<K>(q));
+  } else {
+    const int wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; q++)
+      if (lane == scatter_lane<K>(q)) x.lw[q][wid] = mine;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      long long t = LLONG_MAX;
+      for (int w = 0; w < nw; w++) t = x.lw[q][w] < t ? x.lw[q][w] : t;
+      v[q] = t;
+    }
+    __syncthreads();
+  }
   if constexpr (C > 1) {
     if (threadIdx.x == 0) {
 #pragma unroll
