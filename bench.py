@@ -45,10 +45,10 @@ CPU_TREND = "cfg4m"   # the second point of the CPU scaling trend
 # particle's position 12, velocity 12, mass 4 and ID 8 read, its distance and
 # flag 8 written
 BYTES_PER_ELEMENT_PASS = 44
-# DRAM bytes (read + write) per element-pass of k_halo_main: 3.53 GB over
-# 136.4M element-passes in one ncu capture of the 256^3 workload's launches
-# (`--config cfg2 --steps 1 --warmup 0 --no-cpu --no-layer --no-e2e`)
-DRAM_BYTES_PER_ELEMENT_PASS = 25.9
+# DRAM bytes (read + write) per element-pass of k_halo_main: 3.60 GB over
+# 136.4M element-passes in one ncu capture of the 256^3 workload's 14 launches
+# (`--config cfg2 --steps 1 --warmup 0 --no-cpu --no-layer --no-e2e --no-grid`)
+DRAM_BYTES_PER_ELEMENT_PASS = 26.4
 
 
 def peaks():
