@@ -1,6 +1,6 @@
 """Particle input in the reference's formats: the generic file
-(readers/particle_general.f) and GADGET format-2 snapshots
-(readers/gadget_unformatted.f).
+(readers/particle_general.f), GADGET format-2 snapshots
+(readers/gadget_unformatted.f) and MASCLET outputs (readers/masclet.f).
 
 The generic file (readers/particle_general.f) is a
 Fortran unformatted sequential file `simulation/particlesNNNNN` holding
@@ -199,3 +199,200 @@ def read_gadget_unformatted(path: str, var: int = 1, cio_mass: float = 1.0, cio_
     out.m = (raw.m * fact_mass).astype(np.float32)
     out.n = out.x.shape[0]
     return out
+
+
+# ---------------------------------------------------------------- MASCLET
+# READ_PARTICLES_MASCLET (readers/masclet.f:241-525): a MASCLET output
+# `simu_masclet/{grids,cldm,clst}NNNNN`.  `grids` is list-directed text:
+# "IRR T NL MAP", "ZETA", "IR NDXYZ NST0", then per level IR = 1..NL the
+# line "IRR NPATCH NPART NPARTST NPARTBH", one line the reader skips and four
+# lines per patch it skips.  `cldm` is unformatted: a header record, the base
+# density record, then X, Y, Z, VX, VY, VZ (REAL*4) and the IDs (INTEGER*4) of
+# the NDXYZ base-level particles, whose mass is MAP; then per level one
+# record per patch (its density, skipped) and X..VZ, the masses and the IDs
+# of the level's NPART particles.  No unit conversion: MASCLET's units are
+# the code's.  When the heaviest mass exceeds four times the lightest, the
+# particles above 0.9 of the heaviest get a negative ID.  With VAR = 2 the
+# stars come from `clst` (base level: NPARTST(0) + NPARTBH(0) particles,
+# X..mass, two skipped records, no IDs, so their ID stays 0; each level:
+# the patch records, X..mass of NPARTST(IR), two skipped records and IDs
+# that are offset by the largest dark-matter ID; the black holes' nine
+# records are skipped, as the reference does with CONSIDER_BH = 0).
+
+
+def _masclet_grids(path: str):
+    """The header and per-level counts of a MASCLET `grids` file, read with
+    list-directed semantics (values may span lines; a bare READ skips one
+    line)."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    pos = [0]
+
+    def values(n):
+        out = []
+        while len(out) < n:
+            if pos[0] >= len(lines):
+                raise ValueError(f"{path}: ends before {n} values")
+            toks = lines[pos[0]].replace(",", " ").replace("d", "e").replace("D", "E").split()
+            pos[0] += 1
+            out += toks
+        return out[:n]
+
+    def skip():
+        pos[0] += 1
+
+    irr, t, nl, mp = values(4)
+    (zeta,) = values(1)
+    _, ndxyz, nst0 = values(3)
+    nl = int(nl)
+    npatch, npart, npartst, npartbh = [0], [int(ndxyz)], [int(nst0)], [0]
+    for ir in range(1, nl + 1):
+        v = values(5)
+        npatch.append(int(v[1]))
+        npart.append(int(v[2]))
+        npartst.append(int(v[3]))
+        npartbh.append(int(v[4]))
+        skip()
+        for _ in range(4 * npatch[ir]):
+            skip()
+    return SimpleNamespace(t=float(np.float32(float(t))), nl=nl, map=np.float32(float(mp)),
+                           zeta=float(np.float32(float(zeta))), npatch=npatch, npart=npart,
+                           npartst=npartst, npartbh=npartbh)
+
+
+def _first(rec: bytes | None, dtype, n: int, what: str):
+    if rec is None:
+        raise ValueError(f"{what}: the file ends early")
+    a = np.frombuffer(rec, dtype)
+    if a.shape[0] < n:  # a longer record is read in part, as Fortran does
+        raise ValueError(f"{what}: {a.shape[0]} values for {n} particles")
+    return a[:n]
+
+
+def read_masclet(directory: str, it: int, var: int = 1) -> SimpleNamespace:
+    """READ_PARTICLES_MASCLET (readers/masclet.f:241-525) on the files of
+    output `it` in `directory` (the reference's ./simu_masclet): the
+    particles (dark matter level by level, then stars when var = 2) as
+    float32/int32 arrays, with t, zeta, n_dm and n_st."""
+    import os
+    tag = "%05d" % it
+    g = _masclet_grids(os.path.join(directory, "grids" + tag))
+    cols = {k: [] for k in FIELDS + ("id",)}
+    with open(os.path.join(directory, "cldm" + tag), "rb") as f:
+        read_record(f)  # header
+        read_record(f)  # base-level density
+        n0 = g.npart[0]
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            cols[k].append(_first(read_record(f), np.float32, n0, "cldm " + k))
+        cols["id"].append(_first(read_record(f), np.int32, n0, "cldm id"))
+        cols["m"].append(np.full(n0, g.map, np.float32))
+        for ir in range(1, g.nl + 1):
+            for _ in range(g.npatch[ir]):
+                read_record(f)  # patch density
+            n = g.npart[ir]
+            for k in FIELDS:
+                cols[k].append(_first(read_record(f), np.float32, n, f"cldm level {ir} {k}"))
+            cols["id"].append(_first(read_record(f), np.int32, n, f"cldm level {ir} id"))
+    dm = {k: np.concatenate(v) if v else np.zeros(0) for k, v in cols.items()}
+    dm["id"] = dm["id"].astype(np.int32)
+    n_dm = int(dm["x"].shape[0])
+    if n_dm:  # heavier species: negative IDs (masclet.f:389-400)
+        mx = np.float32(dm["m"].max())
+        if mx > np.float32(4.0) * np.float32(dm["m"].min()):
+            bas = np.float32(np.float32(0.9) * mx)
+            heavy = dm["m"] > bas
+            dm["id"][heavy] = -np.abs(dm["id"][heavy])
+    st = {k: [] for k in FIELDS + ("id",)}
+    if var == 2:
+        max_id = int(dm["id"].max()) if n_dm else 0
+        with open(os.path.join(directory, "clst" + tag), "rb") as f:
+            read_record(f)  # header
+            read_record(f)  # base-level stellar density
+            nb = g.npartst[0] + g.npartbh[0]
+            for k in FIELDS:
+                st[k].append(_first(read_record(f), np.float32, nb, "clst " + k))
+            read_record(f)
+            read_record(f)
+            st["id"].append(np.zeros(nb, np.int32))  # not read at the base level
+            for ir in range(1, g.nl + 1):
+                for _ in range(g.npatch[ir]):
+                    read_record(f)
+                nb = g.npartst[ir]
+                for k in FIELDS:
+                    st[k].append(_first(read_record(f), np.float32, nb, f"clst level {ir} {k}"))
+                read_record(f)
+                read_record(f)
+                ids = _first(read_record(f), np.int32, nb, f"clst level {ir} id")
+                st["id"].append((ids.astype(np.int64) + max_id).astype(np.int32))
+                for _ in range(9):  # black holes, not considered
+                    read_record(f)
+    stars = {k: np.concatenate(v) if v else np.zeros(0, np.int32 if k == "id" else np.float32)
+             for k, v in st.items()}
+    out = SimpleNamespace(t=g.t, zeta=g.zeta, n_dm=n_dm, n_st=int(stars["x"].shape[0]))
+    for k in FIELDS:
+        setattr(out, k, np.concatenate([dm[k], stars[k]]).astype(np.float32))
+    out.id = np.concatenate([dm["id"], stars["id"]]).astype(np.int32)
+    out.n = out.x.shape[0]
+    return out
+
+
+def write_masclet(directory: str, it: int, t: float, zeta: float, mp: float, levels: list,
+                  stars: list | None = None, nbh: list | None = None) -> None:
+    """Writes a MASCLET output in the layout read_masclet reads.  levels[ir]
+    holds the dark matter of level ir (x..vz and id; m too for ir >= 1) and,
+    for ir >= 1, npatch; stars[ir] (x..m, and id for ir >= 1) the stars; nbh
+    the black-hole counts per level (their records hold zeros).  The grid
+    records (densities, patch geometry) hold placeholders: the reader skips
+    them."""
+    import os
+    os.makedirs(directory, exist_ok=True)
+    tag = "%05d" % it
+    nl = len(levels) - 1
+    nbh = nbh if nbh is not None else [0] * (nl + 1)
+    sts = stars if stars is not None else [None] * (nl + 1)
+    nst = [0 if s is None else int(np.asarray(s["x"]).shape[0]) for s in sts]
+    npatch = [0] + [int(levels[ir]["npatch"]) for ir in range(1, nl + 1)]
+    with open(os.path.join(directory, "grids" + tag), "w") as f:
+        f.write(f" {it} {t!r} {nl} {float(np.float32(mp))!r}\n {zeta!r}\n")
+        f.write(f" 0 {int(np.asarray(levels[0]['x']).shape[0])} {nst[0]}\n")
+        for ir in range(1, nl + 1):
+            f.write(f" {ir} {npatch[ir]} {int(np.asarray(levels[ir]['x']).shape[0])} {nst[ir]} {nbh[ir]}\n")
+            f.write(" ------\n")
+            for p in range(npatch[ir]):
+                f.write(" 8 8 8\n 1 1 1\n 0.0 0.0 0.0\n 0\n")
+    dens = np.zeros(8, np.float32).tobytes()
+    with open(os.path.join(directory, "cldm" + tag), "wb") as f:
+        write_record(f, struct.pack("<ifff", it, t, 0.0, zeta))
+        write_record(f, dens)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            write_record(f, np.ascontiguousarray(levels[0][k], np.float32).tobytes())
+        write_record(f, np.ascontiguousarray(levels[0]["id"], np.int32).tobytes())
+        for ir in range(1, nl + 1):
+            for _ in range(npatch[ir]):
+                write_record(f, dens)
+            for k in FIELDS:
+                write_record(f, np.ascontiguousarray(levels[ir][k], np.float32).tobytes())
+            write_record(f, np.ascontiguousarray(levels[ir]["id"], np.int32).tobytes())
+    if stars is None:
+        return
+    with open(os.path.join(directory, "clst" + tag), "wb") as f:
+        write_record(f, struct.pack("<iff", it, t, zeta))
+        write_record(f, dens)
+        for k in FIELDS:
+            write_record(f, np.ascontiguousarray(sts[0][k], np.float32).tobytes())
+        write_record(f, dens)
+        write_record(f, dens)
+        for ir in range(1, nl + 1):
+            for _ in range(npatch[ir]):
+                write_record(f, dens)
+            s = sts[ir]
+            for k in FIELDS:
+                write_record(f, np.ascontiguousarray(s[k] if s is not None else [], np.float32).tobytes())
+            write_record(f, dens)
+            write_record(f, dens)
+            write_record(f, np.ascontiguousarray(s["id"] if s is not None else [], np.int32).tobytes())
+            z = np.zeros(nbh[ir], np.float32).tobytes()
+            for _ in range(7):
+                write_record(f, z)
+            write_record(f, z)
+            write_record(f, np.zeros(nbh[ir], np.int32).tobytes())
