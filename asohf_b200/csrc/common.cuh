@@ -136,6 +136,9 @@ struct asohf_ctx {
   // the last RADX(0:NX+1) the layer was given (h_radx: its host copy)
   float* d_s2 = nullptr;
   int s2_nx = 0;
+  // the FFT convolution's twiddle table W_N^j, j < tw_n
+  float2* d_tw = nullptr;
+  int tw_n = 0;
   float* d_radx = nullptr;
   float* h_radx = nullptr;
   int radx_n = 0;

@@ -268,6 +268,7 @@ extern "C" int asohf_destroy(asohf_ctx* c) {
   cudaFree(c->rows[0]);
   cudaFree(c->rows[1]);
   cudaFree(c->d_s2);
+  cudaFree(c->d_tw);
   cudaFree(c->d_radx);
   free(c->h_radx);
   cudaFree(c->d_ndmpart_x);

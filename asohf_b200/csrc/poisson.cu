@@ -4,10 +4,12 @@
 // The reference packs the real density into a full complex array and runs a
 // complex FFT (Numerical-Recipes FOURN) forward, multiplies by KKK, inverse,
 // real part / N^3.  For real input that is exactly an R2C / C2R pair on the
-// half spectrum, which is what cuFFT runs here; the Green's function
-// KKK = -(DX/2)^2 / sum sin^2(pi k/N) (KKK(1,1,1) from the 1e30 denominator)
-// and the 1/N^3 normalisation are applied in one pass over the half
-// spectrum.
+// half spectrum.  For NX in {64, 128, 256, 512} it runs as cuFFT's 2-D R2C
+// of the planes, one hand-written pass doing the z transforms and the
+// Green's multiply (fftconv.cu), and cuFFT's 2-D C2R; for other sizes as a
+// cuFFT 3-D pair with the Green's function KKK = -(DX/2)^2 / sum
+// sin^2(pi k/N) (KKK(1,1,1) from the 1e30 denominator) and the 1/N^3
+// normalisation applied in one pass over the half spectrum (k_green).
 #include <cufft.h>
 #include <math.h>
 #include <stdlib.h>
@@ -19,6 +21,7 @@
 
 #include "common.cuh"
 
+int fftconv_z_green_2d(asohf_ctx* c, int nx, int batch, void* spec, const float* s2, float del2, float inv_n3);
 int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* dradx, int batch,
                          int64_t n_per, const float* x, const float* y, const float* z,
                          const float* m, float denbas, float* acc);
@@ -34,18 +37,22 @@ int tsc_base_batched_f32(asohf_ctx* c, int nx, float xl, float dx, const float* 
 
 struct FftPlan {
   int nx = 0, batch = 0;
-  cufftHandle r2c = 0, c2r = 0;
+  cufftHandle r2c = 0, c2r = 0;      // 3-D, batch copies
+  cufftHandle r2c2 = 0, c2r2 = 0;    // 2-D over the batch * nx planes
   cudaStream_t stream = 0;
 };
 
 static FftPlan g_plans[8];
 
+// the sizes the fused z pass covers (fftconv.cu); the others take 3-D transforms
+static bool fftconv_size(int nx) { return nx == 64 || nx == 128 || nx == 256 || nx == 512; }
+
 static int get_plan(asohf_ctx* c, int nx, int batch, FftPlan** out) {
   for (auto& p : g_plans)
     if (p.nx == nx && p.batch == batch) {
       if (p.stream != c->stream) {
-        ASOHF_CUFFT(cufftSetStream(p.r2c, c->stream));
-        ASOHF_CUFFT(cufftSetStream(p.c2r, c->stream));
+        for (cufftHandle h : {p.r2c, p.c2r, p.r2c2, p.c2r2})
+          if (h) ASOHF_CUFFT(cufftSetStream(h, c->stream));
         p.stream = c->stream;
       }
       *out = &p;
@@ -56,16 +63,25 @@ static int get_plan(asohf_ctx* c, int nx, int batch, FftPlan** out) {
     if (p.nx == 0) { slot = &p; break; }
   if (!slot) {
     slot = &g_plans[0];
-    cufftDestroy(slot->r2c);
-    cufftDestroy(slot->c2r);
+    for (cufftHandle h : {slot->r2c, slot->c2r, slot->r2c2, slot->c2r2})
+      if (h) cufftDestroy(h);
     *slot = FftPlan();
   }
-  int n[3] = {nx, nx, nx};
-  int64_t g = (int64_t)nx * nx * nx, gc = (int64_t)nx * nx * (nx / 2 + 1);
-  ASOHF_CUFFT(cufftPlanMany(&slot->r2c, 3, n, nullptr, 1, (int)g, nullptr, 1, (int)gc, CUFFT_R2C, batch));
-  ASOHF_CUFFT(cufftPlanMany(&slot->c2r, 3, n, nullptr, 1, (int)gc, nullptr, 1, (int)g, CUFFT_C2R, batch));
-  ASOHF_CUFFT(cufftSetStream(slot->r2c, c->stream));
-  ASOHF_CUFFT(cufftSetStream(slot->c2r, c->stream));
+  if (fftconv_size(nx)) {  // 2-D transforms of the batch * nx planes
+    int n2[2] = {nx, nx};
+    int64_t g2 = (int64_t)nx * nx, gc2 = (int64_t)nx * (nx / 2 + 1);
+    ASOHF_CUFFT(cufftPlanMany(&slot->r2c2, 2, n2, nullptr, 1, (int)g2, nullptr, 1, (int)gc2, CUFFT_R2C, batch * nx));
+    ASOHF_CUFFT(cufftPlanMany(&slot->c2r2, 2, n2, nullptr, 1, (int)gc2, nullptr, 1, (int)g2, CUFFT_C2R, batch * nx));
+    ASOHF_CUFFT(cufftSetStream(slot->r2c2, c->stream));
+    ASOHF_CUFFT(cufftSetStream(slot->c2r2, c->stream));
+  } else {
+    int n[3] = {nx, nx, nx};
+    int64_t g = (int64_t)nx * nx * nx, gc = (int64_t)nx * nx * (nx / 2 + 1);
+    ASOHF_CUFFT(cufftPlanMany(&slot->r2c, 3, n, nullptr, 1, (int)g, nullptr, 1, (int)gc, CUFFT_R2C, batch));
+    ASOHF_CUFFT(cufftPlanMany(&slot->c2r, 3, n, nullptr, 1, (int)gc, nullptr, 1, (int)g, CUFFT_C2R, batch));
+    ASOHF_CUFFT(cufftSetStream(slot->r2c, c->stream));
+    ASOHF_CUFFT(cufftSetStream(slot->c2r, c->stream));
+  }
   slot->nx = nx;
   slot->batch = batch;
   slot->stream = c->stream;
@@ -156,13 +172,25 @@ static int poisson_dev(asohf_ctx* c, int nx, float dx, int batch, const float* r
   if (!spec) return ASOHF_ERR_CAPACITY;
   const float* ds2;
   ASOHF_CHECK(green_table(c, nx, &ds2));
+  float del2 = (dx * 0.5f) * (dx * 0.5f);
+  float inv_n3 = 1.0f / ((float)nx * (float)nx * (float)nx);
   FftPlan* P;
   ASOHF_CHECK(get_plan(c, nx, batch, &P));
+  if (fftconv_size(nx)) {
+    // 2-D R2C of the planes, the fused z pass (fftconv.cu), 2-D C2R
+    int kt2 = ktime_begin(c, "fft_r2c_2d");
+    ASOHF_CUFFT(cufftExecR2C(P->r2c2, (cufftReal*)rho, spec));
+    ktime_end(c, kt2);
+    ASOHF_CHECK(fftconv_z_green_2d(c, nx, batch, spec, ds2, del2, inv_n3));
+    kt2 = ktime_begin(c, "fft_c2r_2d");
+    ASOHF_CUFFT(cufftExecC2R(P->c2r2, spec, (cufftReal*)pot));
+    ktime_end(c, kt2);
+    ASOHF_CUDA(cudaGetLastError());
+    return ASOHF_OK;
+  }
   int kt_ = ktime_begin(c, "fft_r2c");
   ASOHF_CUFFT(cufftExecR2C(P->r2c, (cufftReal*)rho, spec));
   ktime_end(c, kt_);
-  float del2 = (dx * 0.5f) * (dx * 0.5f);
-  float inv_n3 = 1.0f / ((float)nx * (float)nx * (float)nx);
   {
     int kt_ = ktime_begin(c, "green_multiply");
     const int64_t total = (int64_t)batch * nx * nx * (nx / 2 + 1);
