@@ -151,7 +151,9 @@ int asohf_interpolate_density_tsc(asohf_ctx *ctx, int nx, float lado0, float dx,
 
 /* MOMENTO + POFFT3D (poisson.f:98-249): periodic potential of `batch`
  * fields rho (NX^3 each) into pot.  Green's function -(DX/2)^2/sum sin^2,
- * zero mode from the 1e30 denominator. */
+ * zero mode from the 1e30 denominator.  Each field is solved on its own
+ * (no rounding of one reaches another); results equal an FFT solve within
+ * float32 rounding. */
 int asohf_poisson_fft(asohf_ctx *ctx, int nx, float dx, int batch, const float *rho,
                       float *pot, int on_device);
 
