@@ -230,9 +230,11 @@ int x_order(asohf_ctx* c, const float* dx, int n, int32_t** sidx, float** sx) {
   void* t = arena_alloc(c, tb);
   if (!k0 || !k1 || !v0 || !v1 || !s || !t) return ASOHF_ERR_CAPACITY;
   if (n > 0) {
+    int kt_ = ktime_begin(c, "clean_x_sort");
     k_x_keys<<<(n + 255) / 256, 256, 0, c->stream>>>(dx, n, k0, v0);
     ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, n, 0, 32, c->stream));
     k_sorted_x<<<(n + 255) / 256, 256, 0, c->stream>>>(v1, dx, n, s);
+    ktime_end(c, kt_);
     c->launches += 2;
   }
   *sidx = v1;

@@ -152,7 +152,7 @@ struct asohf_ctx {
   KRec* krec = nullptr;
   int nkrec = 0, capkrec = 0;
   struct KSum { const char* name; double ms; int64_t n; };
-  static constexpr int KSUM_CAP = 160;
+  static constexpr int KSUM_CAP = 256;
   KSum ksum[KSUM_CAP];
   int nksum = 0;
 };

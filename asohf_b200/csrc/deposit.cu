@@ -319,9 +319,13 @@ extern "C" int asohf_sort_dm_particles_localdensity(asohf_ctx* c, int nx, float 
     k_cell_density_general<<<grid_for(g, 256), 256, 0, c->stream>>>(offs, order, c->p.m, g, bas, dens);
     c->launches += 2;
   }
-  k_species<<<grid_for(n, 256), 256, 0, c->stream>>>(cell, dens, n, ASOHF_N_ESP, logf(8.0f), spec);
-  k_species_block_counts<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, bc);
-  ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(tscan, cub_scan, bc, boff, nb * ASOHF_N_ESP, c->stream));
+  {
+    int kt_ = ktime_begin(c, "species_classify");
+    k_species<<<grid_for(n, 256), 256, 0, c->stream>>>(cell, dens, n, ASOHF_N_ESP, logf(8.0f), spec);
+    k_species_block_counts<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, bc);
+    ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(tscan, cub_scan, bc, boff, nb * ASOHF_N_ESP, c->stream));
+    ktime_end(c, kt_);
+  }
   {
     int kt_ = ktime_begin(c, "species_scatter");
     k_species_scatter<<<nb, SPEC_BLOCK, 0, c->stream>>>(spec, n, nb, boff, perm);
@@ -475,11 +479,13 @@ static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B, DAll
   cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, B->start, (int)(nbin + 1));
   void* t = arena_alloc(c, tb);
   if (!binof || !cnt || !B->start || !B->idx || !t) return ASOHF_ERR_CAPACITY;
+  int kt_ = ktime_begin(c, "particle_bins");
   ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (nbin + 1), c->stream));
   k_bin_count<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, *B, binof, cnt);
   ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(t, tb, cnt, B->start, (int)(nbin + 1), c->stream));
   ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (nbin + 1), c->stream));
   k_bin_fill<<<grid_for(n, 256), 256, 0, c->stream>>>(binof, n, B->start, cnt, B->idx);
+  ktime_end(c, kt_);
   c->launches += 2;
   return ASOHF_OK;
 }
@@ -1137,7 +1143,11 @@ extern "C" int asohf_density(asohf_ctx* c, int nx, float lado0, float dx, float 
       c->launches++;
     }
   }
-  k_finish_f64<<<grid_for(g, 256), 256, 0, c->stream>>>(acc, g, denbas, du1);
+  {
+    int kt_ = ktime_begin(c, "density_finish");
+    k_finish_f64<<<grid_for(g, 256), 256, 0, c->stream>>>(acc, g, denbas, du1);
+    ktime_end(c, kt_);
+  }
   c->launches++;
   ASOHF_CUDA(cudaGetLastError());
   if (!on_device) ASOHF_CUDA(cudaMemcpyAsync(u1, du1, 4 * g, cudaMemcpyDeviceToHost, c->stream));

@@ -2334,7 +2334,11 @@ extern "C" int asohf_halofind_particles(asohf_ctx* c, const asohf_consts* k, con
       ASOHF_CHECK(join_all(c));
       ktime_end(c, kt_);
     }
-    k_eigen<<<(ns + 127) / 128, 128, 0, c->stream>>>(sg.eig, d_work, ns, m.d.eigenval);
+    {
+      int kt_ = ktime_begin(c, "halo_eigen");
+      k_eigen<<<(ns + 127) / 128, 128, 0, c->stream>>>(sg.eig, d_work, ns, m.d.eigenval);
+      ktime_end(c, kt_);
+    }
     c->launches++;
     ASOHF_CUDA(cudaGetLastError());
     ASOHF_CUDA(cudaMemcpyAsync(hst, g.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
@@ -3139,10 +3143,14 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
     for (int iter = 0; na > 0 && rc == ASOHF_OK; iter++) {
       if (iter > 200) { rc = ASOHF_ERR_TIMEOUT; break; }
       ASOHF_CUDA(cudaMemcpyAsync(d_act, h_act, 4 * (size_t)na, cudaMemcpyHostToDevice, c->stream));
-      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cx, t_cx);
-      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cy, t_cy);
-      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cz, t_cz);
-      k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.r, t_r);
+      {
+        int kt_ = ktime_begin(c, "sub_jacobi_prep");
+        k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cx, t_cx);
+        k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cy, t_cy);
+        k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.cz, t_cz);
+        k_gather_f<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, pr.r, t_r);
+        ktime_end(c, kt_);
+      }
       c->launches += 4;
       unsigned long long* keys;
       int32_t* vals;
@@ -3156,8 +3164,12 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
                          jo);
         ktime_end(c, kt_);
       }
-      k_jacobi_scatter<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, jo, t_r, f_jjac, f_masadm, f_rclus,
-                                                                f_rlast);
+      {
+        int kt_ = ktime_begin(c, "sub_jacobi_scatter");
+        k_jacobi_scatter<<<(na + 255) / 256, 256, 0, c->stream>>>(d_act, na, jo, t_r, f_jjac, f_masadm, f_rclus,
+                                                                  f_rlast);
+        ktime_end(c, kt_);
+      }
       c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       ASOHF_CUDA(cudaMemcpyAsync(h_done, jo.done, 4 * (size_t)na, cudaMemcpyDeviceToHost, c->stream));
@@ -3178,7 +3190,9 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       if (fin_total > fin0) {
         ASOHF_CHECK(sfin_reserve(c, fin_total, fin0));
         ASOHF_CUDA(cudaMemcpyAsync(d_ids_off, h_dst.data(), 8 * (size_t)na, cudaMemcpyHostToDevice, c->stream));
+        int kt_ = ktime_begin(c, "sub_keep_segments");
         k_copy_segments<<<na, 256, 0, c->stream>>>(keys, vals, d_off, d_konta, d_ids_off, c->sfin_k, c->sfin_v);
+        ktime_end(c, kt_);
         c->launches++;
         ASOHF_CUDA(cudaGetLastError());
       }
@@ -3207,7 +3221,9 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
       ASOHF_CUDA(cudaMemcpyAsync(d_konta, h_st, 4 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
       ASOHF_CUDA(cudaMemcpyAsync(d_off, h_off, 8 * (size_t)(ns + 1), cudaMemcpyHostToDevice, c->stream));
       if (T > 0) {
+        int kt_ = ktime_begin(c, "sub_final_segments");
         k_copy_segments<<<ns, 256, 0, c->stream>>>(c->sfin_k, c->sfin_v, d_src, d_konta, d_ids_off, keys, vals);
+        ktime_end(c, kt_);
         c->launches++;
       }
       ASOHF_CUDA(cudaGetLastError());
@@ -3254,7 +3270,11 @@ extern "C" int asohf_substructure_particles(asohf_ctx* c, const asohf_consts* k,
         LAUNCH_TIERS_CTA(k_sub_main_g, ts, S, H, m.d, d_work, in, sg);
         ktime_end(c, kt_);
       }
-      k_eigen<<<(ns + 127) / 128, 128, 0, c->stream>>>(sg.eig, d_work, ns, m.d.eigenval);
+      {
+        int kt_ = ktime_begin(c, "sub_eigen");
+        k_eigen<<<(ns + 127) / 128, 128, 0, c->stream>>>(sg.eig, d_work, ns, m.d.eigenval);
+        ktime_end(c, kt_);
+      }
       c->launches++;
       ASOHF_CUDA(cudaGetLastError());
       ASOHF_CUDA(cudaMemcpyAsync(h_st, pr.status, 4 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));

@@ -129,7 +129,11 @@ int build_column_index(asohf_ctx* c, int nx, float lado0) {
   int32_t* v1 = (int32_t*)arena_alloc(c, 4 * n);
   void* t = arena_alloc(c, tb);
   if (!k0 || !k1 || !v0 || !v1 || !t) return ASOHF_ERR_CAPACITY;
-  k_colkeys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.y, c->p.z, n, c->col_xl, c->col_dx, ncol, k0, v0);
+  {
+    int kt_ = ktime_begin(c, "column_index_keys");
+    k_colkeys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.y, c->p.z, n, c->col_xl, c->col_dx, ncol, k0, v0);
+    ktime_end(c, kt_);
+  }
   int kt_ = ktime_begin(c, "column_index_radix");
   ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)n, 0, bits, c->stream));
   ktime_end(c, kt_);
@@ -181,17 +185,25 @@ extern "C" int asohf_sort_dm_particles_x(asohf_ctx* c, int nx, float lado0, int3
     int64_t* perm = (int64_t*)arena_alloc(c, 8 * n);
     void* t = arena_alloc(c, tb);
     if (!k0 || !k1 || !v0 || !v1 || !perm || !t) return ASOHF_ERR_CAPACITY;
+    int kt_ = ktime_begin(c, "sort_x_keys");
     k_xkeys_reversed<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, n, k0, v0);
-    int kt_ = ktime_begin(c, "sort_x_radix");
+    ktime_end(c, kt_);
+    kt_ = ktime_begin(c, "sort_x_radix");
     ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tb, k0, k1, v0, v1, (int)n, 0, 32, c->stream));
     ktime_end(c, kt_);
+    kt_ = ktime_begin(c, "sort_x_widen");
     k_widen<<<grid_for(n, 256), 256, 0, c->stream>>>(v1, n, perm);
+    ktime_end(c, kt_);
     c->launches += 2;
     ASOHF_CHECK(permute_store(c, perm));
   }
   float xl = -lado0 / 2.0f;
   float dxl = lado0 / (float)nx;
-  k_ndmpart_x<<<(nx + 1 + 255) / 256, 256, 0, c->stream>>>(c->p.x, n, nx, xl, dxl, c->d_ndmpart_x);
+  {
+    int kt_ = ktime_begin(c, "ndmpart_x");
+    k_ndmpart_x<<<(nx + 1 + 255) / 256, 256, 0, c->stream>>>(c->p.x, n, nx, xl, dxl, c->d_ndmpart_x);
+    ktime_end(c, kt_);
+  }
   c->launches++;
   ASOHF_CUDA(cudaGetLastError());
   arena_reset(c);

@@ -259,6 +259,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs: only the device-timed steps)")
     ap.add_argument("--no-grid", action="store_true", help="skip the grid halo finder leg")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default size-tier thresholds (no launch-shape tuning before the timed steps)")
     ap.add_argument("--layer-only", action="store_true",
                     help="only the deposit+Poisson layer leg (profiling runs of its kernels)")
     args = ap.parse_args()
@@ -295,7 +297,7 @@ def main():
     import torch
     import torch.distributed as dist
     from types import SimpleNamespace
-    from asohf_b200 import api, driver, synth
+    from asohf_b200 import api, autotune, driver, synth
 
     torch.cuda.set_device(local)
     # the hot path on a high-priority stream: the library's size-tier streams
@@ -315,6 +317,14 @@ def main():
     with_subs = not args.no_subs
     b = api.DeviceBackend(local)
     b.a.set_stream(torch.cuda.current_stream().cuda_stream)
+    # the size-tier thresholds: tuned on this workload before the timed steps
+    # (coordinate descent, 2 timed runs per setting, the chosen setting's
+    # catalogue checked against the defaults'), or the defaults
+    launch = {"setting": dict(autotune.DEFAULTS), "tuned": False}
+    if not args.no_tune:
+        best, ms_best, trials = autotune.tune_plan(plan, b, with_subs=with_subs, reps=2, rounds=1)
+        launch = {"setting": best, "tuned": True, "settings_timed": len(trials),
+                  "ms_chosen": round(ms_best, 2), "ms_defaults": round(trials[0][1], 2)}
 
     def step():
         return driver.execute(plan, b, with_subs=with_subs, download=False)
@@ -356,6 +366,7 @@ def main():
                                   vy=host[4].numpy(), vz=host[5].numpy(), m=host[6].numpy(), id=host[7].numpy(), n=n)
         be = api.GpuBackend(local)
         be.a.set_stream(torch.cuda.current_stream().cuda_stream)
+        autotune.apply(be.a, launch["setting"])
 
         def step_e2e():
             return driver.execute(plan, be, with_subs=with_subs, particles=parts_h, download=False)
@@ -420,6 +431,7 @@ def main():
                    "global_batch": world * n, "parallelism": f"replicas x{world}",
                    "l2": "inputs > L2 (4.3 GB of particles per step)"},
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": int(launches),
+        "launch_shape": launch,
         "device_memory_in_use_gb": round((total_b - free_b) / 1e9, 2),
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in
                                 sorted(kstats.items(), key=lambda kv: -kv[1][0])
