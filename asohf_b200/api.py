@@ -62,7 +62,7 @@ def load():
                      "asohf_work_counters", "asohf_set_cluster_threshold", "asohf_set_group_tiers",
                      "asohf_copy_to_host_sm", "asohf_set_cluster_share", "asohf_prefetch_particles",
                      "asohf_copy_to_host_async", "asohf_copy_wait",
-                     "asohf_check_rubish", "asohf_accidental_substructure"]:
+                     "asohf_check_rubish", "asohf_accidental_substructure", "asohf_re_sort_haloes"]:
             getattr(L, name).restype = C.c_int
         _LIB = L
     return _LIB
@@ -372,6 +372,21 @@ class Asohf:
                                                     C.byref(n)), "ACCIDENTAL_SUBSTRUCTURE")
         return n.value
 
+    def re_sort_haloes(self, cat, nhallev, ir):
+        """RE_SORT_HALOES (haloes_particles.f:2-56) on the host catalogue:
+        drops the REALCLUS = 0 entries of level ir in order; nhallev[ir] and
+        cat.nclus are updated; returns the window's keep mask."""
+        nh = np.array(nhallev, np.int32)
+        w = int(nh[ir])
+        keep = np.zeros(max(w, 1), np.uint8)
+        cc = cat.as_c()
+        _check(self.L.asohf_re_sort_haloes(self.h, C.byref(cc), nh.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           C.c_int(ir), keep.ctypes.data_as(C.POINTER(C.c_uint8))),
+               "RE_SORT_HALOES")
+        nhallev[ir] = nh[ir]
+        cat.nclus = cc.nclus
+        return keep[:w].astype(bool) if w else np.zeros(0, bool)
+
     def overlapping(self, cat, ir, nhallev, vol_solap_low):
         """OVERLAPPING at level ir (nhallev[l]: haloes of level l); returns
         the number of removed haloes among level ir's."""
@@ -591,6 +606,9 @@ class GpuBackend:
 
     def accidental_substructure(self, cat):
         return self.a.accidental_substructure(cat)
+
+    def re_sort_haloes(self, cat, nhallev, ir):
+        return self.a.re_sort_haloes(cat, nhallev, ir)
 
     def overlapping(self, cat, ir, nhallev, vol_solap_low):
         return self.a.overlapping(cat, ir, nhallev, vol_solap_low)

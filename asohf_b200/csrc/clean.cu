@@ -638,3 +638,47 @@ extern "C" int asohf_overlapping(asohf_ctx* c, asohf_catalogue* cat, int ir, con
   if (removed) *removed = z;
   return ASOHF_OK;
 }
+
+// RE_SORT_HALOES (haloes_particles.f:2-56) on the host arrays: one pass over
+// the level's window moving the kept entries down; the renumbering uses the
+// final old->new map of the window (the Fortran's RESORT(REALCLUS(I)) is
+// undefined where REALCLUS points past I or at a dropped entry).
+extern "C" int asohf_re_sort_haloes(asohf_ctx* c, asohf_catalogue* cat, int32_t* nhallev, int ir, uint8_t* keep) {
+  if (!c || !cat || !nhallev || ir < 0) return ASOHF_ERR_INVALID;
+  int64_t low1 = 1, low2 = 0;
+  for (int l = 0; l < ir; l++) low1 += nhallev[l];
+  low2 = low1 - 1 + nhallev[ir];
+  if (nhallev[ir] < 0 || low2 > cat->capacity || low1 < 1) return ASOHF_ERR_INVALID;
+  const int64_t w = low2 - low1 + 1;
+  std::vector<int32_t> resort((size_t)(w > 0 ? w : 1), 0);
+  int64_t j = low1 - 1;  // 0-based destination
+  for (int64_t i = low1 - 1; i < low2; i++) {
+    const bool k = cat->realclus[i] != 0;
+    if (keep) keep[i - (low1 - 1)] = k ? 1 : 0;
+    if (k) resort[(size_t)(i - (low1 - 1))] = (int32_t)(++j);  // 1-based new position
+  }
+  const int64_t kept = j - (low1 - 1);
+  if (kept != w) {
+    j = low1 - 1;
+    for (int64_t i = low1 - 1; i < low2; i++) {
+      const int32_t rc = cat->realclus[i];
+      if (rc == 0) continue;
+      cat->clusrx[j] = cat->clusrx[i];
+      cat->clusry[j] = cat->clusry[i];
+      cat->clusrz[j] = cat->clusrz[i];
+      cat->radio[j] = cat->radio[i];
+      cat->masa[j] = cat->masa[i];
+      cat->levhal[j] = cat->levhal[i];
+      cat->patchclus[j] = cat->patchclus[i];
+      cat->dmpclus[j] = cat->dmpclus[i];
+      cat->clusrxcm[j] = cat->clusrxcm[i];
+      cat->clusrycm[j] = cat->clusrycm[i];
+      cat->clusrzcm[j] = cat->clusrzcm[i];
+      cat->realclus[j] = (rc > 0 && rc >= low1 && rc <= low2) ? resort[(size_t)(rc - low1)] : rc;
+      j++;
+    }
+  }
+  nhallev[ir] = (int32_t)kept;
+  cat->nclus = (int32_t)(low1 - 1 + kept);
+  return ASOHF_OK;
+}

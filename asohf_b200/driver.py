@@ -153,11 +153,12 @@ def execute(plan: Plan, backend, with_subs: bool = True, interp_degree: int = 2,
         cat.nclus = s0 + n_new
         nhallev[ir] = n_new
         truth = cand.truth[lo:hi]
-        truth = truth[re_sort_haloes(cat, nhallev, ir)]
+        resort = getattr(backend, "re_sort_haloes", re_sort_haloes)
+        truth = truth[resort(cat, nhallev, ir)]
         low1 = int(nhallev[:ir].sum()) + 1
         low2 = int(nhallev[: ir + 1].sum())
         backend.prune_poor_haloes(consts, cat, low1, low2, np.float32(1.0), 1)
-        truth = truth[re_sort_haloes(cat, nhallev, ir)]
+        truth = truth[resort(cat, nhallev, ir)]
         low1 = int(nhallev[:ir].sum()) + 1
         low2 = int(nhallev[: ir + 1].sum())
         known = truth >= 0

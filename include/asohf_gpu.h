@@ -244,6 +244,16 @@ int asohf_check_rubish(asohf_ctx *ctx, asohf_catalogue *cat, int nclus, int low1
  * requirement.  *removed (may be NULL) receives KONTA. */
 int asohf_accidental_substructure(asohf_ctx *ctx, asohf_catalogue *cat, int nclus, int on_device,
                                   int32_t *removed);
+/* RE_SORT_HALOES (haloes_particles.f:2-56), host arrays: the entries of
+ * level ir (LOWH1 = SUM(NHALLEV(0:ir-1))+1 .. LOWH2 = SUM(NHALLEV(0:ir));
+ * nhallev: host array of ir+1 counts) with REALCLUS = 0 are dropped, the
+ * others moved down in order (CLUSRX/Y/Z, RADIO, MASA, LEVHAL, PATCHCLUS,
+ * DMPCLUS, CLUSRX/Y/ZCM; the catalogue has no HALBORDERS), and a positive
+ * REALCLUS inside the window renumbered to its entry's new position (0
+ * when that entry was dropped; outside the window it is kept).
+ * NHALLEV(ir) and NCLUS receive the counts.  keep (may be NULL; LOWH2 -
+ * LOWH1 + 1 bytes) receives 1 for the kept entries, 0 for the dropped. */
+int asohf_re_sort_haloes(asohf_ctx *ctx, asohf_catalogue *cat, int32_t *nhallev, int ir, uint8_t *keep);
 /* OVERLAPPING (haloes_grids.f:27-201), called by the grid finder at the end
  * of each level (haloes_grids.f:577, 1081): over the haloes 1..lowh2, with
  * the new level lowh3..lowh2 (lowh3 = SUM(NHALLEV(0:ir-1))+1, lowh2 =
