@@ -432,25 +432,17 @@ __device__ __forceinline__ int bin_of(float v, float xl, float bsz, int nb) {
   return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
 }
 
-__global__ void k_bin_count(const float* __restrict__ x, const float* __restrict__ y,
-                            const float* __restrict__ z, int64_t n, Bins B, int32_t* __restrict__ binof,
-                            int32_t* __restrict__ cnt) {
+// bin key and index of every particle, and the bin counts
+__global__ void k_bin_keys(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                           int64_t n, Bins B, uint32_t* __restrict__ keys, int32_t* __restrict__ vals,
+                           int32_t* __restrict__ cnt) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int b = (bin_of(z[i], B.xl, B.bsz, B.nb) * B.nb + bin_of(y[i], B.xl, B.bsz, B.nb)) * B.nb +
             bin_of(x[i], B.xl, B.bsz, B.nb);
-    binof[i] = b;
+    keys[i] = (uint32_t)b;
+    vals[i] = (int32_t)i;
     atomicAdd(&cnt[b], 1);
-  }
-}
-
-__global__ void k_bin_fill(const int32_t* __restrict__ binof, int64_t n, const int32_t* __restrict__ start,
-                           int32_t* __restrict__ fill, int32_t* __restrict__ idx) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int b = binof[i];
-    int pos = start[b] + atomicAdd(&fill[b], 1);
-    idx[pos] = (int32_t)i;
   }
 }
 
@@ -462,6 +454,23 @@ struct DAlloc {
   void* get(size_t bytes) const { return pool ? dpool_alloc(c, 0, bytes) : arena_alloc(c, bytes); }
 };
 
+// start[b] = first position of bin b (count and exclusive scan), idx = the
+// particles grouped by bin (a stable radix sort of (bin, index): ascending
+// index within a bin, the same grouping on every run).
+static int bin_key_bits(int64_t nbin) {
+  int bits = 1;
+  while ((1ll << bits) < nbin) bits++;
+  return bits;
+}
+
+static void bins_temp(int64_t n, int64_t nbin, size_t* scan_b, size_t* sort_b) {
+  *scan_b = 0;
+  *sort_b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, *scan_b, (int32_t*)nullptr, (int32_t*)nullptr, (int)(nbin + 1));
+  cub::DeviceRadixSort::SortPairs(nullptr, *sort_b, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
+                                  (int32_t*)nullptr, (int)(n > 0 ? n : 1), 0, bin_key_bits(nbin));
+}
+
 static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B, DAlloc A = DAlloc{nullptr, false}) {
   int64_t n = c->p.n;
   int nx = (int)lrintf(lado0 / dx);
@@ -471,32 +480,36 @@ static int build_bins(asohf_ctx* c, float lado0, float dx, int bw, Bins* B, DAll
   B->nb = nb;
   B->xl = -lado0 / 2.0f;
   B->bsz = lado0 / (float)nb;
-  int32_t* binof = (int32_t*)arena_alloc(c, 4 * n);
+  uint32_t* k0 = (uint32_t*)arena_alloc(c, 4 * n + 4);
+  uint32_t* k1 = (uint32_t*)arena_alloc(c, 4 * n + 4);
+  int32_t* v0 = (int32_t*)arena_alloc(c, 4 * n + 4);
   int32_t* cnt = (int32_t*)arena_alloc(c, 4 * (nbin + 1));
   B->start = (int32_t*)(A.pool ? A.get(4 * (nbin + 1)) : arena_alloc(c, 4 * (nbin + 1)));
-  B->idx = (int32_t*)arena_alloc(c, 4 * n);
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, B->start, (int)(nbin + 1));
-  void* t = arena_alloc(c, tb);
-  if (!binof || !cnt || !B->start || !B->idx || !t) return ASOHF_ERR_CAPACITY;
+  B->idx = (int32_t*)arena_alloc(c, 4 * n + 4);
+  size_t ts, tr;
+  bins_temp(n, nbin, &ts, &tr);
+  void* t = arena_alloc(c, ts > tr ? ts : tr);
+  if (!k0 || !k1 || !v0 || !cnt || !B->start || !B->idx || !t) return ASOHF_ERR_CAPACITY;
   int kt_ = ktime_begin(c, "particle_bins");
   ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (nbin + 1), c->stream));
-  k_bin_count<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, *B, binof, cnt);
-  ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(t, tb, cnt, B->start, (int)(nbin + 1), c->stream));
-  ASOHF_CUDA(cudaMemsetAsync(cnt, 0, 4 * (nbin + 1), c->stream));
-  k_bin_fill<<<grid_for(n, 256), 256, 0, c->stream>>>(binof, n, B->start, cnt, B->idx);
+  k_bin_keys<<<grid_for(n, 256), 256, 0, c->stream>>>(c->p.x, c->p.y, c->p.z, n, *B, k0, v0, cnt);
+  ASOHF_CUDA(cub::DeviceScan::ExclusiveSum(t, ts, cnt, B->start, (int)(nbin + 1), c->stream));
+  if (n > 0)
+    ASOHF_CUDA(cub::DeviceRadixSort::SortPairs(t, tr, k0, k1, v0, B->idx, (int)n, 0, bin_key_bits(nbin),
+                                               c->stream));
   ktime_end(c, kt_);
-  c->launches += 2;
+  c->launches++;
   return ASOHF_OK;
 }
 
 static size_t bins_bytes(int64_t n, float lado0, float dx, int bw) {
   int nx = (int)lrintf(lado0 / dx);
   int nb = (nx + bw - 1) / bw;
+  if (nb < 1) nb = 1;
   int64_t nbin = (int64_t)nb * nb * nb;
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, (int32_t*)nullptr, (int32_t*)nullptr, (int)(nbin + 1));
-  return 8 * (size_t)n + 8 * (size_t)(nbin + 1) + tb + 4096;
+  size_t ts, tr;
+  bins_temp(n, nbin, &ts, &tr);
+  return 16 * (size_t)n + 8 * (size_t)(nbin + 1) + (ts > tr ? ts : tr) + 8192;
 }
 
 // Device copy of the patch table.
