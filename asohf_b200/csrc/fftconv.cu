@@ -22,12 +22,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
-#include <cooperative_groups.h>
 #include <vector>
 
 #include "common.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace {
 
@@ -41,8 +38,9 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 
-// index with one pad element per 32: the scattered writes of a transform's
-// output (stride R across lanes) then take two wavefronts, as a row does
+// index of a line element in shared memory, one pad element per 32: with an
+// odd line stride, the tile's loads (one element of each of 16 lines) and a
+// warp's reads along its line are free of bank conflicts
 __host__ __device__ constexpr int pad(int f) { return f + (f >> 5); }
 
 __host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v >> 1); }
