@@ -12,6 +12,9 @@ subhaloes); inputs (4.3 GB of particles) are far larger than L2.
   e2e    particles/s through the same public API from pinned host arrays,
          host->device copy of the particles and device->host copy of the
          catalogue and IDs inside the timed region.
+Before the timed steps the size-tier thresholds of the per-halo kernels are
+tuned on the workload itself (asohf_b200/autotune.py; --no-tune keeps the
+defaults); the line names the setting used (launch_shape).
 Multi-GPU: the path does not exchange data, so every rank runs a replica
 on its own snapshot (weak scaling).
 
