@@ -786,7 +786,7 @@ __device__ __forceinline__ void density_patch_item(const int2 it, const DevMesh&
     int a = threadIdx.x % 3 - 1, b = (threadIdx.x / 3) % 3 - 1, cc = threadIdx.x / 9 - 1;
     s_t27[threadIdx.x] = (double)__fmul_rn(__fmul_rn(__fmul_rn(m0, kc[a]), kc[b]), kc[cc]);
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t v0 = (int64_t)it.y * PSLICE, v1 = v0 + PSLICE;
   int64_t vbase = 0;
   for (int r0 = 0; r0 < g.rows; r0 += PROWS) {
