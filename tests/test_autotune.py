@@ -89,3 +89,12 @@ def test_host_copies_of_tensors():
     assert isinstance(h, np.ndarray) and h.tolist() == [0, 1, 2, 3]
     a = np.arange(3)
     assert at._host(a) is not a and at._host(a).tolist() == [0, 1, 2]
+
+
+
+def test_signature_names_the_workload():
+    from types import SimpleNamespace
+    import numpy as np
+    cfg = SimpleNamespace(name="cfgX", nx=64, nl=3)
+    plan = SimpleNamespace(snap=SimpleNamespace(cfg=cfg, x=np.zeros(10)), cand=SimpleNamespace(clusrx=np.zeros(7)))
+    assert at.signature(plan) == "cfgX:n10:nx64:nl3:c7"
